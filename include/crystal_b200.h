@@ -1,0 +1,163 @@
+/* crystal_b200.h -- C ABI of the B200 execution layer for crystal-sycl's fused
+ * star-join query pipeline (fact scan -> predicate -> dimension perfect-hash
+ * build/probe -> group-by aggregate).
+ *
+ * Every entry point is plain C: pointers, sizes and int status codes; no C++
+ * types and no exceptions cross it.  Functions return CX_OK (0) on success or a
+ * negative CX_E_* code; cx_last_error() then describes the failure (per thread).
+ *
+ * The reference hands generated source to ICompiler::compile and the resulting
+ * library to IExecutor::execute (include/core/execution.h:291-301), both behind
+ * QueryEngine::executeQuery (src/core/execution.cpp:652-725).  The functions
+ * below replace that pair: cx_compile stands where AdaptiveCppCompiler::compile
+ * shelled out to `acpp` (src/core/execution.cpp:114-151), and cx_execute stands
+ * where DynamicLibraryExecutor::execute dlopen()ed the library and called its
+ * `execute_query(ExecutionContext*)` (src/core/execution.cpp:161-192).  The
+ * execution context mirrors db::ExecutionContext's named buffers
+ * (include/core/execution.h:131-282).
+ */
+#ifndef CRYSTAL_B200_H
+#define CRYSTAL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CX_ABI_VERSION 1
+
+enum {
+  CX_OK = 0,
+  CX_E_INVALID = -1,     /* bad argument or plan */
+  CX_E_COMPILE = -2,     /* NVRTC rejected the source (log filled) */
+  CX_E_CUDA = -3,        /* a CUDA runtime/driver call failed */
+  CX_E_MISSING = -4,     /* a buffer the query binds is not in the context */
+  CX_E_CAPACITY = -5,    /* a caller buffer or the memory budget is too small */
+  CX_E_KERNEL = -6,      /* a kernel raised an error code (see cx_ctx_kernel_error) */
+  CX_E_NO_DEVICE = -7,   /* no CUDA device */
+  CX_E_REJECTED = -8     /* admission control refused a request */
+};
+
+typedef struct cx_module cx_module;     /* compiled query: cubin + launch plan */
+typedef struct cx_exec_ctx cx_exec_ctx; /* named device buffers + scratch + timing */
+
+/* Launch shape for generated scan kernels (the autotuner's search space). */
+typedef struct cx_tuning {
+  int block_threads;     /* BLOCK_THREADS, multiple of 32 (default 256) */
+  int items_per_thread;  /* ITEMS_PER_THREAD (default 4) */
+  int stages;            /* TMA staging depth; 0 = read fact columns directly */
+  int ctas_per_sm;       /* persistent CTAs per SM (default 2) */
+  int group_placement;   /* 0 auto, 1 shared-memory group tables, 2 global atomics */
+  int smem_group_budget; /* bytes a shared-memory group table may use */
+} cx_tuning;
+
+/* Shape of a compiled query's result buffer. */
+typedef struct cx_result_info {
+  uint64_t groups;          /* perfect-hash group slots (1 for scalar aggregates) */
+  uint32_t storage_ts;      /* u64 slots per group while aggregating */
+  uint32_t visible_ts;      /* u64 slots per group after finalisation */
+  uint64_t result_words;    /* u64 words the caller's result buffer must hold */
+  uint64_t validity_words;  /* u64 words of the result validity bitmap */
+  uint64_t final_words;     /* u64 words of the final result (groups x ts) */
+  int sparse;               /* 1 = fast sparse output (no validity bits set) */
+  int finalized;            /* 1 = AVG finalisation compacts to visible_ts */
+} cx_result_info;
+
+/* Timing of the last cx_execute on a context (CUDA events, ms). */
+typedef struct cx_timing {
+  float build_ms;  /* memsets + hash-table build kernels */
+  float scan_ms;   /* fused scan/probe/aggregate kernel */
+  float post_ms;   /* epilogue / finalisation kernels */
+  float total_ms;  /* whole execute */
+  int scan_grid;   /* CTAs of the scan launch */
+  int gpu_launches;/* kernels launched by the last execute */
+} cx_timing;
+
+int cx_abi_version(void);
+const char* cx_last_error(void);
+
+/* Default tuning (filled in place). */
+void cx_tuning_default(cx_tuning* t);
+
+/* Generates the CUDA C++ source of a star-join plan (S-expression text; see
+ * the package's plan builder).  Replaces JITOperatorVisitor::generateCode
+ * (src/core/visitor.cpp:4771-4878) for this path.  Writes at most out_cap bytes
+ * (NUL-terminated) and the full length to *out_len; call with out=NULL to size. */
+int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap,
+               size_t* out_len);
+
+/* Compiles generated source with NVRTC for sm_100a into an in-memory cubin and
+ * parses its embedded launch plan.  `key` names the module in the process-wide
+ * cache (the reference keys its cache on "query_" + ABI version + hash(sql),
+ * src/core/execution.cpp:696-697); a hit returns the cached module with its
+ * reference count raised.  On CX_E_COMPILE the NVRTC log goes to `log`.
+ * Replaces ICompiler::compile / AdaptiveCppCompiler::compile. */
+int cx_compile(const char* src, size_t src_len, const char* key, cx_module** out, char* log, size_t log_cap);
+
+/* Drops one reference; the cubin is unloaded when the last one goes. */
+int cx_module_release(cx_module* m);
+
+int cx_module_result_info(const cx_module* m, cx_result_info* info);
+
+/* Execution context: db::ExecutionContext's buffer registry. */
+cx_exec_ctx* cx_ctx_create(void);
+void cx_ctx_destroy(cx_exec_ctx* c);
+/* Registers a device column as "d_<column>" (ctx->buffers_, execution.h:137). */
+int cx_ctx_set_buffer(cx_exec_ctx* c, const char* name, const void* dev_ptr, uint64_t elems);
+/* Registers a column's validity words (bit r = row r valid; ctx->null_bitmaps_). */
+int cx_ctx_set_null_bitmap(cx_exec_ctx* c, const char* name, const uint64_t* dev_words, uint64_t words);
+/* Row count of a table (the reference bakes these in as LO_LEN, C_LEN ...). */
+int cx_ctx_set_table_rows(cx_exec_ctx* c, const char* table, uint64_t rows);
+/* Caller-owned result and validity buffers (ctx->result_buffer_ /
+ * result_validity_buffer_); sizes in u64 words. */
+int cx_ctx_set_result(cx_exec_ctx* c, uint64_t* dev_result, uint64_t result_words, uint64_t* dev_validity,
+                      uint64_t validity_words);
+/* Optional caller-owned scratch for hash tables and group bitmaps.  Without it
+ * the context allocates grow-only scratch itself (the reference's
+ * getScratchIntBuffer high-water reuse, execution.h:186-207). */
+int cx_ctx_set_scratch(cx_exec_ctx* c, void* dev_ptr, uint64_t bytes);
+/* Bytes of scratch `m` needs under the context's current table sizes. */
+int cx_module_scratch_bytes(const cx_module* m, const cx_exec_ctx* c, uint64_t* bytes);
+/* Overrides the multiprocessor count used to size persistent grids (0 = device's). */
+int cx_ctx_set_sm_count(cx_exec_ctx* c, int sms);
+
+/* Enqueues the query on `stream` (a cudaStream_t; NULL = legacy default
+ * stream).  Asynchronous: call cx_ctx_sync before reading results.  Replaces
+ * IExecutor::execute / DynamicLibraryExecutor::execute. */
+int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream);
+/* Waits for the context's last execute, reads its device error word and fills
+ * timing.  Returns CX_E_KERNEL if a kernel raised an error. */
+int cx_ctx_sync(cx_exec_ctx* c);
+int cx_ctx_timing(const cx_exec_ctx* c, cx_timing* t);
+/* Error code raised by a kernel in the last execute (0 = none; 1 = staging
+ * wait timeout; 2 = GROUP BY key outside its catalog domain). */
+int cx_ctx_kernel_error(const cx_exec_ctx* c, uint32_t* code);
+
+/* Sparse-result compaction: copies every group tuple with a non-zero slot to
+ * `dst` in group order and writes the row count to *dev_count (device u64).
+ * Same rows as the reference's CompactSparseAggregateResult
+ * (src/db/database_instance.cpp:286-307), deterministic order. */
+int cx_compact_sparse(const uint64_t* dev_src, uint64_t groups, uint32_t tuple_size, uint64_t* dev_dst,
+                      uint64_t* dev_count, void* stream);
+
+/* Seeded synthetic column generator (device; no reference counterpart: the
+ * reference loads SSB dbgen output from disk, include/crystal/utils.h:242-253).
+ * Row r of generator stream `gen_stream` gets lo + below(hash(seed, stream, r),
+ * hi - lo + 1); practice_b200/datagen.py restates the same function in numpy. */
+int cx_gen_uniform(uint64_t gen_stream, uint64_t seed, int64_t lo, int64_t hi, uint64_t row0, uint64_t rows,
+                   int32_t* dev_out, void* stream);
+/* yyyymmdd keys of a uniformly drawn day in [1992-01-01, +days). */
+int cx_gen_datekey(uint64_t gen_stream, uint64_t seed, uint32_t days, uint64_t row0, uint64_t rows, int32_t* dev_out,
+                   void* stream);
+/* Seeded Bernoulli validity words: bit r is 0 (NULL) with probability
+ * null_permille/1000; unused bits of the last word are 0. */
+int cx_gen_validity(uint64_t gen_stream, uint64_t seed, uint64_t rows, uint32_t null_permille, uint64_t* dev_out,
+                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CRYSTAL_B200_H */

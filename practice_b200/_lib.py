@@ -1,0 +1,195 @@
+"""ctypes binding of libcrystal_b200.so (include/crystal_b200.h).
+
+The library is the product: if it is missing, importing this module raises
+instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libcrystal_b200.so"
+
+CX_OK = 0
+ERRORS = {
+    -1: "CX_E_INVALID", -2: "CX_E_COMPILE", -3: "CX_E_CUDA", -4: "CX_E_MISSING",
+    -5: "CX_E_CAPACITY", -6: "CX_E_KERNEL", -7: "CX_E_NO_DEVICE", -8: "CX_E_REJECTED",
+}
+
+# Every symbol include/crystal_b200.h declares (checked by the CPU tests).
+EXPORTS = [
+    "cx_abi_version", "cx_last_error", "cx_tuning_default", "cx_codegen", "cx_compile",
+    "cx_module_release", "cx_module_result_info", "cx_ctx_create", "cx_ctx_destroy",
+    "cx_ctx_set_buffer", "cx_ctx_set_null_bitmap", "cx_ctx_set_table_rows", "cx_ctx_set_result",
+    "cx_ctx_set_scratch", "cx_module_scratch_bytes", "cx_ctx_set_sm_count", "cx_execute",
+    "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse",
+    "cx_gen_uniform", "cx_gen_datekey", "cx_gen_validity",
+]
+
+
+class CxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Tuning(C.Structure):
+    _fields_ = [("block_threads", C.c_int), ("items_per_thread", C.c_int), ("stages", C.c_int),
+                ("ctas_per_sm", C.c_int), ("group_placement", C.c_int), ("smem_group_budget", C.c_int)]
+
+
+class ResultInfo(C.Structure):
+    _fields_ = [("groups", C.c_uint64), ("storage_ts", C.c_uint32), ("visible_ts", C.c_uint32),
+                ("result_words", C.c_uint64), ("validity_words", C.c_uint64), ("final_words", C.c_uint64),
+                ("sparse", C.c_int), ("finalized", C.c_int)]
+
+
+class Timing(C.Structure):
+    _fields_ = [("build_ms", C.c_float), ("scan_ms", C.c_float), ("post_ms", C.c_float),
+                ("total_ms", C.c_float), ("scan_grid", C.c_int), ("gpu_launches", C.c_int)]
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is not built; run `python -m practice_b200.build`")
+    lib = C.CDLL(str(LIB_PATH))
+    vp, u64, i64, u32, sz = C.c_void_p, C.c_uint64, C.c_int64, C.c_uint32, C.c_size_t
+    sig = {
+        "cx_abi_version": (C.c_int, []),
+        "cx_last_error": (C.c_char_p, []),
+        "cx_tuning_default": (None, [C.POINTER(Tuning)]),
+        "cx_codegen": (C.c_int, [C.c_char_p, sz, C.POINTER(Tuning), C.c_char_p, sz, C.POINTER(sz)]),
+        "cx_compile": (C.c_int, [C.c_char_p, sz, C.c_char_p, C.POINTER(vp), C.c_char_p, sz]),
+        "cx_module_release": (C.c_int, [vp]),
+        "cx_module_result_info": (C.c_int, [vp, C.POINTER(ResultInfo)]),
+        "cx_ctx_create": (vp, []),
+        "cx_ctx_destroy": (None, [vp]),
+        "cx_ctx_set_buffer": (C.c_int, [vp, C.c_char_p, vp, u64]),
+        "cx_ctx_set_null_bitmap": (C.c_int, [vp, C.c_char_p, vp, u64]),
+        "cx_ctx_set_table_rows": (C.c_int, [vp, C.c_char_p, u64]),
+        "cx_ctx_set_result": (C.c_int, [vp, vp, u64, vp, u64]),
+        "cx_ctx_set_scratch": (C.c_int, [vp, vp, u64]),
+        "cx_module_scratch_bytes": (C.c_int, [vp, vp, C.POINTER(u64)]),
+        "cx_ctx_set_sm_count": (C.c_int, [vp, C.c_int]),
+        "cx_execute": (C.c_int, [vp, vp, vp]),
+        "cx_ctx_sync": (C.c_int, [vp]),
+        "cx_ctx_timing": (C.c_int, [vp, C.POINTER(Timing)]),
+        "cx_ctx_kernel_error": (C.c_int, [vp, C.POINTER(u32)]),
+        "cx_compact_sparse": (C.c_int, [vp, u64, u32, vp, vp, vp]),
+        "cx_gen_uniform": (C.c_int, [u64, u64, i64, i64, u64, u64, vp, vp]),
+        "cx_gen_datekey": (C.c_int, [u64, u64, u32, u64, u64, vp, vp]),
+        "cx_gen_validity": (C.c_int, [u64, u64, u64, u32, vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != CX_OK:
+        msg = lib.cx_last_error().decode(errors="replace")
+        raise CxError(rc, f"{what}: {msg}" if what else msg)
+
+
+def default_tuning() -> Tuning:
+    t = Tuning()
+    lib.cx_tuning_default(C.byref(t))
+    return t
+
+
+def codegen(plan_text: str, tuning: Tuning | None = None) -> str:
+    raw = plan_text.encode()
+    n = C.c_size_t(0)
+    tp = C.byref(tuning) if tuning is not None else None
+    check(lib.cx_codegen(raw, len(raw), tp, None, 0, C.byref(n)), "cx_codegen")
+    buf = C.create_string_buffer(n.value + 1)
+    check(lib.cx_codegen(raw, len(raw), tp, buf, n.value + 1, C.byref(n)), "cx_codegen")
+    return buf.value.decode()
+
+
+class Module:
+    """A compiled query (cx_module*)."""
+
+    def __init__(self, source: str, key: str | None = None):
+        raw = source.encode()
+        handle = C.c_void_p()
+        log = C.create_string_buffer(1 << 16)
+        rc = lib.cx_compile(raw, len(raw), key.encode() if key else None, C.byref(handle), log, len(log))
+        if rc != CX_OK:
+            raise CxError(rc, lib.cx_last_error().decode(errors="replace"))
+        self.handle = handle
+        self.source = source
+        self.log = log.value.decode(errors="replace")
+        info = ResultInfo()
+        check(lib.cx_module_result_info(self.handle, C.byref(info)), "cx_module_result_info")
+        self.info = info
+        sb = C.c_uint64()
+        check(lib.cx_module_scratch_bytes(self.handle, None, C.byref(sb)), "cx_module_scratch_bytes")
+        self.scratch_bytes = sb.value
+
+    def close(self) -> None:
+        if self.handle:
+            lib.cx_module_release(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ExecCtx:
+    """An execution context (cx_exec_ctx*): named device buffers and scratch."""
+
+    def __init__(self):
+        self.handle = lib.cx_ctx_create()
+        if not self.handle:
+            raise MemoryError("cx_ctx_create failed")
+
+    def set_buffer(self, name: str, ptr: int, elems: int) -> None:
+        check(lib.cx_ctx_set_buffer(self.handle, name.encode(), ptr, elems), "cx_ctx_set_buffer")
+
+    def set_null_bitmap(self, name: str, ptr: int, words: int) -> None:
+        check(lib.cx_ctx_set_null_bitmap(self.handle, name.encode(), ptr, words), "cx_ctx_set_null_bitmap")
+
+    def set_rows(self, table: str, rows: int) -> None:
+        check(lib.cx_ctx_set_table_rows(self.handle, table.encode(), rows), "cx_ctx_set_table_rows")
+
+    def set_result(self, res_ptr: int, res_words: int, val_ptr: int, val_words: int) -> None:
+        check(lib.cx_ctx_set_result(self.handle, res_ptr, res_words, val_ptr, val_words), "cx_ctx_set_result")
+
+    def set_scratch(self, ptr: int | None, nbytes: int) -> None:
+        check(lib.cx_ctx_set_scratch(self.handle, ptr, nbytes), "cx_ctx_set_scratch")
+
+    def execute(self, module: Module, stream: int = 0) -> None:
+        check(lib.cx_execute(module.handle, self.handle, stream or None), "cx_execute")
+
+    def sync(self) -> None:
+        check(lib.cx_ctx_sync(self.handle), "cx_ctx_sync")
+
+    def timing(self) -> Timing:
+        t = Timing()
+        check(lib.cx_ctx_timing(self.handle, C.byref(t)), "cx_ctx_timing")
+        return t
+
+    def kernel_error(self) -> int:
+        v = C.c_uint32()
+        check(lib.cx_ctx_kernel_error(self.handle, C.byref(v)))
+        return v.value
+
+    def close(self) -> None:
+        if self.handle:
+            lib.cx_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass

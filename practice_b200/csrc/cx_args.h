@@ -1,0 +1,26 @@
+// cx_args.h -- the single by-value argument block every generated kernel takes.
+//
+// The reference binds column pointers by name inside its generated host function
+// (`ctx->getBuffer<int>("d_<col>")`, src/core/visitor.cpp:4808-4818).  NVRTC
+// compiles device code only, so the generic executor resolves the same names on
+// the host and passes them in slots; the launch plan embedded in the generated
+// source records which name sits in which slot.  Shared by the host runtime
+// (g++) and the NVRTC-compiled kernels, so it holds plain C types only.
+#pragma once
+
+#define CX_MAX_COLS 40
+#define CX_MAX_HTS 8
+#define CX_MAX_TABLES 8
+
+struct CxArgs {
+  const int* col[CX_MAX_COLS];                 // device column bases, by slot
+  const unsigned long long* nul[CX_MAX_COLS];  // validity words (1 = valid), by slot
+  int* ht[CX_MAX_HTS];                         // perfect hash tables (zeroed before builds)
+  unsigned int* htv[CX_MAX_HTS];               // payload validity bits of PHT_2V tables
+  unsigned long long* result;                  // groups x storage tuple, u64
+  unsigned long long* result_validity;         // result validity bits
+  unsigned int* touched;                       // per-group "row seen" bits (global group path)
+  unsigned long long* finalize_tmp;            // visible tuple staging for AVG finalisation
+  unsigned int* err;                           // first error code raised by any kernel
+  long long rows[CX_MAX_TABLES];               // row count per plan table slot
+};

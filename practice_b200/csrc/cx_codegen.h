@@ -1,0 +1,26 @@
+// cx_codegen.h -- CUDA C++ generation for star-join plans.
+#pragma once
+
+#include <string>
+
+#include "cx_plan.h"
+
+namespace cx {
+
+// Launch shape of the generated fact-scan kernel.  The autotuner searches this
+// space per query shape; defaults are the measured best general setting.
+struct Tuning {
+  int block_threads = 256;     // BLOCK_THREADS (multiple of 32, <= 1024)
+  int items_per_thread = 4;    // ITEMS_PER_THREAD
+  int stages = 4;              // TMA staging ring depth (0 disables staging)
+  int ctas_per_sm = 2;         // persistent grid = SMs x this (occupancy-capped)
+  int group_placement = 0;     // 0 auto, 1 shared-memory tables, 2 global atomics
+  int smem_group_budget = 96 * 1024;  // bytes of shared memory a group table may use
+  int wait_limit_log2 = 24;    // mbarrier poll limit before a wait gives up
+};
+
+// Returns the CUDA source for `plan` with its launch plan embedded as a
+// leading `/*@cx-launch ... @*/` block.  Throws PlanError on unsupported shapes.
+std::string generate_cuda(const Plan& plan, const Tuning& tuning);
+
+}  // namespace cx

@@ -1,0 +1,346 @@
+// cx_plan.cpp -- S-expression reader and validation for star-join plans.
+#include "cx_plan.h"
+
+#include <cctype>
+#include <cstdlib>
+#include <functional>
+
+namespace cx {
+
+namespace {
+
+struct Node {
+  bool atom = false;
+  std::string text;
+  std::vector<Node> items;
+};
+
+class Reader {
+ public:
+  explicit Reader(const std::string& s) : s_(s) {}
+  Node read() {
+    skip();
+    Node n = read_node();
+    skip();
+    if (pos_ != s_.size()) fail("trailing text after plan");
+    return n;
+  }
+
+ private:
+  const std::string& s_;
+  size_t pos_ = 0;
+
+  [[noreturn]] void fail(const std::string& m) {
+    throw PlanError("plan parse error at offset " + std::to_string(pos_) + ": " + m);
+  }
+  void skip() {
+    while (pos_ < s_.size()) {
+      if (std::isspace((unsigned char)s_[pos_])) {
+        ++pos_;
+      } else if (s_[pos_] == ';') {
+        while (pos_ < s_.size() && s_[pos_] != '\n') ++pos_;
+      } else {
+        break;
+      }
+    }
+  }
+  Node read_node() {
+    skip();
+    if (pos_ >= s_.size()) fail("unexpected end of plan");
+    Node n;
+    if (s_[pos_] == '(') {
+      ++pos_;
+      for (;;) {
+        skip();
+        if (pos_ >= s_.size()) fail("missing ')'");
+        if (s_[pos_] == ')') { ++pos_; break; }
+        n.items.push_back(read_node());
+      }
+      return n;
+    }
+    if (s_[pos_] == ')') fail("unexpected ')'");
+    n.atom = true;
+    while (pos_ < s_.size() && !std::isspace((unsigned char)s_[pos_]) && s_[pos_] != '(' && s_[pos_] != ')')
+      n.text.push_back(s_[pos_++]);
+    return n;
+  }
+};
+
+const std::string& head(const Node& n) {
+  static const std::string empty;
+  if (n.atom || n.items.empty() || !n.items[0].atom) return empty;
+  return n.items[0].text;
+}
+
+long long to_int(const Node& n, const char* what) {
+  if (!n.atom) throw PlanError(std::string("expected integer for ") + what);
+  char* end = nullptr;
+  errno = 0;
+  long long v = std::strtoll(n.text.c_str(), &end, 10);
+  if (errno != 0 || end == n.text.c_str() || *end != '\0')
+    throw PlanError(std::string("bad integer '") + n.text + "' for " + what);
+  return v;
+}
+
+const std::string& to_name(const Node& n, const char* what) {
+  if (!n.atom) throw PlanError(std::string("expected name for ") + what);
+  return n.text;
+}
+
+// (key value) lookup inside a list node.
+const Node* field(const Node& n, const std::string& key) {
+  for (size_t i = 1; i < n.items.size(); ++i)
+    if (head(n.items[i]) == key) return &n.items[i];
+  return nullptr;
+}
+
+struct OpName {
+  const char* name;
+  Op op;
+  int arity;
+};
+const OpName kOps[] = {
+    {"add", Op::Add, 2}, {"sub", Op::Sub, 2}, {"mul", Op::Mul, 2}, {"div", Op::Div, 2},
+    {"eq", Op::Eq, 2},   {"ne", Op::Ne, 2},   {"lt", Op::Lt, 2},   {"le", Op::Le, 2},
+    {"gt", Op::Gt, 2},   {"ge", Op::Ge, 2},   {"and", Op::And, 2}, {"or", Op::Or, 2},
+    {"not", Op::Not, 1}, {"isnull", Op::IsNull, 1}, {"notnull", Op::NotNull, 1},
+    {"case", Op::Case, 3},
+};
+
+std::unique_ptr<Expr> to_expr(const Node& n) {
+  const std::string& h = head(n);
+  auto e = std::make_unique<Expr>();
+  if (h == "col") {
+    if (n.items.size() != 2) throw PlanError("(col NAME) takes one name");
+    e->op = Op::Col;
+    e->name = to_name(n.items[1], "col");
+    return e;
+  }
+  if (h == "int") {
+    if (n.items.size() != 2) throw PlanError("(int N) takes one integer");
+    e->op = Op::Int;
+    e->ival = to_int(n.items[1], "int literal");
+    return e;
+  }
+  if (h == "null") { e->op = Op::Null; return e; }
+  if (h == "star") { e->op = Op::Star; return e; }
+  for (const auto& o : kOps) {
+    if (h == o.name) {
+      if ((int)n.items.size() != o.arity + 1)
+        throw PlanError(std::string("(") + o.name + " ...) takes " + std::to_string(o.arity) + " operands");
+      e->op = o.op;
+      for (int k = 1; k <= o.arity; ++k) e->kids.push_back(to_expr(n.items[k]));
+      return e;
+    }
+  }
+  throw PlanError("unknown expression '" + (h.empty() ? std::string("<atom>") : h) + "'");
+}
+
+void collect_cols(const Expr* e, std::vector<std::string>& out) {
+  if (!e) return;
+  if (e->op == Op::Col) out.push_back(e->name);
+  for (const auto& k : e->kids) collect_cols(k.get(), out);
+}
+
+}  // namespace
+
+bool is_arith(Op op) { return op == Op::Add || op == Op::Sub || op == Op::Mul || op == Op::Div; }
+bool is_compare(Op op) {
+  return op == Op::Eq || op == Op::Ne || op == Op::Lt || op == Op::Le || op == Op::Gt || op == Op::Ge;
+}
+const char* op_name(Op op) {
+  for (const auto& o : kOps)
+    if (o.op == op) return o.name;
+  switch (op) {
+    case Op::Col: return "col";
+    case Op::Int: return "int";
+    case Op::Null: return "null";
+    case Op::Star: return "star";
+    default: return "?";
+  }
+}
+
+int Plan::table_slot(const std::string& t) const {
+  for (size_t i = 0; i < tables.size(); ++i)
+    if (tables[i].name == t) return (int)i;
+  return -1;
+}
+
+unsigned long long Plan::group_count() const {
+  unsigned long long g = 1;
+  for (const auto& k : groups) g *= (unsigned long long)k.card;
+  return g;
+}
+
+int Plan::hidden_count_slots() const {
+  int n = 0;
+  for (const auto& a : aggs) n += (a.fn == AggFn::Avg);
+  return n;
+}
+
+int Plan::storage_ts() const {
+  const int s = (int)(groups.size() + aggs.size()) + hidden_count_slots();
+  return s == 0 ? 1 : s;
+}
+
+int Plan::hidden_count_slot(size_t agg_idx) const {
+  if (agg_idx >= aggs.size() || aggs[agg_idx].fn != AggFn::Avg) return -1;
+  int slot = visible_ts();
+  for (size_t i = 0; i < agg_idx; ++i) slot += (aggs[i].fn == AggFn::Avg);
+  return slot;
+}
+
+bool Plan::has_min() const {
+  for (const auto& a : aggs)
+    if (a.fn == AggFn::Min) return true;
+  return false;
+}
+
+std::unique_ptr<Plan> parse_plan(const std::string& text) {
+  Reader rd(text);
+  Node root = rd.read();
+  if (head(root) != "query") throw PlanError("plan must start with (query ...)");
+  auto p = std::make_unique<Plan>();
+  bool have_agg = false;
+
+  for (size_t i = 1; i < root.items.size(); ++i) {
+    const Node& n = root.items[i];
+    const std::string& h = head(n);
+    if (h == "table") {
+      Table t;
+      if (n.items.size() < 3) throw PlanError("(table NAME [fact] (cols ...))");
+      t.name = to_name(n.items[1], "table");
+      for (size_t k = 2; k < n.items.size(); ++k) {
+        if (n.items[k].atom && n.items[k].text == "fact") t.fact = true;
+        else if (head(n.items[k]) == "cols")
+          for (size_t c = 1; c < n.items[k].items.size(); ++c) t.cols.push_back(to_name(n.items[k].items[c], "cols"));
+        else throw PlanError("unexpected item in (table " + t.name + " ...)");
+      }
+      if (p->table_slot(t.name) >= 0) throw PlanError("table declared twice: " + t.name);
+      if (t.fact && !p->tables.empty() && p->tables[0].fact) throw PlanError("two fact tables");
+      if (t.fact) p->tables.insert(p->tables.begin(), std::move(t));
+      else p->tables.push_back(std::move(t));
+    } else if (h == "nullable") {
+      for (size_t k = 1; k < n.items.size(); ++k) p->nullable.insert(to_name(n.items[k], "nullable"));
+    } else if (h == "filter") {
+      if (have_agg) throw PlanError("filter after aggregate is not part of the scan pipeline");
+      if (n.items.size() != 2) throw PlanError("(filter EXPR)");
+      Step s;
+      s.kind = Step::Filter;
+      s.filter = to_expr(n.items[1]);
+      p->steps.push_back(std::move(s));
+    } else if (h == "join") {
+      if (have_agg) throw PlanError("join after aggregate");
+      Step s;
+      s.kind = Step::JoinStep;
+      Join& j = s.join;
+      j.dim = to_name(n.items.at(1), "join table");
+      const Node* pk = field(n, "pk");
+      const Node* fk = field(n, "fk");
+      const Node* len = field(n, "len");
+      const Node* km = field(n, "keymin");
+      if (!pk || pk->items.size() != 2 || !fk || fk->items.size() < 2 || !len || !km)
+        throw PlanError("(join DIM (pk C) (fk C...) (len N) (keymin N) ...) is incomplete for " + j.dim);
+      j.pk = to_name(pk->items[1], "pk");
+      for (size_t k = 1; k < fk->items.size(); ++k) j.fks.push_back(to_name(fk->items[k], "fk"));
+      j.len = to_int(len->items.at(1), "len");
+      j.keymin = to_int(km->items.at(1), "keymin");
+      if (const Node* f = field(n, "filter")) j.filter = to_expr(f->items.at(1));
+      if (const Node* pl = field(n, "payload")) j.payload = to_name(pl->items.at(1), "payload");
+      if (j.len <= 0 || j.len > (1LL << 30)) throw PlanError("join len out of range for " + j.dim);
+      if (j.fks.size() != 1) throw PlanError("OR-joins over several fact keys are not supported on this path");
+      p->steps.push_back(std::move(s));
+    } else if (h == "aggregate") {
+      if (have_agg) throw PlanError("two aggregates");
+      have_agg = true;
+      for (size_t k = 1; k < n.items.size(); ++k) {
+        const Node& a = n.items[k];
+        const std::string& ah = head(a);
+        if (ah == "group") {
+          GroupKey g;
+          g.expr = to_expr(a.items.at(1));
+          const Node* mn = field(a, "min");
+          const Node* cd = field(a, "card");
+          const Node* nl = field(a, "nullable");
+          if (!mn || !cd) throw PlanError("(group EXPR (min N) (card N) [(nullable 0|1)])");
+          g.min = to_int(mn->items.at(1), "group min");
+          g.card = to_int(cd->items.at(1), "group card");
+          g.nullable = nl ? to_int(nl->items.at(1), "nullable") != 0 : false;
+          if (g.card <= 0) throw PlanError("group card must be positive");
+          if (g.expr->op != Op::Col && g.expr->op != Op::Case)
+            throw PlanError("GROUP BY expression is not supported by perfect hash codegen: " +
+                            std::string(op_name(g.expr->op)));
+          p->groups.push_back(std::move(g));
+        } else if (ah == "sparse") {
+          p->sparse = to_int(a.items.at(1), "sparse") != 0;
+        } else {
+          Agg g;
+          if (ah == "count") g.fn = AggFn::Count;
+          else if (ah == "sum") g.fn = AggFn::Sum;
+          else if (ah == "min") g.fn = AggFn::Min;
+          else if (ah == "max") g.fn = AggFn::Max;
+          else if (ah == "avg") g.fn = AggFn::Avg;
+          else throw PlanError("unknown aggregate '" + ah + "'");
+          if (a.items.size() != 2) throw PlanError("aggregate takes one argument");
+          g.arg = to_expr(a.items[1]);
+          if (g.arg->op == Op::Star && g.fn != AggFn::Count)
+            throw PlanError("only COUNT accepts '*'");
+          p->aggs.push_back(std::move(g));
+        }
+      }
+      if (p->aggs.empty()) throw PlanError("aggregate needs at least one aggregate function");
+    } else {
+      throw PlanError("unknown plan item '" + h + "'");
+    }
+  }
+
+  if (!have_agg) throw PlanError("plan has no aggregate (projection plans are not on this path)");
+  if (p->tables.empty() || !p->tables[0].fact) throw PlanError("plan declares no fact table");
+  if ((int)p->tables.size() > 8) throw PlanError("too many tables");
+  for (size_t t = 0; t < p->tables.size(); ++t)
+    for (const auto& c : p->tables[t].cols) {
+      if (p->table_of_col.count(c)) throw PlanError("column declared twice: " + c);
+      p->table_of_col[c] = (int)t;
+    }
+
+  // Column/table consistency: fact-side expressions may reference fact columns
+  // and the payloads of joins already probed; build-side filters only their
+  // own dimension.
+  std::set<std::string> visible;
+  for (const auto& c : p->tables[0].cols) visible.insert(c);
+  auto check = [&](const Expr* e, const std::set<std::string>& allowed, const std::string& where) {
+    std::vector<std::string> cols;
+    collect_cols(e, cols);
+    for (const auto& c : cols) {
+      if (!p->table_of_col.count(c)) throw PlanError("unknown column '" + c + "' in " + where);
+      if (!allowed.count(c)) throw PlanError("column '" + c + "' is not available in " + where);
+    }
+  };
+  std::set<std::string> seen_dims;
+  for (auto& s : p->steps) {
+    if (s.kind == Step::Filter) {
+      check(s.filter.get(), visible, "fact-side filter");
+      continue;
+    }
+    Join& j = s.join;
+    const int dt = p->table_slot(j.dim);
+    if (dt <= 0) throw PlanError("join dimension '" + j.dim + "' is not a declared dimension table");
+    if (seen_dims.count(j.dim)) throw PlanError("dimension joined twice: " + j.dim);
+    seen_dims.insert(j.dim);
+    std::set<std::string> dimcols(p->tables[dt].cols.begin(), p->tables[dt].cols.end());
+    if (!dimcols.count(j.pk)) throw PlanError("pk '" + j.pk + "' is not a column of " + j.dim);
+    for (const auto& fk : j.fks)
+      if (!visible.count(fk) || p->table_of_col[fk] != 0) throw PlanError("fk '" + fk + "' is not a fact column");
+    if (j.filter) check(j.filter.get(), dimcols, "build filter of " + j.dim);
+    if (!j.payload.empty()) {
+      if (!dimcols.count(j.payload) || j.payload == j.pk) throw PlanError("bad payload column for " + j.dim);
+      visible.insert(j.payload);
+    }
+  }
+  for (const auto& g : p->groups) check(g.expr.get(), visible, "GROUP BY");
+  for (const auto& a : p->aggs) check(a.arg.get(), visible, "aggregate");
+  if (p->group_count() > (1ULL << 31)) throw PlanError("group domain too large for a perfect hash");
+  return p;
+}
+
+}  // namespace cx

@@ -1,0 +1,685 @@
+// cx_runtime.cpp -- NVRTC compiler, module cache and generic executor behind
+// the C ABI in include/crystal_b200.h.
+//
+// The reference compiles each generated program out of process with `acpp` and
+// dlopen()s it (src/core/execution.cpp:114-192); the generated library then
+// runs its own host code.  Here the generated source holds device code plus a
+// launch plan; NVRTC compiles it in memory for sm_100a and one generic
+// executor (this file) runs the plan: memsets, build kernels, the fused scan,
+// epilogues.  Driver-API entry points are obtained through the runtime
+// (cudaGetDriverEntryPointByVersion), so the library links no libcuda and
+// loads on hosts without a GPU.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/crystal_b200.h"
+#include "cx_args.h"
+#include "cx_codegen.h"
+#include "cx_plan.h"
+
+// Generated at build time from crystal_sm100.cuh and cx_args.h.
+#include "cx_embedded.inc"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[2048];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define CX_CUDA(call)                                                                          \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return fail(CX_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_));    \
+  } while (0)
+
+// ----------------------------------------------------------- driver entry ---
+struct Driver {
+  CUresult (*ModuleLoadData)(CUmodule*, const void*) = nullptr;
+  CUresult (*ModuleGetFunction)(CUfunction*, CUmodule, const char*) = nullptr;
+  CUresult (*ModuleUnload)(CUmodule) = nullptr;
+  CUresult (*FuncSetAttribute)(CUfunction, CUfunction_attribute, int) = nullptr;
+  CUresult (*LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
+                           void**, void**) = nullptr;
+  CUresult (*Occupancy)(int*, CUfunction, int, size_t) = nullptr;
+  CUresult (*GetErrorString)(CUresult, const char**) = nullptr;
+  bool ok = false;
+};
+
+template <typename F>
+bool entry(const char* name, F& fn) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPointByVersion(name, &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !p)
+    return false;
+  fn = reinterpret_cast<F>(p);
+  return true;
+}
+
+Driver& driver() {
+  static Driver d;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    d.ok = entry("cuModuleLoadData", d.ModuleLoadData) && entry("cuModuleGetFunction", d.ModuleGetFunction) &&
+           entry("cuModuleUnload", d.ModuleUnload) && entry("cuFuncSetAttribute", d.FuncSetAttribute) &&
+           entry("cuLaunchKernel", d.LaunchKernel) &&
+           entry("cuOccupancyMaxActiveBlocksPerMultiprocessor", d.Occupancy) &&
+           entry("cuGetErrorString", d.GetErrorString);
+  });
+  return d;
+}
+
+int drv_fail(CUresult r, const char* what) {
+  const char* s = "unknown";
+  if (driver().GetErrorString) driver().GetErrorString(r, &s);
+  return fail(CX_E_CUDA, "%s: %s", what, s);
+}
+
+// ------------------------------------------------------------ launch plan ---
+struct KernelSpec {
+  std::string name, kind;
+  int table = 0, block = 128, tile = 512, ctas_per_sm = 1;
+  size_t smem = 0;
+};
+
+struct LaunchPlan {
+  std::vector<std::string> tables;
+  struct Col { int slot; std::string name; int table; };
+  std::vector<Col> cols;
+  std::vector<std::pair<int, std::string>> nulls;
+  struct Ht { int slot; std::string name; uint64_t words; };
+  std::vector<Ht> hts;
+  std::map<int, uint64_t> htv_words;
+  uint64_t result_words = 0, groups = 1;
+  int storage_ts = 1, visible_ts = 1, sparse = 0;
+  uint64_t touched_words = 0;
+  bool finalize = false;
+  uint64_t fin_groups = 0;
+  int fin_vts = 0;
+  std::vector<KernelSpec> kernels;
+};
+
+bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err) {
+  const size_t b = src.find("/*@cx-launch");
+  const size_t e = src.find("@*/");
+  if (b == std::string::npos || e == std::string::npos || e < b) {
+    err = "source has no /*@cx-launch ... @*/ block (not generated by cx_codegen)";
+    return false;
+  }
+  std::istringstream in(src.substr(b + 12, e - b - 12));
+  std::string line;
+  while (std::getline(in, line)) {
+    std::istringstream ls(line);
+    std::string k;
+    if (!(ls >> k)) continue;
+    if (k == "v") {
+      int v = 0;
+      ls >> v;
+      if (v != 1) { err = "unsupported launch plan version"; return false; }
+    } else if (k == "table") {
+      int s; std::string n;
+      ls >> s >> n;
+      if (s != (int)lp.tables.size()) { err = "table slots out of order"; return false; }
+      lp.tables.push_back(n);
+    } else if (k == "col") {
+      LaunchPlan::Col c;
+      ls >> c.slot >> c.name >> c.table;
+      lp.cols.push_back(c);
+    } else if (k == "null") {
+      int s; std::string n;
+      ls >> s >> n;
+      lp.nulls.emplace_back(s, n);
+    } else if (k == "ht") {
+      LaunchPlan::Ht h;
+      ls >> h.slot >> h.name >> h.words;
+      lp.hts.push_back(h);
+    } else if (k == "htv") {
+      int s; uint64_t w;
+      ls >> s >> w;
+      lp.htv_words[s] = w;
+    } else if (k == "result") {
+      ls >> lp.result_words >> lp.groups >> lp.storage_ts >> lp.visible_ts >> lp.sparse;
+    } else if (k == "touched") {
+      ls >> lp.touched_words;
+    } else if (k == "finalize") {
+      lp.finalize = true;
+      ls >> lp.fin_groups >> lp.fin_vts;
+    } else if (k == "kernel") {
+      KernelSpec ks;
+      ls >> ks.name >> ks.kind >> ks.table >> ks.block;
+      if (ks.kind == "build") ls >> ks.tile;
+      else if (ks.kind == "scan") ls >> ks.tile >> ks.smem >> ks.ctas_per_sm;
+      else { size_t z; ls >> z; }
+      lp.kernels.push_back(ks);
+    } else {
+      err = "unknown launch plan line: " + line;
+      return false;
+    }
+    if (ls.fail()) { err = "malformed launch plan line: " + line; return false; }
+  }
+  if (lp.cols.size() > CX_MAX_COLS || lp.hts.size() > CX_MAX_HTS || lp.tables.size() > CX_MAX_TABLES) {
+    err = "launch plan exceeds argument slots";
+    return false;
+  }
+  return true;
+}
+
+uint64_t align256(uint64_t x) { return (x + 255) & ~255ULL; }
+
+// Scratch layout of one execute: hash tables, payload validity, group
+// touched bits, finalisation staging and the error word.
+struct ScratchLayout {
+  std::vector<uint64_t> ht_off, htv_off;
+  uint64_t touched_off = 0, fin_off = 0, err_off = 0, total = 0;
+};
+
+ScratchLayout scratch_layout(const LaunchPlan& lp) {
+  ScratchLayout s;
+  uint64_t off = 0;
+  for (const auto& h : lp.hts) {
+    s.ht_off.push_back(off);
+    off = align256(off + h.words * 4);
+  }
+  for (const auto& h : lp.hts) {
+    auto it = lp.htv_words.find(h.slot);
+    s.htv_off.push_back(off);
+    if (it != lp.htv_words.end()) off = align256(off + it->second * 4);
+  }
+  s.touched_off = off;
+  off = align256(off + lp.touched_words * 4);
+  s.fin_off = off;
+  if (lp.finalize) {
+    const uint64_t vis = lp.fin_groups * (uint64_t)lp.fin_vts;
+    off = align256(off + (vis + (vis + 63) / 64 + 1) * 8);
+  }
+  s.err_off = off;
+  off = align256(off + 16);
+  s.total = off;
+  return s;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- module ---
+struct cx_module {
+  std::string key;
+  size_t src_hash = 0;
+  std::vector<char> cubin;
+  LaunchPlan lp;
+  ScratchLayout sl;
+  std::atomic<int> refs{1};
+  std::mutex mu;
+  struct Loaded {
+    CUmodule mod = nullptr;
+    std::vector<CUfunction> fns;
+    std::vector<int> occupancy;  // scan kernels: CTAs per SM at their smem size
+  };
+  std::map<int, Loaded> per_device;
+};
+
+struct cx_exec_ctx {
+  std::unordered_map<std::string, std::pair<const void*, uint64_t>> buffers;
+  std::unordered_map<std::string, std::pair<const uint64_t*, uint64_t>> nulls;
+  std::unordered_map<std::string, uint64_t> rows;
+  uint64_t* result = nullptr;
+  uint64_t result_words = 0;
+  uint64_t* validity = nullptr;
+  uint64_t validity_words = 0;
+  void* user_scratch = nullptr;
+  uint64_t user_scratch_bytes = 0;
+  void* own_scratch = nullptr;
+  uint64_t own_scratch_bytes = 0;
+  int device = -1;
+  int sm_override = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  unsigned int* host_err = nullptr;  // pinned
+  bool pending = false;
+  cx_timing timing{};
+  uint32_t kernel_err = 0;
+};
+
+namespace {
+
+std::mutex g_cache_mu;
+std::unordered_map<std::string, cx_module*> g_cache;
+
+int load_on_device(cx_module* m, int dev, cx_module::Loaded** out) {
+  std::lock_guard<std::mutex> lk(m->mu);
+  auto it = m->per_device.find(dev);
+  if (it != m->per_device.end()) { *out = &it->second; return CX_OK; }
+  Driver& d = driver();
+  if (!d.ok) return fail(CX_E_CUDA, "CUDA driver entry points unavailable");
+  cx_module::Loaded L;
+  CUresult r = d.ModuleLoadData(&L.mod, m->cubin.data());
+  if (r != CUDA_SUCCESS) return drv_fail(r, "cuModuleLoadData");
+  for (const auto& k : m->lp.kernels) {
+    CUfunction f = nullptr;
+    r = d.ModuleGetFunction(&f, L.mod, k.name.c_str());
+    if (r != CUDA_SUCCESS) { d.ModuleUnload(L.mod); return drv_fail(r, k.name.c_str()); }
+    int occ = 1;
+    if (k.kind == "scan") {
+      if (k.smem > 48 * 1024) {
+        r = d.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)k.smem);
+        if (r != CUDA_SUCCESS) { d.ModuleUnload(L.mod); return drv_fail(r, "cuFuncSetAttribute(smem)"); }
+      }
+      r = d.Occupancy(&occ, f, k.block, k.smem);
+      if (r != CUDA_SUCCESS) { d.ModuleUnload(L.mod); return drv_fail(r, "cuOccupancyMaxActiveBlocksPerMultiprocessor"); }
+      if (occ < 1) { d.ModuleUnload(L.mod); return fail(CX_E_CAPACITY, "scan kernel %s cannot be resident (smem %zu)", k.name.c_str(), k.smem); }
+    }
+    L.fns.push_back(f);
+    L.occupancy.push_back(occ);
+  }
+  auto ins = m->per_device.emplace(dev, std::move(L));
+  *out = &ins.first->second;
+  return CX_OK;
+}
+
+int ensure_ctx_device(cx_exec_ctx* c, int dev) {
+  if (c->device == dev && c->ev[0]) return CX_OK;
+  if (c->ev[0]) {
+    for (auto& e : c->ev) { cudaEventDestroy(e); e = nullptr; }
+  }
+  for (auto& e : c->ev) CX_CUDA(cudaEventCreate(&e));
+  if (!c->host_err) CX_CUDA(cudaMallocHost((void**)&c->host_err, sizeof(unsigned int)));
+  c->device = dev;
+  return CX_OK;
+}
+
+}  // namespace
+
+// ================================================================== C ABI ===
+extern "C" {
+
+int cx_abi_version(void) { return CX_ABI_VERSION; }
+const char* cx_last_error(void) { return g_last_error.c_str(); }
+
+void cx_tuning_default(cx_tuning* t) {
+  if (!t) return;
+  cx::Tuning d;
+  t->block_threads = d.block_threads;
+  t->items_per_thread = d.items_per_thread;
+  t->stages = d.stages;
+  t->ctas_per_sm = d.ctas_per_sm;
+  t->group_placement = d.group_placement;
+  t->smem_group_budget = d.smem_group_budget;
+}
+
+int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap, size_t* out_len) {
+  if (!plan) return fail(CX_E_INVALID, "cx_codegen: plan is NULL");
+  try {
+    auto p = cx::parse_plan(std::string(plan, plan_len));
+    cx::Tuning t;
+    if (tuning) {
+      t.block_threads = tuning->block_threads;
+      t.items_per_thread = tuning->items_per_thread;
+      t.stages = tuning->stages;
+      t.ctas_per_sm = tuning->ctas_per_sm;
+      t.group_placement = tuning->group_placement;
+      t.smem_group_budget = tuning->smem_group_budget;
+    }
+    const std::string s = cx::generate_cuda(*p, t);
+    if (out_len) *out_len = s.size();
+    if (out && out_cap) {
+      const size_t n = s.size() < out_cap - 1 ? s.size() : out_cap - 1;
+      memcpy(out, s.data(), n);
+      out[n] = '\0';
+      if (n < s.size()) return fail(CX_E_CAPACITY, "cx_codegen: output buffer too small (%zu < %zu)", out_cap, s.size() + 1);
+    }
+    return CX_OK;
+  } catch (const std::exception& e) {
+    return fail(CX_E_INVALID, "%s", e.what());
+  }
+}
+
+int cx_compile(const char* src, size_t src_len, const char* key, cx_module** out, char* log, size_t log_cap) {
+  if (!src || !out) return fail(CX_E_INVALID, "cx_compile: NULL argument");
+  if (log && log_cap) log[0] = '\0';
+  const std::string source(src, src_len);
+  const size_t h = std::hash<std::string>{}(source);
+  std::string ck = key ? std::string(key) : std::string();
+  if (ck.empty()) ck = "anon_" + std::to_string(h);
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto it = g_cache.find(ck);
+    if (it != g_cache.end() && it->second->src_hash == h) {
+      it->second->refs.fetch_add(1);
+      *out = it->second;
+      return CX_OK;
+    }
+  }
+  auto m = std::make_unique<cx_module>();
+  m->key = ck;
+  m->src_hash = h;
+  std::string perr;
+  if (!parse_launch_plan(source, m->lp, perr)) return fail(CX_E_INVALID, "cx_compile: %s", perr.c_str());
+  m->sl = scratch_layout(m->lp);
+
+  nvrtcProgram prog;
+  const char* headers[] = {kCxEmbeddedCrystalHeader, kCxEmbeddedArgsHeader};
+  const char* names[] = {"crystal_sm100.cuh", "cx_args.h"};
+  nvrtcResult r = nvrtcCreateProgram(&prog, source.c_str(), "cx_query.cu", 2, headers, names);
+  if (r != NVRTC_SUCCESS) return fail(CX_E_COMPILE, "nvrtcCreateProgram: %s", nvrtcGetErrorString(r));
+  const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-default-device"};
+  r = nvrtcCompileProgram(prog, 4, opts);
+  size_t lsz = 0;
+  nvrtcGetProgramLogSize(prog, &lsz);
+  std::string plog(lsz, '\0');
+  if (lsz) nvrtcGetProgramLog(prog, &plog[0]);
+  if (log && log_cap) {
+    const size_t n = plog.size() < log_cap - 1 ? plog.size() : log_cap - 1;
+    memcpy(log, plog.data(), n);
+    log[n] = '\0';
+  }
+  if (r != NVRTC_SUCCESS) {
+    nvrtcDestroyProgram(&prog);
+    return fail(CX_E_COMPILE, "NVRTC compile failed: %s\n%.1500s", nvrtcGetErrorString(r), plog.c_str());
+  }
+  size_t csz = 0;
+  nvrtcGetCUBINSize(prog, &csz);
+  m->cubin.resize(csz);
+  nvrtcGetCUBIN(prog, m->cubin.data());
+  nvrtcDestroyProgram(&prog);
+
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  auto it = g_cache.find(ck);
+  if (it != g_cache.end()) {
+    // Same key, different source: the newer program replaces the cache entry;
+    // holders of the old module keep it alive through their references.
+    if (it->second->refs.fetch_sub(1) == 1) {
+      cx_module* old = it->second;
+      for (auto& kv : old->per_device)
+        if (kv.second.mod && driver().ok) driver().ModuleUnload(kv.second.mod);
+      delete old;
+    }
+    g_cache.erase(it);
+  }
+  cx_module* raw = m.release();
+  raw->refs.store(2);  // one for the cache, one for the caller
+  g_cache[ck] = raw;
+  *out = raw;
+  return CX_OK;
+}
+
+int cx_module_release(cx_module* m) {
+  if (!m) return CX_OK;
+  if (m->refs.fetch_sub(1) == 1) {
+    for (auto& kv : m->per_device)
+      if (kv.second.mod && driver().ok) driver().ModuleUnload(kv.second.mod);
+    delete m;
+  }
+  return CX_OK;
+}
+
+int cx_module_result_info(const cx_module* m, cx_result_info* info) {
+  if (!m || !info) return fail(CX_E_INVALID, "cx_module_result_info: NULL argument");
+  const LaunchPlan& lp = m->lp;
+  info->groups = lp.groups;
+  info->storage_ts = (uint32_t)lp.storage_ts;
+  info->visible_ts = (uint32_t)lp.visible_ts;
+  info->result_words = lp.result_words;
+  info->validity_words = (lp.result_words + 63) / 64;
+  info->finalized = lp.finalize ? 1 : 0;
+  info->final_words = lp.finalize ? lp.groups * (uint64_t)lp.visible_ts : lp.result_words;
+  info->sparse = lp.sparse;
+  return CX_OK;
+}
+
+cx_exec_ctx* cx_ctx_create(void) { return new (std::nothrow) cx_exec_ctx(); }
+
+void cx_ctx_destroy(cx_exec_ctx* c) {
+  if (!c) return;
+  if (c->pending && c->ev[3]) cudaEventSynchronize(c->ev[3]);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->own_scratch) cudaFree(c->own_scratch);
+  if (c->host_err) cudaFreeHost(c->host_err);
+  delete c;
+}
+
+int cx_ctx_set_buffer(cx_exec_ctx* c, const char* name, const void* p, uint64_t elems) {
+  if (!c || !name) return fail(CX_E_INVALID, "cx_ctx_set_buffer: NULL argument");
+  c->buffers[name] = {p, elems};
+  return CX_OK;
+}
+
+int cx_ctx_set_null_bitmap(cx_exec_ctx* c, const char* name, const uint64_t* p, uint64_t words) {
+  if (!c || !name) return fail(CX_E_INVALID, "cx_ctx_set_null_bitmap: NULL argument");
+  c->nulls[name] = {p, words};
+  return CX_OK;
+}
+
+int cx_ctx_set_table_rows(cx_exec_ctx* c, const char* table, uint64_t rows) {
+  if (!c || !table) return fail(CX_E_INVALID, "cx_ctx_set_table_rows: NULL argument");
+  if (rows > (1ULL << 40)) return fail(CX_E_INVALID, "cx_ctx_set_table_rows: %llu rows is out of range", (unsigned long long)rows);
+  c->rows[table] = rows;
+  return CX_OK;
+}
+
+int cx_ctx_set_result(cx_exec_ctx* c, uint64_t* r, uint64_t rw, uint64_t* v, uint64_t vw) {
+  if (!c) return fail(CX_E_INVALID, "cx_ctx_set_result: NULL context");
+  c->result = r;
+  c->result_words = rw;
+  c->validity = v;
+  c->validity_words = vw;
+  return CX_OK;
+}
+
+int cx_ctx_set_scratch(cx_exec_ctx* c, void* p, uint64_t bytes) {
+  if (!c) return fail(CX_E_INVALID, "cx_ctx_set_scratch: NULL context");
+  if (p && ((uintptr_t)p & 255)) return fail(CX_E_INVALID, "cx_ctx_set_scratch: scratch must be 256-byte aligned");
+  c->user_scratch = p;
+  c->user_scratch_bytes = p ? bytes : 0;
+  return CX_OK;
+}
+
+int cx_ctx_set_sm_count(cx_exec_ctx* c, int sms) {
+  if (!c || sms < 0) return fail(CX_E_INVALID, "cx_ctx_set_sm_count: bad argument");
+  c->sm_override = sms;
+  return CX_OK;
+}
+
+int cx_module_scratch_bytes(const cx_module* m, const cx_exec_ctx* c, uint64_t* bytes) {
+  (void)c;
+  if (!m || !bytes) return fail(CX_E_INVALID, "cx_module_scratch_bytes: NULL argument");
+  *bytes = m->sl.total;
+  return CX_OK;
+}
+
+int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream_v) {
+  if (!m || !c) return fail(CX_E_INVALID, "cx_execute: NULL argument");
+  const LaunchPlan& lp = m->lp;
+  cudaStream_t stream = (cudaStream_t)stream_v;
+
+  // Resolve tables, columns and result buffers before touching the GPU.
+  CxArgs a;
+  memset(&a, 0, sizeof a);
+  std::vector<long long> rows(lp.tables.size(), 0);
+  for (size_t t = 0; t < lp.tables.size(); ++t) {
+    auto it = c->rows.find(lp.tables[t]);
+    if (it == c->rows.end()) return fail(CX_E_MISSING, "cx_execute: row count of table %s is not set", lp.tables[t].c_str());
+    rows[t] = (long long)it->second;
+    a.rows[t] = rows[t];
+  }
+  for (const auto& col : lp.cols) {
+    auto it = c->buffers.find(col.name);
+    if (it == c->buffers.end() || (!it->second.first && rows[col.table] > 0))
+      return fail(CX_E_MISSING, "cx_execute: buffer %s is not in the execution context", col.name.c_str());
+    if (it->second.second < (uint64_t)rows[col.table])
+      return fail(CX_E_CAPACITY, "cx_execute: buffer %s holds %llu rows, table has %lld", col.name.c_str(),
+                  (unsigned long long)it->second.second, rows[col.table]);
+    a.col[col.slot] = (const int*)it->second.first;
+  }
+  for (const auto& nl : lp.nulls) {
+    auto it = c->nulls.find(nl.second);
+    if (it == c->nulls.end()) continue;  // no bitmap registered: every row valid (getNullBitmap -> nullptr)
+    int table = 0;
+    for (const auto& col : lp.cols)
+      if (col.slot == nl.first) table = col.table;
+    if (it->second.second < ((uint64_t)rows[table] + 63) / 64)
+      return fail(CX_E_CAPACITY, "cx_execute: validity of %s is shorter than its table", nl.second.c_str());
+    a.nul[nl.first] = (const unsigned long long*)it->second.first;
+  }
+  const uint64_t vwords = (lp.result_words + 63) / 64;
+  if (!c->result || c->result_words < lp.result_words)
+    return fail(CX_E_CAPACITY, "cx_execute: result buffer holds %llu words, query needs %llu",
+                (unsigned long long)c->result_words, (unsigned long long)lp.result_words);
+  if (!c->validity || c->validity_words < vwords)
+    return fail(CX_E_CAPACITY, "cx_execute: validity buffer holds %llu words, query needs %llu",
+                (unsigned long long)c->validity_words, (unsigned long long)vwords);
+  a.result = (unsigned long long*)c->result;
+  a.result_validity = (unsigned long long*)c->validity;
+
+  int dev = 0;
+  CX_CUDA(cudaGetDevice(&dev));
+  int rc = ensure_ctx_device(c, dev);
+  if (rc) return rc;
+  cx_module::Loaded* L = nullptr;
+  rc = load_on_device(m, dev, &L);
+  if (rc) return rc;
+
+  // Scratch.
+  char* scratch = nullptr;
+  if (c->user_scratch) {
+    if (c->user_scratch_bytes < m->sl.total)
+      return fail(CX_E_CAPACITY, "cx_execute: caller scratch holds %llu bytes, query needs %llu",
+                  (unsigned long long)c->user_scratch_bytes, (unsigned long long)m->sl.total);
+    scratch = (char*)c->user_scratch;
+  } else {
+    if (c->own_scratch_bytes < m->sl.total) {
+      if (c->own_scratch) {
+        if (c->pending) cudaEventSynchronize(c->ev[3]);
+        cudaFree(c->own_scratch);
+        c->own_scratch = nullptr;
+        c->own_scratch_bytes = 0;
+      }
+      const uint64_t grow = m->sl.total + m->sl.total / 2;  // 1.5x high-water, as DynamicDeviceBuffer
+      CX_CUDA(cudaMalloc(&c->own_scratch, grow));
+      c->own_scratch_bytes = grow;
+    }
+    scratch = (char*)c->own_scratch;
+  }
+  for (size_t i = 0; i < lp.hts.size(); ++i) {
+    a.ht[lp.hts[i].slot] = (int*)(scratch + m->sl.ht_off[i]);
+    if (lp.htv_words.count(lp.hts[i].slot)) a.htv[lp.hts[i].slot] = (unsigned int*)(scratch + m->sl.htv_off[i]);
+  }
+  a.touched = (unsigned int*)(scratch + m->sl.touched_off);
+  a.finalize_tmp = (unsigned long long*)(scratch + m->sl.fin_off);
+  a.err = (unsigned int*)(scratch + m->sl.err_off);
+
+  int sms = c->sm_override;
+  if (sms <= 0) CX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+
+  Driver& d = driver();
+  int launches = 0, scan_grid = 0;
+  void* params[] = {&a};
+  auto launch = [&](size_t ki, unsigned grid) -> int {
+    const KernelSpec& k = lp.kernels[ki];
+    if (grid == 0) return CX_OK;
+    CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, (unsigned)k.smem, (CUstream)stream, params, nullptr);
+    if (r != CUDA_SUCCESS) return drv_fail(r, k.name.c_str());
+    ++launches;
+    return CX_OK;
+  };
+
+  CX_CUDA(cudaEventRecord(c->ev[0], stream));
+  CX_CUDA(cudaMemsetAsync(scratch, 0, m->sl.total, stream));
+  CX_CUDA(cudaMemsetAsync(c->result, 0, lp.result_words * 8, stream));
+  CX_CUDA(cudaMemsetAsync(c->validity, 0, vwords * 8, stream));
+  size_t ki = 0;
+  // Phase 1: slot initialisation and hash-table builds.
+  for (; ki < lp.kernels.size() && lp.kernels[ki].kind != "scan"; ++ki) {
+    const KernelSpec& k = lp.kernels[ki];
+    unsigned grid = 0;
+    if (k.kind == "groups") grid = (unsigned)((lp.groups + k.block - 1) / k.block);
+    else if (k.kind == "build") {
+      const long long tiles = (rows[k.table] + k.tile - 1) / k.tile;
+      grid = (unsigned)std::min<long long>(tiles, (long long)sms * 16);
+    }
+    if ((rc = launch(ki, grid))) return rc;
+  }
+  CX_CUDA(cudaEventRecord(c->ev[1], stream));
+  // Phase 2: the fused scan.
+  if (ki < lp.kernels.size()) {
+    const KernelSpec& k = lp.kernels[ki];
+    const long long tiles = (rows[0] + k.tile - 1) / k.tile;
+    const int per_sm = std::max(1, std::min(k.ctas_per_sm, L->occupancy[ki]));
+    const long long grid = std::min<long long>(tiles, (long long)sms * per_sm);
+    scan_grid = (int)grid;
+    if ((rc = launch(ki, (unsigned)grid))) return rc;
+    ++ki;
+  }
+  CX_CUDA(cudaEventRecord(c->ev[2], stream));
+  // Phase 3: epilogues.
+  for (; ki < lp.kernels.size(); ++ki) {
+    const KernelSpec& k = lp.kernels[ki];
+    unsigned grid = (unsigned)((lp.groups + k.block - 1) / k.block);
+    if ((rc = launch(ki, grid))) return rc;
+  }
+  if (lp.finalize) {
+    const uint64_t vis = lp.fin_groups * (uint64_t)lp.fin_vts;
+    CX_CUDA(cudaMemcpyAsync(c->result, a.finalize_tmp, vis * 8, cudaMemcpyDeviceToDevice, stream));
+    CX_CUDA(cudaMemcpyAsync(c->validity, a.finalize_tmp + vis, ((vis + 63) / 64) * 8, cudaMemcpyDeviceToDevice, stream));
+  }
+  CX_CUDA(cudaMemcpyAsync(c->host_err, a.err, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
+  CX_CUDA(cudaEventRecord(c->ev[3], stream));
+  c->pending = true;
+  c->timing = cx_timing{};
+  c->timing.scan_grid = scan_grid;
+  c->timing.gpu_launches = launches;
+  return CX_OK;
+}
+
+int cx_ctx_sync(cx_exec_ctx* c) {
+  if (!c) return fail(CX_E_INVALID, "cx_ctx_sync: NULL context");
+  if (!c->pending) return CX_OK;
+  CX_CUDA(cudaEventSynchronize(c->ev[3]));
+  c->pending = false;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+  c->timing.build_ms = ms;
+  cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]);
+  c->timing.scan_ms = ms;
+  cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+  c->timing.post_ms = ms;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[3]);
+  c->timing.total_ms = ms;
+  c->kernel_err = *c->host_err;
+  if (c->kernel_err) return fail(CX_E_KERNEL, "kernel raised error code %u", c->kernel_err);
+  return CX_OK;
+}
+
+int cx_ctx_timing(const cx_exec_ctx* c, cx_timing* t) {
+  if (!c || !t) return fail(CX_E_INVALID, "cx_ctx_timing: NULL argument");
+  *t = c->timing;
+  return CX_OK;
+}
+
+int cx_ctx_kernel_error(const cx_exec_ctx* c, uint32_t* code) {
+  if (!c || !code) return fail(CX_E_INVALID, "cx_ctx_kernel_error: NULL argument");
+  *code = c->kernel_err;
+  return CX_OK;
+}
+
+}  // extern "C"

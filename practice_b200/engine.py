@@ -1,0 +1,162 @@
+"""Host facade over libcrystal_b200.so: resident tables, compiled-query cache,
+query execution and result fetch.
+
+This plays the role of the reference's DatabaseInstance + QueryEngine for the
+hot path (src/db/database_instance.cpp:138-439, src/core/execution.cpp:652-725):
+columns are loaded once and stay resident in HBM, each plan is generated,
+compiled (cached by plan text and tuning) and executed through the C ABI, and
+results come back as typed rows.  PyTorch only provides device memory and
+streams; every kernel comes from the library.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib, datagen
+from .plan import Plan, Table
+from .results import rows as result_rows
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("crystal-b200 needs a CUDA device (no CPU fallback exists)")
+    return torch
+
+
+@dataclass
+class QueryResult:
+    words: np.ndarray      # u64 result words (final layout)
+    validity: np.ndarray   # u64 validity words
+    timing: _lib.Timing
+    kernel_error: int
+
+    def rows(self, plan: Plan) -> list[tuple]:
+        return result_rows(plan, self.words, self.validity)
+
+
+class Database:
+    """Resident star-schema tables on one GPU."""
+
+    def __init__(self, device: int = 0):
+        torch = _torch()
+        self.torch = torch
+        self.device = torch.device("cuda", device)
+        torch.cuda.set_device(self.device)
+        self.cols: dict[str, object] = {}      # name -> int32 tensor
+        self.valid: dict[str, object] = {}     # name -> int64 tensor of validity words
+        self.rows: dict[str, int] = {}         # table -> rows
+        self.tables: dict[str, Table] = {}
+        self._modules: dict[tuple, _lib.Module] = {}
+        self.ctx = _lib.ExecCtx()
+        self._bound: set[str] = set()
+
+    def reset(self) -> None:
+        """Drops every resident table and starts a fresh execution context."""
+        self.ctx.close()
+        self.ctx = _lib.ExecCtx()
+        self.cols.clear()
+        self.valid.clear()
+        self.rows.clear()
+        self.tables.clear()
+
+    # ------------------------------------------------------------ loading
+    def load_column(self, table: str, name: str, data) -> None:
+        torch = self.torch
+        if isinstance(data, np.ndarray):
+            t = torch.from_numpy(np.ascontiguousarray(data, dtype=np.int32)).to(self.device)
+        else:
+            t = data
+        self.cols[name] = t
+        self.rows[table] = int(t.numel()) if table not in self.rows else self.rows[table]
+        self.ctx.set_buffer("d_" + name, t.data_ptr(), t.numel())
+
+    def load_validity(self, name: str, words) -> None:
+        torch = self.torch
+        if isinstance(words, np.ndarray):
+            t = torch.from_numpy(np.ascontiguousarray(words).view(np.int64)).to(self.device)
+        else:
+            t = words
+        self.valid[name] = t
+        self.ctx.set_null_bitmap("d_" + name, t.data_ptr(), t.numel())
+
+    def set_rows(self, table: str, rows: int) -> None:
+        self.rows[table] = rows
+        self.ctx.set_rows(table, rows)
+
+    def load_host_tables(self, ht: datagen.HostTables, tables: dict[str, Table]) -> None:
+        for tname, t in tables.items():
+            present = [c for c in t.cols if c in ht.columns]
+            if not present:
+                continue
+            for c in present:
+                self.load_column(tname, c, ht.columns[c])
+            self.set_rows(tname, len(ht.columns[present[0]]))
+            self.tables[tname] = t
+        for c, w in ht.validity.items():
+            self.load_validity(c, w)
+
+    def generate_ssb(self, fact_rows: int, seed: int, fact_cols: list[str], nulls: dict[str, int] | None = None,
+                     dims: tuple[str, ...] = ("DDATE", "CUSTOMER", "SUPPLIER", "PART")) -> None:
+        """Generates the fact table on the device and the dimensions on the host."""
+        torch = self.torch
+        tables = datagen.ssb_tables(fact_rows, fact_cols)
+        for c in fact_cols:
+            t = torch.empty(fact_rows, dtype=torch.int32, device=self.device)
+            datagen.fact_column_device(c, seed, fact_rows, t.data_ptr(), torch.cuda.current_stream().cuda_stream)
+            self.load_column("LINEORDER", c, t)
+        self.set_rows("LINEORDER", fact_rows)
+        self.tables["LINEORDER"] = tables["LINEORDER"]
+        for d in dims:
+            for c, v in datagen.dim_columns(d, seed).items():
+                self.load_column(d, c, v)
+            self.set_rows(d, datagen.DIM_ROWS[d])
+            self.tables[d] = tables[d]
+        for c, permille in (nulls or {}).items():
+            rows = fact_rows if c.startswith("lo_") else datagen.DIM_ROWS[
+                {"c": "CUSTOMER", "s": "SUPPLIER", "p": "PART", "d": "DDATE"}[c[0]]]
+            w = torch.empty((rows + 63) // 64, dtype=torch.int64, device=self.device)
+            datagen.validity_device(c, seed, rows, permille, w.data_ptr(), torch.cuda.current_stream().cuda_stream)
+            self.load_validity(c, w)
+        torch.cuda.synchronize()
+
+    # ----------------------------------------------------------- queries
+    def compile(self, plan: Plan, tuning: _lib.Tuning | None = None) -> _lib.Module:
+        tkey = tuple(getattr(tuning, f) for f, _ in _lib.Tuning._fields_) if tuning is not None else None
+        key = (plan.text(), tkey)
+        m = self._modules.get(key)
+        if m is None:
+            src = _lib.codegen(plan.text(), tuning)
+            m = _lib.Module(src, key=f"{plan.name}_{abs(hash(key))}")
+            self._modules[key] = m
+        return m
+
+    def alloc_result(self, module: _lib.Module):
+        torch = self.torch
+        res = torch.empty(max(int(module.info.result_words), 1), dtype=torch.int64, device=self.device)
+        val = torch.empty(max(int(module.info.validity_words), 1), dtype=torch.int64, device=self.device)
+        return res, val
+
+    def execute(self, plan: Plan, tuning: _lib.Tuning | None = None, stream=None) -> QueryResult:
+        torch = self.torch
+        m = self.compile(plan, tuning)
+        res, val = self.alloc_result(m)
+        for t, n in self.rows.items():
+            self.ctx.set_rows(t, n)
+        self.ctx.set_result(res.data_ptr(), res.numel(), val.data_ptr(), val.numel())
+        s = stream if stream is not None else torch.cuda.current_stream()
+        self.ctx.execute(m, s.cuda_stream)
+        err = 0
+        try:
+            self.ctx.sync()
+        except _lib.CxError as e:
+            if e.code != -6:
+                raise
+            err = self.ctx.kernel_error()
+        fw = int(m.info.final_words)
+        words = res.cpu().numpy().view(np.uint64)[:fw].copy()
+        validity = val.cpu().numpy().view(np.uint64)[: (fw + 63) // 64].copy()
+        return QueryResult(words, validity, self.ctx.timing(), err)

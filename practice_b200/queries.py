@@ -1,0 +1,155 @@
+"""Query plans of the measured workloads and of the reference's known-answer set.
+
+* ``config1`` -- plain single query over a 6M-row fact table: date join with
+  year = 1995 (PHT_1), discount in [2, 4], quantity < 30,
+  SUM(extendedprice * discount) (SSB Q1.1 shape, test/queries/sql/q11.sql).
+* ``config2`` -- four-dimension star: customer region = r, supplier region = r,
+  year in [1992, 1997], GROUP BY (c_nation, s_nation, d_year), SUM(revenue),
+  ORDER BY year ASC, sum DESC (SSB Q3.1 shape, test/queries/sql/q31.sql).
+* ``config3`` -- the nullable three-valued-logic variant: NULL revenue and
+  NULL customer.city, IS NULL / IS NOT NULL and range predicates that yield
+  UNKNOWN; COUNT(*), COUNT(revenue), SUM(revenue) grouped by a nullable key.
+* ``template(t, rng)`` -- the four shared-scan templates: T0 range filters +
+  scalar SUM; T1 date join + GROUP BY year; T2 three joins + GROUP BY
+  (nation, year); T3 four joins + GROUP BY (brand, year) (<= 7,000 groups).
+* ``kat_*`` -- the five queries of test/nullable_data/queries.sql.
+"""
+from __future__ import annotations
+
+import random
+
+from .datagen import GROUP_STATS, ssb_tables
+from .plan import Group, Plan, PlanBuilder, Table, and_, case, col, lit, not_, or_, star
+
+C1_COLS = ["lo_orderdate", "lo_quantity", "lo_discount", "lo_extendedprice"]
+C2_COLS = ["lo_orderdate", "lo_custkey", "lo_suppkey", "lo_partkey", "lo_revenue", "lo_supplycost"]
+C4_COLS = ["lo_orderdate", "lo_custkey", "lo_suppkey", "lo_partkey", "lo_quantity", "lo_discount",
+           "lo_revenue", "lo_supplycost"]
+
+
+def _g(name: str, nullable: bool = False) -> Group:
+    mn, card = GROUP_STATS[name]
+    return Group(col(name), mn, card, nullable)
+
+
+def config1(fact_rows: int = 6_000_000, year: int = 1995, disc: tuple[int, int] = (2, 4), qty: int = 30) -> Plan:
+    t = ssb_tables(fact_rows, C1_COLS)
+    b = PlanBuilder(t, "LINEORDER", name="config1")
+    b.filter(and_(col("lo_discount").ge(disc[0]), col("lo_discount").le(disc[1]), col("lo_quantity").lt(qty)))
+    b.join("DDATE", "lo_orderdate", where=col("d_year").eq(year))
+    return b.aggregate([], [("sum", col("lo_extendedprice") * col("lo_discount"))])
+
+
+def config2(fact_rows: int = 60_000_000, region: int = 2, years: tuple[int, int] = (1992, 1997)) -> Plan:
+    t = ssb_tables(fact_rows, C2_COLS)
+    b = PlanBuilder(t, "LINEORDER", name="config2")
+    b.join("CUSTOMER", "lo_custkey", where=col("c_region").eq(region))
+    b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(region))
+    b.join("DDATE", "lo_orderdate", where=and_(col("d_year").ge(years[0]), col("d_year").le(years[1])))
+    return b.aggregate([_g("c_nation"), _g("s_nation"), _g("d_year")], [("sum", col("lo_revenue"))],
+                       order_by=[(2, False), (3, True)])
+
+
+def config3(fact_rows: int = 60_000_000, region: int = 1, years: tuple[int, int] = (1993, 1998),
+            rev_floor: int = 2_000_000) -> Plan:
+    t = ssb_tables(fact_rows, C2_COLS)
+    nullable = {"lo_revenue", "c_city"}
+    b = PlanBuilder(t, "LINEORDER", nullable=nullable, name="config3")
+    # (revenue >= floor OR revenue IS NULL) AND NOT (revenue > 9,500,000): UNKNOWN
+    # for NULL revenue on the range terms, rescued by IS NULL on the OR.
+    b.filter(and_(or_(col("lo_revenue").ge(rev_floor), col("lo_revenue").is_null()),
+                  not_(col("lo_revenue").gt(9_500_000))))
+    b.join("CUSTOMER", "lo_custkey", where=col("c_region").eq(region), payload="c_city")
+    b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(region))
+    b.join("DDATE", "lo_orderdate", where=and_(col("d_year").ge(years[0]), col("d_year").le(years[1])))
+    return b.aggregate([_g("c_city", nullable=True), _g("d_year")],
+                       [("count", star()), ("count", col("lo_revenue")), ("sum", col("lo_revenue"))],
+                       order_by=[(1, False), (0, False)])
+
+
+def config3_tables(fact_rows: int) -> dict[str, Table]:
+    return ssb_tables(fact_rows, C2_COLS)
+
+
+# --------------------------------------------------------------- templates
+
+TEMPLATE_NAMES = ["T0_scan_sum", "T1_date_year", "T2_nation_year", "T3_brand_year"]
+
+
+def template(t: int, rng: random.Random, fact_rows: int = 600_000_000) -> Plan:
+    """One query of template t with constants drawn from rng (selectivity
+    0.01%-20%)."""
+    tables = ssb_tables(fact_rows, C4_COLS)
+    if t == 0:
+        q_hi = rng.randint(2, 50)
+        q_lo = rng.randint(1, q_hi)
+        d_lo = rng.randint(0, 10)
+        d_hi = rng.randint(d_lo, min(10, d_lo + 3))
+        b = PlanBuilder(tables, "LINEORDER", name="T0")
+        b.filter(and_(col("lo_quantity").ge(q_lo), col("lo_quantity").le(q_hi),
+                      col("lo_discount").ge(d_lo), col("lo_discount").le(d_hi)))
+        return b.aggregate([], [("sum", col("lo_revenue") * col("lo_discount"))])
+    if t == 1:
+        y_lo = rng.randint(1992, 1998)
+        y_hi = rng.randint(y_lo, 1998)
+        q = rng.randint(2, 50)
+        b = PlanBuilder(tables, "LINEORDER", name="T1")
+        b.filter(col("lo_quantity").lt(q))
+        b.join("DDATE", "lo_orderdate", where=and_(col("d_year").ge(y_lo), col("d_year").le(y_hi)))
+        return b.aggregate([_g("d_year")], [("sum", col("lo_revenue"))])
+    if t == 2:
+        r = rng.randint(0, 4)
+        s = rng.randint(0, 4)
+        y_lo = rng.randint(1992, 1998)
+        y_hi = rng.randint(y_lo, 1998)
+        b = PlanBuilder(tables, "LINEORDER", name="T2")
+        b.join("CUSTOMER", "lo_custkey", where=col("c_region").eq(r))
+        b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(s))
+        b.join("DDATE", "lo_orderdate", where=and_(col("d_year").ge(y_lo), col("d_year").le(y_hi)))
+        return b.aggregate([_g("c_nation"), _g("d_year")], [("sum", col("lo_revenue"))])
+    cat = rng.randint(0, 24)
+    r = rng.randint(0, 4)
+    s = rng.randint(0, 4)
+    b = PlanBuilder(tables, "LINEORDER", name="T3")
+    b.join("PART", "lo_partkey", where=col("p_category").eq(cat))
+    b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(s))
+    b.join("CUSTOMER", "lo_custkey", where=col("c_region").le(r))
+    b.join("DDATE", "lo_orderdate")
+    return b.aggregate([_g("p_brand1"), _g("d_year")], [("sum", col("lo_revenue") - col("lo_supplycost"))])
+
+
+def batch(n: int, seed: int, fact_rows: int = 600_000_000) -> list[Plan]:
+    rng = random.Random(seed)
+    return [template(rng.randrange(4), rng, fact_rows) for _ in range(n)]
+
+
+# ------------------------------------------------------- known-answer set
+
+KAT_COLS = ["id", "grp", "val", "flag"]
+
+
+def kat_tables(rows: int = 12) -> dict[str, Table]:
+    return {"NULLABLE_NUMBERS": Table("NULLABLE_NUMBERS", list(KAT_COLS), rows, fact=True)}
+
+
+def kat_plans(rows: int = 12, grp_card: int = 4) -> dict[str, Plan]:
+    """test/nullable_data/queries.sql q1-q5 as plans (val and flag nullable)."""
+    t = kat_tables(rows)
+    nul = {"val", "flag"}
+    grp = Group(col("grp"), 1, grp_card, False)
+    plans = {}
+    b = PlanBuilder(t, "NULLABLE_NUMBERS", nullable=nul, name="q1")
+    plans["q1"] = b.aggregate([], [("count", star()), ("count", col("val")), ("sum", col("val")), ("avg", col("val"))])
+    b = PlanBuilder(t, "NULLABLE_NUMBERS", nullable=nul, name="q2")
+    plans["q2"] = b.aggregate([grp], [("count", star()), ("count", col("val")), ("sum", col("val"))],
+                              order_by=[(0, False)])
+    b = PlanBuilder(t, "NULLABLE_NUMBERS", nullable=nul, name="q3")
+    b.filter(col("val").is_null())
+    plans["q3"] = b.aggregate([], [("count", star())])
+    b = PlanBuilder(t, "NULLABLE_NUMBERS", nullable=nul, name="q4")
+    b.filter(col("flag").eq(1))
+    plans["q4"] = b.aggregate([], [("count", star())])
+    b = PlanBuilder(t, "NULLABLE_NUMBERS", nullable=nul, name="q5")
+    plans["q5"] = b.aggregate([Group(col("grp"), 1, grp_card, False)],
+                              [("sum", case(col("val").is_null(), lit(1), lit(0)))], order_by=[(0, False)])
+    return plans

@@ -1,0 +1,158 @@
+"""CPU tests of the product library: it loads without a GPU, exports every
+symbol include/crystal_b200.h declares, generates CUDA for every workload plan
+and compiles it with NVRTC for sm_100a (NVRTC needs no device), and rejects bad
+input with status codes instead of exceptions."""
+import random
+import re
+from pathlib import Path
+
+import pytest
+
+from practice_b200 import _lib, queries
+from practice_b200.plan import PlanBuilder, Table, col, star
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "crystal_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cx_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(_lib.lib, s), s
+    assert sorted(_lib.EXPORTS) == syms
+    assert _lib.lib.cx_abi_version() == 1
+
+
+def all_plans():
+    rng = random.Random(3)
+    plans = {"config1": queries.config1(), "config2": queries.config2(), "config3": queries.config3()}
+    for t in range(4):
+        plans[f"T{t}"] = queries.template(t, rng)
+    for k, p in queries.kat_plans().items():
+        plans["kat_" + k] = p
+    return plans
+
+
+@pytest.mark.parametrize("name", list(all_plans()))
+def test_generated_source_compiles_for_sm100a(name):
+    plan = all_plans()[name]
+    src = _lib.codegen(plan.text())
+    assert src.startswith("/*@cx-launch")
+    m = _lib.Module(src, key="cpu_" + name)
+    assert m.info.result_words == plan.group_slots * plan.storage_ts
+    assert m.info.sparse == int(plan.sparse)
+    if plan.steps and any(k == "join" for k, _ in plan.steps):
+        assert "BlockProbeAndPHT" in src and "build_hashtable_" in src
+    assert "cp.async.bulk" not in src  # staging goes through the header helper
+    assert "cx::bulk_g2s" in src
+
+
+@pytest.mark.parametrize("bt,ipt,stages,place", [(128, 4, 4, 0), (256, 8, 2, 0), (512, 2, 3, 2), (256, 4, 0, 1),
+                                                 (1024, 1, 2, 0)])
+def test_tuning_space_compiles(bt, ipt, stages, place):
+    t = _lib.default_tuning()
+    t.block_threads, t.items_per_thread, t.stages, t.group_placement = bt, ipt, stages, place
+    for name in ("config2", "config3"):
+        plan = all_plans()[name]
+        _lib.Module(_lib.codegen(plan.text(), t), key=f"tune_{name}_{bt}_{ipt}_{stages}_{place}")
+
+
+def test_reference_style_primitive_calls_compile_against_header():
+    """Lines in the shape the reference visitor emits (visitor.cpp:4233-4288,
+    1838-1880, 4640-4660) compile against crystal_sm100.cuh unchanged."""
+    src = r'''/*@cx-launch
+v 1
+@*/
+#include "cx_args.h"
+#include "crystal_sm100.cuh"
+extern "C" __global__ void ref_style(int* d_lo_quantity, int* d_lo_orderdate, int* d_d_hash_table,
+                                     unsigned long long* d_result, uint64_t* n_lo_quantity, int n) {
+  constexpr int BLOCK_THREADS = 128, ITEMS_PER_THREAD = 4, TILE_SIZE = 512;
+  int tid = threadIdx.x;
+  int tile_offset = blockIdx.x * TILE_SIZE;
+  int num_tile_items = (blockIdx.x == gridDim.x - 1) ? n - tile_offset : TILE_SIZE;
+  int items[ITEMS_PER_THREAD]; int flags[ITEMS_PER_THREAD]; int items2[ITEMS_PER_THREAD];
+  int items_valid[ITEMS_PER_THREAD]; int d_year[ITEMS_PER_THREAD];
+  InitFlags<BLOCK_THREADS, ITEMS_PER_THREAD>(flags);
+  BlockLoad<int, BLOCK_THREADS, ITEMS_PER_THREAD>(d_lo_quantity + tile_offset, tid, tile_offset, items, num_tile_items);
+  BlockLoadValidity<BLOCK_THREADS, ITEMS_PER_THREAD>(n_lo_quantity, tid, tile_offset, items_valid, num_tile_items);
+  BlockPredAGTE<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, items, flags, 2, num_tile_items);
+  BlockPredOrEq<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, items, flags, 7, num_tile_items);
+  BlockApplyValidityAnd<BLOCK_THREADS, ITEMS_PER_THREAD>(tid, flags, items_valid, num_tile_items);
+  BlockLoad<int, BLOCK_THREADS, ITEMS_PER_THREAD>(d_lo_orderdate + tile_offset, tid, tile_offset, items2, num_tile_items);
+  BlockProbeAndPHT_2<int, int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, items2, d_year, flags, d_d_hash_table, 61131, 19920101, num_tile_items);
+  BlockBuildSelectivePHT_1<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, items, flags, d_d_hash_table, 61131, 19920101, num_tile_items);
+  BlockPredALT_Cols<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, items, items2, flags, num_tile_items);
+  for (int i = 0; i < ITEMS_PER_THREAD; ++i) {
+    if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {
+      int hash = (d_year[i] - 1992) % 7;
+      d_result[hash * 2] = static_cast<unsigned long long>(d_year[i]);
+      db::atomic_add_ull(d_result[hash * 2 + 1], (unsigned long long)items[i] * items2[i]);
+      if (db::safe_lt(items[i], db::safe_mul(items2[i], 3))) db::atomic_min_ull(d_result[0], 1ULL);
+    }
+  }
+}
+'''
+    _lib.Module(src, key="ref_style_snippet")
+
+
+def test_bad_plans_return_invalid_status():
+    with pytest.raises(_lib.CxError) as e:
+        _lib.codegen("(query (table T fact (cols a)) (filter (col nope)) (aggregate (count (star))))")
+    assert e.value.code == -1 and "nope" in str(e.value)
+    with pytest.raises(_lib.CxError):
+        _lib.codegen("(query (table T fact (cols a)))")  # no aggregate
+    with pytest.raises(_lib.CxError):
+        _lib.codegen("(query (table T fact (cols a)) (aggregate (group (add (col a) (int 1)) (min 0) (card 2)) (count (star))))")
+    with pytest.raises(_lib.CxError) as e:
+        _lib.Module("__global__ void k() {}")
+    assert e.value.code == -1
+
+
+def test_compile_errors_come_back_with_the_nvrtc_log():
+    with pytest.raises(_lib.CxError) as e:
+        _lib.Module("/*@cx-launch\nv 1\n@*/\n__global__ void k() { this is not cuda; }", key="broken")
+    assert e.value.code == -2 and "error" in str(e.value)
+
+
+def test_module_cache_reuses_compiled_source():
+    plan = all_plans()["kat_q3"]
+    src = _lib.codegen(plan.text())
+    a = _lib.Module(src, key="cache_probe")
+    b = _lib.Module(src, key="cache_probe")
+    assert a.handle.value == b.handle.value
+
+
+def test_execute_without_bound_buffers_reports_missing():
+    plan = all_plans()["kat_q3"]
+    m = _lib.Module(_lib.codegen(plan.text()), key="missing_probe")
+    ctx = _lib.ExecCtx()
+    with pytest.raises(_lib.CxError) as e:
+        ctx.execute(m)
+    assert e.value.code == -4  # rows of NULLABLE_NUMBERS not set: fails before touching a GPU
+    ctx.set_rows("NULLABLE_NUMBERS", 12)
+    with pytest.raises(_lib.CxError) as e:
+        ctx.execute(m)
+    assert e.value.code == -4 and "d_val" in str(e.value)
+
+
+def test_scratch_and_result_shapes():
+    plan = all_plans()["config3"]
+    m = _lib.Module(_lib.codegen(plan.text()), key="shape_probe")
+    assert m.info.groups == 251 * 7
+    assert m.info.storage_ts == 5 and m.info.visible_ts == 5
+    # three hash tables of 2*len ints each plus the payload-validity bits of c_city
+    assert m.scratch_bytes >= 4 * 2 * (300_000 + 20_000 + 61131)
+
+
+def test_plan_text_is_deterministic():
+    assert queries.config2().text() == queries.config2().text()
+    t = {"T": Table("T", ["a"], 1, fact=True)}
+    p = PlanBuilder(t, "T").filter(col("a").gt(3)).aggregate([], [("count", star())])
+    assert "(filter (gt (col a) (int 3)))" in p.text()

@@ -1,0 +1,198 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle on the
+same seeded tables.  Integer work, so the bar is bit-exact: every word of the
+raw aggregate buffer and of its validity bitmap must match."""
+import random
+
+import numpy as np
+import pytest
+
+import oracle
+from practice_b200 import _lib, datagen, queries, results
+from practice_b200.plan import Group, PlanBuilder, and_, col, lit, not_, or_, star
+
+pytestmark = pytest.mark.gpu
+
+DIM_ROWS = {"CUSTOMER": 300_000, "SUPPLIER": 20_000, "DDATE": 2556, "PART": 200_000}
+
+
+@pytest.fixture(scope="module")
+def db():
+    from practice_b200.engine import Database
+    return Database(0)
+
+
+def load(db, seed, n, fact_cols, nulls=None):
+    ht = datagen.host_tables(seed, n, fact_cols, nulls)
+    db.reset()
+    db.load_host_tables(ht, datagen.ssb_tables(n, fact_cols))
+    return ht
+
+
+def oracle_run(plan, ht):
+    rows = {"LINEORDER": ht.fact_rows, **DIM_ROWS}
+    return oracle.run_plan(plan.text(), ht.columns, ht.validity, rows, plan.group_slots * plan.storage_ts)
+
+
+def assert_parity(db, plan, ht, tuning=None):
+    ref = oracle_run(plan, ht)
+    got = db.execute(plan, tuning)
+    assert got.kernel_error == 0
+    np.testing.assert_array_equal(got.words, ref.words)
+    np.testing.assert_array_equal(got.validity, ref.validity)
+    return got, ref
+
+
+@pytest.mark.parametrize("n", [1_000_000, 1_000_003, 511, 1])
+def test_config1_shape(db, n):
+    ht = load(db, 11, n, queries.C1_COLS)
+    got, _ = assert_parity(db, queries.config1(n), ht)
+    if n >= 1_000_000:
+        assert got.words[0] != 0
+
+
+def test_config2_shape(db):
+    n = 2_000_000
+    ht = load(db, 12, n, queries.C2_COLS)
+    plan = queries.config2(n)
+    got, _ = assert_parity(db, plan, ht)
+    assert len(got.rows(plan)) > 100
+
+
+def test_config3_nullable(db):
+    n = 2_000_003
+    ht = load(db, 13, n, queries.C2_COLS, nulls={"lo_revenue": 100, "c_city": 50})
+    plan = queries.config3(n)
+    got, _ = assert_parity(db, plan, ht)
+    rs = got.rows(plan)
+    assert any(r[0] is None for r in rs), "NULL c_city must form its own group"
+    assert any(r[2] < r[1] for r in rs), "COUNT(revenue) must skip NULL revenue"
+
+
+@pytest.mark.parametrize("t", [0, 1, 2, 3])
+def test_shared_scan_templates(db, t):
+    n = 1_500_000
+    ht = load(db, 14, n, queries.C4_COLS)
+    rng = random.Random(100 + t)
+    for _ in range(3):
+        assert_parity(db, queries.template(t, rng, n), ht)
+
+
+@pytest.mark.parametrize("bt,ipt,stages,place", [(128, 4, 4, 0), (256, 8, 2, 0), (512, 2, 3, 2), (256, 4, 0, 1),
+                                                 (1024, 1, 2, 0), (256, 4, 6, 2)])
+def test_tuning_invariance(db, bt, ipt, stages, place):
+    n = 777_777
+    ht = load(db, 15, n, queries.C2_COLS, nulls={"lo_revenue": 100, "c_city": 50})
+    t = _lib.default_tuning()
+    t.block_threads, t.items_per_thread, t.stages, t.group_placement = bt, ipt, stages, place
+    assert_parity(db, queries.config3(n), ht, t)
+    assert_parity(db, queries.config2(n), ht, t)
+
+
+def test_empty_fact_table(db):
+    ht = load(db, 16, 0, queries.C1_COLS)
+    got, ref = assert_parity(db, queries.config1(0), ht)
+    assert int(got.words[0]) == 0
+
+
+def test_empty_selection_and_all_null(db):
+    n = 100_000
+    ht = load(db, 17, n, queries.C2_COLS, nulls={"lo_revenue": 1000, "c_city": 1000})
+    assert_parity(db, queries.config2(n, years=(2050, 2060)), ht)
+    plan = queries.config3(n)
+    got, _ = assert_parity(db, plan, ht)
+    assert all(r[0] is None and r[2] == 0 for r in got.rows(plan))
+
+
+def test_min_max_avg_and_case(db):
+    n = 300_001
+    ht = load(db, 18, n, queries.C4_COLS, nulls={"lo_revenue": 200})
+    tabs = datagen.ssb_tables(n, queries.C4_COLS)
+    nul = {"lo_revenue"}
+    b = PlanBuilder(tabs, "LINEORDER", nullable=nul)
+    b.filter(or_(col("lo_quantity").lt(10), col("lo_revenue").is_null()))
+    b.join("DDATE", "lo_orderdate", where=col("d_month").le(6))
+    plan = b.aggregate([Group(col("d_year"), 1992, 7)],
+                       [("min", col("lo_revenue")), ("max", col("lo_revenue") - col("lo_supplycost")),
+                        ("avg", col("lo_revenue")), ("count", col("lo_revenue")),
+                        ("sum", queries.case(col("lo_revenue").is_null(), lit(1), lit(0)))])
+    assert_parity(db, plan, ht)
+    b = PlanBuilder(tabs, "LINEORDER", nullable=nul)
+    b.filter(not_(col("lo_discount").ge(5)))
+    plan = b.aggregate([], [("min", col("lo_revenue")), ("max", col("lo_supplycost")), ("avg", col("lo_quantity")),
+                            ("count", star()), ("sum", col("lo_quantity") * col("lo_discount") + lit(3))])
+    assert_parity(db, plan, ht)
+
+
+def test_kat_on_gpu(db):
+    import json
+    from pathlib import Path
+    gold = json.loads((Path(__file__).parent / "golden" / "reference_kats.json").read_text())
+    t = gold["nullable_kat"]["columns"]
+    n = len(t["id"])
+    db.reset()
+    for c in t:
+        db.load_column("NULLABLE_NUMBERS", c, np.array([v if v is not None else 0 for v in t[c]], dtype=np.int32))
+    for c in ("val", "flag"):
+        bits = np.zeros(64, dtype=np.uint8)
+        bits[:n] = [v is not None for v in t[c]]
+        db.load_validity(c, np.packbits(bits, bitorder="little").view("<u8").astype(np.uint64))
+    db.set_rows("NULLABLE_NUMBERS", n)
+    for q, plan in queries.kat_plans(n).items():
+        got = db.execute(plan)
+        rs = got.rows(plan)
+        if q == "q4":
+            assert rs == [(5,)]
+            continue
+        exp = gold["nullable_kat"]["expected"][q]["rows"]
+        assert [list(r) for r in rs] == [[pytest.approx(v) if isinstance(v, float) else v for v in e] for e in exp]
+
+
+def test_group_domain_violation_is_reported(db):
+    """A GROUP BY key outside its catalog domain raises error code 2 (the
+    reference folds it silently into another group)."""
+    n = 50_000
+    ht = load(db, 19, n, queries.C4_COLS)
+    tabs = datagen.ssb_tables(n, queries.C4_COLS)
+    b = PlanBuilder(tabs, "LINEORDER")
+    b.join("DDATE", "lo_orderdate")
+    plan = b.aggregate([Group(col("d_year"), 1992, 5)], [("count", star())])
+    ref = oracle_run(plan, ht)
+    got = db.execute(plan)
+    assert ref.domain_errors > 0
+    assert got.kernel_error == 2
+
+
+def test_device_generator_matches_host(db):
+    import torch
+    n = 1_000_037
+    for c in queries.C4_COLS + ["lo_extendedprice"]:
+        t = torch.empty(n, dtype=torch.int32, device="cuda")
+        datagen.fact_column_device(c, 5, n, t.data_ptr())
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(t.cpu().numpy(), datagen.fact_column(c, 5, 0, n))
+    w = torch.empty((n + 63) // 64, dtype=torch.int64, device="cuda")
+    datagen.validity_device("lo_revenue", 5, n, 100, w.data_ptr())
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(w.cpu().numpy().view(np.uint64),
+                                  datagen.validity_words(5, datagen.STREAMS["valid_lo_revenue"], n, 100))
+
+
+def test_sparse_compaction(db):
+    import torch
+    n = 400_000
+    ht = load(db, 20, n, queries.C4_COLS)
+    plan = queries.template(3, random.Random(7), n)
+    assert plan.sparse
+    got = db.execute(plan)
+    src = torch.from_numpy(got.words.view(np.int64)).cuda()
+    dst = torch.zeros_like(src)
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    _lib.check(_lib.lib.cx_compact_sparse(src.data_ptr(), plan.group_slots, plan.storage_ts, dst.data_ptr(),
+                                          cnt.data_ptr(), None))
+    torch.cuda.synchronize()
+    k = int(cnt.item())
+    ts = plan.storage_ts
+    tuples = got.words.reshape(-1, ts)
+    expect = tuples[(tuples != 0).any(axis=1)]
+    assert k == len(expect) > 0
+    np.testing.assert_array_equal(dst.cpu().numpy().view(np.uint64)[: k * ts].reshape(-1, ts), expect)

@@ -660,12 +660,13 @@ CX_DEVICE bool mbar_wait_bounded(unsigned long long* bar, unsigned phase, unsign
   return false;
 }
 
-// After a staging wait gave up, waits (bounded) for the copies this CTA still
-// has in flight -- local iterations k_iter .. k_iter+nstage-1 of the tile
-// sequence blockIdx.x + k*gridDim.x -- so no bulk copy lands in shared memory
+// After a staging wait gave up, waits (bounded) for the copies this warp still
+// has in flight -- local iterations k_iter .. k_iter+nstage-1 of its tile
+// sequence first, first+stride, ... -- so no bulk copy lands in shared memory
 // after the CTA has exited.  Cold path, kept out of line.
-static __device__ __noinline__ void drain_stages(unsigned long long* bars, int nstage, long long k_iter, long long full_tiles,
-                                          unsigned limit);
+static __device__ __noinline__ void drain_stages(unsigned long long* bars, int nstage, long long k_iter,
+                                                 long long first, long long stride, long long full_tiles,
+                                                 unsigned limit);
 
 // L2 policy that marks streamed fact bytes evict-first so dimension hash tables
 // stay resident in L2.
@@ -687,11 +688,12 @@ CX_DEVICE void bulk_g2s(void* smem_dst, const void* gmem_src, unsigned bytes, un
       : "memory");
 }
 
-static __device__ __noinline__ void drain_stages(unsigned long long* bars, int nstage, long long k_iter, long long full_tiles,
-                                          unsigned limit) {
+static __device__ __noinline__ void drain_stages(unsigned long long* bars, int nstage, long long k_iter,
+                                                 long long first, long long stride, long long full_tiles,
+                                                 unsigned limit) {
   for (int j = 0; j < nstage; ++j) {
     const long long kk = k_iter + j;
-    const long long tt = (long long)blockIdx.x + kk * gridDim.x;
+    const long long tt = first + kk * stride;
     if (tt < full_tiles) (void)mbar_wait_bounded(&bars[kk % nstage], (unsigned)((kk / nstage) & 1), limit);
   }
 }

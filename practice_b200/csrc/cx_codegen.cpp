@@ -361,9 +361,10 @@ struct Emitter {
 
   // ----------------------------------------------------------------- scan --
   void emit_scan() {
-    const int BT = tu.block_threads, IPT = tu.items_per_thread;
-    const int TILE = BT * IPT;
-    if (BT % 32 || BT < 32 || BT > 1024 || IPT < 1 || IPT > 16) throw PlanError("bad block shape");
+    const int CTA = tu.block_threads, IPT = tu.items_per_thread;
+    if (CTA % 32 || CTA < 32 || CTA > 1024 || IPT < 1 || IPT > 16) throw PlanError("bad block shape");
+    const int NW = CTA / 32;
+    const int WT = 32 * IPT;  // rows of one warp tile
     const std::string fact = p.tables[0].name;
 
     // Fact columns the pipeline reads, in first-use order.
@@ -397,39 +398,46 @@ struct Emitter {
     for (const auto& ag : p.aggs) n_avg += ag.fn == AggFn::Avg;
     const int NACC = NA + n_avg;                 // accumulator words per group
     std::vector<int> seen_idx(NA, -1);           // SUM/MIN/MAX track "any valid input"
+    std::vector<int> avg_idx(NA, -1);            // accumulator word of an AVG's hidden count
     int NSEEN = 0;
-    for (int k = 0; k < NA; ++k) {
+    for (int k = 0, ai = 0; k < NA; ++k) {
       const AggFn f = p.aggs[k].fn;
       if (f == AggFn::Sum || f == AggFn::Min || f == AggFn::Max) seen_idx[k] = NSEEN++;
+      if (f == AggFn::Avg) avg_idx[k] = NA + ai++;
     }
-    const unsigned long long TW = (G + 31) / 32;  // bitmap words per group bitmap
+    const int NSEEN_T = p.sparse ? 0 : NSEEN;    // seen bitmaps actually kept
+    const unsigned long long TW = (G + 31) / 32; // words of one group bitmap
 
-    // Shared memory layout.
-    const unsigned long long stage_bytes = (unsigned long long)STAGES * NSC * TILE * 4;
-    unsigned long long off = stage_bytes;
-    const unsigned long long bars_off = off; off += (unsigned long long)std::max(STAGES, 1) * 8;
-    const unsigned long long red_off = off; off += (unsigned long long)(BT / 32) * 8;
+    // Shared memory: per-warp staging rings, per-warp mbarriers, reduction
+    // scratch, then the group tables (one per CTA, or one per warp when the
+    // group domain is small enough to replicate).
+    const unsigned long long warp_stage_ints = (unsigned long long)STAGES * NSC * WT;
+    unsigned long long off = (unsigned long long)NW * warp_stage_ints * 4;
+    const unsigned long long bars_off = off; off += (unsigned long long)NW * std::max(STAGES, 1) * 8;
+    const unsigned long long red_off = off; off += (unsigned long long)NW * 8;
     bool smem_groups = false;
+    int REP = 1;
     unsigned long long acc_off = 0, touch_off = 0, seen_off = 0;
     if (grouped) {
-      const unsigned long long need = G * NACC * 8 + TW * 4 * (1 + (p.sparse ? 0 : NSEEN));
+      const unsigned long long one = G * NACC * 8 + TW * 4 * (1 + NSEEN_T);
       if (tu.group_placement == 1) smem_groups = true;
       else if (tu.group_placement == 2) smem_groups = false;
-      else smem_groups = need <= (unsigned long long)tu.smem_group_budget;
+      else smem_groups = one <= (unsigned long long)tu.smem_group_budget;
       if (smem_groups) {
-        acc_off = (off + 15) & ~15ULL; off = acc_off + G * NACC * 8;
-        touch_off = off; off += TW * 4;
-        seen_off = off; off += (p.sparse ? 0 : NSEEN) * TW * 4;
+        if (G <= 256 && one * NW <= (unsigned long long)tu.smem_group_budget) REP = NW;
+        acc_off = (off + 15) & ~15ULL; off = acc_off + (unsigned long long)REP * G * NACC * 8;
+        touch_off = off; off += (unsigned long long)REP * TW * 4;
+        seen_off = off; off += (unsigned long long)REP * NSEEN_T * TW * 4;
       }
     }
     const unsigned long long smem_total = (off + 127) & ~127ULL;
-    if (smem_total > 227 * 1024) throw PlanError("scan kernel shared memory exceeds 227 KB; lower stages or tile size");
+    if (smem_total > 227 * 1024) throw PlanError("scan kernel shared memory exceeds 227 KB; lower stages or items per thread");
+    const unsigned wait_limit = 1u << std::min(30, std::max(10, tu.wait_limit_log2));
 
     const std::string kname = "Scan_" + fact;
-    meta << "kernel " << kname << " scan 0 " << BT << " " << TILE << " " << smem_total << " " << tu.ctas_per_sm << "\n";
+    meta << "kernel " << kname << " scan 0 " << CTA << " " << WT << " " << smem_total << " " << tu.ctas_per_sm << "\n";
     if (grouped && !smem_groups) meta << "touched " << TW << "\n";
 
-    // Register names the body uses.
     std::vector<std::string> reg_cols = fact_cols;
     for (const auto& c : payload_cols) reg_cols.push_back(c);
 
@@ -438,17 +446,24 @@ struct Emitter {
     tile_ptr = [](const std::string& c) { return "t_" + c; };
 
     std::ostringstream& o = src;
-    o << "extern \"C\" __global__ void __launch_bounds__(" << BT << ") " << kname << "(const CxArgs a) {\n";
-    o << "  constexpr int BLOCK_THREADS = " << BT << ", ITEMS_PER_THREAD = " << IPT << ", TILE_SIZE = " << TILE << ";\n";
-    o << "  constexpr int NSTAGE = " << STAGES << ", NSC = " << NSC << ";\n";
+    o << "// Warp-tiled persistent scan: every warp owns a TMA staging ring and\n"
+         "// walks its own sequence of " << WT << "-row tiles; the main loop has no\n"
+         "// CTA-wide barrier, so independent warps hide probe latency.\n";
+    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ") " << kname << "(const CxArgs a) {\n";
+    o << "  constexpr int BLOCK_THREADS = 32, ITEMS_PER_THREAD = " << IPT << ", TILE_SIZE = " << WT << ";\n";
+    o << "  constexpr int NWARP = " << NW << ", NSTAGE = " << STAGES << ", NSC = " << NSC << ";\n";
     o << "  extern __shared__ __align__(1024) unsigned char cx_smem[];\n";
-    o << "  int* stage_buf = (int*)cx_smem; (void)stage_buf;\n";
-    o << "  unsigned long long* bars = (unsigned long long*)(cx_smem + " << bars_off << "); (void)bars;\n";
+    o << "  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
+    o << "  const int tid = lane;\n";
+    o << "  int* stage_buf = (int*)cx_smem + (long long)warp * " << warp_stage_ints << "LL; (void)stage_buf;\n";
+    o << "  unsigned long long* bars = (unsigned long long*)(cx_smem + " << bars_off << ") + warp * "
+      << std::max(STAGES, 1) << "; (void)bars;\n";
     o << "  unsigned long long* red = (unsigned long long*)(cx_smem + " << red_off << "); (void)red;\n";
-    o << "  const int tid = threadIdx.x;\n";
     o << "  const long long n_rows = a.rows[0];\n";
     o << "  const long long num_tiles = (n_rows + TILE_SIZE - 1) / TILE_SIZE;\n";
     o << "  const long long full_tiles = n_rows / TILE_SIZE;\n";
+    o << "  const long long gwarp = (long long)blockIdx.x * NWARP + warp;\n";
+    o << "  const long long nwarps = (long long)gridDim.x * NWARP;\n";
     o << "  unsigned long long* d_result = a.result; (void)d_result;\n";
     o << "  uint64_t* d_result_validity = (uint64_t*)a.result_validity; (void)d_result_validity;\n";
     declare_cols(o, fact_cols, "  ");
@@ -468,75 +483,67 @@ struct Emitter {
         if (p.aggs[k].fn == AggFn::Avg) o << "  unsigned long long cnt_" << k << " = 0ULL;\n";
       }
     } else if (smem_groups) {
-      o << "  unsigned long long* s_acc = (unsigned long long*)(cx_smem + " << acc_off << ");\n";
-      o << "  unsigned int* s_touch = (unsigned int*)(cx_smem + " << touch_off << ");\n";
-      o << "  unsigned int* s_seen = (unsigned int*)(cx_smem + " << seen_off << "); (void)s_seen;\n";
-      o << "  for (long long w = tid; w < " << G * NACC << "LL; w += BLOCK_THREADS) {\n";
-      o << "    const int s = (int)(w % " << NACC << ");\n";
-      o << "    s_acc[w] = ";
+      o << "  unsigned long long* s_acc_all = (unsigned long long*)(cx_smem + " << acc_off << ");\n";
+      o << "  unsigned int* s_touch_all = (unsigned int*)(cx_smem + " << touch_off << ");\n";
+      o << "  unsigned int* s_seen_all = (unsigned int*)(cx_smem + " << seen_off << "); (void)s_seen_all;\n";
+      o << "  unsigned long long* s_acc = s_acc_all + " << (REP > 1 ? "(long long)warp * " + std::to_string(G * NACC) + "LL" : "0") << ";\n";
+      o << "  unsigned int* s_touch = s_touch_all + " << (REP > 1 ? "(long long)warp * " + std::to_string(TW) + "LL" : "0") << ";\n";
+      o << "  unsigned int* s_seen = s_seen_all + " << (REP > 1 ? "(long long)warp * " + std::to_string(NSEEN_T * TW) + "LL" : "0") << "; (void)s_seen;\n";
+      std::string init = "0ULL";
       {
-        // MIN accumulators start at ~0.
-        std::string init = "0ULL";
-        std::vector<int> mins;
+        std::string cond;
         for (int k = 0; k < NA; ++k)
-          if (p.aggs[k].fn == AggFn::Min) mins.push_back(k);
-        if (!mins.empty()) {
-          std::string cond;
-          for (int k : mins) cond += (cond.empty() ? "" : " || ") + std::string("s == ") + std::to_string(k);
-          init = "(" + cond + ") ? ~0ULL : 0ULL";
-        }
-        o << init << ";\n";
+          if (p.aggs[k].fn == AggFn::Min) cond += (cond.empty() ? "" : " || ") + std::string("s == ") + std::to_string(k);
+        if (!cond.empty()) init = "(" + cond + ") ? ~0ULL : 0ULL";
       }
+      o << "  for (long long w = threadIdx.x; w < " << (unsigned long long)REP * G * NACC << "LL; w += " << CTA << ") {\n";
+      o << "    const int s = (int)(w % " << NACC << "); (void)s;\n";
+      o << "    s_acc_all[w] = " << init << ";\n";
       o << "  }\n";
-      o << "  for (long long w = tid; w < " << TW * (1 + (p.sparse ? 0 : NSEEN)) << "LL; w += BLOCK_THREADS) s_touch[w] = 0u;\n";
-      o << "  (void)s_seen;\n";
+      o << "  for (long long w = threadIdx.x; w < " << (unsigned long long)REP * TW * (1 + NSEEN_T) << "LL; w += " << CTA
+        << ") s_touch_all[w] = 0u;\n";
     } else {
       o << "  unsigned int* g_touch = a.touched;\n";
     }
 
-    // TMA staging ring.
+    // Per-warp TMA staging rings.
     if (STAGES > 0) {
       o << "  bool staged_ok = true;\n";
       for (const auto& c : fact_cols) o << "  staged_ok = staged_ok && ((((unsigned long long)d_" << c << ") & 15ULL) == 0ULL);\n";
       o << "  unsigned long long l2_policy = 0;\n";
-      o << "  if (tid == 0) {\n";
+      o << "  if (lane == 0) {\n";
       o << "    for (int s = 0; s < NSTAGE; ++s) cx::mbar_init(&bars[s], 1);\n";
       o << "    cx::fence_mbar_init();\n";
       o << "    l2_policy = cx::l2_evict_first_policy();\n";
       o << "  }\n";
-      o << "  __syncthreads();\n";
-      // Producer: one expect_tx then one bulk copy per staged column.
       o << "#define CX_ISSUE(TILE_, STAGE_) do { \\\n";
-      o << "    cx::mbar_expect_tx(&bars[(STAGE_)], " << (unsigned long long)NSC * TILE * 4 << "u); \\\n";
+      o << "    cx::mbar_expect_tx(&bars[(STAGE_)], " << (unsigned long long)NSC * WT * 4 << "u); \\\n";
       for (int c = 0; c < NSC; ++c)
         o << "    cx::bulk_g2s(stage_buf + ((STAGE_) * NSC + " << c << ") * TILE_SIZE, d_" << fact_cols[c]
-          << " + (TILE_) * TILE_SIZE, " << TILE * 4 << "u, &bars[(STAGE_)], l2_policy); \\\n";
+          << " + (TILE_) * TILE_SIZE, " << WT * 4 << "u, &bars[(STAGE_)], l2_policy); \\\n";
       o << "  } while (0)\n";
-      o << "  if (tid == 0 && staged_ok) {\n";
+    }
+    o << "  __syncthreads();\n";
+    if (STAGES > 0) {
+      o << "  if (lane == 0 && staged_ok) {\n";
       o << "    for (int k = 0; k < NSTAGE; ++k) {\n";
-      o << "      const long long t = (long long)blockIdx.x + (long long)k * gridDim.x;\n";
+      o << "      const long long t = gwarp + (long long)k * nwarps;\n";
       o << "      if (t < full_tiles) CX_ISSUE(t, k);\n";
       o << "    }\n";
       o << "  }\n";
-    } else if (grouped && smem_groups) {
-      o << "  __syncthreads();\n";
-    }
-    if (STAGES > 0 && grouped && smem_groups) {
-      // the ring prologue barrier above also orders the group-table init
     }
 
     o << "  long long k_iter = 0;\n";
     o << "  bool aborted = false; (void)aborted;\n";
-    o << "  for (long long t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k_iter) {\n";
+    o << "  for (long long t = gwarp; t < num_tiles; t += nwarps, ++k_iter) {\n";
     o << "    const long long tile_offset = t * TILE_SIZE;\n";
     o << "    const int num_tile_items = (int)(n_rows - tile_offset < TILE_SIZE ? n_rows - tile_offset : TILE_SIZE);\n";
     if (STAGES > 0) {
       o << "    const int stage = (int)(k_iter % NSTAGE);\n";
       o << "    const bool staged = staged_ok && t < full_tiles;\n";
       o << "    bool timed_out = false;\n";
-      o << "    if (staged) timed_out = !cx::mbar_wait_bounded(&bars[stage], (unsigned)((k_iter / NSTAGE) & 1), "
-        << (1u << std::min(30, std::max(10, tu.wait_limit_log2))) << "u);\n";
-      o << "    if (__syncthreads_or(timed_out)) { if (tid == 0) cx::raise(a.err, cx::ERR_WAIT_TIMEOUT); aborted = true; break; }\n";
+      o << "    if (staged) timed_out = !cx::mbar_wait_bounded(&bars[stage], (unsigned)((k_iter / NSTAGE) & 1), " << wait_limit << "u);\n";
+      o << "    if (__any_sync(0xffffffffu, timed_out)) { if (lane == 0) cx::raise(a.err, cx::ERR_WAIT_TIMEOUT); aborted = true; break; }\n";
       for (int c = 0; c < NSC; ++c)
         o << "    const int* t_" << fact_cols[c] << " = staged ? stage_buf + (stage * NSC + " << c << ") * TILE_SIZE : d_"
           << fact_cols[c] << " + tile_offset;\n";
@@ -548,7 +555,7 @@ struct Emitter {
     declare_regs(o, reg_cols, "    ");
     o << "    InitFlags<BLOCK_THREADS, ITEMS_PER_THREAD>(flags);\n";
 
-    // Pipeline body.
+    // Pipeline body: the reference's primitive calls, one warp tile at a time.
     const std::string ind = "    ";
     for (const auto& s : p.steps) {
       if (s.kind == Step::Filter) {
@@ -607,8 +614,7 @@ struct Emitter {
       o << ind << "  bool act = flags[i] && (tid + BLOCK_THREADS * i < num_tile_items);\n";
       o << ind << "  int hash = 0;\n";
       o << ind << "  if (act) {\n";
-      std::string horner;
-      std::string dom;
+      std::string horner, dom;
       for (size_t k = 0; k < p.groups.size(); ++k) {
         o << ind << "    const int gt" << k << " = " << group_term(k) << ";\n";
         horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(eff_card(k)) + " + gt" + std::to_string(k) + ")";
@@ -619,70 +625,80 @@ struct Emitter {
       o << ind << "    if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
       o << ind << "    if ((unsigned)hash >= " << G << "u) act = false;\n";
       o << ind << "  }\n";
-      const std::string bit = "(1u << (hash & 31))";
-      if (smem_groups) {
-        o << ind << "  if (act) atomicOr(&s_touch[hash >> 5], " << bit << ");\n";
-      } else {
-        o << ind << "  if (act) atomicOr(&g_touch[hash >> 5], " << bit << ");\n";
-      }
+      // One match per item: lanes with the same group merge their updates and
+      // the lowest lane applies them.
+      o << ind << "  const unsigned peers = __match_any_sync(0xffffffffu, act ? (unsigned)hash : 0xffffffffu);\n";
       for (int k = 0; k < NA; ++k) {
         const Agg& ag = p.aggs[k];
         const std::string v = ag.arg->op == Op::Star ? "1" : valid_of(ag.arg.get());
-        const std::string x = ag.fn == AggFn::Count ? "1ULL" : math_push(ag.arg.get(), true);
-        const int slot = (int)p.groups.size() + k;
-        const std::string acc = smem_groups ? "s_acc[(long long)g_ * " + std::to_string(NACC) + " + " + std::to_string(k) + "]"
-                                            : "d_result[(unsigned long long)g_ * " + std::to_string(TS) + "ULL + " +
-                                                  std::to_string(slot) + "]";
-        o << ind << "  {\n";
-        o << ind << "    const bool v_ = act && (" << v << ");\n";
-        if (ag.fn == AggFn::Min || ag.fn == AggFn::Max) {
-          o << ind << "    if (v_) { const int g_ = hash; atomic" << (ag.fn == AggFn::Min ? "Min" : "Max") << "(&" << acc << ", (unsigned long long)(" << x << ")); }\n";
-        } else {
-          o << ind << "    const unsigned long long x_ = v_ ? (unsigned long long)(" << x << ") : 0ULL;\n";
-          o << ind << "    cx::warp_group_add(v_, hash, x_, [&](int g_, unsigned long long s_) { atomicAdd(&" << acc << ", s_); });\n";
-        }
-        if (seen_idx[k] >= 0 && !p.sparse) {
-          if (smem_groups)
-            o << ind << "    if (v_) atomicOr(&s_seen[" << (unsigned long long)seen_idx[k] * TW << "ULL + (hash >> 5)], " << bit << ");\n";
-          else
-            o << ind << "    if (v_) db::atomic_set_valid_bit(d_result_validity, (unsigned long long)hash * " << TS << "ULL + " << slot << ");\n";
-        }
-        if (ag.fn == AggFn::Avg) {
-          const int cs = p.hidden_count_slot(k);
-          const std::string cacc = smem_groups ? "s_acc[(long long)g_ * " + std::to_string(NACC) + " + " + std::to_string(NA + [&] {
-                                                   int r = 0;
-                                                   for (int q = 0; q < k; ++q) r += p.aggs[q].fn == AggFn::Avg;
-                                                   return r;
-                                                 }()) + "]"
-                                               : "d_result[(unsigned long long)g_ * " + std::to_string(TS) + "ULL + " +
-                                                     std::to_string(cs) + "]";
-          o << ind << "    cx::warp_group_add(v_, hash, 1ULL, [&](int g_, unsigned long long s_) { atomicAdd(&" << cacc << ", s_); });\n";
-        }
-        if (ag.fn == AggFn::Count && !p.sparse && !smem_groups) {
-          o << ind << "    if (act) db::atomic_set_valid_bit(d_result_validity, (unsigned long long)hash * " << TS << "ULL + " << slot << ");\n";
-        }
-        o << ind << "  }\n";
+        const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + math_push(ag.arg.get(), true) + ")";
+        o << ind << "  bool v" << k << " = act && (" << v << ");\n";
+        o << ind << "  unsigned long long x" << k << " = v" << k << " ? " << x << " : "
+          << (ag.fn == AggFn::Min ? "~0ULL" : "0ULL") << ";\n";
       }
+      o << ind << "  if (act) {\n";
+      o << ind << "    const int leader = __ffs(peers) - 1;\n";
+      o << ind << "    if (__popc(peers) > 1) {\n";
+      for (int k = 0; k < NA; ++k) {
+        const AggFn f = p.aggs[k].fn;
+        o << ind << "      { unsigned long long r_ = 0" << (f == AggFn::Min ? "xffffffffffffffffULL" : "ULL") << ";\n";
+        o << ind << "        for (unsigned m = peers; m; m &= m - 1) {\n";
+        o << ind << "          const unsigned long long y_ = __shfl_sync(peers, x" << k << ", __ffs(m) - 1);\n";
+        if (f == AggFn::Min) o << ind << "          r_ = y_ < r_ ? y_ : r_;\n";
+        else if (f == AggFn::Max) o << ind << "          r_ = y_ > r_ ? y_ : r_;\n";
+        else o << ind << "          r_ += y_;\n";
+        o << ind << "        }\n";
+        o << ind << "        x" << k << " = r_; }\n";
+        if (f == AggFn::Avg || (seen_idx[k] >= 0 && NSEEN_T > 0))
+          o << ind << "      v" << k << " = __ballot_sync(peers, v" << k << ") != 0u;\n";
+      }
+      o << ind << "    }\n";
+      o << ind << "    if (lane == leader) {\n";
+      const std::string bit = "(1u << (hash & 31))";
+      if (smem_groups) o << ind << "      atomicOr(&s_touch[hash >> 5], " << bit << ");\n";
+      else o << ind << "      atomicOr(&g_touch[hash >> 5], " << bit << ");\n";
+      for (int k = 0; k < NA; ++k) {
+        const Agg& ag = p.aggs[k];
+        const int slot = (int)p.groups.size() + k;
+        const std::string acc = smem_groups ? "s_acc[(long long)hash * " + std::to_string(NACC) + " + " + std::to_string(k) + "]"
+                                            : "d_result[(unsigned long long)hash * " + std::to_string(TS) + "ULL + " +
+                                                  std::to_string(slot) + "]";
+        if (ag.fn == AggFn::Min) o << ind << "      if (v" << k << ") atomicMin(&" << acc << ", x" << k << ");\n";
+        else if (ag.fn == AggFn::Max) o << ind << "      if (v" << k << ") atomicMax(&" << acc << ", x" << k << ");\n";
+        else o << ind << "      if (x" << k << ") atomicAdd(&" << acc << ", x" << k << ");\n";
+        if (seen_idx[k] >= 0 && NSEEN_T > 0) {
+          if (smem_groups)
+            o << ind << "      if (v" << k << ") atomicOr(&s_seen[" << (unsigned long long)seen_idx[k] * TW << "ULL + (hash >> 5)], " << bit << ");\n";
+          else
+            o << ind << "      if (v" << k << ") db::atomic_set_valid_bit(d_result_validity, (unsigned long long)hash * " << TS << "ULL + " << slot << ");\n";
+        }
+        if (ag.fn == AggFn::Count && !p.sparse && !smem_groups)
+          o << ind << "      db::atomic_set_valid_bit(d_result_validity, (unsigned long long)hash * " << TS << "ULL + " << slot << ");\n";
+      }
+      o << ind << "    }\n";
+      for (int k = 0; k < NA; ++k) {
+        if (p.aggs[k].fn != AggFn::Avg) continue;
+        const std::string cacc = smem_groups ? "s_acc[(long long)hash * " + std::to_string(NACC) + " + " + std::to_string(avg_idx[k]) + "]"
+                                             : "d_result[(unsigned long long)hash * " + std::to_string(TS) + "ULL + " +
+                                                   std::to_string(p.hidden_count_slot(k)) + "]";
+        o << ind << "    { const unsigned c_ = __popc(__ballot_sync(peers, act && (" << (p.aggs[k].arg->op == Op::Star ? std::string("1") : valid_of(p.aggs[k].arg.get())) << ")));\n";
+        o << ind << "      if (lane == leader && c_) atomicAdd(&" << cacc << ", (unsigned long long)c_); }\n";
+      }
+      o << ind << "  }\n";
       o << ind << "}\n";
     }
 
-    // Next tile of this stage.
     if (STAGES > 0) {
-      o << "    __syncthreads();\n";
-      o << "    if (tid == 0 && staged_ok) {\n";
-      o << "      const long long t2 = t + (long long)NSTAGE * gridDim.x;\n";
+      o << "    __syncwarp();\n";
+      o << "    if (lane == 0 && staged_ok) {\n";
+      o << "      const long long t2 = t + (long long)NSTAGE * nwarps;\n";
       o << "      if (t2 < full_tiles) CX_ISSUE(t2, stage);\n";
       o << "    }\n";
     }
     o << "  }\n";
-
-    if (STAGES > 0) {
-      // After a timeout, wait (bounded) for the copies still in flight before
-      // the CTA releases its shared memory.
-      o << "  if (aborted && tid == 0 && staged_ok) cx::drain_stages(bars, NSTAGE, k_iter, full_tiles, "
-        << (1u << std::min(30, std::max(10, tu.wait_limit_log2))) << "u);\n";
-      o << "  if (aborted) return;\n";
-    }
+    if (STAGES > 0)
+      o << "  if (aborted && lane == 0 && staged_ok) cx::drain_stages(bars, NSTAGE, k_iter, gwarp, nwarps, full_tiles, "
+        << wait_limit << "u);\n";
 
     // Flush block-private state.
     if (!grouped) {
@@ -690,50 +706,59 @@ struct Emitter {
         const Agg& ag = p.aggs[k];
         o << "  {\n";
         if (ag.fn == AggFn::Min) {
-          o << "    const unsigned long long r_ = cx::block_min_u64<BLOCK_THREADS>(acc_" << k << ", red);\n";
-          o << "    if (tid == 0) db::atomic_min_ull(d_result[" << k << "], r_);\n";
+          o << "    const unsigned long long r_ = cx::block_min_u64<" << CTA << ">(acc_" << k << ", red);\n";
+          o << "    if (threadIdx.x == 0) db::atomic_min_ull(d_result[" << k << "], r_);\n";
         } else if (ag.fn == AggFn::Max) {
-          o << "    const unsigned long long r_ = cx::block_max_u64<BLOCK_THREADS>(acc_" << k << ", red);\n";
-          o << "    if (tid == 0) db::atomic_max_ull(d_result[" << k << "], r_);\n";
+          o << "    const unsigned long long r_ = cx::block_max_u64<" << CTA << ">(acc_" << k << ", red);\n";
+          o << "    if (threadIdx.x == 0) db::atomic_max_ull(d_result[" << k << "], r_);\n";
         } else {
-          o << "    const unsigned long long r_ = cx::block_sum_u64<BLOCK_THREADS>(acc_" << k << ", red);\n";
-          o << "    if (tid == 0) db::atomic_add_ull(d_result[" << k << "], r_);\n";
+          o << "    const unsigned long long r_ = cx::block_sum_u64<" << CTA << ">(acc_" << k << ", red);\n";
+          o << "    if (threadIdx.x == 0) db::atomic_add_ull(d_result[" << k << "], r_);\n";
         }
-        if (ag.fn == AggFn::Count) o << "    if (tid == 0) db::atomic_set_valid_bit(d_result_validity, " << k << ");\n";
+        if (ag.fn == AggFn::Count) o << "    if (threadIdx.x == 0) db::atomic_set_valid_bit(d_result_validity, " << k << ");\n";
         if (seen_idx[k] >= 0) {
-          o << "    const unsigned long long s_ = cx::block_sum_u64<BLOCK_THREADS>(seen_" << k << ", red);\n";
-          o << "    if (tid == 0 && s_ != 0ULL) db::atomic_set_valid_bit(d_result_validity, " << k << ");\n";
+          o << "    const unsigned long long s_ = cx::block_sum_u64<" << CTA << ">(seen_" << k << ", red);\n";
+          o << "    if (threadIdx.x == 0 && s_ != 0ULL) db::atomic_set_valid_bit(d_result_validity, " << k << ");\n";
         }
         if (ag.fn == AggFn::Avg) {
-          o << "    const unsigned long long c_ = cx::block_sum_u64<BLOCK_THREADS>(cnt_" << k << ", red);\n";
-          o << "    if (tid == 0) db::atomic_add_ull(d_result[" << p.hidden_count_slot(k) << "], c_);\n";
+          o << "    const unsigned long long c_ = cx::block_sum_u64<" << CTA << ">(cnt_" << k << ", red);\n";
+          o << "    if (threadIdx.x == 0) db::atomic_add_ull(d_result[" << p.hidden_count_slot(k) << "], c_);\n";
         }
         o << "  }\n";
       }
     } else if (smem_groups) {
       o << "  __syncthreads();\n";
-      o << "  for (long long g = tid; g < " << G << "LL; g += BLOCK_THREADS) {\n";
-      o << "    if (!((s_touch[g >> 5] >> (g & 31)) & 1u)) continue;\n";
+      o << "  for (long long g = threadIdx.x; g < " << G << "LL; g += " << CTA << ") {\n";
+      o << "    unsigned touched_ = 0u;\n";
+      o << "    for (int r = 0; r < " << REP << "; ++r) touched_ |= (s_touch_all[(long long)r * " << TW << "LL + (g >> 5)] >> (g & 31)) & 1u;\n";
+      o << "    if (!touched_) continue;\n";
       emit_key_store(o, "g", "    ");
-      int avg_i = 0;
       for (int k = 0; k < NA; ++k) {
         const Agg& ag = p.aggs[k];
         const int slot = (int)p.groups.size() + k;
         const std::string dst = "d_result[(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot) + "]";
-        o << "    { const unsigned long long v_ = s_acc[g * " << NACC << " + " << k << "];\n";
+        const std::string vb = "(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
+        o << "    { unsigned long long v_ = " << (ag.fn == AggFn::Min ? "~0ULL" : "0ULL") << "; unsigned seen_ = 0u; (void)seen_;\n";
+        o << "      for (int r = 0; r < " << REP << "; ++r) {\n";
+        o << "        const unsigned long long y_ = s_acc_all[((long long)r * " << G << "LL + g) * " << NACC << " + " << k << "];\n";
+        if (ag.fn == AggFn::Min) o << "        v_ = y_ < v_ ? y_ : v_;\n";
+        else if (ag.fn == AggFn::Max) o << "        v_ = y_ > v_ ? y_ : v_;\n";
+        else o << "        v_ += y_;\n";
+        if (seen_idx[k] >= 0 && NSEEN_T > 0)
+          o << "        seen_ |= (s_seen_all[(long long)r * " << (unsigned long long)NSEEN_T * TW << "LL + " << (unsigned long long)seen_idx[k] * TW
+            << "LL + (g >> 5)] >> (g & 31)) & 1u;\n";
+        o << "      }\n";
         if (ag.fn == AggFn::Min) o << "      if (v_ != ~0ULL) atomicMin(&" << dst << ", v_);\n";
         else if (ag.fn == AggFn::Max) o << "      if (v_ != 0ULL) atomicMax(&" << dst << ", v_);\n";
         else o << "      if (v_ != 0ULL) atomicAdd(&" << dst << ", v_);\n";
         if (!p.sparse) {
-          const std::string vb = "(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
           if (ag.fn == AggFn::Count) o << "      db::atomic_set_valid_bit(d_result_validity, " << vb << ");\n";
-          if (seen_idx[k] >= 0)
-            o << "      if ((s_seen[" << (unsigned long long)seen_idx[k] * TW << "ULL + (g >> 5)] >> (g & 31)) & 1u) db::atomic_set_valid_bit(d_result_validity, " << vb << ");\n";
+          if (seen_idx[k] >= 0) o << "      if (seen_) db::atomic_set_valid_bit(d_result_validity, " << vb << ");\n";
         }
         if (ag.fn == AggFn::Avg) {
-          o << "      const unsigned long long c_ = s_acc[g * " << NACC << " + " << (NA + avg_i) << "];\n";
+          o << "      unsigned long long c_ = 0ULL;\n";
+          o << "      for (int r = 0; r < " << REP << "; ++r) c_ += s_acc_all[((long long)r * " << G << "LL + g) * " << NACC << " + " << avg_idx[k] << "];\n";
           o << "      if (c_ != 0ULL) atomicAdd(&d_result[(unsigned long long)g * " << TS << "ULL + " << p.hidden_count_slot(k) << "], c_);\n";
-          ++avg_i;
         }
         o << "    }\n";
       }

@@ -10,7 +10,12 @@ streams; every kernel comes from the library.
 """
 from __future__ import annotations
 
+import itertools
+import json
+import os
+import re
 from dataclasses import dataclass
+from pathlib import Path
 
 import numpy as np
 
@@ -38,6 +43,29 @@ class QueryResult:
         return result_rows(plan, self.words, self.validity)
 
 
+def shape_key(plan: Plan) -> str:
+    """A plan's shape: its text with every integer literal abstracted.  Queries
+    of one shape share a launch configuration."""
+    return re.sub(r"\(int -?\d+\)", "(int ?)", plan.text())
+
+
+DEFAULT_CANDIDATES = [
+    dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=cs)
+    for bt, ipt, st, cs in itertools.product((256, 512, 1024), (2, 4, 8), (0, 2, 4), (1, 16))
+]
+
+
+def make_tuning(**kw) -> _lib.Tuning:
+    t = _lib.default_tuning()
+    for k, v in kw.items():
+        setattr(t, k, v)
+    return t
+
+
+def tuning_dict(t: _lib.Tuning) -> dict:
+    return {f: getattr(t, f) for f, _ in _lib.Tuning._fields_}
+
+
 class Database:
     """Resident star-schema tables on one GPU."""
 
@@ -53,6 +81,13 @@ class Database:
         self._modules: dict[tuple, _lib.Module] = {}
         self.ctx = _lib.ExecCtx()
         self._bound: set[str] = set()
+        self.tuned: dict[str, dict] = {}
+        self.tuning_cache = Path(os.environ.get("CRYSTAL_B200_TUNING", Path.home() / ".cache" / "crystal_b200" / "tuning.json"))
+        if self.tuning_cache.exists():
+            try:
+                self.tuned = json.loads(self.tuning_cache.read_text())
+            except (OSError, ValueError):
+                self.tuned = {}
 
     def reset(self) -> None:
         """Drops every resident table and starts a fresh execution context."""
@@ -134,6 +169,53 @@ class Database:
             self._modules[key] = m
         return m
 
+    def tuning_for(self, plan: Plan) -> _lib.Tuning | None:
+        """The autotuned launch shape of the plan's shape, if one was tuned."""
+        best = self.tuned.get(shape_key(plan))
+        return make_tuning(**best["tuning"]) if best else None
+
+    def autotune(self, plan: Plan, candidates: list[dict] | None = None, reps: int = 3, persist: bool = True) -> dict:
+        """Times every feasible candidate launch shape on the resident tables
+        (CUDA events around the fused scan) and keeps the fastest for the
+        plan's shape.  Infeasible shapes (shared memory, registers) are skipped."""
+        key = shape_key(plan)
+        table = []
+        res = val = None
+        for cand in candidates or DEFAULT_CANDIDATES:
+            t = make_tuning(**cand)
+            try:
+                m = self.compile(plan, t)
+            except _lib.CxError:
+                continue
+            if res is None or res.numel() < m.info.result_words or val.numel() < m.info.validity_words:
+                res, val = self.alloc_result(m)
+            for tn, n in self.rows.items():
+                self.ctx.set_rows(tn, n)
+            self.ctx.set_result(res.data_ptr(), res.numel(), val.data_ptr(), val.numel())
+            times = []
+            try:
+                for _ in range(reps + 1):
+                    self.ctx.execute(m, self.torch.cuda.current_stream().cuda_stream)
+                    self.ctx.sync()
+                    times.append(self.ctx.timing().scan_ms)
+            except _lib.CxError:
+                continue
+            table.append((min(times[1:]), cand))
+        if not table:
+            raise RuntimeError("autotune: no feasible launch shape")
+        table.sort(key=lambda x: x[0])
+        best = {"tuning": tuning_dict(make_tuning(**table[0][1])), "scan_ms": table[0][0],
+                "tried": len(table)}
+        self.tuned[key] = best
+        if persist:
+            try:
+                self.tuning_cache.parent.mkdir(parents=True, exist_ok=True)
+                self.tuning_cache.write_text(json.dumps(self.tuned, indent=1))
+            except OSError:
+                pass
+        best["table"] = table
+        return best
+
     def alloc_result(self, module: _lib.Module):
         torch = self.torch
         res = torch.empty(max(int(module.info.result_words), 1), dtype=torch.int64, device=self.device)
@@ -142,7 +224,7 @@ class Database:
 
     def execute(self, plan: Plan, tuning: _lib.Tuning | None = None, stream=None) -> QueryResult:
         torch = self.torch
-        m = self.compile(plan, tuning)
+        m = self.compile(plan, tuning if tuning is not None else self.tuning_for(plan))
         res, val = self.alloc_result(m)
         for t, n in self.rows.items():
             self.ctx.set_rows(t, n)

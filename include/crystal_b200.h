@@ -142,6 +142,21 @@ int cx_ctx_kernel_error(const cx_exec_ctx* c, uint32_t* code);
 int cx_compact_sparse(const uint64_t* dev_src, uint64_t groups, uint32_t tuple_size, uint64_t* dev_dst,
                       uint64_t* dev_count, void* stream);
 
+/* Sparse-result compaction that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that cannot let this library allocate
+ * device memory -- a serving loop that has reserved the whole HBM budget for
+ * admitted queries, or an engine whose memory guard must account every device
+ * byte before a query runs.  Same output as cx_compact_sparse.  Its scratch is
+ * a fixed file-scope device array of 16384 block counts (128 KiB, held by
+ * every GPU that loads the library until exit), so `groups` may be at most
+ * 16384 * 2048 = 33,554,432; larger inputs return CX_E_CAPACITY.  The first
+ * call on a device resolves the array's address on that device, so make that
+ * first call before any stream capture.  All calls share the one array: calls
+ * whose work overlaps on the GPU (other streams, other threads) race and
+ * corrupt each other's results. */
+int cx_compact_sparse_noalloc(const uint64_t* dev_src, uint64_t groups, uint32_t tuple_size, uint64_t* dev_dst,
+                              uint64_t* dev_count, void* stream);
+
 /* Seeded synthetic column generator (device; no reference counterpart: the
  * reference loads SSB dbgen output from disk, include/crystal/utils.h:242-253).
  * Row r of generator stream `gen_stream` gets lo + below(hash(seed, stream, r),

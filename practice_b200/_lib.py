@@ -22,7 +22,7 @@ EXPORTS = [
     "cx_module_release", "cx_module_result_info", "cx_ctx_create", "cx_ctx_destroy",
     "cx_ctx_set_buffer", "cx_ctx_set_null_bitmap", "cx_ctx_set_table_rows", "cx_ctx_set_result",
     "cx_ctx_set_scratch", "cx_module_scratch_bytes", "cx_ctx_set_sm_count", "cx_execute",
-    "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse",
+    "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse", "cx_compact_sparse_noalloc",
     "cx_gen_uniform", "cx_gen_datekey", "cx_gen_validity",
 ]
 
@@ -76,6 +76,7 @@ def _load() -> C.CDLL:
         "cx_ctx_timing": (C.c_int, [vp, C.POINTER(Timing)]),
         "cx_ctx_kernel_error": (C.c_int, [vp, C.POINTER(u32)]),
         "cx_compact_sparse": (C.c_int, [vp, u64, u32, vp, vp, vp]),
+        "cx_compact_sparse_noalloc": (C.c_int, [vp, u64, u32, vp, vp, vp]),
         "cx_gen_uniform": (C.c_int, [u64, u64, i64, i64, u64, u64, vp, vp]),
         "cx_gen_datekey": (C.c_int, [u64, u64, u32, u64, u64, vp, vp]),
         "cx_gen_validity": (C.c_int, [u64, u64, u64, u32, vp, vp]),

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 #include "../../include/crystal_b200.h"
@@ -172,6 +173,64 @@ extern "C" int cx_compact_sparse(const uint64_t* src, uint64_t groups, uint32_t 
                                                             (unsigned long long*)dst);
   e = cudaGetLastError();
   cudaFreeAsync(counts, s);
+  return e == cudaSuccess ? CX_OK : cuda_fail(e, "compaction launch");
+}
+
+// ------------------------------------------------ no-allocation compaction ---
+// Some callers cannot let this library allocate device memory: a serving loop
+// that has reserved the whole HBM budget for admitted queries (an allocation
+// here could fail or silently break its accounting), and engines whose memory
+// guard must see every device byte before a query runs.  For them the block
+// counts of the compaction live in this fixed file-scope array instead of a
+// cudaMallocAsync buffer.  It holds kNoAllocMaxBlocks counts (128 KiB), so one
+// call compacts at most kNoAllocMaxBlocks * kCompactPerBlock group tuples; every
+// GPU that loads the library keeps the array until the process exits.
+constexpr unsigned long long kNoAllocMaxBlocks = 16384;
+static __device__ __align__(256) unsigned long long g_noalloc_block_counts[kNoAllocMaxBlocks];
+
+namespace {
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_ptr[256] = {};  // device address of the array, per device ordinal
+}  // namespace
+
+extern "C" int cx_compact_sparse_noalloc(const uint64_t* src, uint64_t groups, uint32_t ts, uint64_t* dst,
+                                         uint64_t* dev_count, void* stream_v) {
+  if (!src || !dst || !dev_count || ts == 0) return CX_E_INVALID;
+  const unsigned long long nblocks = (groups + kCompactPerBlock - 1) / kCompactPerBlock;
+  if (nblocks > kNoAllocMaxBlocks) {
+    snprintf(g_err, sizeof g_err, "cx_compact_sparse_noalloc: %llu groups exceed the fixed maximum of %llu",
+             (unsigned long long)groups, kNoAllocMaxBlocks * kCompactPerBlock);
+    return CX_E_CAPACITY;
+  }
+  cudaStream_t s = (cudaStream_t)stream_v;
+  if (nblocks == 0) {
+    cudaError_t e = cudaMemsetAsync(dev_count, 0, 8, s);
+    return e == cudaSuccess ? CX_OK : cuda_fail(e, "cudaMemsetAsync");
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= 256) return CX_E_INVALID;
+  unsigned long long* counts = nullptr;
+  {
+    // First call on a device: resolve the array's device address with that
+    // device current.  The host-side symbol itself is not a device address.
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_block_counts);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
+      g_noalloc_ptr[dev] = (unsigned long long*)p;
+    }
+    counts = g_noalloc_ptr[dev];
+  }
+  // compact_count writes every one of the nblocks counts, so the array needs
+  // no clearing between calls.
+  compact_count<<<(unsigned)nblocks, kCompactBlock, 0, s>>>((const unsigned long long*)src, groups, ts, counts);
+  compact_scan<<<1, 1024, 0, s>>>(counts, nblocks, (unsigned long long*)dev_count);
+  compact_write<<<(unsigned)nblocks, kCompactBlock, 0, s>>>((const unsigned long long*)src, groups, ts, counts,
+                                                            (unsigned long long*)dst);
+  e = cudaGetLastError();
   return e == cudaSuccess ? CX_OK : cuda_fail(e, "compaction launch");
 }
 

@@ -51,6 +51,7 @@ typedef struct cx_tuning {
   int ctas_per_sm;       /* persistent CTAs per SM (default 2) */
   int group_placement;   /* 0 auto, 1 shared-memory group tables, 2 global atomics */
   int smem_group_budget; /* bytes a shared-memory group table may use */
+  int bitmap_budget;     /* bytes of shared memory for join membership bitmaps (0 = none) */
 } cx_tuning;
 
 /* Shape of a compiled query's result buffer. */

@@ -487,6 +487,24 @@ CX_DEVICE void BlockProbeAndPHT_2V(int tid, K (&items)[ITEMS_PER_THREAD], V (&re
   });
 }
 
+// Membership pre-filter from a slot-occupancy bitmap (bit h = slot h of the
+// PHT holds a key), typically copied into shared memory.  Clears the flag of
+// every item whose slot is empty or out of range; a key of 0 keeps its flag on
+// an empty slot because the PHT probe matches 0 against the empty sentinel
+// (join.h:7-41).  Exact: a following BlockProbeAndPHT_* confirms the key.  No
+// counterpart in the reference API.
+template <typename K, int BLOCK_THREADS, int ITEMS_PER_THREAD>
+CX_DEVICE void BlockProbeBitmapAnd(int tid, K (&items)[ITEMS_PER_THREAD], int (&flags)[ITEMS_PER_THREAD],
+                                   const unsigned int* bitmap, int ht_len, K key_mins, int num_items) {
+  cx_detail::for_items<BLOCK_THREADS, ITEMS_PER_THREAD>(tid, num_items, !cx_detail::tile_is_full<BLOCK_THREADS, ITEMS_PER_THREAD>(num_items), [&](int i) {
+    if (!flags[i]) return;
+    const int h = cx_detail::pht_slot<K>(items[i], ht_len, key_mins);
+    if (h < 0) { flags[i] = 0; return; }
+    const bool occupied = (bitmap[h >> 5] >> (h & 31)) & 1u;
+    flags[i] = (occupied || items[i] == K(0)) ? 1 : 0;
+  });
+}
+
 // Push-model thread-local probes (join.h:258-274).
 template <typename K>
 CX_DEVICE bool ProbePHT_1(K key, const K* ht, int ht_len, K key_mins) {

@@ -17,6 +17,7 @@ struct CxArgs {
   const unsigned long long* nul[CX_MAX_COLS];  // validity words (1 = valid), by slot
   int* ht[CX_MAX_HTS];                         // perfect hash tables (zeroed before builds)
   unsigned int* htv[CX_MAX_HTS];               // payload validity bits of PHT_2V tables
+  unsigned int* bm[CX_MAX_HTS];                // slot-occupancy bits of each hash table
   unsigned long long* result;                  // groups x storage tuple, u64
   unsigned long long* result_validity;         // result validity bits
   unsigned int* touched;                       // per-group "row seen" bits (global group path)

@@ -323,6 +323,25 @@ struct Emitter {
     o << "  }\n}\n\n";
   }
 
+  // Slot-occupancy bitmap of a built PHT: bit h is set when slot h holds a key.
+  void emit_occupancy(const Join& j) {
+    const int h = ht_slot.at(j.dim);
+    const long long words = (j.len + 31) / 32;
+    const std::string kname = "occupancy_" + lower(j.dim);
+    meta << "kernel " << kname << " fixed " << (words + 255) / 256 << " 256 0\n";
+    src << "extern \"C\" __global__ void __launch_bounds__(256) " << kname << "(const CxArgs a) {\n";
+    src << "  const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n";
+    src << "  if (w >= " << words << "LL) return;\n";
+    src << "  const int* ht = a.ht[" << h << "];\n";
+    src << "  unsigned bits = 0u;\n";
+    src << "  for (int b = 0; b < 32; ++b) {\n";
+    src << "    const long long slot = w * 32 + b;\n";
+    src << "    if (slot < " << j.len << "LL && ht[slot" << (j.payload.empty() ? "" : " * 2") << "] != 0) bits |= 1u << b;\n";
+    src << "  }\n";
+    src << "  a.bm[" << h << "][w] = bits;\n";
+    src << "}\n\n";
+  }
+
   // --------------------------------------------------------- group hash ---
   std::string group_term(size_t k) const {
     const GroupKey& g = p.groups[k];
@@ -415,6 +434,22 @@ struct Emitter {
     unsigned long long off = (unsigned long long)NW * warp_stage_ints * 4;
     const unsigned long long bars_off = off; off += (unsigned long long)NW * std::max(STAGES, 1) * 8;
     const unsigned long long red_off = off; off += (unsigned long long)NW * 8;
+    // Join membership bitmaps kept in shared memory (in join order, while they fit the budget).
+    struct SBm { std::string dim, fk; int h; long long len, keymin; unsigned long long words, off; };
+    std::vector<SBm> sbms;
+    {
+      unsigned long long used = 0;
+      for (const auto& s : p.steps) {
+        if (s.kind != Step::JoinStep) continue;
+        const unsigned long long words = (unsigned long long)((s.join.len + 31) / 32);
+        const unsigned long long bytes = ((words * 4) + 15) & ~15ULL;
+        if (used + bytes > (unsigned long long)std::max(0, tu.bitmap_budget)) continue;
+        off = (off + 15) & ~15ULL;
+        sbms.push_back({s.join.dim, s.join.fks[0], ht_slot.at(s.join.dim), s.join.len, s.join.keymin, words, off});
+        off += bytes;
+        used += bytes;
+      }
+    }
     bool smem_groups = false;
     int REP = 1;
     unsigned long long acc_off = 0, touch_off = 0, seen_off = 0;
@@ -506,6 +541,13 @@ struct Emitter {
       o << "  unsigned int* g_touch = a.touched;\n";
     }
 
+    // Join membership bitmaps: global -> shared once per CTA.
+    for (const auto& b : sbms) {
+      o << "  unsigned int* s_bm_" << lower(b.dim) << " = (unsigned int*)(cx_smem + " << b.off << ");\n";
+      o << "  for (long long w = threadIdx.x; w < " << b.words << "LL; w += " << CTA << ") s_bm_" << lower(b.dim)
+        << "[w] = a.bm[" << b.h << "][w];\n";
+    }
+
     // Per-warp TMA staging rings.
     if (STAGES > 0) {
       o << "  bool staged_ok = true;\n";
@@ -557,6 +599,13 @@ struct Emitter {
 
     // Pipeline body: the reference's primitive calls, one warp tile at a time.
     const std::string ind = "    ";
+    // Membership of every bitmap-filtered join first (shared memory), so the
+    // L2 probes below only run for rows that qualify on all of them.
+    for (const auto& b : sbms) {
+      ensure_loaded(o, b.fk, ind);
+      o << ind << "BlockProbeBitmapAnd<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << b.fk << ", flags, s_bm_"
+        << lower(b.dim) << ", " << b.len << ", " << b.keymin << ", num_tile_items);\n";
+    }
     for (const auto& s : p.steps) {
       if (s.kind == Step::Filter) {
         emit_filter(o, s.filter.get(), ind);
@@ -856,6 +905,7 @@ struct Emitter {
       meta << "ht " << h << " " << ht_name(s.join.dim) << " " << words << "\n";
       if (!s.join.payload.empty() && payload_valid.count(s.join.payload))
         meta << "htv " << h << " " << (s.join.len + 31) / 32 << "\n";
+      meta << "bm " << h << " " << (s.join.len + 31) / 32 << "\n";
       ++h;
     }
     if (h > CX_MAX_HTS_) throw PlanError("too many joins");
@@ -866,6 +916,8 @@ struct Emitter {
     if (p.has_min()) emit_init_min();
     for (const auto& s : p.steps)
       if (s.kind == Step::JoinStep) emit_build(s.join);
+    for (const auto& s : p.steps)
+      if (s.kind == Step::JoinStep) emit_occupancy(s.join);
     emit_scan();
     if (p.hidden_count_slots() > 0) emit_finalize();
 

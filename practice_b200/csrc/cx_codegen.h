@@ -16,6 +16,7 @@ struct Tuning {
   int ctas_per_sm = 2;         // persistent grid = SMs x this (occupancy-capped)
   int group_placement = 0;     // 0 auto, 1 shared-memory tables, 2 global atomics
   int smem_group_budget = 96 * 1024;  // bytes of shared memory a group table may use
+  int bitmap_budget = 96 * 1024;      // bytes of shared memory for join membership bitmaps
   int wait_limit_log2 = 24;    // mbarrier poll limit before a wait gives up
 };
 

@@ -112,6 +112,7 @@ struct LaunchPlan {
   struct Ht { int slot; std::string name; uint64_t words; };
   std::vector<Ht> hts;
   std::map<int, uint64_t> htv_words;
+  std::map<int, uint64_t> bm_words;
   uint64_t result_words = 0, groups = 1;
   int storage_ts = 1, visible_ts = 1, sparse = 0;
   uint64_t touched_words = 0;
@@ -159,6 +160,10 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       int s; uint64_t w;
       ls >> s >> w;
       lp.htv_words[s] = w;
+    } else if (k == "bm") {
+      int s; uint64_t w;
+      ls >> s >> w;
+      lp.bm_words[s] = w;
     } else if (k == "result") {
       ls >> lp.result_words >> lp.groups >> lp.storage_ts >> lp.visible_ts >> lp.sparse;
     } else if (k == "touched") {
@@ -191,7 +196,7 @@ uint64_t align256(uint64_t x) { return (x + 255) & ~255ULL; }
 // Scratch layout of one execute: hash tables, payload validity, group
 // touched bits, finalisation staging and the error word.
 struct ScratchLayout {
-  std::vector<uint64_t> ht_off, htv_off;
+  std::vector<uint64_t> ht_off, htv_off, bm_off;
   uint64_t touched_off = 0, fin_off = 0, err_off = 0, total = 0;
 };
 
@@ -206,6 +211,11 @@ ScratchLayout scratch_layout(const LaunchPlan& lp) {
     auto it = lp.htv_words.find(h.slot);
     s.htv_off.push_back(off);
     if (it != lp.htv_words.end()) off = align256(off + it->second * 4);
+  }
+  for (const auto& h : lp.hts) {
+    auto it = lp.bm_words.find(h.slot);
+    s.bm_off.push_back(off);
+    if (it != lp.bm_words.end()) off = align256(off + it->second * 4);
   }
   s.touched_off = off;
   off = align256(off + lp.touched_words * 4);
@@ -324,6 +334,7 @@ void cx_tuning_default(cx_tuning* t) {
   t->ctas_per_sm = d.ctas_per_sm;
   t->group_placement = d.group_placement;
   t->smem_group_budget = d.smem_group_budget;
+  t->bitmap_budget = d.bitmap_budget;
 }
 
 int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap, size_t* out_len) {
@@ -338,6 +349,7 @@ int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char*
       t.ctas_per_sm = tuning->ctas_per_sm;
       t.group_placement = tuning->group_placement;
       t.smem_group_budget = tuning->smem_group_budget;
+      t.bitmap_budget = tuning->bitmap_budget;
     }
     const std::string s = cx::generate_cuda(*p, t);
     if (out_len) *out_len = s.size();
@@ -583,6 +595,7 @@ int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream_v) {
   for (size_t i = 0; i < lp.hts.size(); ++i) {
     a.ht[lp.hts[i].slot] = (int*)(scratch + m->sl.ht_off[i]);
     if (lp.htv_words.count(lp.hts[i].slot)) a.htv[lp.hts[i].slot] = (unsigned int*)(scratch + m->sl.htv_off[i]);
+    if (lp.bm_words.count(lp.hts[i].slot)) a.bm[lp.hts[i].slot] = (unsigned int*)(scratch + m->sl.bm_off[i]);
   }
   a.touched = (unsigned int*)(scratch + m->sl.touched_off);
   a.finalize_tmp = (unsigned long long*)(scratch + m->sl.fin_off);
@@ -613,6 +626,7 @@ int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream_v) {
     const KernelSpec& k = lp.kernels[ki];
     unsigned grid = 0;
     if (k.kind == "groups") grid = (unsigned)((lp.groups + k.block - 1) / k.block);
+    else if (k.kind == "fixed") grid = (unsigned)k.table;
     else if (k.kind == "build") {
       const long long tiles = (rows[k.table] + k.tile - 1) / k.tile;
       grid = (unsigned)std::min<long long>(tiles, (long long)sms * 16);

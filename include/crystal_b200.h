@@ -52,6 +52,7 @@ typedef struct cx_tuning {
   int group_placement;   /* 0 auto, 1 shared-memory group tables, 2 global atomics */
   int smem_group_budget; /* bytes a shared-memory group table may use */
   int bitmap_budget;     /* bytes of shared memory for join membership bitmaps (0 = none) */
+  int group_merge;       /* 0 auto, 1 merge equal groups within a warp first, 2 per-lane atomics */
 } cx_tuning;
 
 /* Shape of a compiled query's result buffer. */

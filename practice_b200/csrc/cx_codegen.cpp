@@ -674,9 +674,13 @@ struct Emitter {
       o << ind << "    if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
       o << ind << "    if ((unsigned)hash >= " << G << "u) act = false;\n";
       o << ind << "  }\n";
-      // One match per item: lanes with the same group merge their updates and
-      // the lowest lane applies them.
-      o << ind << "  const unsigned peers = __match_any_sync(0xffffffffu, act ? (unsigned)hash : 0xffffffffu);\n";
+      // Warp-uniform skip when no lane of the warp aggregates this item; else
+      // lanes with the same group merge their updates (one match per item) and
+      // the lowest lane applies them -- or, with per-warp tables and direct
+      // merging, every active lane applies its own update.
+      const bool direct = tu.group_merge == 2 || (tu.group_merge == 0 && smem_groups && REP > 1);
+      o << ind << "  const unsigned amask = __ballot_sync(0xffffffffu, act);\n";
+      o << ind << "  if (amask != 0u) {\n";
       for (int k = 0; k < NA; ++k) {
         const Agg& ag = p.aggs[k];
         const std::string v = ag.arg->op == Op::Star ? "1" : valid_of(ag.arg.get());
@@ -686,6 +690,8 @@ struct Emitter {
           << (ag.fn == AggFn::Min ? "~0ULL" : "0ULL") << ";\n";
       }
       o << ind << "  if (act) {\n";
+      if (direct) o << ind << "    const unsigned peers = 1u << lane;\n";
+      else o << ind << "    const unsigned peers = __popc(amask) == 1 ? amask : __match_any_sync(amask, (unsigned)hash);\n";
       o << ind << "    const int leader = __ffs(peers) - 1;\n";
       o << ind << "    if (__popc(peers) > 1) {\n";
       for (int k = 0; k < NA; ++k) {
@@ -733,6 +739,7 @@ struct Emitter {
         o << ind << "    { const unsigned c_ = __popc(__ballot_sync(peers, act && (" << (p.aggs[k].arg->op == Op::Star ? std::string("1") : valid_of(p.aggs[k].arg.get())) << ")));\n";
         o << ind << "      if (lane == leader && c_) atomicAdd(&" << cacc << ", (unsigned long long)c_); }\n";
       }
+      o << ind << "  }\n";
       o << ind << "  }\n";
       o << ind << "}\n";
     }

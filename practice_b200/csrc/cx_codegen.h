@@ -17,6 +17,7 @@ struct Tuning {
   int group_placement = 0;     // 0 auto, 1 shared-memory tables, 2 global atomics
   int smem_group_budget = 96 * 1024;  // bytes of shared memory a group table may use
   int bitmap_budget = 96 * 1024;      // bytes of shared memory for join membership bitmaps
+  int group_merge = 0;         // 0 auto, 1 warp match-merge, 2 direct per-lane atomics
   int wait_limit_log2 = 24;    // mbarrier poll limit before a wait gives up
 };
 

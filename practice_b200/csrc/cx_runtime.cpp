@@ -335,6 +335,7 @@ void cx_tuning_default(cx_tuning* t) {
   t->group_placement = d.group_placement;
   t->smem_group_budget = d.smem_group_budget;
   t->bitmap_budget = d.bitmap_budget;
+  t->group_merge = d.group_merge;
 }
 
 int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap, size_t* out_len) {
@@ -350,6 +351,7 @@ int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char*
       t.group_placement = tuning->group_placement;
       t.smem_group_budget = tuning->smem_group_budget;
       t.bitmap_budget = tuning->bitmap_budget;
+      t.group_merge = tuning->group_merge;
     }
     const std::string s = cx::generate_cuda(*p, t);
     if (out_len) *out_len = s.size();

@@ -78,13 +78,15 @@ def test_shared_scan_templates(db, t):
         assert_parity(db, queries.template(t, rng, n), ht)
 
 
-@pytest.mark.parametrize("bt,ipt,stages,place", [(128, 4, 4, 0), (256, 8, 2, 0), (512, 2, 3, 2), (256, 4, 0, 1),
-                                                 (1024, 1, 2, 0), (256, 4, 6, 2)])
-def test_tuning_invariance(db, bt, ipt, stages, place):
+@pytest.mark.parametrize("bt,ipt,stages,place,merge,bitmaps", [
+    (128, 4, 4, 0, 0, 98304), (256, 8, 2, 0, 1, 0), (512, 2, 3, 2, 0, 98304), (256, 4, 0, 1, 2, 98304),
+    (1024, 1, 2, 0, 2, 0), (256, 4, 6, 2, 1, 98304), (1024, 2, 0, 1, 1, 98304)])
+def test_tuning_invariance(db, bt, ipt, stages, place, merge, bitmaps):
     n = 777_777
     ht = load(db, 15, n, queries.C2_COLS, nulls={"lo_revenue": 100, "c_city": 50})
     t = _lib.default_tuning()
     t.block_threads, t.items_per_thread, t.stages, t.group_placement = bt, ipt, stages, place
+    t.group_merge, t.bitmap_budget = merge, bitmaps
     assert_parity(db, queries.config3(n), ht, t)
     assert_parity(db, queries.config2(n), ht, t)
 

@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="plain", choices=["plain", "shared"])
+    ap.add_argument("--mode", default="shared", choices=["plain", "shared"])
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--rows", type=int, default=600_000_000)
     ap.add_argument("--seed", type=int, default=2024)
@@ -201,6 +201,32 @@ def config_block(args):
 
 # ------------------------------------------------------------------ GPU arm
 
+PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=98304)
+                    for bt, ipt, st in ((1024, 2, 0), (1024, 4, 0), (512, 2, 0), (512, 8, 2), (1024, 4, 2))]
+SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16)
+                     for bt, ipt, st in ((256, 2, 0), (512, 2, 0), (1024, 2, 0), (512, 4, 0), (256, 2, 2),
+                                         (512, 2, 2), (256, 4, 2))]
+
+
+def time_steps(torch, stream, steps, run_step, sampler=None):
+    """CUDA-event time of `steps` calls of run_step on `stream` (ms), plus the
+    per-step start events and per-query completion events it records."""
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    step_start = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    marks = []
+    start.record(stream)
+    for s in range(steps):
+        step_start[s].record(stream)
+        marks.append(run_step())
+    end.record(stream)
+    end.synchronize()
+    lat = []
+    for s in range(steps):
+        for ev in marks[s]:
+            lat.append(step_start[s].elapsed_time(ev))
+    return start.elapsed_time(end), lat
+
 
 def main():
     args = parse()
@@ -219,9 +245,16 @@ def main():
     db = Database(local)
     db.generate_ssb(args.rows, args.seed + rank, queries.C4_COLS)
     plans = queries.batch(args.batch, args.seed, args.rows)
-    mods = [db.compile(p) for p in plans]
-    results = [db.alloc_result(m) for m in mods]
     stream = torch.cuda.Stream(device)
+    peak, peak_kind = peaks()
+    union_cols = sorted({c for p in plans for c in p.columns_read()})
+
+    # ---- plain path: one fused kernel per query, one query after another
+    for p in plans:
+        if db.tuning_for(p) is None:
+            db.autotune(p, candidates=PLAIN_CANDIDATES, reps=1, persist=False)
+    mods = [db.compile(p, db.tuning_for(p)) for p in plans]
+    results = [db.alloc_result(m) for m in mods]
     ctxs = []
     for m, (res, val) in zip(mods, results):
         c = _lib.ExecCtx()
@@ -232,75 +265,115 @@ def main():
         c.set_result(res.data_ptr(), res.numel(), val.data_ptr(), val.numel())
         ctxs.append(c)
 
-    def run_step(record=None):
-        # one batch, one query after another on one stream
-        for i, (m, c) in enumerate(zip(mods, ctxs)):
+    def plain_step():
+        evs = []
+        for m, c in zip(mods, ctxs):
             c.execute(m, stream.cuda_stream)
-            if record is not None:
-                record[i].record(stream)
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(stream)
+            evs.append(ev)
+        return evs
 
-    # warmup (also loads modules on the device)
     for _ in range(args.warmup):
-        run_step()
+        plain_step()
     stream.synchronize()
     for c in ctxs:
         c.sync()
-
-    # timed region
-    sampler = ClockSampler(local)
     barrier(pg, device)
-    sampler.start()
-    time.sleep(0.3)
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    done = [[torch.cuda.Event(enable_timing=True) for _ in mods] for _ in range(args.steps)]
-    step_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    scan_ms = [0.0] * len(mods)
-    start.record(stream)
-    for s in range(args.steps):
-        step_start[s].record(stream)
-        run_step(done[s])
-    end.record(stream)
-    end.synchronize()
-    clocks = sampler.stop()
-    total_ms = start.elapsed_time(end)
-    for i, c in enumerate(ctxs):
+    plain_ms, plain_lat = time_steps(torch, stream, args.steps, plain_step)
+    for c in ctxs:
         c.sync()
-        scan_ms[i] = c.timing().scan_ms  # last step's scan kernel duration, per query
-    lat = []
-    for s in range(args.steps):
-        for i in range(len(mods)):
-            lat.append(step_start[s].elapsed_time(done[s][i]))
-    total_ms = max_over_ranks(pg, total_ms, device)
+    plain_scan_ms = [c.timing().scan_ms for c in ctxs]
+    plain_launches = sum(c.timing().gpu_launches for c in ctxs)
+    plain_ms = max_over_ranks(pg, plain_ms, device)
+    plain_bytes = sum(len(p.columns_read()) * 4 * args.rows for p in plans)
+    plain = {"queries_per_s": len(plans) * args.steps * world / (plain_ms / 1000.0),
+             "ms_per_step": plain_ms / args.steps,
+             "p50_ms": statistics.median(plain_lat), "p99_ms": float(np.percentile(plain_lat, 99)),
+             "scan_GBps": plain_bytes / (sum(plain_scan_ms) / 1000.0) / 1e9,
+             "scan_frac_of_peak": plain_bytes / (sum(plain_scan_ms) / 1000.0) / 1e9 / peak,
+             "scan_ms": {"mean": statistics.mean(plain_scan_ms), "min": min(plain_scan_ms), "max": max(plain_scan_ms)}}
+
+    # ---- shared scan: the whole batch in one persistent kernel
+    shared = None
+    sctx = db.ctx
+    if args.mode == "shared" and all(db.shareable(p) for p in plans):
+        if db.shared_tuning_for(plans) is None:
+            db.autotune_shared(plans, SHARED_CANDIDATES, reps=1)
+        tun = db.shared_tuning_for(plans)
+        prog = db.shared_program(plans, tun)
+        squeries, sparams, sbufs = db.shared_prepare(prog, plans)
+        for t, n in db.rows.items():
+            sctx.set_rows(t, n)
+
+        def shared_step():
+            sctx.shared_execute(prog.module, squeries, sparams, stream.cuda_stream)
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(stream)
+            return [ev] * len(plans)
+
+        for _ in range(args.warmup):
+            shared_step()
+        sctx.sync()
+        barrier(pg, device)
+        sampler = ClockSampler(local)
+        sampler.start()
+        time.sleep(0.3)
+        shared_ms, shared_lat = time_steps(torch, stream, args.steps, shared_step)
+        clocks = sampler.stop()
+        sctx.sync()
+        scan_ms = sctx.timing().scan_ms
+        shared_ms = max_over_ranks(pg, shared_ms, device)
+        shared_bytes = len(union_cols) * 4 * args.rows
+        shared = {"ms_per_step": shared_ms / args.steps, "scan_ms": scan_ms, "bytes": shared_bytes,
+                  "lat": shared_lat, "launches": sctx.timing().gpu_launches,
+                  "tuning": {k: getattr(tun, k) for k, _ in _lib.Tuning._fields_} if tun else None}
+    else:
+        sampler = ClockSampler(local)
+        sampler.start()
+        time.sleep(0.3)
+        _, _ = time_steps(torch, stream, 1, plain_step)
+        clocks = sampler.stop()
+        for c in ctxs:
+            c.sync()
     barrier(pg, device)
 
-    nq = len(mods) * args.steps * world
-    value = nq / (total_ms / 1000.0)
-    # roofline of the dominant kernel (the fused scan): algorithmic fact bytes / scan time
-    bytes_per_query = [len(p.columns_read()) * 4 * args.rows for p in plans]
-    achieved = sum(bytes_per_query) / (sum(scan_ms) / 1000.0) / 1e9
-    peak, peak_kind = peaks()
-    launches = sum(c.timing().gpu_launches for c in ctxs)
-
-    # end to end through the public API: execute + result read back per query
-    e2e = None
-    if rank == 0 or True:
-        pinned = [torch.empty(r.numel(), dtype=torch.int64, pin_memory=True) for r, _ in results]
-        pinned_v = [torch.empty(v.numel(), dtype=torch.int64, pin_memory=True) for _, v in results]
+    # ---- end to end through the public API: per-step descriptor upload and
+    # every query's result read back to pinned host memory
+    e2e_steps = max(2, args.steps)
+    if shared is not None:
+        pinned = [torch.empty(r.numel(), dtype=torch.int64, pin_memory=True) for r, _, _ in sbufs]
+        pinned_v = [torch.empty(v.numel(), dtype=torch.int64, pin_memory=True) for _, v, _ in sbufs]
+        h2d = len(squeries) * 32 + len(sparams) * 4
         d2h = sum(p.numel() * 8 + q.numel() * 8 for p, q in zip(pinned, pinned_v))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for _ in range(max(1, args.steps // 2)):
+        for _ in range(e2e_steps):
+            prog2 = db.shared_program(plans, db.shared_tuning_for(plans))
+            q2, p2, _ = squeries, sparams, None
+            sctx.shared_execute(prog2.module, q2, p2, stream.cuda_stream)
+            for i, (r, v, _) in enumerate(sbufs):
+                pinned[i].copy_(r, non_blocking=True)
+                pinned_v[i].copy_(v, non_blocking=True)
+            stream.synchronize()
+        e2e_s = time.perf_counter() - t0
+    else:
+        pinned = [torch.empty(r.numel(), dtype=torch.int64, pin_memory=True) for r, _ in results]
+        pinned_v = [torch.empty(v.numel(), dtype=torch.int64, pin_memory=True) for _, v in results]
+        h2d = 0
+        d2h = sum(p.numel() * 8 + q.numel() * 8 for p, q in zip(pinned, pinned_v))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
             for i, (m, c) in enumerate(zip(mods, ctxs)):
-                mm = db.compile(plans[i])  # cache lookup, as QueryEngine does per query
-                c.execute(mm, stream.cuda_stream)
+                c.execute(db.compile(plans[i], db.tuning_for(plans[i])), stream.cuda_stream)
                 pinned[i].copy_(results[i][0], non_blocking=True)
                 pinned_v[i].copy_(results[i][1], non_blocking=True)
             stream.synchronize()
         e2e_s = time.perf_counter() - t0
-        e2e = {"value": len(mods) * max(1, args.steps // 2) * world / e2e_s, "unit": "queries/s",
-               "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(d2h),
-               "note": "fact table resident in HBM; results read back to pinned host memory every query"}
+    e2e = {"value": len(plans) * e2e_steps * world / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h),
+           "note": "fact table resident in HBM; query descriptors uploaded and every result read back each step"}
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -310,20 +383,37 @@ def main():
             cb = {"value": None, "unit": "queries/s", "error": str(e)[:200]}
 
     if rank == 0:
+        if shared is not None:
+            value = len(plans) * args.steps * world / (shared["ms_per_step"] * args.steps / 1000.0)
+            ms_step = shared["ms_per_step"]
+            lat = shared["lat"]
+            achieved = shared["bytes"] / (shared["scan_ms"] / 1000.0) / 1e9
+            kernel = "SharedScan_LINEORDER (one pass over the union of the batch's fact columns)"
+            launches = shared["launches"]
+            alg = f"union of fact columns read by the batch ({len(union_cols)}) x 4 B x rows, per launch"
+        else:
+            value = plain["queries_per_s"]
+            ms_step = plain["ms_per_step"]
+            lat = plain_lat
+            achieved = plain["scan_GBps"]
+            kernel = "Scan_LINEORDER (plain fused scan/probe/aggregate)"
+            launches = plain_launches
+            alg = "distinct fact columns read x 4 B x rows, per query"
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32/u64", "data": "synthetic",
             "config": config_block(args),
             "latency_ms": {"p50": statistics.median(lat), "p99": float(np.percentile(lat, 99)),
                            "definition": "query completion since its batch started"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                         "kernel": "Scan_LINEORDER (plain fused scan/probe/aggregate)",
-                         "algorithmic_bytes": "distinct fact columns read x 4 B x rows, per query"},
+                         "kernel": kernel, "algorithmic_bytes": alg},
             "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
             "cpu_baseline": cb,
-            "plain_scan_ms": {"mean": statistics.mean(scan_ms), "min": min(scan_ms), "max": max(scan_ms)},
+            "plain": plain,
+            "shared_vs_plain": (value / plain["queries_per_s"]) if shared is not None else 1.0,
+            "shared_tuning": shared["tuning"] if shared is not None else None,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

@@ -137,6 +137,37 @@ int cx_ctx_timing(const cx_exec_ctx* c, cx_timing* t);
  * wait timeout; 2 = GROUP BY key outside its catalog domain). */
 int cx_ctx_kernel_error(const cx_exec_ctx* c, uint32_t* code);
 
+/* ---------------------------------------------------------- shared scans ---
+ * A shared scan runs a batch of queries in one pass over the fact table: every
+ * fact tile is staged once and every query of the batch is applied to it.
+ * Queries are grouped by plan shape (the plan with its integer literals
+ * abstracted); one compiled program serves any batch of its shapes, with each
+ * query's literals passed as parameters.  No counterpart in the reference,
+ * which runs one generated program per query (src/core/execution.cpp:652-725);
+ * each query's result buffer is bit-identical to running it alone. */
+typedef struct cx_shared_query {
+  int shape;              /* index of the query's shape in the program */
+  int param_off;          /* offset of its literals in the batch parameter array */
+  uint64_t* result;       /* groups x storage_ts u64, device, caller-owned */
+  uint64_t result_words;
+  uint64_t* validity;     /* validity words, device, caller-owned */
+  uint64_t validity_words;
+} cx_shared_query;
+
+/* Literals of a plan in the order that numbers its shape's parameters. */
+int cx_plan_literals(const char* plan, size_t plan_len, int64_t* out, int cap, int* n);
+/* Shared-scan program for `nshapes` plan shapes (one representative plan per
+ * shape; its literals are ignored).  Same output contract as cx_codegen; fails
+ * with CX_E_INVALID for shapes that cannot share a scan (nullable columns,
+ * aggregates other than COUNT/SUM, conflicting joins). */
+int cx_shared_codegen(const char* const* plans, const size_t* plan_lens, int nshapes, const cx_tuning* tuning,
+                      char* out, size_t out_cap, size_t* out_len);
+/* Enqueues one batch (<= 256 queries, <= 4096 parameters) of a compiled shared
+ * program on `stream`; cx_ctx_sync waits for it.  Foreign keys of shared joins
+ * must be non-zero (the engine checks column minima before batching). */
+int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queries, int nq, const int32_t* params,
+                      int nparams, void* stream);
+
 /* Sparse-result compaction: copies every group tuple with a non-zero slot to
  * `dst` in group order and writes the row count to *dev_count (device u64).
  * Same rows as the reference's CompactSparseAggregateResult

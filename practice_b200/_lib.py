@@ -23,7 +23,8 @@ EXPORTS = [
     "cx_ctx_set_buffer", "cx_ctx_set_null_bitmap", "cx_ctx_set_table_rows", "cx_ctx_set_result",
     "cx_ctx_set_scratch", "cx_module_scratch_bytes", "cx_ctx_set_sm_count", "cx_execute",
     "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse", "cx_compact_sparse_noalloc",
-    "cx_gen_uniform", "cx_gen_datekey", "cx_gen_validity",
+    "cx_gen_uniform", "cx_gen_datekey", "cx_gen_validity", "cx_plan_literals", "cx_shared_codegen",
+    "cx_shared_execute",
 ]
 
 
@@ -43,6 +44,11 @@ class ResultInfo(C.Structure):
     _fields_ = [("groups", C.c_uint64), ("storage_ts", C.c_uint32), ("visible_ts", C.c_uint32),
                 ("result_words", C.c_uint64), ("validity_words", C.c_uint64), ("final_words", C.c_uint64),
                 ("sparse", C.c_int), ("finalized", C.c_int)]
+
+
+class SharedQuery(C.Structure):
+    _fields_ = [("shape", C.c_int), ("param_off", C.c_int), ("result", C.c_void_p), ("result_words", C.c_uint64),
+                ("validity", C.c_void_p), ("validity_words", C.c_uint64)]
 
 
 class Timing(C.Structure):
@@ -81,6 +87,10 @@ def _load() -> C.CDLL:
         "cx_gen_uniform": (C.c_int, [u64, u64, i64, i64, u64, u64, vp, vp]),
         "cx_gen_datekey": (C.c_int, [u64, u64, u32, u64, u64, vp, vp]),
         "cx_gen_validity": (C.c_int, [u64, u64, u64, u32, vp, vp]),
+        "cx_plan_literals": (C.c_int, [C.c_char_p, sz, C.POINTER(i64), C.c_int, C.POINTER(C.c_int)]),
+        "cx_shared_codegen": (C.c_int, [C.POINTER(C.c_char_p), C.POINTER(sz), C.c_int, C.POINTER(Tuning), C.c_char_p,
+                                        sz, C.POINTER(sz)]),
+        "cx_shared_execute": (C.c_int, [vp, vp, C.POINTER(SharedQuery), C.c_int, C.POINTER(C.c_int32), C.c_int, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -111,6 +121,27 @@ def codegen(plan_text: str, tuning: Tuning | None = None) -> str:
     check(lib.cx_codegen(raw, len(raw), tp, None, 0, C.byref(n)), "cx_codegen")
     buf = C.create_string_buffer(n.value + 1)
     check(lib.cx_codegen(raw, len(raw), tp, buf, n.value + 1, C.byref(n)), "cx_codegen")
+    return buf.value.decode()
+
+
+def plan_literals(plan_text: str) -> list[int]:
+    raw = plan_text.encode()
+    n = C.c_int(0)
+    check(lib.cx_plan_literals(raw, len(raw), None, 0, C.byref(n)), "cx_plan_literals")
+    out = (C.c_int64 * max(n.value, 1))()
+    check(lib.cx_plan_literals(raw, len(raw), out, n.value, C.byref(n)), "cx_plan_literals")
+    return list(out[: n.value])
+
+
+def shared_codegen(plan_texts: list[str], tuning: Tuning | None = None) -> str:
+    raws = [t.encode() for t in plan_texts]
+    arr = (C.c_char_p * len(raws))(*raws)
+    lens = (C.c_size_t * len(raws))(*[len(r) for r in raws])
+    n = C.c_size_t(0)
+    tp = C.byref(tuning) if tuning is not None else None
+    check(lib.cx_shared_codegen(arr, lens, len(raws), tp, None, 0, C.byref(n)), "cx_shared_codegen")
+    buf = C.create_string_buffer(n.value + 1)
+    check(lib.cx_shared_codegen(arr, lens, len(raws), tp, buf, n.value + 1, C.byref(n)), "cx_shared_codegen")
     return buf.value.decode()
 
 
@@ -171,6 +202,13 @@ class ExecCtx:
 
     def execute(self, module: Module, stream: int = 0) -> None:
         check(lib.cx_execute(module.handle, self.handle, stream or None), "cx_execute")
+
+    def shared_execute(self, module: Module, queries, params, stream: int = 0) -> None:
+        nq = len(queries)
+        qa = (SharedQuery * max(nq, 1))(*queries)
+        pa = (C.c_int32 * max(len(params), 1))(*params)
+        check(lib.cx_shared_execute(module.handle, self.handle, qa, nq, pa, len(params), stream or None),
+              "cx_shared_execute")
 
     def sync(self) -> None:
         check(lib.cx_ctx_sync(self.handle), "cx_ctx_sync")

@@ -637,6 +637,7 @@ enum : unsigned int {
   ERR_WAIT_TIMEOUT = 1,      // an mbarrier wait exceeded its iteration limit
   ERR_GROUP_DOMAIN = 2,      // a GROUP BY key fell outside its catalog domain
   ERR_SCRATCH = 3,           // scratch too small for the requested table
+  ERR_DIM_COLLISION = 4,     // two dimension keys share a slot of a shared-scan index
 };
 
 CX_DEVICE void raise(unsigned int* err, unsigned int code) {

@@ -11,6 +11,17 @@
 #define CX_MAX_COLS 40
 #define CX_MAX_HTS 8
 #define CX_MAX_TABLES 8
+#define CX_MAX_SHAPES 16
+
+// One query of a shared-scan batch: its own result buffers, its plan shape and
+// the offset of its literal parameters.
+struct CxSQ {
+  unsigned long long* result;
+  unsigned long long* validity;
+  unsigned int* touched;    // per-group "row seen" bits (grouped shapes)
+  int shape;
+  int param_off;
+};
 
 struct CxArgs {
   const int* col[CX_MAX_COLS];                 // device column bases, by slot
@@ -24,4 +35,11 @@ struct CxArgs {
   unsigned long long* finalize_tmp;            // visible tuple staging for AVG finalisation
   unsigned int* err;                           // first error code raised by any kernel
   long long rows[CX_MAX_TABLES];               // row count per plan table slot
+  // Shared-scan batches (unused by single-query kernels).
+  const struct CxSQ* sq;                       // queries, grouped by shape
+  const int* sparams;                          // literal parameters of all queries
+  int sq_first[CX_MAX_SHAPES];                 // first query of each shape
+  int sq_num[CX_MAX_SHAPES];                   // number of queries of each shape
+  int sq_total;
+  int nparams;
 };

@@ -104,7 +104,18 @@ struct Emitter {
   std::set<std::string> loaded;         // register arrays holding a column
   std::set<std::string> valid_regs;     // columns with a <col>_valid register
 
+  // Shared-scan mode: integer literals become per-query parameters P[k].
+  const std::map<const Expr*, int>* lit_index = nullptr;
+
   Emitter(const Plan& plan, const Tuning& t) : p(plan), tu(t) {}
+
+  std::string int_lit(const Expr* e) const {
+    if (lit_index) {
+      auto it = lit_index->find(e);
+      if (it != lit_index->end()) return "P[" + std::to_string(it->second) + "]";
+    }
+    return std::to_string(e->ival);
+  }
 
   bool nullable(const std::string& c) const { return p.nullable.count(c) != 0; }
 
@@ -153,7 +164,7 @@ struct Emitter {
     if (!e) return "0";
     switch (e->op) {
       case Op::Col: return reg(e->name);
-      case Op::Int: return std::to_string(e->ival);
+      case Op::Int: return int_lit(e);
       case Op::Null: return "0";
       case Op::Star: return "1";
       case Op::IsNull:
@@ -181,7 +192,7 @@ struct Emitter {
     if (!e) return "0";
     switch (e->op) {
       case Op::Col: return cast ? "(unsigned long long)" + reg(e->name) : reg(e->name);
-      case Op::Int: return std::to_string(e->ival);
+      case Op::Int: return int_lit(e);
       case Op::Star: return cast ? "(unsigned long long)1" : "1";
       case Op::Null: return "0";
       case Op::Add: case Op::Sub: case Op::Mul: {
@@ -244,7 +255,7 @@ struct Emitter {
     if (is_compare(e->op) && e->kids[0]->op == Op::Col && e->kids[1]->op == Op::Int &&
         !valid_regs.count(e->kids[0]->name) && e->kids[1]->ival >= -2147483647LL && e->kids[1]->ival <= 2147483647LL) {
       o << ind << "BlockPredA" << pred_suffix(e->op) << "<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, "
-        << e->kids[0]->name << ", flags, " << e->kids[1]->ival << ", num_tile_items);\n";
+        << e->kids[0]->name << ", flags, " << int_lit(e->kids[1].get()) << ", num_tile_items);\n";
       return;
     }
     const std::string cond = and_terms({valid_of(e), value_of(e)});
@@ -947,11 +958,487 @@ struct Emitter {
   static constexpr int CX_MAX_HTS_ = 8;
 };
 
-}  // namespace
-
-std::string generate_cuda(const Plan& plan, const Tuning& tuning) {
+std::string generate_cuda_impl(const Plan& plan, const Tuning& tuning) {
   Emitter e(plan, tuning);
   return e.run();
+}
+
+// ============================================================ shared scan ===
+// One persistent kernel for a batch of queries of several plan shapes: each
+// warp stages a tile of the union of the fact columns once, gathers every
+// joined dimension's slot entry once, then runs every query of the batch on
+// those registers.  A dimension index entry is {key, attr1, attr2, attr3}
+// stored at the PHT slot HASH(key, len, key_min) of its row (index_<dim>
+// kernels); a query's join keeps a row when the slot's key equals the FK and
+// the row passes the query's dimension filter -- the condition under which the
+// reference's filtered PHT would hold that key (join.h:124-253, 7-120), for
+// dimensions whose keys occupy distinct slots (checked while indexing) and
+// non-zero foreign keys (checked by the engine before it forms a batch).
+
+void lits_of(const Expr* e, std::vector<const Expr*>& out) {
+  if (!e) return;
+  if (e->op == Op::Int) out.push_back(e);
+  for (const auto& k : e->kids) lits_of(k.get(), out);
+}
+
+struct SharedGen {
+  const std::vector<const Plan*>& shapes;
+  const Tuning& tu;
+  std::ostringstream meta, src;
+  std::string fact;
+  std::vector<std::string> tables;
+  std::vector<std::string> fact_cols;
+  struct Dim {
+    std::string name, pk, fk;
+    long long len = 0, keymin = 0;
+    std::vector<std::string> attrs;
+    int slot = 0, table = 0;
+  };
+  std::vector<Dim> dims;
+  std::map<std::string, int> col_slot;
+  std::vector<std::pair<std::string, int>> col_order;
+  std::vector<std::map<const Expr*, int>> lit_maps;
+  int max_lits = 0, max_scalar_aggs = 0;
+
+  SharedGen(const std::vector<const Plan*>& s, const Tuning& t) : shapes(s), tu(t) {}
+
+  int table_slot(const std::string& t) {
+    for (size_t i = 0; i < tables.size(); ++i)
+      if (tables[i] == t) return (int)i;
+    tables.push_back(t);
+    return (int)tables.size() - 1;
+  }
+  int slot_of(const std::string& c, int table) {
+    auto it = col_slot.find(c);
+    if (it != col_slot.end()) return it->second;
+    const int s = (int)col_order.size();
+    if (s >= CX_MAX_COLS_) throw PlanError("too many columns in a shared batch");
+    col_slot[c] = s;
+    col_order.push_back({c, table});
+    return s;
+  }
+  Dim* find_dim(const std::string& n) {
+    for (auto& d : dims)
+      if (d.name == n) return &d;
+    return nullptr;
+  }
+  void add_fact(const std::string& c) {
+    if (std::find(fact_cols.begin(), fact_cols.end(), c) == fact_cols.end()) fact_cols.push_back(c);
+  }
+  void add_fact_expr(const Plan& p, const Expr* e) {
+    std::vector<std::string> cs;
+    std::function<void(const Expr*)> walk = [&](const Expr* x) {
+      if (!x) return;
+      if (x->op == Op::Col) cs.push_back(x->name);
+      for (const auto& k : x->kids) walk(k.get());
+    };
+    walk(e);
+    for (const auto& c : cs)
+      if (p.table_of_col.at(c) == 0) add_fact(c);
+  }
+
+  void collect() {
+    if (shapes.empty() || shapes.size() > CX_MAX_SHAPES_) throw PlanError("shared batch needs 1..16 shapes");
+    fact = shapes[0]->tables[0].name;
+    table_slot(fact);
+    for (const Plan* pp : shapes) {
+      const Plan& p = *pp;
+      if (p.tables[0].name != fact) throw PlanError("shared batch mixes fact tables");
+      std::function<void(const Expr*)> no_null = [&](const Expr* x) {
+        if (!x) return;
+        if (x->op == Op::Col && p.nullable.count(x->name)) throw PlanError("nullable column " + x->name + " is not shareable");
+        for (const auto& k : x->kids) no_null(k.get());
+      };
+      for (const auto& a : p.aggs) {
+        if (a.fn != AggFn::Count && a.fn != AggFn::Sum) throw PlanError("shared scans support COUNT and SUM");
+        no_null(a.arg.get());
+        add_fact_expr(p, a.arg.get());
+      }
+      for (const auto& g : p.groups) {
+        if (g.nullable) throw PlanError("nullable group key is not shareable");
+        no_null(g.expr.get());
+        add_fact_expr(p, g.expr.get());
+      }
+      std::map<const Expr*, int> lm;
+      std::vector<const Expr*> lits;
+      collect_literals(p, lits);
+      for (size_t k = 0; k < lits.size(); ++k) {
+        if (lits[k]->ival < -2147483647LL || lits[k]->ival > 2147483647LL) throw PlanError("literal outside int32");
+        lm[lits[k]] = (int)k;
+      }
+      max_lits = std::max(max_lits, (int)lits.size());
+      if (p.groups.empty()) max_scalar_aggs = std::max(max_scalar_aggs, (int)p.aggs.size());
+      lit_maps.push_back(lm);
+      for (const auto& s : p.steps) {
+        if (s.kind == Step::Filter) {
+          no_null(s.filter.get());
+          add_fact_expr(p, s.filter.get());
+          continue;
+        }
+        const Join& j = s.join;
+        Dim* d = find_dim(j.dim);
+        if (!d) {
+          dims.push_back(Dim());
+          d = &dims.back();
+          d->name = j.dim;
+          d->pk = j.pk;
+          d->fk = j.fks[0];
+          d->len = j.len;
+          d->keymin = j.keymin;
+          d->slot = (int)dims.size() - 1;
+          d->table = table_slot(j.dim);
+        } else if (d->pk != j.pk || d->fk != j.fks[0] || d->len != j.len || d->keymin != j.keymin) {
+          throw PlanError("shapes join " + j.dim + " differently");
+        }
+        if (p.nullable.count(j.fks[0]) || p.nullable.count(j.pk)) throw PlanError("nullable join key is not shareable");
+        add_fact(j.fks[0]);
+        std::vector<std::string> need;
+        std::function<void(const Expr*)> walk = [&](const Expr* x) {
+          if (!x) return;
+          if (x->op == Op::Col) need.push_back(x->name);
+          for (const auto& k : x->kids) walk(k.get());
+        };
+        walk(j.filter.get());
+        if (!j.payload.empty()) need.push_back(j.payload);
+        for (const auto& c : need) {
+          if (p.nullable.count(c)) throw PlanError("nullable dimension column " + c + " is not shareable");
+          if (c != d->pk && std::find(d->attrs.begin(), d->attrs.end(), c) == d->attrs.end()) d->attrs.push_back(c);
+        }
+        if (d->attrs.size() > 3) throw PlanError("more than 3 attributes of " + j.dim + " in one shared batch");
+      }
+    }
+    if ((int)dims.size() > CX_MAX_HTS_) throw PlanError("too many dimensions in a shared batch");
+  }
+
+  void emit_index(const Dim& d) {
+    const std::string k = "index_" + lower(d.name);
+    meta << "kernel " << k << " build " << d.table << " 256 1024\n";
+    src << "extern \"C\" __global__ void __launch_bounds__(256) " << k << "(const CxArgs a) {\n";
+    src << "  const long long n = a.rows[" << d.table << "];\n";
+    src << "  int4* dix = (int4*)a.ht[" << d.slot << "];\n";
+    src << "  const int* key = a.col[" << slot_of(d.pk, d.table) << "];\n";
+    for (size_t i = 0; i < d.attrs.size(); ++i)
+      src << "  const int* at" << i << " = a.col[" << slot_of(d.attrs[i], d.table) << "];\n";
+    src << "  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {\n";
+    src << "    const int k = key[r];\n";
+    src << "    if (k == 0) continue;\n";
+    src << "    const int h = (int)HASH(k, " << d.len << ", " << d.keymin << ");\n";
+    src << "    if ((unsigned)h >= " << d.len << "u) continue;\n";
+    src << "    if (atomicCAS(&dix[h].x, 0, k) != 0) { cx::raise(a.err, cx::ERR_DIM_COLLISION); continue; }\n";
+    const char* comp[] = {"y", "z", "w"};
+    for (size_t i = 0; i < d.attrs.size(); ++i) src << "    dix[h]." << comp[i] << " = at" << i << "[r];\n";
+    src << "  }\n}\n\n";
+  }
+
+  std::string run() {
+    collect();
+    meta << "v 1\nshared\n";
+    for (const Dim& d : dims) {
+      meta << "ht " << d.slot << " dix_" << lower(d.name) << " " << d.len * 4 << "\n";
+    }
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      const Plan& p = *shapes[s];
+      Emitter e(p, tu);
+      meta << "sshape " << s << " " << e.total_groups() << " " << p.storage_ts() << " " << (p.groups.empty() ? 0 : 1)
+           << " " << (p.sparse ? 1 : 0) << " " << lit_maps[s].size() << "\n";
+    }
+    for (const Dim& d : dims) emit_index(d);
+    emit_scan();
+    emit_keys();
+    std::ostringstream cols;
+    for (size_t i = 0; i < tables.size(); ++i) meta << "table " << i << " " << tables[i] << "\n";
+    for (size_t i = 0; i < col_order.size(); ++i)
+      meta << "col " << i << " d_" << col_order[i].first << " " << col_order[i].second << "\n";
+    std::ostringstream out;
+    out << "/*@cx-launch\n" << meta.str() << "@*/\n";
+    out << "// Generated by crystal-b200 for sm_100a (shared scan).\n";
+    out << "#include \"cx_args.h\"\n#include \"crystal_sm100.cuh\"\n\n";
+    out << src.str();
+    return out.str();
+  }
+
+  void emit_scan() {
+    const int CTA = tu.block_threads, IPT = tu.items_per_thread;
+    if (CTA % 32 || CTA < 32 || CTA > 1024 || IPT < 1 || IPT > 16) throw PlanError("bad block shape");
+    const int NW = CTA / 32, WT = 32 * IPT;
+    const int NSC = (int)fact_cols.size();
+    const int STAGES = NSC == 0 ? 0 : std::max(0, tu.stages);
+    const int MAXQ = 256, MAXP = 4096;
+    const int NACC = std::max(1, max_scalar_aggs) * 2;  // (sum, count) per scalar aggregate
+    const unsigned long long warp_stage_ints = (unsigned long long)STAGES * NSC * WT;
+    unsigned long long off = (unsigned long long)NW * warp_stage_ints * 4;
+    const unsigned long long bars_off = off; off += (unsigned long long)NW * std::max(STAGES, 1) * 8;
+    const unsigned long long par_off = off; off += (unsigned long long)MAXP * 4;
+    off = (off + 15) & ~15ULL;
+    const unsigned long long acc_off = off; off += (unsigned long long)MAXQ * NACC * 8;
+    const unsigned long long smem_total = (off + 127) & ~127ULL;
+    if (smem_total > 227 * 1024) throw PlanError("shared scan shared memory exceeds 227 KB");
+    const unsigned wait_limit = 1u << std::min(30, std::max(10, tu.wait_limit_log2));
+    const std::string kname = "SharedScan_" + fact;
+    meta << "kernel " << kname << " scan 0 " << CTA << " " << WT << " " << smem_total << " " << tu.ctas_per_sm << "\n";
+
+    std::ostringstream& o = src;
+    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ") " << kname << "(const CxArgs a) {\n";
+    o << "  constexpr int BLOCK_THREADS = 32, ITEMS_PER_THREAD = " << IPT << ", TILE_SIZE = " << WT << ";\n";
+    o << "  constexpr int NWARP = " << NW << ", NSTAGE = " << STAGES << ", NSC = " << NSC << ";\n";
+    o << "  extern __shared__ __align__(1024) unsigned char cx_smem[];\n";
+    o << "  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
+    o << "  const int tid = lane;\n";
+    o << "  int* stage_buf = (int*)cx_smem + (long long)warp * " << warp_stage_ints << "LL; (void)stage_buf;\n";
+    o << "  unsigned long long* bars = (unsigned long long*)(cx_smem + " << bars_off << ") + warp * " << std::max(STAGES, 1) << "; (void)bars;\n";
+    o << "  int* s_params = (int*)(cx_smem + " << par_off << ");\n";
+    o << "  unsigned long long* s_qacc = (unsigned long long*)(cx_smem + " << acc_off << ");\n";
+    o << "  const CxSQ* sq = a.sq;\n";
+    o << "  const long long n_rows = a.rows[0];\n";
+    o << "  const long long num_tiles = (n_rows + TILE_SIZE - 1) / TILE_SIZE;\n";
+    o << "  const long long full_tiles = n_rows / TILE_SIZE;\n";
+    o << "  const long long gwarp = (long long)blockIdx.x * NWARP + warp;\n";
+    o << "  const long long nwarps = (long long)gridDim.x * NWARP;\n";
+    o << "  for (int w = threadIdx.x; w < a.nparams && w < " << MAXP << "; w += " << CTA << ") s_params[w] = a.sparams[w];\n";
+    o << "  for (int w = threadIdx.x; w < " << MAXQ * NACC << "; w += " << CTA << ") s_qacc[w] = 0ULL;\n";
+    for (const auto& c : fact_cols) o << "  const int* __restrict__ d_" << c << " = a.col[" << slot_of(c, 0) << "];\n";
+    for (const Dim& d : dims) o << "  const int4* __restrict__ dix_" << lower(d.name) << " = (const int4*)a.ht[" << d.slot << "];\n";
+    if (STAGES > 0) {
+      o << "  bool staged_ok = true;\n";
+      for (const auto& c : fact_cols) o << "  staged_ok = staged_ok && ((((unsigned long long)d_" << c << ") & 15ULL) == 0ULL);\n";
+      o << "  unsigned long long l2_policy = 0;\n";
+      o << "  if (lane == 0) {\n";
+      o << "    for (int s = 0; s < NSTAGE; ++s) cx::mbar_init(&bars[s], 1);\n";
+      o << "    cx::fence_mbar_init();\n";
+      o << "    l2_policy = cx::l2_evict_first_policy();\n";
+      o << "  }\n";
+      o << "#define CX_ISSUE(TILE_, STAGE_) do { \\\n";
+      o << "    cx::mbar_expect_tx(&bars[(STAGE_)], " << (unsigned long long)NSC * WT * 4 << "u); \\\n";
+      for (int c = 0; c < NSC; ++c)
+        o << "    cx::bulk_g2s(stage_buf + ((STAGE_) * NSC + " << c << ") * TILE_SIZE, d_" << fact_cols[c]
+          << " + (TILE_) * TILE_SIZE, " << WT * 4 << "u, &bars[(STAGE_)], l2_policy); \\\n";
+      o << "  } while (0)\n";
+    }
+    o << "  __syncthreads();\n";
+    if (STAGES > 0) {
+      o << "  if (lane == 0 && staged_ok) {\n";
+      o << "    for (int k = 0; k < NSTAGE; ++k) {\n";
+      o << "      const long long t = gwarp + (long long)k * nwarps;\n";
+      o << "      if (t < full_tiles) CX_ISSUE(t, k);\n";
+      o << "    }\n";
+      o << "  }\n";
+    }
+    o << "  long long k_iter = 0;\n";
+    o << "  bool aborted = false; (void)aborted;\n";
+    o << "  for (long long t = gwarp; t < num_tiles; t += nwarps, ++k_iter) {\n";
+    o << "    const long long tile_offset = t * TILE_SIZE;\n";
+    o << "    const int num_tile_items = (int)(n_rows - tile_offset < TILE_SIZE ? n_rows - tile_offset : TILE_SIZE);\n";
+    if (STAGES > 0) {
+      o << "    const int stage = (int)(k_iter % NSTAGE);\n";
+      o << "    const bool staged = staged_ok && t < full_tiles;\n";
+      o << "    bool timed_out = false;\n";
+      o << "    if (staged) timed_out = !cx::mbar_wait_bounded(&bars[stage], (unsigned)((k_iter / NSTAGE) & 1), " << wait_limit << "u);\n";
+      o << "    if (__any_sync(0xffffffffu, timed_out)) { if (lane == 0) cx::raise(a.err, cx::ERR_WAIT_TIMEOUT); aborted = true; break; }\n";
+      for (int c = 0; c < NSC; ++c)
+        o << "    const int* t_" << fact_cols[c] << " = staged ? stage_buf + (stage * NSC + " << c << ") * TILE_SIZE : d_"
+          << fact_cols[c] << " + tile_offset;\n";
+    } else {
+      for (int c = 0; c < NSC; ++c) o << "    const int* t_" << fact_cols[c] << " = d_" << fact_cols[c] << " + tile_offset;\n";
+    }
+    // Union columns into registers, once per tile for every query.
+    for (const auto& c : fact_cols) {
+      o << "    int " << c << "[ITEMS_PER_THREAD];\n";
+      o << "    BlockLoad<int, BLOCK_THREADS, ITEMS_PER_THREAD>(t_" << c << ", tid, tile_offset, " << c << ", num_tile_items);\n";
+    }
+    // One gather per dimension, shared by every query.
+    const char* comp[] = {"y", "z", "w"};
+    for (const Dim& d : dims) {
+      o << "    int " << d.pk << "[ITEMS_PER_THREAD];\n";
+      for (const auto& at : d.attrs) o << "    int " << at << "[ITEMS_PER_THREAD];\n";
+      o << "    #pragma unroll\n    for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << "      int4 g_ = make_int4(0, 0, 0, 0);\n";
+      o << "      if (tid + BLOCK_THREADS * i < num_tile_items) {\n";
+      o << "        const int h_ = (int)HASH(" << d.fk << "[i], " << d.len << ", " << d.keymin << ");\n";
+      o << "        if ((unsigned)h_ < " << d.len << "u) g_ = __ldg(&dix_" << lower(d.name) << "[h_]);\n";
+      o << "      }\n";
+      o << "      " << d.pk << "[i] = g_.x;\n";
+      for (size_t k = 0; k < d.attrs.size(); ++k) o << "      " << d.attrs[k] << "[i] = g_." << comp[k] << ";\n";
+      o << "    }\n";
+    }
+    // Every query of every shape.
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      const Plan& p = *shapes[s];
+      Emitter e(p, tu);
+      e.lit_index = &lit_maps[s];
+      for (const auto& c : fact_cols) e.loaded.insert(c);
+      for (const Dim& d : dims) {
+        e.loaded.insert(d.pk);
+        for (const auto& at : d.attrs) e.loaded.insert(at);
+      }
+      const std::string ind = "      ";
+      o << "    for (int j_ = 0; j_ < a.sq_num[" << s << "]; ++j_) {\n";
+      o << "      const int q_ = a.sq_first[" << s << "] + j_;\n";
+      o << "      const int* P = s_params + sq[q_].param_off; (void)P;\n";
+      o << "      int flags[ITEMS_PER_THREAD];\n";
+      o << "      InitFlags<BLOCK_THREADS, ITEMS_PER_THREAD>(flags);\n";
+      for (const auto& st : p.steps) {
+        if (st.kind == Step::Filter) {
+          e.emit_filter(o, st.filter.get(), ind);
+          continue;
+        }
+        const Join& j = st.join;
+        std::string cond = j.filter ? and_terms({e.valid_of(j.filter.get()), e.value_of(j.filter.get())}) : "1";
+        o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+        o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+        o << ind << "    bool ok_ = " << j.pk << "[i] != 0 && " << j.pk << "[i] == " << j.fks[0] << "[i];\n";
+        if (!lit_true(cond)) o << ind << "    if (ok_) ok_ = (" << cond << ");\n";
+        o << ind << "    flags[i] = ok_ ? 1 : 0;\n";
+        o << ind << "  }\n" << ind << "}\n";
+      }
+      const int NA = (int)p.aggs.size();
+      if (p.groups.empty()) {
+        for (int k = 0; k < NA; ++k) {
+          const Agg& ag = p.aggs[k];
+          const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
+          const std::string x = ag.fn == AggFn::Count ? "1ULL" : e.math_push(ag.arg.get(), true);
+          o << ind << "{ unsigned long long s_ = 0ULL, c_ = 0ULL;\n";
+          o << ind << "  #pragma unroll\n" << ind << "  for (int i = 0; i < ITEMS_PER_THREAD; ++i)\n";
+          o << ind << "    if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items) && (" << v << ")) { s_ += " << x << "; c_ += 1ULL; }\n";
+          o << ind << "  if (__any_sync(0xffffffffu, c_ != 0ULL)) {\n";
+          o << ind << "    for (int o_ = 16; o_ > 0; o_ >>= 1) { s_ += __shfl_xor_sync(0xffffffffu, s_, o_); c_ += __shfl_xor_sync(0xffffffffu, c_, o_); }\n";
+          o << ind << "    if (lane == 0) { atomicAdd(&s_qacc[(long long)q_ * " << NACC << " + " << 2 * k << "], s_); atomicAdd(&s_qacc[(long long)q_ * " << NACC << " + " << 2 * k + 1 << "], c_); }\n";
+          o << ind << "  }\n" << ind << "}\n";
+        }
+      } else {
+        const unsigned long long G = e.total_groups();
+        const int TS = p.storage_ts();
+        o << ind << "unsigned long long* d_result = sq[q_].result;\n";
+        o << ind << "uint64_t* d_result_validity = (uint64_t*)sq[q_].validity; (void)d_result_validity;\n";
+        o << ind << "unsigned int* g_touch = sq[q_].touched;\n";
+        o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+        o << ind << "  bool act = flags[i] && (tid + BLOCK_THREADS * i < num_tile_items);\n";
+        o << ind << "  int hash = 0;\n";
+        o << ind << "  if (act) {\n";
+        std::string horner, dom;
+        for (size_t k = 0; k < p.groups.size(); ++k) {
+          o << ind << "    const int gt" << k << " = " << e.group_term(k) << ";\n";
+          horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(e.eff_card(k)) + " + gt" + std::to_string(k) + ")";
+          dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " + std::to_string(e.eff_card(k)) + "u";
+        }
+        o << ind << "    hash = (" << horner << ") % " << G << ";\n";
+        o << ind << "    if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+        o << ind << "    if ((unsigned)hash >= " << G << "u) act = false;\n";
+        o << ind << "  }\n";
+        o << ind << "  const unsigned amask = __ballot_sync(0xffffffffu, act);\n";
+        o << ind << "  if (amask != 0u && act) {\n";
+        for (int k = 0; k < NA; ++k) {
+          const Agg& ag = p.aggs[k];
+          const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
+          const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
+          o << ind << "    bool v" << k << " = (" << v << ");\n";
+          o << ind << "    unsigned long long x" << k << " = v" << k << " ? " << x << " : 0ULL;\n";
+        }
+        o << ind << "    const unsigned peers = __popc(amask) == 1 ? amask : __match_any_sync(amask, (unsigned)hash);\n";
+        o << ind << "    const int leader = __ffs(peers) - 1;\n";
+        o << ind << "    if (__popc(peers) > 1) {\n";
+        for (int k = 0; k < NA; ++k) {
+          o << ind << "      { unsigned long long r_ = 0ULL;\n";
+          o << ind << "        for (unsigned m = peers; m; m &= m - 1) r_ += __shfl_sync(peers, x" << k << ", __ffs(m) - 1);\n";
+          o << ind << "        x" << k << " = r_; }\n";
+          if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "      v" << k << " = __ballot_sync(peers, v" << k << ") != 0u;\n";
+        }
+        o << ind << "    }\n";
+        o << ind << "    if (lane == leader) {\n";
+        o << ind << "      atomicOr(&g_touch[hash >> 5], 1u << (hash & 31));\n";
+        for (int k = 0; k < NA; ++k) {
+          const int slot = (int)p.groups.size() + k;
+          const std::string ix = "(unsigned long long)hash * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
+          o << ind << "      if (x" << k << ") atomicAdd(&d_result[" << ix << "], x" << k << ");\n";
+          if (!p.sparse) {
+            if (p.aggs[k].fn == AggFn::Count) o << ind << "      db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+            else o << ind << "      if (v" << k << ") db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+          }
+        }
+        o << ind << "    }\n";
+        o << ind << "  }\n";
+        o << ind << "}\n";
+      }
+      o << "    }\n";
+    }
+    if (STAGES > 0) {
+      o << "    __syncwarp();\n";
+      o << "    if (lane == 0 && staged_ok) {\n";
+      o << "      const long long t2 = t + (long long)NSTAGE * nwarps;\n";
+      o << "      if (t2 < full_tiles) CX_ISSUE(t2, stage);\n";
+      o << "    }\n";
+    }
+    o << "  }\n";
+    if (STAGES > 0)
+      o << "  if (aborted && lane == 0 && staged_ok) cx::drain_stages(bars, NSTAGE, k_iter, gwarp, nwarps, full_tiles, " << wait_limit << "u);\n";
+    // Scalar queries: one flush per CTA.
+    o << "  __syncthreads();\n";
+    o << "  for (int q = threadIdx.x; q < a.sq_total; q += " << CTA << ") {\n";
+    o << "    const CxSQ Q = sq[q];\n";
+    o << "    switch (Q.shape) {\n";
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      const Plan& p = *shapes[s];
+      if (!p.groups.empty()) continue;
+      o << "      case " << s << ": {\n";
+      for (size_t k = 0; k < p.aggs.size(); ++k) {
+        o << "        { const unsigned long long s_ = s_qacc[(long long)q * " << NACC << " + " << 2 * k << "], c_ = s_qacc[(long long)q * " << NACC << " + " << 2 * k + 1 << "];\n";
+        o << "          if (s_) atomicAdd(&Q.result[" << k << "], s_);\n";
+        if (p.aggs[k].fn == AggFn::Count) o << "          db::atomic_set_valid_bit((uint64_t*)Q.validity, " << k << ");\n";
+        else o << "          if (c_) db::atomic_set_valid_bit((uint64_t*)Q.validity, " << k << ");\n";
+        o << "        }\n";
+      }
+      o << "        break; }\n";
+    }
+    o << "      default: break;\n";
+    o << "    }\n";
+    o << "  }\n";
+    o << "}\n";
+    if (STAGES > 0) o << "#undef CX_ISSUE\n";
+    o << "\n";
+  }
+
+  void emit_keys() {
+    meta << "kernel shared_keys_epilogue queries 0 256 0\n";
+    src << "extern \"C\" __global__ void __launch_bounds__(256) shared_keys_epilogue(const CxArgs a) {\n";
+    src << "  const int q = blockIdx.x;\n";
+    src << "  if (q >= a.sq_total) return;\n";
+    src << "  const CxSQ Q = a.sq[q];\n";
+    src << "  unsigned long long* d_result = Q.result; (void)d_result;\n";
+    src << "  uint64_t* d_result_validity = (uint64_t*)Q.validity; (void)d_result_validity;\n";
+    src << "  switch (Q.shape) {\n";
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      const Plan& p = *shapes[s];
+      if (p.groups.empty()) continue;
+      Emitter e(p, tu);
+      src << "    case " << s << ":\n";
+      src << "      for (long long g = threadIdx.x; g < " << e.total_groups() << "LL; g += blockDim.x) {\n";
+      src << "        if (!((Q.touched[g >> 5] >> (g & 31)) & 1u)) continue;\n";
+      e.emit_key_store(src, "g", "        ");
+      src << "      }\n      break;\n";
+    }
+    src << "    default: break;\n  }\n}\n\n";
+  }
+
+  static constexpr int CX_MAX_COLS_ = 40;
+  static constexpr int CX_MAX_HTS_ = 8;
+  static constexpr size_t CX_MAX_SHAPES_ = 16;
+};
+
+}  // namespace
+
+std::string generate_cuda(const Plan& plan, const Tuning& tuning) { return generate_cuda_impl(plan, tuning); }
+
+void collect_literals(const Plan& p, std::vector<const Expr*>& out) {
+  for (const auto& s : p.steps) {
+    if (s.kind == Step::Filter) lits_of(s.filter.get(), out);
+    else lits_of(s.join.filter.get(), out);
+  }
+  for (const auto& g : p.groups) lits_of(g.expr.get(), out);
+  for (const auto& a : p.aggs) lits_of(a.arg.get(), out);
+}
+
+std::string generate_shared_cuda(const std::vector<const Plan*>& shapes, const Tuning& tuning) {
+  SharedGen g(shapes, tuning);
+  return g.run();
 }
 
 }  // namespace cx

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <string>
+#include <vector>
 
 #include "cx_plan.h"
 
@@ -24,5 +25,15 @@ struct Tuning {
 // Returns the CUDA source for `plan` with its launch plan embedded as a
 // leading `/*@cx-launch ... @*/` block.  Throws PlanError on unsupported shapes.
 std::string generate_cuda(const Plan& plan, const Tuning& tuning);
+
+// The integer literals of a plan in the canonical order that numbers the
+// parameters of its shape (steps, then GROUP BY, then aggregates; pre-order).
+void collect_literals(const Plan& plan, std::vector<const Expr*>& out);
+
+// Shared-scan kernel for a set of plan shapes (one representative plan per
+// shape; literals become per-query parameters).  Throws PlanError when a shape
+// cannot share a scan (nullable columns, AVG/MIN/MAX, > 3 attributes of one
+// dimension, conflicting joins, literals outside int32).
+std::string generate_shared_cuda(const std::vector<const Plan*>& shapes, const Tuning& tuning);
 
 }  // namespace cx

@@ -120,6 +120,9 @@ struct LaunchPlan {
   uint64_t fin_groups = 0;
   int fin_vts = 0;
   std::vector<KernelSpec> kernels;
+  bool shared = false;
+  struct SShape { uint64_t groups; int ts, grouped, sparse, nlits; };
+  std::vector<SShape> sshapes;
 };
 
 bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err) {
@@ -160,6 +163,13 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       int s; uint64_t w;
       ls >> s >> w;
       lp.htv_words[s] = w;
+    } else if (k == "shared") {
+      lp.shared = true;
+    } else if (k == "sshape") {
+      int i; LaunchPlan::SShape sh;
+      ls >> i >> sh.groups >> sh.ts >> sh.grouped >> sh.sparse >> sh.nlits;
+      if (i != (int)lp.sshapes.size()) { err = "shape lines out of order"; return false; }
+      lp.sshapes.push_back(sh);
     } else if (k == "bm") {
       int s; uint64_t w;
       ls >> s >> w;
@@ -265,6 +275,8 @@ struct cx_exec_ctx {
   int sm_override = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   unsigned int* host_err = nullptr;  // pinned
+  void* host_stage = nullptr;        // pinned staging of shared-scan descriptors
+  size_t host_stage_bytes = 0;
   bool pending = false;
   cx_timing timing{};
   uint32_t kernel_err = 0;
@@ -469,6 +481,7 @@ void cx_ctx_destroy(cx_exec_ctx* c) {
     if (e) cudaEventDestroy(e);
   if (c->own_scratch) cudaFree(c->own_scratch);
   if (c->host_err) cudaFreeHost(c->host_err);
+  if (c->host_stage) cudaFreeHost(c->host_stage);
   delete c;
 }
 
@@ -524,6 +537,7 @@ int cx_module_scratch_bytes(const cx_module* m, const cx_exec_ctx* c, uint64_t* 
 int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream_v) {
   if (!m || !c) return fail(CX_E_INVALID, "cx_execute: NULL argument");
   const LaunchPlan& lp = m->lp;
+  if (lp.shared) return fail(CX_E_INVALID, "cx_execute: a shared-scan program runs through cx_shared_execute");
   cudaStream_t stream = (cudaStream_t)stream_v;
 
   // Resolve tables, columns and result buffers before touching the GPU.
@@ -640,8 +654,9 @@ int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream_v) {
   if (ki < lp.kernels.size()) {
     const KernelSpec& k = lp.kernels[ki];
     const long long tiles = (rows[0] + k.tile - 1) / k.tile;
+    const long long warps = std::max(1, k.block / 32);
     const int per_sm = std::max(1, std::min(k.ctas_per_sm, L->occupancy[ki]));
-    const long long grid = std::min<long long>(tiles, (long long)sms * per_sm);
+    const long long grid = std::min<long long>((tiles + warps - 1) / warps, (long long)sms * per_sm);
     scan_grid = (int)grid;
     if ((rc = launch(ki, (unsigned)grid))) return rc;
     ++ki;
@@ -658,6 +673,220 @@ int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream_v) {
     CX_CUDA(cudaMemcpyAsync(c->result, a.finalize_tmp, vis * 8, cudaMemcpyDeviceToDevice, stream));
     CX_CUDA(cudaMemcpyAsync(c->validity, a.finalize_tmp + vis, ((vis + 63) / 64) * 8, cudaMemcpyDeviceToDevice, stream));
   }
+  CX_CUDA(cudaMemcpyAsync(c->host_err, a.err, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
+  CX_CUDA(cudaEventRecord(c->ev[3], stream));
+  c->pending = true;
+  c->timing = cx_timing{};
+  c->timing.scan_grid = scan_grid;
+  c->timing.gpu_launches = launches;
+  return CX_OK;
+}
+
+
+int cx_plan_literals(const char* plan, size_t plan_len, int64_t* out, int cap, int* n) {
+  if (!plan || !n) return fail(CX_E_INVALID, "cx_plan_literals: NULL argument");
+  try {
+    auto p = cx::parse_plan(std::string(plan, plan_len));
+    std::vector<const cx::Expr*> lits;
+    cx::collect_literals(*p, lits);
+    *n = (int)lits.size();
+    if (out)
+      for (int i = 0; i < (int)lits.size() && i < cap; ++i) out[i] = lits[i]->ival;
+    if (out && cap < (int)lits.size()) return fail(CX_E_CAPACITY, "cx_plan_literals: %d literals, capacity %d", (int)lits.size(), cap);
+    return CX_OK;
+  } catch (const std::exception& e) {
+    return fail(CX_E_INVALID, "%s", e.what());
+  }
+}
+
+int cx_shared_codegen(const char* const* plans, const size_t* lens, int nshapes, const cx_tuning* tuning, char* out,
+                      size_t out_cap, size_t* out_len) {
+  if (!plans || !lens || nshapes <= 0) return fail(CX_E_INVALID, "cx_shared_codegen: no shapes");
+  try {
+    std::vector<std::unique_ptr<cx::Plan>> owned;
+    std::vector<const cx::Plan*> shapes;
+    for (int i = 0; i < nshapes; ++i) {
+      owned.push_back(cx::parse_plan(std::string(plans[i], lens[i])));
+      shapes.push_back(owned.back().get());
+    }
+    cx::Tuning t;
+    if (tuning) {
+      t.block_threads = tuning->block_threads;
+      t.items_per_thread = tuning->items_per_thread;
+      t.stages = tuning->stages;
+      t.ctas_per_sm = tuning->ctas_per_sm;
+      t.group_placement = tuning->group_placement;
+      t.smem_group_budget = tuning->smem_group_budget;
+      t.bitmap_budget = tuning->bitmap_budget;
+      t.group_merge = tuning->group_merge;
+    }
+    const std::string src = cx::generate_shared_cuda(shapes, t);
+    if (out_len) *out_len = src.size();
+    if (out && out_cap) {
+      const size_t n = src.size() < out_cap - 1 ? src.size() : out_cap - 1;
+      memcpy(out, src.data(), n);
+      out[n] = '\0';
+      if (n < src.size()) return fail(CX_E_CAPACITY, "cx_shared_codegen: output buffer too small");
+    }
+    return CX_OK;
+  } catch (const std::exception& e) {
+    return fail(CX_E_INVALID, "%s", e.what());
+  }
+}
+
+int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queries, int nq, const int32_t* params,
+                      int nparams, void* stream_v) {
+  if (!m || !c || (!queries && nq > 0) || nq < 0 || nparams < 0 || (nparams > 0 && !params))
+    return fail(CX_E_INVALID, "cx_shared_execute: bad argument");
+  const LaunchPlan& lp = m->lp;
+  if (!lp.shared) return fail(CX_E_INVALID, "cx_shared_execute: not a shared-scan program");
+  if (nq > 256 || nparams > 4096) return fail(CX_E_CAPACITY, "cx_shared_execute: batch of %d queries / %d parameters exceeds 256 / 4096", nq, nparams);
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  const int nshapes = (int)lp.sshapes.size();
+
+  CxArgs a;
+  memset(&a, 0, sizeof a);
+  std::vector<long long> rows(lp.tables.size(), 0);
+  for (size_t t = 0; t < lp.tables.size(); ++t) {
+    auto it = c->rows.find(lp.tables[t]);
+    if (it == c->rows.end()) return fail(CX_E_MISSING, "cx_shared_execute: row count of table %s is not set", lp.tables[t].c_str());
+    rows[t] = (long long)it->second;
+    a.rows[t] = rows[t];
+  }
+  for (const auto& col : lp.cols) {
+    auto it = c->buffers.find(col.name);
+    if (it == c->buffers.end() || (!it->second.first && rows[col.table] > 0))
+      return fail(CX_E_MISSING, "cx_shared_execute: buffer %s is not in the execution context", col.name.c_str());
+    if (it->second.second < (uint64_t)rows[col.table])
+      return fail(CX_E_CAPACITY, "cx_shared_execute: buffer %s is shorter than its table", col.name.c_str());
+    a.col[col.slot] = (const int*)it->second.first;
+  }
+  // Queries grouped by shape; validate each query's buffers and parameters.
+  std::vector<int> order;
+  for (int s = 0; s < nshapes; ++s) {
+    a.sq_first[s] = (int)order.size();
+    for (int q = 0; q < nq; ++q)
+      if (queries[q].shape == s) order.push_back(q);
+    a.sq_num[s] = (int)order.size() - a.sq_first[s];
+  }
+  if ((int)order.size() != nq) return fail(CX_E_INVALID, "cx_shared_execute: a query names a shape outside 0..%d", nshapes - 1);
+  a.sq_total = nq;
+  a.nparams = nparams;
+
+  // Scratch: dimension indexes, touched bits per grouped query, descriptors, parameters, error word.
+  uint64_t off = 0;
+  std::vector<uint64_t> dix_off;
+  for (const auto& h : lp.hts) { dix_off.push_back(off); off = align256(off + h.words * 4); }
+  std::vector<uint64_t> touch_off(nq, 0);
+  for (int i = 0; i < nq; ++i) {
+    const auto& sh = lp.sshapes[queries[order[i]].shape];
+    if (sh.grouped) { touch_off[i] = off; off = align256(off + ((sh.groups + 31) / 32) * 4); }
+  }
+  const uint64_t zero_end = off;
+  const uint64_t sq_off = off; off = align256(off + (uint64_t)std::max(nq, 1) * sizeof(CxSQ));
+  const uint64_t par_off = off; off = align256(off + (uint64_t)std::max(nparams, 1) * 4);
+  const uint64_t err_off = off; off = align256(off + 16);
+  const uint64_t total = off;
+
+  int dev = 0;
+  CX_CUDA(cudaGetDevice(&dev));
+  int rc = ensure_ctx_device(c, dev);
+  if (rc) return rc;
+  cx_module::Loaded* L = nullptr;
+  rc = load_on_device(m, dev, &L);
+  if (rc) return rc;
+  if (c->pending) { CX_CUDA(cudaEventSynchronize(c->ev[3])); c->pending = false; }
+
+  char* scratch = nullptr;
+  if (c->user_scratch) {
+    if (c->user_scratch_bytes < total) return fail(CX_E_CAPACITY, "cx_shared_execute: caller scratch too small (%llu < %llu)", (unsigned long long)c->user_scratch_bytes, (unsigned long long)total);
+    scratch = (char*)c->user_scratch;
+  } else {
+    if (c->own_scratch_bytes < total) {
+      if (c->own_scratch) { cudaFree(c->own_scratch); c->own_scratch = nullptr; c->own_scratch_bytes = 0; }
+      const uint64_t grow = total + total / 2;
+      CX_CUDA(cudaMalloc(&c->own_scratch, grow));
+      c->own_scratch_bytes = grow;
+    }
+    scratch = (char*)c->own_scratch;
+  }
+  for (size_t i = 0; i < lp.hts.size(); ++i) a.ht[lp.hts[i].slot] = (int*)(scratch + dix_off[i]);
+  a.err = (unsigned int*)(scratch + err_off);
+  a.sq = (const CxSQ*)(scratch + sq_off);
+  a.sparams = (const int*)(scratch + par_off);
+
+  // Host staging of descriptors and parameters (pinned, reused across batches).
+  const size_t stage_bytes = (size_t)std::max(nq, 1) * sizeof(CxSQ) + (size_t)std::max(nparams, 1) * 4;
+  if (c->host_stage_bytes < stage_bytes) {
+    if (c->host_stage) cudaFreeHost(c->host_stage);
+    c->host_stage = nullptr;
+    c->host_stage_bytes = 0;
+    CX_CUDA(cudaMallocHost(&c->host_stage, stage_bytes * 2));
+    c->host_stage_bytes = stage_bytes * 2;
+  }
+  CxSQ* hsq = (CxSQ*)c->host_stage;
+  int* hpar = (int*)((char*)c->host_stage + (size_t)std::max(nq, 1) * sizeof(CxSQ));
+  for (int i = 0; i < nq; ++i) {
+    const cx_shared_query& q = queries[order[i]];
+    const auto& sh = lp.sshapes[q.shape];
+    const uint64_t need = sh.groups * (uint64_t)sh.ts;
+    if (!q.result || q.result_words < need || !q.validity || q.validity_words < (need + 63) / 64)
+      return fail(CX_E_CAPACITY, "cx_shared_execute: query %d result buffers are smaller than its shape needs (%llu words)", order[i], (unsigned long long)need);
+    if (q.param_off < 0 || q.param_off + sh.nlits > nparams)
+      return fail(CX_E_INVALID, "cx_shared_execute: query %d parameters fall outside the parameter array", order[i]);
+    hsq[i].result = (unsigned long long*)q.result;
+    hsq[i].validity = (unsigned long long*)q.validity;
+    hsq[i].touched = sh.grouped ? (unsigned int*)(scratch + touch_off[i]) : nullptr;
+    hsq[i].shape = q.shape;
+    hsq[i].param_off = q.param_off;
+  }
+  if (nparams) memcpy(hpar, params, (size_t)nparams * 4);
+
+  int sms = c->sm_override;
+  if (sms <= 0) CX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  Driver& d = driver();
+  int launches = 0, scan_grid = 0;
+  void* kparams[] = {&a};
+  auto launch = [&](size_t ki, unsigned grid) -> int {
+    const KernelSpec& k = lp.kernels[ki];
+    if (grid == 0) return CX_OK;
+    CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, (unsigned)k.smem, (CUstream)stream, kparams, nullptr);
+    if (r != CUDA_SUCCESS) return drv_fail(r, k.name.c_str());
+    ++launches;
+    return CX_OK;
+  };
+
+  CX_CUDA(cudaEventRecord(c->ev[0], stream));
+  CX_CUDA(cudaMemcpyAsync(scratch + sq_off, c->host_stage, (size_t)std::max(nq, 1) * sizeof(CxSQ), cudaMemcpyHostToDevice, stream));
+  if (nparams) CX_CUDA(cudaMemcpyAsync(scratch + par_off, hpar, (size_t)nparams * 4, cudaMemcpyHostToDevice, stream));
+  CX_CUDA(cudaMemsetAsync(scratch, 0, zero_end, stream));
+  CX_CUDA(cudaMemsetAsync(scratch + err_off, 0, 16, stream));
+  for (int i = 0; i < nq; ++i) {
+    const auto& sh = lp.sshapes[queries[order[i]].shape];
+    const uint64_t need = sh.groups * (uint64_t)sh.ts;
+    CX_CUDA(cudaMemsetAsync(hsq[i].result, 0, need * 8, stream));
+    CX_CUDA(cudaMemsetAsync(hsq[i].validity, 0, ((need + 63) / 64) * 8, stream));
+  }
+  size_t ki = 0;
+  for (; ki < lp.kernels.size() && lp.kernels[ki].kind != "scan"; ++ki) {
+    const KernelSpec& k = lp.kernels[ki];
+    const long long tiles = (rows[k.table] + k.tile - 1) / k.tile;
+    if ((rc = launch(ki, (unsigned)std::min<long long>(tiles, (long long)sms * 16)))) return rc;
+  }
+  CX_CUDA(cudaEventRecord(c->ev[1], stream));
+  if (ki < lp.kernels.size() && nq > 0) {
+    const KernelSpec& k = lp.kernels[ki];
+    const long long tiles = (rows[0] + k.tile - 1) / k.tile;
+    const long long warps = std::max(1, k.block / 32);
+    const int per_sm = std::max(1, std::min(k.ctas_per_sm, L->occupancy[ki]));
+    const long long grid = std::min<long long>((tiles + warps - 1) / warps, (long long)sms * per_sm);
+    scan_grid = (int)grid;
+    if ((rc = launch(ki, (unsigned)grid))) return rc;
+  }
+  if (ki < lp.kernels.size()) ++ki;
+  CX_CUDA(cudaEventRecord(c->ev[2], stream));
+  for (; ki < lp.kernels.size(); ++ki)
+    if ((rc = launch(ki, (unsigned)nq))) return rc;
   CX_CUDA(cudaMemcpyAsync(c->host_err, a.err, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
   CX_CUDA(cudaEventRecord(c->ev[3], stream));
   c->pending = true;

@@ -32,6 +32,16 @@ def _torch():
     return torch
 
 
+class SharedProgram:
+    """A compiled shared-scan program for a set of plan shapes."""
+
+    def __init__(self, module: _lib.Module, shape_keys: list[str], nlits: list[int]):
+        self.module = module
+        self.shape_keys = shape_keys
+        self.nlits = nlits
+        self.index = {k: i for i, k in enumerate(shape_keys)}
+
+
 @dataclass
 class QueryResult:
     words: np.ndarray      # u64 result words (final layout)
@@ -215,6 +225,121 @@ class Database:
                 pass
         best["table"] = table
         return best
+
+    # ------------------------------------------------------ shared scans
+    def column_min(self, name: str) -> int:
+        cache = self.__dict__.setdefault("_colmin", {})
+        if name not in cache:
+            t = self.cols[name]
+            cache[name] = int(t.min().item()) if t.numel() else 1
+        return cache[name]
+
+    def shareable(self, plan: Plan) -> bool:
+        """A plan can join a shared scan when its shape compiles into one and
+        every foreign key it probes is non-zero (the empty-slot sentinel)."""
+        try:
+            _lib.shared_codegen([plan.text()])
+        except _lib.CxError:
+            return False
+        for kind, s in plan.steps:
+            if kind == "join" and self.column_min(s.fk) <= 0:
+                return False
+        return True
+
+    def shared_program(self, plans: list[Plan], tuning: _lib.Tuning | None = None) -> SharedProgram:
+        keys: list[str] = []
+        reps: list[Plan] = []
+        for p in plans:
+            k = shape_key(p)
+            if k not in keys:
+                keys.append(k)
+                reps.append(p)
+        order = sorted(range(len(keys)), key=lambda i: keys[i])
+        keys = [keys[i] for i in order]
+        reps = [reps[i] for i in order]
+        tkey = tuple(getattr(tuning, f) for f, _ in _lib.Tuning._fields_) if tuning is not None else None
+        ck = ("shared", tuple(keys), tkey)
+        prog = self._modules.get(ck)
+        if prog is None:
+            src = _lib.shared_codegen([r.text() for r in reps], tuning)
+            mod = _lib.Module(src, key=f"shared_{abs(hash(ck))}")
+            prog = SharedProgram(mod, keys, [len(_lib.plan_literals(r.text())) for r in reps])
+            self._modules[ck] = prog
+        return prog
+
+    def shared_prepare(self, prog: SharedProgram, plans: list[Plan]):
+        """Per-query result buffers, descriptors and the parameter array."""
+        torch = self.torch
+        queries, params, bufs = [], [], []
+        for p in plans:
+            s = prog.index[shape_key(p)]
+            words = p.group_slots * p.storage_ts
+            res = torch.empty(max(words, 1), dtype=torch.int64, device=self.device)
+            val = torch.empty(max((words + 63) // 64, 1), dtype=torch.int64, device=self.device)
+            lits = _lib.plan_literals(p.text())
+            queries.append(_lib.SharedQuery(s, len(params), res.data_ptr(), res.numel(), val.data_ptr(), val.numel()))
+            params.extend(lits)
+            bufs.append((res, val, words))
+        return queries, params, bufs
+
+    def execute_shared(self, plans: list[Plan], tuning: _lib.Tuning | None = None,
+                       stream=None) -> list[QueryResult]:
+        torch = self.torch
+        prog = self.shared_program(plans, tuning)
+        queries, params, bufs = self.shared_prepare(prog, plans)
+        for t, n in self.rows.items():
+            self.ctx.set_rows(t, n)
+        s = stream if stream is not None else torch.cuda.current_stream()
+        self.ctx.shared_execute(prog.module, queries, params, s.cuda_stream)
+        err = 0
+        try:
+            self.ctx.sync()
+        except _lib.CxError as e:
+            if e.code != -6:
+                raise
+            err = self.ctx.kernel_error()
+        timing = self.ctx.timing()
+        out = []
+        for res, val, words in bufs:
+            w = res.cpu().numpy().view(np.uint64)[:words].copy()
+            v = val.cpu().numpy().view(np.uint64)[: (words + 63) // 64].copy()
+            out.append(QueryResult(w, v, timing, err))
+        return out
+
+    def autotune_shared(self, plans: list[Plan], candidates: list[dict], reps: int = 2) -> dict:
+        """Times each candidate launch shape of the shared program for the
+        plans' shape set and caches the fastest (keyed by the sorted shapes)."""
+        key = "shared|" + "|".join(sorted({shape_key(p) for p in plans}))
+        table = []
+        for cand in candidates:
+            t = make_tuning(**cand)
+            try:
+                prog = self.shared_program(plans, t)
+            except _lib.CxError:
+                continue
+            queries, params, bufs = self.shared_prepare(prog, plans)
+            for tn, n in self.rows.items():
+                self.ctx.set_rows(tn, n)
+            times = []
+            try:
+                for _ in range(reps + 1):
+                    self.ctx.shared_execute(prog.module, queries, params, self.torch.cuda.current_stream().cuda_stream)
+                    self.ctx.sync()
+                    times.append(self.ctx.timing().scan_ms)
+            except _lib.CxError:
+                continue
+            table.append((min(times[1:]), cand))
+        if not table:
+            raise RuntimeError("autotune_shared: no feasible launch shape")
+        table.sort(key=lambda x: x[0])
+        best = {"tuning": tuning_dict(make_tuning(**table[0][1])), "scan_ms": table[0][0], "tried": len(table)}
+        self.tuned[key] = best
+        best["table"] = table
+        return best
+
+    def shared_tuning_for(self, plans: list[Plan]) -> _lib.Tuning | None:
+        best = self.tuned.get("shared|" + "|".join(sorted({shape_key(p) for p in plans})))
+        return make_tuning(**best["tuning"]) if best else None
 
     def alloc_result(self, module: _lib.Module):
         torch = self.torch

@@ -156,3 +156,35 @@ def test_plan_text_is_deterministic():
     t = {"T": Table("T", ["a"], 1, fact=True)}
     p = PlanBuilder(t, "T").filter(col("a").gt(3)).aggregate([], [("count", star())])
     assert "(filter (gt (col a) (int 3)))" in p.text()
+
+
+def test_shared_program_for_the_four_templates_compiles():
+    rng = random.Random(11)
+    plans = [queries.template(t, rng) for t in range(4)]
+    src = _lib.shared_codegen([p.text() for p in plans])
+    assert "SharedScan_LINEORDER" in src and "index_customer" in src
+    m = _lib.Module(src, key="cpu_shared_templates")
+    assert m.info.result_words >= 0
+    # literals come back in the order that numbers the shape's parameters
+    assert _lib.plan_literals(plans[1].text())[0] == plans[1].steps[0][1].kids[1].val
+
+
+def test_shared_program_rejects_unshareable_shapes():
+    with pytest.raises(_lib.CxError):
+        _lib.shared_codegen([queries.config3(1000).text()])  # nullable columns
+    with pytest.raises(_lib.CxError):
+        _lib.shared_codegen([queries.kat_plans()["q1"].text()])  # AVG
+
+
+def test_shared_execute_validates_before_touching_the_gpu():
+    rng = random.Random(12)
+    p = queries.template(2, rng)
+    m = _lib.Module(_lib.shared_codegen([p.text()]), key="cpu_shared_validate")
+    ctx = _lib.ExecCtx()
+    with pytest.raises(_lib.CxError) as e:
+        ctx.shared_execute(m, [], [])
+    assert e.value.code == -4  # table rows unset
+    plain = _lib.Module(_lib.codegen(p.text()), key="cpu_plain_validate")
+    with pytest.raises(_lib.CxError) as e:
+        ctx.shared_execute(plain, [], [])
+    assert e.value.code == -1

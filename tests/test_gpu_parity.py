@@ -199,3 +199,39 @@ def test_sparse_compaction(db):
     expect = tuples[(tuples != 0).any(axis=1)]
     assert k == len(expect) > 0
     np.testing.assert_array_equal(dst.cpu().numpy().view(np.uint64)[: k * ts].reshape(-1, ts), expect)
+
+
+# ------------------------------------------------------------ shared scans
+
+@pytest.mark.parametrize("nq,tune", [(16, None), (37, (512, 2, 0)), (64, (1024, 4, 2))])
+def test_shared_scan_batch_matches_oracle_per_query(db, nq, tune):
+    """Every query of a mixed-template batch run as ONE shared scan equals the
+    oracle run on that query alone (same words, same validity bits)."""
+    n = 700_001
+    ht = load(db, 30 + nq, n, queries.C4_COLS)
+    plans = queries.batch(nq, 1000 + nq, n)
+    t = None
+    if tune:
+        t = _lib.default_tuning()
+        t.block_threads, t.items_per_thread, t.stages = tune
+    assert all(db.shareable(p) for p in plans)
+    got = db.execute_shared(plans, t)
+    assert got[0].kernel_error == 0
+    for p, g in zip(plans, got):
+        ref = oracle_run(p, ht)
+        np.testing.assert_array_equal(g.words, ref.words)
+        np.testing.assert_array_equal(g.validity, ref.validity)
+
+
+def test_shared_scan_config2_and_repeat(db):
+    """The config-2 shape through the shared path, twice in a row (buffers and
+    dimension indexes are rebuilt per batch)."""
+    n = 500_003
+    ht = load(db, 41, n, queries.C2_COLS)
+    plans = [queries.config2(n, region=r, years=(1992 + r, 1997)) for r in range(5)]
+    for _ in range(2):
+        got = db.execute_shared(plans)
+        for p, g in zip(plans, got):
+            ref = oracle_run(p, ht)
+            np.testing.assert_array_equal(g.words, ref.words)
+            np.testing.assert_array_equal(g.validity, ref.validity)

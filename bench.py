@@ -344,7 +344,7 @@ def main():
     if shared is not None:
         pinned = [torch.empty(r.numel(), dtype=torch.int64, pin_memory=True) for r, _, _ in sbufs]
         pinned_v = [torch.empty(v.numel(), dtype=torch.int64, pin_memory=True) for _, v, _ in sbufs]
-        h2d = len(squeries) * 32 + len(sparams) * 4
+        h2d = len(squeries) * 40 + len(sparams) * 4
         d2h = sum(p.numel() * 8 + q.numel() * 8 for p, q in zip(pinned, pinned_v))
         torch.cuda.synchronize()
         t0 = time.perf_counter()

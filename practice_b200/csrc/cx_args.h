@@ -21,6 +21,8 @@ struct CxSQ {
   unsigned int* touched;    // per-group "row seen" bits (grouped shapes)
   int shape;
   int param_off;
+  int smem_acc;             // u64 offset of its group table in shared memory, -1 = global atomics
+  int smem_bits;            // u32 offset of its touched / seen bits in shared memory
 };
 
 struct CxArgs {
@@ -42,4 +44,6 @@ struct CxArgs {
   int sq_num[CX_MAX_SHAPES];                   // number of queries of each shape
   int sq_total;
   int nparams;
+  int smem_tab_words;                          // u64 words of per-query shared-memory group tables
+  int smem_bit_words;                          // u32 words of their touched / seen bits
 };

@@ -1139,8 +1139,14 @@ struct SharedGen {
     for (size_t s = 0; s < shapes.size(); ++s) {
       const Plan& p = *shapes[s];
       Emitter e(p, tu);
-      meta << "sshape " << s << " " << e.total_groups() << " " << p.storage_ts() << " " << (p.groups.empty() ? 0 : 1)
-           << " " << (p.sparse ? 1 : 0) << " " << lit_maps[s].size() << "\n";
+      const unsigned long long G = e.total_groups();
+      const int NA = (int)p.aggs.size();
+      int nseen = 0;
+      for (const auto& ag : p.aggs) nseen += (ag.fn == AggFn::Sum && !p.sparse);
+      const bool smem_ok = !p.groups.empty() && G * NA * 8 <= 4096ULL;
+      meta << "sshape " << s << " " << G << " " << p.storage_ts() << " " << (p.groups.empty() ? 0 : 1)
+           << " " << (p.sparse ? 1 : 0) << " " << lit_maps[s].size() << " " << (smem_ok ? 1 : 0) << " " << NA << " "
+           << (G + 31) / 32 << " " << nseen << "\n";
     }
     for (const Dim& d : dims) emit_index(d);
     emit_scan();
@@ -1171,8 +1177,10 @@ struct SharedGen {
     const unsigned long long par_off = off; off += (unsigned long long)MAXP * 4;
     off = (off + 15) & ~15ULL;
     const unsigned long long acc_off = off; off += (unsigned long long)MAXQ * NACC * 8;
+    off = (off + 15) & ~15ULL;
+    const unsigned long long tab_off = off;  // per-query group tables follow (sized per batch)
     const unsigned long long smem_total = (off + 127) & ~127ULL;
-    if (smem_total > 227 * 1024) throw PlanError("shared scan shared memory exceeds 227 KB");
+    if (smem_total > 200 * 1024) throw PlanError("shared scan shared memory exceeds 200 KB before group tables");
     const unsigned wait_limit = 1u << std::min(30, std::max(10, tu.wait_limit_log2));
     const std::string kname = "SharedScan_" + fact;
     meta << "kernel " << kname << " scan 0 " << CTA << " " << WT << " " << smem_total << " " << tu.ctas_per_sm << "\n";
@@ -1188,6 +1196,8 @@ struct SharedGen {
     o << "  unsigned long long* bars = (unsigned long long*)(cx_smem + " << bars_off << ") + warp * " << std::max(STAGES, 1) << "; (void)bars;\n";
     o << "  int* s_params = (int*)(cx_smem + " << par_off << ");\n";
     o << "  unsigned long long* s_qacc = (unsigned long long*)(cx_smem + " << acc_off << ");\n";
+    o << "  unsigned long long* s_tab = (unsigned long long*)(cx_smem + " << tab_off << "); (void)s_tab;\n";
+    o << "  unsigned int* s_bits = (unsigned int*)(s_tab + a.smem_tab_words); (void)s_bits;\n";
     o << "  const CxSQ* sq = a.sq;\n";
     o << "  const long long n_rows = a.rows[0];\n";
     o << "  const long long num_tiles = (n_rows + TILE_SIZE - 1) / TILE_SIZE;\n";
@@ -1196,6 +1206,8 @@ struct SharedGen {
     o << "  const long long nwarps = (long long)gridDim.x * NWARP;\n";
     o << "  for (int w = threadIdx.x; w < a.nparams && w < " << MAXP << "; w += " << CTA << ") s_params[w] = a.sparams[w];\n";
     o << "  for (int w = threadIdx.x; w < " << MAXQ * NACC << "; w += " << CTA << ") s_qacc[w] = 0ULL;\n";
+    o << "  for (int w = threadIdx.x; w < a.smem_tab_words; w += " << CTA << ") s_tab[w] = 0ULL;\n";
+    o << "  for (int w = threadIdx.x; w < a.smem_bit_words; w += " << CTA << ") s_bits[w] = 0u;\n";
     for (const auto& c : fact_cols) o << "  const int* __restrict__ d_" << c << " = a.col[" << slot_of(c, 0) << "];\n";
     for (const Dim& d : dims) o << "  const int4* __restrict__ dix_" << lower(d.name) << " = (const int4*)a.ht[" << d.slot << "];\n";
     if (STAGES > 0) {
@@ -1310,6 +1322,8 @@ struct SharedGen {
         o << ind << "unsigned long long* d_result = sq[q_].result;\n";
         o << ind << "uint64_t* d_result_validity = (uint64_t*)sq[q_].validity; (void)d_result_validity;\n";
         o << ind << "unsigned int* g_touch = sq[q_].touched;\n";
+        o << ind << "unsigned long long* qtab = sq[q_].smem_acc >= 0 ? s_tab + sq[q_].smem_acc : nullptr; (void)qtab;\n";
+        o << ind << "unsigned int* qbits = s_bits + (sq[q_].smem_acc >= 0 ? sq[q_].smem_bits : 0); (void)qbits;\n";
         o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
         o << ind << "  bool act = flags[i] && (tid + BLOCK_THREADS * i < num_tile_items);\n";
         o << ind << "  int hash = 0;\n";
@@ -1343,7 +1357,25 @@ struct SharedGen {
           if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "      v" << k << " = __ballot_sync(peers, v" << k << ") != 0u;\n";
         }
         o << ind << "    }\n";
+        const bool smem_ok = G * (unsigned long long)NA * 8 <= 4096ULL;
+        const unsigned long long TWq = (G + 31) / 32;
         o << ind << "    if (lane == leader) {\n";
+        if (smem_ok) {
+          // Block-private table in shared memory, flushed once per CTA.
+          o << ind << "      if (qtab) {\n";
+          o << ind << "        atomicOr(&qbits[hash >> 5], 1u << (hash & 31));\n";
+          int sk = 0;
+          for (int k = 0; k < NA; ++k) {
+            o << ind << "        if (x" << k << ") atomicAdd(&qtab[(long long)hash * " << NA << " + " << k << "], x" << k << ");\n";
+            if (!p.sparse && p.aggs[k].fn == AggFn::Sum) {
+              o << ind << "        if (v" << k << ") atomicOr(&qbits[" << TWq * (1 + sk) << "ULL + (hash >> 5)], 1u << (hash & 31));\n";
+              ++sk;
+            }
+          }
+          o << ind << "      } else {\n";
+        } else {
+          o << ind << "      {\n";
+        }
         o << ind << "      atomicOr(&g_touch[hash >> 5], 1u << (hash & 31));\n";
         for (int k = 0; k < NA; ++k) {
           const int slot = (int)p.groups.size() + k;
@@ -1354,6 +1386,7 @@ struct SharedGen {
             else o << ind << "      if (v" << k << ") db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
           }
         }
+        o << ind << "      }\n";
         o << ind << "    }\n";
         o << ind << "  }\n";
         o << ind << "}\n";
@@ -1387,6 +1420,48 @@ struct SharedGen {
         o << "        }\n";
       }
       o << "        break; }\n";
+    }
+    o << "      default: break;\n";
+    o << "    }\n";
+    o << "  }\n";
+    // Grouped queries with shared-memory tables: one flush per CTA.
+    o << "  for (int q = 0; q < a.sq_total; ++q) {\n";
+    o << "    const CxSQ Q = sq[q];\n";
+    o << "    if (Q.smem_acc < 0) continue;\n";
+    o << "    unsigned long long* d_result = Q.result; (void)d_result;\n";
+    o << "    uint64_t* d_result_validity = (uint64_t*)Q.validity; (void)d_result_validity;\n";
+    o << "    const unsigned long long* qtab = s_tab + Q.smem_acc;\n";
+    o << "    const unsigned int* qbits = s_bits + Q.smem_bits;\n";
+    o << "    switch (Q.shape) {\n";
+    for (size_t s2 = 0; s2 < shapes.size(); ++s2) {
+      const Plan& p = *shapes[s2];
+      if (p.groups.empty()) continue;
+      Emitter e(p, tu);
+      const unsigned long long G = e.total_groups();
+      const int NA = (int)p.aggs.size();
+      if (G * (unsigned long long)NA * 8 > 4096ULL) continue;
+      const unsigned long long TWq = (G + 31) / 32;
+      const int TS = p.storage_ts();
+      o << "      case " << s2 << ":\n";
+      o << "        for (long long g = threadIdx.x; g < " << G << "LL; g += " << CTA << ") {\n";
+      o << "          if (!((qbits[g >> 5] >> (g & 31)) & 1u)) continue;\n";
+      e.emit_key_store(o, "g", "          ");
+      int sk = 0;
+      for (int k = 0; k < NA; ++k) {
+        const int slot = (int)p.groups.size() + k;
+        const std::string ix = "(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
+        o << "          { const unsigned long long v_ = qtab[g * " << NA << " + " << k << "];\n";
+        o << "            if (v_) atomicAdd(&d_result[" << ix << "], v_);\n";
+        if (!p.sparse) {
+          if (p.aggs[k].fn == AggFn::Count) o << "            db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+          else {
+            o << "            if ((qbits[" << TWq * (1 + sk) << "ULL + (g >> 5)] >> (g & 31)) & 1u) db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+            ++sk;
+          }
+        }
+        o << "          }\n";
+      }
+      o << "        }\n        break;\n";
     }
     o << "      default: break;\n";
     o << "    }\n";

@@ -121,7 +121,7 @@ struct LaunchPlan {
   int fin_vts = 0;
   std::vector<KernelSpec> kernels;
   bool shared = false;
-  struct SShape { uint64_t groups; int ts, grouped, sparse, nlits; };
+  struct SShape { uint64_t groups; int ts, grouped, sparse, nlits, smem_ok, naggs; uint64_t tw; int nseen; };
   std::vector<SShape> sshapes;
 };
 
@@ -167,7 +167,7 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       lp.shared = true;
     } else if (k == "sshape") {
       int i; LaunchPlan::SShape sh;
-      ls >> i >> sh.groups >> sh.ts >> sh.grouped >> sh.sparse >> sh.nlits;
+      ls >> i >> sh.groups >> sh.ts >> sh.grouped >> sh.sparse >> sh.nlits >> sh.smem_ok >> sh.naggs >> sh.tw >> sh.nseen;
       if (i != (int)lp.sshapes.size()) { err = "shape lines out of order"; return false; }
       lp.sshapes.push_back(sh);
     } else if (k == "bm") {
@@ -302,7 +302,10 @@ int load_on_device(cx_module* m, int dev, cx_module::Loaded** out) {
     if (r != CUDA_SUCCESS) { d.ModuleUnload(L.mod); return drv_fail(r, k.name.c_str()); }
     int occ = 1;
     if (k.kind == "scan") {
-      if (k.smem > 48 * 1024) {
+      if (m->lp.shared) {
+        r = d.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, 227 * 1024);
+        if (r != CUDA_SUCCESS) { d.ModuleUnload(L.mod); return drv_fail(r, "cuFuncSetAttribute(smem)"); }
+      } else if (k.smem > 48 * 1024) {
         r = d.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)k.smem);
         if (r != CUDA_SUCCESS) { d.ModuleUnload(L.mod); return drv_fail(r, "cuFuncSetAttribute(smem)"); }
       }
@@ -841,6 +844,28 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
     hsq[i].param_off = q.param_off;
   }
   if (nparams) memcpy(hpar, params, (size_t)nparams * 4);
+  // Per-query shared-memory group tables, while they fit next to the kernel's
+  // fixed shared memory; the rest aggregate with global atomics.
+  size_t scan_ki = 0;
+  while (scan_ki < lp.kernels.size() && lp.kernels[scan_ki].kind != "scan") ++scan_ki;
+  const size_t base_smem = scan_ki < lp.kernels.size() ? lp.kernels[scan_ki].smem : 0;
+  uint64_t tab_words = 0, bit_words = 0;
+  for (int i = 0; i < nq; ++i) {
+    const auto& sh = lp.sshapes[hsq[i].shape];
+    hsq[i].smem_acc = -1;
+    hsq[i].smem_bits = 0;
+    if (!sh.smem_ok) continue;
+    const uint64_t tw = tab_words + sh.groups * (uint64_t)sh.naggs;
+    const uint64_t bw = bit_words + sh.tw * (uint64_t)(1 + sh.nseen);
+    if (base_smem + tw * 8 + bw * 4 + 64 > 200 * 1024) continue;
+    hsq[i].smem_acc = (int)tab_words;
+    hsq[i].smem_bits = (int)bit_words;
+    tab_words = tw;
+    bit_words = bw;
+  }
+  a.smem_tab_words = (int)tab_words;
+  a.smem_bit_words = (int)bit_words;
+  const size_t extra_smem = (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
 
   int sms = c->sm_override;
   if (sms <= 0) CX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -850,7 +875,8 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
   auto launch = [&](size_t ki, unsigned grid) -> int {
     const KernelSpec& k = lp.kernels[ki];
     if (grid == 0) return CX_OK;
-    CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, (unsigned)k.smem, (CUstream)stream, kparams, nullptr);
+    const unsigned smem = (unsigned)(k.smem + (ki == scan_ki ? extra_smem : 0));
+    CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, smem, (CUstream)stream, kparams, nullptr);
     if (r != CUDA_SUCCESS) return drv_fail(r, k.name.c_str());
     ++launches;
     return CX_OK;
@@ -878,7 +904,11 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
     const KernelSpec& k = lp.kernels[ki];
     const long long tiles = (rows[0] + k.tile - 1) / k.tile;
     const long long warps = std::max(1, k.block / 32);
-    const int per_sm = std::max(1, std::min(k.ctas_per_sm, L->occupancy[ki]));
+    int occ = 1;
+    CUresult orr = d.Occupancy(&occ, L->fns[ki], k.block, k.smem + extra_smem);
+    if (orr != CUDA_SUCCESS) return drv_fail(orr, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (occ < 1) return fail(CX_E_CAPACITY, "cx_shared_execute: shared scan cannot be resident with %zu bytes of shared memory", k.smem + extra_smem);
+    const int per_sm = std::max(1, std::min(k.ctas_per_sm, occ));
     const long long grid = std::min<long long>((tiles + warps - 1) / warps, (long long)sms * per_sm);
     scan_grid = (int)grid;
     if ((rc = launch(ki, (unsigned)grid))) return rc;

@@ -764,6 +764,20 @@ CX_DEVICE unsigned long long block_max_u64(unsigned long long v, unsigned long l
   return s;
 }
 
+// Bitwise OR of a 32-bit value over the CTA; the result is valid in thread 0.
+template <int BT>
+CX_DEVICE unsigned block_or_u32(unsigned v, unsigned long long* scratch) {
+  v = __reduce_or_sync(0xffffffffu, v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  unsigned s = 0u;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < BT / 32; ++w) s |= (unsigned)scratch[w];
+  return s;
+}
+
 // Warp-aggregated update of a group table.  Every lane of the warp must call
 // this (inactive lanes pass active=false).  Lanes that target the same group
 // are merged with __match_any_sync and a shuffle reduction; one lane per

@@ -462,9 +462,14 @@ struct Emitter {
       }
     }
     bool smem_groups = false;
+    // Tiny group domains accumulate in registers for the whole kernel and are
+    // reduced across the CTA once at the end (the reference's local group
+    // reduce for <= 64 groups, visitor.cpp:2901-2982, without per-tile atomics).
+    const bool reg_groups = grouped && G <= 32 && G * NACC <= 16 &&
+                            (tu.group_placement == 0 || tu.group_placement == 3);
     int REP = 1;
     unsigned long long acc_off = 0, touch_off = 0, seen_off = 0;
-    if (grouped) {
+    if (grouped && !reg_groups) {
       const unsigned long long one = G * NACC * 8 + TW * 4 * (1 + NSEEN_T);
       if (tu.group_placement == 1) smem_groups = true;
       else if (tu.group_placement == 2) smem_groups = false;
@@ -482,7 +487,7 @@ struct Emitter {
 
     const std::string kname = "Scan_" + fact;
     meta << "kernel " << kname << " scan 0 " << CTA << " " << WT << " " << smem_total << " " << tu.ctas_per_sm << "\n";
-    if (grouped && !smem_groups) meta << "touched " << TW << "\n";
+    if (grouped && !smem_groups && !reg_groups) meta << "touched " << TW << "\n";
 
     std::vector<std::string> reg_cols = fact_cols;
     for (const auto& c : payload_cols) reg_cols.push_back(c);
@@ -528,6 +533,15 @@ struct Emitter {
         if (seen_idx[k] >= 0) o << "  unsigned long long seen_" << k << " = 0ULL;\n";
         if (p.aggs[k].fn == AggFn::Avg) o << "  unsigned long long cnt_" << k << " = 0ULL;\n";
       }
+    } else if (reg_groups) {
+      o << "  unsigned long long racc[" << G * NACC << "];\n";
+      o << "  #pragma unroll\n  for (int r = 0; r < " << G * NACC << "; ++r) racc[r] = 0ULL;\n";
+      for (int k = 0; k < NA; ++k)
+        if (p.aggs[k].fn == AggFn::Min)
+          o << "  #pragma unroll\n  for (int g = 0; g < " << G << "; ++g) racc[g * " << NACC << " + " << k << "] = ~0ULL;\n";
+      o << "  unsigned rtouch = 0u;\n";
+      for (int k = 0; k < NA; ++k)
+        if (seen_idx[k] >= 0 && NSEEN_T > 0) o << "  unsigned rseen_" << k << " = 0u;\n";
     } else if (smem_groups) {
       o << "  unsigned long long* s_acc_all = (unsigned long long*)(cx_smem + " << acc_off << ");\n";
       o << "  unsigned int* s_touch_all = (unsigned int*)(cx_smem + " << touch_off << ");\n";
@@ -669,6 +683,39 @@ struct Emitter {
         }
       }
       o << ind << "  }\n" << ind << "}\n";
+    } else if (reg_groups) {
+      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+      std::string horner, dom;
+      for (size_t k = 0; k < p.groups.size(); ++k) {
+        o << ind << "    const int gt" << k << " = " << group_term(k) << ";\n";
+        horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(eff_card(k)) + " + gt" + std::to_string(k) + ")";
+        dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " +
+               std::to_string(eff_card(k)) + "u";
+      }
+      o << ind << "    const int hash = (" << horner << ") % " << G << ";\n";
+      o << ind << "    if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+      o << ind << "    if ((unsigned)hash < " << G << "u) {\n";
+      o << ind << "      rtouch |= 1u << hash;\n";
+      for (int k = 0; k < NA; ++k) {
+        const Agg& ag = p.aggs[k];
+        const std::string v = ag.arg->op == Op::Star ? "1" : valid_of(ag.arg.get());
+        const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + math_push(ag.arg.get(), true) + ")";
+        o << ind << "      if (" << v << ") {\n";
+        o << ind << "        const unsigned long long x_ = " << x << ";\n";
+        o << ind << "        #pragma unroll\n" << ind << "        for (int g = 0; g < " << G << "; ++g) if (hash == g) {\n";
+        const std::string r = "racc[g * " + std::to_string(NACC) + " + " + std::to_string(k) + "]";
+        if (ag.fn == AggFn::Min) o << ind << "          if (x_ < " << r << ") " << r << " = x_;\n";
+        else if (ag.fn == AggFn::Max) o << ind << "          if (x_ > " << r << ") " << r << " = x_;\n";
+        else o << ind << "          " << r << " += x_;\n";
+        if (ag.fn == AggFn::Avg) o << ind << "          racc[g * " << NACC << " + " << avg_idx[k] << "] += 1ULL;\n";
+        o << ind << "        }\n";
+        if (seen_idx[k] >= 0 && NSEEN_T > 0) o << ind << "        rseen_" << k << " |= 1u << hash;\n";
+        o << ind << "      }\n";
+      }
+      o << ind << "    }\n";
+      o << ind << "  }\n";
+      o << ind << "}\n";
     } else {
       o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
       o << ind << "  bool act = flags[i] && (tid + BLOCK_THREADS * i < num_tile_items);\n";
@@ -793,6 +840,43 @@ struct Emitter {
         }
         o << "  }\n";
       }
+    } else if (reg_groups) {
+      o << "  const unsigned touch_all = cx::block_or_u32<" << CTA << ">(rtouch, red);\n";
+      for (int k = 0; k < NA; ++k)
+        if (seen_idx[k] >= 0 && NSEEN_T > 0)
+          o << "  const unsigned seen_all_" << k << " = cx::block_or_u32<" << CTA << ">(rseen_" << k << ", red);\n";
+      o << "  #pragma unroll 1\n  for (int g = 0; g < " << G << "; ++g) {\n";
+      o << "    unsigned long long v_[" << NACC << "];\n";
+      o << "    #pragma unroll\n    for (int k = 0; k < " << NACC << "; ++k) {\n";
+      o << "      unsigned long long x_ = 0ULL;\n";
+      o << "      #pragma unroll\n      for (int h = 0; h < " << G << "; ++h) if (h == g) x_ = racc[h * " << NACC << " + k];\n";
+      o << "      v_[k] = x_;\n";
+      o << "    }\n";
+      for (int k = 0; k < NACC; ++k) {
+        const bool is_min = k < NA && p.aggs[k].fn == AggFn::Min;
+        const bool is_max = k < NA && p.aggs[k].fn == AggFn::Max;
+        if (is_min) o << "    v_[" << k << "] = cx::block_min_u64<" << CTA << ">(v_[" << k << "], red);\n";
+        else if (is_max) o << "    v_[" << k << "] = cx::block_max_u64<" << CTA << ">(v_[" << k << "], red);\n";
+        else o << "    v_[" << k << "] = cx::block_sum_u64<" << CTA << ">(v_[" << k << "], red);\n";
+      }
+      o << "    if (threadIdx.x == 0 && ((touch_all >> g) & 1u)) {\n";
+      emit_key_store(o, "g", "      ");
+      for (int k = 0; k < NA; ++k) {
+        const Agg& ag = p.aggs[k];
+        const int slot = (int)p.groups.size() + k;
+        const std::string ix = "(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
+        if (ag.fn == AggFn::Min) o << "      if (v_[" << k << "] != ~0ULL) atomicMin(&d_result[" << ix << "], v_[" << k << "]);\n";
+        else if (ag.fn == AggFn::Max) o << "      if (v_[" << k << "] != 0ULL) atomicMax(&d_result[" << ix << "], v_[" << k << "]);\n";
+        else o << "      if (v_[" << k << "] != 0ULL) atomicAdd(&d_result[" << ix << "], v_[" << k << "]);\n";
+        if (!p.sparse) {
+          if (ag.fn == AggFn::Count) o << "      db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+          if (seen_idx[k] >= 0) o << "      if ((seen_all_" << k << " >> g) & 1u) db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+        }
+        if (ag.fn == AggFn::Avg)
+          o << "      if (v_[" << avg_idx[k] << "] != 0ULL) atomicAdd(&d_result[(unsigned long long)g * " << TS << "ULL + " << p.hidden_count_slot(k) << "], v_[" << avg_idx[k] << "]);\n";
+      }
+      o << "    }\n";
+      o << "  }\n";
     } else if (smem_groups) {
       o << "  __syncthreads();\n";
       o << "  for (long long g = threadIdx.x; g < " << G << "LL; g += " << CTA << ") {\n";
@@ -835,7 +919,7 @@ struct Emitter {
     if (STAGES > 0) o << "#undef CX_ISSUE\n";
     o << "\n";
 
-    if (grouped && !smem_groups) {
+    if (grouped && !smem_groups && !reg_groups) {
       meta << "kernel group_keys_epilogue groups 0 256 0\n";
       o << "extern \"C\" __global__ void __launch_bounds__(256) group_keys_epilogue(const CxArgs a) {\n";
       o << "  unsigned long long* d_result = a.result;\n";
@@ -1324,6 +1408,79 @@ struct SharedGen {
         o << ind << "unsigned int* g_touch = sq[q_].touched;\n";
         o << ind << "unsigned long long* qtab = sq[q_].smem_acc >= 0 ? s_tab + sq[q_].smem_acc : nullptr; (void)qtab;\n";
         o << ind << "unsigned int* qbits = s_bits + (sq[q_].smem_acc >= 0 ? sq[q_].smem_bits : 0); (void)qbits;\n";
+        if (G <= 32 && G * (unsigned long long)NA <= 16) {
+          // Tiny group domain: per-thread partials in registers for this tile,
+          // then one warp reduction per touched group.
+          o << ind << "unsigned long long tacc[" << G * NA << "];\n";
+          o << ind << "#pragma unroll\n" << ind << "for (int r = 0; r < " << G * NA << "; ++r) tacc[r] = 0ULL;\n";
+          o << ind << "unsigned ttouch = 0u;\n";
+          std::vector<std::string> seen_names;
+          for (int k = 0; k < NA; ++k)
+            if (!p.sparse && p.aggs[k].fn == AggFn::Sum) {
+              o << ind << "unsigned tseen" << k << " = 0u;\n";
+              seen_names.push_back("tseen" + std::to_string(k));
+            }
+          o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+          o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+          std::string horner, dom;
+          for (size_t k = 0; k < p.groups.size(); ++k) {
+            o << ind << "    const int gt" << k << " = " << e.group_term(k) << ";\n";
+            horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(e.eff_card(k)) + " + gt" + std::to_string(k) + ")";
+            dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " + std::to_string(e.eff_card(k)) + "u";
+          }
+          o << ind << "    const int hash = (" << horner << ") % " << G << ";\n";
+          o << ind << "    if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+          o << ind << "    if ((unsigned)hash < " << G << "u) {\n";
+          o << ind << "      ttouch |= 1u << hash;\n";
+          for (int k = 0; k < NA; ++k) {
+            const Agg& ag = p.aggs[k];
+            const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
+            const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
+            o << ind << "      if (" << v << ") { const unsigned long long x_ = " << x << ";\n";
+            o << ind << "        #pragma unroll\n" << ind << "        for (int g = 0; g < " << G << "; ++g) if (hash == g) tacc[g * " << NA << " + " << k << "] += x_;\n";
+            if (!p.sparse && ag.fn == AggFn::Sum) o << ind << "        tseen" << k << " |= 1u << hash;\n";
+            o << ind << "      }\n";
+          }
+          o << ind << "    }\n";
+          o << ind << "  }\n";
+          o << ind << "}\n";
+          o << ind << "ttouch = __reduce_or_sync(0xffffffffu, ttouch);\n";
+          for (const auto& sn : seen_names) o << ind << sn << " = __reduce_or_sync(0xffffffffu, " << sn << ");\n";
+          o << ind << "if (ttouch) {\n";
+          o << ind << "  #pragma unroll\n" << ind << "  for (int g = 0; g < " << G << "; ++g) {\n";
+          o << ind << "    if (!((ttouch >> g) & 1u)) continue;\n";
+          for (int k = 0; k < NA; ++k) {
+            o << ind << "    { unsigned long long s_ = tacc[g * " << NA << " + " << k << "];\n";
+            o << ind << "      for (int o_ = 16; o_ > 0; o_ >>= 1) s_ += __shfl_xor_sync(0xffffffffu, s_, o_);\n";
+            o << ind << "      if (lane == 0) {\n";
+            o << ind << "        if (qtab) { if (s_) atomicAdd(&qtab[g * " << NA << " + " << k << "], s_); }\n";
+            const int slot = (int)p.groups.size() + k;
+            o << ind << "        else if (s_) atomicAdd(&d_result[(unsigned long long)g * " << TS << "ULL + " << slot << "], s_);\n";
+            if (!p.sparse) {
+              const std::string ix = "(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
+              if (p.aggs[k].fn == AggFn::Count) o << ind << "        if (!qtab) db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+              else o << ind << "        if (!qtab && ((tseen" << k << " >> g) & 1u)) db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+            }
+            o << ind << "      }\n";
+            o << ind << "    }\n";
+          }
+          o << ind << "    if (lane == 0) {\n";
+          o << ind << "      if (qtab) atomicOr(&qbits[g >> 5], 1u << (g & 31));\n";
+          o << ind << "      else atomicOr(&g_touch[g >> 5], 1u << (g & 31));\n";
+          {
+            int sk = 0;
+            for (int k = 0; k < NA; ++k)
+              if (!p.sparse && p.aggs[k].fn == AggFn::Sum) {
+                o << ind << "      if (qtab && ((tseen" << k << " >> g) & 1u)) atomicOr(&qbits[" << (G + 31) / 32 * (1 + sk) << " + (g >> 5)], 1u << (g & 31));\n";
+                ++sk;
+              }
+          }
+          o << ind << "    }\n";
+          o << ind << "  }\n";
+          o << ind << "}\n";
+          o << "    }\n";
+          continue;
+        }
         o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
         o << ind << "  bool act = flags[i] && (tid + BLOCK_THREADS * i < num_tile_items);\n";
         o << ind << "  int hash = 0;\n";

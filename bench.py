@@ -204,8 +204,8 @@ def config_block(args):
 PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=98304)
                     for bt, ipt, st in ((1024, 2, 0), (1024, 4, 0), (512, 2, 0), (512, 8, 2), (1024, 4, 2))]
 SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16)
-                     for bt, ipt, st in ((256, 2, 0), (512, 2, 0), (1024, 2, 0), (512, 4, 0), (256, 2, 2),
-                                         (512, 2, 2), (256, 4, 2))]
+                     for bt, ipt, st in ((512, 2, 2), (256, 4, 2), (1024, 1, 2), (512, 4, 2), (1024, 2, 2),
+                                         (256, 8, 2), (512, 2, 3))]
 
 
 def time_steps(torch, stream, steps, run_step, sampler=None):

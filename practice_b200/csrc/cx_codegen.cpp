@@ -1247,319 +1247,284 @@ struct SharedGen {
     return out.str();
   }
 
+  // CTA-tiled, query-parallel shared scan.  Per tile of TR = block x items
+  // rows: thread 0 stages the union of fact columns by TMA bulk copies; all
+  // threads gather every joined dimension once into shared-memory attribute
+  // arrays and a per-row hit mask; then each warp takes (query, row-slice)
+  // units and evaluates its query row by row from shared memory, with
+  // per-lane partial aggregates reduced once per unit.
   void emit_scan() {
     const int CTA = tu.block_threads, IPT = tu.items_per_thread;
-    if (CTA % 32 || CTA < 32 || CTA > 1024 || IPT < 1 || IPT > 16) throw PlanError("bad block shape");
-    const int NW = CTA / 32, WT = 32 * IPT;
+    if (CTA % 32 || CTA < 64 || CTA > 1024 || IPT < 1 || IPT > 16) throw PlanError("bad block shape");
+    const int NW = CTA / 32, TR = CTA * IPT;
     const int NSC = (int)fact_cols.size();
-    const int STAGES = NSC == 0 ? 0 : std::max(0, tu.stages);
+    const int STAGES = std::max(1, tu.stages);
     const int MAXQ = 256, MAXP = 4096;
     const int NACC = std::max(1, max_scalar_aggs) * 2;  // (sum, count) per scalar aggregate
-    const unsigned long long warp_stage_ints = (unsigned long long)STAGES * NSC * WT;
-    unsigned long long off = (unsigned long long)NW * warp_stage_ints * 4;
-    const unsigned long long bars_off = off; off += (unsigned long long)NW * std::max(STAGES, 1) * 8;
+    int nattr = 0;
+    std::map<std::string, int> attr_slot;
+    for (const Dim& d : dims)
+      for (const auto& at : d.attrs) attr_slot[at] = nattr++;
+    unsigned long long off = 0;
+    const unsigned long long stage_off = off; off += (unsigned long long)STAGES * NSC * TR * 4;
+    const unsigned long long attr_off = off; off += (unsigned long long)nattr * TR * 4;
+    const unsigned long long hm_off = off; off += (unsigned long long)TR;
+    off = (off + 15) & ~15ULL;
+    const unsigned long long bars_off = off; off += (unsigned long long)STAGES * 8;
     const unsigned long long par_off = off; off += (unsigned long long)MAXP * 4;
     off = (off + 15) & ~15ULL;
     const unsigned long long acc_off = off; off += (unsigned long long)MAXQ * NACC * 8;
     off = (off + 15) & ~15ULL;
-    const unsigned long long tab_off = off;  // per-query group tables follow (sized per batch)
+    const unsigned long long tab_off = off;
     const unsigned long long smem_total = (off + 127) & ~127ULL;
     if (smem_total > 200 * 1024) throw PlanError("shared scan shared memory exceeds 200 KB before group tables");
     const unsigned wait_limit = 1u << std::min(30, std::max(10, tu.wait_limit_log2));
     const std::string kname = "SharedScan_" + fact;
-    meta << "kernel " << kname << " scan 0 " << CTA << " " << WT << " " << smem_total << " " << tu.ctas_per_sm << "\n";
+    meta << "kernel " << kname << " sharedscan 0 " << CTA << " " << TR << " " << smem_total << " " << tu.ctas_per_sm << "\n";
 
     std::ostringstream& o = src;
     o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ") " << kname << "(const CxArgs a) {\n";
-    o << "  constexpr int BLOCK_THREADS = 32, ITEMS_PER_THREAD = " << IPT << ", TILE_SIZE = " << WT << ";\n";
-    o << "  constexpr int NWARP = " << NW << ", NSTAGE = " << STAGES << ", NSC = " << NSC << ";\n";
+    o << "  constexpr int TR = " << TR << ", NSTAGE = " << STAGES << ", NSC = " << NSC << ", NWARP = " << NW << ";\n";
     o << "  extern __shared__ __align__(1024) unsigned char cx_smem[];\n";
     o << "  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
-    o << "  const int tid = lane;\n";
-    o << "  int* stage_buf = (int*)cx_smem + (long long)warp * " << warp_stage_ints << "LL; (void)stage_buf;\n";
-    o << "  unsigned long long* bars = (unsigned long long*)(cx_smem + " << bars_off << ") + warp * " << std::max(STAGES, 1) << "; (void)bars;\n";
+    o << "  int* stage_buf = (int*)(cx_smem + " << stage_off << ");\n";
+    o << "  int* s_attr = (int*)(cx_smem + " << attr_off << "); (void)s_attr;\n";
+    o << "  unsigned char* s_hm = (unsigned char*)(cx_smem + " << hm_off << "); (void)s_hm;\n";
+    o << "  unsigned long long* bars = (unsigned long long*)(cx_smem + " << bars_off << ");\n";
     o << "  int* s_params = (int*)(cx_smem + " << par_off << ");\n";
     o << "  unsigned long long* s_qacc = (unsigned long long*)(cx_smem + " << acc_off << ");\n";
     o << "  unsigned long long* s_tab = (unsigned long long*)(cx_smem + " << tab_off << "); (void)s_tab;\n";
     o << "  unsigned int* s_bits = (unsigned int*)(s_tab + a.smem_tab_words); (void)s_bits;\n";
     o << "  const CxSQ* sq = a.sq;\n";
     o << "  const long long n_rows = a.rows[0];\n";
-    o << "  const long long num_tiles = (n_rows + TILE_SIZE - 1) / TILE_SIZE;\n";
-    o << "  const long long full_tiles = n_rows / TILE_SIZE;\n";
-    o << "  const long long gwarp = (long long)blockIdx.x * NWARP + warp;\n";
-    o << "  const long long nwarps = (long long)gridDim.x * NWARP;\n";
+    o << "  const long long num_tiles = (n_rows + TR - 1) / TR;\n";
+    o << "  const long long full_tiles = n_rows / TR;\n";
     o << "  for (int w = threadIdx.x; w < a.nparams && w < " << MAXP << "; w += " << CTA << ") s_params[w] = a.sparams[w];\n";
     o << "  for (int w = threadIdx.x; w < " << MAXQ * NACC << "; w += " << CTA << ") s_qacc[w] = 0ULL;\n";
     o << "  for (int w = threadIdx.x; w < a.smem_tab_words; w += " << CTA << ") s_tab[w] = 0ULL;\n";
     o << "  for (int w = threadIdx.x; w < a.smem_bit_words; w += " << CTA << ") s_bits[w] = 0u;\n";
     for (const auto& c : fact_cols) o << "  const int* __restrict__ d_" << c << " = a.col[" << slot_of(c, 0) << "];\n";
     for (const Dim& d : dims) o << "  const int4* __restrict__ dix_" << lower(d.name) << " = (const int4*)a.ht[" << d.slot << "];\n";
-    if (STAGES > 0) {
-      o << "  bool staged_ok = true;\n";
-      for (const auto& c : fact_cols) o << "  staged_ok = staged_ok && ((((unsigned long long)d_" << c << ") & 15ULL) == 0ULL);\n";
-      o << "  unsigned long long l2_policy = 0;\n";
-      o << "  if (lane == 0) {\n";
-      o << "    for (int s = 0; s < NSTAGE; ++s) cx::mbar_init(&bars[s], 1);\n";
-      o << "    cx::fence_mbar_init();\n";
-      o << "    l2_policy = cx::l2_evict_first_policy();\n";
-      o << "  }\n";
-      o << "#define CX_ISSUE(TILE_, STAGE_) do { \\\n";
-      o << "    cx::mbar_expect_tx(&bars[(STAGE_)], " << (unsigned long long)NSC * WT * 4 << "u); \\\n";
-      for (int c = 0; c < NSC; ++c)
-        o << "    cx::bulk_g2s(stage_buf + ((STAGE_) * NSC + " << c << ") * TILE_SIZE, d_" << fact_cols[c]
-          << " + (TILE_) * TILE_SIZE, " << WT * 4 << "u, &bars[(STAGE_)], l2_policy); \\\n";
-      o << "  } while (0)\n";
-    }
+    o << "  bool staged_ok = true;\n";
+    for (const auto& c : fact_cols) o << "  staged_ok = staged_ok && ((((unsigned long long)d_" << c << ") & 15ULL) == 0ULL);\n";
+    o << "  unsigned long long l2_policy = 0;\n";
+    o << "  if (threadIdx.x == 0) {\n";
+    o << "    for (int s = 0; s < NSTAGE; ++s) cx::mbar_init(&bars[s], 1);\n";
+    o << "    cx::fence_mbar_init();\n";
+    o << "    l2_policy = cx::l2_evict_first_policy();\n";
+    o << "  }\n";
+    o << "#define CX_ISSUE(TILE_, STAGE_) do { \\\n";
+    o << "    cx::mbar_expect_tx(&bars[(STAGE_)], " << (unsigned long long)NSC * TR * 4 << "u); \\\n";
+    for (int c = 0; c < NSC; ++c)
+      o << "    cx::bulk_g2s(stage_buf + ((STAGE_) * NSC + " << c << ") * TR, d_" << fact_cols[c] << " + (TILE_) * TR, "
+        << TR * 4 << "u, &bars[(STAGE_)], l2_policy); \\\n";
+    o << "  } while (0)\n";
     o << "  __syncthreads();\n";
-    if (STAGES > 0) {
-      o << "  if (lane == 0 && staged_ok) {\n";
-      o << "    for (int k = 0; k < NSTAGE; ++k) {\n";
-      o << "      const long long t = gwarp + (long long)k * nwarps;\n";
-      o << "      if (t < full_tiles) CX_ISSUE(t, k);\n";
-      o << "    }\n";
-      o << "  }\n";
-    }
+    o << "  if (threadIdx.x == 0 && staged_ok)\n";
+    o << "    for (int k = 0; k < NSTAGE; ++k) {\n";
+    o << "      const long long t = (long long)blockIdx.x + (long long)k * gridDim.x;\n";
+    o << "      if (t < full_tiles) CX_ISSUE(t, k);\n";
+    o << "    }\n";
+    // Units of work per tile: (query, row slice); enough slices to occupy every warp.
+    o << "  const int nq = a.sq_total;\n";
+    o << "  const int slices = nq > 0 ? (NWARP + nq - 1) / nq : 1;\n";
+    o << "  const int units = nq * slices;\n";
     o << "  long long k_iter = 0;\n";
-    o << "  bool aborted = false; (void)aborted;\n";
-    o << "  for (long long t = gwarp; t < num_tiles; t += nwarps, ++k_iter) {\n";
-    o << "    const long long tile_offset = t * TILE_SIZE;\n";
-    o << "    const int num_tile_items = (int)(n_rows - tile_offset < TILE_SIZE ? n_rows - tile_offset : TILE_SIZE);\n";
-    if (STAGES > 0) {
-      o << "    const int stage = (int)(k_iter % NSTAGE);\n";
-      o << "    const bool staged = staged_ok && t < full_tiles;\n";
-      o << "    bool timed_out = false;\n";
-      o << "    if (staged) timed_out = !cx::mbar_wait_bounded(&bars[stage], (unsigned)((k_iter / NSTAGE) & 1), " << wait_limit << "u);\n";
-      o << "    if (__any_sync(0xffffffffu, timed_out)) { if (lane == 0) cx::raise(a.err, cx::ERR_WAIT_TIMEOUT); aborted = true; break; }\n";
-      for (int c = 0; c < NSC; ++c)
-        o << "    const int* t_" << fact_cols[c] << " = staged ? stage_buf + (stage * NSC + " << c << ") * TILE_SIZE : d_"
-          << fact_cols[c] << " + tile_offset;\n";
-    } else {
-      for (int c = 0; c < NSC; ++c) o << "    const int* t_" << fact_cols[c] << " = d_" << fact_cols[c] << " + tile_offset;\n";
-    }
-    // Union columns into registers, once per tile for every query.
-    for (const auto& c : fact_cols) {
-      o << "    int " << c << "[ITEMS_PER_THREAD];\n";
-      o << "    BlockLoad<int, BLOCK_THREADS, ITEMS_PER_THREAD>(t_" << c << ", tid, tile_offset, " << c << ", num_tile_items);\n";
-    }
-    // One gather per dimension, shared by every query.
+    o << "  bool aborted = false;\n";
+    o << "  for (long long t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k_iter) {\n";
+    o << "    const long long tile_offset = t * TR;\n";
+    o << "    const int n_tile = (int)(n_rows - tile_offset < TR ? n_rows - tile_offset : TR);\n";
+    o << "    const int stage = (int)(k_iter % NSTAGE);\n";
+    o << "    const bool staged = staged_ok && t < full_tiles;\n";
+    o << "    bool timed_out = false;\n";
+    o << "    if (staged) timed_out = !cx::mbar_wait_bounded(&bars[stage], (unsigned)((k_iter / NSTAGE) & 1), " << wait_limit << "u);\n";
+    o << "    if (__syncthreads_or(timed_out)) { if (threadIdx.x == 0) cx::raise(a.err, cx::ERR_WAIT_TIMEOUT); aborted = true; break; }\n";
+    o << "    int* tile = stage_buf + stage * NSC * TR;\n";
+    o << "    if (!staged) {\n";  // ragged last tile (or unaligned columns): plain loads into the stage
+    for (int c = 0; c < NSC; ++c)
+      o << "      for (int r = threadIdx.x; r < n_tile; r += " << CTA << ") tile[" << c << " * TR + r] = d_" << fact_cols[c] << "[tile_offset + r];\n";
+    o << "      __syncthreads();\n";
+    o << "    }\n";
+    for (int c = 0; c < NSC; ++c) o << "    const int* " << fact_cols[c] << " = tile + " << c << " * TR;\n";
+    for (const Dim& d : dims)
+      for (const auto& at : d.attrs) o << "    int* " << at << " = s_attr + " << attr_slot[at] << " * TR;\n";
+    // Gather every dimension once per row.
+    o << "    for (int i = threadIdx.x; i < n_tile; i += " << CTA << ") {\n";
+    o << "      unsigned hm_ = 0u;\n";
     const char* comp[] = {"y", "z", "w"};
-    for (const Dim& d : dims) {
-      o << "    int " << d.pk << "[ITEMS_PER_THREAD];\n";
-      for (const auto& at : d.attrs) o << "    int " << at << "[ITEMS_PER_THREAD];\n";
-      o << "    #pragma unroll\n    for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      o << "      int4 g_ = make_int4(0, 0, 0, 0);\n";
-      o << "      if (tid + BLOCK_THREADS * i < num_tile_items) {\n";
-      o << "        const int h_ = (int)HASH(" << d.fk << "[i], " << d.len << ", " << d.keymin << ");\n";
+    for (size_t di = 0; di < dims.size(); ++di) {
+      const Dim& d = dims[di];
+      o << "      {\n";
+      o << "        const int fk_ = " << d.fk << "[i];\n";
+      o << "        const int h_ = (int)HASH(fk_, " << d.len << ", " << d.keymin << ");\n";
+      o << "        int4 g_ = make_int4(0, 0, 0, 0);\n";
       o << "        if ((unsigned)h_ < " << d.len << "u) g_ = __ldg(&dix_" << lower(d.name) << "[h_]);\n";
+      o << "        if (g_.x != 0 && g_.x == fk_) hm_ |= " << (1u << di) << "u;\n";
+      for (size_t k = 0; k < d.attrs.size(); ++k) o << "        " << d.attrs[k] << "[i] = g_." << comp[k] << ";\n";
       o << "      }\n";
-      o << "      " << d.pk << "[i] = g_.x;\n";
-      for (size_t k = 0; k < d.attrs.size(); ++k) o << "      " << d.attrs[k] << "[i] = g_." << comp[k] << ";\n";
-      o << "    }\n";
     }
-    // Every query of every shape.
+    o << "      s_hm[i] = (unsigned char)hm_;\n";
+    o << "    }\n";
+    o << "    __syncthreads();\n";
+    // Query units.
+    o << "    for (int u = warp; u < units; u += NWARP) {\n";
+    o << "      const int q_ = u / slices, sl_ = u - q_ * slices;\n";
+    o << "      const int per_ = (n_tile + slices - 1) / slices;\n";
+    o << "      const int lo_ = sl_ * per_, hi_ = lo_ + per_ < n_tile ? lo_ + per_ : n_tile;\n";
+    o << "      const CxSQ Q = sq[q_];\n";
+    o << "      const int* P = s_params + Q.param_off; (void)P;\n";
+    o << "      switch (Q.shape) {\n";
     for (size_t s = 0; s < shapes.size(); ++s) {
       const Plan& p = *shapes[s];
       Emitter e(p, tu);
       e.lit_index = &lit_maps[s];
-      for (const auto& c : fact_cols) e.loaded.insert(c);
-      for (const Dim& d : dims) {
-        e.loaded.insert(d.pk);
-        for (const auto& at : d.attrs) e.loaded.insert(at);
-      }
-      const std::string ind = "      ";
-      o << "    for (int j_ = 0; j_ < a.sq_num[" << s << "]; ++j_) {\n";
-      o << "      const int q_ = a.sq_first[" << s << "] + j_;\n";
-      o << "      const int* P = s_params + sq[q_].param_off; (void)P;\n";
-      o << "      int flags[ITEMS_PER_THREAD];\n";
-      o << "      InitFlags<BLOCK_THREADS, ITEMS_PER_THREAD>(flags);\n";
+      const std::string ind = "          ";
+      o << "      case " << s << ": {\n";
+      // Row predicate of the shape (filters and dimension joins), in plan order.
+      std::vector<std::string> conds;
       for (const auto& st : p.steps) {
         if (st.kind == Step::Filter) {
-          e.emit_filter(o, st.filter.get(), ind);
+          conds.push_back(and_terms({e.valid_of(st.filter.get()), e.value_of(st.filter.get())}));
           continue;
         }
         const Join& j = st.join;
-        std::string cond = j.filter ? and_terms({e.valid_of(j.filter.get()), e.value_of(j.filter.get())}) : "1";
-        o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-        o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
-        o << ind << "    bool ok_ = " << j.pk << "[i] != 0 && " << j.pk << "[i] == " << j.fks[0] << "[i];\n";
-        if (!lit_true(cond)) o << ind << "    if (ok_) ok_ = (" << cond << ");\n";
-        o << ind << "    flags[i] = ok_ ? 1 : 0;\n";
-        o << ind << "  }\n" << ind << "}\n";
+        size_t di = 0;
+        for (; di < dims.size(); ++di) if (dims[di].name == j.dim) break;
+        std::string c = "((s_hm[i] >> " + std::to_string(di) + ") & 1u)";
+        if (j.filter) c += " && (" + and_terms({e.valid_of(j.filter.get()), e.value_of(j.filter.get())}) + ")";
+        conds.push_back(c);
       }
+      std::string pred;
+      for (const auto& c : conds) pred += (pred.empty() ? "" : " && ") + std::string("(") + c + ")";
+      if (pred.empty()) pred = "true";
       const int NA = (int)p.aggs.size();
+      const int TS = p.storage_ts();
       if (p.groups.empty()) {
+        for (int k = 0; k < NA; ++k) o << ind << "unsigned long long s" << k << "_ = 0ULL, c" << k << "_ = 0ULL;\n";
+        o << ind << "for (int i = lo_ + lane; i < hi_; i += 32) {\n";
+        o << ind << "  if (!(" << pred << ")) continue;\n";
         for (int k = 0; k < NA; ++k) {
           const Agg& ag = p.aggs[k];
           const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
           const std::string x = ag.fn == AggFn::Count ? "1ULL" : e.math_push(ag.arg.get(), true);
-          o << ind << "{ unsigned long long s_ = 0ULL, c_ = 0ULL;\n";
-          o << ind << "  #pragma unroll\n" << ind << "  for (int i = 0; i < ITEMS_PER_THREAD; ++i)\n";
-          o << ind << "    if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items) && (" << v << ")) { s_ += " << x << "; c_ += 1ULL; }\n";
-          o << ind << "  if (__any_sync(0xffffffffu, c_ != 0ULL)) {\n";
-          o << ind << "    for (int o_ = 16; o_ > 0; o_ >>= 1) { s_ += __shfl_xor_sync(0xffffffffu, s_, o_); c_ += __shfl_xor_sync(0xffffffffu, c_, o_); }\n";
-          o << ind << "    if (lane == 0) { atomicAdd(&s_qacc[(long long)q_ * " << NACC << " + " << 2 * k << "], s_); atomicAdd(&s_qacc[(long long)q_ * " << NACC << " + " << 2 * k + 1 << "], c_); }\n";
-          o << ind << "  }\n" << ind << "}\n";
+          o << ind << "  if (" << v << ") { s" << k << "_ += " << x << "; c" << k << "_ += 1ULL; }\n";
+        }
+        o << ind << "}\n";
+        for (int k = 0; k < NA; ++k) {
+          o << ind << "if (__any_sync(0xffffffffu, c" << k << "_ != 0ULL)) {\n";
+          o << ind << "  for (int o_ = 16; o_ > 0; o_ >>= 1) { s" << k << "_ += __shfl_xor_sync(0xffffffffu, s" << k << "_, o_); c" << k << "_ += __shfl_xor_sync(0xffffffffu, c" << k << "_, o_); }\n";
+          o << ind << "  if (lane == 0) { atomicAdd(&s_qacc[(long long)q_ * " << NACC << " + " << 2 * k << "], s" << k << "_); atomicAdd(&s_qacc[(long long)q_ * " << NACC << " + " << 2 * k + 1 << "], c" << k << "_); }\n";
+          o << ind << "}\n";
         }
       } else {
         const unsigned long long G = e.total_groups();
-        const int TS = p.storage_ts();
-        o << ind << "unsigned long long* d_result = sq[q_].result;\n";
-        o << ind << "uint64_t* d_result_validity = (uint64_t*)sq[q_].validity; (void)d_result_validity;\n";
-        o << ind << "unsigned int* g_touch = sq[q_].touched;\n";
-        o << ind << "unsigned long long* qtab = sq[q_].smem_acc >= 0 ? s_tab + sq[q_].smem_acc : nullptr; (void)qtab;\n";
-        o << ind << "unsigned int* qbits = s_bits + (sq[q_].smem_acc >= 0 ? sq[q_].smem_bits : 0); (void)qbits;\n";
-        if (G <= 32 && G * (unsigned long long)NA <= 16) {
-          // Tiny group domain: per-thread partials in registers for this tile,
-          // then one warp reduction per touched group.
+        const unsigned long long TWq = (G + 31) / 32;
+        std::string horner, dom;
+        std::ostringstream terms;
+        for (size_t k = 0; k < p.groups.size(); ++k) {
+          terms << ind << "  const int gt" << k << " = " << e.group_term(k) << ";\n";
+          horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(e.eff_card(k)) + " + gt" + std::to_string(k) + ")";
+          dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " + std::to_string(e.eff_card(k)) + "u";
+        }
+        o << ind << "unsigned long long* d_result = Q.result; (void)d_result;\n";
+        o << ind << "uint64_t* d_result_validity = (uint64_t*)Q.validity; (void)d_result_validity;\n";
+        o << ind << "unsigned int* g_touch = Q.touched; (void)g_touch;\n";
+        o << ind << "unsigned long long* qtab = Q.smem_acc >= 0 ? s_tab + Q.smem_acc : nullptr; (void)qtab;\n";
+        o << ind << "unsigned int* qbits = s_bits + (Q.smem_acc >= 0 ? Q.smem_bits : 0); (void)qbits;\n";
+        const bool tiny = G <= 32 && G * (unsigned long long)NA <= 16;
+        if (tiny) {
           o << ind << "unsigned long long tacc[" << G * NA << "];\n";
           o << ind << "#pragma unroll\n" << ind << "for (int r = 0; r < " << G * NA << "; ++r) tacc[r] = 0ULL;\n";
           o << ind << "unsigned ttouch = 0u;\n";
-          std::vector<std::string> seen_names;
           for (int k = 0; k < NA; ++k)
-            if (!p.sparse && p.aggs[k].fn == AggFn::Sum) {
-              o << ind << "unsigned tseen" << k << " = 0u;\n";
-              seen_names.push_back("tseen" + std::to_string(k));
-            }
-          o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-          o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
-          std::string horner, dom;
-          for (size_t k = 0; k < p.groups.size(); ++k) {
-            o << ind << "    const int gt" << k << " = " << e.group_term(k) << ";\n";
-            horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(e.eff_card(k)) + " + gt" + std::to_string(k) + ")";
-            dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " + std::to_string(e.eff_card(k)) + "u";
-          }
-          o << ind << "    const int hash = (" << horner << ") % " << G << ";\n";
-          o << ind << "    if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
-          o << ind << "    if ((unsigned)hash < " << G << "u) {\n";
-          o << ind << "      ttouch |= 1u << hash;\n";
+            if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "unsigned tseen" << k << " = 0u;\n";
+        }
+        o << ind << "for (int i = lo_ + lane; i < hi_; i += 32) {\n";
+        o << ind << "  if (!(" << pred << ")) continue;\n";
+        o << terms.str();
+        o << ind << "  const int hash = (" << horner << ") % " << G << ";\n";
+        o << ind << "  if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+        o << ind << "  if ((unsigned)hash >= " << G << "u) continue;\n";
+        if (tiny) {
+          o << ind << "  ttouch |= 1u << hash;\n";
           for (int k = 0; k < NA; ++k) {
             const Agg& ag = p.aggs[k];
             const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
             const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
-            o << ind << "      if (" << v << ") { const unsigned long long x_ = " << x << ";\n";
-            o << ind << "        #pragma unroll\n" << ind << "        for (int g = 0; g < " << G << "; ++g) if (hash == g) tacc[g * " << NA << " + " << k << "] += x_;\n";
-            if (!p.sparse && ag.fn == AggFn::Sum) o << ind << "        tseen" << k << " |= 1u << hash;\n";
-            o << ind << "      }\n";
+            o << ind << "  if (" << v << ") { const unsigned long long x_ = " << x << ";\n";
+            o << ind << "    #pragma unroll\n" << ind << "    for (int g = 0; g < " << G << "; ++g) if (hash == g) tacc[g * " << NA << " + " << k << "] += x_;\n";
+            if (!p.sparse && ag.fn == AggFn::Sum) o << ind << "    tseen" << k << " |= 1u << hash;\n";
+            o << ind << "  }\n";
           }
-          o << ind << "    }\n";
-          o << ind << "  }\n";
           o << ind << "}\n";
           o << ind << "ttouch = __reduce_or_sync(0xffffffffu, ttouch);\n";
-          for (const auto& sn : seen_names) o << ind << sn << " = __reduce_or_sync(0xffffffffu, " << sn << ");\n";
-          o << ind << "if (ttouch) {\n";
-          o << ind << "  #pragma unroll\n" << ind << "  for (int g = 0; g < " << G << "; ++g) {\n";
-          o << ind << "    if (!((ttouch >> g) & 1u)) continue;\n";
-          for (int k = 0; k < NA; ++k) {
-            o << ind << "    { unsigned long long s_ = tacc[g * " << NA << " + " << k << "];\n";
-            o << ind << "      for (int o_ = 16; o_ > 0; o_ >>= 1) s_ += __shfl_xor_sync(0xffffffffu, s_, o_);\n";
-            o << ind << "      if (lane == 0) {\n";
-            o << ind << "        if (qtab) { if (s_) atomicAdd(&qtab[g * " << NA << " + " << k << "], s_); }\n";
-            const int slot = (int)p.groups.size() + k;
-            o << ind << "        else if (s_) atomicAdd(&d_result[(unsigned long long)g * " << TS << "ULL + " << slot << "], s_);\n";
-            if (!p.sparse) {
-              const std::string ix = "(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
-              if (p.aggs[k].fn == AggFn::Count) o << ind << "        if (!qtab) db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
-              else o << ind << "        if (!qtab && ((tseen" << k << " >> g) & 1u)) db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
-            }
-            o << ind << "      }\n";
-            o << ind << "    }\n";
-          }
-          o << ind << "    if (lane == 0) {\n";
-          o << ind << "      if (qtab) atomicOr(&qbits[g >> 5], 1u << (g & 31));\n";
-          o << ind << "      else atomicOr(&g_touch[g >> 5], 1u << (g & 31));\n";
-          {
-            int sk = 0;
-            for (int k = 0; k < NA; ++k)
-              if (!p.sparse && p.aggs[k].fn == AggFn::Sum) {
-                o << ind << "      if (qtab && ((tseen" << k << " >> g) & 1u)) atomicOr(&qbits[" << (G + 31) / 32 * (1 + sk) << " + (g >> 5)], 1u << (g & 31));\n";
-                ++sk;
-              }
-          }
-          o << ind << "    }\n";
-          o << ind << "  }\n";
-          o << ind << "}\n";
-          o << "    }\n";
-          continue;
-        }
-        o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-        o << ind << "  bool act = flags[i] && (tid + BLOCK_THREADS * i < num_tile_items);\n";
-        o << ind << "  int hash = 0;\n";
-        o << ind << "  if (act) {\n";
-        std::string horner, dom;
-        for (size_t k = 0; k < p.groups.size(); ++k) {
-          o << ind << "    const int gt" << k << " = " << e.group_term(k) << ";\n";
-          horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(e.eff_card(k)) + " + gt" + std::to_string(k) + ")";
-          dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " + std::to_string(e.eff_card(k)) + "u";
-        }
-        o << ind << "    hash = (" << horner << ") % " << G << ";\n";
-        o << ind << "    if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
-        o << ind << "    if ((unsigned)hash >= " << G << "u) act = false;\n";
-        o << ind << "  }\n";
-        o << ind << "  const unsigned amask = __ballot_sync(0xffffffffu, act);\n";
-        o << ind << "  if (amask != 0u && act) {\n";
-        for (int k = 0; k < NA; ++k) {
-          const Agg& ag = p.aggs[k];
-          const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
-          const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
-          o << ind << "    bool v" << k << " = (" << v << ");\n";
-          o << ind << "    unsigned long long x" << k << " = v" << k << " ? " << x << " : 0ULL;\n";
-        }
-        o << ind << "    const unsigned peers = __popc(amask) == 1 ? amask : __match_any_sync(amask, (unsigned)hash);\n";
-        o << ind << "    const int leader = __ffs(peers) - 1;\n";
-        o << ind << "    if (__popc(peers) > 1) {\n";
-        for (int k = 0; k < NA; ++k) {
-          o << ind << "      { unsigned long long r_ = 0ULL;\n";
-          o << ind << "        for (unsigned m = peers; m; m &= m - 1) r_ += __shfl_sync(peers, x" << k << ", __ffs(m) - 1);\n";
-          o << ind << "        x" << k << " = r_; }\n";
-          if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "      v" << k << " = __ballot_sync(peers, v" << k << ") != 0u;\n";
-        }
-        o << ind << "    }\n";
-        const bool smem_ok = G * (unsigned long long)NA * 8 <= 4096ULL;
-        const unsigned long long TWq = (G + 31) / 32;
-        o << ind << "    if (lane == leader) {\n";
-        if (smem_ok) {
-          // Block-private table in shared memory, flushed once per CTA.
-          o << ind << "      if (qtab) {\n";
-          o << ind << "        atomicOr(&qbits[hash >> 5], 1u << (hash & 31));\n";
+          for (int k = 0; k < NA; ++k)
+            if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "tseen" << k << " = __reduce_or_sync(0xffffffffu, tseen" << k << ");\n";
+          o << ind << "#pragma unroll\n" << ind << "for (int g = 0; g < " << G << "; ++g) {\n";
+          o << ind << "  if (!((ttouch >> g) & 1u)) continue;\n";
           int sk = 0;
           for (int k = 0; k < NA; ++k) {
-            o << ind << "        if (x" << k << ") atomicAdd(&qtab[(long long)hash * " << NA << " + " << k << "], x" << k << ");\n";
-            if (!p.sparse && p.aggs[k].fn == AggFn::Sum) {
-              o << ind << "        if (v" << k << ") atomicOr(&qbits[" << TWq * (1 + sk) << "ULL + (hash >> 5)], 1u << (hash & 31));\n";
-              ++sk;
+            const int slot = (int)p.groups.size() + k;
+            const std::string ix = "(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
+            o << ind << "  { unsigned long long s_ = tacc[g * " << NA << " + " << k << "];\n";
+            o << ind << "    for (int o_ = 16; o_ > 0; o_ >>= 1) s_ += __shfl_xor_sync(0xffffffffu, s_, o_);\n";
+            o << ind << "    if (lane == 0) {\n";
+            o << ind << "      if (qtab) { if (s_) atomicAdd(&qtab[g * " << NA << " + " << k << "], s_); }\n";
+            o << ind << "      else if (s_) atomicAdd(&d_result[" << ix << "], s_);\n";
+            if (!p.sparse) {
+              if (p.aggs[k].fn == AggFn::Count) o << ind << "      if (!qtab) db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+              else {
+                o << ind << "      if ((tseen" << k << " >> g) & 1u) { if (qtab) atomicOr(&qbits[" << TWq * (1 + sk) << "ULL + (g >> 5)], 1u << (g & 31)); else db::atomic_set_valid_bit(d_result_validity, " << ix << "); }\n";
+                ++sk;
+              }
             }
+            o << ind << "    }\n" << ind << "  }\n";
           }
-          o << ind << "      } else {\n";
+          o << ind << "  if (lane == 0) { if (qtab) atomicOr(&qbits[g >> 5], 1u << (g & 31)); else atomicOr(&g_touch[g >> 5], 1u << (g & 31)); }\n";
+          o << ind << "}\n";
         } else {
-          o << ind << "      {\n";
-        }
-        o << ind << "      atomicOr(&g_touch[hash >> 5], 1u << (hash & 31));\n";
-        for (int k = 0; k < NA; ++k) {
-          const int slot = (int)p.groups.size() + k;
-          const std::string ix = "(unsigned long long)hash * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
-          o << ind << "      if (x" << k << ") atomicAdd(&d_result[" << ix << "], x" << k << ");\n";
-          if (!p.sparse) {
-            if (p.aggs[k].fn == AggFn::Count) o << ind << "      db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
-            else o << ind << "      if (v" << k << ") db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+          // Direct per-row updates: shared-memory table when the query has one, else global atomics.
+          o << ind << "  if (qtab) {\n";
+          o << ind << "    atomicOr(&qbits[hash >> 5], 1u << (hash & 31));\n";
+          int sk = 0;
+          for (int k = 0; k < NA; ++k) {
+            const Agg& ag = p.aggs[k];
+            const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
+            const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
+            o << ind << "    if (" << v << ") { const unsigned long long x_ = " << x << "; if (x_) atomicAdd(&qtab[(long long)hash * " << NA << " + " << k << "], x_);";
+            if (!p.sparse && ag.fn == AggFn::Sum) { o << " atomicOr(&qbits[" << TWq * (1 + sk) << "ULL + (hash >> 5)], 1u << (hash & 31));"; ++sk; }
+            o << " }\n";
           }
+          o << ind << "  } else {\n";
+          o << ind << "    atomicOr(&g_touch[hash >> 5], 1u << (hash & 31));\n";
+          for (int k = 0; k < NA; ++k) {
+            const Agg& ag = p.aggs[k];
+            const int slot = (int)p.groups.size() + k;
+            const std::string ix = "(unsigned long long)hash * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
+            const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
+            const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
+            o << ind << "    if (" << v << ") { const unsigned long long x_ = " << x << "; if (x_) atomicAdd(&d_result[" << ix << "], x_);";
+            if (!p.sparse && ag.fn == AggFn::Sum) o << " db::atomic_set_valid_bit(d_result_validity, " << ix << ");";
+            o << " }\n";
+            if (!p.sparse && ag.fn == AggFn::Count) o << ind << "    db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+          }
+          o << ind << "  }\n";
+          o << ind << "}\n";
         }
-        o << ind << "      }\n";
-        o << ind << "    }\n";
-        o << ind << "  }\n";
-        o << ind << "}\n";
       }
-      o << "    }\n";
+      o << "        break; }\n";
     }
-    if (STAGES > 0) {
-      o << "    __syncwarp();\n";
-      o << "    if (lane == 0 && staged_ok) {\n";
-      o << "      const long long t2 = t + (long long)NSTAGE * nwarps;\n";
-      o << "      if (t2 < full_tiles) CX_ISSUE(t2, stage);\n";
-      o << "    }\n";
-    }
+    o << "        default: break;\n";
+    o << "      }\n";
+    o << "    }\n";
+    o << "    __syncthreads();\n";
+    o << "    if (threadIdx.x == 0 && staged_ok) {\n";
+    o << "      const long long t2 = t + (long long)NSTAGE * gridDim.x;\n";
+    o << "      if (t2 < full_tiles) CX_ISSUE(t2, stage);\n";
+    o << "    }\n";
     o << "  }\n";
-    if (STAGES > 0)
-      o << "  if (aborted && lane == 0 && staged_ok) cx::drain_stages(bars, NSTAGE, k_iter, gwarp, nwarps, full_tiles, " << wait_limit << "u);\n";
+    o << "  if (aborted && threadIdx.x == 0 && staged_ok) cx::drain_stages(bars, NSTAGE, k_iter, blockIdx.x, gridDim.x, full_tiles, " << wait_limit << "u);\n";
+    o << "  if (aborted) return;\n";
     // Scalar queries: one flush per CTA.
     o << "  __syncthreads();\n";
     o << "  for (int q = threadIdx.x; q < a.sq_total; q += " << CTA << ") {\n";
@@ -1624,8 +1589,7 @@ struct SharedGen {
     o << "    }\n";
     o << "  }\n";
     o << "}\n";
-    if (STAGES > 0) o << "#undef CX_ISSUE\n";
-    o << "\n";
+    o << "#undef CX_ISSUE\n\n";
   }
 
   void emit_keys() {

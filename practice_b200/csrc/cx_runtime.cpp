@@ -185,7 +185,7 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       KernelSpec ks;
       ls >> ks.name >> ks.kind >> ks.table >> ks.block;
       if (ks.kind == "build") ls >> ks.tile;
-      else if (ks.kind == "scan") ls >> ks.tile >> ks.smem >> ks.ctas_per_sm;
+      else if (ks.kind == "scan" || ks.kind == "sharedscan") ls >> ks.tile >> ks.smem >> ks.ctas_per_sm;
       else { size_t z; ls >> z; }
       lp.kernels.push_back(ks);
     } else {
@@ -301,7 +301,7 @@ int load_on_device(cx_module* m, int dev, cx_module::Loaded** out) {
     r = d.ModuleGetFunction(&f, L.mod, k.name.c_str());
     if (r != CUDA_SUCCESS) { d.ModuleUnload(L.mod); return drv_fail(r, k.name.c_str()); }
     int occ = 1;
-    if (k.kind == "scan") {
+    if (k.kind == "scan" || k.kind == "sharedscan") {
       if (m->lp.shared) {
         r = d.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, 227 * 1024);
         if (r != CUDA_SUCCESS) { d.ModuleUnload(L.mod); return drv_fail(r, "cuFuncSetAttribute(smem)"); }
@@ -847,7 +847,7 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
   // Per-query shared-memory group tables, while they fit next to the kernel's
   // fixed shared memory; the rest aggregate with global atomics.
   size_t scan_ki = 0;
-  while (scan_ki < lp.kernels.size() && lp.kernels[scan_ki].kind != "scan") ++scan_ki;
+  while (scan_ki < lp.kernels.size() && lp.kernels[scan_ki].kind != "scan" && lp.kernels[scan_ki].kind != "sharedscan") ++scan_ki;
   const size_t base_smem = scan_ki < lp.kernels.size() ? lp.kernels[scan_ki].smem : 0;
   uint64_t tab_words = 0, bit_words = 0;
   for (int i = 0; i < nq; ++i) {
@@ -894,7 +894,7 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
     CX_CUDA(cudaMemsetAsync(hsq[i].validity, 0, ((need + 63) / 64) * 8, stream));
   }
   size_t ki = 0;
-  for (; ki < lp.kernels.size() && lp.kernels[ki].kind != "scan"; ++ki) {
+  for (; ki < lp.kernels.size() && ki != scan_ki; ++ki) {
     const KernelSpec& k = lp.kernels[ki];
     const long long tiles = (rows[k.table] + k.tile - 1) / k.tile;
     if ((rc = launch(ki, (unsigned)std::min<long long>(tiles, (long long)sms * 16)))) return rc;
@@ -903,7 +903,7 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
   if (ki < lp.kernels.size() && nq > 0) {
     const KernelSpec& k = lp.kernels[ki];
     const long long tiles = (rows[0] + k.tile - 1) / k.tile;
-    const long long warps = std::max(1, k.block / 32);
+    const long long warps = k.kind == "sharedscan" ? 1 : std::max(1, k.block / 32);
     int occ = 1;
     CUresult orr = d.Occupancy(&occ, L->fns[ki], k.block, k.smem + extra_smem);
     if (orr != CUDA_SUCCESS) return drv_fail(orr, "cuOccupancyMaxActiveBlocksPerMultiprocessor");

@@ -203,7 +203,7 @@ def test_sparse_compaction(db):
 
 # ------------------------------------------------------------ shared scans
 
-@pytest.mark.parametrize("nq,tune", [(16, None), (37, (512, 2, 0)), (64, (256, 4, 2))])
+@pytest.mark.parametrize("nq,tune", [(16, None), (37, (512, 2, 2)), (64, (256, 4, 2)), (5, (1024, 1, 1))])
 def test_shared_scan_batch_matches_oracle_per_query(db, nq, tune):
     """Every query of a mixed-template batch run as ONE shared scan equals the
     oracle run on that query alone (same words, same validity bits)."""

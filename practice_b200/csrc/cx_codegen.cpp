@@ -104,15 +104,18 @@ struct Emitter {
   std::set<std::string> loaded;         // register arrays holding a column
   std::set<std::string> valid_regs;     // columns with a <col>_valid register
 
-  // Shared-scan mode: integer literals become per-query parameters P[k].
+  // Shared-scan mode: integer literals become per-query parameters P[k]
+  // (or hoisted registers P<k> when param_regs is set).
   const std::map<const Expr*, int>* lit_index = nullptr;
+  bool param_regs = false;
 
   Emitter(const Plan& plan, const Tuning& t) : p(plan), tu(t) {}
 
   std::string int_lit(const Expr* e) const {
     if (lit_index) {
       auto it = lit_index->find(e);
-      if (it != lit_index->end()) return "P[" + std::to_string(it->second) + "]";
+      if (it != lit_index->end())
+        return param_regs ? "P" + std::to_string(it->second) : "P[" + std::to_string(it->second) + "]";
     }
     return std::to_string(e->ival);
   }
@@ -1345,9 +1348,9 @@ struct SharedGen {
       o << "      for (int r = threadIdx.x; r < n_tile; r += " << CTA << ") tile[" << c << " * TR + r] = d_" << fact_cols[c] << "[tile_offset + r];\n";
     o << "      __syncthreads();\n";
     o << "    }\n";
-    for (int c = 0; c < NSC; ++c) o << "    const int* " << fact_cols[c] << " = tile + " << c << " * TR;\n";
+    for (int c = 0; c < NSC; ++c) o << "    const int* S_" << fact_cols[c] << " = tile + " << c << " * TR;\n";
     for (const Dim& d : dims)
-      for (const auto& at : d.attrs) o << "    int* " << at << " = s_attr + " << attr_slot[at] << " * TR;\n";
+      for (const auto& at : d.attrs) o << "    int* S_" << at << " = s_attr + " << attr_slot[at] << " * TR;\n";
     // Gather every dimension once per row.
     o << "    for (int i = threadIdx.x; i < n_tile; i += " << CTA << ") {\n";
     o << "      unsigned hm_ = 0u;\n";
@@ -1355,12 +1358,12 @@ struct SharedGen {
     for (size_t di = 0; di < dims.size(); ++di) {
       const Dim& d = dims[di];
       o << "      {\n";
-      o << "        const int fk_ = " << d.fk << "[i];\n";
+      o << "        const int fk_ = S_" << d.fk << "[i];\n";
       o << "        const int h_ = (int)HASH(fk_, " << d.len << ", " << d.keymin << ");\n";
       o << "        int4 g_ = make_int4(0, 0, 0, 0);\n";
       o << "        if ((unsigned)h_ < " << d.len << "u) g_ = __ldg(&dix_" << lower(d.name) << "[h_]);\n";
       o << "        if (g_.x != 0 && g_.x == fk_) hm_ |= " << (1u << di) << "u;\n";
-      for (size_t k = 0; k < d.attrs.size(); ++k) o << "        " << d.attrs[k] << "[i] = g_." << comp[k] << ";\n";
+      for (size_t k = 0; k < d.attrs.size(); ++k) o << "        S_" << d.attrs[k] << "[i] = g_." << comp[k] << ";\n";
       o << "      }\n";
     }
     o << "      s_hm[i] = (unsigned char)hm_;\n";
@@ -1369,7 +1372,7 @@ struct SharedGen {
     // Query units.
     o << "    for (int u = warp; u < units; u += NWARP) {\n";
     o << "      const int q_ = u / slices, sl_ = u - q_ * slices;\n";
-    o << "      const int per_ = (n_tile + slices - 1) / slices;\n";
+    o << "      const int per_ = (((n_tile + slices - 1) / slices) + 3) & ~3;\n";
     o << "      const int lo_ = sl_ * per_, hi_ = lo_ + per_ < n_tile ? lo_ + per_ : n_tile;\n";
     o << "      const CxSQ Q = sq[q_];\n";
     o << "      const int* P = s_params + Q.param_off; (void)P;\n";
@@ -1399,9 +1402,53 @@ struct SharedGen {
       if (pred.empty()) pred = "true";
       const int NA = (int)p.aggs.size();
       const int TS = p.storage_ts();
+      // Parameters of this query in registers for the whole unit.
+      for (size_t k = 0; k < lit_maps[s].size(); ++k) o << ind << "const int P" << k << " = P[" << k << "];\n";
+      // Columns the shape reads, four consecutive rows per lane (16-byte shared loads).
+      std::vector<std::string> need;
+      {
+        std::function<void(const Expr*)> walk = [&](const Expr* x) {
+          if (!x) return;
+          if (x->op == Op::Col && std::find(need.begin(), need.end(), x->name) == need.end()) need.push_back(x->name);
+          for (const auto& kk : x->kids) walk(kk.get());
+        };
+        for (const auto& st : p.steps) walk(st.kind == Step::Filter ? st.filter.get() : st.join.filter.get());
+        for (const auto& g : p.groups) walk(g.expr.get());
+        for (const auto& ag : p.aggs) walk(ag.arg.get());
+      }
+      std::string loop_open = ind + "for (int i0_ = lo_ + lane * 4; i0_ < hi_; i0_ += 128) {\n";
+      for (const auto& c : need) {
+        loop_open += ind + "  int " + c + "[4];\n";
+        loop_open += ind + "  { const int4 v_ = *reinterpret_cast<const int4*>(S_" + c + " + i0_); " + c + "[0] = v_.x; " + c +
+                     "[1] = v_.y; " + c + "[2] = v_.z; " + c + "[3] = v_.w; }\n";
+      }
+      loop_open += ind + "  const unsigned hm4_ = *reinterpret_cast<const unsigned*>(s_hm + i0_); (void)hm4_;\n";
+      loop_open += ind + "  #pragma unroll\n" + ind + "  for (int i = 0; i < 4; ++i) {\n";
+      loop_open += ind + "  if (i0_ + i >= hi_) break;\n";
+      const std::string loop_close = ind + "  }\n" + ind + "}\n";
+      e.param_regs = true;
+      // Re-derive the predicate with register parameters and the packed hit mask.
+      {
+        std::vector<std::string> conds2;
+        for (const auto& st : p.steps) {
+          if (st.kind == Step::Filter) {
+            conds2.push_back(and_terms({e.valid_of(st.filter.get()), e.value_of(st.filter.get())}));
+            continue;
+          }
+          const Join& j = st.join;
+          size_t di = 0;
+          for (; di < dims.size(); ++di) if (dims[di].name == j.dim) break;
+          std::string c = "((hm4_ >> (8 * i + " + std::to_string(di) + ")) & 1u)";
+          if (j.filter) c += " && (" + and_terms({e.valid_of(j.filter.get()), e.value_of(j.filter.get())}) + ")";
+          conds2.push_back(c);
+        }
+        pred.clear();
+        for (const auto& c : conds2) pred += (pred.empty() ? "" : " && ") + std::string("(") + c + ")";
+        if (pred.empty()) pred = "true";
+      }
       if (p.groups.empty()) {
         for (int k = 0; k < NA; ++k) o << ind << "unsigned long long s" << k << "_ = 0ULL, c" << k << "_ = 0ULL;\n";
-        o << ind << "for (int i = lo_ + lane; i < hi_; i += 32) {\n";
+        o << loop_open;
         o << ind << "  if (!(" << pred << ")) continue;\n";
         for (int k = 0; k < NA; ++k) {
           const Agg& ag = p.aggs[k];
@@ -1409,7 +1456,7 @@ struct SharedGen {
           const std::string x = ag.fn == AggFn::Count ? "1ULL" : e.math_push(ag.arg.get(), true);
           o << ind << "  if (" << v << ") { s" << k << "_ += " << x << "; c" << k << "_ += 1ULL; }\n";
         }
-        o << ind << "}\n";
+        o << loop_close;
         for (int k = 0; k < NA; ++k) {
           o << ind << "if (__any_sync(0xffffffffu, c" << k << "_ != 0ULL)) {\n";
           o << ind << "  for (int o_ = 16; o_ > 0; o_ >>= 1) { s" << k << "_ += __shfl_xor_sync(0xffffffffu, s" << k << "_, o_); c" << k << "_ += __shfl_xor_sync(0xffffffffu, c" << k << "_, o_); }\n";
@@ -1439,7 +1486,7 @@ struct SharedGen {
           for (int k = 0; k < NA; ++k)
             if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "unsigned tseen" << k << " = 0u;\n";
         }
-        o << ind << "for (int i = lo_ + lane; i < hi_; i += 32) {\n";
+        o << loop_open;
         o << ind << "  if (!(" << pred << ")) continue;\n";
         o << terms.str();
         o << ind << "  const int hash = (" << horner << ") % " << G << ";\n";
@@ -1456,7 +1503,7 @@ struct SharedGen {
             if (!p.sparse && ag.fn == AggFn::Sum) o << ind << "    tseen" << k << " |= 1u << hash;\n";
             o << ind << "  }\n";
           }
-          o << ind << "}\n";
+          o << loop_close;
           o << ind << "ttouch = __reduce_or_sync(0xffffffffu, ttouch);\n";
           for (int k = 0; k < NA; ++k)
             if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "tseen" << k << " = __reduce_or_sync(0xffffffffu, tseen" << k << ");\n";
@@ -1509,7 +1556,7 @@ struct SharedGen {
             if (!p.sparse && ag.fn == AggFn::Count) o << ind << "    db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
           }
           o << ind << "  }\n";
-          o << ind << "}\n";
+          o << loop_close;
         }
       }
       o << "        break; }\n";

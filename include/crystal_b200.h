@@ -124,6 +124,12 @@ int cx_ctx_set_scratch(cx_exec_ctx* c, void* dev_ptr, uint64_t bytes);
 int cx_module_scratch_bytes(const cx_module* m, const cx_exec_ctx* c, uint64_t* bytes);
 /* Overrides the multiprocessor count used to size persistent grids (0 = device's). */
 int cx_ctx_set_sm_count(cx_exec_ctx* c, int sms);
+/* Registers the value range [lo, hi] of column `name` ("d_<column>").  Shared
+ * scans turn single-column filters on a ranged column into lookup tables over
+ * the first 256 values of the range; filters on unranged columns (or values
+ * past the window) are evaluated row by row per query.  No reference
+ * counterpart: the reference plans one query at a time. */
+int cx_ctx_set_column_range(cx_exec_ctx* c, const char* name, int64_t lo, int64_t hi);
 
 /* Enqueues the query on `stream` (a cudaStream_t; NULL = legacy default
  * stream).  Asynchronous: call cx_ctx_sync before reading results.  Replaces
@@ -163,8 +169,10 @@ int cx_plan_literals(const char* plan, size_t plan_len, int64_t* out, int cap, i
 int cx_shared_codegen(const char* const* plans, const size_t* plan_lens, int nshapes, const cx_tuning* tuning,
                       char* out, size_t out_cap, size_t* out_len);
 /* Enqueues one batch (<= 256 queries, <= 4096 parameters) of a compiled shared
- * program on `stream`; cx_ctx_sync waits for it.  Foreign keys of shared joins
- * must be non-zero (the engine checks column minima before batching). */
+ * program on `stream`; cx_ctx_sync waits for it.  The program answers up to 64
+ * queries per pass over the fact table; larger batches run as consecutive
+ * passes.  Foreign keys of shared joins must be non-zero (the engine checks
+ * column minima before batching). */
 int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queries, int nq, const int32_t* params,
                       int nparams, void* stream);
 

@@ -24,7 +24,7 @@ EXPORTS = [
     "cx_ctx_set_scratch", "cx_module_scratch_bytes", "cx_ctx_set_sm_count", "cx_execute",
     "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse", "cx_compact_sparse_noalloc",
     "cx_gen_uniform", "cx_gen_datekey", "cx_gen_validity", "cx_plan_literals", "cx_shared_codegen",
-    "cx_shared_execute",
+    "cx_shared_execute", "cx_ctx_set_column_range",
 ]
 
 
@@ -78,6 +78,7 @@ def _load() -> C.CDLL:
         "cx_ctx_set_scratch": (C.c_int, [vp, vp, u64]),
         "cx_module_scratch_bytes": (C.c_int, [vp, vp, C.POINTER(u64)]),
         "cx_ctx_set_sm_count": (C.c_int, [vp, C.c_int]),
+        "cx_ctx_set_column_range": (C.c_int, [vp, C.c_char_p, i64, i64]),
         "cx_execute": (C.c_int, [vp, vp, vp]),
         "cx_ctx_sync": (C.c_int, [vp]),
         "cx_ctx_timing": (C.c_int, [vp, C.POINTER(Timing)]),
@@ -193,6 +194,9 @@ class ExecCtx:
 
     def set_rows(self, table: str, rows: int) -> None:
         check(lib.cx_ctx_set_table_rows(self.handle, table.encode(), rows), "cx_ctx_set_table_rows")
+
+    def set_column_range(self, name: str, lo: int, hi: int) -> None:
+        check(lib.cx_ctx_set_column_range(self.handle, name.encode(), lo, hi), "cx_ctx_set_column_range")
 
     def set_result(self, res_ptr: int, res_words: int, val_ptr: int, val_words: int) -> None:
         check(lib.cx_ctx_set_result(self.handle, res_ptr, res_words, val_ptr, val_words), "cx_ctx_set_result")

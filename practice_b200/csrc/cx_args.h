@@ -12,6 +12,7 @@
 #define CX_MAX_HTS 8
 #define CX_MAX_TABLES 8
 #define CX_MAX_SHAPES 16
+#define CX_MAX_FCOLS 8
 
 // One query of a shared-scan batch: its own result buffers, its plan shape and
 // the offset of its literal parameters.
@@ -46,4 +47,7 @@ struct CxArgs {
   int nparams;
   int smem_tab_words;                          // u64 words of per-query shared-memory group tables
   int smem_bit_words;                          // u32 words of their touched / seen bits
+  int* dat[CX_MAX_HTS];                        // extra payload attributes at each dimension's slots
+  int fbase[CX_MAX_FCOLS];                     // first value of each fact filter table window
+  int fwin[CX_MAX_FCOLS];                      // values in the window (0: evaluate every row per query)
 };

@@ -133,7 +133,13 @@ struct Emitter {
   }
 
   // ---------------------------------------------------------- expressions --
-  std::string reg(const std::string& c) const { return c + "[i]"; }
+  // Column spelling override (shared-scan kernels read columns from
+  // shared-memory tiles or dimension rows rather than register arrays).
+  std::map<std::string, std::string> col_expr;
+  std::string reg(const std::string& c) const {
+    auto it = col_expr.find(c);
+    return it != col_expr.end() ? it->second : c + "[i]";
+  }
 
   std::string valid_of(const Expr* e) const {
     if (!e) return "1";
@@ -1051,16 +1057,25 @@ std::string generate_cuda_impl(const Plan& plan, const Tuning& tuning) {
 }
 
 // ============================================================ shared scan ===
-// One persistent kernel for a batch of queries of several plan shapes: each
-// warp stages a tile of the union of the fact columns once, gathers every
-// joined dimension's slot entry once, then runs every query of the batch on
-// those registers.  A dimension index entry is {key, attr1, attr2, attr3}
-// stored at the PHT slot HASH(key, len, key_min) of its row (index_<dim>
-// kernels); a query's join keeps a row when the slot's key equals the FK and
-// the row passes the query's dimension filter -- the condition under which the
-// reference's filtered PHT would hold that key (join.h:124-253, 7-120), for
-// dimensions whose keys occupy distinct slots (checked while indexing) and
-// non-zero foreign keys (checked by the engine before it forms a batch).
+// One persistent kernel answers a batch of up to 64 queries of several plan
+// shapes in one pass over the fact table.  Every query's predicates collapse
+// into one 64-bit query mask per fact row (bit q set: the row passes query q),
+// in the manner of the CJOIN shared star-join operator (Candea, Polyzotis,
+// Vingralek, VLDB 2009):
+//  * index_<dim> kernels store, at the PHT slot HASH(key, len, key_min) of each
+//    dimension row, {key, mask_lo, mask_hi, attr0} and up to three more payload
+//    attributes.  Mask bit q is set when query q does not join the dimension or
+//    the row passes the query's dimension filter -- the condition under which
+//    the reference's filtered PHT would hold that key (join.h:124-253, 7-120).
+//    Keys must occupy distinct slots (checked while indexing) and foreign keys
+//    must be non-zero (checked by the engine before it forms a batch).
+//  * single-column fact filters become per-CTA lookup tables over a window of
+//    FW values of the column, starting at the column minimum the host
+//    registered; values outside the window, and every other filter, are
+//    evaluated per query for the rows still in the mask.
+//  * warps then take (query, row slice) units and aggregate the rows whose bit
+//    is set, four rows per lane, with partial aggregates in registers, a
+//    per-query shared-memory table or global atomics.
 
 void lits_of(const Expr* e, std::vector<const Expr*>& out) {
   if (!e) return;
@@ -1068,24 +1083,56 @@ void lits_of(const Expr* e, std::vector<const Expr*>& out) {
   for (const auto& k : e->kids) lits_of(k.get(), out);
 }
 
+// Top-level AND terms of a filter.  Shared shapes have no nullable columns, so
+// two-valued logic holds and the terms can be evaluated separately.
+void conjuncts_of(const Expr* e, std::vector<const Expr*>& out) {
+  if (!e) return;
+  if (e->op == Op::And) {
+    conjuncts_of(e->kids[0].get(), out);
+    conjuncts_of(e->kids[1].get(), out);
+    return;
+  }
+  out.push_back(e);
+}
+
+void cols_of(const Expr* e, std::vector<std::string>& out) {
+  if (!e) return;
+  if (e->op == Op::Col && std::find(out.begin(), out.end(), e->name) == out.end()) out.push_back(e->name);
+  for (const auto& k : e->kids) cols_of(k.get(), out);
+}
+
 struct SharedGen {
+  static constexpr int MAXQ = 64;       // queries per launch (two 32-bit mask words)
+  static constexpr int FW = 256;        // values per fact filter table
+  static constexpr int MAX_FCOLS = 8;   // fact columns with filter tables
+  static constexpr int MAX_ATTRS = 4;   // payload attributes per dimension
+
   const std::vector<const Plan*>& shapes;
   const Tuning& tu;
   std::ostringstream meta, src;
   std::string fact;
   std::vector<std::string> tables;
-  std::vector<std::string> fact_cols;
+  std::vector<std::string> fact_cols;   // staged fact columns
   struct Dim {
     std::string name, pk, fk;
     long long len = 0, keymin = 0;
-    std::vector<std::string> attrs;
+    std::vector<std::string> attrs;     // payload attributes; attrs[0] rides in the key entry
+    std::vector<std::string> fcols;     // dimension columns read by join filters
     int slot = 0, table = 0;
   };
   std::vector<Dim> dims;
+  std::map<std::string, int> attr_dim;  // payload attribute -> dimension index
   std::map<std::string, int> col_slot;
   std::vector<std::pair<std::string, int>> col_order;
   std::vector<std::map<const Expr*, int>> lit_maps;
   int max_lits = 0, max_scalar_aggs = 0;
+  struct Preds {
+    std::map<int, std::vector<const Expr*>> joins;   // dimension -> its filters (null: join only)
+    std::map<int, std::vector<const Expr*>> pushed;  // filter-table column -> conjuncts on it
+    std::vector<const Expr*> resid;                  // conjuncts evaluated per row and query
+  };
+  std::vector<Preds> preds;
+  std::vector<std::string> fcols;       // fact columns with filter tables
 
   SharedGen(const std::vector<const Plan*>& s, const Tuning& t) : shapes(s), tu(t) {}
 
@@ -1104,48 +1151,38 @@ struct SharedGen {
     col_order.push_back({c, table});
     return s;
   }
-  Dim* find_dim(const std::string& n) {
-    for (auto& d : dims)
-      if (d.name == n) return &d;
-    return nullptr;
+  int dim_index(const std::string& n) const {
+    for (size_t i = 0; i < dims.size(); ++i)
+      if (dims[i].name == n) return (int)i;
+    return -1;
   }
   void add_fact(const std::string& c) {
     if (std::find(fact_cols.begin(), fact_cols.end(), c) == fact_cols.end()) fact_cols.push_back(c);
   }
-  void add_fact_expr(const Plan& p, const Expr* e) {
+  // Columns of a row-level expression: fact columns are staged, any other
+  // column must be a payload attribute of a dimension the shape joins.
+  void need_row_cols(const Plan& p, const Expr* e) {
     std::vector<std::string> cs;
-    std::function<void(const Expr*)> walk = [&](const Expr* x) {
-      if (!x) return;
-      if (x->op == Op::Col) cs.push_back(x->name);
-      for (const auto& k : x->kids) walk(k.get());
-    };
-    walk(e);
-    for (const auto& c : cs)
+    cols_of(e, cs);
+    for (const auto& c : cs) {
       if (p.table_of_col.at(c) == 0) add_fact(c);
+      else if (!attr_dim.count(c)) throw PlanError("column " + c + " is neither a fact column nor a join payload");
+    }
   }
 
   void collect() {
     if (shapes.empty() || shapes.size() > CX_MAX_SHAPES_) throw PlanError("shared batch needs 1..16 shapes");
     fact = shapes[0]->tables[0].name;
     table_slot(fact);
-    for (const Plan* pp : shapes) {
-      const Plan& p = *pp;
+    preds.resize(shapes.size());
+    for (size_t si = 0; si < shapes.size(); ++si) {
+      const Plan& p = *shapes[si];
       if (p.tables[0].name != fact) throw PlanError("shared batch mixes fact tables");
       std::function<void(const Expr*)> no_null = [&](const Expr* x) {
         if (!x) return;
         if (x->op == Op::Col && p.nullable.count(x->name)) throw PlanError("nullable column " + x->name + " is not shareable");
         for (const auto& k : x->kids) no_null(k.get());
       };
-      for (const auto& a : p.aggs) {
-        if (a.fn != AggFn::Count && a.fn != AggFn::Sum) throw PlanError("shared scans support COUNT and SUM");
-        no_null(a.arg.get());
-        add_fact_expr(p, a.arg.get());
-      }
-      for (const auto& g : p.groups) {
-        if (g.nullable) throw PlanError("nullable group key is not shareable");
-        no_null(g.expr.get());
-        add_fact_expr(p, g.expr.get());
-      }
       std::map<const Expr*, int> lm;
       std::vector<const Expr*> lits;
       collect_literals(p, lits);
@@ -1156,73 +1193,169 @@ struct SharedGen {
       max_lits = std::max(max_lits, (int)lits.size());
       if (p.groups.empty()) max_scalar_aggs = std::max(max_scalar_aggs, (int)p.aggs.size());
       lit_maps.push_back(lm);
+      // Joins first: their payloads are the attributes later expressions read.
       for (const auto& s : p.steps) {
-        if (s.kind == Step::Filter) {
-          no_null(s.filter.get());
-          add_fact_expr(p, s.filter.get());
-          continue;
-        }
+        if (s.kind != Step::JoinStep) continue;
         const Join& j = s.join;
-        Dim* d = find_dim(j.dim);
-        if (!d) {
+        if (j.fks.size() != 1) throw PlanError("OR-joins are not shareable");
+        int di = dim_index(j.dim);
+        if (di < 0) {
           dims.push_back(Dim());
-          d = &dims.back();
-          d->name = j.dim;
-          d->pk = j.pk;
-          d->fk = j.fks[0];
-          d->len = j.len;
-          d->keymin = j.keymin;
-          d->slot = (int)dims.size() - 1;
-          d->table = table_slot(j.dim);
-        } else if (d->pk != j.pk || d->fk != j.fks[0] || d->len != j.len || d->keymin != j.keymin) {
-          throw PlanError("shapes join " + j.dim + " differently");
+          Dim& d = dims.back();
+          d.name = j.dim;
+          d.pk = j.pk;
+          d.fk = j.fks[0];
+          d.len = j.len;
+          d.keymin = j.keymin;
+          d.slot = (int)dims.size() - 1;
+          d.table = table_slot(j.dim);
+          di = d.slot;
+        } else {
+          const Dim& d = dims[di];
+          if (d.pk != j.pk || d.fk != j.fks[0] || d.len != j.len || d.keymin != j.keymin)
+            throw PlanError("shapes join " + j.dim + " differently");
         }
+        Dim& d = dims[di];
         if (p.nullable.count(j.fks[0]) || p.nullable.count(j.pk)) throw PlanError("nullable join key is not shareable");
+        if (d.len <= 0 || d.len > (1LL << 30)) throw PlanError("dimension " + j.dim + " has an unusable slot count");
         add_fact(j.fks[0]);
-        std::vector<std::string> need;
-        std::function<void(const Expr*)> walk = [&](const Expr* x) {
-          if (!x) return;
-          if (x->op == Op::Col) need.push_back(x->name);
-          for (const auto& k : x->kids) walk(k.get());
-        };
-        walk(j.filter.get());
-        if (!j.payload.empty()) need.push_back(j.payload);
-        for (const auto& c : need) {
-          if (p.nullable.count(c)) throw PlanError("nullable dimension column " + c + " is not shareable");
-          if (c != d->pk && std::find(d->attrs.begin(), d->attrs.end(), c) == d->attrs.end()) d->attrs.push_back(c);
+        no_null(j.filter.get());
+        std::vector<std::string> fc;
+        cols_of(j.filter.get(), fc);
+        for (const auto& c : fc) {
+          if (p.table_of_col.at(c) != p.table_slot(j.dim)) throw PlanError("join filter of " + j.dim + " reads " + c);
+          if (std::find(d.fcols.begin(), d.fcols.end(), c) == d.fcols.end()) d.fcols.push_back(c);
         }
-        if (d->attrs.size() > 3) throw PlanError("more than 3 attributes of " + j.dim + " in one shared batch");
+        preds[si].joins[di].push_back(j.filter.get());
+        if (!j.payload.empty()) {
+          if (p.nullable.count(j.payload)) throw PlanError("nullable dimension column " + j.payload + " is not shareable");
+          auto it = attr_dim.find(j.payload);
+          if (it != attr_dim.end() && it->second != di) throw PlanError("payload " + j.payload + " of two dimensions");
+          if (std::find(d.attrs.begin(), d.attrs.end(), j.payload) == d.attrs.end()) d.attrs.push_back(j.payload);
+          attr_dim[j.payload] = di;
+          if ((int)d.attrs.size() > MAX_ATTRS) throw PlanError("more than 4 payload attributes of " + j.dim + " in one shared batch");
+        }
+      }
+      for (const auto& s : p.steps) {
+        if (s.kind != Step::Filter) continue;
+        no_null(s.filter.get());
+        std::vector<const Expr*> cj;
+        conjuncts_of(s.filter.get(), cj);
+        for (const Expr* c : cj) {
+          std::vector<std::string> cs;
+          cols_of(c, cs);
+          need_row_cols(p, c);
+          // A conjunct over payload attributes of one joined dimension is a
+          // predicate on the dimension row: it joins that dimension's mask.
+          int dd = -1;
+          bool dim_only = !cs.empty();
+          for (const auto& cc : cs) {
+            auto it = attr_dim.find(cc);
+            if (p.table_of_col.at(cc) == 0 || it == attr_dim.end() || (dd >= 0 && dd != it->second)) { dim_only = false; break; }
+            dd = it->second;
+          }
+          if (dim_only && preds[si].joins.count(dd)) {
+            preds[si].joins[dd].push_back(c);
+            for (const auto& cc : cs)
+              if (std::find(dims[dd].fcols.begin(), dims[dd].fcols.end(), cc) == dims[dd].fcols.end()) dims[dd].fcols.push_back(cc);
+            continue;
+          }
+          if (cs.size() == 1 && p.table_of_col.at(cs[0]) == 0) {
+            auto it = std::find(fcols.begin(), fcols.end(), cs[0]);
+            int k = (int)(it - fcols.begin());
+            if (it == fcols.end()) {
+              if ((int)fcols.size() < MAX_FCOLS) { fcols.push_back(cs[0]); k = (int)fcols.size() - 1; }
+              else k = -1;
+            }
+            if (k >= 0) { preds[si].pushed[k].push_back(c); continue; }
+          }
+          preds[si].resid.push_back(c);
+        }
+      }
+      for (const auto& a : p.aggs) {
+        if (a.fn != AggFn::Count && a.fn != AggFn::Sum) throw PlanError("shared scans support COUNT and SUM");
+        no_null(a.arg.get());
+        need_row_cols(p, a.arg.get());
+      }
+      for (const auto& g : p.groups) {
+        if (g.nullable) throw PlanError("nullable group key is not shareable");
+        no_null(g.expr.get());
+        need_row_cols(p, g.expr.get());
       }
     }
     if ((int)dims.size() > CX_MAX_HTS_) throw PlanError("too many dimensions in a shared batch");
+    if (dims.size() > 32) throw PlanError("too many dimensions in a shared batch");
   }
 
-  void emit_index(const Dim& d) {
+  std::string conj_and(Emitter& e, const std::vector<const Expr*>& cs) const {
+    std::string out;
+    for (const Expr* c : cs) {
+      if (!c) continue;
+      const std::string t = and_terms({e.valid_of(c), e.value_of(c)});
+      if (lit_true(t)) continue;
+      out += (out.empty() ? "" : " && ") + std::string("(") + t + ")";
+    }
+    return out.empty() ? "true" : out;
+  }
+
+  // Per batch: slot entries of one dimension with the batch's query masks.
+  void emit_index(const Dim& d, int di) {
     const std::string k = "index_" + lower(d.name);
     meta << "kernel " << k << " build " << d.table << " 256 1024\n";
     src << "extern \"C\" __global__ void __launch_bounds__(256) " << k << "(const CxArgs a) {\n";
+    src << "  __shared__ int s_shape[" << MAXQ << "], s_poff[" << MAXQ << "];\n";
+    src << "  const int nq = a.sq_total < " << MAXQ << " ? a.sq_total : " << MAXQ << ";\n";
+    src << "  for (int q = threadIdx.x; q < nq; q += blockDim.x) { s_shape[q] = a.sq[q].shape; s_poff[q] = a.sq[q].param_off; }\n";
+    src << "  __syncthreads();\n";
     src << "  const long long n = a.rows[" << d.table << "];\n";
-    src << "  int4* dix = (int4*)a.ht[" << d.slot << "];\n";
-    src << "  const int* key = a.col[" << slot_of(d.pk, d.table) << "];\n";
+    src << "  int4* dkm = (int4*)a.ht[" << d.slot << "];\n";
+    if (d.attrs.size() > 1) src << "  int4* dat = (int4*)a.dat[" << d.slot << "];\n";
+    src << "  const int* __restrict__ key = a.col[" << slot_of(d.pk, d.table) << "];\n";
     for (size_t i = 0; i < d.attrs.size(); ++i)
-      src << "  const int* at" << i << " = a.col[" << slot_of(d.attrs[i], d.table) << "];\n";
+      src << "  const int* __restrict__ at" << i << " = a.col[" << slot_of(d.attrs[i], d.table) << "];\n";
+    for (const auto& c : d.fcols) src << "  const int* __restrict__ F_" << c << " = a.col[" << slot_of(c, d.table) << "];\n";
     src << "  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {\n";
     src << "    const int k = key[r];\n";
     src << "    if (k == 0) continue;\n";
     src << "    const int h = (int)HASH(k, " << d.len << ", " << d.keymin << ");\n";
     src << "    if ((unsigned)h >= " << d.len << "u) continue;\n";
-    src << "    if (atomicCAS(&dix[h].x, 0, k) != 0) { cx::raise(a.err, cx::ERR_DIM_COLLISION); continue; }\n";
-    const char* comp[] = {"y", "z", "w"};
-    for (size_t i = 0; i < d.attrs.size(); ++i) src << "    dix[h]." << comp[i] << " = at" << i << "[r];\n";
+    src << "    if (atomicCAS(&dkm[h].x, 0, k) != 0) { cx::raise(a.err, cx::ERR_DIM_COLLISION); continue; }\n";
+    src << "    unsigned long long m = 0ULL;\n";
+    src << "    for (int q = 0; q < nq; ++q) {\n";
+    src << "      const int* P = a.sparams + s_poff[q]; (void)P;\n";
+    src << "      bool pass = true;\n";
+    src << "      switch (s_shape[q]) {\n";
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      auto it = preds[s].joins.find(di);
+      if (it == preds[s].joins.end()) continue;
+      Emitter e(*shapes[s], tu);
+      e.lit_index = &lit_maps[s];
+      for (const auto& c : d.fcols) e.col_expr[c] = "F_" + c + "[r]";
+      const std::string f = conj_and(e, it->second);
+      if (f == "true") continue;
+      src << "        case " << s << ": pass = " << f << "; break;\n";
+    }
+    src << "        default: break;\n";
+    src << "      }\n";
+    src << "      if (pass) m |= 1ULL << q;\n";
+    src << "    }\n";
+    src << "    dkm[h] = make_int4(k, (int)(unsigned)m, (int)(unsigned)(m >> 32), " << (d.attrs.empty() ? "0" : "at0[r]") << ");\n";
+    if (d.attrs.size() > 1) {
+      src << "    dat[h] = make_int4(";
+      for (size_t i = 1; i < 4; ++i) src << (i > 1 ? ", " : "") << (i < d.attrs.size() ? "at" + std::to_string(i) + "[r]" : "0");
+      src << ", 0);\n";
+    }
     src << "  }\n}\n\n";
   }
 
   std::string run() {
     collect();
-    meta << "v 1\nshared\n";
+    meta << "v 1\nshared " << MAXQ << " " << MAXQ * std::max(1, max_lits) << "\n";
     for (const Dim& d : dims) {
-      meta << "ht " << d.slot << " dix_" << lower(d.name) << " " << d.len * 4 << "\n";
+      meta << "ht " << d.slot << " dkm_" << lower(d.name) << " " << d.len * 4 << "\n";
+      if (d.attrs.size() > 1) meta << "dat " << d.slot << " " << d.len * 4 << "\n";
     }
+    for (size_t k = 0; k < fcols.size(); ++k) meta << "fcol " << k << " d_" << fcols[k] << "\n";
     for (size_t s = 0; s < shapes.size(); ++s) {
       const Plan& p = *shapes[s];
       Emitter e(p, tu);
@@ -1235,10 +1368,9 @@ struct SharedGen {
            << " " << (p.sparse ? 1 : 0) << " " << lit_maps[s].size() << " " << (smem_ok ? 1 : 0) << " " << NA << " "
            << (G + 31) / 32 << " " << nseen << "\n";
     }
-    for (const Dim& d : dims) emit_index(d);
+    for (size_t di = 0; di < dims.size(); ++di) emit_index(dims[di], (int)di);
     emit_scan();
     emit_keys();
-    std::ostringstream cols;
     for (size_t i = 0; i < tables.size(); ++i) meta << "table " << i << " " << tables[i] << "\n";
     for (size_t i = 0; i < col_order.size(); ++i)
       meta << "col " << i << " d_" << col_order[i].first << " " << col_order[i].second << "\n";
@@ -1246,24 +1378,28 @@ struct SharedGen {
     out << "/*@cx-launch\n" << meta.str() << "@*/\n";
     out << "// Generated by crystal-b200 for sm_100a (shared scan).\n";
     out << "#include \"cx_args.h\"\n#include \"crystal_sm100.cuh\"\n\n";
+    out << "template <typename A, typename B>\n"
+           "__device__ __forceinline__ auto cx_mdiv(A x, B y) -> decltype(x / y) {\n"
+           "  return (y == 0) ? (decltype(x / y))0 : x / y;\n}\n\n";
     out << src.str();
     return out.str();
   }
 
-  // CTA-tiled, query-parallel shared scan.  Per tile of TR = block x items
-  // rows: thread 0 stages the union of fact columns by TMA bulk copies; all
-  // threads gather every joined dimension once into shared-memory attribute
-  // arrays and a per-row hit mask; then each warp takes (query, row-slice)
-  // units and evaluates its query row by row from shared memory, with
-  // per-lane partial aggregates reduced once per unit.
+  // CTA-tiled shared scan.  Per tile of TR = block x items rows: thread 0
+  // stages the union of fact columns by TMA bulk copies; every thread builds
+  // the query masks of its rows (filter tables, one gather per dimension,
+  // residual filters) and stores them with the payload attributes in shared
+  // memory; then warps take (query, row slice) units and aggregate the rows
+  // whose mask bit is set.
   void emit_scan() {
     const int CTA = tu.block_threads, IPT = tu.items_per_thread;
     if (CTA % 32 || CTA < 64 || CTA > 1024 || IPT < 1 || IPT > 16) throw PlanError("bad block shape");
     const int NW = CTA / 32, TR = CTA * IPT;
     const int NSC = (int)fact_cols.size();
     const int STAGES = std::max(1, tu.stages);
-    const int MAXQ = 256, MAXP = 4096;
+    const int MAXP = MAXQ * std::max(1, max_lits);
     const int NACC = std::max(1, max_scalar_aggs) * 2;  // (sum, count) per scalar aggregate
+    const int NFC = (int)fcols.size();
     int nattr = 0;
     std::map<std::string, int> attr_slot;
     for (const Dim& d : dims)
@@ -1271,12 +1407,16 @@ struct SharedGen {
     unsigned long long off = 0;
     const unsigned long long stage_off = off; off += (unsigned long long)STAGES * NSC * TR * 4;
     const unsigned long long attr_off = off; off += (unsigned long long)nattr * TR * 4;
-    const unsigned long long hm_off = off; off += (unsigned long long)TR;
-    off = (off + 15) & ~15ULL;
+    const unsigned long long mlo_off = off; off += (unsigned long long)TR * 4;
+    const unsigned long long mhi_off = off; off += (unsigned long long)TR * 4;
     const unsigned long long bars_off = off; off += (unsigned long long)STAGES * 8;
+    off = (off + 15) & ~15ULL;
     const unsigned long long par_off = off; off += (unsigned long long)MAXP * 4;
     off = (off + 15) & ~15ULL;
     const unsigned long long acc_off = off; off += (unsigned long long)MAXQ * NACC * 8;
+    const unsigned long long sq_off = off; off += (unsigned long long)MAXQ * 40;
+    const unsigned long long fm_off = off; off += (unsigned long long)NFC * FW * 8;
+    const unsigned long long nj_off = off; off += (unsigned long long)(dims.size() + 3) * 8;
     off = (off + 15) & ~15ULL;
     const unsigned long long tab_off = off;
     const unsigned long long smem_total = (off + 127) & ~127ULL;
@@ -1292,22 +1432,92 @@ struct SharedGen {
     o << "  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
     o << "  int* stage_buf = (int*)(cx_smem + " << stage_off << ");\n";
     o << "  int* s_attr = (int*)(cx_smem + " << attr_off << "); (void)s_attr;\n";
-    o << "  unsigned char* s_hm = (unsigned char*)(cx_smem + " << hm_off << "); (void)s_hm;\n";
+    o << "  unsigned* s_mlo = (unsigned*)(cx_smem + " << mlo_off << ");\n";
+    o << "  unsigned* s_mhi = (unsigned*)(cx_smem + " << mhi_off << ");\n";
     o << "  unsigned long long* bars = (unsigned long long*)(cx_smem + " << bars_off << ");\n";
     o << "  int* s_params = (int*)(cx_smem + " << par_off << ");\n";
     o << "  unsigned long long* s_qacc = (unsigned long long*)(cx_smem + " << acc_off << ");\n";
+    o << "  CxSQ* s_sq = (CxSQ*)(cx_smem + " << sq_off << ");\n";
+    o << "  unsigned long long* s_fm = (unsigned long long*)(cx_smem + " << fm_off << "); (void)s_fm;\n";
+    o << "  unsigned long long* s_nj = (unsigned long long*)(cx_smem + " << nj_off << ");\n";
     o << "  unsigned long long* s_tab = (unsigned long long*)(cx_smem + " << tab_off << "); (void)s_tab;\n";
     o << "  unsigned int* s_bits = (unsigned int*)(s_tab + a.smem_tab_words); (void)s_bits;\n";
-    o << "  const CxSQ* sq = a.sq;\n";
+    o << "  const int nq = a.sq_total < " << MAXQ << " ? a.sq_total : " << MAXQ << ";\n";
     o << "  const long long n_rows = a.rows[0];\n";
     o << "  const long long num_tiles = (n_rows + TR - 1) / TR;\n";
     o << "  const long long full_tiles = n_rows / TR;\n";
+    o << "  for (int w = threadIdx.x; w < nq; w += " << CTA << ") s_sq[w] = a.sq[w];\n";
     o << "  for (int w = threadIdx.x; w < a.nparams && w < " << MAXP << "; w += " << CTA << ") s_params[w] = a.sparams[w];\n";
     o << "  for (int w = threadIdx.x; w < " << MAXQ * NACC << "; w += " << CTA << ") s_qacc[w] = 0ULL;\n";
     o << "  for (int w = threadIdx.x; w < a.smem_tab_words; w += " << CTA << ") s_tab[w] = 0ULL;\n";
     o << "  for (int w = threadIdx.x; w < a.smem_bit_words; w += " << CTA << ") s_bits[w] = 0u;\n";
+    o << "  __syncthreads();\n";
+    // Filter tables: bit q of s_fm[k * FW + v] clears when query q's conjuncts
+    // on filter column k reject the value fbase[k] + v.
+    if (NFC) {
+      o << "  for (int v = threadIdx.x; v < " << NFC * FW << "; v += " << CTA << ") {\n";
+      o << "    const int k_ = v / " << FW << ";\n";
+      o << "    const int fv_ = (int)((unsigned)a.fbase[k_] + (unsigned)(v - k_ * " << FW << "));\n";
+      o << "    unsigned long long m = ~0ULL;\n";
+      o << "    for (int q = 0; q < nq; ++q) {\n";
+      o << "      const int* P = s_params + s_sq[q].param_off; (void)P;\n";
+      o << "      bool pass = true;\n";
+      o << "      switch (s_sq[q].shape) {\n";
+      for (size_t s = 0; s < shapes.size(); ++s) {
+        if (preds[s].pushed.empty()) continue;
+        Emitter e(*shapes[s], tu);
+        e.lit_index = &lit_maps[s];
+        o << "        case " << s << ":\n";
+        for (const auto& kv : preds[s].pushed) {
+          e.col_expr.clear();
+          e.col_expr[fcols[kv.first]] = "fv_";
+          o << "          if (k_ == " << kv.first << ") pass = " << conj_and(e, kv.second) << ";\n";
+        }
+        o << "          break;\n";
+      }
+      o << "        default: break;\n";
+      o << "      }\n";
+      o << "      if (!pass) m &= ~(1ULL << q);\n";
+      o << "    }\n";
+      o << "    s_fm[v] = m;\n";
+      o << "  }\n";
+    }
+    // Masks of the queries that skip each dimension, that carry residual
+    // filters, that have filter-table conjuncts, and of the whole batch.
+    {
+      std::vector<unsigned> joins(shapes.size(), 0u);
+      std::vector<int> has_res(shapes.size(), 0), has_push(shapes.size(), 0);
+      for (size_t s = 0; s < shapes.size(); ++s) {
+        for (const auto& kv : preds[s].joins) joins[s] |= 1u << kv.first;
+        has_res[s] = !preds[s].resid.empty();
+        has_push[s] = !preds[s].pushed.empty();
+      }
+      o << "  if (threadIdx.x < " << dims.size() + 3 << ") {\n";
+      o << "    const int t_ = threadIdx.x;\n";
+      o << "    unsigned long long m = 0ULL;\n";
+      o << "    for (int q = 0; q < nq; ++q) {\n";
+      o << "      unsigned j_ = 0u; int r_ = 0, p_ = 0;\n";
+      o << "      switch (s_sq[q].shape) {\n";
+      for (size_t s = 0; s < shapes.size(); ++s)
+        o << "        case " << s << ": j_ = " << joins[s] << "u; r_ = " << has_res[s] << "; p_ = " << has_push[s] << "; break;\n";
+      o << "        default: break;\n";
+      o << "      }\n";
+      o << "      bool b_ = false;\n";
+      o << "      if (t_ < " << dims.size() << ") b_ = !((j_ >> t_) & 1u);\n";
+      o << "      else if (t_ == " << dims.size() << ") b_ = r_ != 0;\n";
+      o << "      else if (t_ == " << dims.size() + 1 << ") b_ = p_ != 0;\n";
+      o << "      else b_ = true;\n";
+      o << "      if (b_) m |= 1ULL << q;\n";
+      o << "    }\n";
+      o << "    s_nj[t_] = m;\n";
+      o << "  }\n";
+    }
     for (const auto& c : fact_cols) o << "  const int* __restrict__ d_" << c << " = a.col[" << slot_of(c, 0) << "];\n";
-    for (const Dim& d : dims) o << "  const int4* __restrict__ dix_" << lower(d.name) << " = (const int4*)a.ht[" << d.slot << "];\n";
+    for (const Dim& d : dims) {
+      o << "  const int4* __restrict__ dkm_" << lower(d.name) << " = (const int4*)a.ht[" << d.slot << "];\n";
+      if (d.attrs.size() > 1) o << "  const int4* __restrict__ dat_" << lower(d.name) << " = (const int4*)a.dat[" << d.slot << "];\n";
+    }
+    for (int k = 0; k < NFC; ++k) o << "  const unsigned fb" << k << " = (unsigned)a.fbase[" << k << "], fw" << k << " = (unsigned)a.fwin[" << k << "];\n";
     o << "  bool staged_ok = true;\n";
     for (const auto& c : fact_cols) o << "  staged_ok = staged_ok && ((((unsigned long long)d_" << c << ") & 15ULL) == 0ULL);\n";
     o << "  unsigned long long l2_policy = 0;\n";
@@ -1323,13 +1533,14 @@ struct SharedGen {
         << TR * 4 << "u, &bars[(STAGE_)], l2_policy); \\\n";
     o << "  } while (0)\n";
     o << "  __syncthreads();\n";
+    o << "  const unsigned long long m_res = s_nj[" << dims.size() << "], m_push = s_nj[" << dims.size() + 1
+      << "], m_all = s_nj[" << dims.size() + 2 << "];\n";
+    o << "  (void)m_res; (void)m_push;\n";
     o << "  if (threadIdx.x == 0 && staged_ok)\n";
     o << "    for (int k = 0; k < NSTAGE; ++k) {\n";
     o << "      const long long t = (long long)blockIdx.x + (long long)k * gridDim.x;\n";
     o << "      if (t < full_tiles) CX_ISSUE(t, k);\n";
     o << "    }\n";
-    // Units of work per tile: (query, row slice); enough slices to occupy every warp.
-    o << "  const int nq = a.sq_total;\n";
     o << "  const int slices = nq > 0 ? (NWARP + nq - 1) / nq : 1;\n";
     o << "  const int units = nq * slices;\n";
     o << "  long long k_iter = 0;\n";
@@ -1337,6 +1548,7 @@ struct SharedGen {
     o << "  for (long long t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k_iter) {\n";
     o << "    const long long tile_offset = t * TR;\n";
     o << "    const int n_tile = (int)(n_rows - tile_offset < TR ? n_rows - tile_offset : TR);\n";
+    o << "    const int n4 = (n_tile + 3) & ~3;\n";
     o << "    const int stage = (int)(k_iter % NSTAGE);\n";
     o << "    const bool staged = staged_ok && t < full_tiles;\n";
     o << "    bool timed_out = false;\n";
@@ -1351,31 +1563,79 @@ struct SharedGen {
     for (int c = 0; c < NSC; ++c) o << "    const int* S_" << fact_cols[c] << " = tile + " << c << " * TR;\n";
     for (const Dim& d : dims)
       for (const auto& at : d.attrs) o << "    int* S_" << at << " = s_attr + " << attr_slot[at] << " * TR;\n";
-    // Gather every dimension once per row.
-    o << "    for (int i = threadIdx.x; i < n_tile; i += " << CTA << ") {\n";
-    o << "      unsigned hm_ = 0u;\n";
-    const char* comp[] = {"y", "z", "w"};
+    // Phase A: query masks of the tile's rows.
+    o << "    for (int i = threadIdx.x; i < n4; i += " << CTA << ") {\n";
+    o << "      unsigned long long m = 0ULL;\n";
+    o << "      if (i < n_tile) {\n";
+    o << "        m = m_all;\n";
+    o << "        bool oow = false;\n";
+    for (int k = 0; k < NFC; ++k) {
+      o << "        { const unsigned d_ = (unsigned)S_" << fcols[k] << "[i] - fb" << k << ";\n";
+      o << "          if (d_ < fw" << k << ") m &= s_fm[" << k * FW << " + d_]; else oow = true; }\n";
+    }
+    o << "        if (m != 0ULL) {\n";
+    const char* comp[] = {"x", "y", "z"};
     for (size_t di = 0; di < dims.size(); ++di) {
       const Dim& d = dims[di];
-      o << "      {\n";
-      o << "        const int fk_ = S_" << d.fk << "[i];\n";
-      o << "        const int h_ = (int)HASH(fk_, " << d.len << ", " << d.keymin << ");\n";
-      o << "        int4 g_ = make_int4(0, 0, 0, 0);\n";
-      o << "        if ((unsigned)h_ < " << d.len << "u) g_ = __ldg(&dix_" << lower(d.name) << "[h_]);\n";
-      o << "        if (g_.x != 0 && g_.x == fk_) hm_ |= " << (1u << di) << "u;\n";
-      for (size_t k = 0; k < d.attrs.size(); ++k) o << "        S_" << d.attrs[k] << "[i] = g_." << comp[k] << ";\n";
-      o << "      }\n";
+      const std::string dn = lower(d.name);
+      o << "          {\n";
+      o << "            const int fk_ = S_" << d.fk << "[i];\n";
+      o << "            const int h_ = (int)HASH(fk_, " << d.len << ", " << d.keymin << ");\n";
+      o << "            int4 g_ = make_int4(0, 0, 0, 0);\n";
+      o << "            if ((unsigned)h_ < " << d.len << "u) g_ = __ldg(&dkm_" << dn << "[h_]);\n";
+      o << "            const bool hit_ = g_.x != 0 && g_.x == fk_;\n";
+      o << "            m &= hit_ ? (((unsigned long long)(unsigned)g_.z << 32) | (unsigned)g_.y) : s_nj[" << di << "];\n";
+      if (!d.attrs.empty()) o << "            S_" << d.attrs[0] << "[i] = g_.w;\n";
+      if (d.attrs.size() > 1) {
+        o << "            int4 a_ = make_int4(0, 0, 0, 0);\n";
+        o << "            if (hit_) a_ = __ldg(&dat_" << dn << "[h_]);\n";
+        for (size_t k = 1; k < d.attrs.size(); ++k) o << "            S_" << d.attrs[k] << "[i] = a_." << comp[k - 1] << ";\n";
+      }
+      o << "          }\n";
     }
-    o << "      s_hm[i] = (unsigned char)hm_;\n";
+    o << "        }\n";
+    // Residual filters (and filter-table conjuncts of values outside the window).
+    bool any_slow = false;
+    for (size_t s = 0; s < shapes.size(); ++s) any_slow = any_slow || !preds[s].resid.empty() || !preds[s].pushed.empty();
+    if (any_slow) {
+      o << "        unsigned long long r_ = m & (m_res | (oow ? m_push : 0ULL));\n";
+      o << "        while (r_) {\n";
+      o << "          const int q = __ffsll((long long)r_) - 1;\n";
+      o << "          r_ &= r_ - 1ULL;\n";
+      o << "          const int* P = s_params + s_sq[q].param_off; (void)P;\n";
+      o << "          bool pass = true;\n";
+      o << "          switch (s_sq[q].shape) {\n";
+      for (size_t s = 0; s < shapes.size(); ++s) {
+        if (preds[s].resid.empty() && preds[s].pushed.empty()) continue;
+        Emitter e(*shapes[s], tu);
+        e.lit_index = &lit_maps[s];
+        for (const auto& c : fact_cols) e.col_expr[c] = "S_" + c + "[i]";
+        for (const auto& kv : attr_slot) e.col_expr[kv.first] = "S_" + kv.first + "[i]";
+        std::vector<const Expr*> all_pushed;
+        for (const auto& kv : preds[s].pushed) all_pushed.insert(all_pushed.end(), kv.second.begin(), kv.second.end());
+        o << "            case " << s << ": pass = (" << conj_and(e, preds[s].resid) << ") && (!oow || (" << conj_and(e, all_pushed) << ")); break;\n";
+      }
+      o << "            default: break;\n";
+      o << "          }\n";
+      o << "          if (!pass) m &= ~(1ULL << q);\n";
+      o << "        }\n";
+    } else {
+      o << "        (void)oow;\n";
+    }
+    o << "      }\n";
+    o << "      s_mlo[i] = (unsigned)m;\n";
+    o << "      s_mhi[i] = (unsigned)(m >> 32);\n";
     o << "    }\n";
     o << "    __syncthreads();\n";
-    // Query units.
+    // Phase B: query units aggregate the rows whose bit is set.
     o << "    for (int u = warp; u < units; u += NWARP) {\n";
     o << "      const int q_ = u / slices, sl_ = u - q_ * slices;\n";
     o << "      const int per_ = (((n_tile + slices - 1) / slices) + 3) & ~3;\n";
     o << "      const int lo_ = sl_ * per_, hi_ = lo_ + per_ < n_tile ? lo_ + per_ : n_tile;\n";
-    o << "      const CxSQ Q = sq[q_];\n";
+    o << "      const CxSQ& Q = s_sq[q_];\n";
     o << "      const int* P = s_params + Q.param_off; (void)P;\n";
+    o << "      const unsigned* mw_ = q_ < 32 ? s_mlo : s_mhi;\n";
+    o << "      const int qb_ = q_ & 31;\n";
     o << "      switch (Q.shape) {\n";
     for (size_t s = 0; s < shapes.size(); ++s) {
       const Plan& p = *shapes[s];
@@ -1383,78 +1643,40 @@ struct SharedGen {
       e.lit_index = &lit_maps[s];
       const std::string ind = "          ";
       o << "      case " << s << ": {\n";
-      // Row predicate of the shape (filters and dimension joins), in plan order.
-      std::vector<std::string> conds;
-      for (const auto& st : p.steps) {
-        if (st.kind == Step::Filter) {
-          conds.push_back(and_terms({e.valid_of(st.filter.get()), e.value_of(st.filter.get())}));
-          continue;
-        }
-        const Join& j = st.join;
-        size_t di = 0;
-        for (; di < dims.size(); ++di) if (dims[di].name == j.dim) break;
-        std::string c = "((s_hm[i] >> " + std::to_string(di) + ") & 1u)";
-        if (j.filter) c += " && (" + and_terms({e.valid_of(j.filter.get()), e.value_of(j.filter.get())}) + ")";
-        conds.push_back(c);
-      }
-      std::string pred;
-      for (const auto& c : conds) pred += (pred.empty() ? "" : " && ") + std::string("(") + c + ")";
-      if (pred.empty()) pred = "true";
       const int NA = (int)p.aggs.size();
       const int TS = p.storage_ts();
-      // Parameters of this query in registers for the whole unit.
-      for (size_t k = 0; k < lit_maps[s].size(); ++k) o << ind << "const int P" << k << " = P[" << k << "];\n";
-      // Columns the shape reads, four consecutive rows per lane (16-byte shared loads).
       std::vector<std::string> need;
+      for (const auto& g : p.groups) cols_of(g.expr.get(), need);
+      for (const auto& ag : p.aggs) cols_of(ag.arg.get(), need);
+      // Parameters of group and aggregate expressions in registers.
       {
-        std::function<void(const Expr*)> walk = [&](const Expr* x) {
-          if (!x) return;
-          if (x->op == Op::Col && std::find(need.begin(), need.end(), x->name) == need.end()) need.push_back(x->name);
-          for (const auto& kk : x->kids) walk(kk.get());
-        };
-        for (const auto& st : p.steps) walk(st.kind == Step::Filter ? st.filter.get() : st.join.filter.get());
-        for (const auto& g : p.groups) walk(g.expr.get());
-        for (const auto& ag : p.aggs) walk(ag.arg.get());
+        std::vector<const Expr*> ls;
+        for (const auto& g : p.groups) lits_of(g.expr.get(), ls);
+        for (const auto& ag : p.aggs) lits_of(ag.arg.get(), ls);
+        std::set<int> ks;
+        for (const Expr* l : ls) ks.insert(lit_maps[s].at(l));
+        for (int k : ks) o << ind << "const int P" << k << " = P[" << k << "];\n";
       }
+      e.param_regs = true;
       std::string loop_open = ind + "for (int i0_ = lo_ + lane * 4; i0_ < hi_; i0_ += 128) {\n";
+      loop_open += ind + "  const uint4 w4_ = *reinterpret_cast<const uint4*>(mw_ + i0_);\n";
+      loop_open += ind + "  const unsigned b4_ = ((w4_.x >> qb_) & 1u) | (((w4_.y >> qb_) & 1u) << 1) | (((w4_.z >> qb_) & 1u) << 2) | (((w4_.w >> qb_) & 1u) << 3);\n";
+      loop_open += ind + "  if (b4_ == 0u) continue;\n";
       for (const auto& c : need) {
         loop_open += ind + "  int " + c + "[4];\n";
         loop_open += ind + "  { const int4 v_ = *reinterpret_cast<const int4*>(S_" + c + " + i0_); " + c + "[0] = v_.x; " + c +
                      "[1] = v_.y; " + c + "[2] = v_.z; " + c + "[3] = v_.w; }\n";
       }
-      loop_open += ind + "  const unsigned hm4_ = *reinterpret_cast<const unsigned*>(s_hm + i0_); (void)hm4_;\n";
       loop_open += ind + "  #pragma unroll\n" + ind + "  for (int i = 0; i < 4; ++i) {\n";
-      loop_open += ind + "  if (i0_ + i >= hi_) break;\n";
+      loop_open += ind + "  if (!((b4_ >> i) & 1u)) continue;\n";
       const std::string loop_close = ind + "  }\n" + ind + "}\n";
-      e.param_regs = true;
-      // Re-derive the predicate with register parameters and the packed hit mask.
-      {
-        std::vector<std::string> conds2;
-        for (const auto& st : p.steps) {
-          if (st.kind == Step::Filter) {
-            conds2.push_back(and_terms({e.valid_of(st.filter.get()), e.value_of(st.filter.get())}));
-            continue;
-          }
-          const Join& j = st.join;
-          size_t di = 0;
-          for (; di < dims.size(); ++di) if (dims[di].name == j.dim) break;
-          std::string c = "((hm4_ >> (8 * i + " + std::to_string(di) + ")) & 1u)";
-          if (j.filter) c += " && (" + and_terms({e.valid_of(j.filter.get()), e.value_of(j.filter.get())}) + ")";
-          conds2.push_back(c);
-        }
-        pred.clear();
-        for (const auto& c : conds2) pred += (pred.empty() ? "" : " && ") + std::string("(") + c + ")";
-        if (pred.empty()) pred = "true";
-      }
       if (p.groups.empty()) {
         for (int k = 0; k < NA; ++k) o << ind << "unsigned long long s" << k << "_ = 0ULL, c" << k << "_ = 0ULL;\n";
         o << loop_open;
-        o << ind << "  if (!(" << pred << ")) continue;\n";
         for (int k = 0; k < NA; ++k) {
           const Agg& ag = p.aggs[k];
-          const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
           const std::string x = ag.fn == AggFn::Count ? "1ULL" : e.math_push(ag.arg.get(), true);
-          o << ind << "  if (" << v << ") { s" << k << "_ += " << x << "; c" << k << "_ += 1ULL; }\n";
+          o << ind << "  s" << k << "_ += " << x << "; c" << k << "_ += 1ULL;\n";
         }
         o << loop_close;
         for (int k = 0; k < NA; ++k) {
@@ -1487,7 +1709,6 @@ struct SharedGen {
             if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "unsigned tseen" << k << " = 0u;\n";
         }
         o << loop_open;
-        o << ind << "  if (!(" << pred << ")) continue;\n";
         o << terms.str();
         o << ind << "  const int hash = (" << horner << ") % " << G << ";\n";
         o << ind << "  if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
@@ -1496,9 +1717,8 @@ struct SharedGen {
           o << ind << "  ttouch |= 1u << hash;\n";
           for (int k = 0; k < NA; ++k) {
             const Agg& ag = p.aggs[k];
-            const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
             const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
-            o << ind << "  if (" << v << ") { const unsigned long long x_ = " << x << ";\n";
+            o << ind << "  { const unsigned long long x_ = " << x << ";\n";
             o << ind << "    #pragma unroll\n" << ind << "    for (int g = 0; g < " << G << "; ++g) if (hash == g) tacc[g * " << NA << " + " << k << "] += x_;\n";
             if (!p.sparse && ag.fn == AggFn::Sum) o << ind << "    tseen" << k << " |= 1u << hash;\n";
             o << ind << "  }\n";
@@ -1536,9 +1756,8 @@ struct SharedGen {
           int sk = 0;
           for (int k = 0; k < NA; ++k) {
             const Agg& ag = p.aggs[k];
-            const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
             const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
-            o << ind << "    if (" << v << ") { const unsigned long long x_ = " << x << "; if (x_) atomicAdd(&qtab[(long long)hash * " << NA << " + " << k << "], x_);";
+            o << ind << "    { const unsigned long long x_ = " << x << "; if (x_) atomicAdd(&qtab[(long long)hash * " << NA << " + " << k << "], x_);";
             if (!p.sparse && ag.fn == AggFn::Sum) { o << " atomicOr(&qbits[" << TWq * (1 + sk) << "ULL + (hash >> 5)], 1u << (hash & 31));"; ++sk; }
             o << " }\n";
           }
@@ -1548,9 +1767,8 @@ struct SharedGen {
             const Agg& ag = p.aggs[k];
             const int slot = (int)p.groups.size() + k;
             const std::string ix = "(unsigned long long)hash * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
-            const std::string v = ag.arg->op == Op::Star ? "1" : e.valid_of(ag.arg.get());
             const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
-            o << ind << "    if (" << v << ") { const unsigned long long x_ = " << x << "; if (x_) atomicAdd(&d_result[" << ix << "], x_);";
+            o << ind << "    { const unsigned long long x_ = " << x << "; if (x_) atomicAdd(&d_result[" << ix << "], x_);";
             if (!p.sparse && ag.fn == AggFn::Sum) o << " db::atomic_set_valid_bit(d_result_validity, " << ix << ");";
             o << " }\n";
             if (!p.sparse && ag.fn == AggFn::Count) o << ind << "    db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
@@ -1574,8 +1792,8 @@ struct SharedGen {
     o << "  if (aborted) return;\n";
     // Scalar queries: one flush per CTA.
     o << "  __syncthreads();\n";
-    o << "  for (int q = threadIdx.x; q < a.sq_total; q += " << CTA << ") {\n";
-    o << "    const CxSQ Q = sq[q];\n";
+    o << "  for (int q = threadIdx.x; q < nq; q += " << CTA << ") {\n";
+    o << "    const CxSQ& Q = s_sq[q];\n";
     o << "    switch (Q.shape) {\n";
     for (size_t s = 0; s < shapes.size(); ++s) {
       const Plan& p = *shapes[s];
@@ -1594,8 +1812,8 @@ struct SharedGen {
     o << "    }\n";
     o << "  }\n";
     // Grouped queries with shared-memory tables: one flush per CTA.
-    o << "  for (int q = 0; q < a.sq_total; ++q) {\n";
-    o << "    const CxSQ Q = sq[q];\n";
+    o << "  for (int q = 0; q < nq; ++q) {\n";
+    o << "    const CxSQ& Q = s_sq[q];\n";
     o << "    if (Q.smem_acc < 0) continue;\n";
     o << "    unsigned long long* d_result = Q.result; (void)d_result;\n";
     o << "    uint64_t* d_result_validity = (uint64_t*)Q.validity; (void)d_result_validity;\n";

@@ -121,6 +121,9 @@ struct LaunchPlan {
   int fin_vts = 0;
   std::vector<KernelSpec> kernels;
   bool shared = false;
+  int shared_maxq = 256, shared_maxp = 4096;           // queries / parameters per shared launch
+  std::map<int, uint64_t> dat_words;                   // shared scans: extra payload attributes per dimension
+  std::vector<std::pair<int, std::string>> fcols;      // shared scans: fact filter table columns
   struct SShape { uint64_t groups; int ts, grouped, sparse, nlits, smem_ok, naggs; uint64_t tw; int nseen; };
   std::vector<SShape> sshapes;
 };
@@ -165,6 +168,18 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       lp.htv_words[s] = w;
     } else if (k == "shared") {
       lp.shared = true;
+      int mq = 0, mp = 0;
+      if (ls >> mq >> mp) { lp.shared_maxq = mq; lp.shared_maxp = mp; }
+      ls.clear();
+    } else if (k == "dat") {
+      int s; uint64_t w;
+      ls >> s >> w;
+      lp.dat_words[s] = w;
+    } else if (k == "fcol") {
+      int s; std::string n;
+      ls >> s >> n;
+      if (s != (int)lp.fcols.size() || s >= CX_MAX_FCOLS) { err = "filter table columns out of order"; return false; }
+      lp.fcols.emplace_back(s, n);
     } else if (k == "sshape") {
       int i; LaunchPlan::SShape sh;
       ls >> i >> sh.groups >> sh.ts >> sh.grouped >> sh.sparse >> sh.nlits >> sh.smem_ok >> sh.naggs >> sh.tw >> sh.nseen;
@@ -263,6 +278,7 @@ struct cx_exec_ctx {
   std::unordered_map<std::string, std::pair<const void*, uint64_t>> buffers;
   std::unordered_map<std::string, std::pair<const uint64_t*, uint64_t>> nulls;
   std::unordered_map<std::string, uint64_t> rows;
+  std::unordered_map<std::string, std::pair<int64_t, int64_t>> ranges;  // registered column value ranges
   uint64_t* result = nullptr;
   uint64_t result_words = 0;
   uint64_t* validity = nullptr;
@@ -530,6 +546,12 @@ int cx_ctx_set_sm_count(cx_exec_ctx* c, int sms) {
   return CX_OK;
 }
 
+int cx_ctx_set_column_range(cx_exec_ctx* c, const char* name, int64_t lo, int64_t hi) {
+  if (!c || !name || lo > hi) return fail(CX_E_INVALID, "cx_ctx_set_column_range: bad argument");
+  c->ranges[name] = {lo, hi};
+  return CX_OK;
+}
+
 int cx_module_scratch_bytes(const cx_module* m, const cx_exec_ctx* c, uint64_t* bytes) {
   (void)c;
   if (!m || !bytes) return fail(CX_E_INVALID, "cx_module_scratch_bytes: NULL argument");
@@ -764,30 +786,66 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
       return fail(CX_E_CAPACITY, "cx_shared_execute: buffer %s is shorter than its table", col.name.c_str());
     a.col[col.slot] = (const int*)it->second.first;
   }
-  // Queries grouped by shape; validate each query's buffers and parameters.
+  // Filter-table windows from the registered column ranges.
+  for (const auto& fc : lp.fcols) {
+    auto it = c->ranges.find(fc.second);
+    a.fbase[fc.first] = 0;
+    a.fwin[fc.first] = 0;
+    if (it == c->ranges.end()) continue;
+    const int64_t lo = std::max<int64_t>(it->second.first, INT32_MIN);
+    const int64_t hi = std::min<int64_t>(it->second.second, INT32_MAX);
+    if (lo > hi) continue;
+    a.fbase[fc.first] = (int)lo;
+    a.fwin[fc.first] = (int)std::min<int64_t>(256, hi - lo + 1);
+  }
+  // Queries grouped by shape; validate every query before touching the GPU.
   std::vector<int> order;
-  for (int s = 0; s < nshapes; ++s) {
-    a.sq_first[s] = (int)order.size();
+  for (int s = 0; s < nshapes; ++s)
     for (int q = 0; q < nq; ++q)
       if (queries[q].shape == s) order.push_back(q);
-    a.sq_num[s] = (int)order.size() - a.sq_first[s];
-  }
   if ((int)order.size() != nq) return fail(CX_E_INVALID, "cx_shared_execute: a query names a shape outside 0..%d", nshapes - 1);
-  a.sq_total = nq;
-  a.nparams = nparams;
+  for (int i = 0; i < nq; ++i) {
+    const cx_shared_query& q = queries[order[i]];
+    const auto& sh = lp.sshapes[q.shape];
+    const uint64_t need = sh.groups * (uint64_t)sh.ts;
+    if (!q.result || q.result_words < need || !q.validity || q.validity_words < (need + 63) / 64)
+      return fail(CX_E_CAPACITY, "cx_shared_execute: query %d result buffers are smaller than its shape needs (%llu words)", order[i], (unsigned long long)need);
+    if (q.param_off < 0 || q.param_off + sh.nlits > nparams)
+      return fail(CX_E_INVALID, "cx_shared_execute: query %d parameters fall outside the parameter array", order[i]);
+  }
+  // Passes of at most maxq queries; each pass gets its own descriptors and a
+  // compacted parameter array.
+  const int maxq = std::max(1, std::min(lp.shared_maxq, 256));
+  const int npass = (nq + maxq - 1) / maxq;
+  std::vector<int> pass_params(std::max(npass, 1), 0);
+  for (int ps = 0; ps < npass; ++ps) {
+    int np = 0;
+    for (int i = ps * maxq; i < std::min(nq, (ps + 1) * maxq); ++i) np += lp.sshapes[queries[order[i]].shape].nlits;
+    if (np > lp.shared_maxp) return fail(CX_E_CAPACITY, "cx_shared_execute: %d parameters in one pass exceed %d", np, lp.shared_maxp);
+    pass_params[ps] = np;
+  }
 
-  // Scratch: dimension indexes, touched bits per grouped query, descriptors, parameters, error word.
+  // Scratch: dimension slot entries (zeroed per pass), touched bits per grouped
+  // query, per-pass descriptors and parameters, error word.
   uint64_t off = 0;
-  std::vector<uint64_t> dix_off;
-  for (const auto& h : lp.hts) { dix_off.push_back(off); off = align256(off + h.words * 4); }
+  std::vector<uint64_t> dkm_off, dat_off;
+  for (const auto& h : lp.hts) {
+    dkm_off.push_back(off);
+    off = align256(off + h.words * 4);
+    auto it = lp.dat_words.find(h.slot);
+    dat_off.push_back(off);
+    if (it != lp.dat_words.end()) off = align256(off + it->second * 4);
+  }
+  const uint64_t dim_end = off;
   std::vector<uint64_t> touch_off(nq, 0);
   for (int i = 0; i < nq; ++i) {
     const auto& sh = lp.sshapes[queries[order[i]].shape];
     if (sh.grouped) { touch_off[i] = off; off = align256(off + ((sh.groups + 31) / 32) * 4); }
   }
-  const uint64_t zero_end = off;
-  const uint64_t sq_off = off; off = align256(off + (uint64_t)std::max(nq, 1) * sizeof(CxSQ));
-  const uint64_t par_off = off; off = align256(off + (uint64_t)std::max(nparams, 1) * 4);
+  const uint64_t touch_end = off;
+  const size_t desc_bytes = (size_t)maxq * sizeof(CxSQ), par_bytes = (size_t)std::max(lp.shared_maxp, 1) * 4;
+  const size_t pass_bytes = align256(desc_bytes + par_bytes);
+  const uint64_t pass_off = off; off += (uint64_t)std::max(npass, 1) * pass_bytes;
   const uint64_t err_off = off; off = align256(off + 16);
   const uint64_t total = off;
 
@@ -813,13 +871,15 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
     }
     scratch = (char*)c->own_scratch;
   }
-  for (size_t i = 0; i < lp.hts.size(); ++i) a.ht[lp.hts[i].slot] = (int*)(scratch + dix_off[i]);
+  for (size_t i = 0; i < lp.hts.size(); ++i) {
+    a.ht[lp.hts[i].slot] = (int*)(scratch + dkm_off[i]);
+    if (lp.dat_words.count(lp.hts[i].slot)) a.dat[lp.hts[i].slot] = (int*)(scratch + dat_off[i]);
+  }
   a.err = (unsigned int*)(scratch + err_off);
-  a.sq = (const CxSQ*)(scratch + sq_off);
-  a.sparams = (const int*)(scratch + par_off);
 
-  // Host staging of descriptors and parameters (pinned, reused across batches).
-  const size_t stage_bytes = (size_t)std::max(nq, 1) * sizeof(CxSQ) + (size_t)std::max(nparams, 1) * 4;
+  // Host staging of every pass's descriptors and parameters (pinned; the
+  // previous batch's copies finished before the wait above).
+  const size_t stage_bytes = (size_t)std::max(npass, 1) * pass_bytes;
   if (c->host_stage_bytes < stage_bytes) {
     if (c->host_stage) cudaFreeHost(c->host_stage);
     c->host_stage = nullptr;
@@ -827,96 +887,107 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
     CX_CUDA(cudaMallocHost(&c->host_stage, stage_bytes * 2));
     c->host_stage_bytes = stage_bytes * 2;
   }
-  CxSQ* hsq = (CxSQ*)c->host_stage;
-  int* hpar = (int*)((char*)c->host_stage + (size_t)std::max(nq, 1) * sizeof(CxSQ));
-  for (int i = 0; i < nq; ++i) {
-    const cx_shared_query& q = queries[order[i]];
-    const auto& sh = lp.sshapes[q.shape];
-    const uint64_t need = sh.groups * (uint64_t)sh.ts;
-    if (!q.result || q.result_words < need || !q.validity || q.validity_words < (need + 63) / 64)
-      return fail(CX_E_CAPACITY, "cx_shared_execute: query %d result buffers are smaller than its shape needs (%llu words)", order[i], (unsigned long long)need);
-    if (q.param_off < 0 || q.param_off + sh.nlits > nparams)
-      return fail(CX_E_INVALID, "cx_shared_execute: query %d parameters fall outside the parameter array", order[i]);
-    hsq[i].result = (unsigned long long*)q.result;
-    hsq[i].validity = (unsigned long long*)q.validity;
-    hsq[i].touched = sh.grouped ? (unsigned int*)(scratch + touch_off[i]) : nullptr;
-    hsq[i].shape = q.shape;
-    hsq[i].param_off = q.param_off;
-  }
-  if (nparams) memcpy(hpar, params, (size_t)nparams * 4);
-  // Per-query shared-memory group tables, while they fit next to the kernel's
-  // fixed shared memory; the rest aggregate with global atomics.
+
   size_t scan_ki = 0;
-  while (scan_ki < lp.kernels.size() && lp.kernels[scan_ki].kind != "scan" && lp.kernels[scan_ki].kind != "sharedscan") ++scan_ki;
-  const size_t base_smem = scan_ki < lp.kernels.size() ? lp.kernels[scan_ki].smem : 0;
-  uint64_t tab_words = 0, bit_words = 0;
-  for (int i = 0; i < nq; ++i) {
-    const auto& sh = lp.sshapes[hsq[i].shape];
-    hsq[i].smem_acc = -1;
-    hsq[i].smem_bits = 0;
-    if (!sh.smem_ok) continue;
-    const uint64_t tw = tab_words + sh.groups * (uint64_t)sh.naggs;
-    const uint64_t bw = bit_words + sh.tw * (uint64_t)(1 + sh.nseen);
-    if (base_smem + tw * 8 + bw * 4 + 64 > 200 * 1024) continue;
-    hsq[i].smem_acc = (int)tab_words;
-    hsq[i].smem_bits = (int)bit_words;
-    tab_words = tw;
-    bit_words = bw;
-  }
-  a.smem_tab_words = (int)tab_words;
-  a.smem_bit_words = (int)bit_words;
-  const size_t extra_smem = (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
+  while (scan_ki < lp.kernels.size() && lp.kernels[scan_ki].kind != "sharedscan") ++scan_ki;
+  if (scan_ki == lp.kernels.size()) return fail(CX_E_INVALID, "cx_shared_execute: program has no shared scan kernel");
+  const KernelSpec& sk = lp.kernels[scan_ki];
+  // Shared-memory group tables go into the slack the scan's own residency
+  // leaves, so they never cost a resident CTA.
+  const int by_threads = std::max(1, 2048 / std::max(sk.block, 1));
+  const int resident = std::max(1, std::min({sk.ctas_per_sm, by_threads, (int)(233472 / (sk.smem + 1024))}));
+  const size_t smem_cap = std::min<size_t>(200 * 1024, 233472 / resident - 1024);
 
   int sms = c->sm_override;
   if (sms <= 0) CX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   Driver& d = driver();
   int launches = 0, scan_grid = 0;
   void* kparams[] = {&a};
-  auto launch = [&](size_t ki, unsigned grid) -> int {
+  auto launch = [&](size_t ki, unsigned grid, size_t extra) -> int {
     const KernelSpec& k = lp.kernels[ki];
     if (grid == 0) return CX_OK;
-    const unsigned smem = (unsigned)(k.smem + (ki == scan_ki ? extra_smem : 0));
-    CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, smem, (CUstream)stream, kparams, nullptr);
+    CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, (unsigned)(k.smem + extra), (CUstream)stream, kparams, nullptr);
     if (r != CUDA_SUCCESS) return drv_fail(r, k.name.c_str());
     ++launches;
     return CX_OK;
   };
 
   CX_CUDA(cudaEventRecord(c->ev[0], stream));
-  CX_CUDA(cudaMemcpyAsync(scratch + sq_off, c->host_stage, (size_t)std::max(nq, 1) * sizeof(CxSQ), cudaMemcpyHostToDevice, stream));
-  if (nparams) CX_CUDA(cudaMemcpyAsync(scratch + par_off, hpar, (size_t)nparams * 4, cudaMemcpyHostToDevice, stream));
-  CX_CUDA(cudaMemsetAsync(scratch, 0, zero_end, stream));
+  CX_CUDA(cudaMemsetAsync(scratch + dim_end, 0, touch_end - dim_end, stream));
   CX_CUDA(cudaMemsetAsync(scratch + err_off, 0, 16, stream));
   for (int i = 0; i < nq; ++i) {
     const auto& sh = lp.sshapes[queries[order[i]].shape];
     const uint64_t need = sh.groups * (uint64_t)sh.ts;
-    CX_CUDA(cudaMemsetAsync(hsq[i].result, 0, need * 8, stream));
-    CX_CUDA(cudaMemsetAsync(hsq[i].validity, 0, ((need + 63) / 64) * 8, stream));
+    CX_CUDA(cudaMemsetAsync(queries[order[i]].result, 0, need * 8, stream));
+    CX_CUDA(cudaMemsetAsync(queries[order[i]].validity, 0, ((need + 63) / 64) * 8, stream));
   }
-  size_t ki = 0;
-  for (; ki < lp.kernels.size() && ki != scan_ki; ++ki) {
-    const KernelSpec& k = lp.kernels[ki];
-    const long long tiles = (rows[k.table] + k.tile - 1) / k.tile;
-    if ((rc = launch(ki, (unsigned)std::min<long long>(tiles, (long long)sms * 16)))) return rc;
-  }
-  CX_CUDA(cudaEventRecord(c->ev[1], stream));
-  if (ki < lp.kernels.size() && nq > 0) {
-    const KernelSpec& k = lp.kernels[ki];
-    const long long tiles = (rows[0] + k.tile - 1) / k.tile;
-    const long long warps = k.kind == "sharedscan" ? 1 : std::max(1, k.block / 32);
+  for (int ps = 0; ps < npass; ++ps) {
+    const int q0 = ps * maxq, qn = std::min(nq, q0 + maxq) - q0;
+    char* hstage = (char*)c->host_stage + (size_t)ps * pass_bytes;
+    CxSQ* hsq = (CxSQ*)hstage;
+    int* hpar = (int*)(hstage + desc_bytes);
+    int poff = 0;
+    uint64_t tab_words = 0, bit_words = 0;
+    for (int j = 0; j < qn; ++j) {
+      const cx_shared_query& q = queries[order[q0 + j]];
+      const auto& sh = lp.sshapes[q.shape];
+      hsq[j].result = (unsigned long long*)q.result;
+      hsq[j].validity = (unsigned long long*)q.validity;
+      hsq[j].touched = sh.grouped ? (unsigned int*)(scratch + touch_off[q0 + j]) : nullptr;
+      hsq[j].shape = q.shape;
+      hsq[j].param_off = poff;
+      if (sh.nlits) memcpy(hpar + poff, params + q.param_off, (size_t)sh.nlits * 4);
+      poff += sh.nlits;
+      hsq[j].smem_acc = -1;
+      hsq[j].smem_bits = 0;
+      if (!sh.smem_ok) continue;
+      const uint64_t tw = tab_words + sh.groups * (uint64_t)sh.naggs;
+      const uint64_t bw = bit_words + sh.tw * (uint64_t)(1 + sh.nseen);
+      if (sk.smem + tw * 8 + bw * 4 + 64 > smem_cap) continue;
+      hsq[j].smem_acc = (int)tab_words;
+      hsq[j].smem_bits = (int)bit_words;
+      tab_words = tw;
+      bit_words = bw;
+    }
+    a.sq = (const CxSQ*)(scratch + pass_off + (uint64_t)ps * pass_bytes);
+    a.sparams = (const int*)(scratch + pass_off + (uint64_t)ps * pass_bytes + desc_bytes);
+    a.sq_total = qn;
+    a.nparams = poff;
+    a.smem_tab_words = (int)tab_words;
+    a.smem_bit_words = (int)bit_words;
+    for (int s = 0; s < CX_MAX_SHAPES; ++s) { a.sq_first[s] = 0; a.sq_num[s] = 0; }
+    for (int j = 0; j < qn; ++j) {
+      const int s = hsq[j].shape;
+      if (s < CX_MAX_SHAPES) { if (a.sq_num[s] == 0) a.sq_first[s] = j; ++a.sq_num[s]; }
+    }
+    const size_t extra_smem = (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
+    CX_CUDA(cudaMemcpyAsync((void*)a.sq, hstage, (size_t)qn * sizeof(CxSQ), cudaMemcpyHostToDevice, stream));
+    if (poff) CX_CUDA(cudaMemcpyAsync((void*)a.sparams, hpar, (size_t)poff * 4, cudaMemcpyHostToDevice, stream));
+    CX_CUDA(cudaMemsetAsync(scratch, 0, dim_end, stream));
+    size_t ki = 0;
+    for (; ki < scan_ki; ++ki) {
+      const KernelSpec& k = lp.kernels[ki];
+      const long long tiles = (rows[k.table] + k.tile - 1) / k.tile;
+      if ((rc = launch(ki, (unsigned)std::min<long long>(tiles, (long long)sms * 16), 0))) return rc;
+    }
+    if (ps == 0) CX_CUDA(cudaEventRecord(c->ev[1], stream));
     int occ = 1;
-    CUresult orr = d.Occupancy(&occ, L->fns[ki], k.block, k.smem + extra_smem);
+    CUresult orr = d.Occupancy(&occ, L->fns[scan_ki], sk.block, sk.smem + extra_smem);
     if (orr != CUDA_SUCCESS) return drv_fail(orr, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (occ < 1) return fail(CX_E_CAPACITY, "cx_shared_execute: shared scan cannot be resident with %zu bytes of shared memory", k.smem + extra_smem);
-    const int per_sm = std::max(1, std::min(k.ctas_per_sm, occ));
-    const long long grid = std::min<long long>((tiles + warps - 1) / warps, (long long)sms * per_sm);
+    if (occ < 1) return fail(CX_E_CAPACITY, "cx_shared_execute: shared scan cannot be resident with %zu bytes of shared memory", sk.smem + extra_smem);
+    const long long tiles = (rows[0] + sk.tile - 1) / sk.tile;
+    const int per_sm = std::max(1, std::min(sk.ctas_per_sm, occ));
+    const long long grid = std::min<long long>(tiles, (long long)sms * per_sm);
     scan_grid = (int)grid;
-    if ((rc = launch(ki, (unsigned)grid))) return rc;
+    if ((rc = launch(scan_ki, (unsigned)grid, extra_smem))) return rc;
+    if (ps == npass - 1) CX_CUDA(cudaEventRecord(c->ev[2], stream));
+    for (ki = scan_ki + 1; ki < lp.kernels.size(); ++ki)
+      if ((rc = launch(ki, (unsigned)qn, 0))) return rc;
   }
-  if (ki < lp.kernels.size()) ++ki;
-  CX_CUDA(cudaEventRecord(c->ev[2], stream));
-  for (; ki < lp.kernels.size(); ++ki)
-    if ((rc = launch(ki, (unsigned)nq))) return rc;
+  if (npass == 0) {
+    CX_CUDA(cudaEventRecord(c->ev[1], stream));
+    CX_CUDA(cudaEventRecord(c->ev[2], stream));
+  }
   CX_CUDA(cudaMemcpyAsync(c->host_err, a.err, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
   CX_CUDA(cudaEventRecord(c->ev[3], stream));
   c->pending = true;

@@ -107,6 +107,7 @@ class Database:
         self.valid.clear()
         self.rows.clear()
         self.tables.clear()
+        self.__dict__.pop("_colmin", None)
 
     # ------------------------------------------------------------ loading
     def load_column(self, table: str, name: str, data) -> None:
@@ -118,6 +119,18 @@ class Database:
         self.cols[name] = t
         self.rows[table] = int(t.numel()) if table not in self.rows else self.rows[table]
         self.ctx.set_buffer("d_" + name, t.data_ptr(), t.numel())
+        self._register_range(name, t)
+
+    def _register_range(self, name: str, t) -> None:
+        """Records the column's value range: the shared scan's filter tables
+        start at the minimum, and shared joins need non-zero foreign keys."""
+        cache = self.__dict__.setdefault("_colmin", {})
+        if t.numel() == 0:
+            cache[name] = 1
+            return
+        lo, hi = (int(v) for v in self.torch.aminmax(t))
+        cache[name] = lo
+        self.ctx.set_column_range("d_" + name, lo, hi)
 
     def load_validity(self, name: str, words) -> None:
         torch = self.torch
@@ -230,8 +243,7 @@ class Database:
     def column_min(self, name: str) -> int:
         cache = self.__dict__.setdefault("_colmin", {})
         if name not in cache:
-            t = self.cols[name]
-            cache[name] = int(t.min().item()) if t.numel() else 1
+            self._register_range(name, self.cols[name])
         return cache[name]
 
     def shareable(self, plan: Plan) -> bool:

@@ -235,3 +235,61 @@ def test_shared_scan_config2_and_repeat(db):
             ref = oracle_run(p, ht)
             np.testing.assert_array_equal(g.words, ref.words)
             np.testing.assert_array_equal(g.validity, ref.validity)
+
+
+def test_shared_scan_two_passes(db):
+    """A batch larger than one pass (64 queries) runs as consecutive passes
+    over the fact table; every query still equals the oracle."""
+    n = 300_007
+    ht = load(db, 43, n, queries.C4_COLS)
+    plans = queries.batch(90, 4242, n)
+    got = db.execute_shared(plans)
+    assert got[0].kernel_error == 0
+    for p, g in zip(plans, got):
+        ref = oracle_run(p, ht)
+        np.testing.assert_array_equal(g.words, ref.words)
+        np.testing.assert_array_equal(g.validity, ref.validity)
+
+
+@pytest.mark.parametrize("rng_lo,rng_hi", [(40, 45), (1000, 2000), (-300, -100)])
+def test_shared_scan_values_outside_filter_windows(db, rng_lo, rng_hi):
+    """Fact values outside the filter tables' window fall back to per-query
+    evaluation: a registered range that misses most values gives the same
+    answers."""
+    n = 400_009
+    ht = load(db, 44, n, queries.C4_COLS)
+    db.ctx.set_column_range("d_lo_quantity", rng_lo, rng_hi)
+    db.ctx.set_column_range("d_lo_discount", rng_lo, rng_hi)
+    plans = queries.batch(24, 77, n)
+    got = db.execute_shared(plans)
+    for p, g in zip(plans, got):
+        ref = oracle_run(p, ht)
+        np.testing.assert_array_equal(g.words, ref.words)
+        np.testing.assert_array_equal(g.validity, ref.validity)
+
+
+def test_shared_scan_residual_filters(db):
+    """Conjuncts over two fact columns are evaluated per row and query after
+    the mask; they share a batch with filter-table and join-only shapes."""
+    n = 350_011
+    ht = load(db, 45, n, queries.C4_COLS)
+    tables = datagen.ssb_tables(n, queries.C4_COLS)
+    plans = []
+    for k in range(3):
+        b = PlanBuilder(tables, "LINEORDER", name="R")
+        b.filter(and_(col("lo_quantity").lt(col("lo_discount") * lit(5 + k)), col("lo_discount").ge(k)))
+        b.join("DDATE", "lo_orderdate", where=col("d_year").ge(1993 + k))
+        plans.append(b.aggregate([Group(col("d_year"), 1992, 7, False)],
+                                 [("sum", col("lo_revenue")), ("count", star())]))
+    for k in range(2):  # a later filter on a join payload joins the dimension's mask
+        b = PlanBuilder(tables, "LINEORDER", name="PF")
+        b.join("DDATE", "lo_orderdate")
+        b.filter(col("d_year").ne(1994 + k))
+        plans.append(b.aggregate([Group(col("d_year"), 1992, 7, False)], [("count", star())]))
+    rng = random.Random(9)
+    plans += [queries.template(t, rng, n) for t in (0, 1, 3)]
+    got = db.execute_shared(plans)
+    for p, g in zip(plans, got):
+        ref = oracle_run(p, ht)
+        np.testing.assert_array_equal(g.words, ref.words)
+        np.testing.assert_array_equal(g.validity, ref.validity)

@@ -1407,8 +1407,8 @@ struct SharedGen {
     unsigned long long off = 0;
     const unsigned long long stage_off = off; off += (unsigned long long)STAGES * NSC * TR * 4;
     const unsigned long long attr_off = off; off += (unsigned long long)nattr * TR * 4;
-    const unsigned long long mlo_off = off; off += (unsigned long long)TR * 4;
-    const unsigned long long mhi_off = off; off += (unsigned long long)TR * 4;
+    const int NB = TR / 32;  // 32-row blocks per tile
+    const unsigned long long qb_off = off; off += (unsigned long long)MAXQ * NB * 4;
     const unsigned long long bars_off = off; off += (unsigned long long)STAGES * 8;
     off = (off + 15) & ~15ULL;
     const unsigned long long par_off = off; off += (unsigned long long)MAXP * 4;
@@ -1426,14 +1426,14 @@ struct SharedGen {
     meta << "kernel " << kname << " sharedscan 0 " << CTA << " " << TR << " " << smem_total << " " << tu.ctas_per_sm << "\n";
 
     std::ostringstream& o = src;
-    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ") " << kname << "(const CxArgs a) {\n";
+    // At least 32 resident warps per SM: registers are capped at 64.
+    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", " << std::max(1, 1024 / CTA) << ") " << kname << "(const CxArgs a) {\n";
     o << "  constexpr int TR = " << TR << ", NSTAGE = " << STAGES << ", NSC = " << NSC << ", NWARP = " << NW << ";\n";
     o << "  extern __shared__ __align__(1024) unsigned char cx_smem[];\n";
     o << "  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
     o << "  int* stage_buf = (int*)(cx_smem + " << stage_off << ");\n";
     o << "  int* s_attr = (int*)(cx_smem + " << attr_off << "); (void)s_attr;\n";
-    o << "  unsigned* s_mlo = (unsigned*)(cx_smem + " << mlo_off << ");\n";
-    o << "  unsigned* s_mhi = (unsigned*)(cx_smem + " << mhi_off << ");\n";
+    o << "  unsigned* s_qb = (unsigned*)(cx_smem + " << qb_off << ");  // [query][32-row block] row bitmaps\n";
     o << "  unsigned long long* bars = (unsigned long long*)(cx_smem + " << bars_off << ");\n";
     o << "  int* s_params = (int*)(cx_smem + " << par_off << ");\n";
     o << "  unsigned long long* s_qacc = (unsigned long long*)(cx_smem + " << acc_off << ");\n";
@@ -1548,7 +1548,8 @@ struct SharedGen {
     o << "  for (long long t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k_iter) {\n";
     o << "    const long long tile_offset = t * TR;\n";
     o << "    const int n_tile = (int)(n_rows - tile_offset < TR ? n_rows - tile_offset : TR);\n";
-    o << "    const int n4 = (n_tile + 3) & ~3;\n";
+    o << "    const int n32 = (n_tile + 31) & ~31;\n";
+    o << "    const int nblk = n32 >> 5;\n";
     o << "    const int stage = (int)(k_iter % NSTAGE);\n";
     o << "    const bool staged = staged_ok && t < full_tiles;\n";
     o << "    bool timed_out = false;\n";
@@ -1563,37 +1564,64 @@ struct SharedGen {
     for (int c = 0; c < NSC; ++c) o << "    const int* S_" << fact_cols[c] << " = tile + " << c << " * TR;\n";
     for (const Dim& d : dims)
       for (const auto& at : d.attrs) o << "    int* S_" << at << " = s_attr + " << attr_slot[at] << " * TR;\n";
-    // Phase A: query masks of the tile's rows.
-    o << "    for (int i = threadIdx.x; i < n4; i += " << CTA << ") {\n";
-    o << "      unsigned long long m = 0ULL;\n";
-    o << "      if (i < n_tile) {\n";
-    o << "        m = m_all;\n";
-    o << "        bool oow = false;\n";
+    // Phase A: query masks of the tile's rows, RB rows per thread with every
+    // dimension gather of those rows in flight together.
+    const int RB = dims.size() <= 2 ? std::min(IPT, 2) : 1;  // 64 registers hold 8 gathered entries
+    o << "    for (int ib_ = threadIdx.x; ib_ < n32; ib_ += " << CTA * RB << ") {\n";
+    o << "      unsigned long long mk_[" << RB << "];\n";
+    o << "      bool ow_[" << RB << "];\n";
+    o << "      #pragma unroll\n";
+    o << "      for (int j = 0; j < " << RB << "; ++j) {\n";
+    o << "        const int i = ib_ + j * " << CTA << ";\n";
+    o << "        mk_[j] = 0ULL;\n";
+    o << "        ow_[j] = false;\n";
+    o << "        if (i < n_tile) {\n";
+    o << "          unsigned long long m = m_all;\n";
     for (int k = 0; k < NFC; ++k) {
-      o << "        { const unsigned d_ = (unsigned)S_" << fcols[k] << "[i] - fb" << k << ";\n";
-      o << "          if (d_ < fw" << k << ") m &= s_fm[" << k * FW << " + d_]; else oow = true; }\n";
+      o << "          { const unsigned d_ = (unsigned)S_" << fcols[k] << "[i] - fb" << k << ";\n";
+      o << "            if (d_ < fw" << k << ") m &= s_fm[" << k * FW << " + d_]; else ow_[j] = true; }\n";
     }
+    o << "          mk_[j] = m;\n";
+    o << "        }\n";
+    o << "      }\n";
+    for (size_t di = 0; di < dims.size(); ++di) o << "      int4 g" << di << "_[" << RB << "];\n";
+    o << "      #pragma unroll\n";
+    o << "      for (int j = 0; j < " << RB << "; ++j) {\n";
+    o << "        const int i = ib_ + j * " << CTA << ";\n";
+    o << "        const bool live_ = i < n_tile && mk_[j] != 0ULL;\n";
+    for (size_t di = 0; di < dims.size(); ++di) {
+      const Dim& d = dims[di];
+      o << "        {\n";
+      o << "          g" << di << "_[j] = make_int4(0, 0, 0, 0);\n";
+      o << "          const int fk_ = live_ ? S_" << d.fk << "[i] : 0;\n";
+      o << "          const int h_ = (int)HASH(fk_, " << d.len << ", " << d.keymin << ");\n";
+      o << "          if (live_ && (unsigned)h_ < " << d.len << "u) g" << di << "_[j] = __ldg(&dkm_" << lower(d.name) << "[h_]);\n";
+      o << "        }\n";
+    }
+    o << "      }\n";
+    o << "      #pragma unroll\n";
+    o << "      for (int j = 0; j < " << RB << "; ++j) {\n";
+    o << "        const int i = ib_ + j * " << CTA << ";\n";
+    o << "        if (i >= n32) break;  // warp-uniform: blocks are whole warps\n";
+    o << "        unsigned long long m = mk_[j];\n";
+    o << "        const bool oow = ow_[j]; (void)oow;\n";
     o << "        if (m != 0ULL) {\n";
     const char* comp[] = {"x", "y", "z"};
     for (size_t di = 0; di < dims.size(); ++di) {
       const Dim& d = dims[di];
       const std::string dn = lower(d.name);
       o << "          {\n";
-      o << "            const int fk_ = S_" << d.fk << "[i];\n";
-      o << "            const int h_ = (int)HASH(fk_, " << d.len << ", " << d.keymin << ");\n";
-      o << "            int4 g_ = make_int4(0, 0, 0, 0);\n";
-      o << "            if ((unsigned)h_ < " << d.len << "u) g_ = __ldg(&dkm_" << dn << "[h_]);\n";
-      o << "            const bool hit_ = g_.x != 0 && g_.x == fk_;\n";
+      o << "            const int4 g_ = g" << di << "_[j];\n";
+      o << "            const bool hit_ = g_.x != 0 && g_.x == S_" << d.fk << "[i];\n";
       o << "            m &= hit_ ? (((unsigned long long)(unsigned)g_.z << 32) | (unsigned)g_.y) : s_nj[" << di << "];\n";
       if (!d.attrs.empty()) o << "            S_" << d.attrs[0] << "[i] = g_.w;\n";
       if (d.attrs.size() > 1) {
         o << "            int4 a_ = make_int4(0, 0, 0, 0);\n";
-        o << "            if (hit_) a_ = __ldg(&dat_" << dn << "[h_]);\n";
+        o << "            if (hit_) a_ = __ldg(&dat_" << dn << "[(int)HASH(S_" << d.fk << "[i], " << d.len << ", " << d.keymin << ")]);\n";
         for (size_t k = 1; k < d.attrs.size(); ++k) o << "            S_" << d.attrs[k] << "[i] = a_." << comp[k - 1] << ";\n";
       }
       o << "          }\n";
     }
-    o << "        }\n";
     // Residual filters (and filter-table conjuncts of values outside the window).
     bool any_slow = false;
     for (size_t s = 0; s < shapes.size(); ++s) any_slow = any_slow || !preds[s].resid.empty() || !preds[s].pushed.empty();
@@ -1619,23 +1647,28 @@ struct SharedGen {
       o << "          }\n";
       o << "          if (!pass) m &= ~(1ULL << q);\n";
       o << "        }\n";
-    } else {
-      o << "        (void)oow;\n";
     }
+    o << "        }\n";
+    // Transpose the warp's 32 row masks into one word per query.
+    o << "        unsigned wl_ = 0u, wh_ = 0u;\n";
+    o << "        for (int q = 0; q < nq; ++q) {\n";
+    o << "          const unsigned b_ = __ballot_sync(0xffffffffu, (unsigned)(m >> q) & 1u);\n";
+    o << "          if (lane == (q & 31)) { if (q < 32) wl_ = b_; else wh_ = b_; }\n";
+    o << "        }\n";
+    o << "        const int blk_ = i >> 5;\n";
+    o << "        if (lane < nq) s_qb[lane * " << NB << " + blk_] = wl_;\n";
+    o << "        if (lane + 32 < nq) s_qb[(lane + 32) * " << NB << " + blk_] = wh_;\n";
     o << "      }\n";
-    o << "      s_mlo[i] = (unsigned)m;\n";
-    o << "      s_mhi[i] = (unsigned)(m >> 32);\n";
     o << "    }\n";
     o << "    __syncthreads();\n";
     // Phase B: query units aggregate the rows whose bit is set.
     o << "    for (int u = warp; u < units; u += NWARP) {\n";
     o << "      const int q_ = u / slices, sl_ = u - q_ * slices;\n";
-    o << "      const int per_ = (((n_tile + slices - 1) / slices) + 3) & ~3;\n";
-    o << "      const int lo_ = sl_ * per_, hi_ = lo_ + per_ < n_tile ? lo_ + per_ : n_tile;\n";
+    o << "      const int perb_ = (nblk + slices - 1) / slices;\n";
+    o << "      const int blo_ = sl_ * perb_, bhi_ = blo_ + perb_ < nblk ? blo_ + perb_ : nblk;\n";
     o << "      const CxSQ& Q = s_sq[q_];\n";
     o << "      const int* P = s_params + Q.param_off; (void)P;\n";
-    o << "      const unsigned* mw_ = q_ < 32 ? s_mlo : s_mhi;\n";
-    o << "      const int qb_ = q_ & 31;\n";
+    o << "      const unsigned* qw_ = s_qb + q_ * " << NB << ";\n";
     o << "      switch (Q.shape) {\n";
     for (size_t s = 0; s < shapes.size(); ++s) {
       const Plan& p = *shapes[s];
@@ -1658,17 +1691,13 @@ struct SharedGen {
         for (int k : ks) o << ind << "const int P" << k << " = P[" << k << "];\n";
       }
       e.param_regs = true;
-      std::string loop_open = ind + "for (int i0_ = lo_ + lane * 4; i0_ < hi_; i0_ += 128) {\n";
-      loop_open += ind + "  const uint4 w4_ = *reinterpret_cast<const uint4*>(mw_ + i0_);\n";
-      loop_open += ind + "  const unsigned b4_ = ((w4_.x >> qb_) & 1u) | (((w4_.y >> qb_) & 1u) << 1) | (((w4_.z >> qb_) & 1u) << 2) | (((w4_.w >> qb_) & 1u) << 3);\n";
-      loop_open += ind + "  if (b4_ == 0u) continue;\n";
-      for (const auto& c : need) {
-        loop_open += ind + "  int " + c + "[4];\n";
-        loop_open += ind + "  { const int4 v_ = *reinterpret_cast<const int4*>(S_" + c + " + i0_); " + c + "[0] = v_.x; " + c +
-                     "[1] = v_.y; " + c + "[2] = v_.z; " + c + "[3] = v_.w; }\n";
-      }
-      loop_open += ind + "  #pragma unroll\n" + ind + "  for (int i = 0; i < 4; ++i) {\n";
-      loop_open += ind + "  if (!((b4_ >> i) & 1u)) continue;\n";
+      for (const auto& c : need) e.col_expr[c] = "S_" + c + "[i]";
+      // Each lane walks the set bits of its 32-row blocks.
+      std::string loop_open = ind + "for (int b_ = blo_ + lane; b_ < bhi_; b_ += 32) {\n";
+      loop_open += ind + "  unsigned w_ = qw_[b_];\n";
+      loop_open += ind + "  while (w_) {\n";
+      loop_open += ind + "  const int i = (b_ << 5) + __ffs(w_) - 1;\n";
+      loop_open += ind + "  w_ &= w_ - 1u;\n";
       const std::string loop_close = ind + "  }\n" + ind + "}\n";
       if (p.groups.empty()) {
         for (int k = 0; k < NA; ++k) o << ind << "unsigned long long s" << k << "_ = 0ULL, c" << k << "_ = 0ULL;\n";

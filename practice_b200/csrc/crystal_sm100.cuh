@@ -798,4 +798,22 @@ CX_DEVICE void warp_group_add(bool active, int group, unsigned long long v, Appl
   if (lane == leader) apply(group, sum);
 }
 
+// 32x32 bit-matrix transpose across a warp: lane r passes row r; lane c gets
+// column c (bit r of the result = bit c of lane r's row).  Five exchange
+// steps swap the off-diagonal blocks of 16, 8, 4, 2 and 1 bits (the
+// recursive block transpose of Hacker's Delight 7-3, one row per lane).
+// Every lane of the warp must call it.
+CX_DEVICE unsigned warp_transpose32(unsigned x, int lane) {
+  const unsigned masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int j = 16 >> s;
+    const unsigned m = masks[s];
+    const unsigned y = __shfl_xor_sync(0xffffffffu, x, j);
+    x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y << j) & ~m));
+  }
+  return x;
+}
+
 }  // namespace cx
+

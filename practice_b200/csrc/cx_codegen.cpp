@@ -1650,14 +1650,13 @@ struct SharedGen {
     }
     o << "        }\n";
     // Transpose the warp's 32 row masks into one word per query.
-    o << "        unsigned wl_ = 0u, wh_ = 0u;\n";
-    o << "        for (int q = 0; q < nq; ++q) {\n";
-    o << "          const unsigned b_ = __ballot_sync(0xffffffffu, (unsigned)(m >> q) & 1u);\n";
-    o << "          if (lane == (q & 31)) { if (q < 32) wl_ = b_; else wh_ = b_; }\n";
-    o << "        }\n";
     o << "        const int blk_ = i >> 5;\n";
+    o << "        const unsigned wl_ = cx::warp_transpose32((unsigned)m, lane);\n";
     o << "        if (lane < nq) s_qb[lane * " << NB << " + blk_] = wl_;\n";
-    o << "        if (lane + 32 < nq) s_qb[(lane + 32) * " << NB << " + blk_] = wh_;\n";
+    o << "        if (nq > 32) {\n";
+    o << "          const unsigned wh_ = cx::warp_transpose32((unsigned)(m >> 32), lane);\n";
+    o << "          if (lane + 32 < nq) s_qb[(lane + 32) * " << NB << " + blk_] = wh_;\n";
+    o << "        }\n";
     o << "      }\n";
     o << "    }\n";
     o << "    __syncthreads();\n";

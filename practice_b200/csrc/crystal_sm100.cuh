@@ -815,5 +815,37 @@ CX_DEVICE unsigned warp_transpose32(unsigned x, int lane) {
   return x;
 }
 
+// Warp reduce-scatter of P (a power of two <= 32) per-lane u64 values.  Each
+// exchange step halves the values a lane carries: the lane keeps the half its
+// lane bit selects and adds the partner's copy of it; once one value is left
+// the remaining steps are a plain butterfly.  Returns the value index whose
+// warp total the lane then holds in v[0]; lanes with (lane & (32 / P - 1)) == 0
+// hold each index exactly once.  Every lane of the warp must call it.
+template <int P>
+CX_DEVICE int warp_reduce_scatter_u64(unsigned long long (&v)[P], int lane) {
+  static_assert(P >= 1 && P <= 32 && (P & (P - 1)) == 0, "P must be a power of two <= 32");
+  int idx = 0;
+  int cnt = P;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    if (cnt > 1) {
+      const int h = cnt / 2;
+      const bool up = (lane & o) != 0;
+#pragma unroll
+      for (int k = 0; k < h; ++k) {
+        const unsigned long long send = up ? v[k] : v[k + h];
+        const unsigned long long keep = up ? v[k + h] : v[k];
+        v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+      if (up) idx += h;
+      cnt = h;
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+    }
+  }
+  return idx;
+}
+
+
 }  // namespace cx
 

@@ -1416,7 +1416,7 @@ struct SharedGen {
     const unsigned long long acc_off = off; off += (unsigned long long)MAXQ * NACC * 8;
     const unsigned long long sq_off = off; off += (unsigned long long)MAXQ * 40;
     const unsigned long long fm_off = off; off += (unsigned long long)NFC * FW * 8;
-    const unsigned long long nj_off = off; off += (unsigned long long)(dims.size() + 4) * 8;
+    const unsigned long long nj_off = off; off += (unsigned long long)(dims.size() + 3) * 8;
     off = (off + 15) & ~15ULL;
     const unsigned long long tab_off = off;
     const unsigned long long smem_total = (off + 127) & ~127ULL;
@@ -1440,7 +1440,6 @@ struct SharedGen {
     o << "  CxSQ* s_sq = (CxSQ*)(cx_smem + " << sq_off << ");\n";
     o << "  unsigned long long* s_fm = (unsigned long long*)(cx_smem + " << fm_off << "); (void)s_fm;\n";
     o << "  unsigned long long* s_nj = (unsigned long long*)(cx_smem + " << nj_off << ");\n";
-    o << "  int* s_ctr = (int*)(s_nj + " << dims.size() + 3 << ");  // next query unit of the tile\n";
     o << "  unsigned long long* s_tab = (unsigned long long*)(cx_smem + " << tab_off << "); (void)s_tab;\n";
     o << "  unsigned int* s_bits = (unsigned int*)(s_tab + a.smem_tab_words); (void)s_bits;\n";
     o << "  const int nq = a.sq_total < " << MAXQ << " ? a.sq_total : " << MAXQ << ";\n";
@@ -1568,7 +1567,6 @@ struct SharedGen {
     // Phase A: query masks of the tile's rows, RB rows per thread with every
     // dimension gather of those rows in flight together.
     const int RB = dims.size() <= 2 ? std::min(IPT, 2) : 1;  // 64 registers hold 8 gathered entries
-    o << "    if (threadIdx.x == 0) *s_ctr = 0;\n";
     o << "    for (int ib_ = threadIdx.x; ib_ < n32; ib_ += " << CTA * RB << ") {\n";
     o << "      unsigned long long mk_[" << RB << "];\n";
     o << "      bool ow_[" << RB << "];\n";
@@ -1663,13 +1661,7 @@ struct SharedGen {
     o << "    }\n";
     o << "    __syncthreads();\n";
     // Phase B: query units aggregate the rows whose bit is set.
-    // Units are taken in turn from a shared counter: their costs differ by
-    // shape and selectivity, so a static split would idle warps at the barrier.
-    o << "    for (;;) {\n";
-    o << "      int u = 0;\n";
-    o << "      if (lane == 0) u = atomicAdd(s_ctr, 1);\n";
-    o << "      u = __shfl_sync(0xffffffffu, u, 0);\n";
-    o << "      if (u >= units) break;\n";
+    o << "    for (int u = warp; u < units; u += NWARP) {\n";
     o << "      const int q_ = u / slices, sl_ = u - q_ * slices;\n";
     o << "      const int perb_ = (nblk + slices - 1) / slices;\n";
     o << "      const int blo_ = sl_ * perb_, bhi_ = blo_ + perb_ < nblk ? blo_ + perb_ : nblk;\n";
@@ -1737,7 +1729,7 @@ struct SharedGen {
         o << ind << "unsigned long long* qtab = Q.smem_acc >= 0 ? s_tab + Q.smem_acc : nullptr; (void)qtab;\n";
         o << ind << "unsigned int* qbits = s_bits + (Q.smem_acc >= 0 ? Q.smem_bits : 0); (void)qbits;\n";
         const bool tiny = G <= 32 && G * (unsigned long long)NA <= 16;
-        if (tiny && tu.group_merge != 1) {
+        if (tiny && tu.group_merge == 2) {
           // Queries with a shared-memory table add straight into it; the
           // touched / seen bits collect in registers until the unit ends.
           o << ind << "if (qtab) {\n";
@@ -1791,19 +1783,26 @@ struct SharedGen {
             o << ind << "  }\n";
           }
           o << loop_close;
+          // One reduce-scatter of all G x NA partials; the lanes that end up
+          // holding a total apply it.
+          int P2 = 1;
+          while (P2 < (int)(G * NA)) P2 <<= 1;
           o << ind << "ttouch = __reduce_or_sync(0xffffffffu, ttouch);\n";
           for (int k = 0; k < NA; ++k)
             if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "tseen" << k << " = __reduce_or_sync(0xffffffffu, tseen" << k << ");\n";
-          o << ind << "#pragma unroll\n" << ind << "for (int g = 0; g < " << G << "; ++g) {\n";
-          o << ind << "  if (!((ttouch >> g) & 1u)) continue;\n";
+          o << ind << "if (ttouch) {\n";
+          o << ind << "  unsigned long long rv_[" << P2 << "];\n";
+          o << ind << "  #pragma unroll\n" << ind << "  for (int r = 0; r < " << P2 << "; ++r) rv_[r] = r < " << G * NA << " ? tacc[r < " << G * NA << " ? r : 0] : 0ULL;\n";
+          o << ind << "  const int ri_ = cx::warp_reduce_scatter_u64<" << P2 << ">(rv_, lane);\n";
+          o << ind << "  const int g = ri_ / " << NA << ", k_ = ri_ - g * " << NA << "; (void)k_;\n";
+          o << ind << "  if ((lane & " << (32 / P2 - 1) << ") == 0 && ri_ < " << G * NA << " && ((ttouch >> g) & 1u)) {\n";
+          o << ind << "    const unsigned long long s_ = rv_[0];\n";
           int sk = 0;
           for (int k = 0; k < NA; ++k) {
             const int slot = (int)p.groups.size() + k;
             const std::string ix = "(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
-            o << ind << "  { unsigned long long s_ = tacc[g * " << NA << " + " << k << "];\n";
-            o << ind << "    for (int o_ = 16; o_ > 0; o_ >>= 1) s_ += __shfl_xor_sync(0xffffffffu, s_, o_);\n";
-            o << ind << "    if (lane == 0) {\n";
-            o << ind << "      if (qtab) { if (s_) atomicAdd(&qtab[g * " << NA << " + " << k << "], s_); }\n";
+            o << ind << "    if (k_ == " << k << ") {\n";
+            o << ind << "      if (qtab) { if (s_) atomicAdd(&qtab[ri_], s_); }\n";
             o << ind << "      else if (s_) atomicAdd(&d_result[" << ix << "], s_);\n";
             if (!p.sparse) {
               if (p.aggs[k].fn == AggFn::Count) o << ind << "      if (!qtab) db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
@@ -1812,11 +1811,12 @@ struct SharedGen {
                 ++sk;
               }
             }
-            o << ind << "    }\n" << ind << "  }\n";
+            o << ind << "    }\n";
           }
-          o << ind << "  if (lane == 0) { if (qtab) atomicOr(&qbits[g >> 5], 1u << (g & 31)); else atomicOr(&g_touch[g >> 5], 1u << (g & 31)); }\n";
+          o << ind << "  }\n";
+          o << ind << "  if (lane == 0) { if (qtab) atomicOr(&qbits[0], ttouch); else atomicOr(&g_touch[0], ttouch); }\n";
           o << ind << "}\n";
-          if (tu.group_merge != 1) o << ind << "}\n";
+          if (tu.group_merge == 2) o << ind << "}\n";
         } else {
           // Direct per-row updates: shared-memory table when the query has one, else global atomics.
           o << ind << "  if (qtab) {\n";

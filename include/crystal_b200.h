@@ -53,6 +53,7 @@ typedef struct cx_tuning {
   int smem_group_budget; /* bytes a shared-memory group table may use */
   int bitmap_budget;     /* bytes of shared memory for join membership bitmaps (0 = none) */
   int group_merge;       /* 0 auto, 1 merge equal groups within a warp first, 2 per-lane atomics */
+  int producer_warps;    /* shared scans: warps that build query masks (0 = 3/8 of the block) */
 } cx_tuning;
 
 /* Shape of a compiled query's result buffer. */

@@ -657,6 +657,10 @@ CX_DEVICE void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
                : "memory");
 }
 
+CX_DEVICE void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 CX_DEVICE bool mbar_try_wait(unsigned long long* bar, unsigned phase) {
   unsigned ok;
   asm volatile(

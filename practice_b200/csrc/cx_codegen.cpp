@@ -1395,8 +1395,12 @@ struct SharedGen {
     const int CTA = tu.block_threads, IPT = tu.items_per_thread;
     if (CTA % 32 || CTA < 64 || CTA > 1024 || IPT < 1 || IPT > 16) throw PlanError("bad block shape");
     const int NW = CTA / 32, TR = CTA * IPT;
+    if (NW < 3) throw PlanError("shared scan needs at least 3 warps (staging, masks, aggregation)");
+    // Warp roles: warp 0 stages tiles, NPW warps build masks, the rest aggregate.
+    const int NPW = tu.producer_warps > 0 ? std::min(tu.producer_warps, NW - 2) : std::max(1, (NW - 1) * 3 / 8);
+    const int NCW = NW - 1 - NPW;
     const int NSC = (int)fact_cols.size();
-    const int STAGES = std::max(1, tu.stages);
+    int STAGES = std::max(2, tu.stages);
     const int MAXP = MAXQ * std::max(1, max_lits);
     const int NACC = std::max(1, max_scalar_aggs) * 2;  // (sum, count) per scalar aggregate
     const int NFC = (int)fcols.size();
@@ -1404,12 +1408,15 @@ struct SharedGen {
     std::map<std::string, int> attr_slot;
     for (const Dim& d : dims)
       for (const auto& at : d.attrs) attr_slot[at] = nattr++;
+    // Fewer stages when the ring would not leave room for the rest.
+    while (STAGES > 2 && (unsigned long long)STAGES * ((unsigned long long)(NSC + nattr) * TR * 4 + MAXQ * (TR / 32) * 4) > 160 * 1024) --STAGES;
     unsigned long long off = 0;
-    const unsigned long long stage_off = off; off += (unsigned long long)STAGES * NSC * TR * 4;
-    const unsigned long long attr_off = off; off += (unsigned long long)nattr * TR * 4;
     const int NB = TR / 32;  // 32-row blocks per tile
-    const unsigned long long qb_off = off; off += (unsigned long long)MAXQ * NB * 4;
-    const unsigned long long bars_off = off; off += (unsigned long long)STAGES * 8;
+    // Per stage: the fact columns, the payload attributes and the per-query row bitmaps of one tile.
+    const unsigned long long stage_off = off; off += (unsigned long long)STAGES * NSC * TR * 4;
+    const unsigned long long attr_off = off; off += (unsigned long long)STAGES * nattr * TR * 4;
+    const unsigned long long qb_off = off; off += (unsigned long long)STAGES * MAXQ * NB * 4;
+    const unsigned long long bars_off = off; off += (unsigned long long)STAGES * 3 * 8 + 16;
     off = (off + 15) & ~15ULL;
     const unsigned long long par_off = off; off += (unsigned long long)MAXP * 4;
     off = (off + 15) & ~15ULL;
@@ -1428,13 +1435,17 @@ struct SharedGen {
     std::ostringstream& o = src;
     // At least 32 resident warps per SM: registers are capped at 64.
     o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", " << std::max(1, 1024 / CTA) << ") " << kname << "(const CxArgs a) {\n";
-    o << "  constexpr int TR = " << TR << ", NSTAGE = " << STAGES << ", NSC = " << NSC << ", NWARP = " << NW << ";\n";
+    o << "  constexpr int TR = " << TR << ", NSTAGE = " << STAGES << ", NSC = " << NSC << ", NPW = " << NPW << ", NCW = " << NCW << ";\n";
     o << "  extern __shared__ __align__(1024) unsigned char cx_smem[];\n";
     o << "  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
     o << "  int* stage_buf = (int*)(cx_smem + " << stage_off << ");\n";
     o << "  int* s_attr = (int*)(cx_smem + " << attr_off << "); (void)s_attr;\n";
-    o << "  unsigned* s_qb = (unsigned*)(cx_smem + " << qb_off << ");  // [query][32-row block] row bitmaps\n";
-    o << "  unsigned long long* bars = (unsigned long long*)(cx_smem + " << bars_off << ");\n";
+    o << "  unsigned* s_qb = (unsigned*)(cx_smem + " << qb_off << ");  // [stage][query][32-row block] row bitmaps\n";
+    o << "  unsigned long long* bar_full = (unsigned long long*)(cx_smem + " << bars_off << ");   // tile staged\n";
+    o << "  unsigned long long* bar_ready = bar_full + NSTAGE;   // masks built\n";
+    o << "  unsigned long long* bar_empty = bar_full + 2 * NSTAGE;  // aggregation done\n";
+    o << "  volatile int* s_abort = (volatile int*)(bar_full + 3 * NSTAGE);\n";
+    o << "  int* s_nissued = (int*)(bar_full + 3 * NSTAGE) + 1;\n";
     o << "  int* s_params = (int*)(cx_smem + " << par_off << ");\n";
     o << "  unsigned long long* s_qacc = (unsigned long long*)(cx_smem + " << acc_off << ");\n";
     o << "  CxSQ* s_sq = (CxSQ*)(cx_smem + " << sq_off << ");\n";
@@ -1522,57 +1533,87 @@ struct SharedGen {
     for (const auto& c : fact_cols) o << "  staged_ok = staged_ok && ((((unsigned long long)d_" << c << ") & 15ULL) == 0ULL);\n";
     o << "  unsigned long long l2_policy = 0;\n";
     o << "  if (threadIdx.x == 0) {\n";
-    o << "    for (int s = 0; s < NSTAGE; ++s) cx::mbar_init(&bars[s], 1);\n";
+    o << "    for (int s = 0; s < NSTAGE; ++s) {\n";
+    o << "      cx::mbar_init(&bar_full[s], 1);\n";
+    o << "      cx::mbar_init(&bar_ready[s], NPW);\n";
+    o << "      cx::mbar_init(&bar_empty[s], NCW);\n";
+    o << "    }\n";
+    o << "    *s_abort = 0;\n";
+    o << "    *s_nissued = 0;\n";
     o << "    cx::fence_mbar_init();\n";
     o << "    l2_policy = cx::l2_evict_first_policy();\n";
     o << "  }\n";
     o << "#define CX_ISSUE(TILE_, STAGE_) do { \\\n";
-    o << "    cx::mbar_expect_tx(&bars[(STAGE_)], " << (unsigned long long)NSC * TR * 4 << "u); \\\n";
+    o << "    cx::mbar_expect_tx(&bar_full[(STAGE_)], " << (unsigned long long)NSC * TR * 4 << "u); \\\n";
     for (int c = 0; c < NSC; ++c)
       o << "    cx::bulk_g2s(stage_buf + ((STAGE_) * NSC + " << c << ") * TR, d_" << fact_cols[c] << " + (TILE_) * TR, "
-        << TR * 4 << "u, &bars[(STAGE_)], l2_policy); \\\n";
+        << TR * 4 << "u, &bar_full[(STAGE_)], l2_policy); \\\n";
     o << "  } while (0)\n";
     o << "  __syncthreads();\n";
     o << "  const unsigned long long m_res = s_nj[" << dims.size() << "], m_push = s_nj[" << dims.size() + 1
       << "], m_all = s_nj[" << dims.size() + 2 << "];\n";
     o << "  (void)m_res; (void)m_push;\n";
-    o << "  if (threadIdx.x == 0 && staged_ok)\n";
-    o << "    for (int k = 0; k < NSTAGE; ++k) {\n";
-    o << "      const long long t = (long long)blockIdx.x + (long long)k * gridDim.x;\n";
-    o << "      if (t < full_tiles) CX_ISSUE(t, k);\n";
-    o << "    }\n";
-    o << "  const int slices = nq > 0 ? (NWARP + nq - 1) / nq : 1;\n";
+    o << "  const int slices = nq > 0 ? (NCW + nq - 1) / nq : 1;\n";
     o << "  const int units = nq * slices;\n";
-    o << "  long long k_iter = 0;\n";
-    o << "  bool aborted = false;\n";
-    o << "  for (long long t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k_iter) {\n";
-    o << "    const long long tile_offset = t * TR;\n";
-    o << "    const int n_tile = (int)(n_rows - tile_offset < TR ? n_rows - tile_offset : TR);\n";
-    o << "    const int n32 = (n_tile + 31) & ~31;\n";
-    o << "    const int nblk = n32 >> 5;\n";
-    o << "    const int stage = (int)(k_iter % NSTAGE);\n";
-    o << "    const bool staged = staged_ok && t < full_tiles;\n";
-    o << "    bool timed_out = false;\n";
-    o << "    if (staged) timed_out = !cx::mbar_wait_bounded(&bars[stage], (unsigned)((k_iter / NSTAGE) & 1), " << wait_limit << "u);\n";
-    o << "    if (__syncthreads_or(timed_out)) { if (threadIdx.x == 0) cx::raise(a.err, cx::ERR_WAIT_TIMEOUT); aborted = true; break; }\n";
-    o << "    int* tile = stage_buf + stage * NSC * TR;\n";
-    o << "    if (!staged) {\n";  // ragged last tile (or unaligned columns): plain loads into the stage
-    for (int c = 0; c < NSC; ++c)
-      o << "      for (int r = threadIdx.x; r < n_tile; r += " << CTA << ") tile[" << c << " * TR + r] = d_" << fact_cols[c] << "[tile_offset + r];\n";
-    o << "      __syncthreads();\n";
+    const std::string LIM = std::to_string(wait_limit) + "u";
+    // Per-tile views of one stage.
+    auto tile_ptrs = [&](const std::string& ind) {
+      o << ind << "const long long tile_offset = t * TR;\n";
+      o << ind << "const int n_tile = (int)(n_rows - tile_offset < TR ? n_rows - tile_offset : TR);\n";
+      o << ind << "const int nblk = (n_tile + 31) >> 5;\n";
+      o << ind << "int* tile = stage_buf + s * NSC * TR;\n";
+      for (int c = 0; c < NSC; ++c) o << ind << "const int* S_" << fact_cols[c] << " = tile + " << c << " * TR;\n";
+      for (const Dim& d : dims)
+        for (const auto& at : d.attrs)
+          o << ind << "int* S_" << at << " = s_attr + (s * " << nattr << " + " << attr_slot[at] << ") * TR;\n";
+      o << ind << "unsigned* s_qb_t = s_qb + s * " << MAXQ * NB << ";\n";
+    };
+    // Staging warp: refills a stage once the aggregation warps released it.
+    o << "  if (warp == 0) {\n";
+    o << "    if (lane == 0) {\n";
+    o << "      long long k = 0;\n";
+    o << "      for (long long t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k) {\n";
+    o << "        const int s = (int)(k % NSTAGE);\n";
+    o << "        if (k >= NSTAGE && !cx::mbar_wait_bounded(&bar_empty[s], (unsigned)(((k / NSTAGE) - 1) & 1), " << LIM << ")) {\n";
+    o << "          cx::raise(a.err, cx::ERR_WAIT_TIMEOUT);\n";
+    o << "          *s_abort = 1;\n";
+    o << "          break;\n";
+    o << "        }\n";
+    o << "        if (*s_abort) break;\n";
+    o << "        cx::fence_proxy_async_smem();\n";
+    o << "        if (staged_ok && t < full_tiles) CX_ISSUE(t, s); else cx::mbar_arrive(&bar_full[s]);\n";
+    o << "        *s_nissued = (int)(k + 1);\n";
+    o << "      }\n";
     o << "    }\n";
-    for (int c = 0; c < NSC; ++c) o << "    const int* S_" << fact_cols[c] << " = tile + " << c << " * TR;\n";
-    for (const Dim& d : dims)
-      for (const auto& at : d.attrs) o << "    int* S_" << at << " = s_attr + " << attr_slot[at] << " * TR;\n";
+    // Mask warps.
+    o << "  } else if (warp <= NPW) {\n";
+    o << "    const int pw = warp - 1;\n";
+    o << "    long long k = 0;\n";
+    o << "    for (long long t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k) {\n";
+    o << "      const int s = (int)(k % NSTAGE);\n";
+    o << "      const bool ok_ = cx::mbar_wait_bounded(&bar_full[s], (unsigned)((k / NSTAGE) & 1), " << LIM << ");\n";
+    o << "      if (__any_sync(0xffffffffu, !ok_)) { if (lane == 0) { cx::raise(a.err, cx::ERR_WAIT_TIMEOUT); *s_abort = 1; } break; }\n";
+    o << "      if (__any_sync(0xffffffffu, *s_abort != 0)) break;\n";
+    tile_ptrs("      ");
+    o << "      const bool staged = staged_ok && t < full_tiles;\n";
     // Phase A: query masks of the tile's rows, RB rows per thread with every
     // dimension gather of those rows in flight together.
     const int RB = dims.size() <= 2 ? std::min(IPT, 2) : 1;  // 64 registers hold 8 gathered entries
-    o << "    for (int ib_ = threadIdx.x; ib_ < n32; ib_ += " << CTA * RB << ") {\n";
+    o << "    for (int b0_ = pw; b0_ < nblk; b0_ += " << NPW * RB << ") {\n";
+    // Ragged last tile (or unaligned columns): each mask warp loads the rows of its own blocks.
+    o << "      if (!staged) {\n";
+    o << "        for (int j = 0; j < " << RB << "; ++j) {\n";
+    o << "          const int r = ((b0_ + j * NPW) << 5) + lane;\n";
+    o << "          if (r >= n_tile) continue;\n";
+    for (int c = 0; c < NSC; ++c) o << "          tile[" << c << " * TR + r] = d_" << fact_cols[c] << "[tile_offset + r];\n";
+    o << "        }\n";
+    o << "        __syncwarp();\n";
+    o << "      }\n";
     o << "      unsigned long long mk_[" << RB << "];\n";
     o << "      bool ow_[" << RB << "];\n";
     o << "      #pragma unroll\n";
     o << "      for (int j = 0; j < " << RB << "; ++j) {\n";
-    o << "        const int i = ib_ + j * " << CTA << ";\n";
+    o << "        const int i = ((b0_ + j * NPW) << 5) + lane;\n";
     o << "        mk_[j] = 0ULL;\n";
     o << "        ow_[j] = false;\n";
     o << "        if (i < n_tile) {\n";
@@ -1587,7 +1628,7 @@ struct SharedGen {
     for (size_t di = 0; di < dims.size(); ++di) o << "      int4 g" << di << "_[" << RB << "];\n";
     o << "      #pragma unroll\n";
     o << "      for (int j = 0; j < " << RB << "; ++j) {\n";
-    o << "        const int i = ib_ + j * " << CTA << ";\n";
+    o << "        const int i = ((b0_ + j * NPW) << 5) + lane;\n";
     o << "        const bool live_ = i < n_tile && mk_[j] != 0ULL;\n";
     for (size_t di = 0; di < dims.size(); ++di) {
       const Dim& d = dims[di];
@@ -1601,8 +1642,8 @@ struct SharedGen {
     o << "      }\n";
     o << "      #pragma unroll\n";
     o << "      for (int j = 0; j < " << RB << "; ++j) {\n";
-    o << "        const int i = ib_ + j * " << CTA << ";\n";
-    o << "        if (i >= n32) break;  // warp-uniform: blocks are whole warps\n";
+    o << "        const int i = ((b0_ + j * NPW) << 5) + lane;\n";
+    o << "        if (b0_ + j * NPW >= nblk) break;  // warp-uniform: a block is one warp's 32 rows\n";
     o << "        unsigned long long m = mk_[j];\n";
     o << "        const bool oow = ow_[j]; (void)oow;\n";
     o << "        if (m != 0ULL) {\n";
@@ -1652,22 +1693,33 @@ struct SharedGen {
     // Transpose the warp's 32 row masks into one word per query.
     o << "        const int blk_ = i >> 5;\n";
     o << "        const unsigned wl_ = cx::warp_transpose32((unsigned)m, lane);\n";
-    o << "        if (lane < nq) s_qb[lane * " << NB << " + blk_] = wl_;\n";
+    o << "        if (lane < nq) s_qb_t[lane * " << NB << " + blk_] = wl_;\n";
     o << "        if (nq > 32) {\n";
     o << "          const unsigned wh_ = cx::warp_transpose32((unsigned)(m >> 32), lane);\n";
-    o << "          if (lane + 32 < nq) s_qb[(lane + 32) * " << NB << " + blk_] = wh_;\n";
+    o << "          if (lane + 32 < nq) s_qb_t[(lane + 32) * " << NB << " + blk_] = wh_;\n";
     o << "        }\n";
     o << "      }\n";
     o << "    }\n";
-    o << "    __syncthreads();\n";
-    // Phase B: query units aggregate the rows whose bit is set.
-    o << "    for (int u = warp; u < units; u += NWARP) {\n";
+    o << "    __syncwarp();\n";
+    o << "    if (lane == 0) cx::mbar_arrive(&bar_ready[s]);\n";
+    o << "    }\n";
+    // Aggregation warps: query units aggregate the rows whose bit is set.
+    o << "  } else {\n";
+    o << "    const int cw = warp - 1 - NPW;\n";
+    o << "    long long k = 0;\n";
+    o << "    for (long long t = blockIdx.x; t < num_tiles; t += gridDim.x, ++k) {\n";
+    o << "      const int s = (int)(k % NSTAGE);\n";
+    o << "      const bool ok_ = cx::mbar_wait_bounded(&bar_ready[s], (unsigned)((k / NSTAGE) & 1), " << LIM << ");\n";
+    o << "      if (__any_sync(0xffffffffu, !ok_)) { if (lane == 0) { cx::raise(a.err, cx::ERR_WAIT_TIMEOUT); *s_abort = 1; } break; }\n";
+    o << "      if (__any_sync(0xffffffffu, *s_abort != 0)) break;\n";
+    tile_ptrs("      ");
+    o << "    for (int u = cw; u < units; u += NCW) {\n";
     o << "      const int q_ = u / slices, sl_ = u - q_ * slices;\n";
     o << "      const int perb_ = (nblk + slices - 1) / slices;\n";
     o << "      const int blo_ = sl_ * perb_, bhi_ = blo_ + perb_ < nblk ? blo_ + perb_ : nblk;\n";
     o << "      const CxSQ& Q = s_sq[q_];\n";
     o << "      const int* P = s_params + Q.param_off; (void)P;\n";
-    o << "      const unsigned* qw_ = s_qb + q_ * " << NB << ";\n";
+    o << "      const unsigned* qw_ = s_qb_t + q_ * " << NB << ";\n";
     o << "      switch (Q.shape) {\n";
     for (size_t s = 0; s < shapes.size(); ++s) {
       const Plan& p = *shapes[s];
@@ -1850,16 +1902,21 @@ struct SharedGen {
     o << "        default: break;\n";
     o << "      }\n";
     o << "    }\n";
-    o << "    __syncthreads();\n";
-    o << "    if (threadIdx.x == 0 && staged_ok) {\n";
-    o << "      const long long t2 = t + (long long)NSTAGE * gridDim.x;\n";
-    o << "      if (t2 < full_tiles) CX_ISSUE(t2, stage);\n";
+    o << "    __syncwarp();\n";
+    o << "    if (lane == 0) cx::mbar_arrive(&bar_empty[s]);\n";
     o << "    }\n";
     o << "  }\n";
-    o << "  if (aborted && threadIdx.x == 0 && staged_ok) cx::drain_stages(bars, NSTAGE, k_iter, blockIdx.x, gridDim.x, full_tiles, " << wait_limit << "u);\n";
-    o << "  if (aborted) return;\n";
-    // Scalar queries: one flush per CTA.
     o << "  __syncthreads();\n";
+    // After a timeout: wait (bounded) for the copies still in flight, then leave.
+    o << "  if (*s_abort) {\n";
+    o << "    if (threadIdx.x == 0 && staged_ok) {\n";
+    o << "      const int ni = *s_nissued;\n";
+    o << "      for (int kk = ni - NSTAGE < 0 ? 0 : ni - NSTAGE; kk < ni; ++kk)\n";
+    o << "        if ((long long)blockIdx.x + (long long)kk * gridDim.x < full_tiles)\n";
+    o << "          (void)cx::mbar_wait_bounded(&bar_full[kk % NSTAGE], (unsigned)((kk / NSTAGE) & 1), " << LIM << ");\n";
+    o << "    }\n";
+    o << "    return;\n";
+    o << "  }\n";
     o << "  for (int q = threadIdx.x; q < nq; q += " << CTA << ") {\n";
     o << "    const CxSQ& Q = s_sq[q];\n";
     o << "    switch (Q.shape) {\n";

@@ -367,6 +367,7 @@ void cx_tuning_default(cx_tuning* t) {
   t->smem_group_budget = d.smem_group_budget;
   t->bitmap_budget = d.bitmap_budget;
   t->group_merge = d.group_merge;
+  t->producer_warps = d.producer_warps;
 }
 
 int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap, size_t* out_len) {
@@ -383,6 +384,7 @@ int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char*
       t.smem_group_budget = tuning->smem_group_budget;
       t.bitmap_budget = tuning->bitmap_budget;
       t.group_merge = tuning->group_merge;
+      t.producer_warps = tuning->producer_warps;
     }
     const std::string s = cx::generate_cuda(*p, t);
     if (out_len) *out_len = s.size();
@@ -744,6 +746,7 @@ int cx_shared_codegen(const char* const* plans, const size_t* lens, int nshapes,
       t.smem_group_budget = tuning->smem_group_budget;
       t.bitmap_budget = tuning->bitmap_budget;
       t.group_merge = tuning->group_merge;
+      t.producer_warps = tuning->producer_warps;
     }
     const std::string src = cx::generate_shared_cuda(shapes, t);
     if (out_len) *out_len = src.size();

@@ -65,6 +65,11 @@ DEFAULT_CANDIDATES = [
 ]
 
 
+# Shared-scan launch shape before autotuning: one 32-warp CTA per SM, 1024-row
+# tiles, a three-stage ring.
+SHARED_DEFAULT = dict(block_threads=1024, items_per_thread=1, stages=3, ctas_per_sm=1)
+
+
 def make_tuning(**kw) -> _lib.Tuning:
     t = _lib.default_tuning()
     for k, v in kw.items():
@@ -297,6 +302,8 @@ class Database:
     def execute_shared(self, plans: list[Plan], tuning: _lib.Tuning | None = None,
                        stream=None) -> list[QueryResult]:
         torch = self.torch
+        if tuning is None:
+            tuning = self.shared_tuning_for(plans) or make_tuning(**SHARED_DEFAULT)
         prog = self.shared_program(plans, tuning)
         queries, params, bufs = self.shared_prepare(prog, plans)
         for t, n in self.rows.items():

@@ -1717,6 +1717,10 @@ struct SharedGen {
     o << "      const int q_ = u / slices, sl_ = u - q_ * slices;\n";
     o << "      const int perb_ = (nblk + slices - 1) / slices;\n";
     o << "      const int blo_ = sl_ * perb_, bhi_ = blo_ + perb_ < nblk ? blo_ + perb_ : nblk;\n";
+    // Fewer blocks than lanes: lanes share a block, each taking a bit range of its word.
+    o << "      const int lpb_ = perb_ >= 32 ? 1 : perb_ >= 16 ? 2 : perb_ >= 8 ? 4 : perb_ >= 4 ? 8 : perb_ >= 2 ? 16 : 32;\n";
+    o << "      const int bw_ = 32 / lpb_, sub_ = lane % lpb_;\n";
+    o << "      const unsigned bm_ = (bw_ == 32 ? 0xffffffffu : ((1u << bw_) - 1u)) << (sub_ * bw_);\n";
     o << "      const CxSQ& Q = s_sq[q_];\n";
     o << "      const int* P = s_params + Q.param_off; (void)P;\n";
     o << "      const unsigned* qw_ = s_qb_t + q_ * " << NB << ";\n";
@@ -1744,8 +1748,8 @@ struct SharedGen {
       e.param_regs = true;
       for (const auto& c : need) e.col_expr[c] = "S_" + c + "[i]";
       // Each lane walks the set bits of its 32-row blocks.
-      std::string loop_open = ind + "for (int b_ = blo_ + lane; b_ < bhi_; b_ += 32) {\n";
-      loop_open += ind + "  unsigned w_ = qw_[b_];\n";
+      std::string loop_open = ind + "for (int b_ = blo_ + lane / lpb_; b_ < bhi_; b_ += 32 / lpb_) {\n";
+      loop_open += ind + "  unsigned w_ = qw_[b_] & bm_;\n";
       loop_open += ind + "  while (w_) {\n";
       loop_open += ind + "  const int i = (b_ << 5) + __ffs(w_) - 1;\n";
       loop_open += ind + "  w_ &= w_ - 1u;\n";

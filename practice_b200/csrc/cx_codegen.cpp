@@ -1408,14 +1408,30 @@ struct SharedGen {
     std::map<std::string, int> attr_slot;
     for (const Dim& d : dims)
       for (const auto& at : d.attrs) attr_slot[at] = nattr++;
+    // Shapes with a small group domain and literal-free group keys get per-group
+    // row bitmaps (plus one word of out-of-domain rows) built with the masks.
+    std::vector<int> gm_base(shapes.size(), -1);
+    int gm_words = 0;
+    for (size_t si = 0; si < shapes.size(); ++si) {
+      const Plan& p = *shapes[si];
+      if (p.groups.empty() || tu.group_merge == 2) continue;
+      Emitter e(p, tu);
+      const unsigned long long G = e.total_groups();
+      std::vector<const Expr*> gl;
+      for (const auto& g : p.groups) lits_of(g.expr.get(), gl);
+      if (G <= 31 && G * p.aggs.size() <= 16 && gl.empty()) {
+        gm_base[si] = gm_words;
+        gm_words += (int)G + 1;
+      }
+    }
     // Fewer stages when the ring would not leave room for the rest.
-    while (STAGES > 2 && (unsigned long long)STAGES * ((unsigned long long)(NSC + nattr) * TR * 4 + MAXQ * (TR / 32) * 4) > 160 * 1024) --STAGES;
+    while (STAGES > 2 && (unsigned long long)STAGES * ((unsigned long long)(NSC + nattr) * TR * 4 + (MAXQ + gm_words) * (TR / 32) * 4) > 160 * 1024) --STAGES;
     unsigned long long off = 0;
     const int NB = TR / 32;  // 32-row blocks per tile
     // Per stage: the fact columns, the payload attributes and the per-query row bitmaps of one tile.
     const unsigned long long stage_off = off; off += (unsigned long long)STAGES * NSC * TR * 4;
     const unsigned long long attr_off = off; off += (unsigned long long)STAGES * nattr * TR * 4;
-    const unsigned long long qb_off = off; off += (unsigned long long)STAGES * MAXQ * NB * 4;
+    const unsigned long long gm_off = off; off += (unsigned long long)STAGES * gm_words * NB * 4;
     const unsigned long long bars_off = off; off += (unsigned long long)STAGES * 3 * 8 + 16;
     off = (off + 15) & ~15ULL;
     const unsigned long long par_off = off; off += (unsigned long long)MAXP * 4;
@@ -1425,9 +1441,13 @@ struct SharedGen {
     const unsigned long long fm_off = off; off += (unsigned long long)NFC * FW * 8;
     const unsigned long long nj_off = off; off += (unsigned long long)(dims.size() + 3) * 8;
     off = (off + 15) & ~15ULL;
-    const unsigned long long tab_off = off;
-    const unsigned long long smem_total = (off + 127) & ~127ULL;
-    if (smem_total > 200 * 1024) throw PlanError("shared scan shared memory exceeds 200 KB before group tables");
+    // The per-query row bitmaps (STAGES x NB words per query of the pass) and
+    // the group tables follow the fixed part; the host sizes both per pass.
+    const unsigned long long qb_off = (off + 15) & ~15ULL;
+    const unsigned long long smem_total = qb_off;
+    if (smem_total + (unsigned long long)MAXQ * STAGES * NB * 4 > 200 * 1024)
+      throw PlanError("shared scan shared memory exceeds 200 KB before group tables");
+    meta << "sqb " << STAGES * NB * 4 << "\n";
     const unsigned wait_limit = 1u << std::min(30, std::max(10, tu.wait_limit_log2));
     const std::string kname = "SharedScan_" + fact;
     meta << "kernel " << kname << " sharedscan 0 " << CTA << " " << TR << " " << smem_total << " " << tu.ctas_per_sm << "\n";
@@ -1441,6 +1461,8 @@ struct SharedGen {
     o << "  int* stage_buf = (int*)(cx_smem + " << stage_off << ");\n";
     o << "  int* s_attr = (int*)(cx_smem + " << attr_off << "); (void)s_attr;\n";
     o << "  unsigned* s_qb = (unsigned*)(cx_smem + " << qb_off << ");  // [stage][query][32-row block] row bitmaps\n";
+    o << "  const int nq_ = a.sq_total < " << MAXQ << " ? a.sq_total : " << MAXQ << ";\n";
+    o << "  unsigned* s_gm = (unsigned*)(cx_smem + " << gm_off << "); (void)s_gm;  // [stage][shape group][32-row block]\n";
     o << "  unsigned long long* bar_full = (unsigned long long*)(cx_smem + " << bars_off << ");   // tile staged\n";
     o << "  unsigned long long* bar_ready = bar_full + NSTAGE;   // masks built\n";
     o << "  unsigned long long* bar_empty = bar_full + 2 * NSTAGE;  // aggregation done\n";
@@ -1451,7 +1473,7 @@ struct SharedGen {
     o << "  CxSQ* s_sq = (CxSQ*)(cx_smem + " << sq_off << ");\n";
     o << "  unsigned long long* s_fm = (unsigned long long*)(cx_smem + " << fm_off << "); (void)s_fm;\n";
     o << "  unsigned long long* s_nj = (unsigned long long*)(cx_smem + " << nj_off << ");\n";
-    o << "  unsigned long long* s_tab = (unsigned long long*)(cx_smem + " << tab_off << "); (void)s_tab;\n";
+    o << "  unsigned long long* s_tab = (unsigned long long*)(cx_smem + " << qb_off << " + ((NSTAGE * nq_ * " << NB * 4 << " + 15) & ~15)); (void)s_tab;\n";
     o << "  unsigned int* s_bits = (unsigned int*)(s_tab + a.smem_tab_words); (void)s_bits;\n";
     o << "  const int nq = a.sq_total < " << MAXQ << " ? a.sq_total : " << MAXQ << ";\n";
     o << "  const long long n_rows = a.rows[0];\n";
@@ -1566,7 +1588,8 @@ struct SharedGen {
       for (const Dim& d : dims)
         for (const auto& at : d.attrs)
           o << ind << "int* S_" << at << " = s_attr + (s * " << nattr << " + " << attr_slot[at] << ") * TR;\n";
-      o << ind << "unsigned* s_qb_t = s_qb + s * " << MAXQ * NB << ";\n";
+      o << ind << "unsigned* s_qb_t = s_qb + s * nq * " << NB << ";\n";
+      o << ind << "unsigned* s_gm_t = s_gm + s * " << gm_words * NB << "; (void)s_gm_t;\n";
     };
     // Staging warp: refills a stage once the aggregation warps released it.
     o << "  if (warp == 0) {\n";
@@ -1690,8 +1713,37 @@ struct SharedGen {
       o << "        }\n";
     }
     o << "        }\n";
-    // Transpose the warp's 32 row masks into one word per query.
     o << "        const int blk_ = i >> 5;\n";
+    for (size_t si = 0; si < shapes.size(); ++si) {
+      if (gm_base[si] < 0) continue;
+      const Plan& p = *shapes[si];
+      Emitter e(p, tu);
+      for (const auto& c : fact_cols) e.col_expr[c] = "S_" + c + "[i]";
+      for (const auto& kv : attr_slot) e.col_expr[kv.first] = "S_" + kv.first + "[i]";
+      const unsigned long long G = e.total_groups();
+      std::string horner, dom;
+      o << "        {  // group rows of shape " << si << "\n";
+      o << "          int h_ = " << G << ";\n";
+      o << "          bool bad_ = false;\n";
+      o << "          if (m != 0ULL) {\n";
+      for (size_t k = 0; k < p.groups.size(); ++k) {
+        o << "            const int gt" << k << " = " << e.group_term(k) << ";\n";
+        horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(e.eff_card(k)) + " + gt" + std::to_string(k) + ")";
+        dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " + std::to_string(e.eff_card(k)) + "u";
+      }
+      o << "            const int hash = (" << horner << ") % " << G << ";\n";
+      o << "            bad_ = !(" << dom << ");\n";
+      o << "            h_ = (unsigned)hash < " << G << "u ? hash : " << G << ";\n";
+      o << "          }\n";
+      o << "          unsigned gw_ = 0u;\n";
+      o << "          #pragma unroll\n";
+      o << "          for (int g = 0; g < " << G << "; ++g) { const unsigned b_ = __ballot_sync(0xffffffffu, h_ == g); if (lane == g) gw_ = b_; }\n";
+      o << "          const unsigned bb_ = __ballot_sync(0xffffffffu, bad_);\n";
+      o << "          if (lane == " << G << ") gw_ = bb_;\n";
+      o << "          if (lane <= " << G << ") s_gm_t[(" << gm_base[si] << " + lane) * " << NB << " + blk_] = gw_;\n";
+      o << "        }\n";
+    }
+    // Transpose the warp's 32 row masks into one word per query.
     o << "        const unsigned wl_ = cx::warp_transpose32((unsigned)m, lane);\n";
     o << "        if (lane < nq) s_qb_t[lane * " << NB << " + blk_] = wl_;\n";
     o << "        if (nq > 32) {\n";
@@ -1784,6 +1836,78 @@ struct SharedGen {
         o << ind << "unsigned int* g_touch = Q.touched; (void)g_touch;\n";
         o << ind << "unsigned long long* qtab = Q.smem_acc >= 0 ? s_tab + Q.smem_acc : nullptr; (void)qtab;\n";
         o << ind << "unsigned int* qbits = s_bits + (Q.smem_acc >= 0 ? Q.smem_bits : 0); (void)qbits;\n";
+        // Flush of a unit's register partials: one reduce-scatter of all G x NA
+        // values; the lanes that end up holding a total apply it.
+        auto tiny_flush = [&]() {
+          int P2 = 1;
+          while (P2 < (int)(G * NA)) P2 <<= 1;
+          o << ind << "ttouch = __reduce_or_sync(0xffffffffu, ttouch);\n";
+          for (int k = 0; k < NA; ++k)
+            if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "tseen" << k << " = __reduce_or_sync(0xffffffffu, tseen" << k << ");\n";
+          o << ind << "if (ttouch) {\n";
+          o << ind << "  unsigned long long rv_[" << P2 << "];\n";
+          o << ind << "  #pragma unroll\n" << ind << "  for (int r = 0; r < " << P2 << "; ++r) rv_[r] = r < " << G * NA << " ? tacc[r < " << G * NA << " ? r : 0] : 0ULL;\n";
+          o << ind << "  const int ri_ = cx::warp_reduce_scatter_u64<" << P2 << ">(rv_, lane);\n";
+          o << ind << "  const int g = ri_ / " << NA << ", k_ = ri_ - g * " << NA << "; (void)k_;\n";
+          o << ind << "  if ((lane & " << (32 / P2 - 1) << ") == 0 && ri_ < " << G * NA << " && ((ttouch >> g) & 1u)) {\n";
+          o << ind << "    const unsigned long long s_ = rv_[0];\n";
+          int sk = 0;
+          for (int k = 0; k < NA; ++k) {
+            const int slot = (int)p.groups.size() + k;
+            const std::string ix = "(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
+            o << ind << "    if (k_ == " << k << ") {\n";
+            o << ind << "      if (qtab) { if (s_) atomicAdd(&qtab[ri_], s_); }\n";
+            o << ind << "      else if (s_) atomicAdd(&d_result[" << ix << "], s_);\n";
+            if (!p.sparse) {
+              if (p.aggs[k].fn == AggFn::Count) o << ind << "      if (!qtab) db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+              else {
+                o << ind << "      if ((tseen" << k << " >> g) & 1u) { if (qtab) atomicOr(&qbits[" << TWq * (1 + sk) << "ULL + (g >> 5)], 1u << (g & 31)); else db::atomic_set_valid_bit(d_result_validity, " << ix << "); }\n";
+                ++sk;
+              }
+            }
+            o << ind << "    }\n";
+          }
+          o << ind << "  }\n";
+          o << ind << "  if (lane == 0) { if (qtab) atomicOr(&qbits[0], ttouch); else atomicOr(&g_touch[0], ttouch); }\n";
+          o << ind << "}\n";
+        };
+        if (gm_base[s] >= 0) {
+          // Group row bitmaps: per block and group, the query's rows of that
+          // group; COUNT is a popcount, SUM walks the rows.
+          o << ind << "unsigned long long tacc[" << G * NA << "];\n";
+          o << ind << "#pragma unroll\n" << ind << "for (int r = 0; r < " << G * NA << "; ++r) tacc[r] = 0ULL;\n";
+          o << ind << "unsigned ttouch = 0u;\n";
+          o << ind << "const unsigned* gm_ = s_gm_t + " << gm_base[s] << " * " << NB << ";\n";
+          o << ind << "for (int b_ = blo_ + lane / lpb_; b_ < bhi_; b_ += 32 / lpb_) {\n";
+          o << ind << "  const unsigned w_ = qw_[b_] & bm_;\n";
+          o << ind << "  if (!w_) continue;\n";
+          o << ind << "  if (w_ & gm_[" << G << " * " << NB << " + b_]) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+          o << ind << "  #pragma unroll\n";
+          o << ind << "  for (int g = 0; g < " << G << "; ++g) {\n";
+          o << ind << "    unsigned wg_ = w_ & gm_[g * " << NB << " + b_];\n";
+          o << ind << "    if (!wg_) continue;\n";
+          o << ind << "    ttouch |= 1u << g;\n";
+          bool any_sum = false;
+          for (int k = 0; k < NA; ++k) {
+            if (p.aggs[k].fn == AggFn::Count) o << ind << "    tacc[g * " << NA << " + " << k << "] += (unsigned long long)__popc(wg_);\n";
+            else any_sum = true;
+          }
+          if (any_sum) {
+            o << ind << "    while (wg_) {\n";
+            o << ind << "      const int i = (b_ << 5) + __ffs(wg_) - 1;\n";
+            o << ind << "      wg_ &= wg_ - 1u;\n";
+            for (int k = 0; k < NA; ++k)
+              if (p.aggs[k].fn == AggFn::Sum)
+                o << ind << "      tacc[g * " << NA << " + " << k << "] += (unsigned long long)(" << e.math_push(p.aggs[k].arg.get(), true) << ");\n";
+            o << ind << "    }\n";
+          }
+          o << ind << "  }\n";
+          o << ind << "}\n";
+          // No nullable columns in a shared shape: a SUM is valid wherever its group was touched.
+          for (int k = 0; k < NA; ++k)
+            if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "unsigned tseen" << k << " = ttouch;\n";
+          tiny_flush();
+        } else {
         const bool tiny = G <= 32 && G * (unsigned long long)NA <= 16;
         if (tiny && tu.group_merge == 2) {
           // Queries with a shared-memory table add straight into it; the
@@ -1839,39 +1963,7 @@ struct SharedGen {
             o << ind << "  }\n";
           }
           o << loop_close;
-          // One reduce-scatter of all G x NA partials; the lanes that end up
-          // holding a total apply it.
-          int P2 = 1;
-          while (P2 < (int)(G * NA)) P2 <<= 1;
-          o << ind << "ttouch = __reduce_or_sync(0xffffffffu, ttouch);\n";
-          for (int k = 0; k < NA; ++k)
-            if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "tseen" << k << " = __reduce_or_sync(0xffffffffu, tseen" << k << ");\n";
-          o << ind << "if (ttouch) {\n";
-          o << ind << "  unsigned long long rv_[" << P2 << "];\n";
-          o << ind << "  #pragma unroll\n" << ind << "  for (int r = 0; r < " << P2 << "; ++r) rv_[r] = r < " << G * NA << " ? tacc[r < " << G * NA << " ? r : 0] : 0ULL;\n";
-          o << ind << "  const int ri_ = cx::warp_reduce_scatter_u64<" << P2 << ">(rv_, lane);\n";
-          o << ind << "  const int g = ri_ / " << NA << ", k_ = ri_ - g * " << NA << "; (void)k_;\n";
-          o << ind << "  if ((lane & " << (32 / P2 - 1) << ") == 0 && ri_ < " << G * NA << " && ((ttouch >> g) & 1u)) {\n";
-          o << ind << "    const unsigned long long s_ = rv_[0];\n";
-          int sk = 0;
-          for (int k = 0; k < NA; ++k) {
-            const int slot = (int)p.groups.size() + k;
-            const std::string ix = "(unsigned long long)g * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
-            o << ind << "    if (k_ == " << k << ") {\n";
-            o << ind << "      if (qtab) { if (s_) atomicAdd(&qtab[ri_], s_); }\n";
-            o << ind << "      else if (s_) atomicAdd(&d_result[" << ix << "], s_);\n";
-            if (!p.sparse) {
-              if (p.aggs[k].fn == AggFn::Count) o << ind << "      if (!qtab) db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
-              else {
-                o << ind << "      if ((tseen" << k << " >> g) & 1u) { if (qtab) atomicOr(&qbits[" << TWq * (1 + sk) << "ULL + (g >> 5)], 1u << (g & 31)); else db::atomic_set_valid_bit(d_result_validity, " << ix << "); }\n";
-                ++sk;
-              }
-            }
-            o << ind << "    }\n";
-          }
-          o << ind << "  }\n";
-          o << ind << "  if (lane == 0) { if (qtab) atomicOr(&qbits[0], ttouch); else atomicOr(&g_touch[0], ttouch); }\n";
-          o << ind << "}\n";
+          tiny_flush();
           if (tu.group_merge == 2) o << ind << "}\n";
         } else {
           // Direct per-row updates: shared-memory table when the query has one, else global atomics.
@@ -1899,6 +1991,7 @@ struct SharedGen {
           }
           o << ind << "  }\n";
           o << loop_close;
+        }
         }
       }
       o << "        break; }\n";

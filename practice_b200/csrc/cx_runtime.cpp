@@ -122,6 +122,7 @@ struct LaunchPlan {
   std::vector<KernelSpec> kernels;
   bool shared = false;
   int shared_maxq = 256, shared_maxp = 4096;           // queries / parameters per shared launch
+  uint64_t shared_qb_bytes = 0;                        // shared memory of row bitmaps per query of a pass
   std::map<int, uint64_t> dat_words;                   // shared scans: extra payload attributes per dimension
   std::vector<std::pair<int, std::string>> fcols;      // shared scans: fact filter table columns
   struct SShape { uint64_t groups; int ts, grouped, sparse, nlits, smem_ok, naggs; uint64_t tw; int nseen; };
@@ -171,6 +172,8 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       int mq = 0, mp = 0;
       if (ls >> mq >> mp) { lp.shared_maxq = mq; lp.shared_maxp = mp; }
       ls.clear();
+    } else if (k == "sqb") {
+      ls >> lp.shared_qb_bytes;
     } else if (k == "dat") {
       int s; uint64_t w;
       ls >> s >> w;
@@ -898,7 +901,8 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
   // Shared-memory group tables go into the slack the scan's own residency
   // leaves, so they never cost a resident CTA.
   const int by_threads = std::max(1, 2048 / std::max(sk.block, 1));
-  const int resident = std::max(1, std::min({sk.ctas_per_sm, by_threads, (int)(233472 / (sk.smem + 1024))}));
+  const size_t qb_max = (size_t)lp.shared_qb_bytes * (size_t)std::min(nq, maxq) + 16;
+  const int resident = std::max(1, std::min({sk.ctas_per_sm, by_threads, (int)(233472 / (sk.smem + qb_max + 1024))}));
   const size_t smem_cap = std::min<size_t>(200 * 1024, 233472 / resident - 1024);
 
   int sms = c->sm_override;
@@ -931,6 +935,7 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
     int* hpar = (int*)(hstage + desc_bytes);
     int poff = 0;
     uint64_t tab_words = 0, bit_words = 0;
+    const size_t qb_bytes = ((size_t)lp.shared_qb_bytes * (size_t)qn + 15) & ~(size_t)15;
     for (int j = 0; j < qn; ++j) {
       const cx_shared_query& q = queries[order[q0 + j]];
       const auto& sh = lp.sshapes[q.shape];
@@ -946,7 +951,7 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
       if (!sh.smem_ok) continue;
       const uint64_t tw = tab_words + sh.groups * (uint64_t)sh.naggs;
       const uint64_t bw = bit_words + sh.tw * (uint64_t)(1 + sh.nseen);
-      if (sk.smem + tw * 8 + bw * 4 + 64 > smem_cap) continue;
+      if (sk.smem + qb_bytes + tw * 8 + bw * 4 + 64 > smem_cap) continue;
       hsq[j].smem_acc = (int)tab_words;
       hsq[j].smem_bits = (int)bit_words;
       tab_words = tw;
@@ -963,7 +968,7 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
       const int s = hsq[j].shape;
       if (s < CX_MAX_SHAPES) { if (a.sq_num[s] == 0) a.sq_first[s] = j; ++a.sq_num[s]; }
     }
-    const size_t extra_smem = (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
+    const size_t extra_smem = qb_bytes + (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
     CX_CUDA(cudaMemcpyAsync((void*)a.sq, hstage, (size_t)qn * sizeof(CxSQ), cudaMemcpyHostToDevice, stream));
     if (poff) CX_CUDA(cudaMemcpyAsync((void*)a.sparams, hpar, (size_t)poff * 4, cudaMemcpyHostToDevice, stream));
     CX_CUDA(cudaMemsetAsync(scratch, 0, dim_end, stream));

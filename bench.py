@@ -193,7 +193,7 @@ def reference_arm(args):
 
 
 def config_block(args):
-    return {"workload": "config4: batched star-join queries, 600M-row fact, 4 templates",
+    return {"workload": "batched star-join queries from 4 templates over a 600M-row, 8-column int32 fact table",
             "fact_rows": args.rows, "fact_columns": 8, "batch_queries": args.batch, "mode": args.mode,
             "seed": args.seed, "parallelism": f"replicas{args.gpus}",
             "l2": "inputs (19.2 GB) larger than L2 (126 MB); no flush needed"}
@@ -203,9 +203,9 @@ def config_block(args):
 
 PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=98304)
                     for bt, ipt, st in ((1024, 2, 0), (1024, 4, 0), (512, 2, 0), (512, 8, 2), (1024, 4, 2))]
-SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16)
-                     for bt, ipt, st in ((512, 2, 2), (256, 4, 2), (1024, 1, 2), (512, 4, 2), (1024, 2, 2),
-                                         (256, 8, 2), (512, 2, 3))]
+SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=2, producer_warps=pw)
+                     for bt, ipt, st, pw in ((1024, 1, 3, 11), (1024, 1, 3, 17), (1024, 1, 3, 14), (512, 2, 2, 5),
+                                             (512, 2, 2, 7))]
 
 
 def time_steps(torch, stream, steps, run_step, sampler=None):

@@ -159,7 +159,7 @@ def cpu_baseline(plans_full, args, batch_rows: int):
     from practice_b200 import datagen, queries
 
     n = min(args.cpu_sample_rows, batch_rows)
-    ht = datagen.host_tables(args.seed, n, queries.C4_COLS)
+    ht = datagen.host_tables(args.seed, n, queries.BATCH_COLS)
     plans = queries.batch(args.batch, args.seed, n)
     t, kind, cores = refbase.time_batch(plans, ht, n)
     scale = batch_rows / n
@@ -243,7 +243,7 @@ def main():
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     db = Database(local)
-    db.generate_ssb(args.rows, args.seed + rank, queries.C4_COLS)
+    db.generate_ssb(args.rows, args.seed + rank, queries.BATCH_COLS)
     plans = queries.batch(args.batch, args.seed, args.rows)
     stream = torch.cuda.Stream(device)
     peak, peak_kind = peaks()

@@ -1,12 +1,12 @@
 """Query plans of the measured workloads and of the reference's known-answer set.
 
-* ``config1`` -- plain single query over a 6M-row fact table: date join with
+* ``ssb_q11`` -- plain single query over a 6M-row fact table: date join with
   year = 1995 (PHT_1), discount in [2, 4], quantity < 30,
   SUM(extendedprice * discount) (SSB Q1.1 shape, test/queries/sql/q11.sql).
-* ``config2`` -- four-dimension star: customer region = r, supplier region = r,
+* ``ssb_q31`` -- four-dimension star: customer region = r, supplier region = r,
   year in [1992, 1997], GROUP BY (c_nation, s_nation, d_year), SUM(revenue),
   ORDER BY year ASC, sum DESC (SSB Q3.1 shape, test/queries/sql/q31.sql).
-* ``config3`` -- the nullable three-valued-logic variant: NULL revenue and
+* ``ssb_q31_nullable`` -- the nullable three-valued-logic variant: NULL revenue and
   NULL customer.city, IS NULL / IS NOT NULL and range predicates that yield
   UNKNOWN; COUNT(*), COUNT(revenue), SUM(revenue) grouped by a nullable key.
 * ``template(t, rng)`` -- the four shared-scan templates: T0 range filters +
@@ -21,9 +21,9 @@ import random
 from .datagen import GROUP_STATS, ssb_tables
 from .plan import Group, Plan, PlanBuilder, Table, and_, case, col, lit, not_, or_, star
 
-C1_COLS = ["lo_orderdate", "lo_quantity", "lo_discount", "lo_extendedprice"]
-C2_COLS = ["lo_orderdate", "lo_custkey", "lo_suppkey", "lo_partkey", "lo_revenue", "lo_supplycost"]
-C4_COLS = ["lo_orderdate", "lo_custkey", "lo_suppkey", "lo_partkey", "lo_quantity", "lo_discount",
+Q11_COLS = ["lo_orderdate", "lo_quantity", "lo_discount", "lo_extendedprice"]
+Q31_COLS = ["lo_orderdate", "lo_custkey", "lo_suppkey", "lo_partkey", "lo_revenue", "lo_supplycost"]
+BATCH_COLS = ["lo_orderdate", "lo_custkey", "lo_suppkey", "lo_partkey", "lo_quantity", "lo_discount",
            "lo_revenue", "lo_supplycost"]
 
 
@@ -32,17 +32,17 @@ def _g(name: str, nullable: bool = False) -> Group:
     return Group(col(name), mn, card, nullable)
 
 
-def config1(fact_rows: int = 6_000_000, year: int = 1995, disc: tuple[int, int] = (2, 4), qty: int = 30) -> Plan:
-    t = ssb_tables(fact_rows, C1_COLS)
-    b = PlanBuilder(t, "LINEORDER", name="config1")
+def ssb_q11(fact_rows: int = 6_000_000, year: int = 1995, disc: tuple[int, int] = (2, 4), qty: int = 30) -> Plan:
+    t = ssb_tables(fact_rows, Q11_COLS)
+    b = PlanBuilder(t, "LINEORDER", name="ssb_q11")
     b.filter(and_(col("lo_discount").ge(disc[0]), col("lo_discount").le(disc[1]), col("lo_quantity").lt(qty)))
     b.join("DDATE", "lo_orderdate", where=col("d_year").eq(year))
     return b.aggregate([], [("sum", col("lo_extendedprice") * col("lo_discount"))])
 
 
-def config2(fact_rows: int = 60_000_000, region: int = 2, years: tuple[int, int] = (1992, 1997)) -> Plan:
-    t = ssb_tables(fact_rows, C2_COLS)
-    b = PlanBuilder(t, "LINEORDER", name="config2")
+def ssb_q31(fact_rows: int = 60_000_000, region: int = 2, years: tuple[int, int] = (1992, 1997)) -> Plan:
+    t = ssb_tables(fact_rows, Q31_COLS)
+    b = PlanBuilder(t, "LINEORDER", name="ssb_q31")
     b.join("CUSTOMER", "lo_custkey", where=col("c_region").eq(region))
     b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(region))
     b.join("DDATE", "lo_orderdate", where=and_(col("d_year").ge(years[0]), col("d_year").le(years[1])))
@@ -50,11 +50,11 @@ def config2(fact_rows: int = 60_000_000, region: int = 2, years: tuple[int, int]
                        order_by=[(2, False), (3, True)])
 
 
-def config3(fact_rows: int = 60_000_000, region: int = 1, years: tuple[int, int] = (1993, 1998),
+def ssb_q31_nullable(fact_rows: int = 60_000_000, region: int = 1, years: tuple[int, int] = (1993, 1998),
             rev_floor: int = 2_000_000) -> Plan:
-    t = ssb_tables(fact_rows, C2_COLS)
+    t = ssb_tables(fact_rows, Q31_COLS)
     nullable = {"lo_revenue", "c_city"}
-    b = PlanBuilder(t, "LINEORDER", nullable=nullable, name="config3")
+    b = PlanBuilder(t, "LINEORDER", nullable=nullable, name="ssb_q31_nullable")
     # (revenue >= floor OR revenue IS NULL) AND NOT (revenue > 9,500,000): UNKNOWN
     # for NULL revenue on the range terms, rescued by IS NULL on the OR.
     b.filter(and_(or_(col("lo_revenue").ge(rev_floor), col("lo_revenue").is_null()),
@@ -67,8 +67,8 @@ def config3(fact_rows: int = 60_000_000, region: int = 1, years: tuple[int, int]
                        order_by=[(1, False), (0, False)])
 
 
-def config3_tables(fact_rows: int) -> dict[str, Table]:
-    return ssb_tables(fact_rows, C2_COLS)
+def ssb_q31_tables(fact_rows: int) -> dict[str, Table]:
+    return ssb_tables(fact_rows, Q31_COLS)
 
 
 # --------------------------------------------------------------- templates
@@ -79,7 +79,7 @@ TEMPLATE_NAMES = ["T0_scan_sum", "T1_date_year", "T2_nation_year", "T3_brand_yea
 def template(t: int, rng: random.Random, fact_rows: int = 600_000_000) -> Plan:
     """One query of template t with constants drawn from rng (selectivity
     0.01%-20%)."""
-    tables = ssb_tables(fact_rows, C4_COLS)
+    tables = ssb_tables(fact_rows, BATCH_COLS)
     if t == 0:
         q_hi = rng.randint(2, 50)
         q_lo = rng.randint(1, q_hi)

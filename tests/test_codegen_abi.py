@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 
 def all_plans():
     rng = random.Random(3)
-    plans = {"config1": queries.config1(), "config2": queries.config2(), "config3": queries.config3()}
+    plans = {"ssb_q11": queries.ssb_q11(), "ssb_q31": queries.ssb_q31(), "ssb_q31_nullable": queries.ssb_q31_nullable()}
     for t in range(4):
         plans[f"T{t}"] = queries.template(t, rng)
     for k, p in queries.kat_plans().items():
@@ -58,7 +58,7 @@ def test_generated_source_compiles_for_sm100a(name):
 def test_tuning_space_compiles(bt, ipt, stages, place):
     t = _lib.default_tuning()
     t.block_threads, t.items_per_thread, t.stages, t.group_placement = bt, ipt, stages, place
-    for name in ("config2", "config3"):
+    for name in ("ssb_q31", "ssb_q31_nullable"):
         plan = all_plans()[name]
         _lib.Module(_lib.codegen(plan.text(), t), key=f"tune_{name}_{bt}_{ipt}_{stages}_{place}")
 
@@ -143,7 +143,7 @@ def test_execute_without_bound_buffers_reports_missing():
 
 
 def test_scratch_and_result_shapes():
-    plan = all_plans()["config3"]
+    plan = all_plans()["ssb_q31_nullable"]
     m = _lib.Module(_lib.codegen(plan.text()), key="shape_probe")
     assert m.info.groups == 251 * 7
     assert m.info.storage_ts == 5 and m.info.visible_ts == 5
@@ -152,7 +152,7 @@ def test_scratch_and_result_shapes():
 
 
 def test_plan_text_is_deterministic():
-    assert queries.config2().text() == queries.config2().text()
+    assert queries.ssb_q31().text() == queries.ssb_q31().text()
     t = {"T": Table("T", ["a"], 1, fact=True)}
     p = PlanBuilder(t, "T").filter(col("a").gt(3)).aggregate([], [("count", star())])
     assert "(filter (gt (col a) (int 3)))" in p.text()
@@ -171,7 +171,7 @@ def test_shared_program_for_the_four_templates_compiles():
 
 def test_shared_program_rejects_unshareable_shapes():
     with pytest.raises(_lib.CxError):
-        _lib.shared_codegen([queries.config3(1000).text()])  # nullable columns
+        _lib.shared_codegen([queries.ssb_q31_nullable(1000).text()])  # nullable columns
     with pytest.raises(_lib.CxError):
         _lib.shared_codegen([queries.kat_plans()["q1"].text()])  # AVG
 

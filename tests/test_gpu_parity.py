@@ -44,25 +44,25 @@ def assert_parity(db, plan, ht, tuning=None):
 
 
 @pytest.mark.parametrize("n", [1_000_000, 1_000_003, 511, 1])
-def test_config1_shape(db, n):
-    ht = load(db, 11, n, queries.C1_COLS)
-    got, _ = assert_parity(db, queries.config1(n), ht)
+def test_q11_shape(db, n):
+    ht = load(db, 11, n, queries.Q11_COLS)
+    got, _ = assert_parity(db, queries.ssb_q11(n), ht)
     if n >= 1_000_000:
         assert got.words[0] != 0
 
 
-def test_config2_shape(db):
+def test_q31_shape(db):
     n = 2_000_000
-    ht = load(db, 12, n, queries.C2_COLS)
-    plan = queries.config2(n)
+    ht = load(db, 12, n, queries.Q31_COLS)
+    plan = queries.ssb_q31(n)
     got, _ = assert_parity(db, plan, ht)
     assert len(got.rows(plan)) > 100
 
 
-def test_config3_nullable(db):
+def test_q31_nullable(db):
     n = 2_000_003
-    ht = load(db, 13, n, queries.C2_COLS, nulls={"lo_revenue": 100, "c_city": 50})
-    plan = queries.config3(n)
+    ht = load(db, 13, n, queries.Q31_COLS, nulls={"lo_revenue": 100, "c_city": 50})
+    plan = queries.ssb_q31_nullable(n)
     got, _ = assert_parity(db, plan, ht)
     rs = got.rows(plan)
     assert any(r[0] is None for r in rs), "NULL c_city must form its own group"
@@ -72,7 +72,7 @@ def test_config3_nullable(db):
 @pytest.mark.parametrize("t", [0, 1, 2, 3])
 def test_shared_scan_templates(db, t):
     n = 1_500_000
-    ht = load(db, 14, n, queries.C4_COLS)
+    ht = load(db, 14, n, queries.BATCH_COLS)
     rng = random.Random(100 + t)
     for _ in range(3):
         assert_parity(db, queries.template(t, rng, n), ht)
@@ -83,33 +83,33 @@ def test_shared_scan_templates(db, t):
     (1024, 1, 2, 0, 2, 0), (256, 4, 6, 2, 1, 98304), (1024, 2, 0, 1, 1, 98304)])
 def test_tuning_invariance(db, bt, ipt, stages, place, merge, bitmaps):
     n = 777_777
-    ht = load(db, 15, n, queries.C2_COLS, nulls={"lo_revenue": 100, "c_city": 50})
+    ht = load(db, 15, n, queries.Q31_COLS, nulls={"lo_revenue": 100, "c_city": 50})
     t = _lib.default_tuning()
     t.block_threads, t.items_per_thread, t.stages, t.group_placement = bt, ipt, stages, place
     t.group_merge, t.bitmap_budget = merge, bitmaps
-    assert_parity(db, queries.config3(n), ht, t)
-    assert_parity(db, queries.config2(n), ht, t)
+    assert_parity(db, queries.ssb_q31_nullable(n), ht, t)
+    assert_parity(db, queries.ssb_q31(n), ht, t)
 
 
 def test_empty_fact_table(db):
-    ht = load(db, 16, 0, queries.C1_COLS)
-    got, ref = assert_parity(db, queries.config1(0), ht)
+    ht = load(db, 16, 0, queries.Q11_COLS)
+    got, ref = assert_parity(db, queries.ssb_q11(0), ht)
     assert int(got.words[0]) == 0
 
 
 def test_empty_selection_and_all_null(db):
     n = 100_000
-    ht = load(db, 17, n, queries.C2_COLS, nulls={"lo_revenue": 1000, "c_city": 1000})
-    assert_parity(db, queries.config2(n, years=(2050, 2060)), ht)
-    plan = queries.config3(n)
+    ht = load(db, 17, n, queries.Q31_COLS, nulls={"lo_revenue": 1000, "c_city": 1000})
+    assert_parity(db, queries.ssb_q31(n, years=(2050, 2060)), ht)
+    plan = queries.ssb_q31_nullable(n)
     got, _ = assert_parity(db, plan, ht)
     assert all(r[0] is None and r[2] == 0 for r in got.rows(plan))
 
 
 def test_min_max_avg_and_case(db):
     n = 300_001
-    ht = load(db, 18, n, queries.C4_COLS, nulls={"lo_revenue": 200})
-    tabs = datagen.ssb_tables(n, queries.C4_COLS)
+    ht = load(db, 18, n, queries.BATCH_COLS, nulls={"lo_revenue": 200})
+    tabs = datagen.ssb_tables(n, queries.BATCH_COLS)
     nul = {"lo_revenue"}
     b = PlanBuilder(tabs, "LINEORDER", nullable=nul)
     b.filter(or_(col("lo_quantity").lt(10), col("lo_revenue").is_null()))
@@ -154,8 +154,8 @@ def test_group_domain_violation_is_reported(db):
     """A GROUP BY key outside its catalog domain raises error code 2 (the
     reference folds it silently into another group)."""
     n = 50_000
-    ht = load(db, 19, n, queries.C4_COLS)
-    tabs = datagen.ssb_tables(n, queries.C4_COLS)
+    ht = load(db, 19, n, queries.BATCH_COLS)
+    tabs = datagen.ssb_tables(n, queries.BATCH_COLS)
     b = PlanBuilder(tabs, "LINEORDER")
     b.join("DDATE", "lo_orderdate")
     plan = b.aggregate([Group(col("d_year"), 1992, 5)], [("count", star())])
@@ -168,7 +168,7 @@ def test_group_domain_violation_is_reported(db):
 def test_device_generator_matches_host(db):
     import torch
     n = 1_000_037
-    for c in queries.C4_COLS + ["lo_extendedprice"]:
+    for c in queries.BATCH_COLS + ["lo_extendedprice"]:
         t = torch.empty(n, dtype=torch.int32, device="cuda")
         datagen.fact_column_device(c, 5, n, t.data_ptr())
         torch.cuda.synchronize()
@@ -183,7 +183,7 @@ def test_device_generator_matches_host(db):
 def test_sparse_compaction(db):
     import torch
     n = 400_000
-    ht = load(db, 20, n, queries.C4_COLS)
+    ht = load(db, 20, n, queries.BATCH_COLS)
     plan = queries.template(3, random.Random(7), n)
     assert plan.sparse
     got = db.execute(plan)
@@ -209,7 +209,7 @@ def test_shared_scan_batch_matches_oracle_per_query(db, nq, tune):
     """Every query of a mixed-template batch run as ONE shared scan equals the
     oracle run on that query alone (same words, same validity bits)."""
     n = 700_001
-    ht = load(db, 30 + nq, n, queries.C4_COLS)
+    ht = load(db, 30 + nq, n, queries.BATCH_COLS)
     plans = queries.batch(nq, 1000 + nq, n)
     t = None
     if tune:
@@ -226,12 +226,12 @@ def test_shared_scan_batch_matches_oracle_per_query(db, nq, tune):
         np.testing.assert_array_equal(g.validity, ref.validity)
 
 
-def test_shared_scan_config2_and_repeat(db):
-    """The config-2 shape through the shared path, twice in a row (buffers and
+def test_shared_scan_q31_and_repeat(db):
+    """The SSB Q3.1 shape through the shared path, twice in a row (buffers and
     dimension indexes are rebuilt per batch)."""
     n = 500_003
-    ht = load(db, 41, n, queries.C2_COLS)
-    plans = [queries.config2(n, region=r, years=(1992 + r, 1997)) for r in range(5)]
+    ht = load(db, 41, n, queries.Q31_COLS)
+    plans = [queries.ssb_q31(n, region=r, years=(1992 + r, 1997)) for r in range(5)]
     for _ in range(2):
         got = db.execute_shared(plans)
         for p, g in zip(plans, got):
@@ -244,7 +244,7 @@ def test_shared_scan_two_passes(db):
     """A batch larger than one pass (64 queries) runs as consecutive passes
     over the fact table; every query still equals the oracle."""
     n = 300_007
-    ht = load(db, 43, n, queries.C4_COLS)
+    ht = load(db, 43, n, queries.BATCH_COLS)
     plans = queries.batch(90, 4242, n)
     got = db.execute_shared(plans)
     assert got[0].kernel_error == 0
@@ -260,7 +260,7 @@ def test_shared_scan_values_outside_filter_windows(db, rng_lo, rng_hi):
     evaluation: a registered range that misses most values gives the same
     answers."""
     n = 400_009
-    ht = load(db, 44, n, queries.C4_COLS)
+    ht = load(db, 44, n, queries.BATCH_COLS)
     db.ctx.set_column_range("d_lo_quantity", rng_lo, rng_hi)
     db.ctx.set_column_range("d_lo_discount", rng_lo, rng_hi)
     plans = queries.batch(24, 77, n)
@@ -275,8 +275,8 @@ def test_shared_scan_residual_filters(db):
     """Conjuncts over two fact columns are evaluated per row and query after
     the mask; they share a batch with filter-table and join-only shapes."""
     n = 350_011
-    ht = load(db, 45, n, queries.C4_COLS)
-    tables = datagen.ssb_tables(n, queries.C4_COLS)
+    ht = load(db, 45, n, queries.BATCH_COLS)
+    tables = datagen.ssb_tables(n, queries.BATCH_COLS)
     plans = []
     for k in range(3):
         b = PlanBuilder(tables, "LINEORDER", name="R")

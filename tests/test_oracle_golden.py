@@ -128,16 +128,16 @@ def test_result_size_known_answers(case):
     if case["size"] == 21000:
         plan = queries.template(3, __import__("random").Random(0), 1000)
     elif case["size"] == 17500:
-        plan = queries.config2(1000)
+        plan = queries.ssb_q31(1000)
     else:
-        plan = queries.config1(1000)
+        plan = queries.ssb_q11(1000)
     assert plan.group_slots * plan.storage_ts == case["size"]
 
 
 # ----------------------------------------------- independent evaluator ---
 
-def _py_eval_config2(cols, region, years):
-    """Plain-Python hash joins for the config-2 query (no shared code with the
+def _py_eval_q31(cols, region, years):
+    """Plain-Python hash joins for the SSB Q3.1-shaped query (no shared code with the
     oracle): returns {(c_nation, s_nation, year): sum}."""
     cust = {int(k): (int(r), int(n)) for k, r, n in zip(cols["c_custkey"], cols["c_region"], cols["c_nation"])}
     supp = {int(k): (int(r), int(n)) for k, r, n in zip(cols["s_suppkey"], cols["s_region"], cols["s_nation"])}
@@ -157,11 +157,11 @@ def _py_eval_config2(cols, region, years):
 def test_oracle_agrees_with_independent_python_evaluator():
     from practice_b200 import datagen
     n = 20_000
-    ht = datagen.host_tables(7, n, queries.C2_COLS)
-    plan = queries.config2(n, region=3, years=(1993, 1996))
+    ht = datagen.host_tables(7, n, queries.Q31_COLS)
+    plan = queries.ssb_q31(n, region=3, years=(1993, 1996))
     r = oracle.run_plan(plan.text(), ht.columns, ht.validity,
                         {"LINEORDER": n, "CUSTOMER": 300_000, "SUPPLIER": 20_000, "DDATE": 2556},
                         plan.group_slots * plan.storage_ts)
     got = {(a, b, c): s for a, b, c, s in results.rows(plan, r.words, r.validity)}
-    assert got == _py_eval_config2(ht.columns, 3, (1993, 1996))
+    assert got == _py_eval_q31(ht.columns, 3, (1993, 1996))
     assert len(got) > 50

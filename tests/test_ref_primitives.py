@@ -19,7 +19,7 @@ DIMS = {"CUSTOMER": 300_000, "SUPPLIER": 20_000, "DDATE": 2556, "PART": 200_000}
 @pytest.fixture(scope="module")
 def tables():
     n = 200_003
-    return n, datagen.host_tables(21, n, queries.C4_COLS + ["lo_extendedprice"])
+    return n, datagen.host_tables(21, n, queries.BATCH_COLS + ["lo_extendedprice"])
 
 
 @pytest.mark.parametrize("t", [0, 1, 2, 3])
@@ -33,9 +33,9 @@ def test_templates_match_reference_primitives(tables, t):
         np.testing.assert_array_equal(ref, got.words)
 
 
-def test_config1_and_config2_match_reference_primitives(tables):
+def test_q11_and_q31_match_reference_primitives(tables):
     n, ht = tables
-    for p in (queries.config1(n), queries.config2(n, region=4)):
+    for p in (queries.ssb_q11(n), queries.ssb_q31(n, region=4)):
         ref = refharness.run(p, ht.columns, DIMS, n)
         got = oracle.run_plan(p.text(), ht.columns, ht.validity, {"LINEORDER": n, **DIMS}, p.group_slots * p.storage_ts)
         np.testing.assert_array_equal(ref, got.words)

@@ -201,6 +201,12 @@ def config_block(args):
 
 # ------------------------------------------------------------------ GPU arm
 
+# DRAM bytes (read + write) per fact row of one shared-scan launch over the
+# 8-column batch table, from the ncu capture in
+# profiles/SharedScan_LINEORDER_batch32_30M.md (974.2 MB for 30M rows); the
+# traffic of a launch grows with its rows.
+SHARED_DRAM_BYTES_PER_ROW = 974.231040e6 / 30e6
+
 PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=98304)
                     for bt, ipt, st in ((1024, 2, 0), (1024, 4, 0), (512, 2, 0), (512, 8, 2), (1024, 4, 2))]
 SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=2, producer_warps=pw)
@@ -407,7 +413,9 @@ def main():
             "latency_ms": {"p50": statistics.median(lat), "p99": float(np.percentile(lat, 99)),
                            "definition": "query completion since its batch started"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": (SHARED_DRAM_BYTES_PER_ROW * args.rows / 1e9) if shared is not None else None,
+                         "traffic_unit": "GB per launch (ncu capture of 30M rows scaled by rows)",
                          "kernel": kernel, "algorithmic_bytes": alg},
             "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
             "cpu_baseline": cb,

@@ -76,6 +76,7 @@ typedef struct cx_timing {
   float total_ms;  /* whole execute */
   int scan_grid;   /* CTAs of the scan launch */
   int gpu_launches;/* kernels launched by the last execute */
+  int graph;       /* shared scans: 0 launched directly, 1 replayed a cached graph, 2 captured a new one */
 } cx_timing;
 
 int cx_abi_version(void);
@@ -131,6 +132,10 @@ int cx_ctx_set_sm_count(cx_exec_ctx* c, int sms);
  * past the window) are evaluated row by row per query.  No reference
  * counterpart: the reference plans one query at a time. */
 int cx_ctx_set_column_range(cx_exec_ctx* c, const char* name, int64_t lo, int64_t hi);
+/* Shared-scan batches are captured once into a CUDA graph and replayed while
+ * the batch keeps the same pass shapes (queries per pass, parameters, shared
+ * memory assignment, buffers); on by default.  0 launches every kernel directly. */
+int cx_ctx_set_graph_replay(cx_exec_ctx* c, int enable);
 
 /* Enqueues the query on `stream` (a cudaStream_t; NULL = legacy default
  * stream).  Asynchronous: call cx_ctx_sync before reading results.  Replaces

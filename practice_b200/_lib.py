@@ -24,7 +24,7 @@ EXPORTS = [
     "cx_ctx_set_scratch", "cx_module_scratch_bytes", "cx_ctx_set_sm_count", "cx_execute",
     "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse", "cx_compact_sparse_noalloc",
     "cx_gen_uniform", "cx_gen_datekey", "cx_gen_validity", "cx_plan_literals", "cx_shared_codegen",
-    "cx_shared_execute", "cx_ctx_set_column_range",
+    "cx_shared_execute", "cx_ctx_set_column_range", "cx_ctx_set_graph_replay",
 ]
 
 
@@ -53,7 +53,7 @@ class SharedQuery(C.Structure):
 
 class Timing(C.Structure):
     _fields_ = [("build_ms", C.c_float), ("scan_ms", C.c_float), ("post_ms", C.c_float),
-                ("total_ms", C.c_float), ("scan_grid", C.c_int), ("gpu_launches", C.c_int)]
+                ("total_ms", C.c_float), ("scan_grid", C.c_int), ("gpu_launches", C.c_int), ("graph", C.c_int)]
 
 
 def _load() -> C.CDLL:
@@ -79,6 +79,7 @@ def _load() -> C.CDLL:
         "cx_module_scratch_bytes": (C.c_int, [vp, vp, C.POINTER(u64)]),
         "cx_ctx_set_sm_count": (C.c_int, [vp, C.c_int]),
         "cx_ctx_set_column_range": (C.c_int, [vp, C.c_char_p, i64, i64]),
+        "cx_ctx_set_graph_replay": (C.c_int, [vp, C.c_int]),
         "cx_execute": (C.c_int, [vp, vp, vp]),
         "cx_ctx_sync": (C.c_int, [vp]),
         "cx_ctx_timing": (C.c_int, [vp, C.POINTER(Timing)]),
@@ -194,6 +195,9 @@ class ExecCtx:
 
     def set_rows(self, table: str, rows: int) -> None:
         check(lib.cx_ctx_set_table_rows(self.handle, table.encode(), rows), "cx_ctx_set_table_rows")
+
+    def set_graph_replay(self, enable: bool) -> None:
+        check(lib.cx_ctx_set_graph_replay(self.handle, int(enable)), "cx_ctx_set_graph_replay")
 
     def set_column_range(self, name: str, lo: int, hi: int) -> None:
         check(lib.cx_ctx_set_column_range(self.handle, name.encode(), lo, hi), "cx_ctx_set_column_range")

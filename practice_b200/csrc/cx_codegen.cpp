@@ -1298,6 +1298,34 @@ struct SharedGen {
     return out.empty() ? "true" : out;
   }
 
+  // Per pass: zeroes every query's result words, validity words and touched
+  // bits (one block per query), so a pass has the same launches whatever its
+  // queries' buffers are.
+  void emit_zero() {
+    meta << "kernel shared_zero zero 0 256 0\n";
+    src << "extern \"C\" __global__ void __launch_bounds__(256) shared_zero(const CxArgs a) {\n";
+    src << "  const int q = blockIdx.x;\n";
+    src << "  if (q >= a.sq_total) return;\n";
+    src << "  const CxSQ Q = a.sq[q];\n";
+    src << "  long long nw = 0, nt = 0;\n";
+    src << "  switch (Q.shape) {\n";
+    for (size_t si = 0; si < shapes.size(); ++si) {
+      const Plan& p = *shapes[si];
+      Emitter e(p, tu);
+      const unsigned long long G = e.total_groups();
+      src << "    case " << si << ": nw = " << G * (unsigned long long)p.storage_ts() << "LL; nt = "
+          << (p.groups.empty() ? 0ULL : (G + 31) / 32) << "LL; break;\n";
+    }
+    src << "    default: break;\n";
+    src << "  }\n";
+    src << "  const long long nv = (nw + 63) / 64;\n";
+    src << "  for (long long i = threadIdx.x; i < nw; i += blockDim.x) Q.result[i] = 0ULL;\n";
+    src << "  for (long long i = threadIdx.x; i < nv; i += blockDim.x) Q.validity[i] = 0ULL;\n";
+    src << "  if (Q.touched)\n";
+    src << "    for (long long i = threadIdx.x; i < nt; i += blockDim.x) Q.touched[i] = 0u;\n";
+    src << "}\n\n";
+  }
+
   // Per batch: slot entries of one dimension with the batch's query masks.
   void emit_index(const Dim& d, int di) {
     const std::string k = "index_" + lower(d.name);
@@ -1368,6 +1396,7 @@ struct SharedGen {
            << " " << (p.sparse ? 1 : 0) << " " << lit_maps[s].size() << " " << (smem_ok ? 1 : 0) << " " << NA << " "
            << (G + 31) / 32 << " " << nseen << "\n";
     }
+    emit_zero();
     for (size_t di = 0; di < dims.size(); ++di) emit_index(dims[di], (int)di);
     emit_scan();
     emit_keys();

@@ -299,6 +299,12 @@ struct cx_exec_ctx {
   bool pending = false;
   cx_timing timing{};
   uint32_t kernel_err = 0;
+  // Shared-scan batches replay a captured CUDA graph while their pass shapes repeat.
+  bool graph_replay = true;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<unsigned char> gsig;
+  int graph_launches = 0;
 };
 
 namespace {
@@ -506,6 +512,8 @@ void cx_ctx_destroy(cx_exec_ctx* c) {
   if (c->own_scratch) cudaFree(c->own_scratch);
   if (c->host_err) cudaFreeHost(c->host_err);
   if (c->host_stage) cudaFreeHost(c->host_stage);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   delete c;
 }
 
@@ -908,27 +916,19 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
   int sms = c->sm_override;
   if (sms <= 0) CX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   Driver& d = driver();
-  int launches = 0, scan_grid = 0;
-  void* kparams[] = {&a};
-  auto launch = [&](size_t ki, unsigned grid, size_t extra) -> int {
-    const KernelSpec& k = lp.kernels[ki];
-    if (grid == 0) return CX_OK;
-    CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, (unsigned)(k.smem + extra), (CUstream)stream, kparams, nullptr);
-    if (r != CUDA_SUCCESS) return drv_fail(r, k.name.c_str());
-    ++launches;
-    return CX_OK;
-  };
 
-  CX_CUDA(cudaEventRecord(c->ev[0], stream));
-  CX_CUDA(cudaMemsetAsync(scratch + dim_end, 0, touch_end - dim_end, stream));
-  CX_CUDA(cudaMemsetAsync(scratch + err_off, 0, 16, stream));
-  for (int i = 0; i < nq; ++i) {
-    const auto& sh = lp.sshapes[queries[order[i]].shape];
-    const uint64_t need = sh.groups * (uint64_t)sh.ts;
-    CX_CUDA(cudaMemsetAsync(queries[order[i]].result, 0, need * 8, stream));
-    CX_CUDA(cudaMemsetAsync(queries[order[i]].validity, 0, ((need + 63) / 64) * 8, stream));
-  }
+  // Plan every pass on the host: descriptors and parameters into the pinned
+  // staging, kernel arguments, grids and shared-memory sizes.
+  struct Pass {
+    CxArgs args;
+    int qn = 0, nparams = 0;
+    size_t extra_smem = 0;
+    unsigned scan_grid = 0;
+    char* hstage = nullptr;
+  };
+  std::vector<Pass> passes(npass);
   for (int ps = 0; ps < npass; ++ps) {
+    Pass& P = passes[ps];
     const int q0 = ps * maxq, qn = std::min(nq, q0 + maxq) - q0;
     char* hstage = (char*)c->host_stage + (size_t)ps * pass_bytes;
     CxSQ* hsq = (CxSQ*)hstage;
@@ -968,40 +968,123 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
       const int s = hsq[j].shape;
       if (s < CX_MAX_SHAPES) { if (a.sq_num[s] == 0) a.sq_first[s] = j; ++a.sq_num[s]; }
     }
-    const size_t extra_smem = qb_bytes + (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
-    CX_CUDA(cudaMemcpyAsync((void*)a.sq, hstage, (size_t)qn * sizeof(CxSQ), cudaMemcpyHostToDevice, stream));
-    if (poff) CX_CUDA(cudaMemcpyAsync((void*)a.sparams, hpar, (size_t)poff * 4, cudaMemcpyHostToDevice, stream));
-    CX_CUDA(cudaMemsetAsync(scratch, 0, dim_end, stream));
-    size_t ki = 0;
-    for (; ki < scan_ki; ++ki) {
-      const KernelSpec& k = lp.kernels[ki];
-      const long long tiles = (rows[k.table] + k.tile - 1) / k.tile;
-      if ((rc = launch(ki, (unsigned)std::min<long long>(tiles, (long long)sms * 16), 0))) return rc;
-    }
-    if (ps == 0) CX_CUDA(cudaEventRecord(c->ev[1], stream));
+    P.args = a;
+    P.qn = qn;
+    P.nparams = poff;
+    P.hstage = hstage;
+    P.extra_smem = qb_bytes + (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
     int occ = 1;
-    CUresult orr = d.Occupancy(&occ, L->fns[scan_ki], sk.block, sk.smem + extra_smem);
+    CUresult orr = d.Occupancy(&occ, L->fns[scan_ki], sk.block, sk.smem + P.extra_smem);
     if (orr != CUDA_SUCCESS) return drv_fail(orr, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (occ < 1) return fail(CX_E_CAPACITY, "cx_shared_execute: shared scan cannot be resident with %zu bytes of shared memory", sk.smem + extra_smem);
+    if (occ < 1) return fail(CX_E_CAPACITY, "cx_shared_execute: shared scan cannot be resident with %zu bytes of shared memory", sk.smem + P.extra_smem);
     const long long tiles = (rows[0] + sk.tile - 1) / sk.tile;
     const int per_sm = std::max(1, std::min(sk.ctas_per_sm, occ));
-    const long long grid = std::min<long long>(tiles, (long long)sms * per_sm);
-    scan_grid = (int)grid;
-    if ((rc = launch(scan_ki, (unsigned)grid, extra_smem))) return rc;
-    if (ps == npass - 1) CX_CUDA(cudaEventRecord(c->ev[2], stream));
-    for (ki = scan_ki + 1; ki < lp.kernels.size(); ++ki)
-      if ((rc = launch(ki, (unsigned)qn, 0))) return rc;
+    P.scan_grid = (unsigned)std::min<long long>(tiles, (long long)sms * per_sm);
   }
-  if (npass == 0) {
-    CX_CUDA(cudaEventRecord(c->ev[1], stream));
-    CX_CUDA(cudaEventRecord(c->ev[2], stream));
+
+  // Enqueues the whole batch on `s`: one fixed sequence per pass shape, so a
+  // captured graph of it replays for every batch with the same pass shapes.
+  int launches = 0;
+  auto enqueue = [&](cudaStream_t s) -> int {
+    launches = 0;
+    auto launch = [&](size_t ki, unsigned grid, size_t extra, CxArgs* args) -> int {
+      const KernelSpec& k = lp.kernels[ki];
+      if (grid == 0) return CX_OK;
+      void* kp[] = {args};
+      CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, (unsigned)(k.smem + extra), (CUstream)s, kp, nullptr);
+      if (r != CUDA_SUCCESS) return drv_fail(r, k.name.c_str());
+      ++launches;
+      return CX_OK;
+    };
+    CX_CUDA(cudaEventRecord(c->ev[0], s));
+    CX_CUDA(cudaMemsetAsync(scratch + err_off, 0, 16, s));
+    for (int ps = 0; ps < npass; ++ps) {
+      Pass& P = passes[ps];
+      CX_CUDA(cudaMemcpyAsync((void*)P.args.sq, P.hstage, (size_t)P.qn * sizeof(CxSQ), cudaMemcpyHostToDevice, s));
+      if (P.nparams)
+        CX_CUDA(cudaMemcpyAsync((void*)P.args.sparams, P.hstage + desc_bytes, (size_t)P.nparams * 4, cudaMemcpyHostToDevice, s));
+      CX_CUDA(cudaMemsetAsync(scratch, 0, dim_end, s));
+      for (size_t ki = 0; ki < scan_ki; ++ki) {
+        const KernelSpec& k = lp.kernels[ki];
+        unsigned grid;
+        if (k.kind == "zero") grid = (unsigned)P.qn;
+        else grid = (unsigned)std::min<long long>((rows[k.table] + k.tile - 1) / k.tile, (long long)sms * 16);
+        int r = launch(ki, grid, 0, &P.args);
+        if (r) return r;
+      }
+      if (ps == 0) CX_CUDA(cudaEventRecord(c->ev[1], s));
+      int r = launch(scan_ki, P.scan_grid, P.extra_smem, &P.args);
+      if (r) return r;
+      if (ps == npass - 1) CX_CUDA(cudaEventRecord(c->ev[2], s));
+      for (size_t ki = scan_ki + 1; ki < lp.kernels.size(); ++ki)
+        if ((r = launch(ki, (unsigned)P.qn, 0, &P.args))) return r;
+    }
+    if (npass == 0) {
+      CX_CUDA(cudaEventRecord(c->ev[1], s));
+      CX_CUDA(cudaEventRecord(c->ev[2], s));
+    }
+    CX_CUDA(cudaMemcpyAsync(c->host_err, scratch + err_off, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    CX_CUDA(cudaEventRecord(c->ev[3], s));
+    return CX_OK;
+  };
+
+  int graph_mode = 0;
+  if (c->graph_replay && npass > 0) {
+    // Everything a captured graph bakes in: module, buffers, staging, and per
+    // pass the kernel arguments, grids, shared memory and copy sizes.
+    std::vector<unsigned char> sig;
+    auto put = [&](const void* p, size_t n) { sig.insert(sig.end(), (const unsigned char*)p, (const unsigned char*)p + n); };
+    const void* ids[] = {m, scratch, c->host_stage, c->host_err};
+    put(ids, sizeof ids);
+    const uint64_t sizes[] = {dim_end, err_off, (uint64_t)npass, (uint64_t)sms};
+    put(sizes, sizeof sizes);
+    for (const Pass& P : passes) {
+      put(&P.args, sizeof(CxArgs));
+      const uint64_t v[] = {(uint64_t)P.qn, (uint64_t)P.nparams, P.extra_smem, P.scan_grid, (uint64_t)(P.hstage - (char*)c->host_stage)};
+      put(v, sizeof v);
+    }
+    if (!(c->gexec && sig == c->gsig)) {
+      if (!c->cap_stream) CX_CUDA(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+      CX_CUDA(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
+      const int er = enqueue(c->cap_stream);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(c->cap_stream, &g);
+      if (er) { if (g) cudaGraphDestroy(g); return er; }
+      if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return fail(CX_E_CUDA, "cx_shared_execute: graph capture: %s", cudaGetErrorString(ce)); }
+      bool updated = false;
+      if (c->gexec) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(c->gexec, g, &info) == cudaSuccess;
+        if (!updated) { cudaGetLastError(); cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+      }
+      if (!updated) {
+        const cudaError_t ie = cudaGraphInstantiate(&c->gexec, g, 0);
+        if (ie != cudaSuccess) { cudaGraphDestroy(g); c->gexec = nullptr; return fail(CX_E_CUDA, "cx_shared_execute: graph instantiate: %s", cudaGetErrorString(ie)); }
+      }
+      cudaGraphDestroy(g);
+      c->gsig = std::move(sig);
+      c->graph_launches = launches;
+      graph_mode = 2;
+    } else {
+      graph_mode = 1;
+    }
+    CX_CUDA(cudaGraphLaunch(c->gexec, stream));
+    launches = c->graph_launches;
+  } else {
+    const int er = enqueue(stream);
+    if (er) return er;
   }
-  CX_CUDA(cudaMemcpyAsync(c->host_err, a.err, sizeof(unsigned int), cudaMemcpyDeviceToHost, stream));
-  CX_CUDA(cudaEventRecord(c->ev[3], stream));
   c->pending = true;
   c->timing = cx_timing{};
-  c->timing.scan_grid = scan_grid;
+  c->timing.scan_grid = npass ? (int)passes.back().scan_grid : 0;
   c->timing.gpu_launches = launches;
+  c->timing.graph = graph_mode;
+  return CX_OK;
+}
+
+int cx_ctx_set_graph_replay(cx_exec_ctx* c, int enable) {
+  if (!c) return fail(CX_E_INVALID, "cx_ctx_set_graph_replay: NULL context");
+  c->graph_replay = enable != 0;
   return CX_OK;
 }
 

@@ -296,3 +296,33 @@ def test_shared_scan_residual_filters(db):
         ref = oracle_run(p, ht)
         np.testing.assert_array_equal(g.words, ref.words)
         np.testing.assert_array_equal(g.validity, ref.validity)
+
+
+def test_shared_scan_graph_replay(db):
+    """A batch is captured into a CUDA graph once; later batches with the same
+    pass shapes (same shape mix, new literals and new result buffers) replay
+    it and still equal the oracle; direct launches give the same answers."""
+    n = 300_017
+    ht = load(db, 46, n, queries.BATCH_COLS)
+    rng = random.Random(78)
+    kinds = [0, 1, 2, 3, 1, 2, 0, 3]
+    modes = []
+    for _ in range(3):
+        plans = [queries.template(t, rng, n) for t in kinds]
+        got = db.execute_shared(plans)
+        modes.append(got[0].timing.graph)
+        for p, g in zip(plans, got):
+            ref = oracle_run(p, ht)
+            np.testing.assert_array_equal(g.words, ref.words)
+            np.testing.assert_array_equal(g.validity, ref.validity)
+    assert modes[0] in (1, 2) and modes[1] == 1 and modes[2] == 1, modes
+    db.ctx.set_graph_replay(False)
+    try:
+        plans = [queries.template(t, rng, n) for t in kinds]
+        got = db.execute_shared(plans)
+        assert got[0].timing.graph == 0
+        for p, g in zip(plans, got):
+            ref = oracle_run(p, ht)
+            np.testing.assert_array_equal(g.words, ref.words)
+    finally:
+        db.ctx.set_graph_replay(True)

@@ -985,8 +985,13 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
   // Enqueues the whole batch on `s`: one fixed sequence per pass shape, so a
   // captured graph of it replays for every batch with the same pass shapes.
   int launches = 0;
-  auto enqueue = [&](cudaStream_t s) -> int {
+  auto enqueue = [&](cudaStream_t s, bool capturing) -> int {
     launches = 0;
+    // Inside a capture only an external record becomes a graph node that
+    // records the timing event.
+    auto rec = [&](cudaEvent_t e) {
+      return capturing ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal) : cudaEventRecord(e, s);
+    };
     auto launch = [&](size_t ki, unsigned grid, size_t extra, CxArgs* args) -> int {
       const KernelSpec& k = lp.kernels[ki];
       if (grid == 0) return CX_OK;
@@ -996,7 +1001,7 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
       ++launches;
       return CX_OK;
     };
-    CX_CUDA(cudaEventRecord(c->ev[0], s));
+    CX_CUDA(rec(c->ev[0]));
     CX_CUDA(cudaMemsetAsync(scratch + err_off, 0, 16, s));
     for (int ps = 0; ps < npass; ++ps) {
       Pass& P = passes[ps];
@@ -1012,19 +1017,19 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
         int r = launch(ki, grid, 0, &P.args);
         if (r) return r;
       }
-      if (ps == 0) CX_CUDA(cudaEventRecord(c->ev[1], s));
+      if (ps == 0) CX_CUDA(rec(c->ev[1]));
       int r = launch(scan_ki, P.scan_grid, P.extra_smem, &P.args);
       if (r) return r;
-      if (ps == npass - 1) CX_CUDA(cudaEventRecord(c->ev[2], s));
+      if (ps == npass - 1) CX_CUDA(rec(c->ev[2]));
       for (size_t ki = scan_ki + 1; ki < lp.kernels.size(); ++ki)
         if ((r = launch(ki, (unsigned)P.qn, 0, &P.args))) return r;
     }
     if (npass == 0) {
-      CX_CUDA(cudaEventRecord(c->ev[1], s));
-      CX_CUDA(cudaEventRecord(c->ev[2], s));
+      CX_CUDA(rec(c->ev[1]));
+      CX_CUDA(rec(c->ev[2]));
     }
     CX_CUDA(cudaMemcpyAsync(c->host_err, scratch + err_off, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-    CX_CUDA(cudaEventRecord(c->ev[3], s));
+    CX_CUDA(rec(c->ev[3]));
     return CX_OK;
   };
 
@@ -1046,7 +1051,7 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
     if (!(c->gexec && sig == c->gsig)) {
       if (!c->cap_stream) CX_CUDA(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
       CX_CUDA(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
-      const int er = enqueue(c->cap_stream);
+      const int er = enqueue(c->cap_stream, true);
       cudaGraph_t g = nullptr;
       const cudaError_t ce = cudaStreamEndCapture(c->cap_stream, &g);
       if (er) { if (g) cudaGraphDestroy(g); return er; }
@@ -1071,7 +1076,7 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
     CX_CUDA(cudaGraphLaunch(c->gexec, stream));
     launches = c->graph_launches;
   } else {
-    const int er = enqueue(stream);
+    const int er = enqueue(stream, false);
     if (er) return er;
   }
   c->pending = true;

@@ -37,7 +37,8 @@ enum {
   CX_E_CAPACITY = -5,    /* a caller buffer or the memory budget is too small */
   CX_E_KERNEL = -6,      /* a kernel raised an error code (see cx_ctx_kernel_error) */
   CX_E_NO_DEVICE = -7,   /* no CUDA device */
-  CX_E_REJECTED = -8     /* admission control refused a request */
+  CX_E_REJECTED = -8,    /* admission control refused a request */
+  CX_E_PENDING = -9      /* a request has not finished within the wait */
 };
 
 typedef struct cx_module cx_module;     /* compiled query: cubin + launch plan */
@@ -217,6 +218,71 @@ int cx_gen_datekey(uint64_t gen_stream, uint64_t seed, uint32_t days, uint64_t r
  * null_permille/1000; unused bits of the last word are 0. */
 int cx_gen_validity(uint64_t gen_stream, uint64_t seed, uint64_t rows, uint32_t null_permille, uint64_t* dev_out,
                     void* stream);
+
+/* ------------------------------------------------------------------------
+ * Request loop (serving).  No reference counterpart: the reference runs one
+ * query per db_cli command on one in-order queue (src/db/database_instance.cpp:23);
+ * the admission estimate generalises its device-memory preflight
+ * (src/core/execution.cpp:298-404).
+ *
+ * A server keeps the caller's resident tables (the context passed at create),
+ * the compiled programs and per-slot scratch on one GPU.  A scheduler thread
+ * admits submitted queries in arrival order while their estimated result and
+ * hash/group bytes fit the HBM budget, fuses the admitted shareable queries
+ * into shared-scan batches (continuous batching: a batch forms from whatever
+ * is waiting when a slot frees up), runs the others through their plain
+ * kernel, and overlaps `slots` launches on separate streams.  Results are
+ * copied to host memory owned by the server until released.
+ * ---------------------------------------------------------------------- */
+typedef struct cx_server cx_server;
+
+typedef struct cx_server_config {
+  uint64_t budget_bytes;  /* HBM for per-query results, hash tables and batch scratch */
+  int max_batch;          /* queries per shared launch, 1..256 (64 per pass) */
+  int slots;              /* launches in flight, each on its own stream, 1..8 */
+  int plain_only;         /* 1: every query runs alone through its plain kernel (baseline loop) */
+  cx_tuning shared_tuning;/* launch shape of the shared-scan programs */
+} cx_server_config;
+
+typedef struct cx_request_info {
+  int status;             /* CX_OK when answered, else the request's error */
+  uint32_t kernel_error;  /* kernel error code of its launch (0 = none) */
+  uint64_t words;         /* u64 words of its result (final layout) */
+  uint64_t validity_words;/* u64 words of its validity bitmap */
+  double queue_ms;        /* submit -> launch */
+  double latency_ms;      /* submit -> result in host memory */
+  int batch_size;         /* queries answered by the same launch (1 = alone) */
+  int shared;             /* 1 = shared scan, 0 = plain kernel */
+} cx_request_info;
+
+typedef struct cx_server_stats {
+  uint64_t submitted, completed, rejected, launches;
+  double p50_ms, p99_ms, max_ms;  /* latency of completed requests */
+  double mean_batch;              /* queries per launch */
+  double queries_per_s;           /* completed / (last completion - first submit) */
+  uint64_t budget_bytes, peak_reserved_bytes;
+} cx_server_stats;
+
+void cx_server_config_default(cx_server_config* cfg);
+/* Starts a server on the current device over the tables bound in `tables`
+ * (buffers, row counts, value ranges; copied at create). */
+int cx_server_create(const cx_exec_ctx* tables, const cx_server_config* cfg, cx_server** out);
+/* Compiles what a plan needs ahead of its first submission (its shared
+ * program shape or its plain kernel), so no request waits for NVRTC. */
+int cx_server_prepare(cx_server* s, const char* plan, size_t plan_len);
+/* Queues one query; `id` identifies it to wait / fetch / release.  A plan
+ * whose estimated bytes exceed the whole budget is refused (CX_E_REJECTED). */
+int cx_server_submit(cx_server* s, const char* plan, size_t plan_len, uint64_t* id);
+/* Waits up to timeout_ms (< 0: forever) for a request; CX_E_PENDING if still running. */
+int cx_server_wait(cx_server* s, uint64_t id, int timeout_ms, cx_request_info* info);
+/* Copies a finished request's result words and validity words. */
+int cx_server_fetch(cx_server* s, uint64_t id, uint64_t* words, uint64_t cap, uint64_t* validity, uint64_t vcap);
+/* Forgets a finished request and its host copy. */
+int cx_server_release(cx_server* s, uint64_t id);
+/* Latency and throughput of requests completed since the last reset. */
+int cx_server_get_stats(cx_server* s, int reset, cx_server_stats* out);
+/* Finishes in-flight work and frees everything. */
+int cx_server_destroy(cx_server* s);
 
 #ifdef __cplusplus
 }

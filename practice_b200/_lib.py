@@ -25,6 +25,8 @@ EXPORTS = [
     "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse", "cx_compact_sparse_noalloc",
     "cx_gen_uniform", "cx_gen_datekey", "cx_gen_validity", "cx_plan_literals", "cx_shared_codegen",
     "cx_shared_execute", "cx_ctx_set_column_range", "cx_ctx_set_graph_replay",
+    "cx_server_config_default", "cx_server_create", "cx_server_prepare", "cx_server_submit", "cx_server_wait",
+    "cx_server_fetch", "cx_server_release", "cx_server_get_stats", "cx_server_destroy",
 ]
 
 
@@ -49,6 +51,24 @@ class ResultInfo(C.Structure):
 class SharedQuery(C.Structure):
     _fields_ = [("shape", C.c_int), ("param_off", C.c_int), ("result", C.c_void_p), ("result_words", C.c_uint64),
                 ("validity", C.c_void_p), ("validity_words", C.c_uint64)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("budget_bytes", C.c_uint64), ("max_batch", C.c_int), ("slots", C.c_int), ("plain_only", C.c_int),
+                ("shared_tuning", Tuning)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("kernel_error", C.c_uint32), ("words", C.c_uint64),
+                ("validity_words", C.c_uint64), ("queue_ms", C.c_double), ("latency_ms", C.c_double),
+                ("batch_size", C.c_int), ("shared", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("rejected", C.c_uint64),
+                ("launches", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
+                ("mean_batch", C.c_double), ("queries_per_s", C.c_double), ("budget_bytes", C.c_uint64),
+                ("peak_reserved_bytes", C.c_uint64)]
 
 
 class Timing(C.Structure):
@@ -80,6 +100,15 @@ def _load() -> C.CDLL:
         "cx_ctx_set_sm_count": (C.c_int, [vp, C.c_int]),
         "cx_ctx_set_column_range": (C.c_int, [vp, C.c_char_p, i64, i64]),
         "cx_ctx_set_graph_replay": (C.c_int, [vp, C.c_int]),
+        "cx_server_config_default": (None, [C.POINTER(ServerConfig)]),
+        "cx_server_create": (C.c_int, [vp, C.POINTER(ServerConfig), C.POINTER(vp)]),
+        "cx_server_prepare": (C.c_int, [vp, C.c_char_p, sz]),
+        "cx_server_submit": (C.c_int, [vp, C.c_char_p, sz, C.POINTER(u64)]),
+        "cx_server_wait": (C.c_int, [vp, u64, C.c_int, C.POINTER(RequestInfo)]),
+        "cx_server_fetch": (C.c_int, [vp, u64, vp, u64, vp, u64]),
+        "cx_server_release": (C.c_int, [vp, u64]),
+        "cx_server_get_stats": (C.c_int, [vp, C.c_int, C.POINTER(ServerStats)]),
+        "cx_server_destroy": (C.c_int, [vp]),
         "cx_execute": (C.c_int, [vp, vp, vp]),
         "cx_ctx_sync": (C.c_int, [vp]),
         "cx_ctx_timing": (C.c_int, [vp, C.POINTER(Timing)]),
@@ -237,6 +266,72 @@ class ExecCtx:
             self.handle = None
 
     def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def server_config(**kw) -> ServerConfig:
+    cfg = ServerConfig()
+    lib.cx_server_config_default(C.byref(cfg))
+    for k, v in kw.items():
+        if k == "shared_tuning":
+            cfg.shared_tuning = v
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+class Server:
+    """The request loop (cx_server_*): submit plans as they arrive, wait for
+    and fetch each result; queries are admitted against the HBM budget and
+    fused into shared-scan launches by the library's scheduler thread."""
+
+    def __init__(self, tables: "ExecCtx", cfg: ServerConfig | None = None):
+        self.handle = C.c_void_p()
+        check(lib.cx_server_create(tables.handle, C.byref(cfg) if cfg is not None else None, C.byref(self.handle)),
+              "cx_server_create")
+
+    def prepare(self, plan_text: str) -> None:
+        raw = plan_text.encode()
+        check(lib.cx_server_prepare(self.handle, raw, len(raw)), "cx_server_prepare")
+
+    def submit(self, plan_text: str) -> int:
+        raw = plan_text.encode()
+        rid = C.c_uint64()
+        check(lib.cx_server_submit(self.handle, raw, len(raw), C.byref(rid)), "cx_server_submit")
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> RequestInfo:
+        info = RequestInfo()
+        rc = lib.cx_server_wait(self.handle, rid, timeout_ms, C.byref(info))
+        if rc not in (CX_OK, -6):
+            check(rc, "cx_server_wait")
+        return info
+
+    def fetch(self, rid: int, info: RequestInfo):
+        import numpy as np
+
+        w = np.zeros(max(int(info.words), 1), dtype=np.uint64)
+        v = np.zeros(max(int(info.validity_words), 1), dtype=np.uint64)
+        check(lib.cx_server_fetch(self.handle, rid, w.ctypes.data, w.size, v.ctypes.data, v.size), "cx_server_fetch")
+        return w[: int(info.words)], v[: int(info.validity_words)]
+
+    def release(self, rid: int) -> None:
+        check(lib.cx_server_release(self.handle, rid), "cx_server_release")
+
+    def stats(self, reset: bool = False) -> ServerStats:
+        st = ServerStats()
+        check(lib.cx_server_get_stats(self.handle, int(reset), C.byref(st)), "cx_server_get_stats")
+        return st
+
+    def close(self) -> None:
+        if self.handle:
+            lib.cx_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
         try:
             self.close()
         except Exception:

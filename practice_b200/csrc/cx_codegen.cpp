@@ -2153,4 +2153,17 @@ std::string generate_shared_cuda(const std::vector<const Plan*>& shapes, const T
   return g.run();
 }
 
+bool shared_shape_ok(const Plan& plan, std::string* why) {
+  std::vector<const Plan*> one{&plan};
+  Tuning t;
+  SharedGen g(one, t);
+  try {
+    g.collect();
+  } catch (const PlanError& e) {
+    if (why) *why = e.what();
+    return false;
+  }
+  return true;
+}
+
 }  // namespace cx

@@ -37,4 +37,8 @@ void collect_literals(const Plan& plan, std::vector<const Expr*>& out);
 // dimension, conflicting joins, literals outside int32).
 std::string generate_shared_cuda(const std::vector<const Plan*>& shapes, const Tuning& tuning);
 
+// Whether one plan shape can join a shared scan (the checks of
+// generate_shared_cuda without generating code); `why` gets the reason if not.
+bool shared_shape_ok(const Plan& plan, std::string* why);
+
 }  // namespace cx

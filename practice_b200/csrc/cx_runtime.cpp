@@ -29,6 +29,7 @@
 #include "../../include/crystal_b200.h"
 #include "cx_args.h"
 #include "cx_codegen.h"
+#include "cx_internal.h"
 #include "cx_plan.h"
 
 // Generated at build time from crystal_sm100.cuh and cx_args.h.
@@ -358,6 +359,30 @@ int ensure_ctx_device(cx_exec_ctx* c, int dev) {
 }
 
 }  // namespace
+
+// ============================================================ internal ===
+namespace cx_internal {
+
+void ctx_copy_tables(const cx_exec_ctx* src, cx_exec_ctx* dst) {
+  dst->buffers = src->buffers;
+  dst->nulls = src->nulls;
+  dst->rows = src->rows;
+  dst->ranges = src->ranges;
+}
+
+bool ctx_column_range(const cx_exec_ctx* c, const std::string& name, int64_t* lo, int64_t* hi) {
+  auto it = c->ranges.find(name);
+  if (it == c->ranges.end()) return false;
+  *lo = it->second.first;
+  *hi = it->second.second;
+  return true;
+}
+
+uint64_t ctx_scratch_bytes(const cx_exec_ctx* c) { return c->own_scratch_bytes; }
+
+int set_error(int code, const std::string& msg) { return fail(code, "%s", msg.c_str()); }
+
+}  // namespace cx_internal
 
 // ================================================================== C ABI ===
 extern "C" {

@@ -7,6 +7,7 @@
 #include <string>
 
 struct cx_exec_ctx;
+struct cx_module;
 
 namespace cx_internal {
 
@@ -19,6 +20,14 @@ bool ctx_column_range(const cx_exec_ctx* c, const std::string& name, int64_t* lo
 
 // Device bytes the context holds as its own scratch (hash tables, indexes).
 uint64_t ctx_scratch_bytes(const cx_exec_ctx* c);
+
+// Scratch bytes cx_shared_execute needs for a batch of queries of `shapes`
+// (program shape indexes) on program `m`.
+uint64_t shared_scratch_need(const cx_module* m, const int* shapes, int nq);
+
+// Scratch bytes a context owns after an execute that needs `need` bytes, when
+// it owns `own` bytes before (own scratch grows to 1.5x the need).
+uint64_t grown_scratch(uint64_t own, uint64_t need);
 
 // Records `msg` as the calling thread's cx_last_error() and returns `code`.
 int set_error(int code, const std::string& msg);

@@ -382,6 +382,28 @@ uint64_t ctx_scratch_bytes(const cx_exec_ctx* c) { return c->own_scratch_bytes; 
 
 int set_error(int code, const std::string& msg) { return fail(code, "%s", msg.c_str()); }
 
+uint64_t grown_scratch(uint64_t own, uint64_t need) { return own >= need ? own : need + need / 2; }
+
+uint64_t shared_scratch_need(const cx_module* m, const int* shapes, int nq) {
+  const LaunchPlan& lp = m->lp;
+  uint64_t off = 0;
+  for (const auto& h : lp.hts) {
+    off = align256(off + h.words * 4);
+    auto it = lp.dat_words.find(h.slot);
+    if (it != lp.dat_words.end()) off = align256(off + it->second * 4);
+  }
+  for (int i = 0; i < nq; ++i) {
+    if (shapes[i] < 0 || shapes[i] >= (int)lp.sshapes.size()) continue;
+    const auto& sh = lp.sshapes[shapes[i]];
+    if (sh.grouped) off = align256(off + ((sh.groups + 31) / 32) * 4);
+  }
+  const int maxq = std::max(1, std::min(lp.shared_maxq, 256));
+  const int npass = (nq + maxq - 1) / maxq;
+  const uint64_t pass_bytes = align256((uint64_t)maxq * sizeof(CxSQ) + (uint64_t)std::max(lp.shared_maxp, 1) * 4);
+  off += (uint64_t)std::max(npass, 1) * pass_bytes;
+  return align256(off + 16);
+}
+
 }  // namespace cx_internal
 
 // ================================================================== C ABI ===

@@ -259,7 +259,10 @@ int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Req
     r->words = std::max<uint64_t>(1, info.result_words);
     r->vwords = std::max<uint64_t>(1, info.validity_words);
     r->final_words = info.final_words;
-    r->est_bytes = (r->words + r->vwords) * 8 + scratch;
+    r->est_bytes = (r->words + r->vwords) * 8;
+    if (r->est_bytes + scratch > s->cfg.budget_bytes)
+      return serr(CX_E_REJECTED, "cx_server_submit: the query needs %llu bytes, the budget is %llu",
+                  (unsigned long long)(r->est_bytes + scratch), (unsigned long long)s->cfg.budget_bytes);
   }
   *out = std::move(r);
   return CX_OK;
@@ -391,25 +394,33 @@ void scheduler(cx_server* s) {
     for (Slot& sl : s->slots) {
       if (sl.busy || s->pending.empty()) continue;
       const uint64_t fixed = fixed_bytes(s);
+      const uint64_t own = cx_internal::ctx_scratch_bytes(sl.ctx);
       std::vector<Request*> batch;
       Request* head = s->pending.front();
-      auto fits = [&](const Request* r) {
-        // A request alone on an idle GPU is always admitted (its size was
-        // checked against the budget at submit).
-        return s->reserved + fixed + r->est_bytes <= s->cfg.budget_bytes || (s->reserved == 0 && batch.empty());
+      // Admission: what is reserved, the scratch the slots own, the scratch
+      // this launch adds to its slot and the new queries' bytes must fit the
+      // budget.  A launch on an idle GPU always goes (sizes were checked
+      // against the whole budget at submit).
+      auto admit = [&](uint64_t growth, uint64_t add) {
+        return s->reserved + fixed + growth + add <= s->cfg.budget_bytes || (s->reserved == 0 && batch.empty());
       };
       bool shared = head->shared && s->universe && s->shape_index.at(head->shape) < (int)s->universe_shapes;
       if (!head->shared) {
-        if (fits(head)) {
+        uint64_t need = 0;
+        cx_module_scratch_bytes(head->plain, sl.ctx, &need);
+        if (admit(cx_internal::grown_scratch(own, need) - own, head->est_bytes)) {
           batch.push_back(head);
           s->pending.pop_front();
         }
       } else if (shared) {
         uint64_t add = 0;
+        std::vector<int> shapes;
         while (!s->pending.empty() && (int)batch.size() < s->cfg.max_batch) {
           Request* r = s->pending.front();
           if (!r->shared || s->shape_index.at(r->shape) >= (int)s->universe_shapes) break;
-          if (!(s->reserved + fixed + add + r->est_bytes <= s->cfg.budget_bytes || (s->reserved == 0 && batch.empty()))) break;
+          shapes.push_back(s->shape_index.at(r->shape));
+          const uint64_t need = cx_internal::shared_scratch_need(s->universe, shapes.data(), (int)shapes.size());
+          if (!admit(cx_internal::grown_scratch(own, need) - own, add + r->est_bytes)) break;
           add += r->est_bytes;
           batch.push_back(r);
           s->pending.pop_front();
@@ -418,7 +429,7 @@ void scheduler(cx_server* s) {
       if (batch.empty()) break;
       launch(s, sl, batch, shared && head->shared);
       s->reserved += sl.reserved;
-      s->peak_reserved = std::max(s->peak_reserved, s->reserved + fixed);
+      s->peak_reserved = std::max(s->peak_reserved, s->reserved + fixed_bytes(s));
       progressed = true;
     }
     bool busy = false;

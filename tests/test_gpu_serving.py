@@ -87,14 +87,25 @@ def test_server_stream_results_equal_alone_and_oracle(db):
 
 
 def test_server_admission_under_a_small_budget(db):
-    """A budget that holds the batch scratch and a few result tables: queries
-    wait for memory, run in smaller launches, all still exact; a query larger
-    than the whole budget is refused."""
+    """A budget that holds the slots' scratch and a few large result tables:
+    queries wait for memory, run in smaller launches and are all still exact;
+    a query larger than the whole budget is refused."""
     n = 300_007
     ht = load(db, 52, n)
     rng = random.Random(9)
-    plans = [queries.template(3, rng, n) for _ in range(12)] + [queries.template(1, rng, n) for _ in range(12)]
-    budget = 12 << 20
+    tables = datagen.ssb_tables(n, queries.BATCH_COLS)
+    big = []
+    for k in range(8):  # 1000 brands x 25 nations x 7 years: 4.2 MB of result words each
+        b = PlanBuilder(tables, "LINEORDER", name="big")
+        b.join("CUSTOMER", "lo_custkey", where=col("c_region").le(k % 5))
+        b.join("PART", "lo_partkey")
+        b.join("DDATE", "lo_orderdate")
+        big.append(b.aggregate([queries._g("p_brand1"), queries._g("c_nation"), queries._g("d_year")],
+                               [("sum", col("lo_revenue"))]))
+    plans = big + [queries.template(3, rng, n) for _ in range(6)] + [queries.template(1, rng, n) for _ in range(6)]
+    # Two slots' dimension indexes (about 14 MB each once grown) plus room for
+    # about three of the big result tables at a time.
+    budget = 40 << 20
     srv = _lib.Server(db.ctx, _lib.server_config(max_batch=64, slots=2, budget_bytes=budget))
     try:
         b = PlanBuilder(datagen.ssb_tables(n, queries.BATCH_COLS), "LINEORDER", name="huge")
@@ -113,6 +124,7 @@ def test_server_admission_under_a_small_budget(db):
         st = srv.stats()
         assert st.completed == len(plans) and st.rejected == 1
         assert st.peak_reserved_bytes <= budget
+        assert st.launches >= 3, "the big queries cannot all be admitted at once"
     finally:
         srv.close()
 

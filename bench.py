@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-sample-rows", type=int, default=4_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=1000.0, help="Poisson arrivals per second (serving leg)")
+    ap.add_argument("--serve-requests", type=int, default=2000, help="requests in the serving leg (0 skips it)")
     return ap.parse_args()
 
 
@@ -190,6 +192,70 @@ def reference_arm(args):
         "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def serving_leg(db, plans, args, shared_tuning):
+    """The request loop under a Poisson arrival stream drawn from the batch's
+    queries: the shared loop (continuous batching into shared scans) and the
+    plain one-query-at-a-time loop over the same stream, plus each query's
+    latency alone on an idle GPU."""
+    import numpy as np
+
+    from practice_b200 import _lib
+
+    rng = np.random.default_rng(args.seed)
+    n = args.serve_requests
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
+    picks = rng.integers(0, len(plans), n)
+    texts = [p.text() for p in plans]
+
+    def stream(srv):
+        srv.stats(reset=True)
+        ids = []
+        t0 = time.perf_counter()
+        for i in range(n):
+            target = t0 + arrivals[i]
+            while time.perf_counter() < target:
+                pass
+            ids.append(srv.submit(texts[picks[i]]))
+        bad = 0
+        for rid in ids:
+            info = srv.wait(rid)
+            bad += int(info.status != 0 or info.kernel_error != 0)
+            srv.release(rid)
+        st = srv.stats()
+        return {"queries_per_s": st.queries_per_s, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "max_ms": st.max_ms,
+                "mean_batch": st.mean_batch, "launches": int(st.launches), "failed": bad,
+                "peak_reserved_GB": st.peak_reserved_bytes / 1e9}
+
+    plain = _lib.Server(db.ctx, _lib.server_config(plain_only=1, slots=1))
+    try:
+        for t in texts:
+            plain.prepare(t)
+        lone = []
+        for t in texts:  # each query alone on an idle GPU, submit to result on the host
+            for _ in range(2):
+                info = plain.wait(plain.submit(t))
+            lone.append(info.latency_ms)
+        plain_stream = stream(plain)
+    finally:
+        plain.close()
+    cfg = _lib.server_config(max_batch=64, slots=2)
+    if shared_tuning is not None:
+        cfg.shared_tuning = shared_tuning
+    srv = _lib.Server(db.ctx, cfg)
+    try:
+        for t in texts:
+            srv.prepare(t)
+        shared_stream = stream(srv)
+    finally:
+        srv.close()
+    lone_ms = float(np.median(lone))
+    return {"arrivals": f"Poisson, {args.serve_rate:g} queries/s, {n} requests drawn from the batch's {len(plans)} queries",
+            "budget_GB": 40 * 2**30 / 1e9, "lone_query_ms": {"median": lone_ms, "max": float(np.max(lone))},
+            "shared_loop": shared_stream, "plain_loop": plain_stream,
+            "shared_vs_plain_queries_per_s": shared_stream["queries_per_s"] / max(plain_stream["queries_per_s"], 1e-9),
+            "shared_p99_vs_lone": shared_stream["p99_ms"] / lone_ms}
 
 
 def config_block(args):
@@ -381,6 +447,13 @@ def main():
            "d2h_bytes_per_step": int(d2h),
            "note": "fact table resident in HBM; query descriptors uploaded and every result read back each step"}
 
+    serving = None
+    if rank == 0 and world == 1 and args.serve_requests > 0 and shared is not None:
+        try:
+            serving = serving_leg(db, plans, args, db.shared_tuning_for(plans))
+        except Exception as e:  # reported, not fatal
+            serving = {"error": str(e)[:300]}
+
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -422,6 +495,7 @@ def main():
             "plain": plain,
             "shared_vs_plain": (value / plain["queries_per_s"]) if shared is not None else 1.0,
             "shared_tuning": shared["tuning"] if shared is not None else None,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

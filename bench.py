@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-rate", type=float, default=1000.0, help="Poisson arrivals per second (serving leg)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests in the serving leg (0 skips it)")
+    ap.add_argument("--serve-low-rate", type=float, default=100.0, help="second, light-load arrival rate")
+    ap.add_argument("--serve-slots", type=int, default=2, help="launches in flight in the shared loop")
     return ap.parse_args()
 
 
@@ -203,13 +205,12 @@ def serving_leg(db, plans, args, shared_tuning):
 
     from practice_b200 import _lib
 
-    rng = np.random.default_rng(args.seed)
-    n = args.serve_requests
-    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
-    picks = rng.integers(0, len(plans), n)
     texts = [p.text() for p in plans]
 
-    def stream(srv):
+    def stream(srv, rate, n):
+        rng = np.random.default_rng(args.seed)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+        picks = rng.integers(0, len(plans), n)
         srv.stats(reset=True)
         ids = []
         t0 = time.perf_counter()
@@ -237,25 +238,33 @@ def serving_leg(db, plans, args, shared_tuning):
             for _ in range(2):
                 info = plain.wait(plain.submit(t))
             lone.append(info.latency_ms)
-        plain_stream = stream(plain)
+        n_low = max(50, int(args.serve_requests * args.serve_low_rate / args.serve_rate * 3))
+        plain_stream = stream(plain, args.serve_rate, args.serve_requests)
+        plain_low = stream(plain, args.serve_low_rate, n_low)
     finally:
         plain.close()
-    cfg = _lib.server_config(max_batch=64, slots=2)
+    cfg = _lib.server_config(max_batch=64, slots=args.serve_slots)
     if shared_tuning is not None:
         cfg.shared_tuning = shared_tuning
     srv = _lib.Server(db.ctx, cfg)
     try:
         for t in texts:
             srv.prepare(t)
-        shared_stream = stream(srv)
+        shared_stream = stream(srv, args.serve_rate, args.serve_requests)
+        shared_low = stream(srv, args.serve_low_rate, n_low)
     finally:
         srv.close()
     lone_ms = float(np.median(lone))
-    return {"arrivals": f"Poisson, {args.serve_rate:g} queries/s, {n} requests drawn from the batch's {len(plans)} queries",
-            "budget_GB": 40 * 2**30 / 1e9, "lone_query_ms": {"median": lone_ms, "max": float(np.max(lone))},
-            "shared_loop": shared_stream, "plain_loop": plain_stream,
-            "shared_vs_plain_queries_per_s": shared_stream["queries_per_s"] / max(plain_stream["queries_per_s"], 1e-9),
-            "shared_p99_vs_lone": shared_stream["p99_ms"] / lone_ms}
+    return {"arrivals": f"Poisson, drawn from the batch's {len(plans)} queries; budget 40 GiB",
+            "lone_query_ms": {"median": lone_ms, "max": float(np.max(lone))},
+            "high_load": {"rate_per_s": args.serve_rate, "requests": args.serve_requests,
+                          "shared_loop": shared_stream, "plain_loop": plain_stream,
+                          "shared_vs_plain_queries_per_s": shared_stream["queries_per_s"] / max(plain_stream["queries_per_s"], 1e-9),
+                          "shared_p99_vs_lone": shared_stream["p99_ms"] / lone_ms},
+            "light_load": {"rate_per_s": args.serve_low_rate, "requests": n_low,
+                           "shared_loop": shared_low, "plain_loop": plain_low,
+                           "shared_p99_vs_lone": shared_low["p99_ms"] / lone_ms,
+                           "plain_p99_vs_lone": plain_low["p99_ms"] / lone_ms}}
 
 
 def config_block(args):

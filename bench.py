@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=1000.0, help="Poisson arrivals per second (serving leg)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests in the serving leg (0 skips it)")
     ap.add_argument("--serve-low-rate", type=float, default=100.0, help="second, light-load arrival rate")
-    ap.add_argument("--serve-slots", type=int, default=2, help="launches in flight in the shared loop")
+    ap.add_argument("--serve-slots", type=int, default=1, help="launches in flight in the shared loop")
     return ap.parse_args()
 
 
@@ -231,8 +231,8 @@ def serving_leg(db, plans, args, shared_tuning):
 
     plain = _lib.Server(db.ctx, _lib.server_config(plain_only=1, slots=1))
     try:
-        for t in texts:
-            plain.prepare(t)
+        for p in plans:  # the plain loop runs each query with its autotuned kernel
+            plain.prepare(p.text(), db.tuning_for(p))
         lone = []
         for t in texts:  # each query alone on an idle GPU, submit to result on the host
             for _ in range(2):

@@ -239,7 +239,7 @@ typedef struct cx_server cx_server;
 typedef struct cx_server_config {
   uint64_t budget_bytes;  /* HBM for per-query results, hash tables and batch scratch */
   int max_batch;          /* queries per shared launch, 1..256 (64 per pass) */
-  int slots;              /* launches in flight, each on its own stream, 1..8 */
+  int slots;              /* launches in flight, each on its own stream, 1..8 (default 1) */
   int plain_only;         /* 1: every query runs alone through its plain kernel (baseline loop) */
   cx_tuning shared_tuning;/* launch shape of the shared-scan programs */
 } cx_server_config;
@@ -270,6 +270,9 @@ int cx_server_create(const cx_exec_ctx* tables, const cx_server_config* cfg, cx_
 /* Compiles what a plan needs ahead of its first submission (its shared
  * program shape or its plain kernel), so no request waits for NVRTC. */
 int cx_server_prepare(cx_server* s, const char* plan, size_t plan_len);
+/* Same, compiling the plan's plain kernel with `plain_tuning` (e.g. the
+ * autotuned launch shape of its shape) for when the plan runs alone. */
+int cx_server_prepare_tuned(cx_server* s, const char* plan, size_t plan_len, const cx_tuning* plain_tuning);
 /* Queues one query; `id` identifies it to wait / fetch / release.  A plan
  * whose estimated bytes exceed the whole budget is refused (CX_E_REJECTED). */
 int cx_server_submit(cx_server* s, const char* plan, size_t plan_len, uint64_t* id);

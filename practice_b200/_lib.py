@@ -25,7 +25,8 @@ EXPORTS = [
     "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse", "cx_compact_sparse_noalloc",
     "cx_gen_uniform", "cx_gen_datekey", "cx_gen_validity", "cx_plan_literals", "cx_shared_codegen",
     "cx_shared_execute", "cx_ctx_set_column_range", "cx_ctx_set_graph_replay",
-    "cx_server_config_default", "cx_server_create", "cx_server_prepare", "cx_server_submit", "cx_server_wait",
+    "cx_server_config_default", "cx_server_create", "cx_server_prepare", "cx_server_prepare_tuned",
+    "cx_server_submit", "cx_server_wait",
     "cx_server_fetch", "cx_server_release", "cx_server_get_stats", "cx_server_destroy",
 ]
 
@@ -103,6 +104,7 @@ def _load() -> C.CDLL:
         "cx_server_config_default": (None, [C.POINTER(ServerConfig)]),
         "cx_server_create": (C.c_int, [vp, C.POINTER(ServerConfig), C.POINTER(vp)]),
         "cx_server_prepare": (C.c_int, [vp, C.c_char_p, sz]),
+        "cx_server_prepare_tuned": (C.c_int, [vp, C.c_char_p, sz, C.POINTER(Tuning)]),
         "cx_server_submit": (C.c_int, [vp, C.c_char_p, sz, C.POINTER(u64)]),
         "cx_server_wait": (C.c_int, [vp, u64, C.c_int, C.POINTER(RequestInfo)]),
         "cx_server_fetch": (C.c_int, [vp, u64, vp, u64, vp, u64]),
@@ -293,9 +295,12 @@ class Server:
         check(lib.cx_server_create(tables.handle, C.byref(cfg) if cfg is not None else None, C.byref(self.handle)),
               "cx_server_create")
 
-    def prepare(self, plan_text: str) -> None:
+    def prepare(self, plan_text: str, plain_tuning: Tuning | None = None) -> None:
         raw = plan_text.encode()
-        check(lib.cx_server_prepare(self.handle, raw, len(raw)), "cx_server_prepare")
+        if plain_tuning is None:
+            check(lib.cx_server_prepare(self.handle, raw, len(raw)), "cx_server_prepare")
+        else:
+            check(lib.cx_server_prepare_tuned(self.handle, raw, len(raw), C.byref(plain_tuning)), "cx_server_prepare_tuned")
 
     def submit(self, plan_text: str) -> int:
         raw = plan_text.encode()

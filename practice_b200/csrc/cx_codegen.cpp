@@ -1468,7 +1468,7 @@ struct SharedGen {
     const unsigned long long acc_off = off; off += (unsigned long long)MAXQ * NACC * 8;
     const unsigned long long sq_off = off; off += (unsigned long long)MAXQ * 40;
     const unsigned long long fm_off = off; off += (unsigned long long)NFC * FW * 8;
-    const unsigned long long nj_off = off; off += (unsigned long long)(dims.size() + 3) * 8;
+    const unsigned long long nj_off = off; off += (unsigned long long)(dims.size() + 4) * 8;
     off = (off + 15) & ~15ULL;
     // The per-query row bitmaps (STAGES x NB words per query of the pass) and
     // the group tables follow the fixed part; the host sizes both per pass.
@@ -1544,8 +1544,26 @@ struct SharedGen {
       o << "    s_fm[v] = m;\n";
       o << "  }\n";
     }
+    // Fact columns each shape reads (bits over the staged columns).
+    std::vector<unsigned long long> colmask(shapes.size(), 0ULL);
+    if (NSC > 64) throw PlanError("more than 64 fact columns in a shared batch");
+    for (size_t si = 0; si < shapes.size(); ++si) {
+      const Plan& p = *shapes[si];
+      std::vector<std::string> cs;
+      for (const auto& st : p.steps) {
+        if (st.kind == Step::Filter) cols_of(st.filter.get(), cs);
+        else cs.push_back(st.join.fks[0]);
+      }
+      for (const auto& g : p.groups) cols_of(g.expr.get(), cs);
+      for (const auto& ag : p.aggs) cols_of(ag.arg.get(), cs);
+      for (const auto& c : cs) {
+        auto it = std::find(fact_cols.begin(), fact_cols.end(), c);
+        if (it != fact_cols.end()) colmask[si] |= 1ULL << (it - fact_cols.begin());
+      }
+    }
     // Masks of the queries that skip each dimension, that carry residual
-    // filters, that have filter-table conjuncts, and of the whole batch.
+    // filters, that have filter-table conjuncts, and of the whole batch; and
+    // the fact columns the batch reads.
     {
       std::vector<unsigned> joins(shapes.size(), 0u);
       std::vector<int> has_res(shapes.size(), 0), has_push(shapes.size(), 0);
@@ -1554,14 +1572,15 @@ struct SharedGen {
         has_res[s] = !preds[s].resid.empty();
         has_push[s] = !preds[s].pushed.empty();
       }
-      o << "  if (threadIdx.x < " << dims.size() + 3 << ") {\n";
+      o << "  if (threadIdx.x < " << dims.size() + 4 << ") {\n";
       o << "    const int t_ = threadIdx.x;\n";
       o << "    unsigned long long m = 0ULL;\n";
       o << "    for (int q = 0; q < nq; ++q) {\n";
-      o << "      unsigned j_ = 0u; int r_ = 0, p_ = 0;\n";
+      o << "      unsigned j_ = 0u; int r_ = 0, p_ = 0; unsigned long long c_ = 0ULL;\n";
       o << "      switch (s_sq[q].shape) {\n";
       for (size_t s = 0; s < shapes.size(); ++s)
-        o << "        case " << s << ": j_ = " << joins[s] << "u; r_ = " << has_res[s] << "; p_ = " << has_push[s] << "; break;\n";
+        o << "        case " << s << ": j_ = " << joins[s] << "u; r_ = " << has_res[s] << "; p_ = " << has_push[s]
+          << "; c_ = " << colmask[s] << "ULL; break;\n";
       o << "        default: break;\n";
       o << "      }\n";
       o << "      bool b_ = false;\n";
@@ -1569,7 +1588,8 @@ struct SharedGen {
       o << "      else if (t_ == " << dims.size() << ") b_ = r_ != 0;\n";
       o << "      else if (t_ == " << dims.size() + 1 << ") b_ = p_ != 0;\n";
       o << "      else b_ = true;\n";
-      o << "      if (b_) m |= 1ULL << q;\n";
+      o << "      if (t_ == " << dims.size() + 3 << ") m |= c_;\n";
+      o << "      else if (b_) m |= 1ULL << q;\n";
       o << "    }\n";
       o << "    s_nj[t_] = m;\n";
       o << "  }\n";
@@ -1594,16 +1614,22 @@ struct SharedGen {
     o << "    cx::fence_mbar_init();\n";
     o << "    l2_policy = cx::l2_evict_first_policy();\n";
     o << "  }\n";
+    // Only the columns the batch's shapes read are staged.
     o << "#define CX_ISSUE(TILE_, STAGE_) do { \\\n";
-    o << "    cx::mbar_expect_tx(&bar_full[(STAGE_)], " << (unsigned long long)NSC * TR * 4 << "u); \\\n";
+    o << "    cx::mbar_expect_tx(&bar_full[(STAGE_)], stage_tx); \\\n";
     for (int c = 0; c < NSC; ++c)
-      o << "    cx::bulk_g2s(stage_buf + ((STAGE_) * NSC + " << c << ") * TR, d_" << fact_cols[c] << " + (TILE_) * TR, "
-        << TR * 4 << "u, &bar_full[(STAGE_)], l2_policy); \\\n";
+      o << "    if ((m_cols >> " << c << ") & 1ULL) cx::bulk_g2s(stage_buf + ((STAGE_) * NSC + " << c << ") * TR, d_" << fact_cols[c]
+        << " + (TILE_) * TR, " << TR * 4 << "u, &bar_full[(STAGE_)], l2_policy); \\\n";
     o << "  } while (0)\n";
     o << "  __syncthreads();\n";
     o << "  const unsigned long long m_res = s_nj[" << dims.size() << "], m_push = s_nj[" << dims.size() + 1
       << "], m_all = s_nj[" << dims.size() + 2 << "];\n";
     o << "  (void)m_res; (void)m_push;\n";
+    o << "  const unsigned long long m_cols = s_nj[" << dims.size() + 3 << "];\n";
+    o << "  const unsigned stage_tx = (unsigned)__popcll(m_cols) * (unsigned)(TR * 4);\n";
+    o << "  (void)stage_tx;\n";
+    for (size_t di = 0; di < dims.size(); ++di)
+      o << "  const unsigned long long jm" << di << " = m_all & ~s_nj[" << di << "];  // queries joining " << dims[di].name << "\n";
     o << "  const int slices = nq > 0 ? (NCW + nq - 1) / nq : 1;\n";
     o << "  const int units = nq * slices;\n";
     const std::string LIM = std::to_string(wait_limit) + "u";
@@ -1671,7 +1697,8 @@ struct SharedGen {
     o << "        if (i < n_tile) {\n";
     o << "          unsigned long long m = m_all;\n";
     for (int k = 0; k < NFC; ++k) {
-      o << "          { const unsigned d_ = (unsigned)S_" << fcols[k] << "[i] - fb" << k << ";\n";
+      const int ck = (int)(std::find(fact_cols.begin(), fact_cols.end(), fcols[k]) - fact_cols.begin());
+      o << "          if ((m_cols >> " << ck << ") & 1ULL) { const unsigned d_ = (unsigned)S_" << fcols[k] << "[i] - fb" << k << ";\n";
       o << "            if (d_ < fw" << k << ") m &= s_fm[" << k * FW << " + d_]; else ow_[j] = true; }\n";
     }
     o << "          mk_[j] = m;\n";
@@ -1686,9 +1713,10 @@ struct SharedGen {
       const Dim& d = dims[di];
       o << "        {\n";
       o << "          g" << di << "_[j] = make_int4(0, 0, 0, 0);\n";
-      o << "          const int fk_ = live_ ? S_" << d.fk << "[i] : 0;\n";
+      o << "          const bool need_ = live_ && (mk_[j] & jm" << di << ") != 0ULL;\n";
+      o << "          const int fk_ = need_ ? S_" << d.fk << "[i] : 0;\n";
       o << "          const int h_ = (int)HASH(fk_, " << d.len << ", " << d.keymin << ");\n";
-      o << "          if (live_ && (unsigned)h_ < " << d.len << "u) g" << di << "_[j] = __ldg(&dkm_" << lower(d.name) << "[h_]);\n";
+      o << "          if (need_ && (unsigned)h_ < " << d.len << "u) g" << di << "_[j] = __ldg(&dkm_" << lower(d.name) << "[h_]);\n";
       o << "        }\n";
     }
     o << "      }\n";

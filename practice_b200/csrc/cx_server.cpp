@@ -177,7 +177,8 @@ int rebuild_universe(cx_server* s) {
 
 // Parses and classifies a plan; compiles what it needs.  Returns a request
 // without an id.
-int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Request>* out) {
+int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Request>* out,
+                 const cx_tuning* plain_tuning = nullptr) {
   auto r = std::make_unique<Request>();
   r->text.assign(plan, len);
   try {
@@ -241,6 +242,16 @@ int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Req
         std::string src;
         try {
           cx::Tuning t;
+          if (plain_tuning) {
+            t.block_threads = plain_tuning->block_threads;
+            t.items_per_thread = plain_tuning->items_per_thread;
+            t.stages = plain_tuning->stages;
+            t.ctas_per_sm = plain_tuning->ctas_per_sm;
+            t.group_placement = plain_tuning->group_placement;
+            t.smem_group_budget = plain_tuning->smem_group_budget;
+            t.bitmap_budget = plain_tuning->bitmap_budget;
+            t.group_merge = plain_tuning->group_merge;
+          }
           src = cx::generate_cuda(p, t);
         } catch (const std::exception& e) {
           return serr(CX_E_INVALID, "plan: %s", e.what());
@@ -448,7 +459,7 @@ void cx_server_config_default(cx_server_config* cfg) {
   memset(cfg, 0, sizeof *cfg);
   cfg->budget_bytes = 40ULL << 30;
   cfg->max_batch = 64;
-  cfg->slots = 2;
+  cfg->slots = 1;
   cfg->plain_only = 0;
   cx_tuning_default(&cfg->shared_tuning);
   cfg->shared_tuning.block_threads = 1024;
@@ -489,9 +500,13 @@ int cx_server_create(const cx_exec_ctx* tables, const cx_server_config* cfg, cx_
 }
 
 int cx_server_prepare(cx_server* s, const char* plan, size_t plan_len) {
-  if (!s || !plan) return CX_E_INVALID;
+  return cx_server_prepare_tuned(s, plan, plan_len, nullptr);
+}
+
+int cx_server_prepare_tuned(cx_server* s, const char* plan, size_t plan_len, const cx_tuning* plain_tuning) {
+  if (!s || !plan) return serr(CX_E_INVALID, "cx_server_prepare: NULL argument");
   std::unique_ptr<Request> r;
-  return make_request(s, plan, plan_len, &r);
+  return make_request(s, plan, plan_len, &r, plain_tuning);
 }
 
 int cx_server_submit(cx_server* s, const char* plan, size_t plan_len, uint64_t* id) {

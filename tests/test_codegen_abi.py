@@ -192,7 +192,7 @@ def test_shared_execute_validates_before_touching_the_gpu():
 
 def test_server_config_defaults_and_create_without_a_device():
     cfg = _lib.server_config()
-    assert cfg.budget_bytes == 40 << 30 and cfg.max_batch == 64 and cfg.slots == 2 and cfg.plain_only == 0
+    assert cfg.budget_bytes == 40 << 30 and cfg.max_batch == 64 and cfg.slots == 1 and cfg.plain_only == 0
     assert cfg.shared_tuning.block_threads == 1024
     bad = _lib.server_config(slots=0)
     with pytest.raises(_lib.CxError) as e:

@@ -32,6 +32,7 @@ def main(argv: list[str] | None = None) -> None:
     ap.add_argument("--rows", type=int, default=30_000_000)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--query", default="T1", help="T0..T3, q11 or q31 (plain mode)")
+    ap.add_argument("--template", type=int, default=-1, help="shared mode: draw every query from this template")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--tuning", nargs="*", default=[], help="key=value launch-shape overrides")
@@ -45,7 +46,11 @@ def main(argv: list[str] | None = None) -> None:
     db = Database(0)
     db.generate_ssb(args.rows, args.seed, queries.BATCH_COLS if args.mode == "shared" else cols)
     if args.mode == "shared":
-        plans = queries.batch(args.batch, args.seed, args.rows)
+        if args.template >= 0:
+            rng = random.Random(args.seed)
+            plans = [queries.template(args.template, rng, args.rows) for _ in range(args.batch)]
+        else:
+            plans = queries.batch(args.batch, args.seed, args.rows)
         t = make_tuning(**{**shared_default, **kw})
         for _ in range(args.reps):
             r = db.execute_shared(plans, t)

@@ -673,12 +673,27 @@ CX_DEVICE bool mbar_try_wait(unsigned long long* bar, unsigned phase) {
   return ok != 0;
 }
 
+// try_wait with a suspend-time hint: the thread sleeps in the barrier until the
+// phase completes or about `ns` nanoseconds pass, instead of spinning.
+CX_DEVICE bool mbar_try_wait_sleep(unsigned long long* bar, unsigned phase, unsigned ns) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(phase), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+
 // Waits for phase `phase` of `bar`; gives up after `limit` polls.  Returns
-// false on timeout so the caller can record an error and leave.
+// false on timeout so the caller can record an error and leave.  After a few
+// quick polls each poll sleeps in the barrier (up to 2 us), so waiting warps
+// leave their issue slots to the warps that work.
 CX_DEVICE bool mbar_wait_bounded(unsigned long long* bar, unsigned phase, unsigned limit) {
   for (unsigned it = 0; it < limit; ++it) {
-    if (mbar_try_wait(bar, phase)) return true;
-    if (it > 64) __nanosleep(64);
+    if (it < 8 ? mbar_try_wait(bar, phase) : mbar_try_wait_sleep(bar, phase, 2000u)) return true;
   }
   return false;
 }

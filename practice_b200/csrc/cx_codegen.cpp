@@ -1630,7 +1630,10 @@ struct SharedGen {
     o << "  (void)stage_tx;\n";
     for (size_t di = 0; di < dims.size(); ++di)
       o << "  const unsigned long long jm" << di << " = m_all & ~s_nj[" << di << "];  // queries joining " << dims[di].name << "\n";
-    o << "  const int slices = nq > 0 ? (NCW + nq - 1) / nq : 1;\n";
+    // Enough (query, slice) units to occupy the aggregation warps, but no
+    // slice under 8 blocks: a small batch leaves warps idle rather than pay a
+    // flush per sliver.
+    o << "  const int slices = nq > 0 ? max(1, min((NCW + nq - 1) / nq, " << std::max(1, NB / 8) << ")) : 1;\n";
     o << "  const int units = nq * slices;\n";
     const std::string LIM = std::to_string(wait_limit) + "u";
     // Per-tile views of one stage.

@@ -1628,8 +1628,6 @@ struct SharedGen {
     o << "  const unsigned long long m_cols = s_nj[" << dims.size() + 3 << "];\n";
     o << "  const unsigned stage_tx = (unsigned)__popcll(m_cols) * (unsigned)(TR * 4);\n";
     o << "  (void)stage_tx;\n";
-    for (size_t di = 0; di < dims.size(); ++di)
-      o << "  const unsigned long long jm" << di << " = m_all & ~s_nj[" << di << "];  // queries joining " << dims[di].name << "\n";
     // Enough (query, slice) units to occupy the aggregation warps, but no
     // slice under 8 blocks: a small batch leaves warps idle rather than pay a
     // flush per sliver.
@@ -1716,10 +1714,9 @@ struct SharedGen {
       const Dim& d = dims[di];
       o << "        {\n";
       o << "          g" << di << "_[j] = make_int4(0, 0, 0, 0);\n";
-      o << "          const bool need_ = live_ && (mk_[j] & jm" << di << ") != 0ULL;\n";
-      o << "          const int fk_ = need_ ? S_" << d.fk << "[i] : 0;\n";
+      o << "          const int fk_ = live_ ? S_" << d.fk << "[i] : 0;\n";
       o << "          const int h_ = (int)HASH(fk_, " << d.len << ", " << d.keymin << ");\n";
-      o << "          if (need_ && (unsigned)h_ < " << d.len << "u) g" << di << "_[j] = __ldg(&dkm_" << lower(d.name) << "[h_]);\n";
+      o << "          if (live_ && (unsigned)h_ < " << d.len << "u) g" << di << "_[j] = __ldg(&dkm_" << lower(d.name) << "[h_]);\n";
       o << "        }\n";
     }
     o << "      }\n";

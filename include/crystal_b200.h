@@ -55,6 +55,8 @@ typedef struct cx_tuning {
   int bitmap_budget;     /* bytes of shared memory for join membership bitmaps (0 = none) */
   int group_merge;       /* 0 auto, 1 merge equal groups within a warp first, 2 per-lane atomics */
   int producer_warps;    /* shared scans: warps that build query masks (0 = 3/8 of the block) */
+  int parametric;        /* plain kernels: 1 = integer literals become launch parameters
+                            (one module per plan shape, literals passed to cx_execute_params) */
 } cx_tuning;
 
 /* Shape of a compiled query's result buffer. */
@@ -142,6 +144,10 @@ int cx_ctx_set_graph_replay(cx_exec_ctx* c, int enable);
  * stream).  Asynchronous: call cx_ctx_sync before reading results.  Replaces
  * IExecutor::execute / DynamicLibraryExecutor::execute. */
 int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream);
+/* cx_execute for a module generated with cx_tuning.parametric = 1: `params`
+ * holds the plan's literals in the order of cx_plan_literals.  No reference
+ * counterpart: the reference compiles a kernel per query text. */
+int cx_execute_params(cx_module* m, cx_exec_ctx* c, const int32_t* params, int nparams, void* stream);
 /* Waits for the context's last execute, reads its device error word and fills
  * timing.  Returns CX_E_KERNEL if a kernel raised an error. */
 int cx_ctx_sync(cx_exec_ctx* c);
@@ -230,8 +236,10 @@ int cx_gen_validity(uint64_t gen_stream, uint64_t seed, uint64_t rows, uint32_t 
  * admits submitted queries in arrival order while their estimated result and
  * hash/group bytes fit the HBM budget, fuses the admitted shareable queries
  * into shared-scan batches (continuous batching: a batch forms from whatever
- * is waiting when a slot frees up), runs the others through their plain
- * kernel, and overlaps `slots` launches on separate streams.  Results are
+ * is waiting when a slot frees up, once at least min_shared_batch wait), runs
+ * the others through their plain kernel -- one parametric module per plan
+ * shape, so new literals compile nothing -- and overlaps `slots` launches on
+ * separate streams.  Results are
  * copied to host memory owned by the server until released.
  * ---------------------------------------------------------------------- */
 typedef struct cx_server cx_server;
@@ -241,6 +249,7 @@ typedef struct cx_server_config {
   int max_batch;          /* queries per shared launch, 1..256 (64 per pass) */
   int slots;              /* launches in flight, each on its own stream, 1..8 (default 1) */
   int plain_only;         /* 1: every query runs alone through its plain kernel (baseline loop) */
+  int min_shared_batch;   /* fewer waiting shareable queries than this run alone (default 5) */
   cx_tuning shared_tuning;/* launch shape of the shared-scan programs */
 } cx_server_config;
 

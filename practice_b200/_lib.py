@@ -22,7 +22,7 @@ EXPORTS = [
     "cx_module_release", "cx_module_result_info", "cx_ctx_create", "cx_ctx_destroy",
     "cx_ctx_set_buffer", "cx_ctx_set_null_bitmap", "cx_ctx_set_table_rows", "cx_ctx_set_result",
     "cx_ctx_set_scratch", "cx_module_scratch_bytes", "cx_ctx_set_sm_count", "cx_execute",
-    "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse", "cx_compact_sparse_noalloc",
+    "cx_execute_params", "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse", "cx_compact_sparse_noalloc",
     "cx_gen_uniform", "cx_gen_datekey", "cx_gen_validity", "cx_plan_literals", "cx_shared_codegen",
     "cx_shared_execute", "cx_ctx_set_column_range", "cx_ctx_set_graph_replay",
     "cx_server_config_default", "cx_server_create", "cx_server_prepare", "cx_server_prepare_tuned",
@@ -40,7 +40,8 @@ class CxError(RuntimeError):
 class Tuning(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("items_per_thread", C.c_int), ("stages", C.c_int),
                 ("ctas_per_sm", C.c_int), ("group_placement", C.c_int), ("smem_group_budget", C.c_int),
-                ("bitmap_budget", C.c_int), ("group_merge", C.c_int), ("producer_warps", C.c_int)]
+                ("bitmap_budget", C.c_int), ("group_merge", C.c_int), ("producer_warps", C.c_int),
+                ("parametric", C.c_int)]
 
 
 class ResultInfo(C.Structure):
@@ -56,7 +57,7 @@ class SharedQuery(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("budget_bytes", C.c_uint64), ("max_batch", C.c_int), ("slots", C.c_int), ("plain_only", C.c_int),
-                ("shared_tuning", Tuning)]
+                ("min_shared_batch", C.c_int), ("shared_tuning", Tuning)]
 
 
 class RequestInfo(C.Structure):
@@ -112,6 +113,7 @@ def _load() -> C.CDLL:
         "cx_server_get_stats": (C.c_int, [vp, C.c_int, C.POINTER(ServerStats)]),
         "cx_server_destroy": (C.c_int, [vp]),
         "cx_execute": (C.c_int, [vp, vp, vp]),
+        "cx_execute_params": (C.c_int, [vp, vp, C.POINTER(C.c_int32), C.c_int, vp]),
         "cx_ctx_sync": (C.c_int, [vp]),
         "cx_ctx_timing": (C.c_int, [vp, C.POINTER(Timing)]),
         "cx_ctx_kernel_error": (C.c_int, [vp, C.POINTER(u32)]),
@@ -239,8 +241,12 @@ class ExecCtx:
     def set_scratch(self, ptr: int | None, nbytes: int) -> None:
         check(lib.cx_ctx_set_scratch(self.handle, ptr, nbytes), "cx_ctx_set_scratch")
 
-    def execute(self, module: Module, stream: int = 0) -> None:
-        check(lib.cx_execute(module.handle, self.handle, stream or None), "cx_execute")
+    def execute(self, module: Module, stream: int = 0, params=None) -> None:
+        if params is None:
+            check(lib.cx_execute(module.handle, self.handle, stream or None), "cx_execute")
+            return
+        pa = (C.c_int32 * max(len(params), 1))(*params)
+        check(lib.cx_execute_params(module.handle, self.handle, pa, len(params), stream or None), "cx_execute_params")
 
     def shared_execute(self, module: Module, queries, params, stream: int = 0) -> None:
         nq = len(queries)

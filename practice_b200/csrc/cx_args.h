@@ -13,6 +13,7 @@
 #define CX_MAX_TABLES 8
 #define CX_MAX_SHAPES 16
 #define CX_MAX_FCOLS 8
+#define CX_MAX_LITS 64
 
 // One query of a shared-scan batch: its own result buffers, its plan shape and
 // the offset of its literal parameters.
@@ -50,4 +51,5 @@ struct CxArgs {
   int* dat[CX_MAX_HTS];                        // extra payload attributes at each dimension's slots
   int fbase[CX_MAX_FCOLS];                     // first value of each fact filter table window
   int fwin[CX_MAX_FCOLS];                      // values in the window (0: evaluate every row per query)
+  int lits[CX_MAX_LITS];                       // literal parameters of a parametric plain kernel
 };

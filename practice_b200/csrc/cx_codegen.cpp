@@ -108,6 +108,11 @@ struct Emitter {
   // (or hoisted registers P<k> when param_regs is set).
   const std::map<const Expr*, int>* lit_index = nullptr;
   bool param_regs = false;
+  int nparams = -1;  // plain parametric kernels: literals read from CxArgs.lits
+
+  std::string param_decl() const {
+    return nparams >= 0 ? "  const int* __restrict__ P = a.lits; (void)P;\n" : "";
+  }
 
   Emitter(const Plan& plan, const Tuning& t) : p(plan), tu(t) {}
 
@@ -310,6 +315,7 @@ struct Emitter {
     tile_ptr = [](const std::string& c) { return "d_" + c + " + tile_offset"; };
     std::ostringstream& o = src;
     o << "extern \"C\" __global__ void __launch_bounds__(128) " << kname << "(const CxArgs a) {\n";
+    o << param_decl();
     o << "  constexpr int BLOCK_THREADS = 128, ITEMS_PER_THREAD = 4, TILE_SIZE = 512;\n";
     o << "  const int tid = threadIdx.x;\n";
     o << "  const long long n_rows = a.rows[" << t << "];\n";
@@ -350,6 +356,7 @@ struct Emitter {
     const std::string kname = "occupancy_" + lower(j.dim);
     meta << "kernel " << kname << " fixed " << (words + 255) / 256 << " 256 0\n";
     src << "extern \"C\" __global__ void __launch_bounds__(256) " << kname << "(const CxArgs a) {\n";
+    src << param_decl();
     src << "  const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n";
     src << "  if (w >= " << words << "LL) return;\n";
     src << "  const int* ht = a.ht[" << h << "];\n";
@@ -510,6 +517,7 @@ struct Emitter {
          "// walks its own sequence of " << WT << "-row tiles; the main loop has no\n"
          "// CTA-wide barrier, so independent warps hide probe latency.\n";
     o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ") " << kname << "(const CxArgs a) {\n";
+    o << param_decl();
     o << "  constexpr int BLOCK_THREADS = 32, ITEMS_PER_THREAD = " << IPT << ", TILE_SIZE = " << WT << ";\n";
     o << "  constexpr int NWARP = " << NW << ", NSTAGE = " << STAGES << ", NSC = " << NSC << ";\n";
     o << "  extern __shared__ __align__(1024) unsigned char cx_smem[];\n";
@@ -1007,6 +1015,7 @@ struct Emitter {
         payload_valid.insert(s.join.payload);
 
     meta << "v 1\n";
+    if (nparams >= 0) meta << "params " << nparams << "\n";
     for (size_t t = 0; t < p.tables.size(); ++t) meta << "table " << t << " " << p.tables[t].name << "\n";
     int h = 0;
     for (const auto& s : p.steps) {
@@ -1053,6 +1062,18 @@ struct Emitter {
 
 std::string generate_cuda_impl(const Plan& plan, const Tuning& tuning) {
   Emitter e(plan, tuning);
+  std::map<const Expr*, int> lm;
+  if (tuning.parametric) {
+    std::vector<const Expr*> lits;
+    collect_literals(plan, lits);
+    if (lits.size() > 64) throw PlanError("more than 64 literals in a parametric kernel");
+    for (size_t k = 0; k < lits.size(); ++k) {
+      if (lits[k]->ival < -2147483647LL || lits[k]->ival > 2147483647LL) throw PlanError("literal outside int32");
+      lm[lits[k]] = (int)k;
+    }
+    e.lit_index = &lm;
+    e.nparams = (int)lits.size();
+  }
   return e.run();
 }
 

@@ -21,6 +21,7 @@ struct Tuning {
   int group_merge = 0;         // 0 auto, 1 warp match-merge, 2 direct per-lane atomics
   int wait_limit_log2 = 24;    // mbarrier poll limit before a wait gives up
   int producer_warps = 0;      // shared scans: warps that build query masks (0 = 3/8 of the block)
+  int parametric = 0;          // plain kernels: literals read from CxArgs.lits at run time
 };
 
 // Returns the CUDA source for `plan` with its launch plan embedded as a

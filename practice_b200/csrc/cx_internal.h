@@ -6,6 +6,9 @@
 #include <cstdint>
 #include <string>
 
+#include "../../include/crystal_b200.h"
+#include "cx_codegen.h"
+
 struct cx_exec_ctx;
 struct cx_module;
 
@@ -28,6 +31,9 @@ uint64_t shared_scratch_need(const cx_module* m, const int* shapes, int nq);
 // Scratch bytes a context owns after an execute that needs `need` bytes, when
 // it owns `own` bytes before (own scratch grows to 1.5x the need).
 uint64_t grown_scratch(uint64_t own, uint64_t need);
+
+// The code generator's tuning for a C-ABI tuning (defaults where null).
+cx::Tuning to_tuning(const cx_tuning* t);
 
 // Records `msg` as the calling thread's cx_last_error() and returns `code`.
 int set_error(int code, const std::string& msg);

@@ -124,6 +124,7 @@ struct LaunchPlan {
   bool shared = false;
   int shared_maxq = 256, shared_maxp = 4096;           // queries / parameters per shared launch
   uint64_t shared_qb_bytes = 0;                        // shared memory of row bitmaps per query of a pass
+  int nparams = -1;                                    // parametric plain kernels: literal count
   std::map<int, uint64_t> dat_words;                   // shared scans: extra payload attributes per dimension
   std::vector<std::pair<int, std::string>> fcols;      // shared scans: fact filter table columns
   struct SShape { uint64_t groups; int ts, grouped, sparse, nlits, smem_ok, naggs; uint64_t tw; int nseen; };
@@ -173,6 +174,9 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       int mq = 0, mp = 0;
       if (ls >> mq >> mp) { lp.shared_maxq = mq; lp.shared_maxp = mp; }
       ls.clear();
+    } else if (k == "params") {
+      ls >> lp.nparams;
+      if (lp.nparams > CX_MAX_LITS) { err = "too many literal parameters"; return false; }
     } else if (k == "sqb") {
       ls >> lp.shared_qb_bytes;
     } else if (k == "dat") {
@@ -382,6 +386,23 @@ uint64_t ctx_scratch_bytes(const cx_exec_ctx* c) { return c->own_scratch_bytes; 
 
 int set_error(int code, const std::string& msg) { return fail(code, "%s", msg.c_str()); }
 
+cx::Tuning to_tuning(const cx_tuning* tuning) {
+  cx::Tuning t;
+  if (tuning) {
+    t.block_threads = tuning->block_threads;
+    t.items_per_thread = tuning->items_per_thread;
+    t.stages = tuning->stages;
+    t.ctas_per_sm = tuning->ctas_per_sm;
+    t.group_placement = tuning->group_placement;
+    t.smem_group_budget = tuning->smem_group_budget;
+    t.bitmap_budget = tuning->bitmap_budget;
+    t.group_merge = tuning->group_merge;
+    t.producer_warps = tuning->producer_warps;
+    t.parametric = tuning->parametric;
+  }
+  return t;
+}
+
 uint64_t grown_scratch(uint64_t own, uint64_t need) { return own >= need ? own : need + need / 2; }
 
 uint64_t shared_scratch_need(const cx_module* m, const int* shapes, int nq) {
@@ -424,24 +445,14 @@ void cx_tuning_default(cx_tuning* t) {
   t->bitmap_budget = d.bitmap_budget;
   t->group_merge = d.group_merge;
   t->producer_warps = d.producer_warps;
+  t->parametric = d.parametric;
 }
 
 int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap, size_t* out_len) {
   if (!plan) return fail(CX_E_INVALID, "cx_codegen: plan is NULL");
   try {
     auto p = cx::parse_plan(std::string(plan, plan_len));
-    cx::Tuning t;
-    if (tuning) {
-      t.block_threads = tuning->block_threads;
-      t.items_per_thread = tuning->items_per_thread;
-      t.stages = tuning->stages;
-      t.ctas_per_sm = tuning->ctas_per_sm;
-      t.group_placement = tuning->group_placement;
-      t.smem_group_budget = tuning->smem_group_budget;
-      t.bitmap_budget = tuning->bitmap_budget;
-      t.group_merge = tuning->group_merge;
-      t.producer_warps = tuning->producer_warps;
-    }
+    const cx::Tuning t = cx_internal::to_tuning(tuning);
     const std::string s = cx::generate_cuda(*p, t);
     if (out_len) *out_len = s.size();
     if (out && out_cap) {
@@ -619,7 +630,9 @@ int cx_module_scratch_bytes(const cx_module* m, const cx_exec_ctx* c, uint64_t* 
   return CX_OK;
 }
 
-int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream_v) {
+int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream_v) { return cx_execute_params(m, c, nullptr, 0, stream_v); }
+
+int cx_execute_params(cx_module* m, cx_exec_ctx* c, const int32_t* params, int nparams, void* stream_v) {
   if (!m || !c) return fail(CX_E_INVALID, "cx_execute: NULL argument");
   const LaunchPlan& lp = m->lp;
   if (lp.shared) return fail(CX_E_INVALID, "cx_execute: a shared-scan program runs through cx_shared_execute");
@@ -628,6 +641,10 @@ int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream_v) {
   // Resolve tables, columns and result buffers before touching the GPU.
   CxArgs a;
   memset(&a, 0, sizeof a);
+  const int want = lp.nparams < 0 ? 0 : lp.nparams;
+  if (nparams != want || (nparams > 0 && !params))
+    return fail(CX_E_INVALID, "cx_execute: the module takes %d literal parameters, %d given", want, nparams);
+  for (int k = 0; k < nparams; ++k) a.lits[k] = params[k];
   std::vector<long long> rows(lp.tables.size(), 0);
   for (size_t t = 0; t < lp.tables.size(); ++t) {
     auto it = c->rows.find(lp.tables[t]);
@@ -707,11 +724,11 @@ int cx_execute(cx_module* m, cx_exec_ctx* c, void* stream_v) {
 
   Driver& d = driver();
   int launches = 0, scan_grid = 0;
-  void* params[] = {&a};
+  void* kargs[] = {&a};
   auto launch = [&](size_t ki, unsigned grid) -> int {
     const KernelSpec& k = lp.kernels[ki];
     if (grid == 0) return CX_OK;
-    CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, (unsigned)k.smem, (CUstream)stream, params, nullptr);
+    CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, (unsigned)k.smem, (CUstream)stream, kargs, nullptr);
     if (r != CUDA_SUCCESS) return drv_fail(r, k.name.c_str());
     ++launches;
     return CX_OK;
@@ -794,18 +811,7 @@ int cx_shared_codegen(const char* const* plans, const size_t* lens, int nshapes,
       owned.push_back(cx::parse_plan(std::string(plans[i], lens[i])));
       shapes.push_back(owned.back().get());
     }
-    cx::Tuning t;
-    if (tuning) {
-      t.block_threads = tuning->block_threads;
-      t.items_per_thread = tuning->items_per_thread;
-      t.stages = tuning->stages;
-      t.ctas_per_sm = tuning->ctas_per_sm;
-      t.group_placement = tuning->group_placement;
-      t.smem_group_budget = tuning->smem_group_budget;
-      t.bitmap_budget = tuning->bitmap_budget;
-      t.group_merge = tuning->group_merge;
-      t.producer_warps = tuning->producer_warps;
-    }
+    const cx::Tuning t = cx_internal::to_tuning(tuning);
     const std::string src = cx::generate_shared_cuda(shapes, t);
     if (out_len) *out_len = src.size();
     if (out && out_cap) {

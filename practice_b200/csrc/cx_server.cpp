@@ -70,7 +70,8 @@ struct Request {
   std::vector<int32_t> lits;
   uint64_t words = 0, vwords = 0, final_words = 0;
   uint64_t est_bytes = 0;
-  cx_module* plain = nullptr;
+  cx_module* plain = nullptr;  // its plain kernel (parametric unless a literal exceeds int32)
+  bool plain_param = false;
   int status = 1;  // 1 queued, 0 running, 2 done
   int rc = CX_OK;
   uint32_t kernel_err = 0;
@@ -147,20 +148,7 @@ int rebuild_universe(cx_server* s) {
   const size_t n = reps.size();
   std::string src;
   try {
-    src = cx::generate_shared_cuda(reps, [&] {
-      cx::Tuning t;
-      const cx_tuning& c = s->cfg.shared_tuning;
-      t.block_threads = c.block_threads;
-      t.items_per_thread = c.items_per_thread;
-      t.stages = c.stages;
-      t.ctas_per_sm = c.ctas_per_sm;
-      t.group_placement = c.group_placement;
-      t.smem_group_budget = c.smem_group_budget;
-      t.bitmap_budget = c.bitmap_budget;
-      t.group_merge = c.group_merge;
-      t.producer_warps = c.producer_warps;
-      return t;
-    }());
+    src = cx::generate_shared_cuda(reps, cx_internal::to_tuning(&s->cfg.shared_tuning));
   } catch (const std::exception& e) {
     return serr(CX_E_INVALID, "shared program: %s", e.what());
   }
@@ -177,6 +165,14 @@ int rebuild_universe(cx_server* s) {
 
 // Parses and classifies a plan; compiles what it needs.  Returns a request
 // without an id.
+std::string tuning_key(const cx_tuning* t) {
+  if (!t) return "default";
+  char buf[256];
+  snprintf(buf, sizeof buf, "%d/%d/%d/%d/%d/%d/%d/%d", t->block_threads, t->items_per_thread, t->stages, t->ctas_per_sm,
+           t->group_placement, t->smem_group_budget, t->bitmap_budget, t->group_merge);
+  return buf;
+}
+
 int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Request>* out,
                  const cx_tuning* plain_tuning = nullptr) {
   auto r = std::make_unique<Request>();
@@ -188,7 +184,15 @@ int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Req
   }
   const cx::Plan& p = *r->plan;
   r->shape = shape_of(r->text);
-  bool shared = !s->cfg.plain_only && cx::shared_shape_ok(p, nullptr);
+  // Literals become launch parameters (plain and shared) when they fit int32.
+  std::vector<const cx::Expr*> lits;
+  cx::collect_literals(p, lits);
+  bool param_ok = lits.size() <= 64;
+  for (const cx::Expr* e : lits) {
+    if (e->ival < -2147483647LL || e->ival > 2147483647LL) param_ok = false;
+    r->lits.push_back((int32_t)e->ival);
+  }
+  bool shared = !s->cfg.plain_only && param_ok && cx::shared_shape_ok(p, nullptr);
   if (shared) {
     // The PHT empty sentinel is key 0: every probed foreign key must be > 0.
     for (const auto& st : p.steps) {
@@ -197,20 +201,46 @@ int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Req
       if (!cx_internal::ctx_column_range(s->tables, "d_" + st.join.fks[0], &lo, &hi) || lo <= 0) shared = false;
     }
   }
-  r->shared = shared;
+  // Its plain kernel: one parametric module per plan shape and tuning, so a
+  // new literal never waits for NVRTC.
+  cx_module* m = nullptr;
+  {
+    std::lock_guard<std::mutex> ck(s->compile_mu);
+    const std::string key = (param_ok ? r->shape : r->text) + "|" + tuning_key(plain_tuning);
+    auto it = s->plain_mods.find(key);
+    if (it != s->plain_mods.end()) {
+      m = it->second;
+    } else {
+      std::string src;
+      try {
+        cx::Tuning t = cx_internal::to_tuning(plain_tuning);
+        t.parametric = param_ok ? 1 : 0;
+        src = cx::generate_cuda(p, t);
+      } catch (const std::exception& e) {
+        return serr(CX_E_INVALID, "plan: %s", e.what());
+      }
+      char log[4096];
+      const int rc = cx_compile(src.data(), src.size(), nullptr, &m, log, sizeof log);
+      if (rc) return rc;
+      s->plain_mods[key] = m;
+    }
+  }
+  r->plain = m;
+  r->plain_param = param_ok;
+  cx_result_info info;
+  cx_module_result_info(m, &info);
+  uint64_t scratch = 0;
+  cx_module_scratch_bytes(m, nullptr, &scratch);
+  r->words = std::max<uint64_t>(1, info.result_words);
+  r->vwords = std::max<uint64_t>(1, info.validity_words);
+  r->final_words = info.final_words;
   const uint64_t groups = p.group_count();
+  r->est_bytes = (r->words + r->vwords) * 8 + (shared ? ((groups + 31) / 32) * 4 + 64 + r->lits.size() * 4 : 0);
+  if (r->est_bytes + scratch > s->cfg.budget_bytes)
+    return serr(CX_E_REJECTED, "cx_server_submit: the query needs %llu bytes, the budget is %llu",
+                (unsigned long long)(r->est_bytes + scratch), (unsigned long long)s->cfg.budget_bytes);
+  r->shared = shared;
   if (shared) {
-    std::vector<const cx::Expr*> lits;
-    cx::collect_literals(p, lits);
-    for (const cx::Expr* e : lits) r->lits.push_back((int32_t)e->ival);
-    r->words = std::max<uint64_t>(1, groups * (uint64_t)p.storage_ts());
-    r->vwords = (r->words + 63) / 64;
-    r->final_words = groups * (uint64_t)p.storage_ts();
-    r->est_bytes = (r->words + r->vwords) * 8 + ((groups + 31) / 32) * 4 + 64 + r->lits.size() * 4;
-    if (r->est_bytes > s->cfg.budget_bytes)
-      return serr(CX_E_REJECTED, "cx_server_submit: the query needs %llu bytes, the budget is %llu",
-                  (unsigned long long)r->est_bytes, (unsigned long long)s->cfg.budget_bytes);
-    int idx = -1;
     {
       std::lock_guard<std::mutex> lk(s->mu);
       auto it = s->shape_index.find(r->shape);
@@ -218,8 +248,7 @@ int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Req
         if (s->shape_reps.size() >= 16) {
           r->shared = false;  // the program holds at most 16 shapes; the rest run alone
         } else {
-          idx = (int)s->shape_reps.size();
-          s->shape_index[r->shape] = idx;
+          s->shape_index[r->shape] = (int)s->shape_reps.size();
           s->shape_keys.push_back(r->shape);
           s->shape_reps.push_back(cx::parse_plan(r->text));
         }
@@ -230,50 +259,6 @@ int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Req
       const int rc = rebuild_universe(s);
       if (rc) return rc;
     }
-  }
-  if (!r->shared) {
-    cx_module* m = nullptr;
-    {
-      std::lock_guard<std::mutex> ck(s->compile_mu);
-      auto it = s->plain_mods.find(r->text);
-      if (it != s->plain_mods.end()) {
-        m = it->second;
-      } else {
-        std::string src;
-        try {
-          cx::Tuning t;
-          if (plain_tuning) {
-            t.block_threads = plain_tuning->block_threads;
-            t.items_per_thread = plain_tuning->items_per_thread;
-            t.stages = plain_tuning->stages;
-            t.ctas_per_sm = plain_tuning->ctas_per_sm;
-            t.group_placement = plain_tuning->group_placement;
-            t.smem_group_budget = plain_tuning->smem_group_budget;
-            t.bitmap_budget = plain_tuning->bitmap_budget;
-            t.group_merge = plain_tuning->group_merge;
-          }
-          src = cx::generate_cuda(p, t);
-        } catch (const std::exception& e) {
-          return serr(CX_E_INVALID, "plan: %s", e.what());
-        }
-        char log[4096];
-        const int rc = cx_compile(src.data(), src.size(), nullptr, &m, log, sizeof log);
-        if (rc) return rc;
-        s->plain_mods[r->text] = m;
-      }
-    }
-    r->plain = m;
-    cx_result_info info;
-    cx_module_result_info(m, &info);
-    uint64_t scratch = 0;
-    cx_module_scratch_bytes(m, nullptr, &scratch);
-    r->words = std::max<uint64_t>(1, info.result_words);
-    r->vwords = std::max<uint64_t>(1, info.validity_words);
-    r->final_words = info.final_words;
-    r->est_bytes = (r->words + r->vwords) * 8;
-    if (r->est_bytes + scratch > s->cfg.budget_bytes)
-      return serr(CX_E_REJECTED, "cx_server_submit: the query needs %llu bytes, the budget is %llu",
-                  (unsigned long long)(r->est_bytes + scratch), (unsigned long long)s->cfg.budget_bytes);
   }
   *out = std::move(r);
   return CX_OK;
@@ -331,7 +316,9 @@ void launch(cx_server* s, Slot& sl, std::vector<Request*>& batch, bool shared) {
     Request* r = batch[0];
     sl.mod = r->plain;
     rc = cx_ctx_set_result(sl.ctx, (uint64_t*)r->d_res, r->words, (uint64_t*)r->d_val, r->vwords);
-    if (!rc) rc = cx_execute(r->plain, sl.ctx, sl.stream);
+    if (!rc)
+      rc = cx_execute_params(r->plain, sl.ctx, r->plain_param ? r->lits.data() : nullptr,
+                             r->plain_param ? (int)r->lits.size() : 0, sl.stream);
   }
   for (Request* r : batch) {
     if (rc) break;
@@ -416,14 +403,24 @@ void scheduler(cx_server* s) {
         return s->reserved + fixed + growth + add <= s->cfg.budget_bytes || (s->reserved == 0 && batch.empty());
       };
       bool shared = head->shared && s->universe && s->shape_index.at(head->shape) < (int)s->universe_shapes;
-      if (!head->shared) {
+      if (shared) {
+        // A short queue runs its head alone through the plain kernel: one
+        // shared launch costs about as much as a few plain ones.
+        int ready = 0;
+        for (Request* r : s->pending) {
+          if (!r->shared || s->shape_index.at(r->shape) >= (int)s->universe_shapes || ready >= s->cfg.min_shared_batch) break;
+          ++ready;
+        }
+        if (ready < s->cfg.min_shared_batch) shared = false;
+      }
+      if (!shared) {
         uint64_t need = 0;
         cx_module_scratch_bytes(head->plain, sl.ctx, &need);
         if (admit(cx_internal::grown_scratch(own, need) - own, head->est_bytes)) {
           batch.push_back(head);
           s->pending.pop_front();
         }
-      } else if (shared) {
+      } else {
         uint64_t add = 0;
         std::vector<int> shapes;
         while (!s->pending.empty() && (int)batch.size() < s->cfg.max_batch) {
@@ -438,7 +435,7 @@ void scheduler(cx_server* s) {
         }
       }
       if (batch.empty()) break;
-      launch(s, sl, batch, shared && head->shared);
+      launch(s, sl, batch, shared);
       s->reserved += sl.reserved;
       s->peak_reserved = std::max(s->peak_reserved, s->reserved + fixed_bytes(s));
       progressed = true;
@@ -460,6 +457,7 @@ void cx_server_config_default(cx_server_config* cfg) {
   cfg->budget_bytes = 40ULL << 30;
   cfg->max_batch = 64;
   cfg->slots = 1;
+  cfg->min_shared_batch = 5;
   cfg->plain_only = 0;
   cx_tuning_default(&cfg->shared_tuning);
   cfg->shared_tuning.block_threads = 1024;
@@ -473,6 +471,7 @@ int cx_server_create(const cx_exec_ctx* tables, const cx_server_config* cfg, cx_
   auto s = std::make_unique<cx_server>();
   if (cfg) s->cfg = *cfg;
   else cx_server_config_default(&s->cfg);
+  if (s->cfg.min_shared_batch < 1) s->cfg.min_shared_batch = 1;
   if (s->cfg.max_batch < 1 || s->cfg.max_batch > 256 || s->cfg.slots < 1 || s->cfg.slots > 8 || s->cfg.budget_bytes == 0)
     return serr(CX_E_INVALID, "cx_server_create: max_batch 1..256, slots 1..8 and a non-zero budget");
   if (cudaGetDevice(&s->device) != cudaSuccess) return serr(CX_E_NO_DEVICE, "cx_server_create: no CUDA device");

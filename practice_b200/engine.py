@@ -188,8 +188,10 @@ class Database:
 
     # ----------------------------------------------------------- queries
     def compile(self, plan: Plan, tuning: _lib.Tuning | None = None) -> _lib.Module:
+        """The plan's fused kernel.  With `tuning.parametric` set, one module
+        serves every plan of the same shape (literals are passed at execute)."""
         tkey = tuple(getattr(tuning, f) for f, _ in _lib.Tuning._fields_) if tuning is not None else None
-        key = (plan.text(), tkey)
+        key = (shape_key(plan) if tuning is not None and tuning.parametric else plan.text(), tkey)
         m = self._modules.get(key)
         if m is None:
             src = _lib.codegen(plan.text(), tuning)
@@ -368,13 +370,15 @@ class Database:
 
     def execute(self, plan: Plan, tuning: _lib.Tuning | None = None, stream=None) -> QueryResult:
         torch = self.torch
-        m = self.compile(plan, tuning if tuning is not None else self.tuning_for(plan))
+        tuning = tuning if tuning is not None else self.tuning_for(plan)
+        m = self.compile(plan, tuning)
         res, val = self.alloc_result(m)
         for t, n in self.rows.items():
             self.ctx.set_rows(t, n)
         self.ctx.set_result(res.data_ptr(), res.numel(), val.data_ptr(), val.numel())
         s = stream if stream is not None else torch.cuda.current_stream()
-        self.ctx.execute(m, s.cuda_stream)
+        params = _lib.plan_literals(plan.text()) if tuning is not None and tuning.parametric else None
+        self.ctx.execute(m, s.cuda_stream, params)
         err = 0
         try:
             self.ctx.sync()

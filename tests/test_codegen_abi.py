@@ -193,8 +193,24 @@ def test_shared_execute_validates_before_touching_the_gpu():
 def test_server_config_defaults_and_create_without_a_device():
     cfg = _lib.server_config()
     assert cfg.budget_bytes == 40 << 30 and cfg.max_batch == 64 and cfg.slots == 1 and cfg.plain_only == 0
+    assert cfg.min_shared_batch == 5
     assert cfg.shared_tuning.block_threads == 1024
     bad = _lib.server_config(slots=0)
     with pytest.raises(_lib.CxError) as e:
         _lib.Server(_lib.ExecCtx(), bad)
     assert e.value.code in (-1, -7)
+
+
+def test_parametric_plain_codegen_takes_literals_at_launch():
+    rng = random.Random(21)
+    t = _lib.default_tuning()
+    t.parametric = 1
+    a, b = queries.template(2, rng), queries.template(2, rng)
+    sa, sb = _lib.codegen(a.text(), t), _lib.codegen(b.text(), t)
+    assert sa == sb, "plans of one shape generate one parametric source"
+    assert "params 4" in sa and "a.lits" in sa
+    m = _lib.Module(sa, key="cpu_param_probe")
+    ctx = _lib.ExecCtx()
+    with pytest.raises(_lib.CxError) as e:
+        ctx.execute(m, 0, [1, 2])  # wrong literal count fails before touching a GPU
+    assert e.value.code == -1

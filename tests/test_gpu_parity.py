@@ -326,3 +326,38 @@ def test_shared_scan_graph_replay(db):
             np.testing.assert_array_equal(g.words, ref.words)
     finally:
         db.ctx.set_graph_replay(True)
+
+
+def test_parametric_plain_kernel_serves_every_literal(db):
+    """One parametric module per plan shape, the literals passed at launch,
+    returns what a kernel compiled for each query's literals returns."""
+    n = 250_013
+    ht = load(db, 47, n, queries.BATCH_COLS)
+    rng = random.Random(81)
+    t = _lib.default_tuning()
+    t.parametric = 1
+    for tpl in range(4):
+        plans = [queries.template(tpl, rng, n) for _ in range(3)]
+        mods = set()
+        for p in plans:
+            got = db.execute(p, t)
+            mods.add(db.compile(p, t).handle.value)
+            assert got.kernel_error == 0
+            ref = oracle_run(p, ht)
+            np.testing.assert_array_equal(got.words, ref.words[: len(got.words)])
+            np.testing.assert_array_equal(got.validity, ref.validity[: (len(got.words) + 63) // 64])
+        assert len(mods) == 1
+
+
+def test_parametric_plain_kernel_nullable_shape(db):
+    n = 300_019
+    ht = load(db, 48, n, queries.Q31_COLS, nulls={"lo_revenue": 100, "c_city": 50})
+    t = _lib.default_tuning()
+    t.parametric = 1
+    for region, years, floor in ((1, (1993, 1998), 2_000_000), (3, (1992, 1995), 500_000)):
+        plan = queries.ssb_q31_nullable(n, region=region, years=years, rev_floor=floor)
+        got = db.execute(plan, t)
+        ref = oracle_run(plan, ht)
+        fw = len(got.words)
+        np.testing.assert_array_equal(got.words, ref.words[:fw])
+        np.testing.assert_array_equal(got.validity, ref.validity[: (fw + 63) // 64])

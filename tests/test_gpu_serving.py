@@ -142,3 +142,22 @@ def test_server_plain_only_runs_one_query_per_launch(db):
         assert srv.stats().launches == len(plans)
     finally:
         srv.close()
+
+
+def test_server_short_queues_run_plain_kernels(db):
+    """Shareable queries that find fewer than min_shared_batch others waiting
+    run alone through their parametric plain kernel; one module per shape
+    serves queries with different literals."""
+    n = 200_029
+    ht = load(db, 54, n)
+    rng = random.Random(11)
+    plans = [queries.template(t, rng, n) for t in (1, 2, 1, 3, 0, 2)]
+    srv = _lib.Server(db.ctx, _lib.server_config(min_shared_batch=1_000_000))
+    try:
+        infos = []
+        for p in plans:
+            rid = srv.submit(p.text())
+            infos.append(check(srv, db, rid, p, ht, alone=False))
+        assert all(i.batch_size == 1 and i.shared == 0 for i in infos)
+    finally:
+        srv.close()

@@ -261,7 +261,7 @@ typedef struct cx_request_info {
   double queue_ms;        /* submit -> launch */
   double latency_ms;      /* submit -> result in host memory */
   int batch_size;         /* queries answered by the same launch (1 = alone) */
-  int shared;             /* 1 = shared scan, 0 = plain kernel */
+  int shared;             /* 1 = answered by a shared scan, 0 = by its plain kernel */
 } cx_request_info;
 
 typedef struct cx_server_stats {

@@ -77,6 +77,7 @@ struct Request {
   uint32_t kernel_err = 0;
   double t_submit = 0, t_launch = 0, t_done = 0;
   int batch_size = 0;
+  bool ran_shared = false;  // answered by a shared scan (else by its plain kernel)
   void* d_res = nullptr;
   void* d_val = nullptr;
   size_t host_off = 0;  // offset of its result in the slot's pinned landing area
@@ -276,6 +277,7 @@ void launch(cx_server* s, Slot& sl, std::vector<Request*>& batch, bool shared) {
     r->status = 0;
     r->t_launch = t;
     r->batch_size = (int)batch.size();
+    r->ran_shared = shared;
     sl.reserved += r->est_bytes;
   }
   int rc = CX_OK;
@@ -555,7 +557,7 @@ int cx_server_wait(cx_server* s, uint64_t id, int timeout_ms, cx_request_info* i
     info->queue_ms = r->t_launch - r->t_submit;
     info->latency_ms = r->t_done - r->t_submit;
     info->batch_size = r->batch_size;
-    info->shared = r->shared ? 1 : 0;
+    info->shared = r->ran_shared ? 1 : 0;
   }
   return r->rc;
 }

@@ -248,8 +248,8 @@ def serving_leg(db, plans, args, shared_tuning):
         cfg.shared_tuning = shared_tuning
     srv = _lib.Server(db.ctx, cfg)
     try:
-        for t in texts:
-            srv.prepare(t)
+        for p in plans:  # short queues run these autotuned plain kernels
+            srv.prepare(p.text(), db.tuning_for(p))
         shared_stream = stream(srv, args.serve_rate, args.serve_requests)
         shared_low = stream(srv, args.serve_low_rate, n_low)
     finally:

@@ -127,6 +127,7 @@ struct cx_server {
   size_t universe_shapes = 0;
   std::mutex compile_mu;
   std::map<std::string, cx_module*> plain_mods;
+  std::map<std::string, cx_tuning> shape_tunings;  // plain launch shape given at prepare, per plan shape
   std::thread th;
   bool stop = false;
   // Statistics since the last reset.
@@ -203,10 +204,21 @@ int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Req
     }
   }
   // Its plain kernel: one parametric module per plan shape and tuning, so a
-  // new literal never waits for NVRTC.
+  // new literal never waits for NVRTC.  A shape prepared with a tuning keeps
+  // it for later submissions.
   cx_module* m = nullptr;
+  cx_tuning remembered;
   {
     std::lock_guard<std::mutex> ck(s->compile_mu);
+    if (plain_tuning) {
+      s->shape_tunings[r->shape] = *plain_tuning;
+    } else {
+      auto st = s->shape_tunings.find(r->shape);
+      if (st != s->shape_tunings.end()) {
+        remembered = st->second;
+        plain_tuning = &remembered;
+      }
+    }
     const std::string key = (param_ok ? r->shape : r->text) + "|" + tuning_key(plain_tuning);
     auto it = s->plain_mods.find(key);
     if (it != s->plain_mods.end()) {

@@ -226,6 +226,40 @@ int cx_gen_validity(uint64_t gen_stream, uint64_t seed, uint64_t rows, uint32_t 
                     void* stream);
 
 /* ------------------------------------------------------------------------
+ * Result finalisation on the device.  Replaces the reference's generated
+ * post-processing: AggregateDenseCount / AggregateDenseWrite
+ * (src/core/visitor.cpp:2589-2697) -- present groups become columnar rows in
+ * group order -- and the SortLimit kernels (src/core/visitor.cpp:307-581) --
+ * rows ordered by the keys (each compared in its column's result type, a
+ * valid value before NULL, ties by row index), then cut to LIMIT.  The row
+ * offsets come from a device prefix sum instead of a host loop.
+ * ---------------------------------------------------------------------- */
+enum { CX_COL_INT64 = 0, CX_COL_UINT64 = 1, CX_COL_FLOAT64 = 2 };
+
+typedef struct cx_result_layout {
+  uint64_t groups;                 /* group tuples in the aggregate buffer */
+  uint32_t tuple_size;             /* u64 words per tuple (visible columns first) */
+  uint32_t columns;                /* visible columns, 1..32 */
+  int sparse;                      /* fast sparse output: all-zero tuples dropped, every value valid */
+  int scalar;                      /* no GROUP BY: exactly one row */
+  const uint8_t* column_type;      /* per column CX_COL_*; NULL = all UINT64 */
+  const uint8_t* column_nullable;  /* per column 1 = carries validity; NULL = none */
+} cx_result_layout;
+
+typedef struct cx_sort_key {
+  int column;
+  int descending;
+} cx_sort_key;
+
+/* Writes the result rows column by column: column c at dev_columns + c *
+ * row_cap, its validity bits at dev_col_validity + c * ((row_cap + 63) / 64).
+ * row_cap must cover the group count.  `limit` = UINT64_MAX for none.  Returns
+ * the number of rows in *rows (synchronises `stream`). */
+int cx_finalize(const uint64_t* dev_result, const uint64_t* dev_validity, const cx_result_layout* layout,
+                const cx_sort_key* keys, int nkeys, uint64_t limit, uint64_t* dev_columns,
+                uint64_t* dev_col_validity, uint64_t row_cap, uint64_t* rows, void* stream);
+
+/* ------------------------------------------------------------------------
  * Request loop (serving).  No reference counterpart: the reference runs one
  * query per db_cli command on one in-order queue (src/db/database_instance.cpp:23);
  * the admission estimate generalises its device-memory preflight

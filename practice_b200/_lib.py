@@ -27,7 +27,7 @@ EXPORTS = [
     "cx_shared_execute", "cx_ctx_set_column_range", "cx_ctx_set_graph_replay",
     "cx_server_config_default", "cx_server_create", "cx_server_prepare", "cx_server_prepare_tuned",
     "cx_server_submit", "cx_server_wait",
-    "cx_server_fetch", "cx_server_release", "cx_server_get_stats", "cx_server_destroy",
+    "cx_server_fetch", "cx_server_release", "cx_server_get_stats", "cx_server_destroy", "cx_finalize",
 ]
 
 
@@ -53,6 +53,15 @@ class ResultInfo(C.Structure):
 class SharedQuery(C.Structure):
     _fields_ = [("shape", C.c_int), ("param_off", C.c_int), ("result", C.c_void_p), ("result_words", C.c_uint64),
                 ("validity", C.c_void_p), ("validity_words", C.c_uint64)]
+
+
+class ResultLayout(C.Structure):
+    _fields_ = [("groups", C.c_uint64), ("tuple_size", C.c_uint32), ("columns", C.c_uint32), ("sparse", C.c_int),
+                ("scalar", C.c_int), ("column_type", C.POINTER(C.c_uint8)), ("column_nullable", C.POINTER(C.c_uint8))]
+
+
+class SortKey(C.Structure):
+    _fields_ = [("column", C.c_int), ("descending", C.c_int)]
 
 
 class ServerConfig(C.Structure):
@@ -112,6 +121,8 @@ def _load() -> C.CDLL:
         "cx_server_release": (C.c_int, [vp, u64]),
         "cx_server_get_stats": (C.c_int, [vp, C.c_int, C.POINTER(ServerStats)]),
         "cx_server_destroy": (C.c_int, [vp]),
+        "cx_finalize": (C.c_int, [vp, vp, C.POINTER(ResultLayout), C.POINTER(SortKey), C.c_int, u64, vp, vp, u64,
+                                  C.POINTER(u64), vp]),
         "cx_execute": (C.c_int, [vp, vp, vp]),
         "cx_execute_params": (C.c_int, [vp, vp, C.POINTER(C.c_int32), C.c_int, vp]),
         "cx_ctx_sync": (C.c_int, [vp]),
@@ -347,3 +358,22 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+COL_INT64, COL_UINT64, COL_FLOAT64 = 0, 1, 2
+
+
+def finalize(result_ptr: int, validity_ptr: int, groups: int, tuple_size: int, types: list[int],
+             nullable: list[bool], sparse: bool, scalar: bool, keys: list[tuple[int, bool]], limit: int | None,
+             cols_ptr: int, cvalid_ptr: int, row_cap: int, stream: int = 0) -> int:
+    """cx_finalize: result rows written column by column on the device; returns the row count."""
+    n = len(types)
+    ta = (C.c_uint8 * n)(*types)
+    na = (C.c_uint8 * n)(*[int(x) for x in nullable])
+    lay = ResultLayout(groups, tuple_size, n, int(sparse), int(scalar), ta, na)
+    ka = (SortKey * max(len(keys), 1))(*[SortKey(c, int(d)) for c, d in keys])
+    rows = C.c_uint64()
+    lim = (1 << 64) - 1 if limit is None else limit
+    check(lib.cx_finalize(result_ptr, validity_ptr or None, C.byref(lay), ka, len(keys), lim, cols_ptr, cvalid_ptr,
+                          row_cap, C.byref(rows), stream or None), "cx_finalize")
+    return rows.value

@@ -21,7 +21,7 @@ NVCC = CUDA_HOME / "bin" / "nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SOURCES = ["cx_plan.cpp", "cx_codegen.cpp", "cx_runtime.cpp", "cx_server.cpp"]
-CUDA_SOURCES = ["cx_kernels.cu"]
+CUDA_SOURCES = ["cx_kernels.cu", "cx_finalize.cu"]
 EMBEDDED = ["crystal_sm100.cuh", "cx_args.h"]
 
 

@@ -362,6 +362,26 @@ class Database:
         best = self.tuned.get("shared|" + "|".join(sorted({shape_key(p) for p in plans})))
         return make_tuning(**best["tuning"]) if best else None
 
+    def finalize_rows(self, plan: Plan, res, val, limit: int | None = None) -> list[tuple]:
+        """The plan's result rows, finalised and ordered on the device
+        (cx_finalize) from its aggregate buffer (`res`, `val`: device tensors
+        left by execute), then copied to the host."""
+        from . import results
+
+        torch = self.torch
+        finalized = any(a.fn == "avg" for a in plan.aggs)
+        ts = plan.visible_ts if finalized else plan.storage_ts
+        groups = plan.group_slots
+        ncols = plan.visible_ts
+        cap = max(groups, 1)
+        cols = torch.empty(ncols * cap, dtype=torch.int64, device=self.device)
+        cval = torch.empty(ncols * ((cap + 63) // 64), dtype=torch.int64, device=self.device)
+        nullable = results.output_nullable(plan) if not plan.sparse else [False] * ncols
+        n = _lib.finalize(res.data_ptr(), val.data_ptr(), groups, ts, results.column_types(plan), nullable,
+                          plan.sparse, not plan.groups, list(plan.order_by), limit, cols.data_ptr(), cval.data_ptr(),
+                          cap, torch.cuda.current_stream().cuda_stream)
+        return results.device_rows(plan, cols.cpu().numpy().view(np.uint64), cval.cpu().numpy().view(np.uint64), n, cap)
+
     def alloc_result(self, module: _lib.Module):
         torch = self.torch
         res = torch.empty(max(int(module.info.result_words), 1), dtype=torch.int64, device=self.device)

@@ -85,3 +85,43 @@ def order(plan: Plan, rs: list[tuple]) -> list[tuple]:
         return tuple(keys) + tuple(_key(v) for v in r)
 
     return sorted(rs, key=k)
+
+
+# ------------------------------------------------------------ device rows
+
+def _expr_type(e) -> int:
+    """Result type of a GROUP BY expression (src/core/visitor.cpp:77-107):
+    comparisons, logic and IS [NOT] NULL are UInt64, CASE takes its branches'
+    widest type, everything else (columns, arithmetic, literals) is Int64."""
+    if e.op in ("eq", "ne", "lt", "le", "gt", "ge", "and", "or", "not", "isnull", "notnull", "null"):
+        return 1
+    if e.op == "case":
+        t = {_expr_type(e.kids[1]), _expr_type(e.kids[2])}
+        return 2 if 2 in t else 0 if 0 in t else 1
+    return 0
+
+
+def column_types(plan: Plan) -> list[int]:
+    """Result column types (src/core/visitor.cpp:109-123): GROUP BY keys by
+    their expression, AVG Float64, every other aggregate UInt64."""
+    out = [_expr_type(g.expr) for g in plan.groups]
+    out += [2 if a.fn == "avg" else 1 for a in plan.aggs]
+    return out
+
+
+def device_rows(plan: Plan, cols: np.ndarray, cvalid: np.ndarray, nrows: int, row_cap: int) -> list[tuple]:
+    """Typed rows from cx_finalize's columnar output, in its order."""
+    types = column_types(plan)
+    vw = (row_cap + 63) // 64
+    out = []
+    for r in range(nrows):
+        row = []
+        for c, t in enumerate(types):
+            if not ((int(cvalid[c * vw + (r >> 6)]) >> (r & 63)) & 1):
+                row.append(None)
+            elif t == 2:
+                row.append(float(cols[c * row_cap + r : c * row_cap + r + 1].view(np.float64)[0]))
+            else:
+                row.append(int(cols[c * row_cap + r : c * row_cap + r + 1].view(np.int64)[0]))
+        out.append(tuple(row))
+    return out

@@ -131,10 +131,22 @@ def test_templates_with_order_and_limit(db, t):
     p = queries.template(t, rng, n)
     if p.groups:
         p.order_by = [(len(p.groups), True), (0, False)]  # by the aggregate, then the first key
-    got = check(db, p)
-    if t == 3:
-        assert len(got) > 2048, "large results go through the global bitonic network"
+    check(db, p)
     check(db, p, limit=5)
+
+
+def test_large_result_uses_the_global_network(db):
+    """More than 2048 rows: the bitonic network runs in global memory."""
+    n = 2_000_029
+    load(db, 65, n, queries.BATCH_COLS)
+    b = PlanBuilder(datagen.ssb_tables(n, queries.BATCH_COLS), "LINEORDER", name="big")
+    b.join("DDATE", "lo_orderdate")
+    p = b.aggregate([Group(col("lo_quantity"), 1, 50, False), Group(col("lo_discount"), 0, 11, False),
+                     queries._g("d_year")], [("sum", col("lo_revenue")), ("count", star())],
+                    order_by=[(4, False), (3, True)])
+    got = check(db, p)
+    assert len(got) > 2048
+    check(db, p, limit=100)
 
 
 def test_kat_and_scalar_results(db):

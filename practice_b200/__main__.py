@@ -28,7 +28,7 @@ def _tuning(pairs: list[str]):
 
 def main(argv: list[str] | None = None) -> None:
     ap = argparse.ArgumentParser(prog="python -m practice_b200")
-    ap.add_argument("mode", choices=["shared", "plain"])
+    ap.add_argument("mode", choices=["shared", "plain", "tour"])
     ap.add_argument("--rows", type=int, default=30_000_000)
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--query", default="T1", help="T0..T3, q11 or q31 (plain mode)")
@@ -41,6 +41,9 @@ def main(argv: list[str] | None = None) -> None:
     from practice_b200 import queries
     from practice_b200.engine import Database
 
+    if args.mode == "tour":
+        tour(args)
+        return
     kw, shared_default, make_tuning = _tuning(args.tuning)
     cols = {"q11": queries.Q11_COLS, "q31": queries.Q31_COLS}.get(args.query, queries.BATCH_COLS)
     db = Database(0)
@@ -69,6 +72,53 @@ def main(argv: list[str] | None = None) -> None:
         r = db.execute(plan, t)
         print(f"{plan.name}: scan {r.timing.scan_ms:.4f} ms, total {r.timing.total_ms:.4f} ms, "
               f"kernel error {r.kernel_error}", flush=True)
+
+
+def tour(args) -> None:
+    """Runs every kernel of the library once or twice on a generated table:
+    the plain fused scan (Q1.1-, Q3.1- and nullable Q3.1-shaped queries, a
+    parametric one, AVG finalisation), a shared-scan batch, result
+    finalisation on the device and sparse compaction (both entry points)."""
+    import numpy as np
+
+    from practice_b200 import _lib, queries
+    from practice_b200.engine import SHARED_DEFAULT, Database, make_tuning
+    from practice_b200.plan import PlanBuilder, col
+
+    cols = sorted(set(queries.BATCH_COLS) | set(queries.Q11_COLS))
+    db = Database(0)
+    db.generate_ssb(args.rows, args.seed, cols, nulls={"c_city": 50})
+    torch = db.torch
+    rng = random.Random(args.seed)
+    plans = [queries.ssb_q11(args.rows), queries.ssb_q31(args.rows), queries.ssb_q31_nullable(args.rows)]
+    b = PlanBuilder(queries.ssb_tables(args.rows, cols), "LINEORDER", name="avg")
+    b.join("DDATE", "lo_orderdate")
+    plans.append(b.aggregate([queries._g("d_year")], [("avg", col("lo_supplycost")), ("min", col("lo_quantity"))]))
+    for p in plans:
+        m = db.compile(p)
+        res, val = db.alloc_result(m)
+        db.ctx.set_result(res.data_ptr(), res.numel(), val.data_ptr(), val.numel())
+        db.ctx.execute(m, torch.cuda.current_stream().cuda_stream)
+        db.ctx.sync()
+        rows = db.finalize_rows(p, res, val, limit=20)
+        print(f"{p.name}: scan {db.ctx.timing().scan_ms:.3f} ms, {len(rows)} rows after device finalisation")
+    t = make_tuning(parametric=1)
+    p = queries.template(2, rng, args.rows)
+    r = db.execute(p, t)
+    print(f"parametric {p.name}: scan {r.timing.scan_ms:.3f} ms")
+    batch = [queries.template(rng.randrange(4), rng, args.rows) for _ in range(args.batch)]
+    r = db.execute_shared(batch, make_tuning(**SHARED_DEFAULT))
+    print(f"shared batch of {len(batch)}: scan {r[0].timing.scan_ms:.3f} ms")
+    words = torch.from_numpy(r[1].words.view(np.int64).copy()).to(db.device)
+    groups = batch[1].group_slots
+    ts = batch[1].storage_ts
+    dst = torch.empty_like(words)
+    cnt = torch.zeros(1, dtype=torch.int64, device=db.device)
+    for fn in (_lib.lib.cx_compact_sparse, _lib.lib.cx_compact_sparse_noalloc):
+        _lib.check(fn(words.data_ptr(), groups, ts, dst.data_ptr(), cnt.data_ptr(),
+                      torch.cuda.current_stream().cuda_stream), "compaction")
+    torch.cuda.synchronize()
+    print(f"sparse compaction: {int(cnt.item())} groups")
 
 
 if __name__ == "__main__":

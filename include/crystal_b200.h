@@ -125,7 +125,9 @@ int cx_ctx_set_result(cx_exec_ctx* c, uint64_t* dev_result, uint64_t result_word
  * the context allocates grow-only scratch itself (the reference's
  * getScratchIntBuffer high-water reuse, execution.h:186-207). */
 int cx_ctx_set_scratch(cx_exec_ctx* c, void* dev_ptr, uint64_t bytes);
-/* Bytes of scratch `m` needs under the context's current table sizes. */
+/* Bytes of scratch `m` needs under the context's current table sizes.  A
+ * multi-value hash join adds 4 bytes per build row, counted only when `c` is
+ * given (NULL: the size-independent part). */
 int cx_module_scratch_bytes(const cx_module* m, const cx_exec_ctx* c, uint64_t* bytes);
 /* Overrides the multiprocessor count used to size persistent grids (0 = device's). */
 int cx_ctx_set_sm_count(cx_exec_ctx* c, int sms);

@@ -141,11 +141,18 @@ typedef struct {
 
 typedef struct {
   int dim_table;
-  int pk, fk, payload; /* column ids, payload -1 for PHT_1 */
+  int pk, payload;      /* column ids, payload -1 for PHT_1 */
+  int fks[4], nfk;      /* probe keys; more than one is an OR-join */
+  int multi;            /* multi-value hash table (non-unique build key) */
+  int gathers[8], ngather; /* MHT: build columns read through the row id */
   long long len, keymin;
   Expr* filter;
   int32_t* ht;          /* 2*len ints */
   unsigned char* hv;    /* payload validity per slot (nullable payloads) */
+  int32_t* mkey;        /* MHT directory: key, count and first position per slot */
+  int32_t* mcnt;
+  long long* moff;
+  int32_t* mrows;       /* MHT payload: build row ids grouped by slot */
 } JoinS;
 
 typedef struct {
@@ -466,14 +473,30 @@ static int parse(Oracle* o, const char* text) {
       for (int t = 0; t < o->ntables; ++t)
         if (!strcmp(o->tables[t], n->items[1]->text)) j->dim_table = t;
       j->pk = col_index(o, field(n, "pk")->items[1]->text);
-      j->fk = col_index(o, field(n, "fk")->items[1]->text);
+      const Node* fkn = field(n, "fk");
+      int bad = fkn->n < 2 || fkn->n > 5;
+      for (int k = 1; k < fkn->n && k <= 4; ++k) {
+        j->fks[j->nfk] = col_index(o, fkn->items[k]->text);
+        bad |= j->fks[j->nfk++] < 0;
+      }
       j->len = strtoll(field(n, "len")->items[1]->text, NULL, 10);
       j->keymin = strtoll(field(n, "keymin")->items[1]->text, NULL, 10);
+      const Node* mu = field(n, "multi");
+      j->multi = mu ? atoi(mu->items[1]->text) != 0 : 0;
       const Node* f = field(n, "filter");
       j->filter = f ? to_expr(o, f->items[1]) : NULL;
       const Node* p = field(n, "payload");
-      j->payload = p ? col_index(o, p->items[1]->text) : -1;
-      if (j->dim_table < 0 || j->pk < 0 || j->fk < 0 || (f && !j->filter) || (p && j->payload < 0)) {
+      j->payload = -1;
+      if (p && j->multi) {
+        for (int k = 1; k < p->n && k <= 8; ++k) {
+          j->gathers[j->ngather] = col_index(o, p->items[k]->text);
+          bad |= j->gathers[j->ngather++] < 0;
+        }
+      } else if (p) {
+        j->payload = col_index(o, p->items[1]->text);
+        bad |= j->payload < 0;
+      }
+      if (j->dim_table < 0 || j->pk < 0 || bad || (f && !j->filter)) {
         snprintf(o->err, sizeof o->err, "bad join");
         rc = -1;
       }
@@ -506,6 +529,148 @@ static int parse(Oracle* o, const char* text) {
 
 static void set_bit(uint64_t* bm, uint64_t bit) { bm[bit >> 6] |= 1ULL << (bit & 63); }
 static int get_bit(const uint64_t* bm, uint64_t bit) { return (int)((bm[bit >> 6] >> (bit & 63)) & 1ULL); }
+
+/* Aggregation state of the scan. */
+typedef struct {
+  Oracle* o;
+  uint64_t* result;
+  uint64_t* validity;
+  uint64_t G;
+  int ts, vts;
+  uint64_t acc[32], seen[32], cnt[32];
+  unsigned char* touched;
+  long long derr;
+} ScanState;
+
+/* One qualifying (expanded) row into the aggregate: scalar :3017-3124,
+ * grouped :3125-3195. */
+static void consume(ScanState* st, RowCtx* rcx) {
+  Oracle* o = st->o;
+  if (o->ngroups == 0) {
+    for (int a = 0; a < o->naggs; ++a) {
+      const AggS* ag = &o->aggs[a];
+      const int v = ag->arg->op == E_STAR ? 1 : valid_of(rcx, ag->arg);
+      if (!v) continue;
+      const uint64_t x = ag->fn == 0 ? 1 : convert(math_push(rcx, ag->arg, 1), T_U64).bits;
+      switch (ag->fn) {
+        case 0: st->acc[a] += 1; break;
+        case 1: st->acc[a] += x; st->seen[a]++; break;
+        case 4: st->acc[a] += x; st->cnt[a]++; break;
+        case 2: if (x < st->acc[a]) st->acc[a] = x; st->seen[a]++; break;
+        case 3: if (x > st->acc[a]) st->acc[a] = x; st->seen[a]++; break;
+      }
+    }
+    return;
+  }
+  /* Grouped: perfect hash. */
+  long long hsh = 0;
+  int dom_ok = 1;
+  for (int g = 0; g < o->ngroups; ++g) {
+    const GroupS* gs = &o->groups[g];
+    const long long card = gs->card + (gs->nullable ? 1 : 0);
+    long long term;
+    const int64_t v = as_i64(value_of(rcx, gs->e));
+    if (gs->nullable) term = valid_of(rcx, gs->e) ? v - gs->min + 1 : 0;
+    else term = v - gs->min;
+    if (term < 0 || term >= card) dom_ok = 0;
+    hsh = g == 0 ? term : hsh * card + term;
+  }
+  hsh = hsh % (long long)st->G;
+  if (!dom_ok) st->derr++;
+  if (hsh < 0 || (uint64_t)hsh >= st->G) return;
+  const uint64_t base = (uint64_t)hsh * st->ts;
+  uint64_t* result = st->result;
+  st->touched[hsh] = 1;
+  int avg_i = 0;
+  for (int a = 0; a < o->naggs; ++a) {
+    const AggS* ag = &o->aggs[a];
+    const int slot = o->ngroups + a;
+    const int v = ag->arg->op == E_STAR ? 1 : valid_of(rcx, ag->arg);
+    if (ag->fn == 0) {
+      if (v) result[base + slot] += 1;
+      if (!o->sparse) set_bit(st->validity, base + slot);
+      continue;
+    }
+    if (ag->fn == 4) {
+      if (v) {
+        result[base + slot] += convert(math_push(rcx, ag->arg, 1), T_U64).bits;
+        result[base + st->vts + avg_i] += 1;
+      }
+      avg_i++;
+      continue;
+    }
+    if (!v) continue;
+    const uint64_t x = convert(math_push(rcx, ag->arg, 1), T_U64).bits;
+    if (ag->fn == 1) result[base + slot] += x;
+    else if (ag->fn == 2) { if (x < result[base + slot]) result[base + slot] = x; }
+    else { if (x > result[base + slot]) result[base + slot] = x; }
+    if (!o->sparse) set_bit(st->validity, base + slot);
+  }
+}
+
+/* PHT probe of one key; publishes the payload on a hit (join.h:43-120). */
+static int probe_pht(Oracle* o, JoinS* j, int fk) {
+  const long long h = ((long long)fk - j->keymin) % j->len;
+  if (h < 0 || h >= j->len) return 0;
+  if (j->payload < 0) return j->ht[h] == fk;
+  if (j->ht[2 * h] != fk) return 0;
+  o->payload_val[j->payload] = j->ht[2 * h + 1];
+  o->payload_valid[j->payload] = o->cols[j->payload].nullable ? j->hv[h] : 1;
+  return 1;
+}
+
+/* Runs pipeline steps s.. for the current fact row.  An expanding join (an
+ * OR over several fact keys, visitor.cpp:4587-4640, or an MHT probe,
+ * :4672-4730) runs the rest of the pipeline once per distinct non-NULL key
+ * (a key equal to an earlier valid key of the row is skipped) and, for an
+ * MHT, once per matching build row. */
+static void walk(ScanState* st, RowCtx* rcx, int s) {
+  Oracle* o = st->o;
+  for (; s < o->nsteps; ++s) {
+    StepS* sp = &o->steps[s];
+    if (sp->kind == 0) {
+      if (!passes(rcx, sp->filter)) return;
+      continue;
+    }
+    JoinS* j = &sp->join;
+    if (j->nfk == 1 && !j->multi) {
+      int fv;
+      const int fk = col_value(rcx, j->fks[0], &fv);
+      if (!fv || !probe_pht(o, j, fk)) return;
+      continue;
+    }
+    for (int f = 0; f < j->nfk; ++f) {
+      int fv;
+      const int fk = col_value(rcx, j->fks[f], &fv);
+      if (!fv) continue;
+      int dup = 0;
+      for (int q = 0; q < f; ++q) {
+        int pv;
+        const int pk = col_value(rcx, j->fks[q], &pv);
+        if (pv && pk == fk) dup = 1;
+      }
+      if (dup) continue;
+      if (!j->multi) {
+        if (probe_pht(o, j, fk)) walk(st, rcx, s + 1);
+        continue;
+      }
+      const long long h = ((long long)fk - j->keymin) % j->len;
+      if (h < 0 || h >= j->len || j->mcnt[h] == 0 || j->mkey[h] != fk) continue;
+      for (long long k = 0; k < j->mcnt[h]; ++k) {
+        const long long rid = j->mrows[j->moff[h] + k];
+        for (int g = 0; g < j->ngather; ++g) {
+          const Col* c = &o->cols[j->gathers[g]];
+          o->payload_val[j->gathers[g]] = c->data[rid];
+          o->payload_valid[j->gathers[g]] =
+              (c->nullable && c->valid) ? (int)((c->valid[rid >> 6] >> (rid & 63)) & 1ULL) : 1;
+        }
+        walk(st, rcx, s + 1);
+      }
+    }
+    return;
+  }
+  consume(st, rcx);
+}
 
 /* Evaluates a plan over host columns.  Returns 0, or -1 with `err` filled.
  * `domain_errors` receives the number of rows whose GROUP BY key fell outside
@@ -555,10 +720,48 @@ int oracle_run(const char* plan, int ncol, const char* const* names, const int32
     JoinS* j = &o->steps[s].join;
     for (int i = 0; i < o->ncols; ++i)
       if (!o->cols[i].data && o->cols[i].table == j->dim_table) { snprintf(o->err, sizeof o->err, "column %s has no data", o->cols[i].name); rc = -1; goto done; }
-    j->ht = (int32_t*)calloc((size_t)(2 * j->len), sizeof(int32_t));
-    j->hv = (unsigned char*)calloc((size_t)j->len, 1);
     const long long n = o->rows[j->dim_table];
     RowCtx rcx = {o, 0};
+    if (j->multi) {
+      /* MHT build (visitor.cpp:4295-4464): count per slot, exclusive prefix
+       * sum, then row ids grouped by slot (ascending here; the device order
+       * within a slot is unspecified and aggregation does not depend on it).
+       * Two distinct keys in one slot are an error (the reference merges them
+       * into one directory entry under whichever key was written last). */
+      j->mkey = (int32_t*)calloc((size_t)j->len, sizeof(int32_t));
+      j->mcnt = (int32_t*)calloc((size_t)j->len, sizeof(int32_t));
+      j->moff = (long long*)calloc((size_t)j->len + 1, sizeof(long long));
+      for (long long r = 0; r < n; ++r) {
+        rcx.row = r;
+        if (j->filter && !passes(&rcx, j->filter)) continue;
+        int kv;
+        const int key = col_value(&rcx, j->pk, &kv);
+        if (!kv) continue;
+        const long long h = ((long long)key - j->keymin) % j->len;
+        if (h < 0 || h >= j->len) continue;
+        if (j->mcnt[h] && j->mkey[h] != key) { snprintf(o->err, sizeof o->err, "MHT slot collision in %s", o->tables[j->dim_table]); rc = -1; goto done; }
+        j->mkey[h] = key;
+        j->mcnt[h]++;
+      }
+      for (long long h = 0; h < j->len; ++h) j->moff[h + 1] = j->moff[h] + j->mcnt[h];
+      j->mrows = (int32_t*)calloc((size_t)j->moff[j->len] + 1, sizeof(int32_t));
+      long long* pos = (long long*)calloc((size_t)j->len, sizeof(long long));
+      for (long long r = 0; r < n; ++r) {
+        rcx.row = r;
+        if (j->filter && !passes(&rcx, j->filter)) continue;
+        int kv;
+        const int key = col_value(&rcx, j->pk, &kv);
+        if (!kv) continue;
+        const long long h = ((long long)key - j->keymin) % j->len;
+        if (h < 0 || h >= j->len) continue;
+        j->mrows[j->moff[h] + pos[h]++] = (int32_t)r;
+      }
+      free(pos);
+      for (int g = 0; g < j->ngather; ++g) o->cols[j->gathers[g]].is_payload = 1;
+      continue;
+    }
+    j->ht = (int32_t*)calloc((size_t)(2 * j->len), sizeof(int32_t));
+    j->hv = (unsigned char*)calloc((size_t)j->len, 1);
     for (long long r = 0; r < n; ++r) {
       rcx.row = r;
       if (j->filter && !passes(&rcx, j->filter)) continue;
@@ -584,94 +787,26 @@ int oracle_run(const char* plan, int ncol, const char* const* names, const int32
   /* Scan. */
   {
     const long long N = o->rows[0];
-    uint64_t acc[32], seen[32], cnt[32];
-    for (int a = 0; a < o->naggs; ++a) { acc[a] = o->aggs[a].fn == 2 ? ~0ULL : 0; seen[a] = cnt[a] = 0; }
-    unsigned char* touched = o->ngroups ? (unsigned char*)calloc(G, 1) : NULL;
-    long long derr = 0;
+    ScanState st;
+    memset(&st, 0, sizeof st);
+    st.o = o;
+    st.result = result;
+    st.validity = validity;
+    st.G = G;
+    st.ts = ts;
+    st.vts = vts;
+    for (int a = 0; a < o->naggs; ++a) st.acc[a] = o->aggs[a].fn == 2 ? ~0ULL : 0;
+    st.touched = o->ngroups ? (unsigned char*)calloc(G, 1) : NULL;
     RowCtx rcx = {o, 0};
     for (long long r = 0; r < N; ++r) {
       rcx.row = r;
-      int pass = 1;
-      for (int s = 0; s < o->nsteps && pass; ++s) {
-        StepS* st = &o->steps[s];
-        if (st->kind == 0) { pass = passes(&rcx, st->filter); continue; }
-        JoinS* j = &st->join;
-        int fv;
-        const int fk = col_value(&rcx, j->fk, &fv);
-        if (!fv) { pass = 0; continue; }
-        const long long h = ((long long)fk - j->keymin) % j->len;
-        if (h < 0 || h >= j->len) { pass = 0; continue; }
-        if (j->payload < 0) {
-          pass = j->ht[h] == fk;
-        } else {
-          pass = j->ht[2 * h] == fk;
-          if (pass) {
-            o->payload_val[j->payload] = j->ht[2 * h + 1];
-            o->payload_valid[j->payload] = o->cols[j->payload].nullable ? j->hv[h] : 1;
-          }
-        }
-      }
-      if (!pass) continue;
-      if (o->ngroups == 0) {
-        for (int a = 0; a < o->naggs; ++a) {
-          const AggS* ag = &o->aggs[a];
-          const int v = ag->arg->op == E_STAR ? 1 : valid_of(&rcx, ag->arg);
-          if (!v) continue;
-          const uint64_t x = ag->fn == 0 ? 1 : convert(math_push(&rcx, ag->arg, 1), T_U64).bits;
-          switch (ag->fn) {
-            case 0: acc[a] += 1; break;
-            case 1: acc[a] += x; seen[a]++; break;
-            case 4: acc[a] += x; cnt[a]++; break;
-            case 2: if (x < acc[a]) acc[a] = x; seen[a]++; break;
-            case 3: if (x > acc[a]) acc[a] = x; seen[a]++; break;
-          }
-        }
-        continue;
-      }
-      /* Grouped: perfect hash. */
-      long long hsh = 0;
-      int dom_ok = 1;
-      for (int g = 0; g < o->ngroups; ++g) {
-        const GroupS* gs = &o->groups[g];
-        const long long card = gs->card + (gs->nullable ? 1 : 0);
-        long long term;
-        const int64_t v = as_i64(value_of(&rcx, gs->e));
-        if (gs->nullable) term = valid_of(&rcx, gs->e) ? v - gs->min + 1 : 0;
-        else term = v - gs->min;
-        if (term < 0 || term >= card) dom_ok = 0;
-        hsh = g == 0 ? term : hsh * card + term;
-      }
-      hsh = hsh % (long long)G;
-      if (!dom_ok) derr++;
-      if (hsh < 0 || (uint64_t)hsh >= G) continue;
-      const uint64_t base = (uint64_t)hsh * ts;
-      touched[hsh] = 1;
-      int avg_i = 0;
-      for (int a = 0; a < o->naggs; ++a) {
-        const AggS* ag = &o->aggs[a];
-        const int slot = o->ngroups + a;
-        const int v = ag->arg->op == E_STAR ? 1 : valid_of(&rcx, ag->arg);
-        if (ag->fn == 0) {
-          if (v) result[base + slot] += 1;
-          if (!o->sparse) set_bit(validity, base + slot);
-          continue;
-        }
-        if (ag->fn == 4) {
-          if (v) {
-            result[base + slot] += convert(math_push(&rcx, ag->arg, 1), T_U64).bits;
-            result[base + vts + avg_i] += 1;
-          }
-          avg_i++;
-          continue;
-        }
-        if (!v) continue;
-        const uint64_t x = convert(math_push(&rcx, ag->arg, 1), T_U64).bits;
-        if (ag->fn == 1) result[base + slot] += x;
-        else if (ag->fn == 2) { if (x < result[base + slot]) result[base + slot] = x; }
-        else { if (x > result[base + slot]) result[base + slot] = x; }
-        if (!o->sparse) set_bit(validity, base + slot);
-      }
+      walk(&st, &rcx, 0);
     }
+    uint64_t* acc = st.acc;
+    uint64_t* seen = st.seen;
+    uint64_t* cnt = st.cnt;
+    unsigned char* touched = st.touched;
+    const long long derr = st.derr;
     if (o->ngroups == 0) {
       int avg_i = 0;
       for (int a = 0; a < o->naggs; ++a) {
@@ -747,7 +882,16 @@ done:
   if (rc && err && errlen > 0) snprintf(err, (size_t)errlen, "%s", o->err);
   for (int s = 0; s < o->nsteps; ++s) {
     if (o->steps[s].kind == 0) free_expr(o->steps[s].filter);
-    else { free_expr(o->steps[s].join.filter); free(o->steps[s].join.ht); free(o->steps[s].join.hv); }
+    else {
+      JoinS* j = &o->steps[s].join;
+      free_expr(j->filter);
+      free(j->ht);
+      free(j->hv);
+      free(j->mkey);
+      free(j->mcnt);
+      free(j->moff);
+      free(j->mrows);
+    }
   }
   for (int g = 0; g < o->ngroups; ++g) free_expr(o->groups[g].e);
   for (int a = 0; a < o->naggs; ++a) free_expr(o->aggs[a].arg);

@@ -3,7 +3,9 @@ primitives compiled for the host).  TEST/BENCH INFRASTRUCTURE ONLY.
 
 Translates a star-join plan of the supported shape (AND-chains of
 `column op literal` filters, PHT_1/PHT_2 joins, GROUP BY over columns, SUM of a
-column / product / difference, COUNT(*)) into the harness's query struct.
+column / product / difference, COUNT(*)) into the harness's query struct.  One
+join may expand rows: an OR over two fact keys, or a multi-value hash table
+publishing at most one build column.
 """
 from __future__ import annotations
 
@@ -24,7 +26,8 @@ class RefPred(C.Structure):
 
 class RefJoin(C.Structure):
     _fields_ = [("fk", C.c_int), ("pk", C.c_int), ("payload", C.c_int), ("len", C.c_int), ("keymin", C.c_int),
-                ("dim_rows", C.c_int), ("npred", C.c_int), ("preds", RefPred * 8)]
+                ("dim_rows", C.c_int), ("npred", C.c_int), ("preds", RefPred * 8), ("fk2", C.c_int),
+                ("multi", C.c_int)]
 
 
 class RefOperand(C.Structure):
@@ -94,10 +97,21 @@ def translate(plan, dim_rows: dict[str, int]):
     for k, (c, op, lit) in enumerate(fact_preds):
         q.preds[k] = RefPred(idx(c), op, lit)
     q.njoin = len(joins)
+    if sum(1 for s in joins if s.expands) > 1:
+        raise ValueError("more than one expanding join is outside the reference harness")
     for j, s in enumerate(joins):
         J = q.joins[j]
         J.fk, J.pk = idx(s.fk), idx(s.pk)
-        J.payload = idx(s.payload) if s.payload else -1
+        if len(s.more_fks) > 1 or len(s.gathers) > 1:
+            raise ValueError("OR-join over more than two keys or MHT with several columns")
+        J.fk2 = idx(s.more_fks[0]) if s.more_fks else -1
+        J.multi = int(s.multi)
+        if s.multi:
+            J.payload = idx(s.gathers[0]) if s.gathers else -1
+            if s.gathers:
+                payload_of[s.gathers[0]] = j
+        else:
+            J.payload = idx(s.payload) if s.payload else -1
         J.len, J.keymin, J.dim_rows = s.length, s.keymin, dim_rows[s.dim]
         leaves = _and_leaves(s.filter) if s.filter is not None else []
         J.npred = len(leaves)

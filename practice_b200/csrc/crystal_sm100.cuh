@@ -637,7 +637,8 @@ enum : unsigned int {
   ERR_WAIT_TIMEOUT = 1,      // an mbarrier wait exceeded its iteration limit
   ERR_GROUP_DOMAIN = 2,      // a GROUP BY key fell outside its catalog domain
   ERR_SCRATCH = 3,           // scratch too small for the requested table
-  ERR_DIM_COLLISION = 4,     // two dimension keys share a slot of a shared-scan index
+  ERR_DIM_COLLISION = 4,     // two distinct dimension keys share a slot of a shared-scan
+                             // index or of a multi-value hash table
 };
 
 CX_DEVICE void raise(unsigned int* err, unsigned int code) {
@@ -734,6 +735,35 @@ static __device__ __noinline__ void drain_stages(unsigned long long* bars, int n
     const long long tt = first + kk * stride;
     if (tt < full_tiles) (void)mbar_wait_bounded(&bars[kk % nstage], (unsigned)((kk / nstage) & 1), limit);
   }
+}
+
+// Exclusive prefix sum of a 64-bit value over the CTA (every thread gets the
+// sum of the values of lower-numbered threads); `*total` receives the CTA sum
+// in every thread.  `scratch` holds BT/32 + 1 words.
+template <int BT>
+CX_DEVICE long long block_exclusive_scan_i64(long long v, long long* scratch, long long* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  long long inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  __syncthreads();
+  if (lane == 31) scratch[warp] = inc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long run = 0;
+    for (int w = 0; w < BT / 32; ++w) {
+      const long long t = scratch[w];
+      scratch[w] = run;
+      run += t;
+    }
+    scratch[BT / 32] = run;
+  }
+  __syncthreads();
+  *total = scratch[BT / 32];
+  return scratch[warp] + inc - v;
 }
 
 // Sum of a 64-bit value over the CTA; the result is valid in thread 0.

@@ -52,4 +52,5 @@ struct CxArgs {
   int fbase[CX_MAX_FCOLS];                     // first value of each fact filter table window
   int fwin[CX_MAX_FCOLS];                      // values in the window (0: evaluate every row per query)
   int lits[CX_MAX_LITS];                       // literal parameters of a parametric plain kernel
+  int* mpay[CX_MAX_HTS];                       // multi-value hash tables: build row ids grouped by slot
 };

@@ -298,7 +298,160 @@ struct Emitter {
   }
 
   // ------------------------------------------------------------- builds ---
+  // Multi-value hash table scratch (ints, one `ht` slot): the directory
+  // [key, offset, count] per slot at 0, then counts, offsets, write cursors
+  // and the per-4096-slot block sums of the offset scan.
+  static long long mht_blocks(const Join& j) { return (j.len + 4095) / 4096; }
+  static long long mht_words(const Join& j) { return 6 * j.len + mht_blocks(j) + 1; }
+
+  // Build-side prologue shared by the PHT and MHT build kernels: the tile loop
+  // over the dimension, its filter and the key's validity.
+  void build_prologue(std::ostream& o, const Join& j, const std::vector<std::string>& cols, int t) {
+    o << "  constexpr int BLOCK_THREADS = 128, ITEMS_PER_THREAD = 4, TILE_SIZE = 512;\n";
+    o << "  const int tid = threadIdx.x;\n";
+    o << "  const long long n_rows = a.rows[" << t << "];\n";
+    declare_cols(o, cols, "  ");
+    o << "  for (long long tile = blockIdx.x; tile * TILE_SIZE < n_rows; tile += gridDim.x) {\n";
+    o << "    const long long tile_offset = tile * TILE_SIZE;\n";
+    o << "    const int num_tile_items = (int)(n_rows - tile_offset < TILE_SIZE ? n_rows - tile_offset : TILE_SIZE);\n";
+    o << "    int flags[ITEMS_PER_THREAD];\n";
+    declare_regs(o, cols, "    ");
+    o << "    InitFlags<BLOCK_THREADS, ITEMS_PER_THREAD>(flags);\n";
+    if (j.filter) emit_filter(o, j.filter.get(), "    ");
+    ensure_loaded(o, j.pk, "    ");
+    if (nullable(j.pk))
+      o << "    BlockApplyValidityAnd<BLOCK_THREADS, ITEMS_PER_THREAD>(tid, flags, " << j.pk << "_valid, num_tile_items);\n";
+  }
+
+  // MHT build (emitMHTBuildKernels, visitor.cpp:4295-4464): count per slot,
+  // a three-kernel exclusive scan of the counts, then the write of build row
+  // ids.  The payload array is sized by the dimension's rows, so nothing is
+  // read back to the host between the passes.  A slot that receives two
+  // distinct keys raises ERR_DIM_COLLISION (the count pass stores each row's
+  // key, the write pass checks it before the directory is rewritten).
+  void emit_mht_build(const Join& j) {
+    const int t = p.table_slot(j.dim);
+    const int h = ht_slot.at(j.dim);
+    const long long L = j.len, NB = mht_blocks(j);
+    const std::string d = lower(j.dim);
+    std::vector<std::string> cols;
+    if (j.filter) collect(j.filter.get(), cols);
+    if (std::find(cols.begin(), cols.end(), j.pk) == cols.end()) cols.push_back(j.pk);
+    const std::string Ls = std::to_string(L) + "LL";
+    auto views = [&](std::ostream& o) {
+      o << "  int* ht_dir = a.ht[" << h << "]; (void)ht_dir;\n";
+      o << "  int* mht_counts = ht_dir + 3 * " << Ls << "; (void)mht_counts;\n";
+      o << "  int* mht_offsets = ht_dir + 4 * " << Ls << "; (void)mht_offsets;\n";
+      o << "  int* mht_wpos = ht_dir + 5 * " << Ls << "; (void)mht_wpos;\n";
+      o << "  int* mht_bsum = ht_dir + 6 * " << Ls << "; (void)mht_bsum;\n";
+    };
+    auto key_loop = [&](std::ostream& o, const std::string& body) {
+      o << "    #pragma unroll\n    for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << "      if (flags[i] && tid + BLOCK_THREADS * i < num_tile_items) {\n";
+      o << "        const int s_ = cx_detail::pht_slot<int>(" << j.pk << "[i], " << L << ", " << j.keymin << ");\n";
+      o << "        if (s_ >= 0) " << body << "\n";
+      o << "      }\n    }\n";
+    };
+
+    // Pass 1: count.
+    {
+      const std::string kname = "mht_count_" + d;
+      meta << "kernel " << kname << " build " << t << " 128 512\n";
+      loaded.clear();
+      valid_regs.clear();
+      tile_ptr = [](const std::string& c) { return "d_" + c + " + tile_offset"; };
+      std::ostringstream& o = src;
+      o << "extern \"C\" __global__ void __launch_bounds__(128) " << kname << "(const CxArgs a) {\n";
+      o << param_decl();
+      views(o);
+      build_prologue(o, j, cols, t);
+      o << "    BlockBuildMHT_Count<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << j.pk << ", flags, mht_counts, " << L
+        << ", " << j.keymin << ", num_tile_items);\n";
+      key_loop(o, "ht_dir[3LL * s_] = " + j.pk + "[i];");
+      o << "  }\n}\n\n";
+    }
+    // Pass 2: per-block sums of 4096 counts.
+    {
+      const std::string kname = "mht_blocksum_" + d;
+      meta << "kernel " << kname << " fixed " << NB << " 256 0\n";
+      src << "extern \"C\" __global__ void __launch_bounds__(256) " << kname << "(const CxArgs a) {\n";
+      views(src);
+      src << "  __shared__ unsigned long long red[8];\n";
+      src << "  const long long base = (long long)blockIdx.x * 4096LL;\n";
+      src << "  unsigned long long s = 0;\n";
+      src << "  for (int k = threadIdx.x; k < 4096; k += 256) {\n";
+      src << "    const long long x = base + k;\n";
+      src << "    if (x < " << Ls << ") s += (unsigned long long)mht_counts[x];\n";
+      src << "  }\n";
+      src << "  s = cx::block_sum_u64<256>(s, red);\n";
+      src << "  if (threadIdx.x == 0) mht_bsum[blockIdx.x] = (int)s;\n";
+      src << "}\n\n";
+    }
+    // Pass 3: exclusive scan of the block sums (one CTA).
+    {
+      const std::string kname = "mht_blockscan_" + d;
+      meta << "kernel " << kname << " fixed 1 1024 0\n";
+      src << "extern \"C\" __global__ void __launch_bounds__(1024) " << kname << "(const CxArgs a) {\n";
+      views(src);
+      src << "  __shared__ long long sc[33];\n";
+      src << "  long long carry = 0;\n";
+      src << "  for (long long b0 = 0; b0 < " << NB << "LL; b0 += 1024) {\n";
+      src << "    const long long b = b0 + threadIdx.x;\n";
+      src << "    const long long v = b < " << NB << "LL ? (long long)mht_bsum[b] : 0LL;\n";
+      src << "    long long tot = 0;\n";
+      src << "    const long long ex = cx::block_exclusive_scan_i64<1024>(v, sc, &tot);\n";
+      src << "    if (b < " << NB << "LL) mht_bsum[b] = (int)(carry + ex);\n";
+      src << "    carry += tot;\n";
+      src << "  }\n";
+      src << "}\n\n";
+    }
+    // Pass 4: slot offsets = block base + scan within the block.
+    {
+      const std::string kname = "mht_offsets_" + d;
+      meta << "kernel " << kname << " fixed " << NB << " 256 0\n";
+      src << "extern \"C\" __global__ void __launch_bounds__(256) " << kname << "(const CxArgs a) {\n";
+      views(src);
+      src << "  __shared__ long long sc[9];\n";
+      src << "  const long long base = (long long)blockIdx.x * 4096LL + (long long)threadIdx.x * 16;\n";
+      src << "  int v[16];\n";
+      src << "  long long loc = 0;\n";
+      src << "  #pragma unroll\n  for (int k = 0; k < 16; ++k) {\n";
+      src << "    v[k] = base + k < " << Ls << " ? mht_counts[base + k] : 0;\n";
+      src << "    loc += v[k];\n";
+      src << "  }\n";
+      src << "  long long tot = 0;\n";
+      src << "  long long run = (long long)mht_bsum[blockIdx.x] + cx::block_exclusive_scan_i64<256>(loc, sc, &tot);\n";
+      src << "  #pragma unroll\n  for (int k = 0; k < 16; ++k) {\n";
+      src << "    if (base + k < " << Ls << ") mht_offsets[base + k] = (int)run;\n";
+      src << "    run += v[k];\n";
+      src << "  }\n";
+      src << "}\n\n";
+    }
+    // Pass 5: write row ids and the directory.
+    {
+      const std::string kname = "mht_write_" + d;
+      meta << "kernel " << kname << " build " << t << " 128 512\n";
+      loaded.clear();
+      valid_regs.clear();
+      tile_ptr = [](const std::string& c) { return "d_" + c + " + tile_offset"; };
+      std::ostringstream& o = src;
+      o << "extern \"C\" __global__ void __launch_bounds__(128) " << kname << "(const CxArgs a) {\n";
+      o << param_decl();
+      views(o);
+      o << "  int* mht_payload = a.mpay[" << h << "];\n";
+      build_prologue(o, j, cols, t);
+      o << "    int row_ids[ITEMS_PER_THREAD];\n";
+      o << "    BlockMakeRowIds<BLOCK_THREADS, ITEMS_PER_THREAD>(tid, (int)tile_offset, row_ids, num_tile_items);\n";
+      key_loop(o, "{ if (((volatile int*)ht_dir)[3LL * s_] != " + j.pk + "[i]) cx::raise(a.err, cx::ERR_DIM_COLLISION); }");
+      o << "    BlockBuildMHT_Write<int, int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << j.pk
+        << ", row_ids, flags, ht_dir, mht_offsets, mht_wpos, mht_counts, mht_payload, " << L << ", " << j.keymin
+        << ", num_tile_items);\n";
+      o << "  }\n}\n\n";
+    }
+  }
+
   void emit_build(const Join& j) {
+    if (j.multi) return emit_mht_build(j);
     const int t = p.table_slot(j.dim);
     const int h = ht_slot.at(j.dim);
     std::vector<std::string> cols;
@@ -316,22 +469,9 @@ struct Emitter {
     std::ostringstream& o = src;
     o << "extern \"C\" __global__ void __launch_bounds__(128) " << kname << "(const CxArgs a) {\n";
     o << param_decl();
-    o << "  constexpr int BLOCK_THREADS = 128, ITEMS_PER_THREAD = 4, TILE_SIZE = 512;\n";
-    o << "  const int tid = threadIdx.x;\n";
-    o << "  const long long n_rows = a.rows[" << t << "];\n";
-    declare_cols(o, cols, "  ");
     o << "  int* " << ht_name(j.dim) << " = a.ht[" << h << "];\n";
     if (v2v) o << "  unsigned int* " << ht_name(j.dim) << "_valid = a.htv[" << h << "];\n";
-    o << "  for (long long tile = blockIdx.x; tile * TILE_SIZE < n_rows; tile += gridDim.x) {\n";
-    o << "    const long long tile_offset = tile * TILE_SIZE;\n";
-    o << "    const int num_tile_items = (int)(n_rows - tile_offset < TILE_SIZE ? n_rows - tile_offset : TILE_SIZE);\n";
-    o << "    int flags[ITEMS_PER_THREAD];\n";
-    declare_regs(o, cols, "    ");
-    o << "    InitFlags<BLOCK_THREADS, ITEMS_PER_THREAD>(flags);\n";
-    if (j.filter) emit_filter(o, j.filter.get(), "    ");
-    ensure_loaded(o, j.pk, "    ");
-    if (nullable(j.pk))
-      o << "    BlockApplyValidityAnd<BLOCK_THREADS, ITEMS_PER_THREAD>(tid, flags, " << j.pk << "_valid, num_tile_items);\n";
+    build_prologue(o, j, cols, t);
     if (!v2) {
       o << "    BlockBuildSelectivePHT_1<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << j.pk << ", flags, "
         << ht_name(j.dim) << ", " << j.len << ", " << j.keymin << ", num_tile_items);\n";
@@ -351,6 +491,7 @@ struct Emitter {
 
   // Slot-occupancy bitmap of a built PHT: bit h is set when slot h holds a key.
   void emit_occupancy(const Join& j) {
+    if (j.multi) return;
     const int h = ht_slot.at(j.dim);
     const long long words = (j.len + 31) / 32;
     const std::string kname = "occupancy_" + lower(j.dim);
@@ -433,6 +574,17 @@ struct Emitter {
     }
     for (const auto& g : p.groups) add_fact(g.expr.get());
     for (const auto& ag : p.aggs) add_fact(ag.arg.get());
+    // The first join that can emit a row more than once (an OR over several
+    // fact keys or an MHT) switches the rest of the pipeline to item mode.
+    std::vector<std::string> gather_cols;
+    size_t xs = p.steps.size();
+    for (size_t k = 0; k < p.steps.size(); ++k) {
+      const Step& s = p.steps[k];
+      if (s.kind != Step::JoinStep) continue;
+      for (const auto& g : s.join.gathers) gather_cols.push_back(g);
+      if (s.join.expands() && xs == p.steps.size()) xs = k;
+    }
+    const bool expanding = xs < p.steps.size();
 
     const int NSC = (int)fact_cols.size();
     const int STAGES = (NSC == 0) ? 0 : std::max(0, tu.stages);
@@ -467,7 +619,7 @@ struct Emitter {
     {
       unsigned long long used = 0;
       for (const auto& s : p.steps) {
-        if (s.kind != Step::JoinStep) continue;
+        if (s.kind != Step::JoinStep || s.join.expands()) continue;
         const unsigned long long words = (unsigned long long)((s.join.len + 31) / 32);
         const unsigned long long bytes = ((words * 4) + 15) & ~15ULL;
         if (used + bytes > (unsigned long long)std::max(0, tu.bitmap_budget)) continue;
@@ -507,6 +659,7 @@ struct Emitter {
 
     std::vector<std::string> reg_cols = fact_cols;
     for (const auto& c : payload_cols) reg_cols.push_back(c);
+    for (const auto& c : gather_cols) reg_cols.push_back(c);
 
     loaded.clear();
     valid_regs.clear();
@@ -535,10 +688,12 @@ struct Emitter {
     o << "  unsigned long long* d_result = a.result; (void)d_result;\n";
     o << "  uint64_t* d_result_validity = (uint64_t*)a.result_validity; (void)d_result_validity;\n";
     declare_cols(o, fact_cols, "  ");
+    declare_cols(o, gather_cols, "  ");
     for (const auto& s : p.steps) {
       if (s.kind != Step::JoinStep) continue;
       const int h = ht_slot.at(s.join.dim);
       o << "  const int* " << ht_name(s.join.dim) << " = a.ht[" << h << "];\n";
+      if (s.join.multi) o << "  const int* mpay_" << lower(s.join.dim) << " = a.mpay[" << h << "];\n";
       if (!s.join.payload.empty() && payload_valid.count(s.join.payload))
         o << "  const unsigned int* " << ht_name(s.join.dim) << "_valid = a.htv[" << h << "];\n";
     }
@@ -648,7 +803,8 @@ struct Emitter {
       o << ind << "BlockProbeBitmapAnd<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << b.fk << ", flags, s_bm_"
         << lower(b.dim) << ", " << b.len << ", " << b.keymin << ", num_tile_items);\n";
     }
-    for (const auto& s : p.steps) {
+    for (size_t k = 0; k < xs; ++k) {
+      const Step& s = p.steps[k];
       if (s.kind == Step::Filter) {
         emit_filter(o, s.filter.get(), ind);
         continue;
@@ -673,18 +829,13 @@ struct Emitter {
         loaded.insert(j.payload);
       }
     }
-    for (const auto& g : p.groups) load_expr_cols(o, g.expr.get(), ind);
-    for (const auto& ag : p.aggs) load_expr_cols(o, ag.arg.get(), ind);
-
-    // Aggregate consume.
-    if (!grouped) {
-      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+    // Per-row aggregate updates shared by the vector and the item-mode paths.
+    // Ungrouped: thread-private accumulators.
+    auto scalar_update = [&](const std::string& ii) {
       for (int k = 0; k < NA; ++k) {
         const Agg& ag = p.aggs[k];
         const std::string v = ag.arg->op == Op::Star ? "1" : valid_of(ag.arg.get());
         const std::string x = ag.fn == AggFn::Count ? "1ULL" : math_push(ag.arg.get(), true);
-        const std::string ii = ind + "    ";
         switch (ag.fn) {
           case AggFn::Count: o << ii << "if (" << v << ") acc_" << k << " += 1ULL;\n"; break;
           case AggFn::Sum: o << ii << "if (" << v << ") { acc_" << k << " += " << x << "; seen_" << k << " += 1ULL; }\n"; break;
@@ -699,37 +850,181 @@ struct Emitter {
             break;
         }
       }
-      o << ind << "  }\n" << ind << "}\n";
-    } else if (reg_groups) {
-      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+    };
+    // Grouped: the perfect-hash group of the row in `hash`.
+    auto group_hash = [&](const std::string& ii) {
       std::string horner, dom;
       for (size_t k = 0; k < p.groups.size(); ++k) {
-        o << ind << "    const int gt" << k << " = " << group_term(k) << ";\n";
+        o << ii << "const int gt" << k << " = " << group_term(k) << ";\n";
         horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(eff_card(k)) + " + gt" + std::to_string(k) + ")";
         dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " +
                std::to_string(eff_card(k)) + "u";
       }
-      o << ind << "    const int hash = (" << horner << ") % " << G << ";\n";
-      o << ind << "    if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
-      o << ind << "    if ((unsigned)hash < " << G << "u) {\n";
-      o << ind << "      rtouch |= 1u << hash;\n";
+      o << ii << "const int hash = (" << horner << ") % " << G << ";\n";
+      o << ii << "if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+    };
+    // Tiny group domains: register accumulators selected by a compare chain.
+    auto reg_update = [&](const std::string& ii) {
+      o << ii << "rtouch |= 1u << hash;\n";
       for (int k = 0; k < NA; ++k) {
         const Agg& ag = p.aggs[k];
         const std::string v = ag.arg->op == Op::Star ? "1" : valid_of(ag.arg.get());
         const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + math_push(ag.arg.get(), true) + ")";
-        o << ind << "      if (" << v << ") {\n";
-        o << ind << "        const unsigned long long x_ = " << x << ";\n";
-        o << ind << "        #pragma unroll\n" << ind << "        for (int g = 0; g < " << G << "; ++g) if (hash == g) {\n";
+        o << ii << "if (" << v << ") {\n";
+        o << ii << "  const unsigned long long x_ = " << x << ";\n";
+        o << ii << "  #pragma unroll\n" << ii << "  for (int g = 0; g < " << G << "; ++g) if (hash == g) {\n";
         const std::string r = "racc[g * " + std::to_string(NACC) + " + " + std::to_string(k) + "]";
-        if (ag.fn == AggFn::Min) o << ind << "          if (x_ < " << r << ") " << r << " = x_;\n";
-        else if (ag.fn == AggFn::Max) o << ind << "          if (x_ > " << r << ") " << r << " = x_;\n";
-        else o << ind << "          " << r << " += x_;\n";
-        if (ag.fn == AggFn::Avg) o << ind << "          racc[g * " << NACC << " + " << avg_idx[k] << "] += 1ULL;\n";
-        o << ind << "        }\n";
-        if (seen_idx[k] >= 0 && NSEEN_T > 0) o << ind << "        rseen_" << k << " |= 1u << hash;\n";
-        o << ind << "      }\n";
+        if (ag.fn == AggFn::Min) o << ii << "    if (x_ < " << r << ") " << r << " = x_;\n";
+        else if (ag.fn == AggFn::Max) o << ii << "    if (x_ > " << r << ") " << r << " = x_;\n";
+        else o << ii << "    " << r << " += x_;\n";
+        if (ag.fn == AggFn::Avg) o << ii << "    racc[g * " << NACC << " + " << avg_idx[k] << "] += 1ULL;\n";
+        o << ii << "  }\n";
+        if (seen_idx[k] >= 0 && NSEEN_T > 0) o << ii << "  rseen_" << k << " |= 1u << hash;\n";
+        o << ii << "}\n";
       }
+    };
+    // Item mode, larger domains: one atomic update per row into the shared or
+    // global group table (no warp merging: lanes run different expansions).
+    auto atomic_update = [&](const std::string& ii) {
+      const std::string bit = "(1u << (hash & 31))";
+      o << ii << (smem_groups ? "atomicOr(&s_touch[hash >> 5], " : "atomicOr(&g_touch[hash >> 5], ") << bit << ");\n";
+      for (int k = 0; k < NA; ++k) {
+        const Agg& ag = p.aggs[k];
+        const int slot = (int)p.groups.size() + k;
+        const std::string v = ag.arg->op == Op::Star ? "1" : valid_of(ag.arg.get());
+        const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + math_push(ag.arg.get(), true) + ")";
+        const std::string row = "(unsigned long long)hash * " + std::to_string(TS) + "ULL";
+        const std::string acc = smem_groups ? "s_acc[(long long)hash * " + std::to_string(NACC) + " + " + std::to_string(k) + "]"
+                                            : "d_result[" + row + " + " + std::to_string(slot) + "]";
+        o << ii << "if (" << v << ") {\n";
+        o << ii << "  const unsigned long long x_ = " << x << ";\n";
+        if (ag.fn == AggFn::Min) o << ii << "  atomicMin(&" << acc << ", x_);\n";
+        else if (ag.fn == AggFn::Max) o << ii << "  atomicMax(&" << acc << ", x_);\n";
+        else o << ii << "  atomicAdd(&" << acc << ", x_);\n";
+        if (seen_idx[k] >= 0 && NSEEN_T > 0) {
+          if (smem_groups)
+            o << ii << "  atomicOr(&s_seen[" << (unsigned long long)seen_idx[k] * TW << "ULL + (hash >> 5)], " << bit << ");\n";
+          else
+            o << ii << "  db::atomic_set_valid_bit(d_result_validity, " << row << " + " << slot << ");\n";
+        }
+        if (ag.fn == AggFn::Avg) {
+          if (smem_groups) o << ii << "  atomicAdd(&s_acc[(long long)hash * " << NACC << " + " << avg_idx[k] << "], 1ULL);\n";
+          else o << ii << "  atomicAdd(&d_result[" << row << " + " << p.hidden_count_slot(k) << "], 1ULL);\n";
+        }
+        o << ii << "}\n";
+        if (ag.fn == AggFn::Count && !p.sparse && !smem_groups)
+          o << ii << "db::atomic_set_valid_bit(d_result_validity, " << row << " + " << slot << ");\n";
+      }
+    };
+    auto item_consume = [&](const std::string& ii) {
+      if (!grouped) return scalar_update(ii);
+      o << ii << "{\n";
+      group_hash(ii + "  ");
+      o << ii << "  if ((unsigned)hash < " << G << "u) {\n";
+      if (reg_groups) reg_update(ii + "    ");
+      else atomic_update(ii + "    ");
+      o << ii << "  }\n" << ii << "}\n";
+    };
+    // Steps from k on for item i (consumeHashJoinVector's OR-join branches and
+    // MHT expansion loop, visitor.cpp:4587-4730; later joins probe in item
+    // mode like consumeHashJoinItem).  A fact key equal to an earlier valid key
+    // of the same row is skipped, so one dimension row is never counted twice.
+    std::function<void(size_t, const std::string&)> item_steps = [&](size_t k, const std::string& ii) {
+      if (k == p.steps.size()) return item_consume(ii);
+      const Step& s = p.steps[k];
+      if (s.kind == Step::Filter) {
+        o << ii << "if (" << and_terms({valid_of(s.filter.get()), value_of(s.filter.get())}) << ") {\n";
+        item_steps(k + 1, ii + "  ");
+        o << ii << "}\n";
+        return;
+      }
+      const Join& j = s.join;
+      const std::string K = std::to_string(k), ht = ht_name(j.dim);
+      for (size_t f = 0; f < j.fks.size(); ++f) {
+        const std::string& fk = j.fks[f];
+        std::vector<std::string> terms{valid_regs.count(fk) ? fk + "_valid[i]" : "1"};
+        for (size_t q = 0; q < f; ++q) {
+          const std::string& pf = j.fks[q];
+          const std::string pv = valid_regs.count(pf) ? pf + "_valid[i]" : "1";
+          terms.push_back(lit_true(pv) ? fk + "[i] != " + pf + "[i]" : "(!(" + pv + ") || " + fk + "[i] != " + pf + "[i])");
+        }
+        o << ii << "if (" << and_terms(terms) << ") {\n";
+        const std::string i2 = ii + "  ";
+        if (j.multi) {
+          const std::string off = "off" + K, cnt = "cnt" + K, fl = "fl" + K, jj = "j" + K, rid = "rid" + K;
+          o << i2 << "int " << off << " = 0, " << cnt << " = 0, " << fl << " = 1;\n";
+          o << i2 << "ProbeMultiHT<int>(" << fk << "[i], " << off << ", " << cnt << ", " << fl << ", " << ht << ", " << j.len
+            << ", " << j.keymin << ");\n";
+          o << i2 << "for (int " << jj << " = 0; " << jj << " < " << cnt << "; ++" << jj << ") {\n";
+          o << i2 << "  const long long " << rid << " = mpay_" << lower(j.dim) << "[" << off << " + " << jj << "];\n";
+          for (const auto& g : j.gathers) {
+            o << i2 << "  " << g << "[i] = d_" << g << "[" << rid << "];\n";
+            if (nullable(g))
+              o << i2 << "  " << g << "_valid[i] = n_" << g << " ? (int)((n_" << g << "[" << rid << " >> 6] >> (" << rid
+                << " & 63)) & 1ULL) : 1;\n";
+          }
+          item_steps(k + 1, i2 + "  ");
+          o << i2 << "}\n";
+        } else {
+          const std::string hs = "h" + K + "_" + std::to_string(f);
+          o << i2 << "const int " << hs << " = cx_detail::pht_slot<int>(" << fk << "[i], " << j.len << ", " << j.keymin << ");\n";
+          if (j.payload.empty()) {
+            o << i2 << "if (" << hs << " >= 0 && " << ht << "[" << hs << "] == " << fk << "[i]) {\n";
+          } else {
+            o << i2 << "if (" << hs << " >= 0 && " << ht << "[2LL * " << hs << "] == " << fk << "[i]) {\n";
+            o << i2 << "  " << j.payload << "[i] = " << ht << "[2LL * " << hs << " + 1];\n";
+            if (payload_valid.count(j.payload))
+              o << i2 << "  " << j.payload << "_valid[i] = (int)((" << ht << "_valid[" << hs << " >> 5] >> (" << hs
+                << " & 31)) & 1u);\n";
+          }
+          item_steps(k + 1, i2 + "  ");
+          o << i2 << "}\n";
+        }
+        o << ii << "}\n";
+      }
+    };
+
+    if (expanding) {
+      // Columns the expansion publishes are written inside the item loop;
+      // every fact column the rest of the pipeline reads is loaded once here.
+      for (size_t k = xs; k < p.steps.size(); ++k) {
+        const Step& s = p.steps[k];
+        if (s.kind != Step::JoinStep) continue;
+        for (const auto& c : s.join.gathers) {
+          loaded.insert(c);
+          if (nullable(c)) valid_regs.insert(c);
+        }
+        if (!s.join.payload.empty()) {
+          loaded.insert(s.join.payload);
+          if (payload_valid.count(s.join.payload)) valid_regs.insert(s.join.payload);
+        }
+      }
+      for (size_t k = xs; k < p.steps.size(); ++k) {
+        const Step& s = p.steps[k];
+        if (s.kind == Step::Filter) load_expr_cols(o, s.filter.get(), ind);
+        else for (const auto& fk : s.join.fks) ensure_loaded(o, fk, ind);
+      }
+    }
+    for (const auto& g : p.groups) load_expr_cols(o, g.expr.get(), ind);
+    for (const auto& ag : p.aggs) load_expr_cols(o, ag.arg.get(), ind);
+
+    // Aggregate consume.
+    if (expanding) {
+      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+      item_steps(xs, ind + "    ");
+      o << ind << "  }\n" << ind << "}\n";
+    } else if (!grouped) {
+      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+      scalar_update(ind + "    ");
+      o << ind << "  }\n" << ind << "}\n";
+    } else if (reg_groups) {
+      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+      group_hash(ind + "    ");
+      o << ind << "    if ((unsigned)hash < " << G << "u) {\n";
+      reg_update(ind + "      ");
       o << ind << "    }\n";
       o << ind << "  }\n";
       o << ind << "}\n";
@@ -1021,6 +1316,12 @@ struct Emitter {
     for (const auto& s : p.steps) {
       if (s.kind != Step::JoinStep) continue;
       ht_slot[s.join.dim] = h;
+      if (s.join.multi) {
+        meta << "ht " << h << " " << ht_name(s.join.dim) << " " << mht_words(s.join) << "\n";
+        meta << "mht " << h << " " << p.table_slot(s.join.dim) << "\n";
+        ++h;
+        continue;
+      }
       const long long words = 2 * s.join.len;  // 2 x len, as the reference allocates (visitor.cpp:4216-4218)
       meta << "ht " << h << " " << ht_name(s.join.dim) << " " << words << "\n";
       if (!s.join.payload.empty() && payload_valid.count(s.join.payload))
@@ -1219,6 +1520,7 @@ struct SharedGen {
         if (s.kind != Step::JoinStep) continue;
         const Join& j = s.join;
         if (j.fks.size() != 1) throw PlanError("OR-joins are not shareable");
+        if (j.multi) throw PlanError("multi-value hash joins are not shareable");
         int di = dim_index(j.dim);
         if (di < 0) {
           dims.push_back(Dim());

@@ -1,6 +1,7 @@
 // cx_plan.cpp -- S-expression reader and validation for star-join plans.
 #include "cx_plan.h"
 
+#include <algorithm>
 #include <cctype>
 #include <cstdlib>
 #include <functional>
@@ -246,9 +247,19 @@ std::unique_ptr<Plan> parse_plan(const std::string& text) {
       j.len = to_int(len->items.at(1), "len");
       j.keymin = to_int(km->items.at(1), "keymin");
       if (const Node* f = field(n, "filter")) j.filter = to_expr(f->items.at(1));
-      if (const Node* pl = field(n, "payload")) j.payload = to_name(pl->items.at(1), "payload");
+      if (const Node* mu = field(n, "multi")) j.multi = to_int(mu->items.at(1), "multi") != 0;
+      if (const Node* pl = field(n, "payload")) {
+        if (pl->items.size() < 2) throw PlanError("(payload C ...) names no column for " + j.dim);
+        if (j.multi) {
+          for (size_t k = 1; k < pl->items.size(); ++k) j.gathers.push_back(to_name(pl->items[k], "payload"));
+        } else {
+          if (pl->items.size() != 2) throw PlanError("a perfect-hash join publishes one payload column: " + j.dim);
+          j.payload = to_name(pl->items[1], "payload");
+        }
+      }
       if (j.len <= 0 || j.len > (1LL << 30)) throw PlanError("join len out of range for " + j.dim);
-      if (j.fks.size() != 1) throw PlanError("OR-joins over several fact keys are not supported on this path");
+      if (j.fks.size() > 4) throw PlanError("an OR-join takes at most 4 fact keys: " + j.dim);
+      if (j.gathers.size() > 8) throw PlanError("an MHT join publishes at most 8 columns: " + j.dim);
       p->steps.push_back(std::move(s));
     } else if (h == "aggregate") {
       if (have_agg) throw PlanError("two aggregates");
@@ -329,12 +340,21 @@ std::unique_ptr<Plan> parse_plan(const std::string& text) {
     seen_dims.insert(j.dim);
     std::set<std::string> dimcols(p->tables[dt].cols.begin(), p->tables[dt].cols.end());
     if (!dimcols.count(j.pk)) throw PlanError("pk '" + j.pk + "' is not a column of " + j.dim);
-    for (const auto& fk : j.fks)
+    for (size_t k = 0; k < j.fks.size(); ++k) {
+      const std::string& fk = j.fks[k];
       if (!visible.count(fk) || p->table_of_col[fk] != 0) throw PlanError("fk '" + fk + "' is not a fact column");
+      for (size_t q = 0; q < k; ++q)
+        if (j.fks[q] == fk) throw PlanError("fk '" + fk + "' listed twice in the OR-join with " + j.dim);
+    }
     if (j.filter) check(j.filter.get(), dimcols, "build filter of " + j.dim);
     if (!j.payload.empty()) {
       if (!dimcols.count(j.payload) || j.payload == j.pk) throw PlanError("bad payload column for " + j.dim);
       visible.insert(j.payload);
+    }
+    for (const auto& c : j.gathers) {
+      if (!dimcols.count(c)) throw PlanError("payload '" + c + "' is not a column of " + j.dim);
+      if (std::count(j.gathers.begin(), j.gathers.end(), c) != 1) throw PlanError("payload '" + c + "' listed twice");
+      visible.insert(c);
     }
   }
   for (const auto& g : p->groups) check(g.expr.get(), visible, "GROUP BY");

@@ -16,6 +16,9 @@
 //     (filter EXPR)
 //     (join DDATE (pk d_datekey) (fk lo_orderdate) (len 61131) (keymin 19920101)
 //           (filter EXPR) (payload d_year))
+//     (join CUSTOMER (pk c_custkey) (fk lo_custkey) (len N) (keymin N) (multi 1)
+//           (payload c_city c_nation))
+//     (join DDATE (pk d_datekey) (fk lo_orderdate lo_commitdate) ...)
 //     (aggregate (group EXPR (min 1992) (card 7) (nullable 0)) ... (sum EXPR) (count (star))
 //                (sparse 0)))
 // EXPR: (col NAME) (int N) (null) (star) (add|sub|mul|div E E)
@@ -68,7 +71,15 @@ struct Join {
   long long len = 0;               // PHT slots (HASH modulus)
   long long keymin = 0;            // HASH offset
   std::unique_ptr<Expr> filter;    // build-side predicate, may be null
-  std::string payload;             // PHT_2 payload column; empty => PHT_1
+  std::string payload;             // PHT_2 payload column; empty => PHT_1 (or MHT)
+  // Multi-value hash table (non-unique build key, visitor.cpp:3947-3968): the
+  // directory maps a key to the build row ids that carry it and every match
+  // expands the probe row; `gathers` are the build columns read by row id.
+  bool multi = false;
+  std::vector<std::string> gathers;
+  // A join whose probe can emit a row more than once: an MHT, or an OR over
+  // several fact keys (each distinct key probes, visitor.cpp:4566-4640).
+  bool expands() const { return multi || fks.size() > 1; }
 };
 
 struct Step {

@@ -114,6 +114,7 @@ struct LaunchPlan {
   std::vector<Ht> hts;
   std::map<int, uint64_t> htv_words;
   std::map<int, uint64_t> bm_words;
+  std::map<int, int> mht_table;                        // multi-value hash table slot -> build table slot
   uint64_t result_words = 0, groups = 1;
   int storage_ts = 1, visible_ts = 1, sparse = 0;
   uint64_t touched_words = 0;
@@ -193,6 +194,10 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       ls >> i >> sh.groups >> sh.ts >> sh.grouped >> sh.sparse >> sh.nlits >> sh.smem_ok >> sh.naggs >> sh.tw >> sh.nseen;
       if (i != (int)lp.sshapes.size()) { err = "shape lines out of order"; return false; }
       lp.sshapes.push_back(sh);
+    } else if (k == "mht") {
+      int sl = 0, t = 0;
+      ls >> sl >> t;
+      lp.mht_table[sl] = t;
     } else if (k == "bm") {
       int s; uint64_t w;
       ls >> s >> w;
@@ -261,6 +266,14 @@ ScratchLayout scratch_layout(const LaunchPlan& lp) {
   off = align256(off + 16);
   s.total = off;
   return s;
+}
+
+// Bytes of the row-id payloads of a plan's multi-value hash tables: one int
+// per build row, so they are sized when the row counts are known.
+uint64_t mht_payload_bytes(const LaunchPlan& lp, const std::vector<long long>& rows) {
+  uint64_t b = 0;
+  for (const auto& kv : lp.mht_table) b += align256((uint64_t)std::max<long long>(1, rows[kv.second]) * 4);
+  return b;
 }
 
 }  // namespace
@@ -624,9 +637,17 @@ int cx_ctx_set_column_range(cx_exec_ctx* c, const char* name, int64_t lo, int64_
 }
 
 int cx_module_scratch_bytes(const cx_module* m, const cx_exec_ctx* c, uint64_t* bytes) {
-  (void)c;
   if (!m || !bytes) return fail(CX_E_INVALID, "cx_module_scratch_bytes: NULL argument");
   *bytes = m->sl.total;
+  if (!m->lp.mht_table.empty() && c) {
+    std::vector<long long> rows(m->lp.tables.size(), 0);
+    for (size_t t = 0; t < m->lp.tables.size(); ++t) {
+      auto it = c->rows.find(m->lp.tables[t]);
+      if (it == c->rows.end()) return fail(CX_E_MISSING, "cx_module_scratch_bytes: row count of table %s is not set", m->lp.tables[t].c_str());
+      rows[t] = (long long)it->second;
+    }
+    *bytes += mht_payload_bytes(m->lp, rows);
+  }
   return CX_OK;
 }
 
@@ -689,22 +710,23 @@ int cx_execute_params(cx_module* m, cx_exec_ctx* c, const int32_t* params, int n
   rc = load_on_device(m, dev, &L);
   if (rc) return rc;
 
-  // Scratch.
+  // Scratch: the plan's fixed layout, then the MHT row-id payloads.
+  const uint64_t need = m->sl.total + mht_payload_bytes(lp, rows);
   char* scratch = nullptr;
   if (c->user_scratch) {
-    if (c->user_scratch_bytes < m->sl.total)
+    if (c->user_scratch_bytes < need)
       return fail(CX_E_CAPACITY, "cx_execute: caller scratch holds %llu bytes, query needs %llu",
-                  (unsigned long long)c->user_scratch_bytes, (unsigned long long)m->sl.total);
+                  (unsigned long long)c->user_scratch_bytes, (unsigned long long)need);
     scratch = (char*)c->user_scratch;
   } else {
-    if (c->own_scratch_bytes < m->sl.total) {
+    if (c->own_scratch_bytes < need) {
       if (c->own_scratch) {
         if (c->pending) cudaEventSynchronize(c->ev[3]);
         cudaFree(c->own_scratch);
         c->own_scratch = nullptr;
         c->own_scratch_bytes = 0;
       }
-      const uint64_t grow = m->sl.total + m->sl.total / 2;  // 1.5x high-water, as DynamicDeviceBuffer
+      const uint64_t grow = need + need / 2;  // 1.5x high-water, as DynamicDeviceBuffer
       CX_CUDA(cudaMalloc(&c->own_scratch, grow));
       c->own_scratch_bytes = grow;
     }
@@ -718,6 +740,13 @@ int cx_execute_params(cx_module* m, cx_exec_ctx* c, const int32_t* params, int n
   a.touched = (unsigned int*)(scratch + m->sl.touched_off);
   a.finalize_tmp = (unsigned long long*)(scratch + m->sl.fin_off);
   a.err = (unsigned int*)(scratch + m->sl.err_off);
+  {
+    uint64_t off = m->sl.total;
+    for (const auto& kv : lp.mht_table) {
+      a.mpay[kv.first] = (int*)(scratch + off);
+      off += align256((uint64_t)std::max<long long>(1, rows[kv.second]) * 4);
+    }
+  }
 
   int sms = c->sm_override;
   if (sms <= 0) CX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

@@ -243,7 +243,7 @@ int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Req
   cx_result_info info;
   cx_module_result_info(m, &info);
   uint64_t scratch = 0;
-  cx_module_scratch_bytes(m, nullptr, &scratch);
+  cx_module_scratch_bytes(m, s->tables, &scratch);
   r->words = std::max<uint64_t>(1, info.result_words);
   r->vwords = std::max<uint64_t>(1, info.validity_words);
   r->final_words = info.final_words;

@@ -29,11 +29,13 @@ DATE_DAYS = 2556  # 1992-01-01 .. 1998-12-30
 # Generator stream of every synthetic column (stable ids).
 STREAMS = {
     "lo_orderdate": 1, "lo_custkey": 2, "lo_suppkey": 3, "lo_partkey": 4, "lo_quantity": 5,
-    "lo_discount": 6, "lo_extendedprice": 7, "lo_revenue": 8, "lo_supplycost": 9,
+    "lo_discount": 6, "lo_extendedprice": 7, "lo_revenue": 8, "lo_supplycost": 9, "lo_commitdate": 10,
     "c_region": 20, "c_nation": 21, "c_city": 22,
     "s_region": 30, "s_nation": 31, "s_city": 32,
     "p_mfgr": 40, "p_category": 41, "p_brand1": 42,
+    "ps_partkey": 50, "ps_tier": 51, "ps_availqty": 52, "ps_supplycost": 53,
     "valid_lo_revenue": 100, "valid_c_city": 101, "valid_lo_quantity": 102, "valid_lo_discount": 103,
+    "valid_ps_tier": 104, "valid_lo_commitdate": 105,
 }
 
 # Uniform fact columns: (lo, hi) inclusive.
@@ -45,7 +47,8 @@ FACT_UNIFORM = {
     "lo_supplycost": (100, 10_000_000),
 }
 
-DIM_ROWS = {"CUSTOMER": 300_000, "SUPPLIER": 20_000, "PART": 200_000, "DDATE": DATE_DAYS}
+DIM_ROWS = {"CUSTOMER": 300_000, "SUPPLIER": 20_000, "PART": 200_000, "DDATE": DATE_DAYS, "PARTSUPP": 400_000}
+COMMIT_LAG_DAYS = 91  # lo_commitdate = lo_orderdate + 0..90 days (may run past the date table)
 
 
 def _splitmix64(z: np.ndarray) -> np.ndarray:
@@ -91,6 +94,19 @@ def datekeys(seed: int, stream: int, row0: int, rows: int) -> np.ndarray:
     return DATE_KEYS[idx]
 
 
+_EXT_DATES = [(_dt.date(1992, 1, 1) + _dt.timedelta(days=d)) for d in range(DATE_DAYS + COMMIT_LAG_DAYS)]
+EXT_DATE_KEYS = np.array([d.year * 10000 + d.month * 100 + d.day for d in _EXT_DATES], dtype=np.int32)
+
+
+def commitdates(seed: int, row0: int, rows: int) -> np.ndarray:
+    """lo_commitdate: the row's order date plus 0..90 days, so about one row
+    in 91 commits on its order date and the last 90 days of orders commit past
+    the date dimension."""
+    idx = below(hashes(seed, STREAMS["lo_orderdate"], row0, rows), DATE_DAYS).astype(np.int64)
+    lag = below(hashes(seed, STREAMS["lo_commitdate"], row0, rows), COMMIT_LAG_DAYS).astype(np.int64)
+    return EXT_DATE_KEYS[idx + lag]
+
+
 def validity_words(seed: int, stream: int, rows: int, null_permille: int) -> np.ndarray:
     """uint64 words, bit r = 1 when row r is valid (the reference's .valid64)."""
     nulls = below(hashes(seed, stream, 0, rows), 1000) < np.uint64(null_permille)
@@ -103,6 +119,8 @@ def fact_column(name: str, seed: int, row0: int, rows: int) -> np.ndarray:
     s = STREAMS[name]
     if name == "lo_orderdate":
         return datekeys(seed, s, row0, rows)
+    if name == "lo_commitdate":
+        return commitdates(seed, row0, rows)
     if name == "lo_custkey":
         return uniform(seed, s, 1, DIM_ROWS["CUSTOMER"], row0, rows)
     if name == "lo_suppkey":
@@ -118,6 +136,8 @@ def fact_column_device(name: str, seed: int, rows: int, out_ptr: int, stream: in
     from ._lib import check, lib
 
     s = STREAMS[name]
+    if name == "lo_commitdate":
+        raise ValueError("lo_commitdate has no device generator; load fact_column() output")
     if name == "lo_orderdate":
         check(lib.cx_gen_datekey(s, seed, DATE_DAYS, row0, rows, out_ptr, stream or None), "cx_gen_datekey")
         return
@@ -146,6 +166,15 @@ def dim_columns(table: str, seed: int) -> dict[str, np.ndarray]:
             "d_year": np.array([d.year for d in _DATES], dtype=np.int32),
             "d_month": np.array([d.month for d in _DATES], dtype=np.int32),
             "d_weeknum": np.array([(d.timetuple().tm_yday - 1) // 7 + 1 for d in _DATES], dtype=np.int32),
+        }
+    if table == "PARTSUPP":
+        # Non-unique key: part keys drawn with replacement (0..several rows per
+        # part, about 13.5% of parts have none).
+        return {
+            "ps_partkey": uniform(seed, STREAMS["ps_partkey"], 1, DIM_ROWS["PART"], 0, n),
+            "ps_tier": uniform(seed, STREAMS["ps_tier"], 0, 4, 0, n),
+            "ps_availqty": uniform(seed, STREAMS["ps_availqty"], 1, 9999, 0, n),
+            "ps_supplycost": uniform(seed, STREAMS["ps_supplycost"], 1, 1000, 0, n),
         }
     p = {"CUSTOMER": "c", "SUPPLIER": "s", "PART": "p"}[table]
     key = np.arange(1, n + 1, dtype=np.int32)
@@ -177,6 +206,9 @@ def ssb_tables(fact_rows: int, fact_cols: list[str] | None = None) -> dict[str, 
                           key_col="s_suppkey", key_min=1, key_max=DIM_ROWS["SUPPLIER"]),
         "PART": Table("PART", ["p_partkey", "p_mfgr", "p_category", "p_brand1"], DIM_ROWS["PART"],
                       key_col="p_partkey", key_min=1, key_max=DIM_ROWS["PART"]),
+        "PARTSUPP": Table("PARTSUPP", ["ps_partkey", "ps_tier", "ps_availqty", "ps_supplycost"],
+                          DIM_ROWS["PARTSUPP"], key_col="ps_partkey", key_min=1, key_max=DIM_ROWS["PART"],
+                          key_unique=False),
     }
 
 
@@ -187,7 +219,14 @@ GROUP_STATS = {
     "s_region": (0, 5), "s_nation": (0, 25), "s_city": (0, 250),
     "p_mfgr": (0, 5), "p_category": (0, 25), "p_brand1": (0, 1000),
     "lo_quantity": (1, 50), "lo_discount": (0, 11),
+    "ps_tier": (0, 5),
 }
+
+
+def dim_of_column(c: str) -> str:
+    if c.startswith("ps_"):
+        return "PARTSUPP"
+    return {"c": "CUSTOMER", "s": "SUPPLIER", "p": "PART", "d": "DDATE"}[c[0]]
 
 
 @dataclass
@@ -209,7 +248,6 @@ def host_tables(seed: int, fact_rows: int, fact_cols: list[str], nulls: dict[str
         cols.update(dim_columns(d, seed))
     validity: dict[str, np.ndarray] = {}
     for c, permille in (nulls or {}).items():
-        rows = fact_rows if c.startswith("lo_") else DIM_ROWS[{"c": "CUSTOMER", "s": "SUPPLIER", "p": "PART",
-                                                                "d": "DDATE"}[c[0]]]
+        rows = fact_rows if c.startswith("lo_") else DIM_ROWS[dim_of_column(c)]
         validity[c] = validity_words(seed, STREAMS["valid_" + c], rows, permille)
     return HostTables(seed, fact_rows, cols, validity)

@@ -168,6 +168,9 @@ class Database:
         torch = self.torch
         tables = datagen.ssb_tables(fact_rows, fact_cols)
         for c in fact_cols:
+            if c == "lo_commitdate":  # derived from the order date on the host
+                self.load_column("LINEORDER", c, datagen.fact_column(c, seed, 0, fact_rows))
+                continue
             t = torch.empty(fact_rows, dtype=torch.int32, device=self.device)
             datagen.fact_column_device(c, seed, fact_rows, t.data_ptr(), torch.cuda.current_stream().cuda_stream)
             self.load_column("LINEORDER", c, t)
@@ -179,8 +182,7 @@ class Database:
             self.set_rows(d, datagen.DIM_ROWS[d])
             self.tables[d] = tables[d]
         for c, permille in (nulls or {}).items():
-            rows = fact_rows if c.startswith("lo_") else datagen.DIM_ROWS[
-                {"c": "CUSTOMER", "s": "SUPPLIER", "p": "PART", "d": "DDATE"}[c[0]]]
+            rows = fact_rows if c.startswith("lo_") else datagen.DIM_ROWS[datagen.dim_of_column(c)]
             w = torch.empty((rows + 63) // 64, dtype=torch.int64, device=self.device)
             datagen.validity_device(c, seed, rows, permille, w.data_ptr(), torch.cuda.current_stream().cuda_stream)
             self.load_validity(c, w)
@@ -261,7 +263,7 @@ class Database:
         except _lib.CxError:
             return False
         for kind, s in plan.steps:
-            if kind == "join" and self.column_min(s.fk) <= 0:
+            if kind == "join" and (s.expands or self.column_min(s.fk) <= 0):
                 return False
         return True
 

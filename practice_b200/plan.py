@@ -123,6 +123,7 @@ class Table:
     key_col: str | None = None  # dimension key column (for generic build ranges)
     key_min: int = 0
     key_max: int = 0
+    key_unique: bool = True     # catalog: the key column holds each value at most once
 
 
 @dataclass
@@ -134,6 +135,17 @@ class Join:
     keymin: int
     filter: E | None = None
     payload: str | None = None
+    more_fks: tuple[str, ...] = ()   # further fact keys of an OR-join
+    multi: bool = False              # multi-value hash table (non-unique build key)
+    gathers: tuple[str, ...] = ()    # MHT: build columns read through the row id
+
+    @property
+    def fks(self) -> tuple[str, ...]:
+        return (self.fk,) + tuple(self.more_fks)
+
+    @property
+    def expands(self) -> bool:
+        return self.multi or len(self.more_fks) > 0
 
 
 @dataclass
@@ -176,10 +188,14 @@ class Plan:
                 out.append(f"  (filter {s.sexpr()})")
             else:
                 j: Join = s
-                parts = [f"(join {j.dim} (pk {j.pk}) (fk {j.fk}) (len {j.length}) (keymin {j.keymin})"]
+                parts = [f"(join {j.dim} (pk {j.pk}) (fk {' '.join(j.fks)}) (len {j.length}) (keymin {j.keymin})"]
+                if j.multi:
+                    parts.append(" (multi 1)")
                 if j.filter is not None:
                     parts.append(f" (filter {j.filter.sexpr()})")
-                if j.payload:
+                if j.multi and j.gathers:
+                    parts.append(f" (payload {' '.join(j.gathers)})")
+                elif j.payload:
                     parts.append(f" (payload {j.payload})")
                 out.append("  " + "".join(parts) + ")")
         agg = ["  (aggregate"]
@@ -223,7 +239,7 @@ class Plan:
             if kind == "filter":
                 add(s.columns())
             else:
-                add([s.fk])
+                add(list(s.fks))
         for g in self.groups:
             add(g.expr.columns())
         for a in self.aggs:
@@ -308,8 +324,12 @@ class PlanBuilder:
         self._steps.append(("filter", pred))
         return self
 
-    def join(self, dim: str, fk: str, pk: str | None = None, where: E | None = None,
+    def join(self, dim: str, fk: str | tuple[str, ...], pk: str | None = None, where: E | None = None,
              payload: str | None = None) -> "PlanBuilder":
+        """Joins a dimension.  `fk` may name several fact keys: the SQL form
+        `(fk1 = pk OR fk2 = pk)`, probed once per distinct key
+        (visitor.cpp:4587-4640).  A dimension whose key the catalog marks
+        non-unique becomes a multi-value hash table (:3947-3968)."""
         d = self.all_tables[dim]
         pk = pk or d.key_col or d.cols[0]
         self._pending_joins.append((len(self._steps), dim, pk, fk, where, payload))
@@ -343,10 +363,17 @@ class PlanBuilder:
             for kind, s in steps[idx + 1:]:
                 if kind == "filter":
                     later_filter_cols += s.columns()
-            if payload is None:
-                payload = choose_payload(d, pk, agg_cols, later_filter_cols)
+            fks = (fk,) if isinstance(fk, str) else tuple(fk)
             length, keymin = build_params(d)
-            steps[idx] = ("join", Join(dim, pk, fk, length, keymin, where, payload))
+            if not d.key_unique:
+                # MHT: the payload is the build row id, so every dimension column
+                # used above the join is read through it.
+                gathers = tuple(c for c in dict.fromkeys(agg_cols + later_filter_cols) if c in d.cols)
+                steps[idx] = ("join", Join(dim, pk, fks[0], length, keymin, where, None, fks[1:], True, gathers))
+            else:
+                if payload is None:
+                    payload = choose_payload(d, pk, agg_cols, later_filter_cols)
+                steps[idx] = ("join", Join(dim, pk, fks[0], length, keymin, where, payload, fks[1:]))
             used_tables.append(d)
         plan = Plan(tables=used_tables, nullable=set(self.nullable), steps=steps, groups=gl, aggs=al,
                     order_by=list(order_by or []), name=self.name)

@@ -13,6 +13,12 @@
   scalar SUM; T1 date join + GROUP BY year; T2 three joins + GROUP BY
   (nation, year); T3 four joins + GROUP BY (brand, year) (<= 7,000 groups).
 * ``kat_*`` -- the five queries of test/nullable_data/queries.sql.
+* ``or_join_year`` -- the OR-join over two fact keys of
+  test/queries/sql/custom1.sql: (lo_orderdate = d_datekey OR lo_commitdate =
+  d_datekey), year in [1992, 1997], GROUP BY d_year, SUM(revenue).
+* ``mht_*`` -- joins on PARTSUPP, whose key ps_partkey is non-unique, so each
+  fact row expands to every matching build row (multi-value hash table,
+  test/queries/sql/mht/non_unique_projection.sql semantics under an aggregate).
 """
 from __future__ import annotations
 
@@ -25,6 +31,8 @@ Q11_COLS = ["lo_orderdate", "lo_quantity", "lo_discount", "lo_extendedprice"]
 Q31_COLS = ["lo_orderdate", "lo_custkey", "lo_suppkey", "lo_partkey", "lo_revenue", "lo_supplycost"]
 BATCH_COLS = ["lo_orderdate", "lo_custkey", "lo_suppkey", "lo_partkey", "lo_quantity", "lo_discount",
            "lo_revenue", "lo_supplycost"]
+OR_COLS = ["lo_orderdate", "lo_commitdate", "lo_revenue"]
+MHT_COLS = ["lo_orderdate", "lo_suppkey", "lo_partkey", "lo_quantity", "lo_revenue"]
 
 
 def _g(name: str, nullable: bool = False) -> Group:
@@ -69,6 +77,63 @@ def ssb_q31_nullable(fact_rows: int = 60_000_000, region: int = 1, years: tuple[
 
 def ssb_q31_tables(fact_rows: int) -> dict[str, Table]:
     return ssb_tables(fact_rows, Q31_COLS)
+
+
+# --------------------------------------------------- OR-joins and MHT joins
+
+
+def or_join_year(fact_rows: int = 60_000_000, years: tuple[int, int] = (1992, 1997),
+                 nullable: tuple[str, ...] = ()) -> Plan:
+    t = ssb_tables(fact_rows, OR_COLS)
+    b = PlanBuilder(t, "LINEORDER", nullable=nullable, name="or_join_year")
+    b.join("DDATE", ("lo_orderdate", "lo_commitdate"),
+           where=and_(col("d_year").ge(years[0]), col("d_year").le(years[1])))
+    return b.aggregate([_g("d_year")], [("sum", col("lo_revenue"))])
+
+
+def or_join_then_filter(fact_rows: int = 60_000_000, month: int = 6) -> Plan:
+    """OR-join whose payload feeds a later fact-side filter and a grouped
+    MIN/MAX/AVG/COUNT over a nullable key (item-mode tail after the OR)."""
+    t = ssb_tables(fact_rows, OR_COLS)
+    b = PlanBuilder(t, "LINEORDER", nullable=("lo_revenue",), name="or_join_then_filter")
+    b.join("DDATE", ("lo_commitdate", "lo_orderdate"), payload="d_month")
+    b.filter(or_(col("d_month").le(month), col("lo_revenue").is_null()))
+    return b.aggregate([_g("d_month")], [("count", star()), ("min", col("lo_revenue")), ("max", col("lo_revenue")),
+                                         ("avg", col("lo_revenue"))])
+
+
+def mht_year_tier(fact_rows: int = 60_000_000, avail: int = 5000) -> Plan:
+    t = ssb_tables(fact_rows, MHT_COLS)
+    b = PlanBuilder(t, "LINEORDER", name="mht_year_tier")
+    b.join("DDATE", "lo_orderdate")
+    b.join("PARTSUPP", "lo_partkey", where=col("ps_availqty").lt(avail))
+    return b.aggregate([_g("d_year"), _g("ps_tier")], [("sum", col("lo_revenue")), ("count", star())])
+
+
+def mht_then_supplier(fact_rows: int = 60_000_000, region: int = 2, tier_max: int = 3) -> Plan:
+    """MHT first, a PHT join and a filter over a gathered column after it,
+    scalar SUM over a gathered column times a fact column."""
+    t = ssb_tables(fact_rows, MHT_COLS)
+    b = PlanBuilder(t, "LINEORDER", name="mht_then_supplier")
+    b.filter(col("lo_quantity").lt(40))
+    b.join("PARTSUPP", "lo_partkey")
+    b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(region))
+    b.filter(col("ps_tier").le(tier_max))
+    return b.aggregate([], [("sum", col("lo_quantity") * col("ps_supplycost")), ("count", star()),
+                            ("max", col("ps_availqty"))])
+
+
+def mht_brand(fact_rows: int = 60_000_000, nullable_tier: bool = False) -> Plan:
+    """MHT after two PHT joins, a large group domain (shared-memory or global
+    atomics in item mode) and optionally a nullable gathered group key."""
+    t = ssb_tables(fact_rows, MHT_COLS)
+    nullable = ("ps_tier",) if nullable_tier else ()
+    b = PlanBuilder(t, "LINEORDER", nullable=nullable, name="mht_brand")
+    b.join("PART", "lo_partkey", where=col("p_mfgr").le(1))
+    b.join("DDATE", "lo_orderdate")
+    b.join("PARTSUPP", "lo_partkey")
+    return b.aggregate([_g("p_brand1"), _g("d_year"), _g("ps_tier", nullable_tier)],
+                       [("sum", col("lo_revenue")), ("count", star())])
 
 
 # --------------------------------------------------------------- templates

@@ -36,6 +36,8 @@ def all_plans():
         plans[f"T{t}"] = queries.template(t, rng)
     for k, p in queries.kat_plans().items():
         plans["kat_" + k] = p
+    for name in ("or_join_year", "or_join_then_filter", "mht_year_tier", "mht_then_supplier", "mht_brand"):
+        plans[name] = getattr(queries, name)()
     return plans
 
 
@@ -48,7 +50,11 @@ def test_generated_source_compiles_for_sm100a(name):
     assert m.info.result_words == plan.group_slots * plan.storage_ts
     assert m.info.sparse == int(plan.sparse)
     if plan.steps and any(k == "join" for k, _ in plan.steps):
-        assert "BlockProbeAndPHT" in src and "build_hashtable_" in src
+        assert "BlockProbeAndPHT" in src or "ProbeMultiHT" in src or "pht_slot" in src
+        assert "build_hashtable_" in src or "mht_count_" in src
+    if any(k == "join" and s.multi for k, s in plan.steps):
+        for kern in ("mht_count_", "mht_blocksum_", "mht_blockscan_", "mht_offsets_", "mht_write_"):
+            assert kern in src
     assert "cp.async.bulk" not in src  # staging goes through the header helper
     assert "cx::bulk_g2s" in src
 

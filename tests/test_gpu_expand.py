@@ -1,0 +1,117 @@
+"""GPU parity of the joins that expand rows: OR-joins over several fact keys
+and multi-value hash tables (non-unique build keys), through the C ABI, against
+the CPU oracle on the same seeded tables.  Bit-exact on every word of the raw
+aggregate buffer and its validity bitmap."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import oracle
+from practice_b200 import _lib, datagen, queries
+from practice_b200.engine import make_tuning
+
+pytestmark = pytest.mark.gpu
+
+DIMS = dict(datagen.DIM_ROWS)
+ALL_COLS = sorted(set(queries.OR_COLS + queries.MHT_COLS))
+
+
+@pytest.fixture(scope="module")
+def db():
+    from practice_b200.engine import Database
+    return Database(0)
+
+
+def load(db, seed, n, nulls=None):
+    ht = datagen.host_tables(seed, n, ALL_COLS, nulls, dims=("DDATE", "SUPPLIER", "PART", "PARTSUPP"))
+    db.reset()
+    db.load_host_tables(ht, datagen.ssb_tables(n, ALL_COLS))
+    return ht
+
+
+def assert_parity(db, plan, ht, tuning=None):
+    ref = oracle.run_plan(plan.text(), ht.columns, ht.validity, {"LINEORDER": ht.fact_rows, **DIMS},
+                          plan.group_slots * plan.storage_ts)
+    got = db.execute(plan, tuning)
+    assert got.kernel_error == 0
+    fw = len(got.words)
+    np.testing.assert_array_equal(got.words, ref.words[:fw])
+    np.testing.assert_array_equal(got.validity, ref.validity[: (fw + 63) // 64])
+    return got
+
+
+@pytest.mark.parametrize("n", [2_000_000, 1_000_003, 33, 1])
+def test_or_join_year(db, n):
+    ht = load(db, 41, n)
+    got = assert_parity(db, queries.or_join_year(n), ht)
+    if n >= 1_000_000:
+        assert got.words[1] != 0
+    assert_parity(db, queries.or_join_year(n, (1995, 1998)), ht)
+
+
+def test_or_join_nullable_second_key_and_payload_filter(db):
+    n = 1_500_001
+    ht = load(db, 42, n, nulls={"lo_commitdate": 150, "lo_revenue": 80})
+    assert_parity(db, queries.or_join_year(n, nullable=("lo_commitdate",)), ht)
+    assert_parity(db, queries.or_join_then_filter(n), ht)
+
+
+@pytest.mark.parametrize("tuning", [None, dict(block_threads=256, items_per_thread=4, stages=2),
+                                    dict(block_threads=128, items_per_thread=8, stages=0)])
+def test_mht_year_tier(db, tuning):
+    n = 1_200_007
+    ht = load(db, 43, n)
+    t = make_tuning(**tuning) if tuning else None
+    for avail in (5000, 10_000, 1):
+        got = assert_parity(db, queries.mht_year_tier(n, avail), ht, t)
+        if avail == 1:
+            assert not got.words.any()
+
+
+def test_mht_then_pht_and_gathered_filter(db):
+    n = 1_000_001
+    ht = load(db, 44, n)
+    got = assert_parity(db, queries.mht_then_supplier(n), ht)
+    assert got.words[1] != 0
+
+
+@pytest.mark.parametrize("placement", [0, 2])
+def test_mht_large_group_domain(db, placement):
+    n = 1_000_000
+    ht = load(db, 45, n, nulls={"ps_tier": 100})
+    t = make_tuning(group_placement=placement)
+    assert_parity(db, queries.mht_brand(n), ht, t)
+    assert_parity(db, queries.mht_brand(n, nullable_tier=True), ht, t)
+
+
+@pytest.mark.parametrize("placement", [0, 1, 2])
+def test_group_placements_in_item_mode(db, placement):
+    """Register (or_join_year default), shared-memory and global group
+    tables, each updated per expanded row."""
+    n = 700_001
+    ht = load(db, 48, n, nulls={"lo_revenue": 60})
+    t = make_tuning(group_placement=placement)
+    for p in (queries.or_join_year(n), queries.or_join_then_filter(n), queries.mht_year_tier(n)):
+        assert_parity(db, p, ht, t)
+
+
+def test_mht_slot_collision_raises_a_kernel_error(db):
+    n = 100_000
+    ht = load(db, 46, n)
+    p = queries.mht_year_tier(n)
+    steps = [(k, dataclasses.replace(s, length=100_000) if k == "join" and s.multi else s) for k, s in p.steps]
+    got = db.execute(dataclasses.replace(p, steps=steps))
+    assert got.kernel_error == 4  # ERR_DIM_COLLISION
+    with pytest.raises(RuntimeError, match="collision"):
+        oracle.run_plan(dataclasses.replace(p, steps=steps).text(), ht.columns, ht.validity,
+                        {"LINEORDER": n, **DIMS}, p.group_slots * p.storage_ts)
+
+
+def test_expanding_plans_are_not_shared(db):
+    n = 1000
+    load(db, 47, n)
+    for p in (queries.or_join_year(n), queries.mht_year_tier(n)):
+        assert not db.shareable(p)
+        with pytest.raises(_lib.CxError):
+            _lib.shared_codegen([p.text()])

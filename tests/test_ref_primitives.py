@@ -39,3 +39,25 @@ def test_q11_and_q31_match_reference_primitives(tables):
         ref = refharness.run(p, ht.columns, DIMS, n)
         got = oracle.run_plan(p.text(), ht.columns, ht.validity, {"LINEORDER": n, **DIMS}, p.group_slots * p.storage_ts)
         np.testing.assert_array_equal(ref, got.words)
+
+
+@pytest.fixture(scope="module")
+def expand_tables():
+    n = 150_001
+    cols = sorted(set(queries.OR_COLS + queries.MHT_COLS))
+    return n, datagen.host_tables(22, n, cols, dims=("DDATE", "SUPPLIER", "PART", "PARTSUPP"))
+
+
+@pytest.mark.parametrize("make", [lambda n: queries.or_join_year(n), lambda n: queries.or_join_year(n, (1994, 1998)),
+                                  lambda n: queries.mht_year_tier(n), lambda n: queries.mht_year_tier(n, 300)])
+def test_or_joins_and_mht_match_reference_primitives(expand_tables, make):
+    """OR-join (two fact keys, duplicate keys skipped) and MHT row expansion:
+    the oracle against the reference's own BlockBuildMHT_Count/Write,
+    ProbeMultiHT and vector OR-join probes."""
+    n, ht = expand_tables
+    dims = {**DIMS, "PARTSUPP": datagen.DIM_ROWS["PARTSUPP"]}
+    p = make(n)
+    ref = refharness.run(p, ht.columns, dims, n)
+    got = oracle.run_plan(p.text(), ht.columns, ht.validity, {"LINEORDER": n, **dims}, p.group_slots * p.storage_ts)
+    np.testing.assert_array_equal(ref, got.words)
+    assert ref.any()

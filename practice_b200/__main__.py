@@ -5,8 +5,8 @@
     python -m practice_b200 shared ... --tuning block_threads=1024 items_per_thread=1 stages=3
 
 `shared` runs a mixed batch from the four query templates as one shared scan;
-`plain` runs one query (a template, or the SSB Q1.1 / Q3.1 shapes) as its own
-fused kernel.  Each repetition prints the device time of the scan kernel.
+`plain` runs one query (a template, the SSB Q1.1 / Q3.1 shapes, an OR-join or
+a multi-value hash join) as its own fused kernel.  Each repetition prints the device time of the scan kernel.
 Used for kernel profiles: every repetition launches the same kernels on the
 same resident tables.
 """
@@ -31,7 +31,8 @@ def main(argv: list[str] | None = None) -> None:
     ap.add_argument("mode", choices=["shared", "plain", "tour"])
     ap.add_argument("--rows", type=int, default=30_000_000)
     ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--query", default="T1", help="T0..T3, q11 or q31 (plain mode)")
+    ap.add_argument("--query", default="T1", help="T0..T3, q11, q31 or one of " + ", ".join(EXPANDING) +
+                    " (plain mode)")
     ap.add_argument("--template", type=int, default=-1, help="shared mode: draw every query from this template")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--reps", type=int, default=3)
@@ -46,8 +47,12 @@ def main(argv: list[str] | None = None) -> None:
         return
     kw, shared_default, make_tuning = _tuning(args.tuning)
     cols = {"q11": queries.Q11_COLS, "q31": queries.Q31_COLS}.get(args.query, queries.BATCH_COLS)
+    dims = ("DDATE", "CUSTOMER", "SUPPLIER", "PART")
+    if args.query in EXPANDING:
+        cols = sorted(set(queries.OR_COLS) | set(queries.MHT_COLS))
+        dims = dims + ("PARTSUPP",)
     db = Database(0)
-    db.generate_ssb(args.rows, args.seed, queries.BATCH_COLS if args.mode == "shared" else cols)
+    db.generate_ssb(args.rows, args.seed, queries.BATCH_COLS if args.mode == "shared" else cols, dims=dims)
     if args.mode == "shared":
         if args.template >= 0:
             rng = random.Random(args.seed)
@@ -65,19 +70,28 @@ def main(argv: list[str] | None = None) -> None:
         plan = queries.template(int(q[1:]), random.Random(args.seed), args.rows)
     elif q == "q11":
         plan = queries.ssb_q11(args.rows)
+    elif q in EXPANDING:
+        plan = getattr(queries, EXPANDING[q])(args.rows)
     else:
         plan = queries.ssb_q31(args.rows)
     t = make_tuning(**kw) if kw else None
     for _ in range(args.reps):
         r = db.execute(plan, t)
-        print(f"{plan.name}: scan {r.timing.scan_ms:.4f} ms, total {r.timing.total_ms:.4f} ms, "
-              f"kernel error {r.kernel_error}", flush=True)
+        print(f"{plan.name}: build {r.timing.build_ms:.4f} ms, scan {r.timing.scan_ms:.4f} ms, "
+              f"total {r.timing.total_ms:.4f} ms, kernel error {r.kernel_error}", flush=True)
+
+
+# Plain-mode names of the OR-join and multi-value hash join queries.
+EXPANDING = {"or_year": "or_join_year", "or_filter": "or_join_then_filter", "mht_tier": "mht_year_tier",
+             "mht_supp": "mht_then_supplier", "mht_brand": "mht_brand"}
+
 
 
 def tour(args) -> None:
     """Runs every kernel of the library once or twice on a generated table:
     the plain fused scan (Q1.1-, Q3.1- and nullable Q3.1-shaped queries, a
-    parametric one, AVG finalisation), a shared-scan batch, result
+    parametric one, AVG finalisation, an OR-join and a multi-value hash join
+    with its five build kernels), a shared-scan batch, result
     finalisation on the device and sparse compaction (both entry points)."""
     import numpy as np
 
@@ -85,15 +99,17 @@ def tour(args) -> None:
     from practice_b200.engine import SHARED_DEFAULT, Database, make_tuning
     from practice_b200.plan import PlanBuilder, col
 
-    cols = sorted(set(queries.BATCH_COLS) | set(queries.Q11_COLS))
+    cols = sorted(set(queries.BATCH_COLS) | set(queries.Q11_COLS) | set(queries.OR_COLS))
     db = Database(0)
-    db.generate_ssb(args.rows, args.seed, cols, nulls={"c_city": 50})
+    db.generate_ssb(args.rows, args.seed, cols, nulls={"c_city": 50},
+                    dims=("DDATE", "CUSTOMER", "SUPPLIER", "PART", "PARTSUPP"))
     torch = db.torch
     rng = random.Random(args.seed)
     plans = [queries.ssb_q11(args.rows), queries.ssb_q31(args.rows), queries.ssb_q31_nullable(args.rows)]
     b = PlanBuilder(queries.ssb_tables(args.rows, cols), "LINEORDER", name="avg")
     b.join("DDATE", "lo_orderdate")
     plans.append(b.aggregate([queries._g("d_year")], [("avg", col("lo_supplycost")), ("min", col("lo_quantity"))]))
+    plans += [queries.or_join_year(args.rows), queries.mht_year_tier(args.rows)]
     for p in plans:
         m = db.compile(p)
         res, val = db.alloc_result(m)

@@ -282,8 +282,11 @@ def config_block(args):
 # traffic of a launch grows with its rows.
 SHARED_DRAM_BYTES_PER_ROW = 974.231040e6 / 30e6
 
-PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=98304)
-                    for bt, ipt, st in ((1024, 2, 0), (1024, 4, 0), (512, 2, 0), (512, 8, 2), (1024, 4, 2))]
+PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=bm,
+                         prefetch=pf, group_placement=pl)
+                    for bt, ipt, st, bm, pf, pl in ((1024, 4, 0, 49152, 1, 0), (1024, 4, 0, 0, 1, 4),
+                                                    (512, 2, 0, 0, 1, 4), (1024, 2, 0, 0, 0, 4),
+                                                    (512, 8, 4, 0, 0, 0))]
 SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=2, producer_warps=pw)
                      for bt, ipt, st, pw in ((1024, 1, 3, 11), (1024, 1, 3, 17), (1024, 1, 3, 14), (512, 2, 2, 5),
                                              (512, 2, 2, 7))]

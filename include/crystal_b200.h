@@ -46,17 +46,24 @@ typedef struct cx_exec_ctx cx_exec_ctx; /* named device buffers + scratch + timi
 
 /* Launch shape for generated scan kernels (the autotuner's search space). */
 typedef struct cx_tuning {
-  int block_threads;     /* BLOCK_THREADS, multiple of 32 (default 256) */
+  int block_threads;     /* BLOCK_THREADS, multiple of 32 (default 1024) */
   int items_per_thread;  /* ITEMS_PER_THREAD (default 4) */
-  int stages;            /* TMA staging depth; 0 = read fact columns directly */
-  int ctas_per_sm;       /* persistent CTAs per SM (default 2) */
-  int group_placement;   /* 0 auto, 1 shared-memory group tables, 2 global atomics */
+  int stages;            /* TMA staging depth; 0 = read fact columns directly (default) */
+  int ctas_per_sm;       /* persistent CTAs per SM, capped by occupancy (default 16) */
+  int group_placement;   /* 0 auto, 1 shared-memory group tables, 2 global atomics, 3 register
+                          * accumulators (tiny domains), 4 per-thread shared-memory accumulators
+                          * (tiny domains; auto picks them when they fit the group budget) */
   int smem_group_budget; /* bytes a shared-memory group table may use */
-  int bitmap_budget;     /* bytes of shared memory for join membership bitmaps (0 = none) */
+  int bitmap_budget;     /* bytes of shared memory for exact join membership bitmaps (0 = none;
+                            default 48 KiB) */
   int group_merge;       /* 0 auto, 1 merge equal groups within a warp first, 2 per-lane atomics */
   int producer_warps;    /* shared scans: warps that build query masks (0 = 3/8 of the block) */
   int parametric;        /* plain kernels: 1 = integer literals become launch parameters
                             (one module per plan shape, literals passed to cx_execute_params) */
+  int prefetch;          /* unstaged plain scans (stages = 0): 0 = each column loaded where the
+                            pipeline first reads it, 1 = vector loads of every column at the tile
+                            start (default), 2 = as 1 with the next tile's loads issued a tile
+                            ahead */
 } cx_tuning;
 
 /* Shape of a compiled query's result buffer. */
@@ -180,7 +187,9 @@ int cx_plan_literals(const char* plan, size_t plan_len, int64_t* out, int cap, i
 /* Shared-scan program for `nshapes` plan shapes (one representative plan per
  * shape; its literals are ignored).  Same output contract as cx_codegen; fails
  * with CX_E_INVALID for shapes that cannot share a scan (nullable columns,
- * aggregates other than COUNT/SUM, conflicting joins). */
+ * aggregates other than COUNT/SUM, conflicting joins, OR-joins, multi-value
+ * hash joins).  A NULL tuning means 1024 threads, 1 row per thread, 3 staging
+ * stages, 1 CTA per SM. */
 int cx_shared_codegen(const char* const* plans, const size_t* plan_lens, int nshapes, const cx_tuning* tuning,
                       char* out, size_t out_cap, size_t* out_len);
 /* Enqueues one batch (<= 256 queries, <= 4096 parameters) of a compiled shared

@@ -65,9 +65,13 @@ template <int BT, int IPT>
 CX_DEVICE bool tile_is_full(int num_items) { return BT * IPT == num_items; }
 
 // Slot of `key` in a perfect hash table of `len` slots, or -1 when the slot
-// would fall outside the table.
+// would fall outside the table.  A key inside [key_min, key_min + len) is its
+// own offset (HASH's modulo is the identity there), so the division runs only
+// for keys outside that window.
 template <typename K>
 CX_DEVICE int pht_slot(K key, int len, K key_min) {
+  const K d = key - key_min;
+  if (d >= K(0) && d < K(len)) return (int)d;
   const int h = (int)HASH(key, len, key_min);
   return ((unsigned)h < (unsigned)len) ? h : -1;
 }
@@ -131,6 +135,38 @@ CX_DEVICE void BlockLoadValidity(const uint64_t* null_bitmap, int tid, long long
     const int local = i * BLOCK_THREADS + tid;
     valid[i] = (local < num_items) ? ColumnValidAt(null_bitmap, tile_offset + local) : 0;
   }
+}
+
+// Vector-striped tile layout (full warp tiles of 32 x IPT rows, no
+// reference counterpart): with VW = min(IPT, 4), item i of a lane holds row
+// (i / VW) * 32 * VW + lane * VW + i % VW, so each lane reads VW consecutive
+// rows with one vector load and a warp covers a contiguous segment per load.
+// Rows are loaded with the streaming cache hint (read once).
+template <int IPT>
+CX_DEVICE void WarpLoadTileV(const int* tile, int lane, int (&items)[IPT]) {
+  constexpr int VW = IPT >= 4 ? 4 : IPT;
+  static_assert(IPT % VW == 0, "items per thread must be 1, 2 or a multiple of 4");
+#pragma unroll
+  for (int v = 0; v < IPT / VW; ++v) {
+    const int* p = tile + v * 32 * VW + lane * VW;
+    if constexpr (VW == 4) {
+      asm("ld.global.cs.v4.s32 {%0, %1, %2, %3}, [%4];"
+          : "=r"(items[4 * v]), "=r"(items[4 * v + 1]), "=r"(items[4 * v + 2]), "=r"(items[4 * v + 3])
+          : "l"(p));
+    } else if constexpr (VW == 2) {
+      asm("ld.global.cs.v2.s32 {%0, %1}, [%2];" : "=r"(items[2 * v]), "=r"(items[2 * v + 1]) : "l"(p));
+    } else {
+      asm("ld.global.cs.s32 %0, [%1];" : "=r"(items[v]) : "l"(p));
+    }
+  }
+}
+// Validity bits in the same vector-striped layout.
+template <int IPT>
+CX_DEVICE void WarpLoadValidityV(const uint64_t* null_bitmap, int lane, long long tile_offset, int (&valid)[IPT]) {
+  constexpr int VW = IPT >= 4 ? 4 : IPT;
+#pragma unroll
+  for (int i = 0; i < IPT; ++i)
+    valid[i] = ColumnValidAt(null_bitmap, tile_offset + (i / VW) * 32 * VW + lane * VW + i % VW);
 }
 
 template <int BLOCK_THREADS, int ITEMS_PER_THREAD>
@@ -331,13 +367,23 @@ namespace cx_detail {
 template <typename K, typename V, int BT, int IPT, bool PAIR>
 CX_DEVICE void pht_probe(int tid, K (&items)[IPT], V* res, int (&flags)[IPT], const K* ht, int ht_len, K key_min,
                          int num_items, bool guarded) {
+  const bool pair8 = PAIR && sizeof(K) == 4 && (reinterpret_cast<unsigned long long>(ht) & 7ULL) == 0ULL;
   for_items<BT, IPT>(tid, num_items, guarded, [&](int i) {
     if (!flags[i]) return;
     const int h = pht_slot<K>(items[i], ht_len, key_min);
     if (h < 0) { flags[i] = 0; return; }
     if (PAIR) {
-      const K k = ht[(long long)h << 1];
-      if (k == items[i]) res[i] = static_cast<V>(ht[((long long)h << 1) + 1]);
+      K k, v;
+      if (pair8) {
+        // Key and payload of a slot are adjacent: one 8-byte load.
+        const int2 kv = *reinterpret_cast<const int2*>(ht + ((long long)h << 1));
+        k = (K)kv.x;
+        v = (K)kv.y;
+      } else {
+        k = ht[(long long)h << 1];
+        v = ht[((long long)h << 1) + 1];
+      }
+      if (k == items[i]) res[i] = static_cast<V>(v);
       else flags[i] = 0;
     } else {
       flags[i] = (ht[h] == items[i]) ? 1 : 0;
@@ -503,6 +549,65 @@ CX_DEVICE void BlockProbeBitmapAnd(int tid, K (&items)[ITEMS_PER_THREAD], int (&
     const bool occupied = (bitmap[h >> 5] >> (h & 31)) & 1u;
     flags[i] = (occupied || items[i] == K(0)) ? 1 : 0;
   });
+}
+
+// Exact membership from a slot bitmap in which bit h is set when slot h of a
+// finished PHT holds the key key_min + h.  For a key inside the window
+// [key_min, key_min + len) that bit is the probe's answer (HASH maps the key
+// to slot key - key_min), so no table access is needed; a key outside the
+// window falls back to the full probe of `ht` (`pair` = 1 for [key, payload]
+// slots).  Clears the flag of every item that misses; no branch for in-window
+// keys.  No counterpart in the reference API.
+template <typename K, int BLOCK_THREADS, int ITEMS_PER_THREAD>
+CX_DEVICE void BlockProbeExactBitmap(int tid, K (&items)[ITEMS_PER_THREAD], int (&flags)[ITEMS_PER_THREAD],
+                                     const unsigned int* bitmap, const K* ht, int pair, int ht_len, K key_min,
+                                     int num_items) {
+  const bool guarded = !cx_detail::tile_is_full<BLOCK_THREADS, ITEMS_PER_THREAD>(num_items);
+#pragma unroll
+  for (int i = 0; i < ITEMS_PER_THREAD; ++i) {
+    if (guarded && i * BLOCK_THREADS + tid >= num_items) continue;
+    const K d = items[i] - key_min;
+    int hit;
+    if (d >= K(0) && d < K(ht_len)) {
+      hit = (int)((bitmap[(unsigned)d >> 5] >> ((unsigned)d & 31u)) & 1u);
+    } else {
+      hit = 0;
+      if (flags[i]) {
+        const int h = cx_detail::pht_slot<K>(items[i], ht_len, key_min);
+        hit = (h >= 0 && ht[(long long)h << pair] == items[i]) ? 1 : 0;
+      }
+    }
+    flags[i] = (flags[i] && hit) ? 1 : 0;
+  }
+}
+
+// PHT_2 payload of every flagged item whose membership is already known (the
+// slot of its key holds the key): one table load per qualifying row.
+template <typename K, typename V, int BLOCK_THREADS, int ITEMS_PER_THREAD>
+CX_DEVICE void BlockFetchPayloadPHT_2(int tid, K (&items)[ITEMS_PER_THREAD], V (&res)[ITEMS_PER_THREAD],
+                                      int (&flags)[ITEMS_PER_THREAD], const K* ht, int ht_len, K key_min,
+                                      int num_items) {
+  cx_detail::for_items<BLOCK_THREADS, ITEMS_PER_THREAD>(
+      tid, num_items, !cx_detail::tile_is_full<BLOCK_THREADS, ITEMS_PER_THREAD>(num_items), [&](int i) {
+        if (!flags[i]) return;
+        const int h = cx_detail::pht_slot<K>(items[i], ht_len, key_min);
+        if (h >= 0) res[i] = static_cast<V>(ht[((long long)h << 1) + 1]);
+      });
+}
+// The same with the payload's validity bit (PHT_2V tables).
+template <typename K, typename V, int BLOCK_THREADS, int ITEMS_PER_THREAD>
+CX_DEVICE void BlockFetchPayloadPHT_2V(int tid, K (&items)[ITEMS_PER_THREAD], V (&res)[ITEMS_PER_THREAD],
+                                       int (&res_valid)[ITEMS_PER_THREAD], int (&flags)[ITEMS_PER_THREAD],
+                                       const K* ht, const unsigned int* ht_valid, int ht_len, K key_min,
+                                       int num_items) {
+  cx_detail::for_items<BLOCK_THREADS, ITEMS_PER_THREAD>(
+      tid, num_items, !cx_detail::tile_is_full<BLOCK_THREADS, ITEMS_PER_THREAD>(num_items), [&](int i) {
+        if (!flags[i]) return;
+        const int h = cx_detail::pht_slot<K>(items[i], ht_len, key_min);
+        if (h < 0) return;
+        res[i] = static_cast<V>(ht[((long long)h << 1) + 1]);
+        res_valid[i] = (int)((ht_valid[h >> 5] >> (h & 31)) & 1u);
+      });
 }
 
 // Push-model thread-local probes (join.h:258-274).

@@ -489,7 +489,11 @@ struct Emitter {
     o << "  }\n}\n\n";
   }
 
-  // Slot-occupancy bitmap of a built PHT: bit h is set when slot h holds a key.
+  // Exact-membership bitmap of a built PHT: bit h is set when slot h holds
+  // the key key_min + h, i.e. when a probe of that in-window key hits.
+  static bool exact_window_ok(const Join& j) {
+    return j.keymin >= -2147483648LL && j.keymin + j.len - 1 <= 2147483647LL;
+  }
   void emit_occupancy(const Join& j) {
     if (j.multi) return;
     const int h = ht_slot.at(j.dim);
@@ -504,7 +508,8 @@ struct Emitter {
     src << "  unsigned bits = 0u;\n";
     src << "  for (int b = 0; b < 32; ++b) {\n";
     src << "    const long long slot = w * 32 + b;\n";
-    src << "    if (slot < " << j.len << "LL && ht[slot" << (j.payload.empty() ? "" : " * 2") << "] != 0) bits |= 1u << b;\n";
+    src << "    if (slot < " << j.len << "LL && ht[slot" << (j.payload.empty() ? "" : " * 2") << "] == (int)(" << j.keymin
+        << "LL + slot)) bits |= 1u << b;\n";
     src << "  }\n";
     src << "  a.bm[" << h << "][w] = bits;\n";
     src << "}\n\n";
@@ -614,17 +619,18 @@ struct Emitter {
     const unsigned long long bars_off = off; off += (unsigned long long)NW * std::max(STAGES, 1) * 8;
     const unsigned long long red_off = off; off += (unsigned long long)NW * 8;
     // Join membership bitmaps kept in shared memory (in join order, while they fit the budget).
-    struct SBm { std::string dim, fk; int h; long long len, keymin; unsigned long long words, off; };
+    struct SBm { std::string dim, fk; int h; long long len, keymin; unsigned long long words, off; bool pair; };
     std::vector<SBm> sbms;
     {
       unsigned long long used = 0;
       for (const auto& s : p.steps) {
-        if (s.kind != Step::JoinStep || s.join.expands()) continue;
+        if (s.kind != Step::JoinStep || s.join.expands() || !exact_window_ok(s.join)) continue;
         const unsigned long long words = (unsigned long long)((s.join.len + 31) / 32);
         const unsigned long long bytes = ((words * 4) + 15) & ~15ULL;
         if (used + bytes > (unsigned long long)std::max(0, tu.bitmap_budget)) continue;
         off = (off + 15) & ~15ULL;
-        sbms.push_back({s.join.dim, s.join.fks[0], ht_slot.at(s.join.dim), s.join.len, s.join.keymin, words, off});
+        sbms.push_back({s.join.dim, s.join.fks[0], ht_slot.at(s.join.dim), s.join.len, s.join.keymin, words, off,
+                        !s.join.payload.empty()});
         off += bytes;
         used += bytes;
       }
@@ -633,11 +639,22 @@ struct Emitter {
     // Tiny group domains accumulate in registers for the whole kernel and are
     // reduced across the CTA once at the end (the reference's local group
     // reduce for <= 64 groups, visitor.cpp:2901-2982, without per-tile atomics).
-    const bool reg_groups = grouped && G <= 32 && G * NACC <= 16 &&
-                            (tu.group_placement == 0 || tu.group_placement == 3);
+    // Tiny domains live per thread: in shared-memory slots ([word][thread],
+    // conflict-free; one load-add-store per update) when they fit the group
+    // budget, else in registers selected by a compare chain over the groups.
+    const bool tiny = grouped && G <= 32 && G * NACC <= 16;
+    const bool lane_groups = tiny && (tu.group_placement == 4 ||
+                                      (tu.group_placement == 0 &&
+                                       G * NACC * 8ULL * CTA <= (unsigned long long)std::max(0, tu.smem_group_budget)));
+    const bool reg_groups = tiny && !lane_groups && (tu.group_placement == 0 || tu.group_placement == 3);
     int REP = 1;
     unsigned long long acc_off = 0, touch_off = 0, seen_off = 0;
-    if (grouped && !reg_groups) {
+    unsigned long long lacc_off = 0;
+    if (lane_groups) {
+      lacc_off = (off + 15) & ~15ULL;
+      off = lacc_off + G * NACC * 8ULL * CTA;
+    }
+    if (grouped && !reg_groups && !lane_groups) {
       const unsigned long long one = G * NACC * 8 + TW * 4 * (1 + NSEEN_T);
       if (tu.group_placement == 1) smem_groups = true;
       else if (tu.group_placement == 2) smem_groups = false;
@@ -655,7 +672,7 @@ struct Emitter {
 
     const std::string kname = "Scan_" + fact;
     meta << "kernel " << kname << " scan 0 " << CTA << " " << WT << " " << smem_total << " " << tu.ctas_per_sm << "\n";
-    if (grouped && !smem_groups && !reg_groups) meta << "touched " << TW << "\n";
+    if (grouped && !smem_groups && !reg_groups && !lane_groups) meta << "touched " << TW << "\n";
 
     std::vector<std::string> reg_cols = fact_cols;
     for (const auto& c : payload_cols) reg_cols.push_back(c);
@@ -705,6 +722,16 @@ struct Emitter {
         if (seen_idx[k] >= 0) o << "  unsigned long long seen_" << k << " = 0ULL;\n";
         if (p.aggs[k].fn == AggFn::Avg) o << "  unsigned long long cnt_" << k << " = 0ULL;\n";
       }
+    } else if (lane_groups) {
+      o << "  unsigned long long* s_lacc = (unsigned long long*)(cx_smem + " << lacc_off << ");\n";
+      for (unsigned long long w = 0; w < G * NACC; ++w) {
+        const int k = (int)(w % NACC);
+        o << "  s_lacc[" << w * CTA << "ULL + threadIdx.x] = " << (k < NA && p.aggs[k].fn == AggFn::Min ? "~0ULL" : "0ULL")
+          << ";\n";
+      }
+      o << "  unsigned rtouch = 0u;\n";
+      for (int k = 0; k < NA; ++k)
+        if (seen_idx[k] >= 0 && NSEEN_T > 0) o << "  unsigned rseen_" << k << " = 0u;\n";
     } else if (reg_groups) {
       o << "  unsigned long long racc[" << G * NACC << "];\n";
       o << "  #pragma unroll\n  for (int r = 0; r < " << G * NACC << "; ++r) racc[r] = 0ULL;\n";
@@ -772,6 +799,22 @@ struct Emitter {
       o << "  }\n";
     }
 
+    // Unstaged scans: every fact column of a full warp tile is read with
+    // vector loads (vector-striped rows) one tile ahead, so the next tile's
+    // loads are in flight while this one probes and aggregates.
+    const bool vec_pf = STAGES == 0 && NSC > 0 && (IPT == 1 || IPT == 2 || IPT % 4 == 0) && tu.prefetch > 0;
+    const bool ahead = vec_pf && tu.prefetch >= 2;
+    if (vec_pf) {
+      o << "  bool vec_ok = true;\n";
+      for (const auto& c : fact_cols) o << "  vec_ok = vec_ok && ((((unsigned long long)d_" << c << ") & 15ULL) == 0ULL);\n";
+    }
+    if (ahead) {
+      for (const auto& c : fact_cols) o << "  int pf_" << c << "[ITEMS_PER_THREAD];\n";
+      o << "  if (vec_ok && gwarp < full_tiles) {\n";
+      for (const auto& c : fact_cols)
+        o << "    WarpLoadTileV<ITEMS_PER_THREAD>(d_" << c << " + gwarp * TILE_SIZE, lane, pf_" << c << ");\n";
+      o << "  }\n";
+    }
     o << "  long long k_iter = 0;\n";
     o << "  bool aborted = false; (void)aborted;\n";
     o << "  for (long long t = gwarp; t < num_tiles; t += nwarps, ++k_iter) {\n";
@@ -793,15 +836,50 @@ struct Emitter {
     o << "    int flags[ITEMS_PER_THREAD];\n";
     declare_regs(o, reg_cols, "    ");
     o << "    InitFlags<BLOCK_THREADS, ITEMS_PER_THREAD>(flags);\n";
+    if (vec_pf) {
+      o << "    if (vec_ok && t < full_tiles) {\n";
+      if (ahead) {
+        o << "      #pragma unroll\n      for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+        for (const auto& c : fact_cols) o << "        " << c << "[i] = pf_" << c << "[i];\n";
+        o << "      }\n";
+        o << "      if (t + nwarps < full_tiles) {\n";
+        for (const auto& c : fact_cols)
+          o << "        WarpLoadTileV<ITEMS_PER_THREAD>(d_" << c << " + (t + nwarps) * TILE_SIZE, lane, pf_" << c << ");\n";
+        o << "      }\n";
+      } else {
+        for (const auto& c : fact_cols)
+          o << "      WarpLoadTileV<ITEMS_PER_THREAD>(d_" << c << " + tile_offset, lane, " << c << ");\n";
+      }
+      for (const auto& c : fact_cols)
+        if (nullable(c)) o << "      WarpLoadValidityV<ITEMS_PER_THREAD>(n_" << c << ", lane, tile_offset, " << c << "_valid);\n";
+      o << "    } else {\n";
+      for (const auto& c : fact_cols) {
+        o << "      BlockLoad<int, BLOCK_THREADS, ITEMS_PER_THREAD>(t_" << c << ", tid, tile_offset, " << c << ", num_tile_items);\n";
+        if (nullable(c))
+          o << "      BlockLoadValidity<BLOCK_THREADS, ITEMS_PER_THREAD>(n_" << c << ", tid, tile_offset, " << c
+            << "_valid, num_tile_items);\n";
+      }
+      o << "    }\n";
+      for (const auto& c : fact_cols) {
+        loaded.insert(c);
+        if (nullable(c)) valid_regs.insert(c);
+      }
+    }
 
     // Pipeline body: the reference's primitive calls, one warp tile at a time.
     const std::string ind = "    ";
-    // Membership of every bitmap-filtered join first (shared memory), so the
-    // L2 probes below only run for rows that qualify on all of them.
+    // Membership of every join with a shared-memory exact bitmap first: those
+    // joins need no table access at all for in-window keys, and the payload
+    // loads and L2 probes below only run for rows that qualify on all of them.
+    std::set<std::string> exact_dims;
     for (const auto& b : sbms) {
       ensure_loaded(o, b.fk, ind);
-      o << ind << "BlockProbeBitmapAnd<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << b.fk << ", flags, s_bm_"
-        << lower(b.dim) << ", " << b.len << ", " << b.keymin << ", num_tile_items);\n";
+      if (valid_regs.count(b.fk))
+        o << ind << "BlockApplyValidityAnd<BLOCK_THREADS, ITEMS_PER_THREAD>(tid, flags, " << b.fk << "_valid, num_tile_items);\n";
+      o << ind << "BlockProbeExactBitmap<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << b.fk << ", flags, s_bm_"
+        << lower(b.dim) << ", " << ht_name(b.dim) << ", " << (b.pair ? 1 : 0) << ", " << b.len << ", " << b.keymin
+        << ", num_tile_items);\n";
+      exact_dims.insert(b.dim);
     }
     for (size_t k = 0; k < xs; ++k) {
       const Step& s = p.steps[k];
@@ -812,6 +890,21 @@ struct Emitter {
       const Join& j = s.join;
       const std::string& fk = j.fks[0];
       ensure_loaded(o, fk, ind);
+      if (exact_dims.count(j.dim)) {
+        // Membership is settled; fetch the payload of qualifying rows.
+        if (j.payload.empty()) continue;
+        if (payload_valid.count(j.payload)) {
+          o << ind << "BlockFetchPayloadPHT_2V<int, int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << fk << ", " << j.payload
+            << ", " << j.payload << "_valid, flags, " << ht_name(j.dim) << ", " << ht_name(j.dim) << "_valid, " << j.len
+            << ", " << j.keymin << ", num_tile_items);\n";
+          valid_regs.insert(j.payload);
+        } else {
+          o << ind << "BlockFetchPayloadPHT_2<int, int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << fk << ", " << j.payload
+            << ", flags, " << ht_name(j.dim) << ", " << j.len << ", " << j.keymin << ", num_tile_items);\n";
+        }
+        loaded.insert(j.payload);
+        continue;
+      }
       if (valid_regs.count(fk))
         o << ind << "BlockApplyValidityAnd<BLOCK_THREADS, ITEMS_PER_THREAD>(tid, flags, " << fk << "_valid, num_tile_items);\n";
       if (j.payload.empty()) {
@@ -860,8 +953,10 @@ struct Emitter {
         dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " +
                std::to_string(eff_card(k)) + "u";
       }
-      o << ii << "const int hash = (" << horner << ") % " << G << ";\n";
-      o << ii << "if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+      // Keys inside their domains give a Horner value below G, where the
+      // reference's `% G` is the identity; only an out-of-domain key pays for it.
+      o << ii << "int hash = " << horner << ";\n";
+      o << ii << "if (!(" << dom << ")) { cx::raise(a.err, cx::ERR_GROUP_DOMAIN); hash = hash % " << G << "; }\n";
     };
     // Tiny group domains: register accumulators selected by a compare chain.
     auto reg_update = [&](const std::string& ii) {
@@ -879,6 +974,25 @@ struct Emitter {
         else o << ii << "    " << r << " += x_;\n";
         if (ag.fn == AggFn::Avg) o << ii << "    racc[g * " << NACC << " + " << avg_idx[k] << "] += 1ULL;\n";
         o << ii << "  }\n";
+        if (seen_idx[k] >= 0 && NSEEN_T > 0) o << ii << "  rseen_" << k << " |= 1u << hash;\n";
+        o << ii << "}\n";
+      }
+    };
+    auto lane_update = [&](const std::string& ii) {
+      o << ii << "rtouch |= 1u << hash;\n";
+      for (int k = 0; k < NA; ++k) {
+        const Agg& ag = p.aggs[k];
+        const std::string v = ag.arg->op == Op::Star ? "1" : valid_of(ag.arg.get());
+        const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + math_push(ag.arg.get(), true) + ")";
+        const std::string r = "s_lacc[((unsigned)hash * " + std::to_string(NACC) + "u + " + std::to_string(k) + "u) * " +
+                              std::to_string(CTA) + "u + threadIdx.x]";
+        o << ii << "if (" << v << ") {\n";
+        o << ii << "  const unsigned long long x_ = " << x << ";\n";
+        if (ag.fn == AggFn::Min) o << ii << "  if (x_ < " << r << ") " << r << " = x_;\n";
+        else if (ag.fn == AggFn::Max) o << ii << "  if (x_ > " << r << ") " << r << " = x_;\n";
+        else o << ii << "  " << r << " += x_;\n";
+        if (ag.fn == AggFn::Avg)
+          o << ii << "  s_lacc[((unsigned)hash * " << NACC << "u + " << avg_idx[k] << "u) * " << CTA << "u + threadIdx.x] += 1ULL;\n";
         if (seen_idx[k] >= 0 && NSEEN_T > 0) o << ii << "  rseen_" << k << " |= 1u << hash;\n";
         o << ii << "}\n";
       }
@@ -922,6 +1036,7 @@ struct Emitter {
       group_hash(ii + "  ");
       o << ii << "  if ((unsigned)hash < " << G << "u) {\n";
       if (reg_groups) reg_update(ii + "    ");
+      else if (lane_groups) lane_update(ii + "    ");
       else atomic_update(ii + "    ");
       o << ii << "  }\n" << ii << "}\n";
     };
@@ -1019,12 +1134,13 @@ struct Emitter {
       o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
       scalar_update(ind + "    ");
       o << ind << "  }\n" << ind << "}\n";
-    } else if (reg_groups) {
+    } else if (reg_groups || lane_groups) {
       o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
       o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
       group_hash(ind + "    ");
       o << ind << "    if ((unsigned)hash < " << G << "u) {\n";
-      reg_update(ind + "      ");
+      if (reg_groups) reg_update(ind + "      ");
+      else lane_update(ind + "      ");
       o << ind << "    }\n";
       o << ind << "  }\n";
       o << ind << "}\n";
@@ -1040,8 +1156,8 @@ struct Emitter {
         dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " +
                std::to_string(eff_card(k)) + "u";
       }
-      o << ind << "    hash = (" << horner << ") % " << G << ";\n";
-      o << ind << "    if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+      o << ind << "    hash = " << horner << ";\n";
+      o << ind << "    if (!(" << dom << ")) { cx::raise(a.err, cx::ERR_GROUP_DOMAIN); hash = hash % " << G << "; }\n";
       o << ind << "    if ((unsigned)hash >= " << G << "u) act = false;\n";
       o << ind << "  }\n";
       // Warp-uniform skip when no lane of the warp aggregates this item; else
@@ -1152,7 +1268,7 @@ struct Emitter {
         }
         o << "  }\n";
       }
-    } else if (reg_groups) {
+    } else if (reg_groups || lane_groups) {
       o << "  const unsigned touch_all = cx::block_or_u32<" << CTA << ">(rtouch, red);\n";
       for (int k = 0; k < NA; ++k)
         if (seen_idx[k] >= 0 && NSEEN_T > 0)
@@ -1161,7 +1277,10 @@ struct Emitter {
       o << "    unsigned long long v_[" << NACC << "];\n";
       o << "    #pragma unroll\n    for (int k = 0; k < " << NACC << "; ++k) {\n";
       o << "      unsigned long long x_ = 0ULL;\n";
-      o << "      #pragma unroll\n      for (int h = 0; h < " << G << "; ++h) if (h == g) x_ = racc[h * " << NACC << " + k];\n";
+      if (lane_groups)
+        o << "      x_ = s_lacc[((unsigned)g * " << NACC << "u + (unsigned)k) * " << CTA << "u + threadIdx.x];\n";
+      else
+        o << "      #pragma unroll\n      for (int h = 0; h < " << G << "; ++h) if (h == g) x_ = racc[h * " << NACC << " + k];\n";
       o << "      v_[k] = x_;\n";
       o << "    }\n";
       for (int k = 0; k < NACC; ++k) {
@@ -1231,7 +1350,7 @@ struct Emitter {
     if (STAGES > 0) o << "#undef CX_ISSUE\n";
     o << "\n";
 
-    if (grouped && !smem_groups && !reg_groups) {
+    if (grouped && !smem_groups && !reg_groups && !lane_groups) {
       meta << "kernel group_keys_epilogue groups 0 256 0\n";
       o << "extern \"C\" __global__ void __launch_bounds__(256) group_keys_epilogue(const CxArgs a) {\n";
       o << "  unsigned long long* d_result = a.result;\n";

@@ -11,17 +11,21 @@ namespace cx {
 // Launch shape of the generated fact-scan kernel.  The autotuner searches this
 // space per query shape; defaults are the measured best general setting.
 struct Tuning {
-  int block_threads = 256;     // BLOCK_THREADS (multiple of 32, <= 1024)
+  int block_threads = 1024;    // BLOCK_THREADS (multiple of 32, <= 1024)
   int items_per_thread = 4;    // ITEMS_PER_THREAD
-  int stages = 4;              // TMA staging ring depth (0 disables staging)
-  int ctas_per_sm = 2;         // persistent grid = SMs x this (occupancy-capped)
-  int group_placement = 0;     // 0 auto, 1 shared-memory tables, 2 global atomics
+  int stages = 0;              // TMA staging ring depth (0 disables staging)
+  int ctas_per_sm = 16;        // persistent grid = SMs x this (occupancy-capped)
+  int group_placement = 0;     // 0 auto, 1 shared-memory tables, 2 global atomics, 3 registers,
+                               // 4 per-thread shared-memory tables (<= 16 words per thread)
   int smem_group_budget = 96 * 1024;  // bytes of shared memory a group table may use
-  int bitmap_budget = 96 * 1024;      // bytes of shared memory for join membership bitmaps
+  int bitmap_budget = 48 * 1024;      // bytes of shared memory for join membership bitmaps
   int group_merge = 0;         // 0 auto, 1 warp match-merge, 2 direct per-lane atomics
   int wait_limit_log2 = 24;    // mbarrier poll limit before a wait gives up
   int producer_warps = 0;      // shared scans: warps that build query masks (0 = 3/8 of the block)
   int parametric = 0;          // plain kernels: literals read from CxArgs.lits at run time
+  int prefetch = 1;            // unstaged plain scans: 0 columns loaded where first used,
+                               // 1 vector loads of every column at the tile start,
+                               // 2 as 1 and the next tile's loads issued one tile ahead
 };
 
 // Returns the CUDA source for `plan` with its launch plan embedded as a

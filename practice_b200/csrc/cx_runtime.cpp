@@ -412,6 +412,7 @@ cx::Tuning to_tuning(const cx_tuning* tuning) {
     t.group_merge = tuning->group_merge;
     t.producer_warps = tuning->producer_warps;
     t.parametric = tuning->parametric;
+    t.prefetch = tuning->prefetch;
   }
   return t;
 }
@@ -459,6 +460,7 @@ void cx_tuning_default(cx_tuning* t) {
   t->group_merge = d.group_merge;
   t->producer_warps = d.producer_warps;
   t->parametric = d.parametric;
+  t->prefetch = d.prefetch;
 }
 
 int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap, size_t* out_len) {
@@ -840,7 +842,15 @@ int cx_shared_codegen(const char* const* plans, const size_t* lens, int nshapes,
       owned.push_back(cx::parse_plan(std::string(plans[i], lens[i])));
       shapes.push_back(owned.back().get());
     }
-    const cx::Tuning t = cx_internal::to_tuning(tuning);
+    cx::Tuning t = cx_internal::to_tuning(tuning);
+    if (!tuning) {
+      // Shared scans default to one 32-warp CTA per SM, one row per thread
+      // and a 3-deep staging ring.
+      t.block_threads = 1024;
+      t.items_per_thread = 1;
+      t.stages = 3;
+      t.ctas_per_sm = 1;
+    }
     const std::string src = cx::generate_shared_cuda(shapes, t);
     if (out_len) *out_len = src.size();
     if (out && out_cap) {

@@ -50,13 +50,16 @@ def test_generated_source_compiles_for_sm100a(name):
     assert m.info.result_words == plan.group_slots * plan.storage_ts
     assert m.info.sparse == int(plan.sparse)
     if plan.steps and any(k == "join" for k, _ in plan.steps):
-        assert "BlockProbeAndPHT" in src or "ProbeMultiHT" in src or "pht_slot" in src
+        assert any(k in src for k in ("BlockProbeAndPHT", "BlockProbeExactBitmap", "ProbeMultiHT", "pht_slot"))
         assert "build_hashtable_" in src or "mht_count_" in src
     if any(k == "join" and s.multi for k, s in plan.steps):
         for kern in ("mht_count_", "mht_blocksum_", "mht_blockscan_", "mht_offsets_", "mht_write_"):
             assert kern in src
     assert "cp.async.bulk" not in src  # staging goes through the header helper
-    assert "cx::bulk_g2s" in src
+    assert "WarpLoadTileV" in src      # default: unstaged vector loads
+    t = _lib.default_tuning()
+    t.block_threads, t.stages = 256, 3
+    assert "cx::bulk_g2s" in _lib.codegen(plan.text(), t)
 
 
 @pytest.mark.parametrize("bt,ipt,stages,place", [(128, 4, 4, 0), (256, 8, 2, 0), (512, 2, 3, 2), (256, 4, 0, 1),

@@ -361,3 +361,37 @@ def test_parametric_plain_kernel_nullable_shape(db):
         fw = len(got.words)
         np.testing.assert_array_equal(got.words, ref.words[:fw])
         np.testing.assert_array_equal(got.validity, ref.validity[: (fw + 63) // 64])
+
+
+@pytest.mark.parametrize("budget", [0, 98304])
+@pytest.mark.parametrize("nullable_payload", [False, True])
+def test_join_keys_outside_the_slot_window(db, budget, nullable_payload):
+    """Foreign keys below the hash window, past it (aliasing into a slot that
+    holds another key), equal to 0, the largest dimension key (which HASH maps
+    to slot 0) and the int32 extremes: the exact shared-memory bitmaps must
+    answer like the full probe (budget 98304) and like no bitmaps (0)."""
+    n = 300_007
+    ht = load(db, 23, n, queries.Q31_COLS, nulls={"c_city": 70} if nullable_payload else None)
+    rng = np.random.default_rng(5)
+    odd_cust = np.array([0, -1, 300_000, 300_001, 600_000, 2**31 - 1, -2**31], dtype=np.int64)
+    odd_date = np.array([0, 19_920_100, 19_920_101 + 61_131, 19_920_101 + 61_131 + 366, 19_981_231, 2**31 - 1,
+                         -2**31, 19_920_101 - 61_131 + 5], dtype=np.int64)
+    cust = ht.columns["lo_custkey"].copy()
+    date = ht.columns["lo_orderdate"].copy()
+    pick = rng.choice(n, 4000, replace=False)
+    cust[pick[:2000]] = odd_cust[rng.integers(0, len(odd_cust), 2000)].astype(np.int32)
+    date[pick[2000:]] = odd_date[rng.integers(0, len(odd_date), 2000)].astype(np.int32)
+    ht.columns["lo_custkey"], ht.columns["lo_orderdate"] = cust, date
+    db.load_column("LINEORDER", "lo_custkey", cust)
+    db.load_column("LINEORDER", "lo_orderdate", date)
+    tabs = datagen.ssb_tables(n, queries.Q31_COLS)
+    nullable = {"c_city"} if nullable_payload else set()
+    b = PlanBuilder(tabs, "LINEORDER", nullable=nullable)
+    b.join("CUSTOMER", "lo_custkey", where=col("c_region").le(3), payload="c_city")
+    b.join("DDATE", "lo_orderdate", where=col("d_year").ge(1993))
+    b.join("SUPPLIER", "lo_suppkey")
+    plan = b.aggregate([Group(col("c_city"), 0, 250, nullable_payload), queries._g("d_year")],
+                       [("count", star()), ("sum", col("lo_revenue"))])
+    from practice_b200.engine import make_tuning
+    for ipt, stages in ((4, 0), (2, 2)):
+        assert_parity(db, plan, ht, make_tuning(items_per_thread=ipt, stages=stages, bitmap_budget=budget))

@@ -2148,6 +2148,7 @@ struct SharedGen {
     o << "        }\n";
     o << "      }\n";
     for (size_t di = 0; di < dims.size(); ++di) o << "      int4 g" << di << "_[" << RB << "];\n";
+    for (size_t di = 0; di < dims.size(); ++di) o << "      int k" << di << "_[" << RB << "];\n";
     o << "      #pragma unroll\n";
     o << "      for (int j = 0; j < " << RB << "; ++j) {\n";
     o << "        const int i = ((b0_ + j * NPW) << 5) + lane;\n";
@@ -2157,8 +2158,9 @@ struct SharedGen {
       o << "        {\n";
       o << "          g" << di << "_[j] = make_int4(0, 0, 0, 0);\n";
       o << "          const int fk_ = live_ ? S_" << d.fk << "[i] : 0;\n";
-      o << "          const int h_ = (int)HASH(fk_, " << d.len << ", " << d.keymin << ");\n";
-      o << "          if (live_ && (unsigned)h_ < " << d.len << "u) g" << di << "_[j] = __ldg(&dkm_" << lower(d.name) << "[h_]);\n";
+      o << "          k" << di << "_[j] = fk_;\n";
+      o << "          const int h_ = cx_detail::pht_slot<int>(fk_, " << d.len << ", " << d.keymin << ");\n";
+      o << "          if (live_ && h_ >= 0) g" << di << "_[j] = __ldg(&dkm_" << lower(d.name) << "[h_]);\n";
       o << "        }\n";
     }
     o << "      }\n";
@@ -2175,12 +2177,12 @@ struct SharedGen {
       const std::string dn = lower(d.name);
       o << "          {\n";
       o << "            const int4 g_ = g" << di << "_[j];\n";
-      o << "            const bool hit_ = g_.x != 0 && g_.x == S_" << d.fk << "[i];\n";
+      o << "            const bool hit_ = g_.x != 0 && g_.x == k" << di << "_[j];\n";
       o << "            m &= hit_ ? (((unsigned long long)(unsigned)g_.z << 32) | (unsigned)g_.y) : s_nj[" << di << "];\n";
       if (!d.attrs.empty()) o << "            S_" << d.attrs[0] << "[i] = g_.w;\n";
       if (d.attrs.size() > 1) {
         o << "            int4 a_ = make_int4(0, 0, 0, 0);\n";
-        o << "            if (hit_) a_ = __ldg(&dat_" << dn << "[(int)HASH(S_" << d.fk << "[i], " << d.len << ", " << d.keymin << ")]);\n";
+        o << "            if (hit_) a_ = __ldg(&dat_" << dn << "[cx_detail::pht_slot<int>(k" << di << "_[j], " << d.len << ", " << d.keymin << ")]);\n";
         for (size_t k = 1; k < d.attrs.size(); ++k) o << "            S_" << d.attrs[k] << "[i] = a_." << comp[k - 1] << ";\n";
       }
       o << "          }\n";
@@ -2230,8 +2232,8 @@ struct SharedGen {
         horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(e.eff_card(k)) + " + gt" + std::to_string(k) + ")";
         dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " + std::to_string(e.eff_card(k)) + "u";
       }
-      o << "            const int hash = (" << horner << ") % " << G << ";\n";
       o << "            bad_ = !(" << dom << ");\n";
+      o << "            const int hash = bad_ ? (" << horner << ") % " << G << " : (" << horner << ");\n";
       o << "            h_ = (unsigned)hash < " << G << "u ? hash : " << G << ";\n";
       o << "          }\n";
       o << "          unsigned gw_ = 0u;\n";
@@ -2417,8 +2419,8 @@ struct SharedGen {
             if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "unsigned tseen" << k << " = 0u;\n";
           o << loop_open;
           o << terms.str();
-          o << ind << "  const int hash = (" << horner << ") % " << G << ";\n";
-          o << ind << "  if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+          o << ind << "  int hash = " << horner << ";\n";
+          o << ind << "  if (!(" << dom << ")) { cx::raise(a.err, cx::ERR_GROUP_DOMAIN); hash = hash % " << G << "; }\n";
           o << ind << "  if ((unsigned)hash >= " << G << "u) continue;\n";
           o << ind << "  ttouch |= 1u << hash;\n";
           for (int k = 0; k < NA; ++k) {
@@ -2448,8 +2450,8 @@ struct SharedGen {
         }
         o << loop_open;
         o << terms.str();
-        o << ind << "  const int hash = (" << horner << ") % " << G << ";\n";
-        o << ind << "  if (!(" << dom << ")) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+        o << ind << "  int hash = " << horner << ";\n";
+        o << ind << "  if (!(" << dom << ")) { cx::raise(a.err, cx::ERR_GROUP_DOMAIN); hash = hash % " << G << "; }\n";
         o << ind << "  if ((unsigned)hash >= " << G << "u) continue;\n";
         if (tiny) {
           o << ind << "  ttouch |= 1u << hash;\n";

@@ -3,7 +3,6 @@ arrive, admitted against an HBM budget and fused into shared-scan launches,
 must each return exactly what the query returns alone (its plain kernel) and
 what the CPU oracle returns."""
 import random
-import time
 
 import numpy as np
 import pytest
@@ -59,23 +58,20 @@ def check(srv, db, rid, plan, ht, alone=True):
 
 
 def test_server_stream_results_equal_alone_and_oracle(db):
-    n = 400_009
+    n = 4_000_037
     ht = load(db, 51, n)
     rng = random.Random(5)
     plans = [queries.template(rng.randrange(4), rng, n) for _ in range(48)]
     plans += [avg_plan(n, 1994)] * 3
     random.Random(6).shuffle(plans)
-    # Small tables run fast, so let two waiting queries form a shared launch.
-    srv = _lib.Server(db.ctx, _lib.server_config(max_batch=16, slots=2, min_shared_batch=2))
+    # One launch in flight: queries submitted while it runs wait together, so
+    # two or more waiting queries form a shared launch.
+    srv = _lib.Server(db.ctx, _lib.server_config(max_batch=16, slots=1, min_shared_batch=2))
     try:
         for t in range(4):  # compile the four shapes and the AVG kernel before the stream
             srv.prepare(queries.template(t, random.Random(t), n).text())
         srv.prepare(plans[[p.name for p in plans].index("avg")].text())
-        ids = []
-        for i, p in enumerate(plans):
-            ids.append(srv.submit(p.text()))
-            if i % 6 == 5:
-                time.sleep(0.003)  # later arrivals join while launches run
+        ids = [srv.submit(p.text()) for p in plans]
         infos = [check(srv, db, rid, p, ht) for rid, p in zip(ids, plans)]
         st = srv.stats()
         assert st.completed == len(plans) and st.rejected == 0

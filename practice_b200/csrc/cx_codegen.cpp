@@ -2448,12 +2448,12 @@ struct SharedGen {
           for (int k = 0; k < NA; ++k)
             if (!p.sparse && p.aggs[k].fn == AggFn::Sum) o << ind << "unsigned tseen" << k << " = 0u;\n";
         }
-        o << loop_open;
-        o << terms.str();
-        o << ind << "  int hash = " << horner << ";\n";
-        o << ind << "  if (!(" << dom << ")) { cx::raise(a.err, cx::ERR_GROUP_DOMAIN); hash = hash % " << G << "; }\n";
-        o << ind << "  if ((unsigned)hash >= " << G << "u) continue;\n";
         if (tiny) {
+          o << loop_open;
+          o << terms.str();
+          o << ind << "  int hash = " << horner << ";\n";
+          o << ind << "  if (!(" << dom << ")) { cx::raise(a.err, cx::ERR_GROUP_DOMAIN); hash = hash % " << G << "; }\n";
+          o << ind << "  if ((unsigned)hash >= " << G << "u) continue;\n";
           o << ind << "  ttouch |= 1u << hash;\n";
           for (int k = 0; k < NA; ++k) {
             const Agg& ag = p.aggs[k];
@@ -2467,31 +2467,64 @@ struct SharedGen {
           tiny_flush();
           if (tu.group_merge == 2) o << ind << "}\n";
         } else {
-          // Direct per-row updates: shared-memory table when the query has one, else global atomics.
-          o << ind << "  if (qtab) {\n";
-          o << ind << "    atomicOr(&qbits[hash >> 5], 1u << (hash & 31));\n";
-          int sk = 0;
+          // Larger domains: one row per lane per round in a warp-uniform loop;
+          // lanes that hit the same group merge their values (one
+          // `__match_any_sync`) so the table sees one atomic per distinct
+          // group, not one per row -- a query's few live groups would
+          // otherwise serialise the warp's atomics.
+          o << ind << "int b_ = blo_ + lane / lpb_;\n";
+          o << ind << "unsigned w_ = b_ < bhi_ ? (qw_[b_] & bm_) : 0u;\n";
+          o << ind << "for (;;) {\n";
+          o << ind << "  while (w_ == 0u && b_ < bhi_) { b_ += 32 / lpb_; w_ = b_ < bhi_ ? (qw_[b_] & bm_) : 0u; }\n";
+          o << ind << "  if (!__any_sync(0xffffffffu, w_ != 0u)) break;\n";
+          o << ind << "  int hash = -1;\n";
+          for (int k = 0; k < NA; ++k) o << ind << "  unsigned long long x" << k << "_ = 0ULL;\n";
+          o << ind << "  if (w_ != 0u) {\n";
+          o << ind << "  const int i = (b_ << 5) + __ffs(w_) - 1;\n";
+          o << ind << "  w_ &= w_ - 1u;\n";
+          o << terms.str();
+          o << ind << "  hash = " << horner << ";\n";
+          o << ind << "  if (!(" << dom << ")) { cx::raise(a.err, cx::ERR_GROUP_DOMAIN); hash = hash % " << G << "; }\n";
           for (int k = 0; k < NA; ++k) {
             const Agg& ag = p.aggs[k];
             const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
-            o << ind << "    { const unsigned long long x_ = " << x << "; if (x_) atomicAdd(&qtab[(long long)hash * " << NA << " + " << k << "], x_);";
-            if (!p.sparse && ag.fn == AggFn::Sum) { o << " atomicOr(&qbits[" << TWq * (1 + sk) << "ULL + (hash >> 5)], 1u << (hash & 31));"; ++sk; }
-            o << " }\n";
+            o << ind << "  x" << k << "_ = " << x << ";\n";
           }
-          o << ind << "  } else {\n";
-          o << ind << "    atomicOr(&g_touch[hash >> 5], 1u << (hash & 31));\n";
+          o << ind << "  }\n";
+          o << ind << "  const bool ok_ = (unsigned)hash < " << G << "u;\n";
+          o << ind << "  const unsigned okm_ = __ballot_sync(0xffffffffu, ok_);\n";
+          o << ind << "  if (ok_) {\n";
+          o << ind << "    const unsigned peers_ = __match_any_sync(okm_, hash);\n";
+          o << ind << "    if (__popc(peers_) > 1) {\n";
+          for (int k = 0; k < NA; ++k) {
+            o << ind << "      { unsigned long long r_ = 0ULL;\n";
+            o << ind << "        for (unsigned m_ = peers_; m_; m_ &= m_ - 1u) r_ += __shfl_sync(peers_, x" << k << "_, __ffs(m_) - 1);\n";
+            o << ind << "        x" << k << "_ = r_; }\n";
+          }
+          o << ind << "    }\n";
+          o << ind << "    if (lane == __ffs(peers_) - 1) {\n";
+          o << ind << "      if (qtab) {\n";
+          o << ind << "        atomicOr(&qbits[hash >> 5], 1u << (hash & 31));\n";
+          int sk = 0;
+          for (int k = 0; k < NA; ++k) {
+            const Agg& ag = p.aggs[k];
+            o << ind << "        if (x" << k << "_) atomicAdd(&qtab[(long long)hash * " << NA << " + " << k << "], x" << k << "_);\n";
+            if (!p.sparse && ag.fn == AggFn::Sum) { o << ind << "        atomicOr(&qbits[" << TWq * (1 + sk) << "ULL + (hash >> 5)], 1u << (hash & 31));\n"; ++sk; }
+          }
+          o << ind << "      } else {\n";
+          o << ind << "        atomicOr(&g_touch[hash >> 5], 1u << (hash & 31));\n";
           for (int k = 0; k < NA; ++k) {
             const Agg& ag = p.aggs[k];
             const int slot = (int)p.groups.size() + k;
             const std::string ix = "(unsigned long long)hash * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
-            const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
-            o << ind << "    { const unsigned long long x_ = " << x << "; if (x_) atomicAdd(&d_result[" << ix << "], x_);";
-            if (!p.sparse && ag.fn == AggFn::Sum) o << " db::atomic_set_valid_bit(d_result_validity, " << ix << ");";
-            o << " }\n";
-            if (!p.sparse && ag.fn == AggFn::Count) o << ind << "    db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+            o << ind << "        if (x" << k << "_) atomicAdd(&d_result[" << ix << "], x" << k << "_);\n";
+            if (!p.sparse && (ag.fn == AggFn::Sum || ag.fn == AggFn::Count))
+              o << ind << "        db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
           }
+          o << ind << "      }\n";
+          o << ind << "    }\n";
           o << ind << "  }\n";
-          o << loop_close;
+          o << ind << "}\n";
         }
         }
       }

@@ -287,9 +287,10 @@ PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas
                     for bt, ipt, st, bm, pf, pl in ((1024, 4, 0, 49152, 1, 0), (1024, 4, 0, 0, 1, 4),
                                                     (512, 2, 0, 0, 1, 4), (1024, 2, 0, 0, 0, 4),
                                                     (512, 8, 4, 0, 0, 0))]
-SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=2, producer_warps=pw)
-                     for bt, ipt, st, pw in ((1024, 1, 3, 11), (1024, 1, 3, 17), (1024, 1, 3, 14), (512, 2, 2, 5),
-                                             (512, 2, 2, 7))]
+SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=2, producer_warps=pw,
+                          group_merge=gm)
+                     for bt, ipt, st, pw, gm in ((1024, 1, 3, 11, 0), (1024, 1, 3, 11, 3), (1024, 1, 3, 14, 0),
+                                                 (1024, 1, 3, 14, 3), (512, 2, 2, 5, 0), (512, 2, 2, 7, 3))]
 
 
 def time_steps(torch, stream, steps, run_step, sampler=None):

@@ -2466,6 +2466,37 @@ struct SharedGen {
           o << loop_close;
           tiny_flush();
           if (tu.group_merge == 2) o << ind << "}\n";
+        } else if (tu.group_merge == 2 || tu.group_merge == 3) {
+          // Direct per-row updates: shared-memory table when the query has one, else global atomics.
+          o << loop_open;
+          o << terms.str();
+          o << ind << "  int hash = " << horner << ";\n";
+          o << ind << "  if (!(" << dom << ")) { cx::raise(a.err, cx::ERR_GROUP_DOMAIN); hash = hash % " << G << "; }\n";
+          o << ind << "  if ((unsigned)hash >= " << G << "u) continue;\n";
+          o << ind << "  if (qtab) {\n";
+          o << ind << "    atomicOr(&qbits[hash >> 5], 1u << (hash & 31));\n";
+          int sk = 0;
+          for (int k = 0; k < NA; ++k) {
+            const Agg& ag = p.aggs[k];
+            const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
+            o << ind << "    { const unsigned long long x_ = " << x << "; if (x_) atomicAdd(&qtab[(long long)hash * " << NA << " + " << k << "], x_);";
+            if (!p.sparse && ag.fn == AggFn::Sum) { o << " atomicOr(&qbits[" << TWq * (1 + sk) << "ULL + (hash >> 5)], 1u << (hash & 31));"; ++sk; }
+            o << " }\n";
+          }
+          o << ind << "  } else {\n";
+          o << ind << "    atomicOr(&g_touch[hash >> 5], 1u << (hash & 31));\n";
+          for (int k = 0; k < NA; ++k) {
+            const Agg& ag = p.aggs[k];
+            const int slot = (int)p.groups.size() + k;
+            const std::string ix = "(unsigned long long)hash * " + std::to_string(TS) + "ULL + " + std::to_string(slot);
+            const std::string x = ag.fn == AggFn::Count ? "1ULL" : "(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")";
+            o << ind << "    { const unsigned long long x_ = " << x << "; if (x_) atomicAdd(&d_result[" << ix << "], x_);";
+            if (!p.sparse && ag.fn == AggFn::Sum) o << " db::atomic_set_valid_bit(d_result_validity, " << ix << ");";
+            o << " }\n";
+            if (!p.sparse && ag.fn == AggFn::Count) o << ind << "    db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+          }
+          o << ind << "  }\n";
+          o << loop_close;
         } else {
           // Larger domains: one row per lane per round in a warp-uniform loop;
           // lanes that hit the same group merge their values (one

@@ -204,7 +204,7 @@ def test_sparse_compaction(db):
 # ------------------------------------------------------------ shared scans
 
 @pytest.mark.parametrize("nq,tune", [(16, None), (37, (512, 2, 2)), (64, (256, 4, 2)), (5, (1024, 1, 1)),
-                                     (33, (512, 2, 2, 2))])
+                                     (33, (512, 2, 2, 2)), (48, (1024, 1, 3, 3))])
 def test_shared_scan_batch_matches_oracle_per_query(db, nq, tune):
     """Every query of a mixed-template batch run as ONE shared scan equals the
     oracle run on that query alone (same words, same validity bits)."""
@@ -216,7 +216,7 @@ def test_shared_scan_batch_matches_oracle_per_query(db, nq, tune):
         t = _lib.default_tuning()
         t.block_threads, t.items_per_thread, t.stages = tune[:3]
         if len(tune) > 3:
-            t.group_merge = tune[3]  # direct shared-memory adds for tiny group domains
+            t.group_merge = tune[3]  # 2: direct adds for tiny domains too; 3: per-row atomics above 32 groups
     assert all(db.shareable(p) for p in plans)
     got = db.execute_shared(plans, t)
     assert got[0].kernel_error == 0

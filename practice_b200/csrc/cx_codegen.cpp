@@ -2236,12 +2236,16 @@ struct SharedGen {
       o << "            const int hash = bad_ ? (" << horner << ") % " << G << " : (" << horner << ");\n";
       o << "            h_ = (unsigned)hash < " << G << "u ? hash : " << G << ";\n";
       o << "          }\n";
-      o << "          unsigned gw_ = 0u;\n";
-      o << "          #pragma unroll\n";
-      o << "          for (int g = 0; g < " << G << "; ++g) { const unsigned b_ = __ballot_sync(0xffffffffu, h_ == g); if (lane == g) gw_ = b_; }\n";
+      // One match over the lanes gives every group's row word at once: the
+      // block's words are cleared, then the lowest lane of each group writes
+      // its group's word (the same lane writes the out-of-domain word).
+      const std::string gm_at = "s_gm_t[(" + std::to_string(gm_base[si]) + " + ";
+      o << "          if (lane <= " << G << ") " << gm_at << "lane) * " << NB << " + blk_] = 0u;\n";
+      o << "          __syncwarp();\n";
+      o << "          const unsigned peers_ = __match_any_sync(0xffffffffu, h_);\n";
+      o << "          if (h_ < " << G << " && lane == __ffs(peers_) - 1) " << gm_at << "h_) * " << NB << " + blk_] = peers_;\n";
       o << "          const unsigned bb_ = __ballot_sync(0xffffffffu, bad_);\n";
-      o << "          if (lane == " << G << ") gw_ = bb_;\n";
-      o << "          if (lane <= " << G << ") s_gm_t[(" << gm_base[si] << " + lane) * " << NB << " + blk_] = gw_;\n";
+      o << "          if (lane == " << G << ") " << gm_at << G << ") * " << NB << " + blk_] = bb_;\n";
       o << "        }\n";
     }
     // Transpose the warp's 32 row masks into one word per query.

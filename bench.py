@@ -278,9 +278,9 @@ def config_block(args):
 
 # DRAM bytes (read + write) per fact row of one shared-scan launch over the
 # 8-column batch table, from the ncu capture in
-# profiles/SharedScan_LINEORDER_batch32_30M.md (974.2 MB for 30M rows); the
+# profiles/SharedScan_LINEORDER_batch32_30M.md (972.2 MB for 30M rows); the
 # traffic of a launch grows with its rows.
-SHARED_DRAM_BYTES_PER_ROW = 974.231040e6 / 30e6
+SHARED_DRAM_BYTES_PER_ROW = (968.458240e6 + 3.693568e6) / 30e6
 
 PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=bm,
                          prefetch=pf, group_placement=pl)

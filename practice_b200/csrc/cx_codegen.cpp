@@ -1099,54 +1099,13 @@ struct Emitter {
       }
     };
 
-    if (expanding) {
-      // Columns the expansion publishes are written inside the item loop;
-      // every fact column the rest of the pipeline reads is loaded once here.
-      for (size_t k = xs; k < p.steps.size(); ++k) {
-        const Step& s = p.steps[k];
-        if (s.kind != Step::JoinStep) continue;
-        for (const auto& c : s.join.gathers) {
-          loaded.insert(c);
-          if (nullable(c)) valid_regs.insert(c);
-        }
-        if (!s.join.payload.empty()) {
-          loaded.insert(s.join.payload);
-          if (payload_valid.count(s.join.payload)) valid_regs.insert(s.join.payload);
-        }
-      }
-      for (size_t k = xs; k < p.steps.size(); ++k) {
-        const Step& s = p.steps[k];
-        if (s.kind == Step::Filter) load_expr_cols(o, s.filter.get(), ind);
-        else for (const auto& fk : s.join.fks) ensure_loaded(o, fk, ind);
-      }
-    }
-    for (const auto& g : p.groups) load_expr_cols(o, g.expr.get(), ind);
-    for (const auto& ag : p.aggs) load_expr_cols(o, ag.arg.get(), ind);
-
-    // Aggregate consume.
-    if (expanding) {
-      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
-      item_steps(xs, ind + "    ");
-      o << ind << "  }\n" << ind << "}\n";
-    } else if (!grouped) {
-      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
-      scalar_update(ind + "    ");
-      o << ind << "  }\n" << ind << "}\n";
-    } else if (reg_groups || lane_groups) {
-      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
-      group_hash(ind + "    ");
-      o << ind << "    if ((unsigned)hash < " << G << "u) {\n";
-      if (reg_groups) reg_update(ind + "      ");
-      else lane_update(ind + "      ");
-      o << ind << "    }\n";
-      o << ind << "  }\n";
-      o << ind << "}\n";
-    } else {
-      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      o << ind << "  bool act = flags[i] && (tid + BLOCK_THREADS * i < num_tile_items);\n";
+    // Group update of one item under the flag `act_init`: lanes with the same
+    // group merge their values (one match) and the lowest applies them -- or,
+    // with per-warp tables and direct merging, every active lane applies its
+    // own.  All lanes of the warp execute it (it ballots).
+    auto merged_update = [&](const std::string& ind, const std::string& act_init) {
+      o << ind << "{\n";
+      o << ind << "  bool act = " << act_init << ";\n";
       o << ind << "  int hash = 0;\n";
       o << ind << "  if (act) {\n";
       std::string horner, dom;
@@ -1227,6 +1186,148 @@ struct Emitter {
       }
       o << ind << "  }\n";
       o << ind << "  }\n";
+      o << ind << "}\n";
+    };
+    if (expanding) {
+      // Columns the expansion publishes are written inside the item loop;
+      // every fact column the rest of the pipeline reads is loaded once here.
+      for (size_t k = xs; k < p.steps.size(); ++k) {
+        const Step& s = p.steps[k];
+        if (s.kind != Step::JoinStep) continue;
+        for (const auto& c : s.join.gathers) {
+          loaded.insert(c);
+          if (nullable(c)) valid_regs.insert(c);
+        }
+        if (!s.join.payload.empty()) {
+          loaded.insert(s.join.payload);
+          if (payload_valid.count(s.join.payload)) valid_regs.insert(s.join.payload);
+        }
+      }
+      for (size_t k = xs; k < p.steps.size(); ++k) {
+        const Step& s = p.steps[k];
+        if (s.kind == Step::Filter) load_expr_cols(o, s.filter.get(), ind);
+        else for (const auto& fk : s.join.fks) ensure_loaded(o, fk, ind);
+      }
+    }
+    for (const auto& g : p.groups) load_expr_cols(o, g.expr.get(), ind);
+    for (const auto& ag : p.aggs) load_expr_cols(o, ag.arg.get(), ind);
+
+    // With group_merge = 1, one expanding join feeding a shared-memory or
+    // global group table runs as a warp-uniform loop (every lane takes its
+    // next match each round): the later steps become a per-lane predicate and
+    // equal groups merge across the warp before the atomics, as in the vector
+    // path.  Otherwise (the default; measured no slower) every expanded row
+    // updates on its own (item_steps).
+    int n_expanding = 0;
+    for (const auto& s : p.steps)
+      if (s.kind == Step::JoinStep && s.join.expands()) ++n_expanding;
+    const bool uniform_expand =
+        expanding && n_expanding == 1 && grouped && !reg_groups && !lane_groups && tu.group_merge == 1;
+    auto uniform_tail = [&](const std::string& ii) {
+      for (size_t k = xs + 1; k < p.steps.size(); ++k) {
+        const Step& s = p.steps[k];
+        if (s.kind == Step::Filter) {
+          o << ii << "act_ = act_ && (" << and_terms({valid_of(s.filter.get()), value_of(s.filter.get())}) << ");\n";
+          continue;
+        }
+        const Join& j = s.join;
+        const std::string& fk = j.fks[0];
+        const std::string ht = ht_name(j.dim), hs = "h" + std::to_string(k) + "_";
+        const std::string fkv = valid_regs.count(fk) ? fk + "_valid[i]" : "1";
+        o << ii << "if (act_) {\n";
+        o << ii << "  const int " << hs << " = cx_detail::pht_slot<int>(" << fk << "[i], " << j.len << ", " << j.keymin << ");\n";
+        if (j.payload.empty()) {
+          o << ii << "  if (!((" << fkv << ") && " << hs << " >= 0 && " << ht << "[" << hs << "] == " << fk << "[i])) act_ = false;\n";
+        } else {
+          o << ii << "  if ((" << fkv << ") && " << hs << " >= 0 && " << ht << "[2LL * " << hs << "] == " << fk << "[i]) {\n";
+          o << ii << "    " << j.payload << "[i] = " << ht << "[2LL * " << hs << " + 1];\n";
+          if (payload_valid.count(j.payload))
+            o << ii << "    " << j.payload << "_valid[i] = (int)((" << ht << "_valid[" << hs << " >> 5] >> (" << hs << " & 31)) & 1u);\n";
+          o << ii << "  } else {\n" << ii << "    act_ = false;\n" << ii << "  }\n";
+        }
+        o << ii << "}\n";
+      }
+      merged_update(ii, "act_");
+    };
+    auto uniform_expansion = [&](const std::string& ii) {
+      const Join& j = p.steps[xs].join;
+      const std::string ht = ht_name(j.dim);
+      o << ii << "#pragma unroll\n" << ii << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << ii << "  const bool base_ = flags[i] && (tid + BLOCK_THREADS * i < num_tile_items);\n";
+      for (size_t f = 0; f < j.fks.size(); ++f) {
+        const std::string& fk = j.fks[f];
+        std::vector<std::string> terms{"base_", valid_regs.count(fk) ? fk + "_valid[i]" : "1"};
+        for (size_t q = 0; q < f; ++q) {
+          const std::string& pf = j.fks[q];
+          const std::string pv = valid_regs.count(pf) ? pf + "_valid[i]" : "1";
+          terms.push_back(lit_true(pv) ? fk + "[i] != " + pf + "[i]" : "(!(" + pv + ") || " + fk + "[i] != " + pf + "[i])");
+        }
+        const std::string i2 = ii + "  ";
+        o << i2 << "{\n";
+        o << i2 << "  const bool br_ = " << and_terms(terms) << ";\n";
+        if (j.multi) {
+          o << i2 << "  int off_ = 0, cnt_ = 0;\n";
+          o << i2 << "  if (br_) { int fl_ = 1; ProbeMultiHT<int>(" << fk << "[i], off_, cnt_, fl_, " << ht << ", " << j.len << ", "
+            << j.keymin << "); }\n";
+          o << i2 << "  for (int j_ = 0; __any_sync(0xffffffffu, j_ < cnt_); ++j_) {\n";
+          o << i2 << "    bool act_ = j_ < cnt_;\n";
+          o << i2 << "    if (act_) {\n";
+          o << i2 << "      const long long rid_ = mpay_" << lower(j.dim) << "[off_ + j_];\n";
+          for (const auto& g : j.gathers) {
+            o << i2 << "      " << g << "[i] = d_" << g << "[rid_];\n";
+            if (nullable(g))
+              o << i2 << "      " << g << "_valid[i] = n_" << g << " ? (int)((n_" << g << "[rid_ >> 6] >> (rid_ & 63)) & 1ULL) : 1;\n";
+          }
+          o << i2 << "    }\n";
+          uniform_tail(i2 + "    ");
+          o << i2 << "  }\n";
+        } else {
+          o << i2 << "  bool act_ = br_;\n";
+          o << i2 << "  if (act_) {\n";
+          o << i2 << "    const int hx_ = cx_detail::pht_slot<int>(" << fk << "[i], " << j.len << ", " << j.keymin << ");\n";
+          if (j.payload.empty()) {
+            o << i2 << "    if (!(hx_ >= 0 && " << ht << "[hx_] == " << fk << "[i])) act_ = false;\n";
+          } else {
+            o << i2 << "    if (hx_ >= 0 && " << ht << "[2LL * hx_] == " << fk << "[i]) {\n";
+            o << i2 << "      " << j.payload << "[i] = " << ht << "[2LL * hx_ + 1];\n";
+            if (payload_valid.count(j.payload))
+              o << i2 << "      " << j.payload << "_valid[i] = (int)((" << ht << "_valid[hx_ >> 5] >> (hx_ & 31)) & 1u);\n";
+            o << i2 << "    } else {\n" << i2 << "      act_ = false;\n" << i2 << "    }\n";
+          }
+          o << i2 << "  }\n";
+          uniform_tail(i2 + "  ");
+        }
+        o << i2 << "}\n";
+      }
+      o << ii << "}\n";
+    };
+
+    // Aggregate consume.
+    if (uniform_expand) {
+      uniform_expansion(ind);
+    } else if (expanding) {
+      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+      item_steps(xs, ind + "    ");
+      o << ind << "  }\n" << ind << "}\n";
+    } else if (!grouped) {
+      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+      scalar_update(ind + "    ");
+      o << ind << "  }\n" << ind << "}\n";
+    } else if (reg_groups || lane_groups) {
+      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+      group_hash(ind + "    ");
+      o << ind << "    if ((unsigned)hash < " << G << "u) {\n";
+      if (reg_groups) reg_update(ind + "      ");
+      else lane_update(ind + "      ");
+      o << ind << "    }\n";
+      o << ind << "  }\n";
+      o << ind << "}\n";
+    } else {
+      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      merged_update(ind + "  ", "flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)");
       o << ind << "}\n";
     }
 

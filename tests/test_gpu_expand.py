@@ -96,6 +96,19 @@ def test_group_placements_in_item_mode(db, placement):
         assert_parity(db, p, ht, t)
 
 
+def test_warp_uniform_expansion(db):
+    """group_merge = 1: the expansion runs as a warp-uniform loop with equal
+    groups merged across the warp before the atomics."""
+    n = 600_011
+    ht = load(db, 49, n, nulls={"lo_revenue": 60, "ps_tier": 80})
+    for placement in (0, 2):
+        t = make_tuning(group_placement=placement, group_merge=1)
+        for p in (queries.or_join_then_filter(n), queries.mht_year_tier(n), queries.mht_brand(n, nullable_tier=True)):
+            src = _lib.codegen(p.text(), t)
+            assert "bool act_" in src
+            assert_parity(db, p, ht, t)
+
+
 def test_mht_slot_collision_raises_a_kernel_error(db):
     n = 100_000
     ht = load(db, 46, n)

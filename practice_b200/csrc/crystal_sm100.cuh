@@ -568,7 +568,7 @@ CX_DEVICE void BlockProbeExactBitmap(int tid, K (&items)[ITEMS_PER_THREAD], int 
     if (guarded && i * BLOCK_THREADS + tid >= num_items) continue;
     const K d = items[i] - key_min;
     int hit;
-    if (d >= K(0) && d < K(ht_len)) {
+    if (sizeof(K) == 4 ? (unsigned)d < (unsigned)ht_len : (d >= K(0) && d < K(ht_len))) {
       hit = (int)((bitmap[(unsigned)d >> 5] >> ((unsigned)d & 31u)) & 1u);
     } else {
       hit = 0;
@@ -577,7 +577,7 @@ CX_DEVICE void BlockProbeExactBitmap(int tid, K (&items)[ITEMS_PER_THREAD], int 
         hit = (h >= 0 && ht[(long long)h << pair] == items[i]) ? 1 : 0;
       }
     }
-    flags[i] = (flags[i] && hit) ? 1 : 0;
+    flags[i] = (int)(flags[i] != 0) & hit;
   }
 }
 

@@ -1558,7 +1558,7 @@ struct Emitter {
     for (const auto& s : p.steps)
       if (s.kind == Step::JoinStep) emit_build(s.join);
     for (const auto& s : p.steps)
-      if (s.kind == Step::JoinStep) emit_occupancy(s.join);
+      if (s.kind == Step::JoinStep) emit_occupancy(s.join);  // exact membership bitmaps
     emit_scan();
     if (p.hidden_count_slots() > 0) emit_finalize();
 

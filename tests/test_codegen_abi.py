@@ -72,6 +72,23 @@ def test_tuning_space_compiles(bt, ipt, stages, place):
         _lib.Module(_lib.codegen(plan.text(), t), key=f"tune_{name}_{bt}_{ipt}_{stages}_{place}")
 
 
+@pytest.mark.parametrize("prefetch,place,merge", [(0, 4, 0), (1, 3, 0), (2, 0, 0), (1, 0, 1), (1, 2, 2), (1, 1, 1)])
+def test_launch_knobs_compile(prefetch, place, merge):
+    """Unstaged loads (where first used / vector loads at the tile start / one
+    tile ahead), per-thread shared-memory and register group slots, warp-merged
+    and per-lane group updates, including the expanding joins' uniform loop."""
+    t = _lib.default_tuning()
+    t.prefetch, t.group_placement, t.group_merge = prefetch, place, merge
+    plans = all_plans()
+    for name in ("T1", "T2", "ssb_q31_nullable", "or_join_then_filter", "mht_year_tier"):
+        src = _lib.codegen(plans[name].text(), t)
+        if prefetch == 0:
+            assert "WarpLoadTileV" not in src
+        if place == 4 and name == "T1":
+            assert "s_lacc" in src
+        _lib.Module(src, key=f"knobs_{name}_{prefetch}_{place}_{merge}")
+
+
 def test_reference_style_primitive_calls_compile_against_header():
     """Lines in the shape the reference visitor emits (visitor.cpp:4233-4288,
     1838-1880, 4640-4660) compile against crystal_sm100.cuh unchanged."""

@@ -141,6 +141,24 @@ def test_bad_plans_return_invalid_status():
     assert e.value.code == -1
 
 
+def test_bad_or_and_multi_value_joins_are_rejected():
+    base = ("(query (table F fact (cols f1 f2 f3 v)) (table D (cols k p q)) {join} "
+            "(aggregate (sum (col v))))")
+    ok = "(join D (pk k) (fk f1 f2) (len 10) (keymin 0) (multi 1) (payload p q))"
+    _lib.codegen(base.format(join=ok))
+    bad = {
+        "(join D (pk k) (fk f1 f1) (len 10) (keymin 0))": "listed twice",
+        "(join D (pk k) (fk f1 f2 f3 f1 f2) (len 10) (keymin 0))": "at most 4",
+        "(join D (pk k) (fk f1) (len 10) (keymin 0) (payload p q))": "one payload",
+        "(join D (pk k) (fk f1) (len 10) (keymin 0) (multi 1) (payload p p))": "listed twice",
+        "(join D (pk k) (fk f1) (len 10) (keymin 0) (multi 1) (payload zz))": "not a column",
+    }
+    for join, msg in bad.items():
+        with pytest.raises(_lib.CxError) as e:
+            _lib.codegen(base.format(join=join))
+        assert e.value.code == -1 and msg in str(e.value), (join, str(e.value))
+
+
 def test_compile_errors_come_back_with_the_nvrtc_log():
     with pytest.raises(_lib.CxError) as e:
         _lib.Module("/*@cx-launch\nv 1\n@*/\n__global__ void k() { this is not cuda; }", key="broken")

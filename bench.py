@@ -120,6 +120,8 @@ class ClockSampler:
 
 
 def dist_setup(ngpus: int):
+    """One process per GPU (torchrun's RANK / WORLD_SIZE / LOCAL_RANK); NCCL
+    on GPUs, gloo where there are none (the host-side tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -127,8 +129,10 @@ def dist_setup(ngpus: int):
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         pg = dist
     return world, rank, local, pg
 
@@ -144,9 +148,18 @@ def max_over_ranks(pg, value: float, device) -> float:
 
 def barrier(pg, device):
     import torch
-    if pg is not None:
-        pg.barrier(device_ids=[device.index])
-    torch.cuda.synchronize(device)
+    if device.type == "cuda":
+        if pg is not None:
+            pg.barrier(device_ids=[device.index])
+        torch.cuda.synchronize(device)
+    elif pg is not None:
+        pg.barrier()
+
+
+def job_rate(units_per_rank: float, world: int, max_ms: float) -> float:
+    """Whole-job throughput: the units every rank processed over the slowest
+    rank's time (weak scaling: each rank holds its own replica)."""
+    return units_per_rank * world / (max_ms / 1000.0)
 
 
 # ------------------------------------------------------------- CPU baseline
@@ -372,7 +385,7 @@ def main():
     plain_launches = sum(c.timing().gpu_launches for c in ctxs)
     plain_ms = max_over_ranks(pg, plain_ms, device)
     plain_bytes = sum(len(p.columns_read()) * 4 * args.rows for p in plans)
-    plain = {"queries_per_s": len(plans) * args.steps * world / (plain_ms / 1000.0),
+    plain = {"queries_per_s": job_rate(len(plans) * args.steps, world, plain_ms),
              "ms_per_step": plain_ms / args.steps,
              "p50_ms": statistics.median(plain_lat), "p99_ms": float(np.percentile(plain_lat, 99)),
              "scan_GBps": plain_bytes / (sum(plain_scan_ms) / 1000.0) / 1e9,
@@ -476,7 +489,7 @@ def main():
 
     if rank == 0:
         if shared is not None:
-            value = len(plans) * args.steps * world / (shared["ms_per_step"] * args.steps / 1000.0)
+            value = job_rate(len(plans) * args.steps, world, shared["ms_per_step"] * args.steps)
             ms_step = shared["ms_per_step"]
             lat = shared["lat"]
             achieved = shared["bytes"] / (shared["scan_ms"] / 1000.0) / 1e9

@@ -35,7 +35,7 @@ STREAMS = {
     "p_mfgr": 40, "p_category": 41, "p_brand1": 42,
     "ps_partkey": 50, "ps_tier": 51, "ps_availqty": 52, "ps_supplycost": 53,
     "valid_lo_revenue": 100, "valid_c_city": 101, "valid_lo_quantity": 102, "valid_lo_discount": 103,
-    "valid_ps_tier": 104, "valid_lo_commitdate": 105,
+    "valid_ps_tier": 104, "valid_lo_commitdate": 105, "valid_c_nation": 106,
 }
 
 # Uniform fact columns: (lo, hi) inclusive.

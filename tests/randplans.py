@@ -46,14 +46,14 @@ def _group(name, nullable=False):
     return Group(col(name), mn, card, nullable)
 
 
-def harness_plan(rng: random.Random, rows: int, name: str = "fuzz"):
+def harness_plan(rng: random.Random, rows: int, name: str = "fuzz", expanding_ok: bool = True):
     b = PlanBuilder(ssb_tables(rows, FACT_COLS), "LINEORDER", name=name)
     preds = [_cmp(rng, "lo_quantity", 1, 50) for _ in range(rng.randint(0, 2))]
     preds += [_cmp(rng, "lo_discount", 0, 10) for _ in range(rng.randint(0, 1))]
     if preds:
         b.filter(and_(*preds))
     dims = rng.sample(["DDATE", "CUSTOMER", "SUPPLIER", "PART"], rng.randint(0, 3))
-    expanding = rng.choice((None, None, "or", "mht"))
+    expanding = rng.choice((None, None, "or", "mht")) if expanding_ok else None
     if expanding == "mht" and "PART" not in dims:
         dims.append("PARTSUPP")
     if expanding == "or" and "DDATE" not in dims:

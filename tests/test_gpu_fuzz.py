@@ -4,7 +4,7 @@ nullable fact and payload columns under three-valued logic, OR / NOT / IS NULL
 filters, filters on join payloads, MIN / MAX / AVG / COUNT(column) / CASE
 aggregates, one to three joins in random order, an OR over two date keys or a
 multi-value PARTSUPP join -- at the default launch shape and at a TMA-staged
-one."""
+one; and random batches of shareable plans through one shared scan."""
 import random
 
 import numpy as np
@@ -14,7 +14,7 @@ import oracle
 from practice_b200 import datagen
 from practice_b200.engine import make_tuning
 
-from randplans import FACT_COLS, engine_plan
+from randplans import FACT_COLS, engine_plan, harness_plan
 
 pytestmark = pytest.mark.gpu
 
@@ -46,3 +46,20 @@ def test_random_plan_matches_oracle(loaded, seed, shape):
     fw = len(got.words)
     np.testing.assert_array_equal(got.words, ref.words[:fw], err_msg=plan.text())
     np.testing.assert_array_equal(got.validity, ref.validity[: (fw + 63) // 64], err_msg=plan.text())
+
+
+@pytest.mark.parametrize("batch", range(6))
+def test_random_shared_batch_matches_oracle_per_query(loaded, batch):
+    """Eight random shareable plans (eight distinct shapes) answered by ONE
+    shared scan: every query equals the oracle run on that query alone."""
+    db, ht = loaded
+    rng = random.Random(1000 + batch)
+    plans = [harness_plan(rng, N, name=f"shared{batch}_{i}", expanding_ok=False) for i in range(8)]
+    assert all(db.shareable(p) for p in plans)
+    got = db.execute_shared(plans)
+    assert got[0].kernel_error == 0
+    for p, g in zip(plans, got):
+        ref = oracle.run_plan(p.text(), ht.columns, ht.validity, {"LINEORDER": N, **datagen.DIM_ROWS},
+                              p.group_slots * p.storage_ts)
+        np.testing.assert_array_equal(g.words, ref.words, err_msg=p.text())
+        np.testing.assert_array_equal(g.validity, ref.validity, err_msg=p.text())

@@ -109,6 +109,31 @@ def test_warp_uniform_expansion(db):
             assert_parity(db, p, ht, t)
 
 
+def test_or_over_three_keys_and_or_inside_a_multi_value_join(db):
+    """(lo_custkey OR lo_suppkey OR lo_partkey) = c_custkey, and
+    (lo_partkey OR lo_suppkey) = ps_partkey on the non-unique PARTSUPP key;
+    some keys are made equal so the duplicate-key rule is exercised."""
+    from practice_b200.plan import PlanBuilder, col, star
+    n = 800_017
+    cols = ALL_COLS + ["lo_custkey"]
+    ht = datagen.host_tables(50, n, cols, dims=("DDATE", "CUSTOMER", "SUPPLIER", "PART", "PARTSUPP"))
+    ht.columns["lo_suppkey"][::50] = ht.columns["lo_custkey"][::50]
+    ht.columns["lo_partkey"][::70] = ht.columns["lo_suppkey"][::70]
+    db.reset()
+    db.load_host_tables(ht, datagen.ssb_tables(n, cols))
+    tabs = datagen.ssb_tables(n, cols)
+    b = PlanBuilder(tabs, "LINEORDER", name="or3")
+    b.join("CUSTOMER", ("lo_custkey", "lo_suppkey", "lo_partkey"), where=col("c_region").le(2))
+    or3 = b.aggregate([queries._g("c_region")], [("sum", col("lo_revenue")), ("count", star())])
+    b = PlanBuilder(tabs, "LINEORDER", name="mht_or")
+    b.join("DDATE", "lo_orderdate")
+    b.join("PARTSUPP", ("lo_partkey", "lo_suppkey"), where=col("ps_availqty").lt(6000))
+    mht_or = b.aggregate([queries._g("d_year"), queries._g("ps_tier")], [("sum", col("lo_revenue")), ("count", star())])
+    for p in (or3, mht_or):
+        got = assert_parity(db, p, ht)
+        assert got.words.any()
+
+
 def test_mht_slot_collision_raises_a_kernel_error(db):
     n = 100_000
     ht = load(db, 46, n)

@@ -12,7 +12,7 @@ import pytest
 
 import oracle
 from practice_b200 import datagen, queries
-from practice_b200.plan import PlanBuilder, col, star
+from practice_b200.plan import PlanBuilder, and_, col, star
 
 N = 120_007
 DIMS = {**{k: v for k, v in datagen.DIM_ROWS.items()}}
@@ -112,3 +112,33 @@ def test_mht_slot_collision_is_an_error(ht):
     steps = [(k, dataclasses.replace(s, length=100_000) if k == "join" and s.multi else s) for k, s in p.steps]
     with pytest.raises(RuntimeError, match="collision"):
         run(dataclasses.replace(p, steps=steps), ht)
+
+
+def test_or_join_over_three_keys_is_the_sum_of_its_distinct_key_branches(ht):
+    """(lo_custkey = c_custkey OR lo_suppkey = c_custkey OR lo_partkey = c_custkey):
+    each key probes unless it equals an earlier key of the row."""
+    def plan(fks, pre=None):
+        b = PlanBuilder(datagen.ssb_tables(N, queries.MHT_COLS + ["lo_custkey"]), "LINEORDER")
+        if pre is not None:
+            b.filter(pre)
+        b.join("CUSTOMER", fks, where=col("c_region").le(2))
+        return b.aggregate([queries._g("c_region")], [("sum", col("lo_revenue")), ("count", star())])
+
+    cols = dict(ht.columns)
+    cols.update(datagen.dim_columns("CUSTOMER", 31))
+    cols["lo_custkey"] = datagen.fact_column("lo_custkey", 31, 0, N)
+    # make some keys equal so the duplicate rule is exercised
+    cols["lo_suppkey"] = cols["lo_suppkey"].copy()
+    cols["lo_suppkey"][::50] = cols["lo_custkey"][::50]
+    cols["lo_partkey"] = cols["lo_partkey"].copy()
+    cols["lo_partkey"][::70] = cols["lo_suppkey"][::70]
+    all3 = run(plan(("lo_custkey", "lo_suppkey", "lo_partkey")), ht, cols).words
+    k1 = run(plan("lo_custkey"), ht, cols).words
+    k2 = run(plan("lo_suppkey", col("lo_suppkey").ne(col("lo_custkey"))), ht, cols).words
+    k3 = run(plan("lo_partkey", and_(col("lo_partkey").ne(col("lo_custkey")), col("lo_partkey").ne(col("lo_suppkey")))),
+             ht, cols).words
+    ts = 3
+    for g in range(5):
+        for k in (1, 2):
+            assert all3[g * ts + k] == k1[g * ts + k] + k2[g * ts + k] + k3[g * ts + k]
+    assert all3[1::3].sum() > k1[1::3].sum() > 0

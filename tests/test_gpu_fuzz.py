@@ -4,14 +4,15 @@ nullable fact and payload columns under three-valued logic, OR / NOT / IS NULL
 filters, filters on join payloads, MIN / MAX / AVG / COUNT(column) / CASE
 aggregates, one to three joins in random order, an OR over two date keys or a
 multi-value PARTSUPP join -- at the default launch shape and at a TMA-staged
-one; and random batches of shareable plans through one shared scan."""
+one; random batches of shareable plans through one shared scan; and a random
+mix through the request loop."""
 import random
 
 import numpy as np
 import pytest
 
 import oracle
-from practice_b200 import datagen
+from practice_b200 import _lib, datagen
 from practice_b200.engine import make_tuning
 
 from randplans import FACT_COLS, engine_plan, harness_plan
@@ -63,3 +64,31 @@ def test_random_shared_batch_matches_oracle_per_query(loaded, batch):
                               p.group_slots * p.storage_ts)
         np.testing.assert_array_equal(g.words, ref.words, err_msg=p.text())
         np.testing.assert_array_equal(g.validity, ref.validity, err_msg=p.text())
+
+
+def test_random_mix_through_the_request_loop(loaded):
+    """Random shareable plans mixed with random plans the shared scan does not
+    take (nullable columns, AVG / MIN / MAX, OR-joins, multi-value joins),
+    submitted back to back to the request loop: every result equals the
+    oracle's, whether it ran in a shared launch or alone."""
+    db, ht = loaded
+    rng = random.Random(777)
+    plans = [harness_plan(rng, N, name=f"mix_h{i}", expanding_ok=False) for i in range(12)]
+    plans += [engine_plan(rng, N, NULLABLE, name=f"mix_e{i}") for i in range(8)]
+    rng.shuffle(plans)
+    srv = _lib.Server(db.ctx, _lib.server_config(max_batch=16, slots=1, min_shared_batch=2))
+    try:
+        ids = [srv.submit(p.text()) for p in plans]
+        for rid, p in zip(ids, plans):
+            info = srv.wait(rid, 120_000)
+            assert info.status == 0 and info.kernel_error == 0, (p.name, info.status, info.kernel_error)
+            w, v = srv.fetch(rid, info)
+            ref = oracle.run_plan(p.text(), ht.columns, ht.validity, {"LINEORDER": N, **datagen.DIM_ROWS},
+                                  p.group_slots * p.storage_ts)
+            np.testing.assert_array_equal(w, ref.words[: len(w)], err_msg=p.text())
+            np.testing.assert_array_equal(v, ref.validity[: len(v)], err_msg=p.text())
+            srv.release(rid)
+        st = srv.stats()
+        assert st.completed == len(plans) and st.rejected == 0
+    finally:
+        srv.close()

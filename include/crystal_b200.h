@@ -56,8 +56,9 @@ typedef struct cx_tuning {
   int smem_group_budget; /* bytes a shared-memory group table may use */
   int bitmap_budget;     /* bytes of shared memory for exact join membership bitmaps (0 = none;
                             default 48 KiB) */
-  int group_merge;       /* 0 auto, 1 merge equal groups within a warp first, 2 per-lane atomics,
-                            3 shared scans: per-row atomics for domains above 32 groups only */
+  int group_merge;       /* 0 auto, 1 merge equal groups within a warp first (for a plan with one
+                            OR / multi-value join: a warp-uniform expansion loop), 2 per-lane
+                            atomics, 3 shared scans: per-row atomics above 32 groups only */
   int producer_warps;    /* shared scans: warps that build query masks (0 = 3/8 of the block) */
   int parametric;        /* plain kernels: 1 = integer literals become launch parameters
                             (one module per plan shape, literals passed to cx_execute_params) */

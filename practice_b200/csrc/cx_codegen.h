@@ -19,8 +19,9 @@ struct Tuning {
                                // 4 per-thread shared-memory tables (<= 16 words per thread)
   int smem_group_budget = 96 * 1024;  // bytes of shared memory a group table may use
   int bitmap_budget = 48 * 1024;      // bytes of shared memory for join membership bitmaps
-  int group_merge = 0;         // 0 auto, 1 warp match-merge, 2 direct per-lane atomics,
-                               // 3 shared scans: direct per-row atomics above 32 groups only
+  int group_merge = 0;         // 0 auto, 1 warp match-merge (one expanding join: warp-uniform
+                               // expansion), 2 direct per-lane atomics, 3 shared scans: direct
+                               // per-row atomics above 32 groups only
   int wait_limit_log2 = 24;    // mbarrier poll limit before a wait gives up
   int producer_warps = 0;      // shared scans: warps that build query masks (0 = 3/8 of the block)
   int parametric = 0;          // plain kernels: literals read from CxArgs.lits at run time

@@ -66,6 +66,12 @@ typedef struct cx_tuning {
                             pipeline first reads it, 1 = vector loads of every column at the tile
                             start (default), 2 = as 1 with the next tile's loads issued a tile
                             ahead */
+  int wait_limit_us;     /* every wait of a kernel on an mbarrier gives up after this many
+                            microseconds (global timer) and raises kernel error 1 (CX_E_KERNEL
+                            from cx_ctx_sync); default 500000, range 1 .. 60000000 */
+  int debug_stall;       /* test hook for the bounded-wait path: 1 = every CTA of the scan first
+                            waits on a barrier that nothing completes, so the wait runs out
+                            (kernel error 1) with no copy in flight; 0 in normal use */
 } cx_tuning;
 
 /* Shape of a compiled query's result buffer. */
@@ -216,9 +222,11 @@ int cx_compact_sparse(const uint64_t* dev_src, uint64_t groups, uint32_t tuple_s
  * byte before a query runs.  Same output as cx_compact_sparse.  Its scratch is
  * a fixed file-scope device array of 16384 block counts (128 KiB, held by
  * every GPU that loads the library until exit), so `groups` may be at most
- * 16384 * 2048 = 33,554,432; larger inputs return CX_E_CAPACITY.  The first
- * call on a device resolves the array's address on that device, so make that
- * first call before any stream capture.  All calls share the one array: calls
+ * 16384 * 2048 = 33,554,432; larger inputs return CX_E_CAPACITY (the message
+ * in cx_last_error() names the maximum).  A call outside stream capture
+ * resolves the array's address in the current device's context; a captured
+ * call reuses the address an earlier call on that device resolved, so make the
+ * first call on a device before any stream capture.  All calls share the one array: calls
  * whose work overlaps on the GPU (other streams, other threads) race and
  * corrupt each other's results. */
 int cx_compact_sparse_noalloc(const uint64_t* dev_src, uint64_t groups, uint32_t tuple_size, uint64_t* dev_dst,

@@ -41,7 +41,8 @@ class Tuning(C.Structure):
     _fields_ = [("block_threads", C.c_int), ("items_per_thread", C.c_int), ("stages", C.c_int),
                 ("ctas_per_sm", C.c_int), ("group_placement", C.c_int), ("smem_group_budget", C.c_int),
                 ("bitmap_budget", C.c_int), ("group_merge", C.c_int), ("producer_warps", C.c_int),
-                ("parametric", C.c_int), ("prefetch", C.c_int)]
+                ("parametric", C.c_int), ("prefetch", C.c_int), ("wait_limit_us", C.c_int),
+                ("debug_stall", C.c_int)]
 
 
 class ResultInfo(C.Structure):

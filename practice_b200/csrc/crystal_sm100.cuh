@@ -739,7 +739,7 @@ namespace cx {
 // Error codes a kernel can raise in its error word (first writer wins).
 enum : unsigned int {
   ERR_NONE = 0,
-  ERR_WAIT_TIMEOUT = 1,      // an mbarrier wait exceeded its iteration limit
+  ERR_WAIT_TIMEOUT = 1,      // an mbarrier wait exceeded its time limit
   ERR_GROUP_DOMAIN = 2,      // a GROUP BY key fell outside its catalog domain
   ERR_SCRATCH = 3,           // scratch too small for the requested table
   ERR_DIM_COLLISION = 4,     // two distinct dimension keys share a slot of a shared-scan
@@ -793,16 +793,42 @@ CX_DEVICE bool mbar_try_wait_sleep(unsigned long long* bar, unsigned phase, unsi
   return ok != 0;
 }
 
-// Waits for phase `phase` of `bar`; gives up after `limit` polls.  Returns
-// false on timeout so the caller can record an error and leave.  After a few
-// quick polls each poll sleeps in the barrier (up to 2 us), so waiting warps
-// leave their issue slots to the warps that work.
-CX_DEVICE bool mbar_wait_bounded(unsigned long long* bar, unsigned phase, unsigned limit) {
-  for (unsigned it = 0; it < limit; ++it) {
-    if (it < 8 ? mbar_try_wait(bar, phase) : mbar_try_wait_sleep(bar, phase, 2000u)) return true;
-  }
-  return false;
+// Nanoseconds of the GPU's global timer.
+CX_DEVICE unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
+
+// Waits for phase `phase` of `bar`; gives up once `limit_us` microseconds
+// (global timer) have passed.  Returns false on timeout so the caller can
+// record an error and leave.  After a few quick polls each poll sleeps in the
+// barrier (up to 2 us), so waiting warps leave their issue slots to the warps
+// that work.
+CX_DEVICE bool mbar_wait_bounded(unsigned long long* bar, unsigned phase, unsigned limit_us) {
+#pragma unroll 1
+  for (int it = 0; it < 8; ++it)
+    if (mbar_try_wait(bar, phase)) return true;
+  const unsigned long long t0 = global_ns();
+  const unsigned long long lim = (unsigned long long)limit_us * 1000ULL;
+#pragma unroll 1
+  while (true) {
+    if (mbar_try_wait_sleep(bar, phase, 2000u)) return true;
+    if (global_ns() - t0 > lim) return false;
+  }
+}
+
+// Test hook of the bounded-wait error path: every thread of the CTA waits on
+// a barrier that nothing arrives at, so the wait runs out after `limit_us`
+// and thread 0 records ERR_WAIT_TIMEOUT.  Called first thing in a kernel, with
+// no copy in flight; the caller returns right after it.
+CX_DEVICE void debug_stall(unsigned long long* bar, unsigned int* err, unsigned limit_us);
+
+// Limit of the waits that collect a CTA's own bulk copies after another wait
+// gave up: never shorter than 200 ms, far above the few microseconds a copy
+// in flight needs to land, so no copy lands in shared memory after the CTA
+// has exited whatever limit the caller chose.
+CX_DEVICE unsigned drain_limit_us(unsigned limit_us) { return limit_us > 200000u ? limit_us : 200000u; }
 
 // After a staging wait gave up, waits (bounded) for the copies this warp still
 // has in flight -- local iterations k_iter .. k_iter+nstage-1 of its tile
@@ -832,13 +858,22 @@ CX_DEVICE void bulk_g2s(void* smem_dst, const void* gmem_src, unsigned bytes, un
       : "memory");
 }
 
+CX_DEVICE void debug_stall(unsigned long long* bar, unsigned int* err, unsigned limit_us) {
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (!mbar_wait_bounded(bar, 0u, limit_us) && threadIdx.x == 0) raise(err, ERR_WAIT_TIMEOUT);
+}
+
 static __device__ __noinline__ void drain_stages(unsigned long long* bars, int nstage, long long k_iter,
                                                  long long first, long long stride, long long full_tiles,
                                                  unsigned limit) {
   for (int j = 0; j < nstage; ++j) {
     const long long kk = k_iter + j;
     const long long tt = first + kk * stride;
-    if (tt < full_tiles) (void)mbar_wait_bounded(&bars[kk % nstage], (unsigned)((kk / nstage) & 1), limit);
+    if (tt < full_tiles) (void)mbar_wait_bounded(&bars[kk % nstage], (unsigned)((kk / nstage) & 1), drain_limit_us(limit));
   }
 }
 

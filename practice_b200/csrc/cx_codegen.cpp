@@ -668,7 +668,7 @@ struct Emitter {
     }
     const unsigned long long smem_total = (off + 127) & ~127ULL;
     if (smem_total > 227 * 1024) throw PlanError("scan kernel shared memory exceeds 227 KB; lower stages or items per thread");
-    const unsigned wait_limit = 1u << std::min(30, std::max(10, tu.wait_limit_log2));
+    const unsigned wait_limit = (unsigned)std::min(60000000, std::max(1, tu.wait_limit_us));
 
     const std::string kname = "Scan_" + fact;
     meta << "kernel " << kname << " scan 0 " << CTA << " " << WT << " " << smem_total << " " << tu.ctas_per_sm << "\n";
@@ -691,6 +691,8 @@ struct Emitter {
     o << "  constexpr int BLOCK_THREADS = 32, ITEMS_PER_THREAD = " << IPT << ", TILE_SIZE = " << WT << ";\n";
     o << "  constexpr int NWARP = " << NW << ", NSTAGE = " << STAGES << ", NSC = " << NSC << ";\n";
     o << "  extern __shared__ __align__(1024) unsigned char cx_smem[];\n";
+    if (tu.debug_stall)
+      o << "  { cx::debug_stall((unsigned long long*)cx_smem, a.err, " << wait_limit << "u); return; }\n";
     o << "  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
     o << "  const int tid = lane;\n";
     o << "  int* stage_buf = (int*)cx_smem + (long long)warp * " << warp_stage_ints << "LL; (void)stage_buf;\n";
@@ -2020,7 +2022,7 @@ struct SharedGen {
     if (smem_total + (unsigned long long)MAXQ * STAGES * NB * 4 > 200 * 1024)
       throw PlanError("shared scan shared memory exceeds 200 KB before group tables");
     meta << "sqb " << STAGES * NB * 4 << "\n";
-    const unsigned wait_limit = 1u << std::min(30, std::max(10, tu.wait_limit_log2));
+    const unsigned wait_limit = (unsigned)std::min(60000000, std::max(1, tu.wait_limit_us));
     const std::string kname = "SharedScan_" + fact;
     meta << "kernel " << kname << " sharedscan 0 " << CTA << " " << TR << " " << smem_total << " " << tu.ctas_per_sm << "\n";
 
@@ -2029,6 +2031,8 @@ struct SharedGen {
     o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", " << std::max(1, 1024 / CTA) << ") " << kname << "(const CxArgs a) {\n";
     o << "  constexpr int TR = " << TR << ", NSTAGE = " << STAGES << ", NSC = " << NSC << ", NPW = " << NPW << ", NCW = " << NCW << ";\n";
     o << "  extern __shared__ __align__(1024) unsigned char cx_smem[];\n";
+    if (tu.debug_stall)
+      o << "  { cx::debug_stall((unsigned long long*)cx_smem, a.err, " << wait_limit << "u); return; }\n";
     o << "  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;\n";
     o << "  int* stage_buf = (int*)(cx_smem + " << stage_off << ");\n";
     o << "  int* s_attr = (int*)(cx_smem + " << attr_off << "); (void)s_attr;\n";
@@ -2680,7 +2684,7 @@ struct SharedGen {
     o << "      const int ni = *s_nissued;\n";
     o << "      for (int kk = ni - NSTAGE < 0 ? 0 : ni - NSTAGE; kk < ni; ++kk)\n";
     o << "        if ((long long)blockIdx.x + (long long)kk * gridDim.x < full_tiles)\n";
-    o << "          (void)cx::mbar_wait_bounded(&bar_full[kk % NSTAGE], (unsigned)((kk / NSTAGE) & 1), " << LIM << ");\n";
+    o << "          (void)cx::mbar_wait_bounded(&bar_full[kk % NSTAGE], (unsigned)((kk / NSTAGE) & 1), cx::drain_limit_us(" << LIM << "));\n";
     o << "    }\n";
     o << "    return;\n";
     o << "  }\n";

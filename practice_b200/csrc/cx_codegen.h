@@ -22,12 +22,13 @@ struct Tuning {
   int group_merge = 0;         // 0 auto, 1 warp match-merge (one expanding join: warp-uniform
                                // expansion), 2 direct per-lane atomics, 3 shared scans: direct
                                // per-row atomics above 32 groups only
-  int wait_limit_log2 = 24;    // mbarrier poll limit before a wait gives up
   int producer_warps = 0;      // shared scans: warps that build query masks (0 = 3/8 of the block)
   int parametric = 0;          // plain kernels: literals read from CxArgs.lits at run time
   int prefetch = 1;            // unstaged plain scans: 0 columns loaded where first used,
                                // 1 vector loads of every column at the tile start,
                                // 2 as 1 and the next tile's loads issued one tile ahead
+  int wait_limit_us = 500000;  // a bounded mbarrier wait gives up after this many microseconds
+  int debug_stall = 0;         // test hook: 1 = every CTA first waits on a barrier nothing completes
 };
 
 // Returns the CUDA source for `plan` with its launch plan embedded as a

@@ -8,16 +8,19 @@
 #include <string>
 
 #include "../../include/crystal_b200.h"
+#include "cx_internal.h"
 #include "cx_rng.h"
 
 namespace {
 
-thread_local char g_err[512];
-
+// Every failure is recorded as the calling thread's cx_last_error().
 int cuda_fail(cudaError_t e, const char* what) {
-  snprintf(g_err, sizeof g_err, "%s: %s", what, cudaGetErrorString(e));
-  return CX_E_CUDA;
+  char buf[512];
+  snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+  return cx_internal::set_error(CX_E_CUDA, buf);
 }
+
+int invalid(const char* what) { return cx_internal::set_error(CX_E_INVALID, what); }
 
 constexpr int kCompactBlock = 256;
 constexpr int kCompactPerBlock = 2048;  // groups per block
@@ -153,11 +156,9 @@ unsigned grid_for(unsigned long long n, unsigned block) {
 
 }  // namespace
 
-extern "C" const char* cx_kernels_last_error(void) { return g_err; }
-
 extern "C" int cx_compact_sparse(const uint64_t* src, uint64_t groups, uint32_t ts, uint64_t* dst, uint64_t* dev_count,
                                  void* stream_v) {
-  if (!src || !dst || !dev_count || ts == 0) return CX_E_INVALID;
+  if (!src || !dst || !dev_count || ts == 0) return invalid("cx_compact_sparse: null buffer or zero tuple size");
   cudaStream_t s = (cudaStream_t)stream_v;
   const unsigned long long nblocks = (groups + kCompactPerBlock - 1) / kCompactPerBlock;
   if (nblocks == 0) {
@@ -190,17 +191,19 @@ static __device__ __align__(256) unsigned long long g_noalloc_block_counts[kNoAl
 
 namespace {
 std::mutex g_noalloc_mu;
-unsigned long long* g_noalloc_ptr[256] = {};  // device address of the array, per device ordinal
+unsigned long long* g_noalloc_ptr[256] = {};  // last resolved device address of the array, per device ordinal
 }  // namespace
 
 extern "C" int cx_compact_sparse_noalloc(const uint64_t* src, uint64_t groups, uint32_t ts, uint64_t* dst,
                                          uint64_t* dev_count, void* stream_v) {
-  if (!src || !dst || !dev_count || ts == 0) return CX_E_INVALID;
+  if (!src || !dst || !dev_count || ts == 0)
+    return invalid("cx_compact_sparse_noalloc: null buffer or zero tuple size");
   const unsigned long long nblocks = (groups + kCompactPerBlock - 1) / kCompactPerBlock;
   if (nblocks > kNoAllocMaxBlocks) {
-    snprintf(g_err, sizeof g_err, "cx_compact_sparse_noalloc: %llu groups exceed the fixed maximum of %llu",
+    char buf[256];
+    snprintf(buf, sizeof buf, "cx_compact_sparse_noalloc: %llu groups exceed the fixed maximum of %llu groups per call",
              (unsigned long long)groups, kNoAllocMaxBlocks * kCompactPerBlock);
-    return CX_E_CAPACITY;
+    return cx_internal::set_error(CX_E_CAPACITY, buf);
   }
   cudaStream_t s = (cudaStream_t)stream_v;
   if (nblocks == 0) {
@@ -210,17 +213,27 @@ extern "C" int cx_compact_sparse_noalloc(const uint64_t* src, uint64_t groups, u
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-  if (dev < 0 || dev >= 256) return CX_E_INVALID;
+  if (dev < 0 || dev >= 256) return invalid("cx_compact_sparse_noalloc: device ordinal out of range");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamIsCapturing");
   unsigned long long* counts = nullptr;
   {
-    // First call on a device: resolve the array's device address with that
-    // device current.  The host-side symbol itself is not a device address.
+    // The host-side symbol is not a device address: resolve the array's
+    // address in the current device's context.  Outside stream capture it is
+    // resolved on every call, so a context re-created after cudaDeviceReset
+    // (or another context made current) gets its own address; inside capture
+    // the address resolved by an earlier call on this device is used, so the
+    // first call on a device must come before any capture.
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_noalloc_block_counts);
       if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
       g_noalloc_ptr[dev] = (unsigned long long*)p;
+    } else if (!g_noalloc_ptr[dev]) {
+      return cx_internal::set_error(CX_E_INVALID,
+                                    "cx_compact_sparse_noalloc: the first call on a device must come before stream capture");
     }
     counts = g_noalloc_ptr[dev];
   }
@@ -236,7 +249,7 @@ extern "C" int cx_compact_sparse_noalloc(const uint64_t* src, uint64_t groups, u
 
 extern "C" int cx_gen_uniform(uint64_t stream, uint64_t seed, int64_t lo, int64_t hi, uint64_t row0, uint64_t rows,
                               int32_t* out, void* cuda_stream) {
-  if (!out || hi < lo || lo < INT32_MIN || hi > INT32_MAX) return CX_E_INVALID;
+  if (!out || hi < lo || lo < INT32_MIN || hi > INT32_MAX) return invalid("cx_gen_uniform: null output or bad range");
   if (rows == 0) return CX_OK;
   gen_uniform_kernel<<<grid_for(rows, 256), 256, 0, (cudaStream_t)cuda_stream>>>(
       stream, seed, lo, (unsigned long long)(hi - lo + 1), row0, rows, out);
@@ -246,7 +259,7 @@ extern "C" int cx_gen_uniform(uint64_t stream, uint64_t seed, int64_t lo, int64_
 
 extern "C" int cx_gen_datekey(uint64_t stream, uint64_t seed, uint32_t days, uint64_t row0, uint64_t rows, int32_t* out,
                               void* cuda_stream) {
-  if (!out || days == 0 || days > 36500) return CX_E_INVALID;
+  if (!out || days == 0 || days > 36500) return invalid("cx_gen_datekey: null output or bad day count");
   if (rows == 0) return CX_OK;
   gen_datekey_kernel<<<grid_for(rows, 256), 256, 0, (cudaStream_t)cuda_stream>>>(stream, seed, days, row0, rows, out);
   cudaError_t e = cudaGetLastError();
@@ -255,7 +268,7 @@ extern "C" int cx_gen_datekey(uint64_t stream, uint64_t seed, uint32_t days, uin
 
 extern "C" int cx_gen_validity(uint64_t stream, uint64_t seed, uint64_t rows, uint32_t null_permille, uint64_t* out,
                                void* cuda_stream) {
-  if (!out || null_permille > 1000) return CX_E_INVALID;
+  if (!out || null_permille > 1000) return invalid("cx_gen_validity: null output or permille above 1000");
   if (rows == 0) return CX_OK;
   gen_validity_kernel<<<grid_for((rows + 63) / 64, 256), 256, 0, (cudaStream_t)cuda_stream>>>(
       stream, seed, rows, null_permille, (unsigned long long*)out);

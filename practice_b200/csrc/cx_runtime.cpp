@@ -413,6 +413,8 @@ cx::Tuning to_tuning(const cx_tuning* tuning) {
     t.producer_warps = tuning->producer_warps;
     t.parametric = tuning->parametric;
     t.prefetch = tuning->prefetch;
+    t.wait_limit_us = tuning->wait_limit_us;
+    t.debug_stall = tuning->debug_stall;
   }
   return t;
 }
@@ -461,6 +463,8 @@ void cx_tuning_default(cx_tuning* t) {
   t->producer_warps = d.producer_warps;
   t->parametric = d.parametric;
   t->prefetch = d.prefetch;
+  t->wait_limit_us = d.wait_limit_us;
+  t->debug_stall = d.debug_stall;
 }
 
 int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap, size_t* out_len) {

@@ -18,11 +18,12 @@ from __future__ import annotations
 
 import csv
 import json
+import os
 import re
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+REF = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CRYSTAL_REFERENCE", "/root/reference"))
 OUT = Path(__file__).resolve().parent / "reference_kats.json"
 
 

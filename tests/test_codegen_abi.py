@@ -258,3 +258,27 @@ def test_parametric_plain_codegen_takes_literals_at_launch():
     with pytest.raises(_lib.CxError) as e:
         ctx.execute(m, 0, [1, 2])  # wrong literal count fails before touching a GPU
     assert e.value.code == -1
+
+
+def test_bounded_wait_limit_and_stall_hook_reach_the_generated_kernels():
+    """Waits are bounded by time (500 ms unless the tuning says otherwise);
+    the stall hook is emitted only when asked for, in plain and shared scans."""
+    t = _lib.default_tuning()
+    assert t.wait_limit_us == 500_000 and t.debug_stall == 0
+    plan = queries.ssb_q31()
+    t.block_threads, t.stages = 256, 3
+    src = _lib.codegen(plan.text(), t)
+    assert "debug_stall" not in src and "500000u" in src
+    t.wait_limit_us, t.debug_stall = 20_000, 1
+    src = _lib.codegen(plan.text(), t)
+    assert "cx::debug_stall((unsigned long long*)cx_smem, a.err, 20000u); return;" in src
+    _lib.Module(src, key="stall_plain")
+    rng = random.Random(5)
+    shapes = [queries.template(k, rng).text() for k in range(4)]
+    t2 = _lib.default_tuning()
+    t2.block_threads, t2.items_per_thread, t2.stages, t2.ctas_per_sm = 1024, 1, 3, 1
+    assert "debug_stall" not in _lib.shared_codegen(shapes, t2)
+    t2.wait_limit_us, t2.debug_stall = 20_000, 1
+    src = _lib.shared_codegen(shapes, t2)
+    assert "cx::debug_stall(" in src and "cx::drain_limit_us(" in src
+    _lib.Module(src, key="stall_shared")

@@ -3,19 +3,25 @@
 Workload (the headline metric's configuration): 8 int32 fact columns
 (orderdate, custkey, suppkey, partkey, quantity, discount, revenue, supplycost;
 19.2 GB resident in HBM) with the SSB-shaped date / customer / supplier / part
-dimensions, and batches of queries drawn by seed from four templates (T0 range
-filters + scalar SUM; T1 date join + GROUP BY year; T2 three joins + GROUP BY
-(nation, year); T3 four joins + GROUP BY (brand, year)).  Synthetic data,
-generated on the device from a counter-based hash (practice_b200/datagen.py).
+dimensions, and batches of 16, 32 or 64 queries drawn by seed from four
+templates (T0 range filters + scalar SUM; T1 date join + GROUP BY year; T2
+three joins + GROUP BY (nation, year); T3 four joins + GROUP BY (brand,
+year)).  Synthetic data, generated on the device from a counter-based hash
+(practice_b200/datagen.py).
 
-One step = one batch of queries over the whole fact table.  ``--mode plain``
-runs the batch one query at a time with the plain fused kernels (the drop-in
-path); ``--mode shared`` runs it as one shared-scan launch.  The JSON line
-reports queries/s of the whole job, per-query latency percentiles, the
-roofline of the dominant kernel against measured HBM bandwidth, the CPU
-baseline (the reference's own primitives compiled for the host, timed on a
-bounded row sample), clocks sampled during the timed region and the end-to-end
-figure through the public API (result read back to the host each query).
+One step = one batch of queries over the whole fact table.  The headline
+(`value`) is the 32-query batch answered by one shared-scan launch; the same
+queries as plain fused kernels one after another (the drop-in path) are timed
+beside it, and both are timed at 16 and 64 queries too.  The JSON line also
+carries: the roofline of the dominant kernel against the measured HBM
+bandwidth; the CPU baseline (the reference's own primitives compiled for the
+host, over the whole 600M-row table) whose results double as the parity check
+of every GPU answer of the run; the plain single-query workloads at their own
+sizes (6M-row SSB Q1.1 shape, 60M-row Q3.1 shape and its nullable variant),
+each with kernel time, roofline, end-to-end rate, the reference CPU path at
+full size and a bit-exact check; clocks sampled during the timed region; the
+end-to-end figure through the public API; and the serving loop under Poisson
+arrivals.
 
 Multi-GPU (torchrun): every rank holds its own 600M-row table and runs its own
 batch (independent replicas, no collective on the data path); value sums the
@@ -38,9 +44,10 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "queries/s + p50/p99 ms, shared-scan vs plain, 600M-row fact; % of HBM peak"
 FALLBACK_HBM_GBS = 6650.0
+DIM_ROWS = {"CUSTOMER": 300_000, "SUPPLIER": 20_000, "DDATE": 2556, "PART": 200_000}
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -48,15 +55,19 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="shared", choices=["plain", "shared"])
     ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--batch-sizes", default="16,32,64", help="shared-scan batches timed beside the headline")
     ap.add_argument("--rows", type=int, default=600_000_000)
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--cpu-sample-rows", type=int, default=4_000_000)
+    ap.add_argument("--cpu-sample-rows", type=int, default=40_000_000,
+                    help="rows of each reference-arm step (a bounded sample of the table)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the 6M / 60M single-query legs")
+    ap.add_argument("--config-rows", default="6000000,60000000", help="rows of the Q1.1 leg and the Q3.1 legs")
     ap.add_argument("--serve-rate", type=float, default=1000.0, help="Poisson arrivals per second (serving leg)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests in the serving leg (0 skips it)")
     ap.add_argument("--serve-low-rate", type=float, default=100.0, help="second, light-load arrival rate")
     ap.add_argument("--serve-slots", type=int, default=1, help="launches in flight in the shared loop")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 def peaks():
@@ -162,51 +173,395 @@ def job_rate(units_per_rank: float, world: int, max_ms: float) -> float:
     return units_per_rank * world / (max_ms / 1000.0)
 
 
+def pct(xs, q):
+    import numpy as np
+    return float(np.percentile(xs, q)) if len(xs) else None
+
+
 # ------------------------------------------------------------- CPU baseline
 
 
-def cpu_baseline(plans_full, args, batch_rows: int):
-    """The reference's CPU path on a bounded row sample of the same batch.
-
-    Uses oracle/_ref (the reference's own crystal primitives compiled for the
-    host with OpenMP) when it was built, else the oracle restatement."""
-    import numpy as np
-
-    from oracle import refbase
-    from practice_b200 import datagen, queries
-
-    n = min(args.cpu_sample_rows, batch_rows)
-    ht = datagen.host_tables(args.seed, n, queries.BATCH_COLS)
-    plans = queries.batch(args.batch, args.seed, n)
-    t, kind, cores = refbase.time_batch(plans, ht, n)
-    scale = batch_rows / n
-    qps = len(plans) / (t * scale)
-    return {"value": qps, "unit": "queries/s", "cores": cores, "kind": kind,
-            "sample": f"{len(plans)}-query batch on the first {n:,} of {batch_rows:,} fact rows, "
-                      f"time scaled by {scale:.0f}x to the full table ({t:.3f} s measured)"}
-
-
 def reference_arm(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    """The reference's CPU path (its own crystal primitives compiled for the
+    host with OpenMP, oracle/_ref; the oracle restatement where that library
+    was not built) on the headline batch, each step a bounded row sample of
+    the fact table, rate scaled to the whole table."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from oracle import refbase
+    from practice_b200 import datagen, queries
+
+    n = min(args.cpu_sample_rows, args.rows)
+    ht = datagen.host_tables(args.seed, n, queries.BATCH_COLS)
+    plans = queries.batch(args.batch, args.seed, n)
     times = []
-    cb = None
+    kind = cores = None
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(None, args, args.rows)
+        t, kind, cores = refbase.time_batch(plans, ht, n)
         if i >= args.warmup:
-            times.append(cb["value"])
-    v = statistics.median(times)
+            times.append(t)
+    t = statistics.median(times)
+    scale = args.rows / n
+    v = len(plans) / (t * scale)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": args.batch / v * 1000.0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": len(plans) / v * 1000.0,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/u64",
         "data": "synthetic", "config": config_block(args),
-        "cpu_baseline": {**cb, "value": v},
+        "cpu_baseline": {"value": v, "unit": "queries/s", "cores": cores, "kind": kind,
+                         "sample": f"{len(plans)}-query batch on the first {n:,} of {args.rows:,} fact rows per step, "
+                                   f"median {t:.3f} s scaled by {scale:.0f}x to the full table"},
         "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def config_block(args):
+    return {"workload": "batched star-join queries from 4 templates over a 600M-row, 8-column int32 fact table",
+            "fact_rows": args.rows, "fact_columns": 8, "batch_queries": args.batch, "mode": args.mode,
+            "seed": args.seed, "parallelism": f"replicas{args.gpus}",
+            "l2": "inputs (19.2 GB) larger than L2 (126 MB); no flush needed"}
+
+
+# ------------------------------------------------------------------ GPU arm
+
+# DRAM bytes (read + write) per fact row of one shared-scan launch over the
+# 8-column batch table: ncu (dram__bytes_read.sum + dram__bytes_write.sum) of
+# one 30M-row launch of the 32-query batch, 972.2 MB; the traffic of a launch
+# grows with its rows.
+SHARED_DRAM_BYTES_PER_ROW = (968.458240e6 + 3.693568e6) / 30e6
+
+PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=bm,
+                         prefetch=pf, group_placement=pl)
+                    for bt, ipt, st, bm, pf, pl in ((1024, 4, 0, 49152, 1, 0), (1024, 4, 0, 0, 1, 4),
+                                                    (512, 2, 0, 0, 1, 4), (1024, 2, 0, 0, 0, 4),
+                                                    (512, 8, 4, 0, 0, 0))]
+SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=2, producer_warps=pw,
+                          group_merge=gm)
+                     for bt, ipt, st, pw, gm in ((1024, 1, 3, 11, 0), (1024, 1, 3, 11, 3), (1024, 1, 3, 14, 0),
+                                                 (1024, 1, 3, 14, 3), (512, 2, 2, 5, 0), (512, 2, 2, 7, 3))]
+
+
+def bound_ctx(db, module, res, val):
+    """A C-ABI execution context bound to the database's tables and one result buffer."""
+    from practice_b200 import _lib
+
+    c = _lib.ExecCtx()
+    for name, t in db.cols.items():
+        c.set_buffer("d_" + name, t.data_ptr(), t.numel())
+    for name, t in db.valid.items():
+        c.set_null_bitmap("d_" + name, t.data_ptr(), t.numel())
+    for t, n in db.rows.items():
+        c.set_rows(t, n)
+    c.set_result(res.data_ptr(), res.numel(), val.data_ptr(), val.numel())
+    return c
+
+
+def result_words(res, val, final_words):
+    import numpy as np
+    w = res.cpu().numpy().view(np.uint64)[:final_words].copy()
+    v = val.cpu().numpy().view(np.uint64)[: (final_words + 63) // 64].copy()
+    return w, v
+
+
+def plain_leg(torch, db, plans, stream, args, pg, device):
+    """Every plan as its autotuned plain fused kernel, one after another.
+    Returns the timing summary, per-step per-query durations and results."""
+    for p in plans:
+        if db.tuning_for(p) is None:
+            db.autotune(p, candidates=PLAIN_CANDIDATES, reps=1, persist=False)
+    mods = [db.compile(p, db.tuning_for(p)) for p in plans]
+    bufs = [db.alloc_result(m) for m in mods]
+    ctxs = [bound_ctx(db, m, r, v) for m, (r, v) in zip(mods, bufs)]
+
+    def step():
+        evs = []
+        for m, c in zip(mods, ctxs):
+            c.execute(m, stream.cuda_stream)
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(stream)
+            evs.append(ev)
+        return evs
+
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+    for c in ctxs:
+        c.sync()
+    barrier(pg, device)
+    starts, marks = [], []
+    for _ in range(args.steps):
+        s0 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        starts.append(s0)
+        marks.append(step())
+    stream.synchronize()
+    scan_ms = []
+    for c in ctxs:
+        c.sync()
+        scan_ms.append(c.timing().scan_ms)
+    launches = sum(c.timing().gpu_launches for c in ctxs)
+    # durations[s][i]: query i of step s, from the previous query's end
+    durations = []
+    for s0, evs in zip(starts, marks):
+        prev, d = s0, []
+        for ev in evs:
+            d.append(prev.elapsed_time(ev))
+            prev = ev
+        durations.append(d)
+    results = [result_words(r, v, int(m.info.final_words)) for m, (r, v) in zip(mods, bufs)]
+    for c in ctxs:
+        c.close()
+    return {"scan_ms": scan_ms, "durations": durations, "launches_per_step": launches,
+            "tunings": [db.tuning_for(p) for p in plans]}, results
+
+
+def plain_summary(pl, plans, b, args, world, pg, device, peak):
+    import numpy as np
+    per_step = [sum(d[:b]) for d in pl["durations"]]
+    ms = max_over_ranks(pg, sum(per_step), device)
+    lat = [sum(d[: i + 1]) for d in pl["durations"] for i in range(b)]
+    byts = sum(len(p.columns_read()) * 4 * args.rows for p in plans[:b])
+    scan_s = sum(pl["scan_ms"][:b]) / 1000.0
+    return {"queries_per_s": job_rate(b * args.steps, world, ms), "ms_per_step": ms / args.steps,
+            "p50_ms": statistics.median(lat), "p99_ms": pct(lat, 99),
+            "scan_GBps": byts / scan_s / 1e9, "scan_frac_of_peak": byts / scan_s / 1e9 / peak,
+            "scan_ms": {"mean": float(np.mean(pl["scan_ms"][:b])), "min": min(pl["scan_ms"][:b]),
+                        "max": max(pl["scan_ms"][:b])}}
+
+
+def shared_leg(torch, db, plans, stream, args, pg, device, sample_clocks: bool):
+    """The batch as one shared-scan launch per step (autotuned launch shape)."""
+    from practice_b200 import _lib
+
+    if db.shared_tuning_for(plans) is None:
+        db.autotune_shared(plans, SHARED_CANDIDATES, reps=1)
+    tun = db.shared_tuning_for(plans)
+    prog = db.shared_program(plans, tun)
+    squeries, sparams, sbufs = db.shared_prepare(prog, plans)
+    sctx = db.ctx
+    for t, n in db.rows.items():
+        sctx.set_rows(t, n)
+
+    def step():
+        sctx.shared_execute(prog.module, squeries, sparams, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    sctx.sync()
+    barrier(pg, device)
+    sampler = None
+    if sample_clocks:
+        sampler = ClockSampler(device.index)
+        sampler.start()
+        time.sleep(0.3)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    scan = []
+    start.record(stream)
+    for _ in range(args.steps):
+        step()
+    end.record(stream)
+    end.synchronize()
+    clocks = sampler.stop() if sampler else None
+    sctx.sync()
+    ms = max_over_ranks(pg, start.elapsed_time(end), device)
+    tm = sctx.timing()
+    scan.append(tm.scan_ms)
+    results = [result_words(r, v, words) for r, v, words in sbufs]
+    return {"ms_per_step": ms / args.steps, "scan_ms": tm.scan_ms, "launches_per_step": tm.gpu_launches,
+            "graph": tm.graph, "tuning": {k: getattr(tun, k) for k, _ in _lib.Tuning._fields_} if tun else None,
+            "prog": prog, "squeries": squeries, "sparams": sparams, "sbufs": sbufs, "clocks": clocks}, results
+
+
+def e2e_shared(torch, db, plans, sh, stream, args, world):
+    """The batch end to end through the public API: the query descriptors and
+    literals uploaded, the shared scan, and every query's result and validity
+    words read back to pinned host memory, each step."""
+    sctx = db.ctx
+    sbufs = sh["sbufs"]
+    pinned = [torch.empty(r.numel(), dtype=torch.int64, pin_memory=True) for r, _, _ in sbufs]
+    pinned_v = [torch.empty(v.numel(), dtype=torch.int64, pin_memory=True) for _, v, _ in sbufs]
+    h2d = len(sh["squeries"]) * 40 + len(sh["sparams"]) * 4
+    d2h = sum(p.numel() * 8 + q.numel() * 8 for p, q in zip(pinned, pinned_v))
+    steps = max(2, args.steps)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        prog = db.shared_program(plans, db.shared_tuning_for(plans))
+        sctx.shared_execute(prog.module, sh["squeries"], sh["sparams"], stream.cuda_stream)
+        for i, (r, v, _) in enumerate(sbufs):
+            pinned[i].copy_(r, non_blocking=True)
+            pinned_v[i].copy_(v, non_blocking=True)
+        stream.synchronize()
+    e2e_s = time.perf_counter() - t0
+    return {"value": len(plans) * steps * world / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h),
+            "note": "fact table resident in HBM; query descriptors uploaded and every result read back each step"}
+
+
+def compare(results, accs, validity: bool = False):
+    """Indexes of GPU result buffers that differ from the combined CPU results
+    (result words always; validity words too when the checker computes them)."""
+    import numpy as np
+    bad = []
+    for i, ((w, v), a) in enumerate(zip(results, accs)):
+        fw = len(w)
+        if not np.array_equal(w, a.words[:fw]) or (validity and not np.array_equal(v, a.validity[: (fw + 63) // 64])):
+            bad.append(i)
+    return bad
+
+
+def batch_cpu_and_parity(db, plans_all, plain_results, shared_results, args):
+    """The reference's CPU path over the whole 600M-row table (range by range,
+    copied back from the device) for every query of the largest batch: its
+    time is the CPU baseline of the headline batch, its results check every
+    GPU answer of the run."""
+    from oracle import chunked, refharness
+    from practice_b200 import queries
+
+    dims, _, dim_rows = chunked.device_dims(db)
+    fetch = chunked.device_fetch(db, queries.BATCH_COLS)
+    if refharness.available():
+        accs, spent, cores = chunked.run_reference(plans_all, fetch, args.rows, dims, dim_rows,
+                                                   chunk_rows=25_000_000)
+        kind = "reference"
+        head_s = sum(a.seconds for a in accs[: args.batch])
+    else:
+        head, spent, cores = chunked.run_oracle(plans_all[: args.batch], fetch, args.rows, dims, {}, dim_rows,
+                                                chunk_rows=25_000_000)
+        rest, _, _ = chunked.run_oracle(plans_all[args.batch:], fetch, args.rows, dims, {}, dim_rows,
+                                        chunk_rows=25_000_000) if len(plans_all) > args.batch else ([], 0, 0)
+        accs = head + rest
+        kind = "port"
+        head_s = spent
+    parity = {"checker": "reference primitives (oracle/_ref)" if kind == "reference" else "oracle restatement",
+              "fact_rows": args.rows, "queries": len(plans_all)}
+    bad_plain = compare(plain_results, accs, validity=kind == "port")
+    parity["plain_bit_exact"] = not bad_plain
+    for b, res in shared_results.items():
+        bad = compare(res, accs[:b], validity=kind == "port")
+        parity[f"shared_{b}_bit_exact"] = not bad
+        if bad:
+            parity[f"shared_{b}_mismatch"] = bad[:8]
+    if bad_plain:
+        parity["plain_mismatch"] = bad_plain[:8]
+    parity["bit_exact"] = all(v for k, v in parity.items() if k.endswith("bit_exact"))
+    cb = {"value": args.batch / head_s, "unit": "queries/s", "cores": cores, "kind": kind,
+          "sample": f"the whole {args.rows:,}-row table in 25M-row ranges, the {args.batch}-query batch "
+                    f"({head_s:.1f} s inside the reference calls; no extrapolation)"}
+    return cb, parity
+
+
+# ----------------------------------------------------- single-query configs
+
+
+def config_leg(torch, name, plan_fn, rows, cols, nulls, args, device, peak, stream):
+    """One plain fused query at its own table size: kernel time and roofline,
+    end to end through the C ABI with the result read back, the reference's
+    CPU path over the whole table, and a bit-exact check of the GPU result."""
+    import numpy as np
+
+    from oracle import chunked, refharness
+    from practice_b200.engine import Database
+
+    db = Database(device.index)
+    db.generate_ssb(rows, args.seed, cols, nulls=nulls)
+    plan = plan_fn(rows)
+    db.autotune(plan, candidates=PLAIN_CANDIDATES, reps=2, persist=False)
+    tun = db.tuning_for(plan)
+    m = db.compile(plan, tun)
+    res, val = db.alloc_result(m)
+    ctx = bound_ctx(db, m, res, val)
+    for _ in range(max(3, args.warmup)):
+        ctx.execute(m, stream.cuda_stream)
+    ctx.sync()
+    scan, total = [], []
+    reps = max(10, args.steps)
+    for _ in range(reps):
+        ctx.execute(m, stream.cuda_stream)
+        ctx.sync()
+        t = ctx.timing()
+        scan.append(t.scan_ms)
+        total.append(t.total_ms)
+    launches = ctx.timing().gpu_launches
+    fw = int(m.info.final_words)
+    got = result_words(res, val, fw)
+    # End to end: execute + result and validity words to pinned host memory.
+    pin = torch.empty(res.numel(), dtype=torch.int64, pin_memory=True)
+    pin_v = torch.empty(val.numel(), dtype=torch.int64, pin_memory=True)
+    torch.cuda.synchronize()
+    e2e = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        ctx.execute(m, stream.cuda_stream)
+        pin.copy_(res, non_blocking=True)
+        pin_v.copy_(val, non_blocking=True)
+        stream.synchronize()
+        e2e.append(time.perf_counter() - t0)
+    ctx.close()
+    nullable_read = [c for c in plan.columns_read() if c in (nulls or {})]
+    byts = len(plan.columns_read()) * 4 * rows + len(nullable_read) * rows / 8
+    scan_s = statistics.median(scan) / 1000.0
+    # The reference's CPU path over the whole table, from the device-resident rows.
+    dims, dval, dim_rows = chunked.device_dims(db)
+    fetch = chunked.device_fetch(db, cols)
+    try:
+        if refharness.available() and not nulls:
+            (acc,), cpu_s, cores = chunked.run_reference([plan], fetch, rows, dims, dim_rows,
+                                                          chunk_rows=30_000_000)
+            kind = "reference"
+        else:
+            (acc,), cpu_s, cores = chunked.run_oracle([plan], fetch, rows, dims, dval, dim_rows,
+                                                       chunk_rows=30_000_000)
+            kind = "port"
+        exact = not compare([got], [acc], validity=kind == "port")
+        cpu = {"value": 1.0 / cpu_s, "unit": "queries/s", "rows_per_s": rows / cpu_s, "cores": cores, "kind": kind,
+               "sample": f"the whole {rows:,}-row table"}
+    except Exception as e:  # reported, not fatal
+        exact, cpu = None, {"error": str(e)[:200]}
+    db.reset()
+    del db
+    torch.cuda.empty_cache()
+    gpu_qps = 1000.0 / statistics.median(total)
+    return {"workload": name, "fact_rows": rows, "columns_read": len(plan.columns_read()),
+            "scan_ms": {"median": statistics.median(scan), "min": min(scan)},
+            "query_ms": statistics.median(total),
+            "rows_per_s": rows / scan_s,
+            "queries_per_s": gpu_qps,
+            "roofline": {"bound": "hbm", "achieved": byts / scan_s / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": byts / scan_s / 1e9 / peak, "algorithmic_bytes": byts},
+            "e2e": {"value": 1.0 / statistics.median(e2e), "unit": "queries/s",
+                    "rows_per_s": rows / statistics.median(e2e), "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(res.numel() * 8 + val.numel() * 8)},
+            "gpu_launches_per_query": launches,
+            "tuning": {k: getattr(tun, k) for k in ("block_threads", "items_per_thread", "stages", "group_placement",
+                                                     "bitmap_budget", "prefetch")} if tun else None,
+            "cpu_baseline": cpu,
+            "gpu_vs_cpu": (rows / scan_s) / cpu["rows_per_s"] if "rows_per_s" in cpu else None,
+            "parity": {"bit_exact": exact, "checker": cpu.get("kind")}}
+
+
+def configs_legs(torch, args, device, peak, stream):
+    from practice_b200 import queries
+
+    q11_rows, q31_rows = (int(x) for x in args.config_rows.split(","))
+    return {
+        "q11_6M": config_leg(torch, "SSB Q1.1 shape: date join (year = 1995), discount in [2,4], quantity < 30, "
+                                    "SUM(extendedprice*discount)", queries.ssb_q11, q11_rows, queries.Q11_COLS,
+                             None, args, device, peak, stream),
+        "q31_60M": config_leg(torch, "SSB Q3.1 shape: customer/supplier/date joins, GROUP BY (c_nation, s_nation, "
+                                     "d_year), SUM(revenue)", queries.ssb_q31, q31_rows, queries.Q31_COLS, None,
+                              args, device, peak, stream),
+        "q31_nullable_60M": config_leg(torch, "nullable Q3.1: 10% NULL revenue, 5% NULL c_city, IS [NOT] NULL, "
+                                              "COUNT(*), COUNT(revenue), SUM(revenue)", queries.ssb_q31_nullable,
+                                       q31_rows, queries.Q31_COLS, {"lo_revenue": 100, "c_city": 50}, args,
+                                       device, peak, stream),
+    }
+
+
+# -------------------------------------------------------------- serving
 
 
 def serving_leg(db, plans, args, shared_tuning):
@@ -280,50 +635,7 @@ def serving_leg(db, plans, args, shared_tuning):
                            "plain_p99_vs_lone": plain_low["p99_ms"] / lone_ms}}
 
 
-def config_block(args):
-    return {"workload": "batched star-join queries from 4 templates over a 600M-row, 8-column int32 fact table",
-            "fact_rows": args.rows, "fact_columns": 8, "batch_queries": args.batch, "mode": args.mode,
-            "seed": args.seed, "parallelism": f"replicas{args.gpus}",
-            "l2": "inputs (19.2 GB) larger than L2 (126 MB); no flush needed"}
-
-
-# ------------------------------------------------------------------ GPU arm
-
-# DRAM bytes (read + write) per fact row of one shared-scan launch over the
-# 8-column batch table, from the ncu capture in
-# profiles/SharedScan_LINEORDER_batch32_30M.md (972.2 MB for 30M rows); the
-# traffic of a launch grows with its rows.
-SHARED_DRAM_BYTES_PER_ROW = (968.458240e6 + 3.693568e6) / 30e6
-
-PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=bm,
-                         prefetch=pf, group_placement=pl)
-                    for bt, ipt, st, bm, pf, pl in ((1024, 4, 0, 49152, 1, 0), (1024, 4, 0, 0, 1, 4),
-                                                    (512, 2, 0, 0, 1, 4), (1024, 2, 0, 0, 0, 4),
-                                                    (512, 8, 4, 0, 0, 0))]
-SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=2, producer_warps=pw,
-                          group_merge=gm)
-                     for bt, ipt, st, pw, gm in ((1024, 1, 3, 11, 0), (1024, 1, 3, 11, 3), (1024, 1, 3, 14, 0),
-                                                 (1024, 1, 3, 14, 3), (512, 2, 2, 5, 0), (512, 2, 2, 7, 3))]
-
-
-def time_steps(torch, stream, steps, run_step, sampler=None):
-    """CUDA-event time of `steps` calls of run_step on `stream` (ms), plus the
-    per-step start events and per-query completion events it records."""
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    step_start = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-    marks = []
-    start.record(stream)
-    for s in range(steps):
-        step_start[s].record(stream)
-        marks.append(run_step())
-    end.record(stream)
-    end.synchronize()
-    lat = []
-    for s in range(steps):
-        for ev in marks[s]:
-            lat.append(step_start[s].elapsed_time(ev))
-    return start.elapsed_time(end), lat
+# ----------------------------------------------------------------- main
 
 
 def main():
@@ -331,147 +643,59 @@ def main():
     if args.impl == "reference":
         reference_arm(args)
         return
-    import numpy as np
     import torch
 
-    from practice_b200 import _lib, queries
+    from practice_b200 import queries
     from practice_b200.engine import Database
 
     world, rank, local, pg = dist_setup(args.gpus)
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    peak, peak_kind = peaks()
+    stream = torch.cuda.Stream(device)
+    sizes = sorted({int(x) for x in args.batch_sizes.split(",") if x} | {args.batch})
+    nmax = max(sizes)
+
+    # Single-query workloads first, each on its own table (freed afterwards).
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        configs = configs_legs(torch, args, device, peak, stream)
+
     db = Database(local)
     db.generate_ssb(args.rows, args.seed + rank, queries.BATCH_COLS)
-    plans = queries.batch(args.batch, args.seed, args.rows)
-    stream = torch.cuda.Stream(device)
-    peak, peak_kind = peaks()
+    plans_all = queries.batch(nmax, args.seed, args.rows)  # smaller batches are its prefixes
+    plans = plans_all[: args.batch]
     union_cols = sorted({c for p in plans for c in p.columns_read()})
 
     # ---- plain path: one fused kernel per query, one query after another
-    for p in plans:
-        if db.tuning_for(p) is None:
-            db.autotune(p, candidates=PLAIN_CANDIDATES, reps=1, persist=False)
-    mods = [db.compile(p, db.tuning_for(p)) for p in plans]
-    results = [db.alloc_result(m) for m in mods]
-    ctxs = []
-    for m, (res, val) in zip(mods, results):
-        c = _lib.ExecCtx()
-        for name, t in db.cols.items():
-            c.set_buffer("d_" + name, t.data_ptr(), t.numel())
-        for t, n in db.rows.items():
-            c.set_rows(t, n)
-        c.set_result(res.data_ptr(), res.numel(), val.data_ptr(), val.numel())
-        ctxs.append(c)
+    pl, plain_results = plain_leg(torch, db, plans_all, stream, args, pg, device)
+    plain = plain_summary(pl, plans_all, args.batch, args, world, pg, device, peak)
+    plain_by_batch = {b: plain_summary(pl, plans_all, b, args, world, pg, device, peak) for b in sizes}
 
-    def plain_step():
-        evs = []
-        for m, c in zip(mods, ctxs):
-            c.execute(m, stream.cuda_stream)
-            ev = torch.cuda.Event(enable_timing=True)
-            ev.record(stream)
-            evs.append(ev)
-        return evs
-
-    for _ in range(args.warmup):
-        plain_step()
-    stream.synchronize()
-    for c in ctxs:
-        c.sync()
-    barrier(pg, device)
-    plain_ms, plain_lat = time_steps(torch, stream, args.steps, plain_step)
-    for c in ctxs:
-        c.sync()
-    plain_scan_ms = [c.timing().scan_ms for c in ctxs]
-    plain_launches = sum(c.timing().gpu_launches for c in ctxs)
-    plain_ms = max_over_ranks(pg, plain_ms, device)
-    plain_bytes = sum(len(p.columns_read()) * 4 * args.rows for p in plans)
-    plain = {"queries_per_s": job_rate(len(plans) * args.steps, world, plain_ms),
-             "ms_per_step": plain_ms / args.steps,
-             "p50_ms": statistics.median(plain_lat), "p99_ms": float(np.percentile(plain_lat, 99)),
-             "scan_GBps": plain_bytes / (sum(plain_scan_ms) / 1000.0) / 1e9,
-             "scan_frac_of_peak": plain_bytes / (sum(plain_scan_ms) / 1000.0) / 1e9 / peak,
-             "scan_ms": {"mean": statistics.mean(plain_scan_ms), "min": min(plain_scan_ms), "max": max(plain_scan_ms)}}
-
-    # ---- shared scan: the whole batch in one persistent kernel
-    shared = None
-    sctx = db.ctx
-    if args.mode == "shared" and all(db.shareable(p) for p in plans):
-        if db.shared_tuning_for(plans) is None:
-            db.autotune_shared(plans, SHARED_CANDIDATES, reps=1)
-        tun = db.shared_tuning_for(plans)
-        prog = db.shared_program(plans, tun)
-        squeries, sparams, sbufs = db.shared_prepare(prog, plans)
-        for t, n in db.rows.items():
-            sctx.set_rows(t, n)
-
-        def shared_step():
-            sctx.shared_execute(prog.module, squeries, sparams, stream.cuda_stream)
-            ev = torch.cuda.Event(enable_timing=True)
-            ev.record(stream)
-            return [ev] * len(plans)
-
-        for _ in range(args.warmup):
-            shared_step()
-        sctx.sync()
-        barrier(pg, device)
-        sampler = ClockSampler(local)
-        sampler.start()
-        time.sleep(0.3)
-        shared_ms, shared_lat = time_steps(torch, stream, args.steps, shared_step)
-        clocks = sampler.stop()
-        sctx.sync()
-        scan_ms = sctx.timing().scan_ms
-        shared_ms = max_over_ranks(pg, shared_ms, device)
-        shared_bytes = len(union_cols) * 4 * args.rows
-        shared = {"ms_per_step": shared_ms / args.steps, "scan_ms": scan_ms, "bytes": shared_bytes,
-                  "lat": shared_lat, "launches": sctx.timing().gpu_launches,
-                  "tuning": {k: getattr(tun, k) for k, _ in _lib.Tuning._fields_} if tun else None}
-    else:
-        sampler = ClockSampler(local)
-        sampler.start()
-        time.sleep(0.3)
-        _, _ = time_steps(torch, stream, 1, plain_step)
-        clocks = sampler.stop()
-        for c in ctxs:
-            c.sync()
-    barrier(pg, device)
-
-    # ---- end to end through the public API: per-step descriptor upload and
-    # every query's result read back to pinned host memory
-    e2e_steps = max(2, args.steps)
+    # ---- shared scan: each batch in one persistent kernel; the headline batch last (clocks sampled)
+    shared_all, shared_results = {}, {}
+    if args.mode == "shared" and all(db.shareable(p) for p in plans_all):
+        for b in [s for s in sizes if s != args.batch] + [args.batch]:
+            sh, res = shared_leg(torch, db, plans_all[:b], stream, args, pg, device, sample_clocks=b == args.batch)
+            shared_all[b] = sh
+            shared_results[b] = res
+    shared = shared_all.get(args.batch)
     if shared is not None:
-        pinned = [torch.empty(r.numel(), dtype=torch.int64, pin_memory=True) for r, _, _ in sbufs]
-        pinned_v = [torch.empty(v.numel(), dtype=torch.int64, pin_memory=True) for _, v, _ in sbufs]
-        h2d = len(squeries) * 40 + len(sparams) * 4
-        d2h = sum(p.numel() * 8 + q.numel() * 8 for p, q in zip(pinned, pinned_v))
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            prog2 = db.shared_program(plans, db.shared_tuning_for(plans))
-            q2, p2, _ = squeries, sparams, None
-            sctx.shared_execute(prog2.module, q2, p2, stream.cuda_stream)
-            for i, (r, v, _) in enumerate(sbufs):
-                pinned[i].copy_(r, non_blocking=True)
-                pinned_v[i].copy_(v, non_blocking=True)
-            stream.synchronize()
-        e2e_s = time.perf_counter() - t0
+        clocks = shared["clocks"]
     else:
-        pinned = [torch.empty(r.numel(), dtype=torch.int64, pin_memory=True) for r, _ in results]
-        pinned_v = [torch.empty(v.numel(), dtype=torch.int64, pin_memory=True) for _, v in results]
-        h2d = 0
-        d2h = sum(p.numel() * 8 + q.numel() * 8 for p, q in zip(pinned, pinned_v))
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            for i, (m, c) in enumerate(zip(mods, ctxs)):
-                c.execute(db.compile(plans[i], db.tuning_for(plans[i])), stream.cuda_stream)
-                pinned[i].copy_(results[i][0], non_blocking=True)
-                pinned_v[i].copy_(results[i][1], non_blocking=True)
-            stream.synchronize()
-        e2e_s = time.perf_counter() - t0
-    e2e = {"value": len(plans) * e2e_steps * world / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(d2h),
-           "note": "fact table resident in HBM; query descriptors uploaded and every result read back each step"}
+        sampler = ClockSampler(local)
+        sampler.start()
+        time.sleep(0.3)
+        plain_leg(torch, db, plans, stream, args, pg, device)
+        clocks = sampler.stop()
+    barrier(pg, device)
+
+    # ---- end to end through the public API
+    if shared is not None:
+        e2e = e2e_shared(torch, db, plans, shared, stream, args, world)
+    else:
+        e2e = {"value": plain["queries_per_s"], "unit": "queries/s", "h2d_bytes_per_step": 0,
+               "d2h_bytes_per_step": 0, "note": "plain mode: results stay on the device"}
 
     serving = None
     if rank == 0 and world == 1 and args.serve_requests > 0 and shared is not None:
@@ -480,10 +704,10 @@ def main():
         except Exception as e:  # reported, not fatal
             serving = {"error": str(e)[:300]}
 
-    cb = None
+    cb, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cb = cpu_baseline(plans, args, args.rows)
+            cb, parity = batch_cpu_and_parity(db, plans_all, plain_results, shared_results, args)
         except Exception as e:  # reported, not fatal
             cb = {"value": None, "unit": "queries/s", "error": str(e)[:200]}
 
@@ -491,36 +715,51 @@ def main():
         if shared is not None:
             value = job_rate(len(plans) * args.steps, world, shared["ms_per_step"] * args.steps)
             ms_step = shared["ms_per_step"]
-            lat = shared["lat"]
-            achieved = shared["bytes"] / (shared["scan_ms"] / 1000.0) / 1e9
+            achieved = len(union_cols) * 4 * args.rows / (shared["scan_ms"] / 1000.0) / 1e9
             kernel = "SharedScan_LINEORDER (one pass over the union of the batch's fact columns)"
-            launches = shared["launches"]
+            launches = shared["launches_per_step"]
             alg = f"union of fact columns read by the batch ({len(union_cols)}) x 4 B x rows, per launch"
+            lat = {"p50": ms_step, "p99": ms_step, "definition": "every query of a batch completes with its launch"}
         else:
             value = plain["queries_per_s"]
             ms_step = plain["ms_per_step"]
-            lat = plain_lat
             achieved = plain["scan_GBps"]
             kernel = "Scan_LINEORDER (plain fused scan/probe/aggregate)"
-            launches = plain_launches
+            launches = pl["launches_per_step"] * len(plans) // len(plans_all)
             alg = "distinct fact columns read x 4 B x rows, per query"
+            lat = {"p50": plain["p50_ms"], "p99": plain["p99_ms"], "definition": "query completion since its batch started"}
+        batches = {}
+        for b in sizes:
+            row = {"plain": plain_by_batch[b]}
+            if b in shared_all:
+                s = shared_all[b]
+                ucols = sorted({c for p in plans_all[:b] for c in p.columns_read()})
+                s_qps = job_rate(b * args.steps, world, s["ms_per_step"] * args.steps)
+                row["shared"] = {"queries_per_s": s_qps, "ms_per_step": s["ms_per_step"], "scan_ms": s["scan_ms"],
+                                 "roofline_frac": len(ucols) * 4 * args.rows / (s["scan_ms"] / 1000.0) / 1e9 / peak,
+                                 "graph": s["graph"], "tuning": s["tuning"]}
+                row["shared_vs_plain"] = s_qps / plain_by_batch[b]["queries_per_s"]
+            batches[str(b)] = row
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32/u64", "data": "synthetic",
             "config": config_block(args),
-            "latency_ms": {"p50": statistics.median(lat), "p99": float(np.percentile(lat, 99)),
-                           "definition": "query completion since its batch started"},
+            "latency_ms": lat,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (SHARED_DRAM_BYTES_PER_ROW * args.rows / 1e9) if shared is not None else None,
                          "traffic_unit": "GB per launch (ncu capture of 30M rows scaled by rows)",
                          "kernel": kernel, "algorithmic_bytes": alg},
-            "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks, "e2e": e2e,
+            "gpu_launches": launches * args.steps, "gpu_launches_per_step": launches,
             "cpu_baseline": cb,
+            "parity": parity,
             "plain": plain,
             "shared_vs_plain": (value / plain["queries_per_s"]) if shared is not None else 1.0,
+            "batches": batches,
             "shared_tuning": shared["tuning"] if shared is not None else None,
+            "configs": configs,
             "serving": serving,
         }
         print(json.dumps(line), flush=True)

@@ -152,6 +152,10 @@ def translate(plan, dim_rows: dict[str, int]):
     return q, names
 
 
+def max_threads() -> int:
+    return _load().ref_max_threads()
+
+
 def run(plan, columns: dict[str, np.ndarray], dim_rows: dict[str, int], n_fact: int, threads: int = 0) -> np.ndarray:
     lib = _load()
     q, names = translate(plan, dim_rows)

@@ -107,9 +107,10 @@ def commitdates(seed: int, row0: int, rows: int) -> np.ndarray:
     return EXT_DATE_KEYS[idx + lag]
 
 
-def validity_words(seed: int, stream: int, rows: int, null_permille: int) -> np.ndarray:
-    """uint64 words, bit r = 1 when row r is valid (the reference's .valid64)."""
-    nulls = below(hashes(seed, stream, 0, rows), 1000) < np.uint64(null_permille)
+def validity_words(seed: int, stream: int, rows: int, null_permille: int, row0: int = 0) -> np.ndarray:
+    """uint64 words, bit r = 1 when row row0 + r is valid (the reference's
+    .valid64); row0 > 0 gives the words of a row range on their own."""
+    nulls = below(hashes(seed, stream, row0, rows), 1000) < np.uint64(null_permille)
     bits = np.zeros(((rows + 63) // 64) * 64, dtype=np.uint8)
     bits[:rows] = ~nulls
     return np.packbits(bits, bitorder="little").view("<u8").astype(np.uint64)

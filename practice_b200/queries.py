@@ -8,7 +8,8 @@
   ORDER BY year ASC, sum DESC (SSB Q3.1 shape, test/queries/sql/q31.sql).
 * ``ssb_q31_nullable`` -- the nullable three-valued-logic variant: NULL revenue and
   NULL customer.city, IS NULL / IS NOT NULL and range predicates that yield
-  UNKNOWN; COUNT(*), COUNT(revenue), SUM(revenue) grouped by a nullable key.
+  UNKNOWN (on a fact column and on a joined payload); COUNT(*),
+  COUNT(revenue), SUM(revenue) grouped by a nullable key.
 * ``template(t, rng)`` -- the four shared-scan templates: T0 range filters +
   scalar SUM; T1 date join + GROUP BY year; T2 three joins + GROUP BY
   (nation, year); T3 four joins + GROUP BY (brand, year) (<= 7,000 groups).
@@ -70,6 +71,10 @@ def ssb_q31_nullable(fact_rows: int = 60_000_000, region: int = 1, years: tuple[
     b.join("CUSTOMER", "lo_custkey", where=col("c_region").eq(region), payload="c_city")
     b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(region))
     b.join("DDATE", "lo_orderdate", where=and_(col("d_year").ge(years[0]), col("d_year").le(years[1])))
+    # IS NOT NULL over a joined payload and a fact column: rows whose city and
+    # revenue are both NULL drop out; a NULL city with a known revenue stays
+    # and forms the NULL group.
+    b.filter(or_(col("c_city").not_null(), col("lo_revenue").not_null()))
     return b.aggregate([_g("c_city", nullable=True), _g("d_year")],
                        [("count", star()), ("count", col("lo_revenue")), ("sum", col("lo_revenue"))],
                        order_by=[(1, False), (0, False)])

@@ -110,6 +110,19 @@ void cx_tuning_default(cx_tuning* t);
 int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap,
                size_t* out_len);
 
+/* Rewrites a program emitted by the reference's code generator
+ * (JITOperatorVisitor::generateCode, src/core/visitor.cpp:4771-4878: SYCL, an
+ * `execute_query(db::ExecutionContext*)` that submits nd_range build and scan
+ * kernels) into this library's CUDA skeleton: the kernel bodies are kept, the
+ * launch skeleton becomes `__global__` kernels over one argument block plus the
+ * embedded launch plan, and the row-count macros (LO_LEN, C_LEN, ...) become the
+ * context's table rows.  cx_compile applies it by itself to such sources, so
+ * the reference's ICompiler::compile can pass the visitor's text unchanged.
+ * Programs that need the host between kernels (dense result materialisation,
+ * multi-value hash tables, projections, ORDER BY) return CX_E_INVALID naming
+ * the construct.  Same output-buffer contract as cx_codegen. */
+int cx_translate_visitor(const char* src, size_t src_len, char* out, size_t out_cap, size_t* out_len);
+
 /* Compiles generated source with NVRTC for sm_100a into an in-memory cubin and
  * parses its embedded launch plan.  `key` names the module in the process-wide
  * cache (the reference keys its cache on "query_" + ABI version + hash(sql),

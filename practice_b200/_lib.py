@@ -18,7 +18,7 @@ ERRORS = {
 
 # Every symbol include/crystal_b200.h declares (checked by the CPU tests).
 EXPORTS = [
-    "cx_abi_version", "cx_last_error", "cx_tuning_default", "cx_codegen", "cx_compile",
+    "cx_abi_version", "cx_last_error", "cx_tuning_default", "cx_codegen", "cx_translate_visitor", "cx_compile",
     "cx_module_release", "cx_module_result_info", "cx_ctx_create", "cx_ctx_destroy",
     "cx_ctx_set_buffer", "cx_ctx_set_null_bitmap", "cx_ctx_set_table_rows", "cx_ctx_set_result",
     "cx_ctx_set_scratch", "cx_module_scratch_bytes", "cx_ctx_set_sm_count", "cx_execute",
@@ -98,6 +98,7 @@ def _load() -> C.CDLL:
         "cx_last_error": (C.c_char_p, []),
         "cx_tuning_default": (None, [C.POINTER(Tuning)]),
         "cx_codegen": (C.c_int, [C.c_char_p, sz, C.POINTER(Tuning), C.c_char_p, sz, C.POINTER(sz)]),
+        "cx_translate_visitor": (C.c_int, [C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
         "cx_compile": (C.c_int, [C.c_char_p, sz, C.c_char_p, C.POINTER(vp), C.c_char_p, sz]),
         "cx_module_release": (C.c_int, [vp]),
         "cx_module_result_info": (C.c_int, [vp, C.POINTER(ResultInfo)]),
@@ -168,6 +169,17 @@ def codegen(plan_text: str, tuning: Tuning | None = None) -> str:
     check(lib.cx_codegen(raw, len(raw), tp, None, 0, C.byref(n)), "cx_codegen")
     buf = C.create_string_buffer(n.value + 1)
     check(lib.cx_codegen(raw, len(raw), tp, buf, n.value + 1, C.byref(n)), "cx_codegen")
+    return buf.value.decode()
+
+
+def translate_visitor(source: str) -> str:
+    """The CUDA program cx_compile makes of a program emitted by the reference's
+    code generator (its kernel bodies under this library's launch skeleton)."""
+    n = C.c_size_t(0)
+    src = source.encode()
+    check(lib.cx_translate_visitor(src, len(src), None, 0, C.byref(n)), "cx_translate_visitor")
+    buf = C.create_string_buffer(n.value + 1)
+    check(lib.cx_translate_visitor(src, len(src), buf, len(buf), C.byref(n)), "cx_translate_visitor")
     return buf.value.decode()
 
 

@@ -20,7 +20,7 @@ CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = CUDA_HOME / "bin" / "nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-HOST_SOURCES = ["cx_plan.cpp", "cx_codegen.cpp", "cx_runtime.cpp", "cx_server.cpp"]
+HOST_SOURCES = ["cx_plan.cpp", "cx_codegen.cpp", "cx_runtime.cpp", "cx_server.cpp", "cx_sycl.cpp"]
 CUDA_SOURCES = ["cx_kernels.cu", "cx_finalize.cu"]
 EMBEDDED = ["crystal_sm100.cuh", "cx_args.h"]
 

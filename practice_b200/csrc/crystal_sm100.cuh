@@ -953,6 +953,21 @@ CX_DEVICE unsigned long long block_max_u64(unsigned long long v, unsigned long l
   return s;
 }
 
+// The reference's sycl::reduce_over_group over one work-group of BT threads
+// (OP 0 sum, 1 minimum, 2 maximum of unsigned 64-bit values): every thread
+// receives the CTA's result.  `scratch` holds BT/32 + 1 words; every thread
+// of the CTA must make the call.
+template <int BT, int OP>
+CX_DEVICE unsigned long long group_reduce_u64(unsigned long long v, unsigned long long* scratch) {
+  const unsigned long long r = OP == 0 ? block_sum_u64<BT>(v, scratch)
+                               : OP == 1 ? block_min_u64<BT>(v, scratch)
+                                         : block_max_u64<BT>(v, scratch);
+  __syncthreads();
+  if (threadIdx.x == 0) scratch[BT / 32] = r;
+  __syncthreads();
+  return scratch[BT / 32];
+}
+
 // Bitwise OR of a 32-bit value over the CTA; the result is valid in thread 0.
 template <int BT>
 CX_DEVICE unsigned block_or_u32(unsigned v, unsigned long long* scratch) {

@@ -35,6 +35,14 @@ uint64_t grown_scratch(uint64_t own, uint64_t need);
 // The code generator's tuning for a C-ABI tuning (defaults where null).
 cx::Tuning to_tuning(const cx_tuning* t);
 
+// Whether `src` is a program of the reference's code generator (a SYCL
+// `execute_query(db::ExecutionContext*)` translation unit, not cx_codegen output).
+bool is_visitor_program(const std::string& src);
+
+// Rewrites such a program's launch skeleton into this library's (kernel
+// bodies kept); throws std::runtime_error naming what it cannot translate.
+std::string translate_visitor_program(const std::string& src);
+
 // Records `msg` as the calling thread's cx_last_error() and returns `code`.
 int set_error(int code, const std::string& msg);
 

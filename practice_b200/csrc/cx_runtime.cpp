@@ -110,7 +110,9 @@ struct LaunchPlan {
   struct Col { int slot; std::string name; int table; };
   std::vector<Col> cols;
   std::vector<std::pair<int, std::string>> nulls;
-  struct Ht { int slot; std::string name; uint64_t words; };
+  // A hash table of `words` ints, or (rows_table >= 0) of mult x the row count
+  // of that table, known at execute.
+  struct Ht { int slot; std::string name; uint64_t words; int rows_table = -1; uint64_t mult = 0; };
   std::vector<Ht> hts;
   std::map<int, uint64_t> htv_words;
   std::map<int, uint64_t> bm_words;
@@ -126,6 +128,7 @@ struct LaunchPlan {
   int shared_maxq = 256, shared_maxp = 4096;           // queries / parameters per shared launch
   uint64_t shared_qb_bytes = 0;                        // shared memory of row bitmaps per query of a pass
   int nparams = -1;                                    // parametric plain kernels: literal count
+  bool rows_sized = false;                             // some hash table is sized by a table's rows
   std::map<int, uint64_t> dat_words;                   // shared scans: extra payload attributes per dimension
   std::vector<std::pair<int, std::string>> fcols;      // shared scans: fact filter table columns
   struct SShape { uint64_t groups; int ts, grouped, sparse, nlits, smem_ok, naggs; uint64_t tw; int nseen; };
@@ -166,6 +169,12 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       LaunchPlan::Ht h;
       ls >> h.slot >> h.name >> h.words;
       lp.hts.push_back(h);
+    } else if (k == "htrows") {
+      LaunchPlan::Ht h;
+      ls >> h.slot >> h.name >> h.mult >> h.rows_table;
+      h.words = h.mult;
+      lp.hts.push_back(h);
+      lp.rows_sized = true;
     } else if (k == "htv") {
       int s; uint64_t w;
       ls >> s >> w;
@@ -212,7 +221,7 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
     } else if (k == "kernel") {
       KernelSpec ks;
       ls >> ks.name >> ks.kind >> ks.table >> ks.block;
-      if (ks.kind == "build") ls >> ks.tile;
+      if (ks.kind == "build" || ks.kind == "tiles" || ks.kind == "tilescan") ls >> ks.tile;
       else if (ks.kind == "scan" || ks.kind == "sharedscan") ls >> ks.tile >> ks.smem >> ks.ctas_per_sm;
       else { size_t z; ls >> z; }
       lp.kernels.push_back(ks);
@@ -226,6 +235,17 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
     err = "launch plan exceeds argument slots";
     return false;
   }
+  for (const auto& h : lp.hts)
+    if (h.rows_table >= (int)lp.tables.size() || h.slot < 0 || h.slot >= CX_MAX_HTS) {
+      err = "hash table line names a slot or table outside the plan";
+      return false;
+    }
+  for (const auto& k : lp.kernels)
+    if ((k.kind == "tiles" || k.kind == "tilescan" || k.kind == "build") &&
+        (k.table < 0 || k.table >= (int)lp.tables.size() || k.tile <= 0 || k.block <= 0 || k.block > 1024)) {
+      err = "kernel line " + k.name + " names a table outside the plan or a bad shape";
+      return false;
+    }
   return true;
 }
 
@@ -238,12 +258,20 @@ struct ScratchLayout {
   uint64_t touched_off = 0, fin_off = 0, err_off = 0, total = 0;
 };
 
-ScratchLayout scratch_layout(const LaunchPlan& lp) {
+// Words of a hash table: fixed, or sized by its table's rows when they are
+// known (at least one row's worth before that).
+uint64_t ht_words(const LaunchPlan::Ht& h, const std::vector<long long>* rows) {
+  if (h.rows_table < 0) return h.words;
+  const long long n = rows ? std::max<long long>(1, (*rows)[h.rows_table]) : 1;
+  return h.mult * (uint64_t)n;
+}
+
+ScratchLayout scratch_layout(const LaunchPlan& lp, const std::vector<long long>* rows = nullptr) {
   ScratchLayout s;
   uint64_t off = 0;
   for (const auto& h : lp.hts) {
     s.ht_off.push_back(off);
-    off = align256(off + h.words * 4);
+    off = align256(off + ht_words(h, rows) * 4);
   }
   for (const auto& h : lp.hts) {
     auto it = lp.htv_words.find(h.slot);
@@ -489,7 +517,16 @@ int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char*
 int cx_compile(const char* src, size_t src_len, const char* key, cx_module** out, char* log, size_t log_cap) {
   if (!src || !out) return fail(CX_E_INVALID, "cx_compile: NULL argument");
   if (log && log_cap) log[0] = '\0';
-  const std::string source(src, src_len);
+  std::string source(src, src_len);
+  // A program from the reference's code generator (SYCL launch skeleton) is
+  // translated to this library's skeleton first.
+  if (cx_internal::is_visitor_program(source)) {
+    try {
+      source = cx_internal::translate_visitor_program(source);
+    } catch (const std::exception& e) {
+      return fail(CX_E_INVALID, "cx_compile: %s", e.what());
+    }
+  }
   const size_t h = std::hash<std::string>{}(source);
   std::string ck = key ? std::string(key) : std::string();
   if (ck.empty()) ck = "anon_" + std::to_string(h);
@@ -645,14 +682,14 @@ int cx_ctx_set_column_range(cx_exec_ctx* c, const char* name, int64_t lo, int64_
 int cx_module_scratch_bytes(const cx_module* m, const cx_exec_ctx* c, uint64_t* bytes) {
   if (!m || !bytes) return fail(CX_E_INVALID, "cx_module_scratch_bytes: NULL argument");
   *bytes = m->sl.total;
-  if (!m->lp.mht_table.empty() && c) {
+  if ((!m->lp.mht_table.empty() || m->lp.rows_sized) && c) {
     std::vector<long long> rows(m->lp.tables.size(), 0);
     for (size_t t = 0; t < m->lp.tables.size(); ++t) {
       auto it = c->rows.find(m->lp.tables[t]);
       if (it == c->rows.end()) return fail(CX_E_MISSING, "cx_module_scratch_bytes: row count of table %s is not set", m->lp.tables[t].c_str());
       rows[t] = (long long)it->second;
     }
-    *bytes += mht_payload_bytes(m->lp, rows);
+    *bytes = scratch_layout(m->lp, &rows).total + mht_payload_bytes(m->lp, rows);
   }
   return CX_OK;
 }
@@ -716,8 +753,10 @@ int cx_execute_params(cx_module* m, cx_exec_ctx* c, const int32_t* params, int n
   rc = load_on_device(m, dev, &L);
   if (rc) return rc;
 
-  // Scratch: the plan's fixed layout, then the MHT row-id payloads.
-  const uint64_t need = m->sl.total + mht_payload_bytes(lp, rows);
+  // Scratch: the plan's layout (hash tables sized by row counts where the plan
+  // says so), then the MHT row-id payloads.
+  const ScratchLayout sl = lp.rows_sized ? scratch_layout(lp, &rows) : m->sl;
+  const uint64_t need = sl.total + mht_payload_bytes(lp, rows);
   char* scratch = nullptr;
   if (c->user_scratch) {
     if (c->user_scratch_bytes < need)
@@ -739,15 +778,15 @@ int cx_execute_params(cx_module* m, cx_exec_ctx* c, const int32_t* params, int n
     scratch = (char*)c->own_scratch;
   }
   for (size_t i = 0; i < lp.hts.size(); ++i) {
-    a.ht[lp.hts[i].slot] = (int*)(scratch + m->sl.ht_off[i]);
-    if (lp.htv_words.count(lp.hts[i].slot)) a.htv[lp.hts[i].slot] = (unsigned int*)(scratch + m->sl.htv_off[i]);
-    if (lp.bm_words.count(lp.hts[i].slot)) a.bm[lp.hts[i].slot] = (unsigned int*)(scratch + m->sl.bm_off[i]);
+    a.ht[lp.hts[i].slot] = (int*)(scratch + sl.ht_off[i]);
+    if (lp.htv_words.count(lp.hts[i].slot)) a.htv[lp.hts[i].slot] = (unsigned int*)(scratch + sl.htv_off[i]);
+    if (lp.bm_words.count(lp.hts[i].slot)) a.bm[lp.hts[i].slot] = (unsigned int*)(scratch + sl.bm_off[i]);
   }
-  a.touched = (unsigned int*)(scratch + m->sl.touched_off);
-  a.finalize_tmp = (unsigned long long*)(scratch + m->sl.fin_off);
-  a.err = (unsigned int*)(scratch + m->sl.err_off);
+  a.touched = (unsigned int*)(scratch + sl.touched_off);
+  a.finalize_tmp = (unsigned long long*)(scratch + sl.fin_off);
+  a.err = (unsigned int*)(scratch + sl.err_off);
   {
-    uint64_t off = m->sl.total;
+    uint64_t off = sl.total;
     for (const auto& kv : lp.mht_table) {
       a.mpay[kv.first] = (int*)(scratch + off);
       off += align256((uint64_t)std::max<long long>(1, rows[kv.second]) * 4);
@@ -770,12 +809,12 @@ int cx_execute_params(cx_module* m, cx_exec_ctx* c, const int32_t* params, int n
   };
 
   CX_CUDA(cudaEventRecord(c->ev[0], stream));
-  CX_CUDA(cudaMemsetAsync(scratch, 0, m->sl.total, stream));
+  CX_CUDA(cudaMemsetAsync(scratch, 0, sl.total, stream));
   CX_CUDA(cudaMemsetAsync(c->result, 0, lp.result_words * 8, stream));
   CX_CUDA(cudaMemsetAsync(c->validity, 0, vwords * 8, stream));
   size_t ki = 0;
   // Phase 1: slot initialisation and hash-table builds.
-  for (; ki < lp.kernels.size() && lp.kernels[ki].kind != "scan"; ++ki) {
+  for (; ki < lp.kernels.size() && lp.kernels[ki].kind != "scan" && lp.kernels[ki].kind != "tilescan"; ++ki) {
     const KernelSpec& k = lp.kernels[ki];
     unsigned grid = 0;
     if (k.kind == "groups") grid = (unsigned)((lp.groups + k.block - 1) / k.block);
@@ -783,12 +822,22 @@ int cx_execute_params(cx_module* m, cx_exec_ctx* c, const int32_t* params, int n
     else if (k.kind == "build") {
       const long long tiles = (rows[k.table] + k.tile - 1) / k.tile;
       grid = (unsigned)std::min<long long>(tiles, (long long)sms * 16);
+    } else if (k.kind == "tiles") {
+      // One CTA per tile of the table (a translated nd_range kernel).
+      grid = (unsigned)((rows[k.table] + k.tile - 1) / k.tile);
     }
     if ((rc = launch(ki, grid))) return rc;
   }
   CX_CUDA(cudaEventRecord(c->ev[1], stream));
   // Phase 2: the fused scan.
-  if (ki < lp.kernels.size()) {
+  if (ki < lp.kernels.size() && lp.kernels[ki].kind == "tilescan") {
+    const KernelSpec& k = lp.kernels[ki];
+    const long long tiles = (rows[k.table] + k.tile - 1) / k.tile;
+    if (tiles > 0x7fffffffLL) return fail(CX_E_CAPACITY, "cx_execute: %lld tiles exceed one grid", tiles);
+    scan_grid = (int)tiles;
+    if ((rc = launch(ki, (unsigned)tiles))) return rc;
+    ++ki;
+  } else if (ki < lp.kernels.size()) {
     const KernelSpec& k = lp.kernels[ki];
     const long long tiles = (rows[0] + k.tile - 1) / k.tile;
     const long long warps = std::max(1, k.block / 32);

@@ -18,9 +18,12 @@ def plan(name: str, n: int):
     t = datagen.ssb_tables(n, ALL_COLS)
     if name == "q11":
         return queries.ssb_q11(n)
-    if name == "q31":
-        return queries.ssb_q31(n)
     b = PlanBuilder(t, "LINEORDER", name=name)
+    if name == "q31":  # the SSB Q3.1 shape without its ORDER BY (the fixture's tree has no sort)
+        b.join("CUSTOMER", "lo_custkey", where=col("c_region").eq(2))
+        b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(2))
+        b.join("DDATE", "lo_orderdate", where=and_(col("d_year").ge(1992), col("d_year").le(1997)))
+        return b.aggregate([_g("c_nation"), _g("s_nation"), _g("d_year")], [("sum", col("lo_revenue"))])
     if name == "t0":
         b.filter(and_(col("lo_quantity").ge(5), col("lo_quantity").le(35), col("lo_discount").ge(3),
                       col("lo_discount").le(5)))

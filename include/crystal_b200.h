@@ -72,6 +72,10 @@ typedef struct cx_tuning {
   int debug_stall;       /* test hook for the bounded-wait path: 1 = every CTA of the scan first
                             waits on a barrier that nothing completes, so the wait runs out
                             (kernel error 1) with no copy in flight; 0 in normal use */
+  int compact;           /* plain grouped scans without expanding joins, unstaged vector loads:
+                            1 = each warp queues the rows that pass the join bitmaps and fact
+                            filters (ballot / popc into shared memory) and runs payload fetches,
+                            remaining probes and the group update on 32 queued rows at a time */
 } cx_tuning;
 
 /* Shape of a compiled query's result buffer. */

@@ -666,6 +666,59 @@ struct Emitter {
         seen_off = off; off += (unsigned long long)REP * NSEEN_T * TW * 4;
       }
     }
+    // Warp compaction of qualifying rows (grouped, non-expanding plans with
+    // every fact column vector-loaded at the tile start): after the cheap
+    // membership tests (exact join bitmaps, filters over fact columns) each
+    // warp appends its qualifying rows' values to a per-warp queue in shared
+    // memory and runs the rest of the pipeline -- payload fetches, remaining
+    // probes and filters, the group update -- on 32 queued rows at a time with
+    // every lane busy, instead of on mostly idle lanes of every tile.
+    const bool vec_pf_all = STAGES == 0 && NSC > 0 && (IPT == 1 || IPT == 2 || IPT % 4 == 0) && tu.prefetch > 0;
+    const bool compact = tu.compact > 0 && !expanding && grouped && vec_pf_all;
+    std::set<std::string> exact_set;
+    for (const auto& b : sbms) exact_set.insert(b.dim);
+    auto fact_only = [&](const Expr* e) {
+      std::vector<std::string> cs;
+      collect(e, cs);
+      for (const auto& c : cs)
+        if (p.table_of_col.at(c) != 0) return false;
+      return true;
+    };
+    std::vector<std::string> qcols;  // fact columns (and validity) the queued rows carry
+    auto add_q = [&](const std::string& c) {
+      if (p.table_of_col.at(c) == 0 && std::find(qcols.begin(), qcols.end(), c) == qcols.end()) qcols.push_back(c);
+    };
+    if (compact) {
+      for (const auto& s : p.steps) {
+        if (s.kind == Step::Filter) {
+          if (!fact_only(s.filter.get())) {
+            std::vector<std::string> cs;
+            collect(s.filter.get(), cs);
+            for (const auto& c : cs) add_q(c);
+          }
+        } else if (!exact_set.count(s.join.dim) || !s.join.payload.empty()) {
+          add_q(s.join.fks[0]);
+        }
+      }
+      for (const auto& g : p.groups) {
+        std::vector<std::string> cs;
+        collect(g.expr.get(), cs);
+        for (const auto& c : cs) add_q(c);
+      }
+      for (const auto& ag : p.aggs) {
+        std::vector<std::string> cs;
+        collect(ag.arg.get(), cs);
+        for (const auto& c : cs) add_q(c);
+      }
+    }
+    int NQ = 0;
+    for (const auto& c : qcols) NQ += 1 + (nullable(c) ? 1 : 0);
+    const int QCAP = 32 * (IPT + 1);
+    unsigned long long q_off = 0;
+    if (compact && NQ > 0) {
+      q_off = (off + 15) & ~15ULL;
+      off = q_off + (unsigned long long)NW * NQ * QCAP * 4;
+    }
     const unsigned long long smem_total = (off + 127) & ~127ULL;
     if (smem_total > 227 * 1024) throw PlanError("scan kernel shared memory exceeds 227 KB; lower stages or items per thread");
     const unsigned wait_limit = (unsigned)std::min(60000000, std::max(1, tu.wait_limit_us));
@@ -819,7 +872,15 @@ struct Emitter {
     }
     o << "  long long k_iter = 0;\n";
     o << "  bool aborted = false; (void)aborted;\n";
-    o << "  for (long long t = gwarp; t < num_tiles; t += nwarps, ++k_iter) {\n";
+    if (compact) {
+      o << "  int* q_base = (int*)(cx_smem + " << q_off << ") + (long long)warp * " << NQ * QCAP << "LL; (void)q_base;\n";
+      o << "  int q_n = 0;  // rows waiting in this warp's queue (warp-uniform)\n";
+      o << "  for (long long t = gwarp; ; t += nwarps, ++k_iter) {\n";
+      o << "   const bool live_ = t < num_tiles;\n";
+      o << "   if (live_) {\n";
+    } else {
+      o << "  for (long long t = gwarp; t < num_tiles; t += nwarps, ++k_iter) {\n";
+    }
     o << "    const long long tile_offset = t * TILE_SIZE;\n";
     o << "    const int num_tile_items = (int)(n_rows - tile_offset < TILE_SIZE ? n_rows - tile_offset : TILE_SIZE);\n";
     if (STAGES > 0) {
@@ -883,14 +944,20 @@ struct Emitter {
         << ", num_tile_items);\n";
       exact_dims.insert(b.dim);
     }
+    // The steps after the membership tests, in plan order (with compaction:
+    // the ones that run on queued rows).
+    auto emit_steps = [&](std::ostream& o, const std::string& ind, bool post) {
     for (size_t k = 0; k < xs; ++k) {
       const Step& s = p.steps[k];
       if (s.kind == Step::Filter) {
-        emit_filter(o, s.filter.get(), ind);
+        const bool early = fact_only(s.filter.get());
+        if (!compact || early != post) emit_filter(o, s.filter.get(), ind);
         continue;
       }
+      if (compact && !post) continue;
       const Join& j = s.join;
       const std::string& fk = j.fks[0];
+      if (exact_dims.count(j.dim) && j.payload.empty()) continue;
       ensure_loaded(o, fk, ind);
       if (exact_dims.count(j.dim)) {
         // Membership is settled; fetch the payload of qualifying rows.
@@ -924,6 +991,8 @@ struct Emitter {
         loaded.insert(j.payload);
       }
     }
+    };
+    emit_steps(o, ind, false);
     // Per-row aggregate updates shared by the vector and the item-mode paths.
     // Ungrouped: thread-private accumulators.
     auto scalar_update = [&](const std::string& ii) {
@@ -1211,8 +1280,10 @@ struct Emitter {
         else for (const auto& fk : s.join.fks) ensure_loaded(o, fk, ind);
       }
     }
-    for (const auto& g : p.groups) load_expr_cols(o, g.expr.get(), ind);
-    for (const auto& ag : p.aggs) load_expr_cols(o, ag.arg.get(), ind);
+    if (!compact) {
+      for (const auto& g : p.groups) load_expr_cols(o, g.expr.get(), ind);
+      for (const auto& ag : p.aggs) load_expr_cols(o, ag.arg.get(), ind);
+    }
 
     // With group_merge = 1, one expanding join feeding a shared-memory or
     // global group table runs as a warp-uniform loop (every lane takes its
@@ -1305,32 +1376,106 @@ struct Emitter {
     };
 
     // Aggregate consume.
-    if (uniform_expand) {
-      uniform_expansion(ind);
-    } else if (expanding) {
-      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
-      item_steps(xs, ind + "    ");
-      o << ind << "  }\n" << ind << "}\n";
-    } else if (!grouped) {
-      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
-      scalar_update(ind + "    ");
-      o << ind << "  }\n" << ind << "}\n";
-    } else if (reg_groups || lane_groups) {
-      o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
-      group_hash(ind + "    ");
-      o << ind << "    if ((unsigned)hash < " << G << "u) {\n";
-      if (reg_groups) reg_update(ind + "      ");
-      else lane_update(ind + "      ");
-      o << ind << "    }\n";
-      o << ind << "  }\n";
-      o << ind << "}\n";
+    auto emit_consume = [&](const std::string& ind) {
+      if (uniform_expand) {
+        uniform_expansion(ind);
+      } else if (expanding) {
+        o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+        o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+        item_steps(xs, ind + "    ");
+        o << ind << "  }\n" << ind << "}\n";
+      } else if (!grouped) {
+        o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+        o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+        scalar_update(ind + "    ");
+        o << ind << "  }\n" << ind << "}\n";
+      } else if (reg_groups || lane_groups) {
+        o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+        o << ind << "  if (flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)) {\n";
+        group_hash(ind + "    ");
+        o << ind << "    if ((unsigned)hash < " << G << "u) {\n";
+        if (reg_groups) reg_update(ind + "      ");
+        else lane_update(ind + "      ");
+        o << ind << "    }\n";
+        o << ind << "  }\n";
+        o << ind << "}\n";
+      } else {
+        o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+        merged_update(ind + "  ", "flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)");
+        o << ind << "}\n";
+      }
+
+    };
+    if (!compact) {
+      emit_consume(ind);
     } else {
+      // Append this tile's qualifying rows to the warp's queue.
       o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
-      merged_update(ind + "  ", "flags[i] && (tid + BLOCK_THREADS * i < num_tile_items)");
+      o << ind << "  const bool f_ = flags[i] && (tid + BLOCK_THREADS * i < num_tile_items);\n";
+      o << ind << "  const unsigned m_ = __ballot_sync(0xffffffffu, f_);\n";
+      o << ind << "  if (f_) {\n";
+      o << ind << "    const int p_ = q_n + __popc(m_ & ((1u << lane) - 1u));\n";
+      {
+        int qi = 0;
+        for (const auto& c : qcols) {
+          o << ind << "    q_base[" << qi++ * QCAP << " + p_] = " << c << "[i];\n";
+          if (nullable(c)) o << ind << "    q_base[" << qi++ * QCAP << " + p_] = " << c << "_valid[i];\n";
+        }
+      }
+      o << ind << "  }\n";
+      o << ind << "  q_n += __popc(m_);\n";
       o << ind << "}\n";
+      o << "   }\n";  // live_
+      // Run the rest of the pipeline on 32 queued rows at a time (the last,
+      // partial batch once the warp has no tiles left).
+      o << "   while (q_n >= 32 || (!live_ && q_n > 0)) {\n";
+      o << "    const int cnt_ = q_n < 32 ? q_n : 32;\n";
+      o << "    __syncwarp();\n";
+      o << "    {\n";
+      o << "    constexpr int ITEMS_PER_THREAD = 1;\n";
+      o << "    const int num_tile_items = cnt_;\n";
+      o << "    int flags[1];\n";
+      o << "    flags[0] = lane < cnt_ ? 1 : 0;\n";
+      std::vector<std::string> dregs = qcols;
+      for (const auto& c : payload_cols) dregs.push_back(c);
+      declare_regs(o, dregs, "    ");
+      const std::set<std::string> saved_loaded = loaded, saved_valid = valid_regs;
+      loaded.clear();
+      valid_regs.clear();
+      {
+        int qi = 0;
+        for (const auto& c : qcols) {
+          o << "    " << c << "[0] = q_base[" << qi++ * QCAP << " + lane];\n";
+          loaded.insert(c);
+          if (nullable(c)) {
+            o << "    " << c << "_valid[0] = q_base[" << qi++ * QCAP << " + lane];\n";
+            valid_regs.insert(c);
+          }
+        }
+      }
+      emit_steps(o, "    ", true);
+      emit_consume("    ");
+      loaded = saved_loaded;
+      valid_regs = saved_valid;
+      o << "    }\n";
+      o << "    __syncwarp();\n";
+      // Move the rows left over to the queue's front.
+      o << "    const int rest_ = q_n - cnt_;\n";
+      o << "    for (int b_ = 0; b_ < rest_; b_ += 32) {\n";
+      o << "      const int e_ = b_ + lane;\n";
+      o << "      int v_[" << std::max(NQ, 1) << "];\n";
+      o << "      if (e_ < rest_) {\n";
+      for (int qi = 0; qi < NQ; ++qi) o << "        v_[" << qi << "] = q_base[" << qi * QCAP << " + 32 + e_];\n";
+      o << "      }\n";
+      o << "      __syncwarp();\n";
+      o << "      if (e_ < rest_) {\n";
+      for (int qi = 0; qi < NQ; ++qi) o << "        q_base[" << qi * QCAP << " + e_] = v_[" << qi << "];\n";
+      o << "      }\n";
+      o << "      __syncwarp();\n";
+      o << "    }\n";
+      o << "    q_n = rest_;\n";
+      o << "   }\n";
+      o << "   if (!live_) break;\n";
     }
 
     if (STAGES > 0) {

@@ -29,6 +29,8 @@ struct Tuning {
                                // 2 as 1 and the next tile's loads issued one tile ahead
   int wait_limit_us = 500000;  // a bounded mbarrier wait gives up after this many microseconds
   int debug_stall = 0;         // test hook: 1 = every CTA first waits on a barrier nothing completes
+  int compact = 0;             // plain grouped scans: 1 = queue qualifying rows per warp after the
+                               // membership tests and run the rest on 32 queued rows at a time
 };
 
 // Returns the CUDA source for `plan` with its launch plan embedded as a

@@ -443,6 +443,7 @@ cx::Tuning to_tuning(const cx_tuning* tuning) {
     t.prefetch = tuning->prefetch;
     t.wait_limit_us = tuning->wait_limit_us;
     t.debug_stall = tuning->debug_stall;
+    t.compact = tuning->compact;
   }
   return t;
 }
@@ -493,6 +494,7 @@ void cx_tuning_default(cx_tuning* t) {
   t->prefetch = d.prefetch;
   t->wait_limit_us = d.wait_limit_us;
   t->debug_stall = d.debug_stall;
+  t->compact = d.compact;
 }
 
 int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap, size_t* out_len) {

@@ -282,3 +282,22 @@ def test_bounded_wait_limit_and_stall_hook_reach_the_generated_kernels():
     src = _lib.shared_codegen(shapes, t2)
     assert "cx::debug_stall(" in src and "cx::drain_limit_us(" in src
     _lib.Module(src, key="stall_shared")
+
+
+@pytest.mark.parametrize("name", ["ssb_q31", "ssb_q31_nullable", "T1", "T2", "T3", "kat_q2"])
+@pytest.mark.parametrize("ipt", [1, 2, 4, 8])
+def test_compacted_scans_compile(name, ipt):
+    """Warp compaction: qualifying rows queue per warp; the payload fetches and
+    the group update run on 32 queued rows at a time."""
+    plan = all_plans()[name]
+    t = _lib.default_tuning()
+    t.items_per_thread, t.compact = ipt, 1
+    if ipt == 8:
+        t.block_threads = 512
+    src = _lib.codegen(plan.text(), t)
+    assert "q_base" in src and "while (q_n >= 32 || (!live_ && q_n > 0))" in src
+    _lib.Module(src, key=f"compact_{name}_{ipt}")
+    # Scalar plans and staged scans keep the direct path.
+    t.stages, t.block_threads = 2, 256
+    assert "q_base" not in _lib.codegen(plan.text(), t)
+    assert "q_base" not in _lib.codegen(all_plans()["ssb_q11"].text(), _lib.default_tuning())

@@ -3,8 +3,8 @@ exact on every word of the raw aggregate buffer and its validity bitmap:
 nullable fact and payload columns under three-valued logic, OR / NOT / IS NULL
 filters, filters on join payloads, MIN / MAX / AVG / COUNT(column) / CASE
 aggregates, one to three joins in random order, an OR over two date keys or a
-multi-value PARTSUPP join -- at the default launch shape and at a TMA-staged
-one; random batches of shareable plans through one shared scan; and a random
+multi-value PARTSUPP join -- at the default launch shape, at a TMA-staged
+one and with warp-compacted rows (two tile shapes); random batches of shareable plans through one shared scan; and a random
 mix through the request loop."""
 import random
 
@@ -21,7 +21,8 @@ pytestmark = pytest.mark.gpu
 
 N = 400_003
 NULLABLE = ("lo_revenue", "c_nation")
-TUNINGS = {"default": None, "tma": dict(block_threads=256, items_per_thread=4, stages=3, ctas_per_sm=2)}
+TUNINGS = {"default": None, "tma": dict(block_threads=256, items_per_thread=4, stages=3, ctas_per_sm=2),
+           "compact": dict(compact=1), "compact_ipt2": dict(block_threads=512, items_per_thread=2, compact=1)}
 
 
 @pytest.fixture(scope="module")

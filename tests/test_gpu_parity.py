@@ -69,24 +69,28 @@ def test_q31_nullable(db):
     assert any(r[2] < r[1] for r in rs), "COUNT(revenue) must skip NULL revenue"
 
 
+@pytest.mark.parametrize("compact", [0, 1])
 @pytest.mark.parametrize("t", [0, 1, 2, 3])
-def test_shared_scan_templates(db, t):
+def test_shared_scan_templates(db, t, compact):
     n = 1_500_000
     ht = load(db, 14, n, queries.BATCH_COLS)
     rng = random.Random(100 + t)
+    tun = _lib.default_tuning()
+    tun.compact = compact
     for _ in range(3):
-        assert_parity(db, queries.template(t, rng, n), ht)
+        assert_parity(db, queries.template(t, rng, n), ht, tun)
 
 
-@pytest.mark.parametrize("bt,ipt,stages,place,merge,bitmaps", [
-    (128, 4, 4, 0, 0, 98304), (256, 8, 2, 0, 1, 0), (512, 2, 3, 2, 0, 98304), (256, 4, 0, 1, 2, 98304),
-    (1024, 1, 2, 0, 2, 0), (256, 4, 6, 2, 1, 98304), (1024, 2, 0, 1, 1, 98304)])
-def test_tuning_invariance(db, bt, ipt, stages, place, merge, bitmaps):
+@pytest.mark.parametrize("bt,ipt,stages,place,merge,bitmaps,compact", [
+    (128, 4, 4, 0, 0, 98304, 0), (256, 8, 2, 0, 1, 0, 0), (512, 2, 3, 2, 0, 98304, 0), (256, 4, 0, 1, 2, 98304, 0),
+    (1024, 1, 2, 0, 2, 0, 0), (256, 4, 6, 2, 1, 98304, 0), (1024, 2, 0, 1, 1, 98304, 0),
+    (1024, 4, 0, 0, 0, 49152, 1), (512, 8, 0, 2, 0, 49152, 1), (1024, 4, 0, 1, 0, 0, 1), (256, 2, 0, 0, 2, 98304, 1)])
+def test_tuning_invariance(db, bt, ipt, stages, place, merge, bitmaps, compact):
     n = 777_777
     ht = load(db, 15, n, queries.Q31_COLS, nulls={"lo_revenue": 100, "c_city": 50})
     t = _lib.default_tuning()
     t.block_threads, t.items_per_thread, t.stages, t.group_placement = bt, ipt, stages, place
-    t.group_merge, t.bitmap_budget = merge, bitmaps
+    t.group_merge, t.bitmap_budget, t.compact = merge, bitmaps, compact
     assert_parity(db, queries.ssb_q31_nullable(n), ht, t)
     assert_parity(db, queries.ssb_q31(n), ht, t)
 

@@ -43,6 +43,9 @@ bool is_visitor_program(const std::string& src);
 // bodies kept); throws std::runtime_error naming what it cannot translate.
 std::string translate_visitor_program(const std::string& src);
 
+// Takes one more reference on a module (dropped with cx_module_release).
+void module_retain(cx_module* m);
+
 // Records `msg` as the calling thread's cx_last_error() and returns `code`.
 int set_error(int code, const std::string& msg);
 

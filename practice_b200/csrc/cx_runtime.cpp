@@ -310,6 +310,7 @@ uint64_t mht_payload_bytes(const LaunchPlan& lp, const std::vector<long long>& r
 struct cx_module {
   std::string key;
   size_t src_hash = 0;
+  uint64_t uid = 0;  // unique per module for the life of the process (graph signatures)
   std::vector<char> cubin;
   LaunchPlan lp;
   ScratchLayout sl;
@@ -427,6 +428,10 @@ uint64_t ctx_scratch_bytes(const cx_exec_ctx* c) { return c->own_scratch_bytes; 
 
 int set_error(int code, const std::string& msg) { return fail(code, "%s", msg.c_str()); }
 
+void module_retain(cx_module* m) {
+  if (m) m->refs.fetch_add(1);
+}
+
 cx::Tuning to_tuning(const cx_tuning* tuning) {
   cx::Tuning t;
   if (tuning) {
@@ -542,8 +547,10 @@ int cx_compile(const char* src, size_t src_len, const char* key, cx_module** out
     }
   }
   auto m = std::make_unique<cx_module>();
+  static std::atomic<uint64_t> next_uid{1};
   m->key = ck;
   m->src_hash = h;
+  m->uid = next_uid.fetch_add(1);
   std::string perr;
   if (!parse_launch_plan(source, m->lp, perr)) return fail(CX_E_INVALID, "cx_compile: %s", perr.c_str());
   m->sl = scratch_layout(m->lp);
@@ -1186,8 +1193,11 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
     // pass the kernel arguments, grids, shared memory and copy sizes.
     std::vector<unsigned char> sig;
     auto put = [&](const void* p, size_t n) { sig.insert(sig.end(), (const unsigned char*)p, (const unsigned char*)p + n); };
-    const void* ids[] = {m, scratch, c->host_stage, c->host_err};
+    // The module by its unique id, not its address: a module freed and a new
+    // one allocated at the same address must not replay the old graph.
+    const void* ids[] = {scratch, c->host_stage, c->host_err};
     put(ids, sizeof ids);
+    put(&m->uid, sizeof m->uid);
     const uint64_t sizes[] = {dim_end, err_off, (uint64_t)npass, (uint64_t)sms};
     put(sizes, sizeof sizes);
     for (const Pass& P : passes) {

@@ -278,21 +278,12 @@ int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Req
   return CX_OK;
 }
 
-// Launches `batch` on `sl` (caller holds s->mu).  On failure the requests are
-// finished with the error.
-void launch(cx_server* s, Slot& sl, std::vector<Request*>& batch, bool shared) {
-  const double t = now_ms();
-  sl.busy = true;
-  sl.shared = shared;
-  sl.reqs = batch;
-  sl.reserved = 0;
-  for (Request* r : batch) {
-    r->status = 0;
-    r->t_launch = t;
-    r->batch_size = (int)batch.size();
-    r->ran_shared = shared;
-    sl.reserved += r->est_bytes;
-  }
+// Launches `batch` on `sl` with module `mod` (the scheduler marked the batch
+// running and retained `mod` under s->mu; this runs without the lock, so
+// submit, wait and the statistics calls are not held up by allocations and
+// kernel enqueues).  `shapes` holds each request's shape index in `mod` for a
+// shared launch.  On failure the requests carry the error code.
+void launch(Slot& sl, std::vector<Request*>& batch, bool shared, cx_module* mod, const std::vector<int>& shapes) {
   int rc = CX_OK;
   size_t need = 0;
   for (Request* r : batch) {
@@ -317,7 +308,7 @@ void launch(cx_server* s, Slot& sl, std::vector<Request*>& batch, bool shared) {
     std::vector<int32_t> params;
     for (size_t i = 0; i < batch.size(); ++i) {
       Request* r = batch[i];
-      q[i].shape = s->shape_index.at(r->shape);
+      q[i].shape = shapes[i];
       q[i].param_off = (int)params.size();
       params.insert(params.end(), r->lits.begin(), r->lits.end());
       q[i].result = (uint64_t*)r->d_res;
@@ -325,14 +316,12 @@ void launch(cx_server* s, Slot& sl, std::vector<Request*>& batch, bool shared) {
       q[i].validity = (uint64_t*)r->d_val;
       q[i].validity_words = r->vwords;
     }
-    sl.mod = s->universe;
-    rc = cx_shared_execute(s->universe, sl.ctx, q.data(), (int)q.size(), params.data(), (int)params.size(), sl.stream);
+    rc = cx_shared_execute(mod, sl.ctx, q.data(), (int)q.size(), params.data(), (int)params.size(), sl.stream);
   } else if (!rc) {
     Request* r = batch[0];
-    sl.mod = r->plain;
     rc = cx_ctx_set_result(sl.ctx, (uint64_t*)r->d_res, r->words, (uint64_t*)r->d_val, r->vwords);
     if (!rc)
-      rc = cx_execute_params(r->plain, sl.ctx, r->plain_param ? r->lits.data() : nullptr,
+      rc = cx_execute_params(mod, sl.ctx, r->plain_param ? r->lits.data() : nullptr,
                              r->plain_param ? (int)r->lits.size() : 0, sl.stream);
   }
   for (Request* r : batch) {
@@ -352,8 +341,6 @@ void launch(cx_server* s, Slot& sl, std::vector<Request*>& batch, bool shared) {
     for (Request* r : batch) r->rc = rc;
     cudaEventRecord(sl.done, sl.stream);
   }
-  ++s->launches;
-  s->launched_queries += batch.size();
 }
 
 // Finishes the launch on `sl` once its event fired (caller holds s->mu).
@@ -382,6 +369,7 @@ void finish(cx_server* s, Slot& sl) {
   sl.reserved = 0;
   sl.reqs.clear();
   sl.busy = false;
+  cx_module_release(sl.mod);  // the reference the scheduler took for this launch
   sl.mod = nullptr;
 }
 
@@ -450,8 +438,33 @@ void scheduler(cx_server* s) {
         }
       }
       if (batch.empty()) break;
-      launch(s, sl, batch, shared);
+      // Mark the batch running and reserve its bytes under the lock; the
+      // launch itself runs without it.  The slot keeps a reference on the
+      // module it launches, so a new shared program compiled meanwhile
+      // cannot unload it while its kernels run.
+      const double t_launch = now_ms();
+      sl.busy = true;
+      sl.shared = shared;
+      sl.reqs = batch;
+      sl.reserved = 0;
+      std::vector<int> shapes;
+      for (Request* r : batch) {
+        r->status = 0;
+        r->t_launch = t_launch;
+        r->batch_size = (int)batch.size();
+        r->ran_shared = shared;
+        sl.reserved += r->est_bytes;
+        if (shared) shapes.push_back(s->shape_index.at(r->shape));
+      }
+      cx_module* mod = shared ? s->universe : head->plain;
+      cx_internal::module_retain(mod);
+      sl.mod = mod;
       s->reserved += sl.reserved;
+      lk.unlock();
+      launch(sl, batch, shared, mod, shapes);
+      lk.lock();
+      ++s->launches;
+      s->launched_queries += batch.size();
       s->peak_reserved = std::max(s->peak_reserved, s->reserved + fixed_bytes(s));
       progressed = true;
     }

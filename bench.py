@@ -63,9 +63,9 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true", help="skip the 6M / 60M single-query legs")
     ap.add_argument("--config-rows", default="6000000,60000000", help="rows of the Q1.1 leg and the Q3.1 legs")
-    ap.add_argument("--serve-rate", type=float, default=1000.0, help="Poisson arrivals per second (serving leg)")
-    ap.add_argument("--serve-requests", type=int, default=2000, help="requests in the serving leg (0 skips it)")
-    ap.add_argument("--serve-low-rate", type=float, default=100.0, help="second, light-load arrival rate")
+    ap.add_argument("--serve-rates", default="50,1000,2000", help="Poisson arrival rates of the serving leg (q/s)")
+    ap.add_argument("--serve-requests", type=int, default=2000, help="most requests per rate (0 skips the leg)")
+    ap.add_argument("--serve-burst", type=int, default=150, help="large queries submitted at once (admission test)")
     ap.add_argument("--serve-slots", type=int, default=1, help="launches in flight in the shared loop")
     return ap.parse_args(argv)
 
@@ -565,21 +565,32 @@ def configs_legs(torch, args, device, peak, stream):
 # -------------------------------------------------------------- serving
 
 
-def serving_leg(db, plans, args, shared_tuning):
-    """The request loop under a Poisson arrival stream drawn from the batch's
-    queries: the shared loop (continuous batching into shared scans) and the
-    plain one-query-at-a-time loop over the same stream, plus each query's
-    latency alone on an idle GPU."""
+def serving_leg(db, args, shared_tuning):
+    """The request loop under Poisson arrival streams of fresh queries (the
+    four templates with new constants per request, and 5 % large-domain
+    queries with 330 MB result buffers): the shared loop (continuous batching
+    into shared scans) and the plain one-query-at-a-time loop over the same
+    streams at several rates, each query's latency alone on an idle GPU, and a
+    burst of large queries that the 40 GiB admission budget has to hold back."""
     import numpy as np
 
-    from practice_b200 import _lib
+    from practice_b200 import _lib, queries
+    from practice_b200.engine import shape_key
 
+    rates = [float(x) for x in args.serve_rates.split(",") if x]
+    counts = [min(args.serve_requests, max(200, int(r * 2))) for r in rates]
+    plans = queries.serving_stream(sum(counts) + 64, args.seed + 7, args.rows)
+    reps = {}
+    for p in plans:
+        reps.setdefault(shape_key(p), p)
+    for p in reps.values():  # the plain kernels of every shape, autotuned
+        if db.tuning_for(p) is None:
+            db.autotune(p, candidates=PLAIN_CANDIDATES, reps=1, persist=False)
     texts = [p.text() for p in plans]
 
-    def stream(srv, rate, n):
-        rng = np.random.default_rng(args.seed)
+    def stream(srv, rate, first, n):
+        rng = np.random.default_rng(args.seed + int(rate))
         arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
-        picks = rng.integers(0, len(plans), n)
         srv.stats(reset=True)
         ids = []
         t0 = time.perf_counter()
@@ -587,53 +598,71 @@ def serving_leg(db, plans, args, shared_tuning):
             target = t0 + arrivals[i]
             while time.perf_counter() < target:
                 pass
-            ids.append(srv.submit(texts[picks[i]]))
+            ids.append(srv.submit(texts[first + i]))
         bad = 0
         for rid in ids:
             info = srv.wait(rid)
             bad += int(info.status != 0 or info.kernel_error != 0)
             srv.release(rid)
         st = srv.stats()
-        return {"queries_per_s": st.queries_per_s, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "max_ms": st.max_ms,
-                "mean_batch": st.mean_batch, "launches": int(st.launches), "failed": bad,
+        return {"requests": n, "queries_per_s": st.queries_per_s, "p50_ms": st.p50_ms, "p99_ms": st.p99_ms,
+                "max_ms": st.max_ms, "mean_batch": st.mean_batch, "launches": int(st.launches), "failed": bad,
                 "peak_reserved_GB": st.peak_reserved_bytes / 1e9}
 
+    out = {"arrivals": "Poisson; fresh constants per request from the 4 templates, 5% large-domain queries "
+                       "(8.25M group slots, 330 MB results); budget 40 GiB", "rates": {}}
     plain = _lib.Server(db.ctx, _lib.server_config(plain_only=1, slots=1))
+    lone = []
     try:
-        for p in plans:  # the plain loop runs each query with its autotuned kernel
+        for p in reps.values():
             plain.prepare(p.text(), db.tuning_for(p))
-        lone = []
-        for t in texts:  # each query alone on an idle GPU, submit to result on the host
+        for t in texts[-64:]:  # queries alone on an idle GPU, submit to result on the host
             for _ in range(2):
                 info = plain.wait(plain.submit(t))
             lone.append(info.latency_ms)
-        n_low = max(50, int(args.serve_requests * args.serve_low_rate / args.serve_rate * 3))
-        plain_stream = stream(plain, args.serve_rate, args.serve_requests)
-        plain_low = stream(plain, args.serve_low_rate, n_low)
+        first = 0
+        for r, n in zip(rates, counts):
+            out["rates"][str(int(r))] = {"plain_loop": stream(plain, r, first, n)}
+            first += n
     finally:
         plain.close()
+    lone_ms = float(np.median(lone))
+    out["lone_query_ms"] = {"median": lone_ms, "p99": float(np.percentile(lone, 99)), "max": float(np.max(lone))}
     cfg = _lib.server_config(max_batch=64, slots=args.serve_slots)
     if shared_tuning is not None:
         cfg.shared_tuning = shared_tuning
     srv = _lib.Server(db.ctx, cfg)
     try:
-        for p in plans:  # short queues run these autotuned plain kernels
+        for p in reps.values():  # short queues run these autotuned plain kernels
             srv.prepare(p.text(), db.tuning_for(p))
-        shared_stream = stream(srv, args.serve_rate, args.serve_requests)
-        shared_low = stream(srv, args.serve_low_rate, n_low)
+        first = 0
+        for r, n in zip(rates, counts):
+            row = out["rates"][str(int(r))]
+            row["shared_loop"] = stream(srv, r, first, n)
+            row["shared_vs_plain_queries_per_s"] = row["shared_loop"]["queries_per_s"] / max(
+                row["plain_loop"]["queries_per_s"], 1e-9)
+            row["shared_p99_vs_lone"] = row["shared_loop"]["p99_ms"] / lone_ms
+            row["plain_p99_vs_lone"] = row["plain_loop"]["p99_ms"] / lone_ms
+            first += n
+        # Burst: more large queries than the budget holds at once.
+        import random as _random
+        rng = _random.Random(args.seed + 11)
+        wide = [queries.wide_groups(rng, args.rows).text() for _ in range(args.serve_burst)]
+        srv.stats(reset=True)
+        t0 = time.perf_counter()
+        ids = [srv.submit(t) for t in wide]
+        bad = 0
+        for rid in ids:
+            info = srv.wait(rid)
+            bad += int(info.status != 0 or info.kernel_error != 0)
+            srv.release(rid)
+        st = srv.stats()
+        out["burst"] = {"queries": len(wide), "result_MB_each": 330.0, "wall_s": time.perf_counter() - t0,
+                        "peak_reserved_GB": st.peak_reserved_bytes / 1e9, "budget_GB": (40 << 30) / 1e9,
+                        "failed": bad, "launches": int(st.launches), "mean_batch": st.mean_batch}
     finally:
         srv.close()
-    lone_ms = float(np.median(lone))
-    return {"arrivals": f"Poisson, drawn from the batch's {len(plans)} queries; budget 40 GiB",
-            "lone_query_ms": {"median": lone_ms, "max": float(np.max(lone))},
-            "high_load": {"rate_per_s": args.serve_rate, "requests": args.serve_requests,
-                          "shared_loop": shared_stream, "plain_loop": plain_stream,
-                          "shared_vs_plain_queries_per_s": shared_stream["queries_per_s"] / max(plain_stream["queries_per_s"], 1e-9),
-                          "shared_p99_vs_lone": shared_stream["p99_ms"] / lone_ms},
-            "light_load": {"rate_per_s": args.serve_low_rate, "requests": n_low,
-                           "shared_loop": shared_low, "plain_loop": plain_low,
-                           "shared_p99_vs_lone": shared_low["p99_ms"] / lone_ms,
-                           "plain_p99_vs_lone": plain_low["p99_ms"] / lone_ms}}
+    return out
 
 
 # ----------------------------------------------------------------- main
@@ -701,7 +730,7 @@ def main():
     serving = None
     if rank == 0 and world == 1 and args.serve_requests > 0 and shared is not None:
         try:
-            serving = serving_leg(db, plans, args, db.shared_tuning_for(plans))
+            serving = serving_leg(db, args, db.shared_tuning_for(plans))
         except Exception as e:  # reported, not fatal
             serving = {"error": str(e)[:300]}
 

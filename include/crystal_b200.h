@@ -225,6 +225,16 @@ int cx_shared_codegen(const char* const* plans, const size_t* plan_lens, int nsh
 int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queries, int nq, const int32_t* params,
                       int nparams, void* stream);
 
+/* cx_shared_execute over the fact-table rows [row0, row0 + nrows) only (the
+ * range is clipped to the table; nrows = UINT64_MAX runs to its end).  With
+ * keep[q] != 0, query q's result and validity words are not zeroed first: the
+ * launch adds this range's rows to what earlier ranges left there, so a query
+ * can be answered over consecutive launches that each scan one range (the
+ * request loop's circular scan lets queries join at any range boundary).
+ * keep may be NULL (every query starts from zero). */
+int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queries, int nq, const int32_t* params,
+                           int nparams, uint64_t row0, uint64_t nrows, const uint8_t* keep, void* stream);
+
 /* Sparse-result compaction: copies every group tuple with a non-zero slot to
  * `dst` in group order and writes the row count to *dev_count (device u64).
  * Same rows as the reference's CompactSparseAggregateResult

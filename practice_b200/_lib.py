@@ -24,7 +24,7 @@ EXPORTS = [
     "cx_ctx_set_scratch", "cx_module_scratch_bytes", "cx_ctx_set_sm_count", "cx_execute",
     "cx_execute_params", "cx_ctx_sync", "cx_ctx_timing", "cx_ctx_kernel_error", "cx_compact_sparse", "cx_compact_sparse_noalloc",
     "cx_gen_uniform", "cx_gen_datekey", "cx_gen_validity", "cx_plan_literals", "cx_shared_codegen",
-    "cx_shared_execute", "cx_ctx_set_column_range", "cx_ctx_set_graph_replay",
+    "cx_shared_execute", "cx_shared_execute_rows", "cx_ctx_set_column_range", "cx_ctx_set_graph_replay",
     "cx_server_config_default", "cx_server_create", "cx_server_prepare", "cx_server_prepare_tuned",
     "cx_server_submit", "cx_server_wait",
     "cx_server_fetch", "cx_server_release", "cx_server_get_stats", "cx_server_destroy", "cx_finalize",
@@ -139,6 +139,8 @@ def _load() -> C.CDLL:
         "cx_shared_codegen": (C.c_int, [C.POINTER(C.c_char_p), C.POINTER(sz), C.c_int, C.POINTER(Tuning), C.c_char_p,
                                         sz, C.POINTER(sz)]),
         "cx_shared_execute": (C.c_int, [vp, vp, C.POINTER(SharedQuery), C.c_int, C.POINTER(C.c_int32), C.c_int, vp]),
+        "cx_shared_execute_rows": (C.c_int, [vp, vp, C.POINTER(SharedQuery), C.c_int, C.POINTER(C.c_int32), C.c_int,
+                                             u64, u64, C.POINTER(C.c_uint8), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -278,6 +280,17 @@ class ExecCtx:
         pa = (C.c_int32 * max(len(params), 1))(*params)
         check(lib.cx_shared_execute(module.handle, self.handle, qa, nq, pa, len(params), stream or None),
               "cx_shared_execute")
+
+    def shared_execute_rows(self, module: Module, queries, params, row0: int, nrows: int, keep=None,
+                            stream: int = 0) -> None:
+        """The batch over fact rows [row0, row0 + nrows); queries whose `keep`
+        entry is true add to the result earlier row ranges left."""
+        nq = len(queries)
+        qa = (SharedQuery * max(nq, 1))(*queries)
+        pa = (C.c_int32 * max(len(params), 1))(*params)
+        ka = (C.c_uint8 * max(nq, 1))(*[1 if k else 0 for k in keep]) if keep is not None else None
+        check(lib.cx_shared_execute_rows(module.handle, self.handle, qa, nq, pa, len(params), row0, nrows, ka,
+                                         stream or None), "cx_shared_execute_rows")
 
     def sync(self) -> None:
         check(lib.cx_ctx_sync(self.handle), "cx_ctx_sync")

@@ -25,6 +25,7 @@ struct CxSQ {
   int param_off;
   int smem_acc;             // u64 offset of its group table in shared memory, -1 = global atomics
   int smem_bits;            // u32 offset of its touched / seen bits in shared memory
+  int keep;                 // 1 = add to the result left by earlier row ranges (not zeroed)
 };
 
 struct CxArgs {

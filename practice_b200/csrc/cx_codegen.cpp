@@ -2009,8 +2009,10 @@ struct SharedGen {
     src << "    default: break;\n";
     src << "  }\n";
     src << "  const long long nv = (nw + 63) / 64;\n";
-    src << "  for (long long i = threadIdx.x; i < nw; i += blockDim.x) Q.result[i] = 0ULL;\n";
-    src << "  for (long long i = threadIdx.x; i < nv; i += blockDim.x) Q.validity[i] = 0ULL;\n";
+    src << "  if (!Q.keep) {  // a query continuing over a later row range keeps its result\n";
+    src << "    for (long long i = threadIdx.x; i < nw; i += blockDim.x) Q.result[i] = 0ULL;\n";
+    src << "    for (long long i = threadIdx.x; i < nv; i += blockDim.x) Q.validity[i] = 0ULL;\n";
+    src << "  }\n";
     src << "  if (Q.touched)\n";
     src << "    for (long long i = threadIdx.x; i < nt; i += blockDim.x) Q.touched[i] = 0u;\n";
     src << "}\n\n";

@@ -929,6 +929,11 @@ int cx_shared_codegen(const char* const* plans, const size_t* lens, int nshapes,
 
 int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queries, int nq, const int32_t* params,
                       int nparams, void* stream_v) {
+  return cx_shared_execute_rows(m, c, queries, nq, params, nparams, 0, UINT64_MAX, nullptr, stream_v);
+}
+
+int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queries, int nq, const int32_t* params,
+                           int nparams, uint64_t row0, uint64_t nrows, const uint8_t* keep, void* stream_v) {
   if (!m || !c || (!queries && nq > 0) || nq < 0 || nparams < 0 || (nparams > 0 && !params))
     return fail(CX_E_INVALID, "cx_shared_execute: bad argument");
   const LaunchPlan& lp = m->lp;
@@ -946,13 +951,18 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
     rows[t] = (long long)it->second;
     a.rows[t] = rows[t];
   }
+  // The fact-table rows this launch scans: [row0, row0 + nrows), clipped to the table.
+  const uint64_t fact_rows = lp.tables.empty() ? 0 : (uint64_t)rows[0];
+  if (row0 > fact_rows) return fail(CX_E_INVALID, "cx_shared_execute: row range starts past the fact table");
+  const uint64_t range_rows = std::min<uint64_t>(nrows, fact_rows - row0);
+  if (!lp.tables.empty()) a.rows[0] = (long long)range_rows;
   for (const auto& col : lp.cols) {
     auto it = c->buffers.find(col.name);
     if (it == c->buffers.end() || (!it->second.first && rows[col.table] > 0))
       return fail(CX_E_MISSING, "cx_shared_execute: buffer %s is not in the execution context", col.name.c_str());
     if (it->second.second < (uint64_t)rows[col.table])
       return fail(CX_E_CAPACITY, "cx_shared_execute: buffer %s is shorter than its table", col.name.c_str());
-    a.col[col.slot] = (const int*)it->second.first;
+    a.col[col.slot] = (const int*)it->second.first + (col.table == 0 ? row0 : 0);
   }
   // Filter-table windows from the registered column ranges.
   for (const auto& fc : lp.fcols) {
@@ -1102,6 +1112,7 @@ int cx_shared_execute(cx_module* m, cx_exec_ctx* c, const cx_shared_query* queri
       poff += sh.nlits;
       hsq[j].smem_acc = -1;
       hsq[j].smem_bits = 0;
+      hsq[j].keep = keep ? (keep[order[q0 + j]] ? 1 : 0) : 0;
       if (!sh.smem_ok) continue;
       const uint64_t tw = tab_words + sh.groups * (uint64_t)sh.naggs;
       const uint64_t bw = bit_words + sh.tw * (uint64_t)(1 + sh.nseen);

@@ -13,6 +13,9 @@
 * ``template(t, rng)`` -- the four shared-scan templates: T0 range filters +
   scalar SUM; T1 date join + GROUP BY year; T2 three joins + GROUP BY
   (nation, year); T3 four joins + GROUP BY (brand, year) (<= 7,000 groups).
+* ``wide_groups`` / ``serving_stream`` -- the serving workload: the templates
+  with fresh constants per request plus a large-domain query (8.25M group
+  slots, a 330 MB result, <= 90,000 groups present).
 * ``kat_*`` -- the five queries of test/nullable_data/queries.sql.
 * ``or_join_year`` -- the OR-join over two fact keys of
   test/queries/sql/custom1.sql: (lo_orderdate = d_datekey OR lo_commitdate =
@@ -191,6 +194,35 @@ def template(t: int, rng: random.Random, fact_rows: int = 600_000_000) -> Plan:
 def batch(n: int, seed: int, fact_rows: int = 600_000_000) -> list[Plan]:
     rng = random.Random(seed)
     return [template(rng.randrange(4), rng, fact_rows) for _ in range(n)]
+
+
+def wide_groups(rng: random.Random, fact_rows: int = 600_000_000) -> Plan:
+    """A large-domain query of the serving stream: customer and supplier region
+    joins, a year, a 3-value discount range; GROUP BY (c_city, s_city,
+    lo_discount, d_month).  The group domain is 250 * 250 * 11 * 12 =
+    8,250,000 slots (a 330 MB result buffer) of which at most 50 * 50 * 3 * 12 =
+    90,000 groups occur."""
+    tables = ssb_tables(fact_rows, BATCH_COLS)
+    r = rng.randint(0, 4)
+    s = rng.randint(0, 4)
+    y = rng.randint(1992, 1998)
+    d0 = rng.randint(0, 8)
+    b = PlanBuilder(tables, "LINEORDER", name="T4")
+    b.filter(and_(col("lo_discount").ge(d0), col("lo_discount").le(d0 + 2)))
+    b.join("CUSTOMER", "lo_custkey", where=col("c_region").eq(r))
+    b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(s))
+    b.join("DDATE", "lo_orderdate", where=col("d_year").eq(y))
+    return b.aggregate([_g("c_city"), _g("s_city"), _g("lo_discount"), _g("d_month")], [("sum", col("lo_revenue"))])
+
+
+def serving_stream(n: int, seed: int, fact_rows: int = 600_000_000, wide_share: float = 0.05) -> list[Plan]:
+    """Requests of the serving workload: the four batch templates with fresh
+    random constants each, and with probability `wide_share` a large-domain
+    query (`wide_groups`); group cardinalities from 1 to 90,000, result
+    buffers from 8 bytes to 330 MB."""
+    rng = random.Random(seed)
+    return [wide_groups(rng, fact_rows) if rng.random() < wide_share else template(rng.randrange(4), rng, fact_rows)
+            for _ in range(n)]
 
 
 # ------------------------------------------------------- known-answer set

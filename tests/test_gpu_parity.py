@@ -399,3 +399,35 @@ def test_join_keys_outside_the_slot_window(db, budget, nullable_payload):
     from practice_b200.engine import make_tuning
     for ipt, stages in ((4, 0), (2, 2)):
         assert_parity(db, plan, ht, make_tuning(items_per_thread=ipt, stages=stages, bitmap_budget=budget))
+
+
+@pytest.mark.parametrize("splits", [[0, 400_000, 1_000_000], [0, 1024, 512_000, 899_968]])
+def test_shared_scan_over_row_ranges_accumulates(db, splits):
+    """A batch answered by consecutive launches over row ranges -- the first
+    zeroing each query's result, the later ones adding to it (keep) -- equals
+    the oracle over the whole table, for every query; a query that joins at a
+    later range and wraps around to the first covers the table too."""
+    n = 1_000_003
+    ht = load(db, 41, n, queries.BATCH_COLS)
+    plans = queries.batch(12, 41, n)
+    prog = db.shared_program(plans)
+    qs, params, bufs = db.shared_prepare(prog, plans)
+    for t, r in db.rows.items():
+        db.ctx.set_rows(t, r)
+    stream = db.torch.cuda.current_stream().cuda_stream
+    bounds = splits + [n]
+    ranges = [(bounds[i], bounds[i + 1] - bounds[i]) for i in range(len(splits))]
+    # Queries 0..5 start at the first range; queries 6..11 start at the second
+    # and wrap around to the first at the end.
+    order_a = ranges
+    order_b = ranges[1:] + ranges[:1]
+    for k in range(len(ranges)):
+        db.ctx.shared_execute_rows(prog.module, qs[:6], params, order_a[k][0], order_a[k][1], keep=[k > 0] * 6,
+                                   stream=stream)
+        db.ctx.sync()
+        db.ctx.shared_execute_rows(prog.module, qs[6:], params, order_b[k][0], order_b[k][1], keep=[k > 0] * 6,
+                                   stream=stream)
+        db.ctx.sync()
+    for p, (res, val, words) in zip(plans, bufs):
+        ref = oracle_run(p, ht)
+        np.testing.assert_array_equal(res.cpu().numpy().view(np.uint64)[:words], ref.words[:words], err_msg=p.name)

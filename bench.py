@@ -66,6 +66,8 @@ def parse(argv=None):
     ap.add_argument("--serve-rates", default="50,1000,2000", help="Poisson arrival rates of the serving leg (q/s)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="most requests per rate (0 skips the leg)")
     ap.add_argument("--serve-burst", type=int, default=150, help="large queries submitted at once (admission test)")
+    ap.add_argument("--serve-chunk-rows", type=int, default=75_000_000,
+                    help="row range of one launch of the circular loop (0 skips it)")
     ap.add_argument("--serve-slots", type=int, default=1, help="launches in flight in the shared loop")
     return ap.parse_args(argv)
 
@@ -628,6 +630,25 @@ def serving_leg(db, args, shared_tuning):
         plain.close()
     lone_ms = float(np.median(lone))
     out["lone_query_ms"] = {"median": lone_ms, "p99": float(np.percentile(lone, 99)), "max": float(np.max(lone))}
+    # The circular loop: each shared launch scans the next range of
+    # serve_chunk_rows rows, so an arrival waits for one range, not a whole scan.
+    if args.serve_chunk_rows > 0:
+        cfg = _lib.server_config(max_batch=64, slots=args.serve_slots, chunk_rows=args.serve_chunk_rows)
+        if shared_tuning is not None:
+            cfg.shared_tuning = shared_tuning
+        srv = _lib.Server(db.ctx, cfg)
+        try:
+            for p in reps.values():
+                srv.prepare(p.text(), db.tuning_for(p))
+            first = 0
+            for r, n in zip(rates, counts):
+                row = out["rates"][str(int(r))]
+                row["circular_loop"] = stream(srv, r, first, n)
+                row["circular_p99_vs_lone"] = row["circular_loop"]["p99_ms"] / lone_ms
+                first += n
+        finally:
+            srv.close()
+        out["circular_chunk_rows"] = args.serve_chunk_rows
     cfg = _lib.server_config(max_batch=64, slots=args.serve_slots)
     if shared_tuning is not None:
         cfg.shared_tuning = shared_tuning

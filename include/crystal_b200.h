@@ -333,6 +333,11 @@ typedef struct cx_server_config {
   int plain_only;         /* 1: every query runs alone through its plain kernel (baseline loop) */
   int min_shared_batch;   /* fewer waiting shareable queries than this run alone (default 5) */
   cx_tuning shared_tuning;/* launch shape of the shared-scan programs */
+  uint64_t chunk_rows;    /* 0: a shared launch scans the whole fact table.  > 0: circular scan --
+                             each shared launch scans the next range of this many rows (rounded up
+                             to 1024); queries join at any range boundary and finish once they
+                             have covered every row, so arrivals wait for one range, not for a
+                             whole-table launch */
 } cx_server_config;
 
 typedef struct cx_request_info {

@@ -43,6 +43,9 @@ bool is_visitor_program(const std::string& src);
 // bodies kept); throws std::runtime_error naming what it cannot translate.
 std::string translate_visitor_program(const std::string& src);
 
+// Rows the context holds for the module's fact table (its first table), 0 if unknown.
+uint64_t module_fact_rows(const cx_module* m, const cx_exec_ctx* c);
+
 // Takes one more reference on a module (dropped with cx_module_release).
 void module_retain(cx_module* m);
 

@@ -428,6 +428,12 @@ uint64_t ctx_scratch_bytes(const cx_exec_ctx* c) { return c->own_scratch_bytes; 
 
 int set_error(int code, const std::string& msg) { return fail(code, "%s", msg.c_str()); }
 
+uint64_t module_fact_rows(const cx_module* m, const cx_exec_ctx* c) {
+  if (!m || !c || m->lp.tables.empty()) return 0;
+  auto it = c->rows.find(m->lp.tables[0]);
+  return it == c->rows.end() ? 0 : it->second;
+}
+
 void module_retain(cx_module* m) {
   if (m) m->refs.fetch_add(1);
 }

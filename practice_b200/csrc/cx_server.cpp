@@ -78,6 +78,12 @@ struct Request {
   double t_submit = 0, t_launch = 0, t_done = 0;
   int batch_size = 0;
   bool ran_shared = false;  // answered by a shared scan (else by its plain kernel)
+  // Circular scans: the query runs over consecutive row ranges of the fact
+  // table, one per launch, until it has covered every row once.
+  bool circ = false;        // joined a circular scan
+  bool started = false;     // holds device result buffers and has scanned at least one range
+  uint64_t rows_left = 0;   // fact rows it still has to scan
+  bool completes = false;   // the launch in flight finishes it
   void* d_res = nullptr;
   void* d_val = nullptr;
   size_t host_off = 0;  // offset of its result in the slot's pinned landing area
@@ -130,6 +136,10 @@ struct cx_server {
   std::map<std::string, cx_tuning> shape_tunings;  // plain launch shape given at prepare, per plan shape
   std::thread th;
   bool stop = false;
+  // Circular scans (cfg.chunk_rows > 0): queries between two of their range
+  // launches, and where the next range starts.
+  std::vector<Request*> circ_idle;
+  uint64_t next_row = 0;
   // Statistics since the last reset.
   std::vector<double> lat;
   uint64_t submitted = 0, completed = 0, rejected = 0, launches = 0, launched_queries = 0;
@@ -283,10 +293,12 @@ int make_request(cx_server* s, const char* plan, size_t len, std::unique_ptr<Req
 // submit, wait and the statistics calls are not held up by allocations and
 // kernel enqueues).  `shapes` holds each request's shape index in `mod` for a
 // shared launch.  On failure the requests carry the error code.
-void launch(Slot& sl, std::vector<Request*>& batch, bool shared, cx_module* mod, const std::vector<int>& shapes) {
+void launch(Slot& sl, std::vector<Request*>& batch, bool shared, cx_module* mod, const std::vector<int>& shapes,
+            uint64_t row0 = 0, uint64_t nrows = UINT64_MAX) {
   int rc = CX_OK;
   size_t need = 0;
   for (Request* r : batch) {
+    if (!r->completes) continue;  // results of finished queries only
     r->host_off = need;
     need += r->words + r->vwords;
   }
@@ -299,12 +311,14 @@ void launch(Slot& sl, std::vector<Request*>& batch, bool shared, cx_module* mod,
   }
   for (Request* r : batch) {
     if (rc) break;
+    if (r->started) continue;  // a circular query keeps its buffers between ranges
     if (cudaMallocAsync(&r->d_res, r->words * 8, sl.stream) != cudaSuccess ||
         cudaMallocAsync(&r->d_val, r->vwords * 8, sl.stream) != cudaSuccess)
       rc = CX_E_CUDA;
   }
   if (!rc && shared) {
     std::vector<cx_shared_query> q(batch.size());
+    std::vector<uint8_t> keep(batch.size());
     std::vector<int32_t> params;
     for (size_t i = 0; i < batch.size(); ++i) {
       Request* r = batch[i];
@@ -315,8 +329,10 @@ void launch(Slot& sl, std::vector<Request*>& batch, bool shared, cx_module* mod,
       q[i].result_words = r->words;
       q[i].validity = (uint64_t*)r->d_val;
       q[i].validity_words = r->vwords;
+      keep[i] = r->started ? 1 : 0;
     }
-    rc = cx_shared_execute(mod, sl.ctx, q.data(), (int)q.size(), params.data(), (int)params.size(), sl.stream);
+    rc = cx_shared_execute_rows(mod, sl.ctx, q.data(), (int)q.size(), params.data(), (int)params.size(), row0, nrows,
+                                keep.data(), sl.stream);
   } else if (!rc) {
     Request* r = batch[0];
     rc = cx_ctx_set_result(sl.ctx, (uint64_t*)r->d_res, r->words, (uint64_t*)r->d_val, r->vwords);
@@ -326,11 +342,13 @@ void launch(Slot& sl, std::vector<Request*>& batch, bool shared, cx_module* mod,
   }
   for (Request* r : batch) {
     if (rc) break;
+    if (!r->completes) continue;
     if (cudaMemcpyAsync(sl.pin + r->host_off, r->d_res, r->words * 8, cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess ||
         cudaMemcpyAsync(sl.pin + r->host_off + r->words, r->d_val, r->vwords * 8, cudaMemcpyDeviceToHost, sl.stream) != cudaSuccess)
       rc = CX_E_CUDA;
   }
   for (Request* r : batch) {
+    if (!r->completes && !rc) continue;  // an error ends every query of the launch
     if (r->d_res) cudaFreeAsync(r->d_res, sl.stream);
     if (r->d_val) cudaFreeAsync(r->d_val, sl.stream);
     r->d_res = r->d_val = nullptr;
@@ -354,7 +372,19 @@ void finish(cx_server* s, Slot& sl) {
   }
   for (Request* r : sl.reqs) {
     if (r->rc == CX_OK && krc != CX_OK && krc != CX_E_KERNEL) r->rc = krc;
-    r->kernel_err = kerr;
+    r->kernel_err |= kerr;
+    if (r->rc == CX_OK && !r->completes) {
+      // A circular query with rows left waits for its next range.
+      r->started = true;
+      s->circ_idle.push_back(r);
+      continue;
+    }
+    if (r->circ && r->rc != CX_OK && !r->completes) {
+      if (r->d_res) cudaFree(r->d_res);
+      if (r->d_val) cudaFree(r->d_val);
+      r->d_res = r->d_val = nullptr;
+    }
+    s->reserved -= std::min(s->reserved, r->est_bytes);
     if (r->rc == CX_OK) {
       r->h_words.assign(sl.pin + r->host_off, sl.pin + r->host_off + r->final_words);
       r->h_val.assign(sl.pin + r->host_off + r->words, sl.pin + r->host_off + r->words + (r->final_words + 63) / 64);
@@ -365,7 +395,6 @@ void finish(cx_server* s, Slot& sl) {
     ++s->completed;
     s->last_done = t;
   }
-  s->reserved -= std::min(s->reserved, sl.reserved);
   sl.reserved = 0;
   sl.reqs.clear();
   sl.busy = false;
@@ -392,12 +421,15 @@ void scheduler(cx_server* s) {
       progressed = true;
     }
     if (progressed) s->cv_done.notify_all();
+    const bool circ_mode = s->cfg.chunk_rows > 0 && !s->cfg.plain_only;
     for (Slot& sl : s->slots) {
-      if (sl.busy || s->pending.empty()) continue;
+      if (sl.busy) continue;
+      const bool circ_waiting = circ_mode && !s->circ_idle.empty();
+      if (s->pending.empty() && !circ_waiting) continue;
       const uint64_t fixed = fixed_bytes(s);
       const uint64_t own = cx_internal::ctx_scratch_bytes(sl.ctx);
       std::vector<Request*> batch;
-      Request* head = s->pending.front();
+      Request* head = s->pending.empty() ? nullptr : s->pending.front();
       // Admission: what is reserved, the scratch the slots own, the scratch
       // this launch adds to its slot and the new queries' bytes must fit the
       // budget.  A launch on an idle GPU always goes (sizes were checked
@@ -405,17 +437,23 @@ void scheduler(cx_server* s) {
       auto admit = [&](uint64_t growth, uint64_t add) {
         return s->reserved + fixed + growth + add <= s->cfg.budget_bytes || (s->reserved == 0 && batch.empty());
       };
-      bool shared = head->shared && s->universe && s->shape_index.at(head->shape) < (int)s->universe_shapes;
-      if (shared) {
+      auto in_universe = [&](const Request* r) {
+        return r->shared && s->universe && s->shape_index.at(r->shape) < (int)s->universe_shapes;
+      };
+      bool shared = head && in_universe(head);
+      if (shared && !circ_waiting) {
         // A short queue runs its head alone through the plain kernel: one
         // shared launch costs about as much as a few plain ones.
         int ready = 0;
         for (Request* r : s->pending) {
-          if (!r->shared || s->shape_index.at(r->shape) >= (int)s->universe_shapes || ready >= s->cfg.min_shared_batch) break;
+          if (!in_universe(r) || ready >= s->cfg.min_shared_batch) break;
           ++ready;
         }
         if (ready < s->cfg.min_shared_batch) shared = false;
       }
+      // Queries between two ranges of a circular scan always continue; a
+      // non-shareable head runs alone first.
+      if (circ_waiting && (!head || in_universe(head))) shared = true;
       if (!shared) {
         uint64_t need = 0;
         cx_module_scratch_bytes(head->plain, sl.ctx, &need);
@@ -426,22 +464,50 @@ void scheduler(cx_server* s) {
       } else {
         uint64_t add = 0;
         std::vector<int> shapes;
+        if (circ_mode) {
+          while (!s->circ_idle.empty() && (int)batch.size() < s->cfg.max_batch) {
+            batch.push_back(s->circ_idle.front());
+            shapes.push_back(s->shape_index.at(s->circ_idle.front()->shape));
+            s->circ_idle.erase(s->circ_idle.begin());
+          }
+        }
         while (!s->pending.empty() && (int)batch.size() < s->cfg.max_batch) {
           Request* r = s->pending.front();
-          if (!r->shared || s->shape_index.at(r->shape) >= (int)s->universe_shapes) break;
+          if (!in_universe(r)) break;
           shapes.push_back(s->shape_index.at(r->shape));
           const uint64_t need = cx_internal::shared_scratch_need(s->universe, shapes.data(), (int)shapes.size());
-          if (!admit(cx_internal::grown_scratch(own, need) - own, add + r->est_bytes)) break;
+          if (!admit(cx_internal::grown_scratch(own, need) - own, add + r->est_bytes)) {
+            shapes.pop_back();
+            break;
+          }
           add += r->est_bytes;
           batch.push_back(r);
           s->pending.pop_front();
         }
       }
       if (batch.empty()) break;
-      // Mark the batch running and reserve its bytes under the lock; the
-      // launch itself runs without it.  The slot keeps a reference on the
-      // module it launches, so a new shared program compiled meanwhile
-      // cannot unload it while its kernels run.
+      // The row range of a circular launch; every other launch covers the table.
+      uint64_t row0 = 0, nrows = UINT64_MAX;
+      if (shared && circ_mode) {
+        const uint64_t fact_rows = cx_internal::module_fact_rows(s->universe, sl.ctx);
+        row0 = s->next_row < fact_rows ? s->next_row : 0;
+        nrows = std::min<uint64_t>(s->cfg.chunk_rows, fact_rows - row0);
+        s->next_row = row0 + nrows >= fact_rows ? 0 : row0 + nrows;
+        for (Request* r : batch) {
+          if (!r->circ) {
+            r->circ = true;
+            r->rows_left = fact_rows;
+          }
+          r->rows_left -= std::min(r->rows_left, nrows);
+          r->completes = r->rows_left == 0;
+        }
+      } else {
+        for (Request* r : batch) r->completes = true;
+      }
+      // Mark the batch running and reserve the bytes of its new queries under
+      // the lock; the launch itself runs without it.  The slot keeps a
+      // reference on the module it launches, so a new shared program compiled
+      // meanwhile cannot unload it while its kernels run.
       const double t_launch = now_ms();
       sl.busy = true;
       sl.shared = shared;
@@ -449,19 +515,20 @@ void scheduler(cx_server* s) {
       sl.reserved = 0;
       std::vector<int> shapes;
       for (Request* r : batch) {
+        if (r->status == 1) {  // first launch of this query
+          r->t_launch = t_launch;
+          s->reserved += r->est_bytes;
+        }
         r->status = 0;
-        r->t_launch = t_launch;
         r->batch_size = (int)batch.size();
         r->ran_shared = shared;
-        sl.reserved += r->est_bytes;
         if (shared) shapes.push_back(s->shape_index.at(r->shape));
       }
       cx_module* mod = shared ? s->universe : head->plain;
       cx_internal::module_retain(mod);
       sl.mod = mod;
-      s->reserved += sl.reserved;
       lk.unlock();
-      launch(sl, batch, shared, mod, shapes);
+      launch(sl, batch, shared, mod, shapes, row0, nrows);
       lk.lock();
       ++s->launches;
       s->launched_queries += batch.size();
@@ -470,7 +537,7 @@ void scheduler(cx_server* s) {
     }
     bool busy = false;
     for (const Slot& sl : s->slots) busy = busy || sl.busy;
-    if (s->stop && !busy && s->pending.empty()) break;
+    if (s->stop && !busy && s->pending.empty() && s->circ_idle.empty()) break;
     if (!progressed) s->cv_sched.wait_for(lk, std::chrono::microseconds(busy ? 20 : 2000));
   }
 }
@@ -486,6 +553,7 @@ void cx_server_config_default(cx_server_config* cfg) {
   cfg->max_batch = 64;
   cfg->slots = 1;
   cfg->min_shared_batch = 5;
+  cfg->chunk_rows = 0;
   cfg->plain_only = 0;
   cx_tuning_default(&cfg->shared_tuning);
   cfg->shared_tuning.block_threads = 1024;
@@ -500,6 +568,8 @@ int cx_server_create(const cx_exec_ctx* tables, const cx_server_config* cfg, cx_
   if (cfg) s->cfg = *cfg;
   else cx_server_config_default(&s->cfg);
   if (s->cfg.min_shared_batch < 1) s->cfg.min_shared_batch = 1;
+  // Range starts stay 4 KiB aligned (bulk-copy alignment of every fact column).
+  if (s->cfg.chunk_rows) s->cfg.chunk_rows = (s->cfg.chunk_rows + 1023) / 1024 * 1024;
   if (s->cfg.max_batch < 1 || s->cfg.max_batch > 256 || s->cfg.slots < 1 || s->cfg.slots > 8 || s->cfg.budget_bytes == 0)
     return serr(CX_E_INVALID, "cx_server_create: max_batch 1..256, slots 1..8 and a non-zero budget");
   if (cudaGetDevice(&s->device) != cudaSuccess) return serr(CX_E_NO_DEVICE, "cx_server_create: no CUDA device");

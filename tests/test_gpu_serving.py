@@ -158,3 +158,36 @@ def test_server_short_queues_run_plain_kernels(db):
         assert all(i.batch_size == 1 and i.shared == 0 for i in infos)
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("chunk", [1_000_000, 1_500_000])
+def test_circular_scan_results_equal_alone_and_oracle(db, chunk):
+    """Circular scans: each shared launch covers the next row range; queries
+    that arrive join at a range boundary, carry their partial results between
+    launches and finish after one revolution.  Every result equals the query
+    alone and the oracle, also for queries that join in the middle and wrap
+    around the end of the table."""
+    n = 4_000_037
+    ht = load(db, 52, n)
+    rng = random.Random(8)
+    plans = [queries.template(rng.randrange(4), rng, n) for _ in range(40)]
+    plans += [avg_plan(n, 1995)] * 2
+    random.Random(9).shuffle(plans)
+    srv = _lib.Server(db.ctx, _lib.server_config(max_batch=16, slots=1, min_shared_batch=2, chunk_rows=chunk))
+    try:
+        for t in range(4):
+            srv.prepare(queries.template(t, random.Random(t), n).text())
+        srv.prepare(plans[[p.name for p in plans].index("avg")].text())
+        ids = []
+        for i, p in enumerate(plans):  # arrivals spread over several ranges
+            ids.append(srv.submit(p.text()))
+            if i % 7 == 6:
+                srv.wait(ids[-1], 120_000)
+        infos = [check(srv, db, rid, p, ht) for rid, p in zip(ids, plans)]
+        st = srv.stats()
+        assert st.completed == len(plans) and st.rejected == 0
+        assert any(i.shared == 1 for i in infos)
+        # A revolution takes ceil(n / chunk) launches, so shared queries ran in several.
+        assert st.launches >= (n + chunk - 1) // chunk
+    finally:
+        srv.close()

@@ -90,8 +90,8 @@ EXPANDING = {"or_year": "or_join_year", "or_filter": "or_join_then_filter", "mht
 def tour(args) -> None:
     """Runs every kernel of the library once or twice on a generated table:
     the plain fused scan (Q1.1-, Q3.1- and nullable Q3.1-shaped queries, a
-    parametric one, AVG finalisation, an OR-join and a multi-value hash join
-    with its five build kernels), a shared-scan batch, result
+    parametric one, AVG finalisation, an OR-join and two multi-value hash
+    joins with their five build kernels), a shared-scan batch, result
     finalisation on the device and sparse compaction (both entry points)."""
     import numpy as np
 
@@ -109,7 +109,7 @@ def tour(args) -> None:
     b = PlanBuilder(queries.ssb_tables(args.rows, cols), "LINEORDER", name="avg")
     b.join("DDATE", "lo_orderdate")
     plans.append(b.aggregate([queries._g("d_year")], [("avg", col("lo_supplycost")), ("min", col("lo_quantity"))]))
-    plans += [queries.or_join_year(args.rows), queries.mht_year_tier(args.rows)]
+    plans += [queries.or_join_year(args.rows), queries.mht_year_tier(args.rows), queries.mht_brand(args.rows)]
     for p in plans:
         m = db.compile(p)
         res, val = db.alloc_result(m)

@@ -235,11 +235,13 @@ def config_block(args):
 SHARED_DRAM_BYTES_PER_ROW = (968.458240e6 + 3.693568e6) / 30e6
 
 PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=bm,
-                         prefetch=pf, group_placement=pl, compact=cp)
-                    for bt, ipt, st, bm, pf, pl, cp in ((1024, 4, 0, 49152, 1, 0, 0), (1024, 4, 0, 0, 1, 4, 0),
-                                                        (512, 2, 0, 0, 1, 4, 0), (1024, 2, 0, 0, 0, 4, 0),
-                                                        (512, 8, 4, 0, 0, 0, 0), (1024, 4, 0, 49152, 1, 0, 1),
-                                                        (512, 4, 0, 49152, 1, 0, 1), (1024, 2, 0, 49152, 1, 0, 1))]
+                         prefetch=pf, group_placement=pl, compact=cp, table_budget=tb)
+                    for bt, ipt, st, bm, pf, pl, cp, tb in (
+                        (1024, 4, 0, 49152, 1, 0, 0, 98304), (1024, 4, 0, 49152, 1, 0, 0, 0),
+                        (1024, 4, 0, 0, 1, 4, 0, 0), (512, 2, 0, 0, 1, 4, 0, 0), (1024, 2, 0, 0, 0, 4, 0, 98304),
+                        (512, 8, 4, 0, 0, 0, 0, 0), (1024, 4, 0, 49152, 1, 0, 1, 98304),
+                        (512, 4, 0, 49152, 1, 0, 1, 98304), (1024, 2, 0, 49152, 1, 0, 1, 98304),
+                        (1024, 2, 0, 49152, 1, 0, 1, 0))]
 SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=2, producer_warps=pw,
                           group_merge=gm)
                      for bt, ipt, st, pw, gm in ((1024, 1, 3, 11, 0), (1024, 1, 3, 11, 3), (1024, 1, 3, 14, 0),

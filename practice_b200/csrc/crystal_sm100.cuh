@@ -581,6 +581,55 @@ CX_DEVICE void BlockProbeExactBitmap(int tid, K (&items)[ITEMS_PER_THREAD], int 
   }
 }
 
+// Exact membership from a payload table in shared memory: byte h is 0xFF when
+// slot h does not hold the key key_min + h, else the slot's payload minus its
+// catalog minimum, or 0xFE for a payload outside the catalog range.  Keys
+// outside the table's window probe the PHT (pair layout).
+template <typename K, int BLOCK_THREADS, int ITEMS_PER_THREAD>
+CX_DEVICE void BlockProbeExactTable(int tid, K (&items)[ITEMS_PER_THREAD], int (&flags)[ITEMS_PER_THREAD],
+                                    const unsigned char* table, const K* ht, int ht_len, K key_min, int num_items) {
+  const bool guarded = !cx_detail::tile_is_full<BLOCK_THREADS, ITEMS_PER_THREAD>(num_items);
+#pragma unroll
+  for (int i = 0; i < ITEMS_PER_THREAD; ++i) {
+    if (guarded && i * BLOCK_THREADS + tid >= num_items) continue;
+    const K d = items[i] - key_min;
+    int hit;
+    if (sizeof(K) == 4 ? (unsigned)d < (unsigned)ht_len : (d >= K(0) && d < K(ht_len))) {
+      hit = table[(unsigned)d] != 0xFFu;
+    } else {
+      hit = 0;
+      if (flags[i]) {
+        const int h = cx_detail::pht_slot<K>(items[i], ht_len, key_min);
+        hit = (h >= 0 && ht[(long long)h << 1] == items[i]) ? 1 : 0;
+      }
+    }
+    flags[i] = (int)(flags[i] != 0) & hit;
+  }
+}
+
+// The payload of every flagged item from the same table (membership already
+// known): its catalog minimum plus the byte, or the PHT's payload where the
+// byte is 0xFE or the key lies outside the window.
+template <typename K, typename V, int BLOCK_THREADS, int ITEMS_PER_THREAD>
+CX_DEVICE void BlockFetchPayloadTable(int tid, K (&items)[ITEMS_PER_THREAD], V (&res)[ITEMS_PER_THREAD],
+                                      int (&flags)[ITEMS_PER_THREAD], const unsigned char* table, const K* ht,
+                                      int ht_len, K key_min, V value_min, int num_items) {
+  cx_detail::for_items<BLOCK_THREADS, ITEMS_PER_THREAD>(
+      tid, num_items, !cx_detail::tile_is_full<BLOCK_THREADS, ITEMS_PER_THREAD>(num_items), [&](int i) {
+        if (!flags[i]) return;
+        const K d = items[i] - key_min;
+        const unsigned b = (sizeof(K) == 4 ? (unsigned)d < (unsigned)ht_len : (d >= K(0) && d < K(ht_len)))
+                               ? (unsigned)table[(unsigned)d]
+                               : 0xFEu;
+        if (b < 0xFEu) {
+          res[i] = value_min + static_cast<V>(b);
+        } else {
+          const int h = cx_detail::pht_slot<K>(items[i], ht_len, key_min);
+          if (h >= 0) res[i] = static_cast<V>(ht[((long long)h << 1) + 1]);
+        }
+      });
+}
+
 // PHT_2 payload of every flagged item whose membership is already known (the
 // slot of its key holds the key): one table load per qualifying row.
 template <typename K, typename V, int BLOCK_THREADS, int ITEMS_PER_THREAD>

@@ -98,6 +98,7 @@ struct Emitter {
   std::map<std::string, int> col_slot;  // column -> CxArgs.col slot
   std::vector<std::string> col_order;
   std::map<std::string, int> ht_slot;   // dimension -> CxArgs.ht slot
+  std::set<std::string> ptable;          // joins whose scan keeps a payload table in shared memory
   std::set<std::string> payload_valid;  // payload columns that carry validity (PHT_2V)
 
   // Per-kernel register state.
@@ -494,8 +495,49 @@ struct Emitter {
   static bool exact_window_ok(const Join& j) {
     return j.keymin >= -2147483648LL && j.keymin + j.len - 1 <= 2147483647LL;
   }
+  // Joins whose payload's catalog range fits a byte get a payload table
+  // instead (one byte per slot, see BlockProbeExactTable), in join order while
+  // the tables fit `table_budget` bytes of shared memory.
+  bool table_candidate(const Join& j) const {
+    return !j.multi && !j.expands() && exact_window_ok(j) && !j.payload.empty() && !payload_valid.count(j.payload) &&
+           j.prange_card >= 1 && j.prange_card <= 254;
+  }
+  void choose_tables() {
+    unsigned long long used = 0;
+    for (const auto& s : p.steps) {
+      if (s.kind != Step::JoinStep || !table_candidate(s.join)) continue;
+      const unsigned long long bytes = (((unsigned long long)s.join.len + 3) / 4 * 4 + 15) & ~15ULL;
+      if (used + bytes > (unsigned long long)std::max(0, tu.table_budget)) continue;
+      ptable.insert(s.join.dim);
+      used += bytes;
+    }
+  }
+  void emit_payload_table(const Join& j) {
+    const int h = ht_slot.at(j.dim);
+    const long long words = (j.len + 3) / 4;
+    const std::string kname = "occupancy_" + lower(j.dim);
+    meta << "kernel " << kname << " fixed " << (words + 255) / 256 << " 256 0\n";
+    src << "extern \"C\" __global__ void __launch_bounds__(256) " << kname << "(const CxArgs a) {\n";
+    src << param_decl();
+    src << "  const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n";
+    src << "  if (w >= " << words << "LL) return;\n";
+    src << "  const int* ht = a.ht[" << h << "];\n";
+    src << "  unsigned bytes = 0u;\n";
+    src << "  for (int b = 0; b < 4; ++b) {\n";
+    src << "    const long long slot = w * 4 + b;\n";
+    src << "    unsigned v = 0xFFu;\n";
+    src << "    if (slot < " << j.len << "LL && ht[slot * 2] == (int)(" << j.keymin << "LL + slot)) {\n";
+    src << "      const long long pv = (long long)ht[slot * 2 + 1] - (" << j.prange_min << "LL);\n";
+    src << "      v = (pv >= 0 && pv < " << j.prange_card << "LL) ? (unsigned)pv : 0xFEu;\n";
+    src << "    }\n";
+    src << "    bytes |= v << (8 * b);\n";
+    src << "  }\n";
+    src << "  a.bm[" << h << "][w] = bytes;\n";
+    src << "}\n\n";
+  }
   void emit_occupancy(const Join& j) {
     if (j.multi) return;
+    if (ptable.count(j.dim)) return emit_payload_table(j);
     const int h = ht_slot.at(j.dim);
     const long long words = (j.len + 31) / 32;
     const std::string kname = "occupancy_" + lower(j.dim);
@@ -619,20 +661,26 @@ struct Emitter {
     const unsigned long long bars_off = off; off += (unsigned long long)NW * std::max(STAGES, 1) * 8;
     const unsigned long long red_off = off; off += (unsigned long long)NW * 8;
     // Join membership bitmaps kept in shared memory (in join order, while they fit the budget).
-    struct SBm { std::string dim, fk; int h; long long len, keymin; unsigned long long words, off; bool pair; };
+    // Payload tables (one byte per slot: membership and payload) take the
+    // joins choose_tables picked; the others get bitmaps while they fit.
+    struct SBm {
+      std::string dim, fk; int h; long long len, keymin; unsigned long long words, off; bool pair, table;
+      long long vmin;
+    };
     std::vector<SBm> sbms;
     {
       unsigned long long used = 0;
       for (const auto& s : p.steps) {
         if (s.kind != Step::JoinStep || s.join.expands() || !exact_window_ok(s.join)) continue;
-        const unsigned long long words = (unsigned long long)((s.join.len + 31) / 32);
+        const bool table = ptable.count(s.join.dim) > 0;
+        const unsigned long long words = (unsigned long long)(table ? (s.join.len + 3) / 4 : (s.join.len + 31) / 32);
         const unsigned long long bytes = ((words * 4) + 15) & ~15ULL;
-        if (used + bytes > (unsigned long long)std::max(0, tu.bitmap_budget)) continue;
+        if (!table && used + bytes > (unsigned long long)std::max(0, tu.bitmap_budget)) continue;
         off = (off + 15) & ~15ULL;
         sbms.push_back({s.join.dim, s.join.fks[0], ht_slot.at(s.join.dim), s.join.len, s.join.keymin, words, off,
-                        !s.join.payload.empty()});
+                        !s.join.payload.empty(), table, s.join.prange_min});
         off += bytes;
-        used += bytes;
+        if (!table) used += bytes;
       }
     }
     bool smem_groups = false;
@@ -939,9 +987,14 @@ struct Emitter {
       ensure_loaded(o, b.fk, ind);
       if (valid_regs.count(b.fk))
         o << ind << "BlockApplyValidityAnd<BLOCK_THREADS, ITEMS_PER_THREAD>(tid, flags, " << b.fk << "_valid, num_tile_items);\n";
-      o << ind << "BlockProbeExactBitmap<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << b.fk << ", flags, s_bm_"
-        << lower(b.dim) << ", " << ht_name(b.dim) << ", " << (b.pair ? 1 : 0) << ", " << b.len << ", " << b.keymin
-        << ", num_tile_items);\n";
+      if (b.table)
+        o << ind << "BlockProbeExactTable<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << b.fk
+          << ", flags, (const unsigned char*)s_bm_" << lower(b.dim) << ", " << ht_name(b.dim) << ", " << b.len << ", "
+          << b.keymin << ", num_tile_items);\n";
+      else
+        o << ind << "BlockProbeExactBitmap<int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << b.fk << ", flags, s_bm_"
+          << lower(b.dim) << ", " << ht_name(b.dim) << ", " << (b.pair ? 1 : 0) << ", " << b.len << ", " << b.keymin
+          << ", num_tile_items);\n";
       exact_dims.insert(b.dim);
     }
     // The steps after the membership tests, in plan order (with compaction:
@@ -967,6 +1020,10 @@ struct Emitter {
             << ", " << j.payload << "_valid, flags, " << ht_name(j.dim) << ", " << ht_name(j.dim) << "_valid, " << j.len
             << ", " << j.keymin << ", num_tile_items);\n";
           valid_regs.insert(j.payload);
+        } else if (ptable.count(j.dim)) {
+          o << ind << "BlockFetchPayloadTable<int, int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << fk << ", " << j.payload
+            << ", flags, (const unsigned char*)s_bm_" << lower(j.dim) << ", " << ht_name(j.dim) << ", " << j.len << ", "
+            << j.keymin << ", (int)(" << j.prange_min << "LL), num_tile_items);\n";
         } else {
           o << ind << "BlockFetchPayloadPHT_2<int, int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << fk << ", " << j.payload
             << ", flags, " << ht_name(j.dim) << ", " << j.len << ", " << j.keymin << ", num_tile_items);\n";
@@ -1679,6 +1736,7 @@ struct Emitter {
     meta << "v 1\n";
     if (nparams >= 0) meta << "params " << nparams << "\n";
     for (size_t t = 0; t < p.tables.size(); ++t) meta << "table " << t << " " << p.tables[t].name << "\n";
+    choose_tables();
     int h = 0;
     for (const auto& s : p.steps) {
       if (s.kind != Step::JoinStep) continue;
@@ -1693,7 +1751,7 @@ struct Emitter {
       meta << "ht " << h << " " << ht_name(s.join.dim) << " " << words << "\n";
       if (!s.join.payload.empty() && payload_valid.count(s.join.payload))
         meta << "htv " << h << " " << (s.join.len + 31) / 32 << "\n";
-      meta << "bm " << h << " " << (s.join.len + 31) / 32 << "\n";
+      meta << "bm " << h << " " << (ptable.count(s.join.dim) ? (s.join.len + 3) / 4 : (s.join.len + 31) / 32) << "\n";
       ++h;
     }
     if (h > CX_MAX_HTS_) throw PlanError("too many joins");
@@ -2929,7 +2987,20 @@ struct SharedGen {
 
 }  // namespace
 
-std::string generate_cuda(const Plan& plan, const Tuning& tuning) { return generate_cuda_impl(plan, tuning); }
+std::string generate_cuda(const Plan& plan, const Tuning& tuning) {
+  // Payload tables are an optimisation: when they leave the scan without the
+  // shared memory its other parts need, smaller table budgets are tried down
+  // to none before the launch shape is refused.
+  Tuning t = tuning;
+  for (;;) {
+    try {
+      return generate_cuda_impl(plan, t);
+    } catch (const PlanError& e) {
+      if (t.table_budget <= 0 || std::string(e.what()).find("shared memory exceeds") == std::string::npos) throw;
+      t.table_budget = t.table_budget >= 16384 ? t.table_budget / 2 : 0;
+    }
+  }
+}
 
 void collect_literals(const Plan& p, std::vector<const Expr*>& out) {
   for (const auto& s : p.steps) {

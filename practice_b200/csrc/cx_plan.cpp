@@ -257,6 +257,13 @@ std::unique_ptr<Plan> parse_plan(const std::string& text) {
           j.payload = to_name(pl->items[1], "payload");
         }
       }
+      if (const Node* pr = field(n, "prange")) {
+        if (pr->items.size() != 3) throw PlanError("(prange MIN CARD) for " + j.dim);
+        j.prange_min = to_int(pr->items[1], "prange");
+        j.prange_card = to_int(pr->items[2], "prange");
+        if (j.prange_card < 0 || j.prange_min < -2147483648LL || j.prange_min > 2147483647LL)
+          throw PlanError("prange out of range for " + j.dim);
+      }
       if (j.len <= 0 || j.len > (1LL << 30)) throw PlanError("join len out of range for " + j.dim);
       if (j.fks.size() > 4) throw PlanError("an OR-join takes at most 4 fact keys: " + j.dim);
       if (j.gathers.size() > 8) throw PlanError("an MHT join publishes at most 8 columns: " + j.dim);

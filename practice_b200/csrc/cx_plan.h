@@ -72,6 +72,10 @@ struct Join {
   long long keymin = 0;            // HASH offset
   std::unique_ptr<Expr> filter;    // build-side predicate, may be null
   std::string payload;             // PHT_2 payload column; empty => PHT_1 (or MHT)
+  // Catalog range of the payload's values (min, distinct count; card 0 =
+  // unknown): a small range lets the scan keep membership and payload of
+  // every slot in one byte of shared memory.
+  long long prange_min = 0, prange_card = 0;
   // Multi-value hash table (non-unique build key, visitor.cpp:3947-3968): the
   // directory maps a key to the build row ids that carry it and every match
   // expands the probe row; `gathers` are the build columns read by row id.

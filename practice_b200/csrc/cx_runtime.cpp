@@ -455,6 +455,7 @@ cx::Tuning to_tuning(const cx_tuning* tuning) {
     t.wait_limit_us = tuning->wait_limit_us;
     t.debug_stall = tuning->debug_stall;
     t.compact = tuning->compact;
+    t.table_budget = tuning->table_budget;
   }
   return t;
 }
@@ -506,6 +507,7 @@ void cx_tuning_default(cx_tuning* t) {
   t->wait_limit_us = d.wait_limit_us;
   t->debug_stall = d.debug_stall;
   t->compact = d.compact;
+  t->table_budget = d.table_budget;
 }
 
 int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap, size_t* out_len) {

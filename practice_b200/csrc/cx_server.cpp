@@ -180,9 +180,9 @@ int rebuild_universe(cx_server* s) {
 std::string tuning_key(const cx_tuning* t) {
   if (!t) return "default";
   char buf[256];
-  snprintf(buf, sizeof buf, "%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d", t->block_threads, t->items_per_thread, t->stages,
-           t->ctas_per_sm, t->group_placement, t->smem_group_budget, t->bitmap_budget, t->group_merge, t->prefetch,
-           t->wait_limit_us, t->debug_stall, t->compact);
+  snprintf(buf, sizeof buf, "%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d", t->block_threads, t->items_per_thread,
+           t->stages, t->ctas_per_sm, t->group_placement, t->smem_group_budget, t->bitmap_budget, t->group_merge,
+           t->prefetch, t->wait_limit_us, t->debug_stall, t->compact, t->table_budget);
   return buf;
 }
 

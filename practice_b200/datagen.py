@@ -197,6 +197,13 @@ FACT_COLS = ["lo_orderdate", "lo_custkey", "lo_suppkey", "lo_partkey", "lo_quant
 
 def ssb_tables(fact_rows: int, fact_cols: list[str] | None = None) -> dict[str, Table]:
     """Catalog entries (Table) of the synthetic SSB schema."""
+    tables = _ssb_tables(fact_rows, fact_cols)
+    for t in tables.values():
+        t.stats = {c: GROUP_STATS[c] for c in t.cols if c in GROUP_STATS}
+    return tables
+
+
+def _ssb_tables(fact_rows: int, fact_cols: list[str] | None) -> dict[str, Table]:
     return {
         "LINEORDER": Table("LINEORDER", list(fact_cols or FACT_COLS), fact_rows, fact=True),
         "DDATE": Table("DDATE", ["d_datekey", "d_year", "d_month", "d_weeknum"], DATE_DAYS, key_col="d_datekey",

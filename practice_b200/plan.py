@@ -124,6 +124,8 @@ class Table:
     key_min: int = 0
     key_max: int = 0
     key_unique: bool = True     # catalog: the key column holds each value at most once
+    # catalog statistics of attribute columns: column -> (min, distinct values)
+    stats: dict = field(default_factory=dict)
 
 
 @dataclass
@@ -138,6 +140,7 @@ class Join:
     more_fks: tuple[str, ...] = ()   # further fact keys of an OR-join
     multi: bool = False              # multi-value hash table (non-unique build key)
     gathers: tuple[str, ...] = ()    # MHT: build columns read through the row id
+    prange: tuple[int, int] | None = None  # catalog (min, cardinality) of the payload's values
 
     @property
     def fks(self) -> tuple[str, ...]:
@@ -197,6 +200,8 @@ class Plan:
                     parts.append(f" (payload {' '.join(j.gathers)})")
                 elif j.payload:
                     parts.append(f" (payload {j.payload})")
+                    if j.prange:
+                        parts.append(f" (prange {j.prange[0]} {j.prange[1]})")
                 out.append("  " + "".join(parts) + ")")
         agg = ["  (aggregate"]
         for g in self.groups:
@@ -373,7 +378,9 @@ class PlanBuilder:
             else:
                 if payload is None:
                     payload = choose_payload(d, pk, agg_cols, later_filter_cols)
-                steps[idx] = ("join", Join(dim, pk, fks[0], length, keymin, where, payload, fks[1:]))
+                prange = d.stats.get(payload) if payload else None
+                steps[idx] = ("join", Join(dim, pk, fks[0], length, keymin, where, payload, fks[1:],
+                                           prange=tuple(prange) if prange else None))
             used_tables.append(d)
         plan = Plan(tables=used_tables, nullable=set(self.nullable), steps=steps, groups=gl, aggs=al,
                     order_by=list(order_by or []), name=self.name)

@@ -50,7 +50,8 @@ def test_generated_source_compiles_for_sm100a(name):
     assert m.info.result_words == plan.group_slots * plan.storage_ts
     assert m.info.sparse == int(plan.sparse)
     if plan.steps and any(k == "join" for k, _ in plan.steps):
-        assert any(k in src for k in ("BlockProbeAndPHT", "BlockProbeExactBitmap", "ProbeMultiHT", "pht_slot"))
+        assert any(k in src for k in ("BlockProbeAndPHT", "BlockProbeExactBitmap", "BlockProbeExactTable", "ProbeMultiHT",
+                                     "pht_slot"))
         assert "build_hashtable_" in src or "mht_count_" in src
     if any(k == "join" and s.multi for k, s in plan.steps):
         for kern in ("mht_count_", "mht_blocksum_", "mht_blockscan_", "mht_offsets_", "mht_write_"):
@@ -301,3 +302,26 @@ def test_compacted_scans_compile(name, ipt):
     t.stages, t.block_threads = 2, 256
     assert "q_base" not in _lib.codegen(plan.text(), t)
     assert "q_base" not in _lib.codegen(all_plans()["ssb_q11"].text(), _lib.default_tuning())
+
+
+def test_payload_tables_follow_the_catalog_range_and_budget():
+    """Joins whose payload has a small catalog range (the plan's prange) keep
+    one byte per hash slot in shared memory; a zero budget or an unknown range
+    falls back to membership bitmaps and payload loads from the hash table."""
+    plan = queries.ssb_q31()
+    text = plan.text()
+    assert "(prange 1992 7)" in text and "(prange 0 25)" in text
+    src = _lib.codegen(text)
+    assert src.count("BlockProbeExactTable") == 2      # date (61,131 slots) and supplier (20,000) fit 96 KiB
+    assert "BlockProbeExactBitmap" in src             # customer (300,000 slots) keeps its bitmap
+    _lib.Module(src, key="ptable_q31")
+    t = _lib.default_tuning()
+    t.table_budget = 0
+    assert "BlockProbeExactTable" not in _lib.codegen(text, t)
+    no_range = text.replace("(prange 1992 7)", "").replace("(prange 0 25)", "")
+    assert "BlockProbeExactTable" not in _lib.codegen(no_range)
+    t = _lib.default_tuning()
+    t.compact = 1
+    src = _lib.codegen(text, t)
+    assert "BlockFetchPayloadTable" in src and "q_base" in src
+    _lib.Module(src, key="ptable_q31_compact")

@@ -431,3 +431,31 @@ def test_shared_scan_over_row_ranges_accumulates(db, splits):
     for p, (res, val, words) in zip(plans, bufs):
         ref = oracle_run(p, ht)
         np.testing.assert_array_equal(res.cpu().numpy().view(np.uint64)[:words], ref.words[:words], err_msg=p.name)
+
+
+@pytest.mark.parametrize("compact", [0, 1])
+def test_payload_tables_with_values_outside_the_catalog_range(db, compact):
+    """A payload range narrower than the data (here years 1994-1995 for a
+    1992-1998 column) marks the other slots 'fetch from the hash table': the
+    result still equals the oracle's; so do the default ranges and no tables."""
+    n = 1_000_003
+    ht = load(db, 43, n, queries.Q31_COLS)
+    plan = queries.ssb_q31(n)
+    ref = oracle_run(plan, ht)
+    variants = [(plan.text(), None), (plan.text().replace("(prange 1992 7)", "(prange 1994 2)"), None),
+                (plan.text(), 0)]
+    for text, budget in variants:
+        t = _lib.default_tuning()
+        t.compact = compact
+        if budget is not None:
+            t.table_budget = budget
+        m = _lib.Module(_lib.codegen(text, t), key=f"ptable_{compact}_{budget}_{hash(text)}")
+        res, val = db.alloc_result(m)
+        for tn, r in db.rows.items():
+            db.ctx.set_rows(tn, r)
+        db.ctx.set_result(res.data_ptr(), res.numel(), val.data_ptr(), val.numel())
+        db.ctx.execute(m, db.torch.cuda.current_stream().cuda_stream)
+        db.ctx.sync()
+        fw = int(m.info.final_words)
+        np.testing.assert_array_equal(res.cpu().numpy().view(np.uint64)[:fw], ref.words[:fw])
+        np.testing.assert_array_equal(val.cpu().numpy().view(np.uint64)[: (fw + 63) // 64], ref.validity[: (fw + 63) // 64])

@@ -304,6 +304,33 @@ struct Emitter {
   // and the per-4096-slot block sums of the offset scan.
   static long long mht_blocks(const Join& j) { return (j.len + 4095) / 4096; }
   static long long mht_words(const Join& j) { return 6 * j.len + mht_blocks(j) + 1; }
+  // The MHT payload holds, per entry, the build row id and a copy of every
+  // build column the probe publishes (and its validity where nullable), each
+  // in its own array of build-table length: a probe reads the values directly
+  // instead of first loading the row id and then gathering by it.
+  int mht_arrays(const Join& j) const {
+    int n = 1;
+    for (const auto& g : j.gathers) n += nullable(g) ? 2 : 1;
+    return n;
+  }
+  // Array index of gathered column g (and of its validity, + 1).
+  int mht_array_of(const Join& j, const std::string& g) const {
+    int n = 1;
+    for (const auto& c : j.gathers) {
+      if (c == g) return n;
+      n += nullable(c) ? 2 : 1;
+    }
+    throw PlanError("column " + g + " is not gathered by the join on " + j.dim);
+  }
+  // Loads of the published columns of MHT entry `pos` (an expression).
+  void emit_mht_gathers(std::ostream& o, const Join& j, const std::string& pos, const std::string& ind) {
+    const std::string d = lower(j.dim);
+    for (const auto& g : j.gathers) {
+      const int k = mht_array_of(j, g);
+      o << ind << g << "[i] = mpay_" << d << "[" << k << "LL * mst_" << d << " + " << pos << "];\n";
+      if (nullable(g)) o << ind << g << "_valid[i] = mpay_" << d << "[" << k + 1 << "LL * mst_" << d << " + " << pos << "];\n";
+    }
+  }
 
   // Build-side prologue shared by the PHT and MHT build kernels: the tile loop
   // over the dimension, its filter and the key's validity.
@@ -440,13 +467,33 @@ struct Emitter {
       o << param_decl();
       views(o);
       o << "  int* mht_payload = a.mpay[" << h << "];\n";
-      build_prologue(o, j, cols, t);
+      o << "  const long long mst_ = a.rows[" << t << "]; (void)mst_;\n";
+      std::vector<std::string> wcols = cols;
+      for (const auto& g : j.gathers)
+        if (std::find(wcols.begin(), wcols.end(), g) == wcols.end()) wcols.push_back(g);
+      build_prologue(o, j, wcols, t);
+      for (const auto& g : j.gathers) ensure_loaded(o, g, "    ");
       o << "    int row_ids[ITEMS_PER_THREAD];\n";
       o << "    BlockMakeRowIds<BLOCK_THREADS, ITEMS_PER_THREAD>(tid, (int)tile_offset, row_ids, num_tile_items);\n";
       key_loop(o, "{ if (((volatile int*)ht_dir)[3LL * s_] != " + j.pk + "[i]) cx::raise(a.err, cx::ERR_DIM_COLLISION); }");
-      o << "    BlockBuildMHT_Write<int, int, BLOCK_THREADS, ITEMS_PER_THREAD>(tid, " << j.pk
-        << ", row_ids, flags, ht_dir, mht_offsets, mht_wpos, mht_counts, mht_payload, " << L << ", " << j.keymin
-        << ", num_tile_items);\n";
+      // BlockBuildMHT_Write (include/crystal/join.h) places each row id at
+      // its slot's next position; the published columns go to the same
+      // position of their own arrays.
+      o << "    #pragma unroll\n    for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
+      o << "      if (!flags[i] || tid + BLOCK_THREADS * i >= num_tile_items) continue;\n";
+      o << "      const int s_ = cx_detail::pht_slot<int>(" << j.pk << "[i], " << L << ", " << j.keymin << ");\n";
+      o << "      if (s_ < 0) continue;\n";
+      o << "      const long long pos_ = (long long)mht_offsets[s_] + atomicAdd(&mht_wpos[s_], 1);\n";
+      o << "      mht_payload[pos_] = row_ids[i];\n";
+      for (const auto& g : j.gathers) {
+        const int k = mht_array_of(j, g);
+        o << "      mht_payload[" << k << "LL * mst_ + pos_] = " << g << "[i];\n";
+        if (nullable(g)) o << "      mht_payload[" << k + 1 << "LL * mst_ + pos_] = " << g << "_valid[i];\n";
+      }
+      o << "      ht_dir[3LL * s_ + 0] = " << j.pk << "[i];\n";
+      o << "      ht_dir[3LL * s_ + 1] = mht_offsets[s_];\n";
+      o << "      ht_dir[3LL * s_ + 2] = mht_counts[s_];\n";
+      o << "    }\n";
       o << "  }\n}\n\n";
     }
   }
@@ -813,7 +860,10 @@ struct Emitter {
       if (s.kind != Step::JoinStep) continue;
       const int h = ht_slot.at(s.join.dim);
       o << "  const int* " << ht_name(s.join.dim) << " = a.ht[" << h << "];\n";
-      if (s.join.multi) o << "  const int* mpay_" << lower(s.join.dim) << " = a.mpay[" << h << "];\n";
+      if (s.join.multi) {
+        o << "  const int* mpay_" << lower(s.join.dim) << " = a.mpay[" << h << "];\n";
+        o << "  const long long mst_" << lower(s.join.dim) << " = a.rows[" << p.table_slot(s.join.dim) << "];\n";
+      }
       if (!s.join.payload.empty() && payload_valid.count(s.join.payload))
         o << "  const unsigned int* " << ht_name(s.join.dim) << "_valid = a.htv[" << h << "];\n";
     }
@@ -1199,13 +1249,8 @@ struct Emitter {
           o << i2 << "ProbeMultiHT<int>(" << fk << "[i], " << off << ", " << cnt << ", " << fl << ", " << ht << ", " << j.len
             << ", " << j.keymin << ");\n";
           o << i2 << "for (int " << jj << " = 0; " << jj << " < " << cnt << "; ++" << jj << ") {\n";
-          o << i2 << "  const long long " << rid << " = mpay_" << lower(j.dim) << "[" << off << " + " << jj << "];\n";
-          for (const auto& g : j.gathers) {
-            o << i2 << "  " << g << "[i] = d_" << g << "[" << rid << "];\n";
-            if (nullable(g))
-              o << i2 << "  " << g << "_valid[i] = n_" << g << " ? (int)((n_" << g << "[" << rid << " >> 6] >> (" << rid
-                << " & 63)) & 1ULL) : 1;\n";
-          }
+          (void)rid;
+          emit_mht_gathers(o, j, "(long long)" + off + " + " + jj, i2 + "  ");
           item_steps(k + 1, i2 + "  ");
           o << i2 << "}\n";
         } else {
@@ -1402,12 +1447,7 @@ struct Emitter {
           o << i2 << "  for (int j_ = 0; __any_sync(0xffffffffu, j_ < cnt_); ++j_) {\n";
           o << i2 << "    bool act_ = j_ < cnt_;\n";
           o << i2 << "    if (act_) {\n";
-          o << i2 << "      const long long rid_ = mpay_" << lower(j.dim) << "[off_ + j_];\n";
-          for (const auto& g : j.gathers) {
-            o << i2 << "      " << g << "[i] = d_" << g << "[rid_];\n";
-            if (nullable(g))
-              o << i2 << "      " << g << "_valid[i] = n_" << g << " ? (int)((n_" << g << "[rid_ >> 6] >> (rid_ & 63)) & 1ULL) : 1;\n";
-          }
+          emit_mht_gathers(o, j, "(long long)off_ + j_", i2 + "      ");
           o << i2 << "    }\n";
           uniform_tail(i2 + "    ");
           o << i2 << "  }\n";
@@ -1743,7 +1783,7 @@ struct Emitter {
       ht_slot[s.join.dim] = h;
       if (s.join.multi) {
         meta << "ht " << h << " " << ht_name(s.join.dim) << " " << mht_words(s.join) << "\n";
-        meta << "mht " << h << " " << p.table_slot(s.join.dim) << "\n";
+        meta << "mht " << h << " " << p.table_slot(s.join.dim) << " " << mht_arrays(s.join) << "\n";
         ++h;
         continue;
       }

@@ -117,6 +117,7 @@ struct LaunchPlan {
   std::map<int, uint64_t> htv_words;
   std::map<int, uint64_t> bm_words;
   std::map<int, int> mht_table;                        // multi-value hash table slot -> build table slot
+  std::map<int, int> mht_arrays;                       // payload arrays (row ids + published columns) per slot
   uint64_t result_words = 0, groups = 1;
   int storage_ts = 1, visible_ts = 1, sparse = 0;
   uint64_t touched_words = 0;
@@ -204,9 +205,12 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       if (i != (int)lp.sshapes.size()) { err = "shape lines out of order"; return false; }
       lp.sshapes.push_back(sh);
     } else if (k == "mht") {
-      int sl = 0, t = 0;
+      int sl = 0, t = 0, na = 1;
       ls >> sl >> t;
+      if (!(ls >> na)) { na = 1; ls.clear(); }
+      if (na < 1 || na > 32) { err = "bad payload array count on an mht line"; return false; }
       lp.mht_table[sl] = t;
+      lp.mht_arrays[sl] = na;
     } else if (k == "bm") {
       int s; uint64_t w;
       ls >> s >> w;
@@ -298,9 +302,17 @@ ScratchLayout scratch_layout(const LaunchPlan& lp, const std::vector<long long>*
 
 // Bytes of the row-id payloads of a plan's multi-value hash tables: one int
 // per build row, so they are sized when the row counts are known.
+// Bytes of one multi-value hash table's payload: its arrays (row ids, then
+// the published columns and their validity) of one int per build row each.
+uint64_t mht_slot_bytes(const LaunchPlan& lp, int slot, long long build_rows) {
+  auto it = lp.mht_arrays.find(slot);
+  const uint64_t arrays = it == lp.mht_arrays.end() ? 1 : (uint64_t)it->second;
+  return align256((uint64_t)std::max<long long>(1, build_rows) * 4 * arrays);
+}
+
 uint64_t mht_payload_bytes(const LaunchPlan& lp, const std::vector<long long>& rows) {
   uint64_t b = 0;
-  for (const auto& kv : lp.mht_table) b += align256((uint64_t)std::max<long long>(1, rows[kv.second]) * 4);
+  for (const auto& kv : lp.mht_table) b += mht_slot_bytes(lp, kv.first, rows[kv.second]);
   return b;
 }
 
@@ -806,7 +818,7 @@ int cx_execute_params(cx_module* m, cx_exec_ctx* c, const int32_t* params, int n
     uint64_t off = sl.total;
     for (const auto& kv : lp.mht_table) {
       a.mpay[kv.first] = (int*)(scratch + off);
-      off += align256((uint64_t)std::max<long long>(1, rows[kv.second]) * 4);
+      off += mht_slot_bytes(lp, kv.first, rows[kv.second]);
     }
   }
 

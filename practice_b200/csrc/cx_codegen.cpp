@@ -16,6 +16,8 @@
 // Horner perfect hash of generatePerfectHash (:2056-2127).
 #include "cx_codegen.h"
 
+#include "cx_args.h"
+
 #include <algorithm>
 #include <cctype>
 #include <functional>
@@ -2256,7 +2258,7 @@ struct SharedGen {
     const unsigned long long par_off = off; off += (unsigned long long)MAXP * 4;
     off = (off + 15) & ~15ULL;
     const unsigned long long acc_off = off; off += (unsigned long long)MAXQ * NACC * 8;
-    const unsigned long long sq_off = off; off += (unsigned long long)MAXQ * 40;
+    const unsigned long long sq_off = off; off += ((unsigned long long)MAXQ * sizeof(CxSQ) + 15) & ~15ULL;
     const unsigned long long fm_off = off; off += (unsigned long long)NFC * FW * 8;
     const unsigned long long nj_off = off; off += (unsigned long long)(dims.size() + 4) * 8;
     off = (off + 15) & ~15ULL;

@@ -306,8 +306,9 @@ void launch(Slot& sl, std::vector<Request*>& batch, bool shared, cx_module* mod,
     if (sl.pin) cudaFreeHost(sl.pin);
     sl.pin = nullptr;
     sl.pin_words = 0;
-    if (cudaMallocHost((void**)&sl.pin, need * 2 * 8) != cudaSuccess) rc = CX_E_CUDA;
-    else sl.pin_words = need * 2;
+    const size_t grow = need + need / 4;  // some headroom, not a doubling: large results are gigabytes
+    if (cudaMallocHost((void**)&sl.pin, grow * 8) != cudaSuccess) rc = CX_E_CUDA;
+    else sl.pin_words = grow;
   }
   for (Request* r : batch) {
     if (rc) break;

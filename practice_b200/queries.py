@@ -13,9 +13,10 @@
 * ``template(t, rng)`` -- the four shared-scan templates: T0 range filters +
   scalar SUM; T1 date join + GROUP BY year; T2 three joins + GROUP BY
   (nation, year); T3 four joins + GROUP BY (brand, year) (<= 7,000 groups).
-* ``wide_groups`` / ``serving_stream`` -- the serving workload: the templates
-  with fresh constants per request plus a large-domain query (8.25M group
-  slots, a 330 MB result, <= 90,000 groups present).
+* ``serving_stream`` / ``city_pairs`` / ``wide_groups`` -- the serving workload:
+  the templates with fresh constants per request plus a many-group query
+  (up to 62,500 groups); and a large-domain query (8.25M group slots, a
+  330 MB result, <= 90,000 groups present) for admission under the budget.
 * ``kat_*`` -- the five queries of test/nullable_data/queries.sql.
 * ``or_join_year`` -- the OR-join over two fact keys of
   test/queries/sql/custom1.sql: (lo_orderdate = d_datekey OR lo_commitdate =
@@ -215,13 +216,28 @@ def wide_groups(rng: random.Random, fact_rows: int = 600_000_000) -> Plan:
     return b.aggregate([_g("c_city"), _g("s_city"), _g("lo_discount"), _g("d_month")], [("sum", col("lo_revenue"))])
 
 
-def serving_stream(n: int, seed: int, fact_rows: int = 600_000_000, wide_share: float = 0.05) -> list[Plan]:
+def city_pairs(rng: random.Random, fact_rows: int = 600_000_000) -> Plan:
+    """A many-group query of the serving stream: customer regions up to r,
+    a supplier region, a year range; GROUP BY (c_city, s_city), SUM(revenue):
+    up to 62,500 groups (a 1.5 MB result)."""
+    tables = ssb_tables(fact_rows, BATCH_COLS)
+    r = rng.randint(0, 4)
+    s = rng.randint(0, 4)
+    y_lo = rng.randint(1992, 1998)
+    y_hi = rng.randint(y_lo, 1998)
+    b = PlanBuilder(tables, "LINEORDER", name="T5")
+    b.join("CUSTOMER", "lo_custkey", where=col("c_region").le(r))
+    b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(s))
+    b.join("DDATE", "lo_orderdate", where=and_(col("d_year").ge(y_lo), col("d_year").le(y_hi)))
+    return b.aggregate([_g("c_city"), _g("s_city")], [("sum", col("lo_revenue"))])
+
+
+def serving_stream(n: int, seed: int, fact_rows: int = 600_000_000, many_share: float = 0.05) -> list[Plan]:
     """Requests of the serving workload: the four batch templates with fresh
-    random constants each, and with probability `wide_share` a large-domain
-    query (`wide_groups`); group cardinalities from 1 to 90,000, result
-    buffers from 8 bytes to 330 MB."""
+    random constants each, and with probability `many_share` a many-group
+    query (`city_pairs`); group cardinalities from 1 to 62,500."""
     rng = random.Random(seed)
-    return [wide_groups(rng, fact_rows) if rng.random() < wide_share else template(rng.randrange(4), rng, fact_rows)
+    return [city_pairs(rng, fact_rows) if rng.random() < many_share else template(rng.randrange(4), rng, fact_rows)
             for _ in range(n)]
 
 

@@ -56,7 +56,7 @@ def test_plain_scan_wait_runs_out_and_context_recovers(loaded, stages):
 
 def test_kernel_error_is_reported_through_the_c_abi(loaded):
     db, _, n = loaded
-    plan = queries.ssb_q11(n)
+    plan = queries.template(0, __import__("random").Random(4), n)
     m = db.compile(plan, make_tuning(wait_limit_us=LIMIT_US, debug_stall=1))
     res, val = db.alloc_result(m)
     for t, r in db.rows.items():

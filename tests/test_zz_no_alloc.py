@@ -46,9 +46,10 @@ class _Pool:
 
     def __init__(self):
         import torch
-        from cuda.bindings import runtime as rt
+        from cuda.bindings import driver, runtime as rt
 
         self.rt = rt
+        self.u64 = driver.cuuint64_t
         err, self.pool = rt.cudaDeviceGetDefaultMemPool(torch.cuda.current_device())
         assert err == rt.cudaError_t.cudaSuccess
 
@@ -60,7 +61,7 @@ class _Pool:
     def reset(self):
         A = self.rt.cudaMemPoolAttr
         for a in (A.cudaMemPoolAttrUsedMemHigh, A.cudaMemPoolAttrReservedMemHigh):
-            (err,) = self.rt.cudaMemPoolSetAttribute(self.pool, a, self.rt.cuuint64_t(0))
+            (err,) = self.rt.cudaMemPoolSetAttribute(self.pool, a, self.u64(0))
             assert err == self.rt.cudaError_t.cudaSuccess
 
     def highs(self):

@@ -143,7 +143,7 @@ std::unique_ptr<AggregateNode> build(const std::string& q) {
     Expr pred = and_(and_(and_(eq("c_region", r), eq("s_region", r)), ge("d_year", y0)), le("d_year", y1));
     if (nul)
       pred = and_(and_(and_(std::move(pred), or_(ge("lo_revenue", 2000000), is_null("lo_revenue"))),
-                       bin(ExprType::OP_NOT, gt("lo_revenue", 9500000), nullptr)),
+                       or_(bin(ExprType::OP_NOT, gt("lo_revenue", 9500000), nullptr), is_null("lo_revenue"))),
                   or_(not_null("c_city"), not_null("lo_revenue")));
     auto a = aggregate(filtered(std::move(pred),
                                 join("lo_orderdate", "d_datekey",

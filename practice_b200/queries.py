@@ -68,10 +68,12 @@ def ssb_q31_nullable(fact_rows: int = 60_000_000, region: int = 1, years: tuple[
     t = ssb_tables(fact_rows, Q31_COLS)
     nullable = {"lo_revenue", "c_city"}
     b = PlanBuilder(t, "LINEORDER", nullable=nullable, name="ssb_q31_nullable")
-    # (revenue >= floor OR revenue IS NULL) AND NOT (revenue > 9,500,000): UNKNOWN
-    # for NULL revenue on the range terms, rescued by IS NULL on the OR.
+    # (revenue >= floor OR revenue IS NULL) AND (NOT (revenue > 9,500,000) OR
+    # revenue IS NULL): the range terms are UNKNOWN for a NULL revenue (NOT
+    # keeps it UNKNOWN), IS NULL on each OR lets such rows through, so
+    # COUNT(revenue) and SUM(revenue) see them and skip them.
     b.filter(and_(or_(col("lo_revenue").ge(rev_floor), col("lo_revenue").is_null()),
-                  not_(col("lo_revenue").gt(9_500_000))))
+                  or_(not_(col("lo_revenue").gt(9_500_000)), col("lo_revenue").is_null())))
     b.join("CUSTOMER", "lo_custkey", where=col("c_region").eq(region), payload="c_city")
     b.join("SUPPLIER", "lo_suppkey", where=col("s_region").eq(region))
     b.join("DDATE", "lo_orderdate", where=and_(col("d_year").ge(years[0]), col("d_year").le(years[1])))

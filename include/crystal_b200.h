@@ -76,10 +76,11 @@ typedef struct cx_tuning {
                             1 = each warp queues the rows that pass the join bitmaps and fact
                             filters (ballot / popc into shared memory) and runs payload fetches,
                             remaining probes and the group update on 32 queued rows at a time */
-  int table_budget;      /* bytes of shared memory for payload tables (default 96 KiB): a join whose
-                            payload's catalog range has at most 254 values keeps one byte per hash
-                            slot -- membership and payload together -- instead of a membership
-                            bitmap and a payload load from the hash table (0 = none) */
+  int table_budget;      /* bytes of shared memory for payload tables (default 0 = none; the
+                            autotuner tries 96 KiB): a join whose payload's catalog range has at
+                            most 254 values keeps one byte per hash slot -- membership and payload
+                            together -- instead of a membership bitmap and a payload load from the
+                            hash table */
 } cx_tuning;
 
 /* Shape of a compiled query's result buffer. */

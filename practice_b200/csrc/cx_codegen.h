@@ -31,7 +31,8 @@ struct Tuning {
   int debug_stall = 0;         // test hook: 1 = every CTA first waits on a barrier nothing completes
   int compact = 0;             // plain grouped scans: 1 = queue qualifying rows per warp after the
                                // membership tests and run the rest on 32 queued rows at a time
-  int table_budget = 96 * 1024;  // bytes of shared memory for payload tables (one byte per slot)
+  int table_budget = 0;        // bytes of shared memory for payload tables (one byte per slot); opt-in:
+                               // measured no faster than bitmaps once rows are warp-compacted
 };
 
 // Returns the CUDA source for `plan` with its launch plan embedded as a

@@ -587,6 +587,10 @@ int cx_server_create(const cx_exec_ctx* tables, const cx_server_config* cfg, cx_
   for (Slot& sl : s->slots) {
     sl.ctx = cx_ctx_create();
     cx_internal::ctx_copy_tables(tables, sl.ctx);
+    // Batches here change from launch to launch (queries, shapes, row
+    // ranges), so a captured graph would be re-captured every time: launch
+    // the kernels directly.
+    cx_ctx_set_graph_replay(sl.ctx, 0);
     if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess)
       return serr(CX_E_CUDA, "cx_server_create: stream or event creation failed");

@@ -311,7 +311,10 @@ def test_payload_tables_follow_the_catalog_range_and_budget():
     plan = queries.ssb_q31()
     text = plan.text()
     assert "(prange 1992 7)" in text and "(prange 0 25)" in text
-    src = _lib.codegen(text)
+    assert "BlockProbeExactTable" not in _lib.codegen(text)  # opt-in
+    on = _lib.default_tuning()
+    on.table_budget = 96 * 1024
+    src = _lib.codegen(text, on)
     assert src.count("BlockProbeExactTable") == 2      # date (61,131 slots) and supplier (20,000) fit 96 KiB
     assert "BlockProbeExactBitmap" in src             # customer (300,000 slots) keeps its bitmap
     _lib.Module(src, key="ptable_q31")
@@ -319,9 +322,9 @@ def test_payload_tables_follow_the_catalog_range_and_budget():
     t.table_budget = 0
     assert "BlockProbeExactTable" not in _lib.codegen(text, t)
     no_range = text.replace("(prange 1992 7)", "").replace("(prange 0 25)", "")
-    assert "BlockProbeExactTable" not in _lib.codegen(no_range)
+    assert "BlockProbeExactTable" not in _lib.codegen(no_range, on)
     t = _lib.default_tuning()
-    t.compact = 1
+    t.compact, t.table_budget = 1, 96 * 1024
     src = _lib.codegen(text, t)
     assert "BlockFetchPayloadTable" in src and "q_base" in src
     _lib.Module(src, key="ptable_q31_compact")

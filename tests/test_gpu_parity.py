@@ -442,13 +442,11 @@ def test_payload_tables_with_values_outside_the_catalog_range(db, compact):
     ht = load(db, 43, n, queries.Q31_COLS)
     plan = queries.ssb_q31(n)
     ref = oracle_run(plan, ht)
-    variants = [(plan.text(), None), (plan.text().replace("(prange 1992 7)", "(prange 1994 2)"), None),
+    variants = [(plan.text(), 96 * 1024), (plan.text().replace("(prange 1992 7)", "(prange 1994 2)"), 96 * 1024),
                 (plan.text(), 0)]
     for text, budget in variants:
         t = _lib.default_tuning()
-        t.compact = compact
-        if budget is not None:
-            t.table_budget = budget
+        t.compact, t.table_budget = compact, budget
         m = _lib.Module(_lib.codegen(text, t), key=f"ptable_{compact}_{budget}_{hash(text)}")
         res, val = db.alloc_result(m)
         for tn, r in db.rows.items():

@@ -2249,10 +2249,14 @@ struct SharedGen {
     while (STAGES > 2 && (unsigned long long)STAGES * ((unsigned long long)(NSC + nattr) * TR * 4 + (MAXQ + gm_words) * (TR / 32) * 4) > 160 * 1024) --STAGES;
     unsigned long long off = 0;
     const int NB = TR / 32;  // 32-row blocks per tile
+    // Row stride of a query's (or a group's) block words: one word of padding,
+    // so the 32 lanes of a mask warp, each storing the word of its own query
+    // for the same block, hit 32 different banks.
+    const int NBS = NB + 1;
     // Per stage: the fact columns, the payload attributes and the per-query row bitmaps of one tile.
     const unsigned long long stage_off = off; off += (unsigned long long)STAGES * NSC * TR * 4;
     const unsigned long long attr_off = off; off += (unsigned long long)STAGES * nattr * TR * 4;
-    const unsigned long long gm_off = off; off += (unsigned long long)STAGES * gm_words * NB * 4;
+    const unsigned long long gm_off = off; off += (unsigned long long)STAGES * gm_words * NBS * 4;
     const unsigned long long bars_off = off; off += (unsigned long long)STAGES * 3 * 8 + 16;
     off = (off + 15) & ~15ULL;
     const unsigned long long par_off = off; off += (unsigned long long)MAXP * 4;
@@ -2266,9 +2270,9 @@ struct SharedGen {
     // the group tables follow the fixed part; the host sizes both per pass.
     const unsigned long long qb_off = (off + 15) & ~15ULL;
     const unsigned long long smem_total = qb_off;
-    if (smem_total + (unsigned long long)MAXQ * STAGES * NB * 4 > 200 * 1024)
+    if (smem_total + (unsigned long long)MAXQ * STAGES * NBS * 4 > 200 * 1024)
       throw PlanError("shared scan shared memory exceeds 200 KB before group tables");
-    meta << "sqb " << STAGES * NB * 4 << "\n";
+    meta << "sqb " << STAGES * NBS * 4 << "\n";
     const unsigned wait_limit = (unsigned)std::min(60000000, std::max(1, tu.wait_limit_us));
     const std::string kname = "SharedScan_" + fact;
     meta << "kernel " << kname << " sharedscan 0 " << CTA << " " << TR << " " << smem_total << " " << tu.ctas_per_sm << "\n";
@@ -2296,7 +2300,7 @@ struct SharedGen {
     o << "  CxSQ* s_sq = (CxSQ*)(cx_smem + " << sq_off << ");\n";
     o << "  unsigned long long* s_fm = (unsigned long long*)(cx_smem + " << fm_off << "); (void)s_fm;\n";
     o << "  unsigned long long* s_nj = (unsigned long long*)(cx_smem + " << nj_off << ");\n";
-    o << "  unsigned long long* s_tab = (unsigned long long*)(cx_smem + " << qb_off << " + ((NSTAGE * nq_ * " << NB * 4 << " + 15) & ~15)); (void)s_tab;\n";
+    o << "  unsigned long long* s_tab = (unsigned long long*)(cx_smem + " << qb_off << " + ((NSTAGE * nq_ * " << NBS * 4 << " + 15) & ~15)); (void)s_tab;\n";
     o << "  unsigned int* s_bits = (unsigned int*)(s_tab + a.smem_tab_words); (void)s_bits;\n";
     o << "  const int nq = a.sq_total < " << MAXQ << " ? a.sq_total : " << MAXQ << ";\n";
     o << "  const long long n_rows = a.rows[0];\n";
@@ -2438,8 +2442,8 @@ struct SharedGen {
       for (const Dim& d : dims)
         for (const auto& at : d.attrs)
           o << ind << "int* S_" << at << " = s_attr + (s * " << nattr << " + " << attr_slot[at] << ") * TR;\n";
-      o << ind << "unsigned* s_qb_t = s_qb + s * nq * " << NB << ";\n";
-      o << ind << "unsigned* s_gm_t = s_gm + s * " << gm_words * NB << "; (void)s_gm_t;\n";
+      o << ind << "unsigned* s_qb_t = s_qb + s * nq * " << NBS << ";\n";
+      o << ind << "unsigned* s_gm_t = s_gm + s * " << gm_words * NBS << "; (void)s_gm_t;\n";
     };
     // Staging warp: refills a stage once the aggregation warps released it.
     o << "  if (warp == 0) {\n";
@@ -2592,20 +2596,20 @@ struct SharedGen {
       // block's words are cleared, then the lowest lane of each group writes
       // its group's word (the same lane writes the out-of-domain word).
       const std::string gm_at = "s_gm_t[(" + std::to_string(gm_base[si]) + " + ";
-      o << "          if (lane <= " << G << ") " << gm_at << "lane) * " << NB << " + blk_] = 0u;\n";
+      o << "          if (lane <= " << G << ") " << gm_at << "lane) * " << NBS << " + blk_] = 0u;\n";
       o << "          __syncwarp();\n";
       o << "          const unsigned peers_ = __match_any_sync(0xffffffffu, h_);\n";
-      o << "          if (h_ < " << G << " && lane == __ffs(peers_) - 1) " << gm_at << "h_) * " << NB << " + blk_] = peers_;\n";
+      o << "          if (h_ < " << G << " && lane == __ffs(peers_) - 1) " << gm_at << "h_) * " << NBS << " + blk_] = peers_;\n";
       o << "          const unsigned bb_ = __ballot_sync(0xffffffffu, bad_);\n";
-      o << "          if (lane == " << G << ") " << gm_at << G << ") * " << NB << " + blk_] = bb_;\n";
+      o << "          if (lane == " << G << ") " << gm_at << G << ") * " << NBS << " + blk_] = bb_;\n";
       o << "        }\n";
     }
     // Transpose the warp's 32 row masks into one word per query.
     o << "        const unsigned wl_ = cx::warp_transpose32((unsigned)m, lane);\n";
-    o << "        if (lane < nq) s_qb_t[lane * " << NB << " + blk_] = wl_;\n";
+    o << "        if (lane < nq) s_qb_t[lane * " << NBS << " + blk_] = wl_;\n";
     o << "        if (nq > 32) {\n";
     o << "          const unsigned wh_ = cx::warp_transpose32((unsigned)(m >> 32), lane);\n";
-    o << "          if (lane + 32 < nq) s_qb_t[(lane + 32) * " << NB << " + blk_] = wh_;\n";
+    o << "          if (lane + 32 < nq) s_qb_t[(lane + 32) * " << NBS << " + blk_] = wh_;\n";
     o << "        }\n";
     o << "      }\n";
     o << "    }\n";
@@ -2632,7 +2636,7 @@ struct SharedGen {
     o << "      const unsigned bm_ = (bw_ == 32 ? 0xffffffffu : ((1u << bw_) - 1u)) << (sub_ * bw_);\n";
     o << "      const CxSQ& Q = s_sq[q_];\n";
     o << "      const int* P = s_params + Q.param_off; (void)P;\n";
-    o << "      const unsigned* qw_ = s_qb_t + q_ * " << NB << ";\n";
+    o << "      const unsigned* qw_ = s_qb_t + q_ * " << NBS << ";\n";
     o << "      switch (Q.shape) {\n";
     for (size_t s = 0; s < shapes.size(); ++s) {
       const Plan& p = *shapes[s];
@@ -2734,14 +2738,14 @@ struct SharedGen {
           o << ind << "unsigned long long tacc[" << G * NA << "];\n";
           o << ind << "#pragma unroll\n" << ind << "for (int r = 0; r < " << G * NA << "; ++r) tacc[r] = 0ULL;\n";
           o << ind << "unsigned ttouch = 0u;\n";
-          o << ind << "const unsigned* gm_ = s_gm_t + " << gm_base[s] << " * " << NB << ";\n";
+          o << ind << "const unsigned* gm_ = s_gm_t + " << gm_base[s] << " * " << NBS << ";\n";
           o << ind << "for (int b_ = blo_ + lane / lpb_; b_ < bhi_; b_ += 32 / lpb_) {\n";
           o << ind << "  const unsigned w_ = qw_[b_] & bm_;\n";
           o << ind << "  if (!w_) continue;\n";
-          o << ind << "  if (w_ & gm_[" << G << " * " << NB << " + b_]) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
+          o << ind << "  if (w_ & gm_[" << G << " * " << NBS << " + b_]) cx::raise(a.err, cx::ERR_GROUP_DOMAIN);\n";
           o << ind << "  #pragma unroll\n";
           o << ind << "  for (int g = 0; g < " << G << "; ++g) {\n";
-          o << ind << "    unsigned wg_ = w_ & gm_[g * " << NB << " + b_];\n";
+          o << ind << "    unsigned wg_ = w_ & gm_[g * " << NBS << " + b_];\n";
           o << ind << "    if (!wg_) continue;\n";
           o << ind << "    ttouch |= 1u << g;\n";
           bool any_sum = false;

@@ -230,10 +230,10 @@ def config_block(args):
 # ------------------------------------------------------------------ GPU arm
 
 # DRAM bytes (read + write) per fact row of one shared-scan launch over the
-# 8-column batch table: ncu (dram__bytes_read.sum + dram__bytes_write.sum) of
-# one 30M-row launch of the 32-query batch, 972.2 MB; the traffic of a launch
-# grows with its rows.
-SHARED_DRAM_BYTES_PER_ROW = (968.458240e6 + 3.693568e6) / 30e6
+# 8-column batch table, by path: ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) of one 30M-row launch of the 32-query batch (per-query
+# masks: 972.2 MB); the traffic of a launch grows with its rows.
+SHARED_DRAM_BYTES_PER_ROW = {"masks": (968.679936e6 + 3.349248e6) / 30e6, "cube": None}
 
 PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=bm,
                          prefetch=pf, group_placement=pl, compact=cp, table_budget=tb)
@@ -243,10 +243,15 @@ PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas
                         (512, 8, 4, 0, 0, 0, 0, 0), (1024, 4, 0, 49152, 1, 0, 1, 98304),
                         (512, 4, 0, 49152, 1, 0, 1, 98304), (1024, 2, 0, 49152, 1, 0, 1, 98304),
                         (1024, 2, 0, 49152, 1, 0, 1, 0))]
+# Per-query mask path (cube = 0) launch shapes, then the aggregate-cube path at
+# 1, 2 and 4 rows per lane (the runtime falls back to the mask path when the
+# batch's attribute ranges do not allow cubes).
 SHARED_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=2, producer_warps=pw,
-                          group_merge=gm)
+                          group_merge=gm, cube=0)
                      for bt, ipt, st, pw, gm in ((1024, 1, 3, 11, 0), (1024, 1, 3, 11, 3), (1024, 1, 3, 14, 0),
                                                  (1024, 1, 3, 14, 3), (512, 2, 2, 5, 0), (512, 2, 2, 7, 3))]
+SHARED_CANDIDATES += [dict(block_threads=1024, items_per_thread=1, stages=3, ctas_per_sm=2, producer_warps=11,
+                           group_merge=3, cube=c) for c in (1, 2, 4)]
 
 
 def bound_ctx(db, module, res, val):
@@ -377,7 +382,7 @@ def shared_leg(torch, db, plans, stream, args, pg, device, sample_clocks: bool):
     scan.append(tm.scan_ms)
     results = [result_words(r, v, words) for r, v, words in sbufs]
     return {"ms_per_step": ms / args.steps, "scan_ms": tm.scan_ms, "launches_per_step": tm.gpu_launches,
-            "graph": tm.graph, "tuning": {k: getattr(tun, k) for k, _ in _lib.Tuning._fields_} if tun else None,
+            "graph": tm.graph, "path": "cube" if tm.mode == 1 else "masks", "tuning": {k: getattr(tun, k) for k, _ in _lib.Tuning._fields_} if tun else None,
             "prog": prog, "squeries": squeries, "sparams": sparams, "sbufs": sbufs, "clocks": clocks}, results
 
 
@@ -773,7 +778,9 @@ def main():
             value = job_rate(len(plans) * args.steps, world, shared["ms_per_step"] * args.steps)
             ms_step = shared["ms_per_step"]
             achieved = len(union_cols) * 4 * args.rows / (shared["scan_ms"] / 1000.0) / 1e9
-            kernel = "SharedScan_LINEORDER (one pass over the union of the batch's fact columns)"
+            kernel = ("CubeScan_LINEORDER (one pass over the union of the batch's fact columns, one aggregate-cube "
+                      "cell update per row and plan shape)" if shared["path"] == "cube" else
+                      "SharedScan_LINEORDER (one pass over the union of the batch's fact columns, per-query row masks)")
             launches = shared["launches_per_step"]
             alg = f"union of fact columns read by the batch ({len(union_cols)}) x 4 B x rows, per launch"
             lat = {"p50": ms_step, "p99": ms_step, "definition": "every query of a batch completes with its launch"}
@@ -794,7 +801,7 @@ def main():
                 s_qps = job_rate(b * args.steps, world, s["ms_per_step"] * args.steps)
                 row["shared"] = {"queries_per_s": s_qps, "ms_per_step": s["ms_per_step"], "scan_ms": s["scan_ms"],
                                  "roofline_frac": len(ucols) * 4 * args.rows / (s["scan_ms"] / 1000.0) / 1e9 / peak,
-                                 "graph": s["graph"], "tuning": s["tuning"]}
+                                 "graph": s["graph"], "path": s["path"], "tuning": s["tuning"]}
                 row["shared_vs_plain"] = s_qps / plain_by_batch[b]["queries_per_s"]
             batches[str(b)] = row
         line = {
@@ -805,7 +812,8 @@ def main():
             "latency_ms": lat,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": (SHARED_DRAM_BYTES_PER_ROW * args.rows / 1e9) if shared is not None else None,
+                         "traffic": (SHARED_DRAM_BYTES_PER_ROW[shared["path"]] * args.rows / 1e9
+                                     if shared is not None and SHARED_DRAM_BYTES_PER_ROW.get(shared["path"]) else None),
                          "traffic_unit": "GB per launch (ncu capture of 30M rows scaled by rows)",
                          "kernel": kernel, "algorithmic_bytes": alg},
             "clocks": clocks, "e2e": e2e,

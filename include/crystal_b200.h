@@ -81,6 +81,14 @@ typedef struct cx_tuning {
                             most 254 values keeps one byte per hash slot -- membership and payload
                             together -- instead of a membership bitmap and a payload load from the
                             hash table */
+  int cube;              /* shared scans: 0 = answer every query from per-query row masks; 1, 2 or
+                            4 (default 4) = the program also carries the aggregate-cube path, which
+                            cx_shared_execute takes when every column the batch's predicates and
+                            GROUP BY keys read has a registered range (cx_ctx_set_column_range) of
+                            at most 65,536 values and each shape's cube has at most 16,777,216
+                            cells: one pass adds every fact row into one cell per plan shape, then
+                            each query sums the cells its predicates accept (the value is the
+                            cube scan's rows per lane) */
 } cx_tuning;
 
 /* Shape of a compiled query's result buffer. */
@@ -104,6 +112,7 @@ typedef struct cx_timing {
   int scan_grid;   /* CTAs of the scan launch */
   int gpu_launches;/* kernels launched by the last execute */
   int graph;       /* shared scans: 0 launched directly, 1 replayed a cached graph, 2 captured a new one */
+  int mode;        /* shared scans: 0 per-query row masks, 1 aggregate cubes */
 } cx_timing;
 
 int cx_abi_version(void);
@@ -171,8 +180,12 @@ int cx_ctx_set_sm_count(cx_exec_ctx* c, int sms);
 /* Registers the value range [lo, hi] of column `name` ("d_<column>").  Shared
  * scans turn single-column filters on a ranged column into lookup tables over
  * the first 256 values of the range; filters on unranged columns (or values
- * past the window) are evaluated row by row per query.  No reference
- * counterpart: the reference plans one query at a time. */
+ * past the window) are evaluated row by row per query.  The aggregate-cube
+ * path (cx_tuning.cube) indexes cells by the values of ranged columns, so it
+ * takes the range as a bound: a value outside it raises kernel error 5 (the
+ * batch's results are then not valid; re-register the range, or run the batch
+ * with cube = 0, whose lookup tables only use the range as a window).  No
+ * reference counterpart: the reference plans one query at a time. */
 int cx_ctx_set_column_range(cx_exec_ctx* c, const char* name, int64_t lo, int64_t hi);
 /* Shared-scan batches are captured once into a CUDA graph and replayed while
  * the batch keeps the same pass shapes (queries per pass, parameters, shared

@@ -62,7 +62,8 @@ def main(argv: list[str] | None = None) -> None:
         t = make_tuning(**{**shared_default, **kw})
         for _ in range(args.reps):
             r = db.execute_shared(plans, t)
-            print(f"shared batch of {len(plans)}: scan {r[0].timing.scan_ms:.4f} ms, "
+            path = "aggregate cubes" if r[0].timing.mode == 1 else "per-query masks"
+            print(f"shared batch of {len(plans)} ({path}): scan {r[0].timing.scan_ms:.4f} ms, "
                   f"total {r[0].timing.total_ms:.4f} ms, kernel error {r[0].kernel_error}", flush=True)
         return
     q = args.query

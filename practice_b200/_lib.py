@@ -42,7 +42,7 @@ class Tuning(C.Structure):
                 ("ctas_per_sm", C.c_int), ("group_placement", C.c_int), ("smem_group_budget", C.c_int),
                 ("bitmap_budget", C.c_int), ("group_merge", C.c_int), ("producer_warps", C.c_int),
                 ("parametric", C.c_int), ("prefetch", C.c_int), ("wait_limit_us", C.c_int),
-                ("debug_stall", C.c_int), ("compact", C.c_int), ("table_budget", C.c_int)]
+                ("debug_stall", C.c_int), ("compact", C.c_int), ("table_budget", C.c_int), ("cube", C.c_int)]
 
 
 class ResultInfo(C.Structure):
@@ -85,7 +85,8 @@ class ServerStats(C.Structure):
 
 class Timing(C.Structure):
     _fields_ = [("build_ms", C.c_float), ("scan_ms", C.c_float), ("post_ms", C.c_float),
-                ("total_ms", C.c_float), ("scan_grid", C.c_int), ("gpu_launches", C.c_int), ("graph", C.c_int)]
+                ("total_ms", C.c_float), ("scan_grid", C.c_int), ("gpu_launches", C.c_int), ("graph", C.c_int),
+                ("mode", C.c_int)]
 
 
 def _load() -> C.CDLL:

@@ -793,6 +793,7 @@ enum : unsigned int {
   ERR_SCRATCH = 3,           // scratch too small for the requested table
   ERR_DIM_COLLISION = 4,     // two distinct dimension keys share a slot of a shared-scan
                              // index or of a multi-value hash table
+  ERR_CUBE_RANGE = 5,        // a value outside the registered range of a cube attribute
 };
 
 CX_DEVICE void raise(unsigned int* err, unsigned int code) {

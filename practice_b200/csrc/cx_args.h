@@ -14,6 +14,8 @@
 #define CX_MAX_SHAPES 16
 #define CX_MAX_FCOLS 8
 #define CX_MAX_LITS 64
+#define CX_MAX_CATTRS 32
+#define CX_MAX_SATTRS 8
 
 // One query of a shared-scan batch: its own result buffers, its plan shape and
 // the offset of its literal parameters.
@@ -54,4 +56,16 @@ struct CxArgs {
   int fwin[CX_MAX_FCOLS];                      // values in the window (0: evaluate every row per query)
   int lits[CX_MAX_LITS];                       // literal parameters of a parametric plain kernel
   int* mpay[CX_MAX_HTS];                       // multi-value hash tables: build row ids grouped by slot
+  // Aggregate cubes of a shared-scan batch: per attribute the registered range
+  // minimum and the number of values; per shape the cell stride of each of its
+  // attributes, its cube in global memory (sums per SUM aggregate, then row
+  // counts) and the u64 offset of its per-CTA copy in shared memory (-1: none).
+  int cube_lo[CX_MAX_CATTRS];
+  int cube_radix[CX_MAX_CATTRS];
+  int cube_stride[CX_MAX_SHAPES * CX_MAX_SATTRS];
+  unsigned long long* cube_g[CX_MAX_SHAPES];
+  long long cube_cells[CX_MAX_SHAPES];
+  int cube_smem[CX_MAX_SHAPES];
+  int cube_smem_words;                         // u64 words of all shared-memory cubes
+  int cube_chunks;                             // answer blocks per query
 };

@@ -2168,8 +2168,398 @@ struct SharedGen {
     src << "  }\n}\n\n";
   }
 
+  // ------------------------------------------------------ aggregate cubes --
+  // The queries of one shape differ only in their literals.  When every column
+  // that a shape's predicates and GROUP BY keys read has a small value range,
+  // one pass adds each fact row's aggregate values into one cell per shape --
+  // the cell indexed by those columns' values, dimension columns taken from the
+  // row the join finds -- and each query is answered afterwards from the cells
+  // its own predicates accept (CUBE-style shared aggregation; integer sums in
+  // any order give the same words).  The per-row work then no longer grows with
+  // the number of queries.  Value ranges are registered on the execution
+  // context, so the program keeps the per-query mask kernels beside the cube
+  // kernels and the runtime picks one path per batch.
+  struct CAttr { int dim; int field; std::string col; };  // dim < 0: a fact column
+  std::vector<CAttr> cattrs;
+  std::map<std::string, int> cattr_id;
+  std::vector<std::vector<int>> sh_attrs;  // per shape: its attributes in cell order (last varies fastest)
+  std::vector<int> dim_fields;             // 16-bit attribute fields used per dimension entry
+  std::string cube_why;                    // why the batch has no cube path ("" = it has one)
+  static constexpr int MAX_CATTRS = 32, MAX_SATTRS = 8;
+
+  void collect_cube() {
+    dim_fields.assign(dims.size(), 0);
+    sh_attrs.assign(shapes.size(), {});
+    auto add = [&](const Plan& p, const std::string& c, std::vector<int>& mine) -> bool {
+      int id;
+      auto it = cattr_id.find(c);
+      if (it != cattr_id.end()) {
+        id = it->second;
+      } else {
+        CAttr at{-1, 0, c};
+        const int ts = p.table_of_col.at(c);
+        if (ts != 0) {
+          const int di = dim_index(p.tables[ts].name);
+          if (di < 0) { cube_why = "column " + c + " is not of a joined dimension"; return false; }
+          if (dim_fields[di] >= 4) { cube_why = "more than four cube attributes of " + dims[di].name; return false; }
+          at.dim = di;
+          at.field = dim_fields[di]++;
+        }
+        if ((int)cattrs.size() >= MAX_CATTRS) { cube_why = "more than 32 cube attributes"; return false; }
+        id = (int)cattrs.size();
+        cattrs.push_back(at);
+        cattr_id[c] = id;
+      }
+      if (std::find(mine.begin(), mine.end(), id) == mine.end()) mine.push_back(id);
+      return true;
+    };
+    for (size_t si = 0; si < shapes.size(); ++si) {
+      const Plan& p = *shapes[si];
+      for (const auto& ag : p.aggs) {
+        std::vector<const Expr*> ls;
+        lits_of(ag.arg.get(), ls);
+        if (!ls.empty()) { cube_why = "an aggregate reads a literal"; return; }
+        std::vector<std::string> cs;
+        cols_of(ag.arg.get(), cs);
+        for (const auto& c : cs)
+          if (p.table_of_col.at(c) != 0) { cube_why = "an aggregate reads dimension column " + c; return; }
+      }
+      std::vector<std::string> cs;
+      for (const auto& st : p.steps) cols_of(st.kind == Step::Filter ? st.filter.get() : st.join.filter.get(), cs);
+      for (const auto& g : p.groups) cols_of(g.expr.get(), cs);
+      for (const auto& c : cs)
+        if (!add(p, c, sh_attrs[si])) return;
+      if ((int)sh_attrs[si].size() > MAX_SATTRS) { cube_why = "a shape reads more than 8 cube attributes"; return; }
+    }
+  }
+
+  int sum_aggs(const Plan& p) const {
+    int n = 0;
+    for (const auto& ag : p.aggs) n += ag.fn == AggFn::Sum;
+    return n;
+  }
+
+  // Per batch: each dimension row's entry at its slot -- key, the shapes one of
+  // whose queries its join filter passes (shapes that do not join the
+  // dimension always set), and its cube attributes as 16-bit offsets from the
+  // registered range minimum.
+  void emit_cube_index(const Dim& d, int di) {
+    const std::string k = "cube_index_" + lower(d.name);
+    meta << "kernel " << k << " cubeidx " << d.table << " 256 1024\n";
+    std::ostringstream& o = src;
+    o << "extern \"C\" __global__ void __launch_bounds__(256) " << k << "(const CxArgs a) {\n";
+    o << "  const long long n = a.rows[" << d.table << "];\n";
+    o << "  int4* ent = (int4*)a.ht[" << d.slot << "];\n";
+    o << "  const int* __restrict__ key = a.col[" << slot_of(d.pk, d.table) << "];\n";
+    std::set<std::string> decl;
+    auto declare = [&](const std::string& c) {
+      if (decl.insert(c).second) o << "  const int* __restrict__ F_" << c << " = a.col[" << slot_of(c, d.table) << "];\n";
+    };
+    for (const auto& c : d.fcols) declare(c);
+    for (const auto& at : cattrs)
+      if (at.dim == di) declare(at.col);
+    unsigned nj = 0;
+    for (size_t s = 0; s < shapes.size(); ++s)
+      if (!preds[s].joins.count(di)) nj |= 1u << s;
+    o << "  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {\n";
+    o << "    const int k = key[r];\n";
+    o << "    if (k == 0) continue;\n";
+    o << "    const int h = (int)HASH(k, " << d.len << ", " << d.keymin << ");\n";
+    o << "    if ((unsigned)h >= " << d.len << "u) continue;\n";
+    o << "    unsigned f_[4] = {0u, 0u, 0u, 0u};\n";
+    o << "    bool bad_ = false;\n";
+    for (size_t id = 0; id < cattrs.size(); ++id) {
+      if (cattrs[id].dim != di) continue;
+      o << "    { const unsigned x_ = (unsigned)(F_" << cattrs[id].col << "[r] - a.cube_lo[" << id << "]);\n";
+      o << "      if (x_ >= (unsigned)a.cube_radix[" << id << "]) bad_ = true; else f_[" << cattrs[id].field << "] = x_; }\n";
+    }
+    o << "    if (bad_) { cx::raise(a.err, cx::ERR_CUBE_RANGE); continue; }\n";
+    o << "    unsigned rel = " << nj << "u;\n";
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      auto it = preds[s].joins.find(di);
+      if (it == preds[s].joins.end()) continue;
+      Emitter e(*shapes[s], tu);
+      e.lit_index = &lit_maps[s];
+      for (const auto& c : d.fcols) e.col_expr[c] = "F_" + c + "[r]";
+      const std::string f = conj_and(e, it->second);
+      if (f == "true") {
+        o << "    if (a.sq_num[" << s << "] > 0) rel |= " << (1u << s) << "u;\n";
+        continue;
+      }
+      o << "    for (int q = a.sq_first[" << s << "]; q < a.sq_first[" << s << "] + a.sq_num[" << s << "]; ++q) {\n";
+      o << "      const int* P = a.sparams + a.sq[q].param_off; (void)P;\n";
+      o << "      if (" << f << ") { rel |= " << (1u << s) << "u; break; }\n";
+      o << "    }\n";
+    }
+    o << "    if (atomicCAS(&ent[h].x, 0, k) != 0) { cx::raise(a.err, cx::ERR_DIM_COLLISION); continue; }\n";
+    o << "    ent[h] = make_int4(k, (int)rel, (int)(f_[0] | (f_[1] << 16)), (int)(f_[2] | (f_[3] << 16)));\n";
+    o << "  }\n}\n\n";
+  }
+
+  // One pass over the fact rows: warp tiles of 32 x IPT rows read with vector
+  // loads; per row the shapes it may belong to (fact filter tables and the
+  // dimension entries, a superset of what any query of the shape accepts),
+  // then per such shape one cell update -- shared-memory cubes per CTA, merged
+  // into the global cube at the end, or global atomics for large cubes.
+  void emit_cube_scan() {
+    const int CTA = 256, IPT = std::max(1, std::min(4, tu.cube)), VW = IPT >= 4 ? 4 : IPT;
+    if (IPT == 3) throw PlanError("cube scans take 1, 2 or 4 rows per lane");
+    const int NFC = (int)fcols.size();
+    const unsigned long long fr_bytes = ((unsigned long long)NFC * FW * 4 + 15) & ~15ULL;
+    const std::string kname = "CubeScan_" + fact;
+    meta << "kernel " << kname << " cubescan 0 " << CTA << " " << 32 * IPT << " " << fr_bytes << " 8\n";
+    std::ostringstream& o = src;
+    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", 2) " << kname << "(const CxArgs a) {\n";
+    o << "  constexpr int IPT = " << IPT << ", VW = " << VW << ", TROWS = " << 32 * IPT << ";\n";
+    o << "  extern __shared__ __align__(16) unsigned char cx_smem[];\n";
+    o << "  unsigned* s_fr = (unsigned*)cx_smem; (void)s_fr;\n";
+    o << "  unsigned long long* s_cube = (unsigned long long*)(cx_smem + " << fr_bytes << ");\n";
+    o << "  const int lane = threadIdx.x & 31;\n";
+    o << "  for (int w = threadIdx.x; w < a.cube_smem_words; w += " << CTA << ") s_cube[w] = 0ULL;\n";
+    o << "  unsigned live = 0u;\n";
+    for (size_t s = 0; s < shapes.size(); ++s) o << "  if (a.sq_num[" << s << "] > 0) live |= " << (1u << s) << "u;\n";
+    // Filter tables: bit s of s_fr[k * FW + v] clears when no query of shape s
+    // accepts the value fbase[k] + v on filter column k.
+    if (NFC) {
+      o << "  for (int v = threadIdx.x; v < " << NFC * FW << "; v += " << CTA << ") {\n";
+      o << "    const int k_ = v / " << FW << ";\n";
+      o << "    const int fv_ = (int)((unsigned)a.fbase[k_] + (unsigned)(v - k_ * " << FW << "));\n";
+      o << "    unsigned m = ~0u;\n";
+      for (size_t s = 0; s < shapes.size(); ++s) {
+        Emitter e(*shapes[s], tu);
+        e.lit_index = &lit_maps[s];
+        for (const auto& kv : preds[s].pushed) {
+          e.col_expr.clear();
+          e.col_expr[fcols[kv.first]] = "fv_";
+          o << "    if (k_ == " << kv.first << " && a.sq_num[" << s << "] > 0) {\n";
+          o << "      bool any_ = false;\n";
+          o << "      for (int q = a.sq_first[" << s << "]; q < a.sq_first[" << s << "] + a.sq_num[" << s << "] && !any_; ++q) {\n";
+          o << "        const int* P = a.sparams + a.sq[q].param_off; (void)P;\n";
+          o << "        any_ = " << conj_and(e, kv.second) << ";\n";
+          o << "      }\n";
+          o << "      if (!any_) m &= ~" << (1u << s) << "u;\n";
+          o << "    }\n";
+        }
+      }
+      o << "    s_fr[v] = m;\n";
+      o << "  }\n";
+    }
+    o << "  __syncthreads();\n";
+    for (const auto& c : fact_cols) o << "  const int* __restrict__ d_" << c << " = a.col[" << slot_of(c, 0) << "];\n";
+    for (const Dim& d : dims) o << "  const int4* __restrict__ ci_" << lower(d.name) << " = (const int4*)a.ht[" << d.slot << "];\n";
+    for (int k = 0; k < NFC; ++k) o << "  const unsigned fb" << k << " = (unsigned)a.fbase[" << k << "], fw" << k << " = (unsigned)a.fwin[" << k << "];\n";
+    o << "  bool vec_ok = true;\n";
+    for (const auto& c : fact_cols) o << "  vec_ok = vec_ok && ((((unsigned long long)d_" << c << ") & 15ULL) == 0ULL);\n";
+    o << "  const long long n = a.rows[0];\n";
+    o << "  const long long ntiles = (n + TROWS - 1) / TROWS;\n";
+    o << "  const long long nw = ((long long)gridDim.x * " << CTA << ") >> 5;\n";
+    o << "  for (long long t = ((long long)blockIdx.x * " << CTA << " + threadIdx.x) >> 5; t < ntiles; t += nw) {\n";
+    o << "    const long long base = t * TROWS;\n";
+    o << "    const int nt = (int)(n - base < TROWS ? n - base : TROWS);\n";
+    for (const auto& c : fact_cols) o << "    int c_" << c << "[IPT];\n";
+    o << "    if (nt == TROWS && vec_ok) {\n";
+    for (const auto& c : fact_cols) o << "      WarpLoadTileV<IPT>(d_" << c << " + base, lane, c_" << c << ");\n";
+    o << "    } else {\n";
+    o << "      #pragma unroll\n";
+    o << "      for (int i = 0; i < IPT; ++i) {\n";
+    o << "        const int r = (i / VW) * 32 * VW + lane * VW + (i % VW);\n";
+    for (const auto& c : fact_cols) o << "        c_" << c << "[i] = r < nt ? d_" << c << "[base + r] : 0;\n";
+    o << "      }\n";
+    o << "    }\n";
+    // Shapes each row may belong to after the fact filter tables.
+    o << "    unsigned rel_[IPT];\n";
+    o << "    #pragma unroll\n";
+    o << "    for (int i = 0; i < IPT; ++i) {\n";
+    o << "      const int r = (i / VW) * 32 * VW + lane * VW + (i % VW);\n";
+    o << "      unsigned m = r < nt ? live : 0u;\n";
+    for (int k = 0; k < NFC; ++k)
+      o << "      { const unsigned d_ = (unsigned)c_" << fcols[k] << "[i] - fb" << k << "; if (d_ < fw" << k << ") m &= s_fr[" << k * FW << " + d_]; }\n";
+    o << "      rel_[i] = m;\n";
+    o << "    }\n";
+    // Every dimension entry of every row in flight together.
+    std::vector<unsigned> joiners(dims.size(), 0u);
+    for (size_t s = 0; s < shapes.size(); ++s)
+      for (const auto& kv : preds[s].joins) joiners[kv.first] |= 1u << s;
+    for (size_t di = 0; di < dims.size(); ++di) o << "    int4 e" << di << "_[IPT];\n";
+    o << "    #pragma unroll\n";
+    o << "    for (int i = 0; i < IPT; ++i) {\n";
+    for (size_t di = 0; di < dims.size(); ++di) {
+      const Dim& d = dims[di];
+      o << "      e" << di << "_[i] = make_int4(0, 0, 0, 0);\n";
+      o << "      if (rel_[i] & " << joiners[di] << "u) {\n";
+      o << "        const int h_ = cx_detail::pht_slot<int>(c_" << d.fk << "[i], " << d.len << ", " << d.keymin << ");\n";
+      o << "        if (h_ >= 0) e" << di << "_[i] = __ldg(&ci_" << lower(d.name) << "[h_]);\n";
+      o << "      }\n";
+    }
+    o << "    }\n";
+    o << "    #pragma unroll\n";
+    o << "    for (int i = 0; i < IPT; ++i) {\n";
+    o << "      unsigned m = rel_[i];\n";
+    for (size_t di = 0; di < dims.size(); ++di) {
+      const Dim& d = dims[di];
+      o << "      { const int4 g_ = e" << di << "_[i];\n";
+      o << "        const bool hit_ = g_.x != 0 && g_.x == c_" << d.fk << "[i];\n";
+      o << "        m &= hit_ ? (unsigned)g_.y : " << (~joiners[di] & ((1u << shapes.size()) - 1u)) << "u; }\n";
+    }
+    o << "      if (m == 0u) continue;\n";
+    const char* fld[4] = {"((unsigned)g_.z & 0xFFFFu)", "((unsigned)g_.z >> 16)", "((unsigned)g_.w & 0xFFFFu)", "((unsigned)g_.w >> 16)"};
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      const Plan& p = *shapes[s];
+      Emitter e(p, tu);
+      for (const auto& c : fact_cols) e.col_expr[c] = "c_" + c + "[i]";
+      const int NS = sum_aggs(p);
+      o << "      if ((m >> " << s << ") & 1u) {\n";
+      o << "        unsigned cell_ = 0u;\n";
+      o << "        bool in_ = true;\n";
+      for (size_t j = 0; j < sh_attrs[s].size(); ++j) {
+        const int id = sh_attrs[s][j];
+        const CAttr& at = cattrs[id];
+        const std::string stride = "(unsigned)a.cube_stride[" + std::to_string(s * MAX_SATTRS + j) + "]";
+        if (at.dim < 0) {
+          o << "        { const unsigned x_ = (unsigned)(c_" << at.col << "[i] - a.cube_lo[" << id << "]);\n";
+          o << "          in_ = in_ && x_ < (unsigned)a.cube_radix[" << id << "];\n";
+          o << "          cell_ += x_ * " << stride << "; }\n";
+        } else {
+          o << "        { const int4 g_ = e" << at.dim << "_[i]; cell_ += " << fld[at.field] << " * " << stride << "; }\n";
+        }
+      }
+      o << "        if (!in_) {\n";
+      o << "          cx::raise(a.err, cx::ERR_CUBE_RANGE);\n";
+      o << "        } else {\n";
+      int ks = 0;
+      for (const auto& ag : p.aggs) {
+        if (ag.fn != AggFn::Sum) continue;
+        o << "          const unsigned long long x" << ks << "_ = (unsigned long long)(" << e.math_push(ag.arg.get(), true) << ");\n";
+        ++ks;
+      }
+      o << "          if (a.cube_smem[" << s << "] >= 0) {\n";
+      o << "            unsigned long long* cs_ = s_cube + a.cube_smem[" << s << "];\n";
+      o << "            const unsigned nc_ = (unsigned)a.cube_cells[" << s << "];\n";
+      for (int k = 0; k < NS; ++k) o << "            if (x" << k << "_) atomicAdd(&cs_[" << k << "u * nc_ + cell_], x" << k << "_);\n";
+      o << "            atomicAdd((unsigned*)(cs_ + " << NS << "u * nc_) + cell_, 1u);\n";
+      o << "          } else {\n";
+      o << "            unsigned long long* cg_ = a.cube_g[" << s << "];\n";
+      o << "            const unsigned long long nc_ = (unsigned long long)a.cube_cells[" << s << "];\n";
+      for (int k = 0; k < NS; ++k) o << "            if (x" << k << "_) atomicAdd(&cg_[" << k << "ULL * nc_ + cell_], x" << k << "_);\n";
+      o << "            atomicAdd(&cg_[" << NS << "ULL * nc_ + cell_], 1ULL);\n";
+      o << "          }\n";
+      o << "        }\n";
+      o << "      }\n";
+    }
+    o << "    }\n";
+    o << "  }\n";
+    // Shared-memory cubes into the global cubes.
+    o << "  __syncthreads();\n";
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      const int NS = sum_aggs(*shapes[s]);
+      o << "  if (a.cube_smem[" << s << "] >= 0 && a.sq_num[" << s << "] > 0) {\n";
+      o << "    const unsigned long long* cs_ = s_cube + a.cube_smem[" << s << "];\n";
+      o << "    const unsigned nc_ = (unsigned)a.cube_cells[" << s << "];\n";
+      o << "    unsigned long long* cg_ = a.cube_g[" << s << "];\n";
+      o << "    for (unsigned c = threadIdx.x; c < nc_; c += " << CTA << ") {\n";
+      o << "      const unsigned n_ = ((const unsigned*)(cs_ + " << NS << "u * nc_))[c];\n";
+      o << "      if (!n_) continue;\n";
+      o << "      atomicAdd(&cg_[" << NS << "ULL * nc_ + c], (unsigned long long)n_);\n";
+      for (int k = 0; k < NS; ++k)
+        o << "      { const unsigned long long v_ = cs_[" << k << "u * nc_ + c]; if (v_) atomicAdd(&cg_[" << k << "ULL * nc_ + c], v_); }\n";
+      o << "    }\n";
+      o << "  }\n";
+    }
+    o << "}\n\n";
+  }
+
+  // Per query: the cells of its shape's cube that its predicates accept, added
+  // into its result the way the per-query path adds rows (touched bits,
+  // validity), each block taking one chunk of the cells.
+  void emit_cube_answer() {
+    meta << "kernel cube_answer cubeans 0 256 0\n";
+    std::ostringstream& o = src;
+    o << "extern \"C\" __global__ void __launch_bounds__(256) cube_answer(const CxArgs a) {\n";
+    o << "  const int nch = a.cube_chunks > 0 ? a.cube_chunks : 1;\n";
+    o << "  const int q = blockIdx.x / nch, ch = blockIdx.x - q * nch;\n";
+    o << "  if (q >= a.sq_total) return;\n";
+    o << "  const CxSQ Q = a.sq[q];\n";
+    o << "  const int* P = a.sparams + Q.param_off; (void)P;\n";
+    o << "  unsigned long long* d_result = Q.result; (void)d_result;\n";
+    o << "  uint64_t* d_result_validity = (uint64_t*)Q.validity; (void)d_result_validity;\n";
+    o << "  unsigned int* g_touch = Q.touched; (void)g_touch;\n";
+    o << "  switch (Q.shape) {\n";
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      const Plan& p = *shapes[s];
+      Emitter e(p, tu);
+      e.lit_index = &lit_maps[s];
+      for (int id : sh_attrs[s]) e.col_expr[cattrs[id].col] = "v_" + cattrs[id].col;
+      const int NS = sum_aggs(p);
+      o << "    case " << s << ": {\n";
+      if (p.groups.empty()) {
+        for (size_t k = 0; k < p.aggs.size(); ++k)
+          if (p.aggs[k].fn == AggFn::Count)
+            o << "      if (ch == 0 && threadIdx.x == 0) db::atomic_set_valid_bit(d_result_validity, " << k << ");\n";
+      }
+      o << "      const unsigned long long* cg_ = a.cube_g[" << s << "];\n";
+      o << "      const long long nc_ = a.cube_cells[" << s << "];\n";
+      o << "      const long long per_ = (nc_ + nch - 1) / nch, c0_ = (long long)ch * per_;\n";
+      o << "      const long long c1_ = c0_ + per_ < nc_ ? c0_ + per_ : nc_;\n";
+      o << "      for (long long c = c0_ + threadIdx.x; c < c1_; c += blockDim.x) {\n";
+      o << "        const unsigned long long n_ = cg_[" << NS << "ULL * (unsigned long long)nc_ + c];\n";
+      o << "        if (!n_) continue;\n";
+      o << "        const unsigned cu_ = (unsigned)c;\n";
+      for (size_t j = 0; j < sh_attrs[s].size(); ++j) {
+        const int id = sh_attrs[s][j];
+        o << "        const int v_" << cattrs[id].col << " = (int)((cu_ / (unsigned)a.cube_stride[" << s * MAX_SATTRS + j
+          << "]) % (unsigned)a.cube_radix[" << id << "]) + a.cube_lo[" << id << "];\n";
+      }
+      std::vector<const Expr*> all;
+      for (const auto& st : p.steps) all.push_back(st.kind == Step::Filter ? st.filter.get() : st.join.filter.get());
+      o << "        if (!(" << conj_and(e, all) << ")) continue;\n";
+      if (p.groups.empty()) {
+        int ks = 0;
+        for (size_t k = 0; k < p.aggs.size(); ++k) {
+          if (p.aggs[k].fn == AggFn::Count) {
+            o << "        atomicAdd(&d_result[" << k << "], n_);\n";
+          } else {
+            o << "        { const unsigned long long v_ = cg_[" << ks << "ULL * (unsigned long long)nc_ + c]; if (v_) atomicAdd(&d_result[" << k << "], v_); }\n";
+            o << "        db::atomic_set_valid_bit(d_result_validity, " << k << ");\n";
+            ++ks;
+          }
+        }
+      } else {
+        const unsigned long long G = e.total_groups();
+        const int TS = p.storage_ts();
+        std::string horner, dom;
+        for (size_t k = 0; k < p.groups.size(); ++k) {
+          o << "        const int gt" << k << " = " << e.group_term(k) << ";\n";
+          horner = horner.empty() ? "gt0" : "(" + horner + " * " + std::to_string(e.eff_card(k)) + " + gt" + std::to_string(k) + ")";
+          dom += (dom.empty() ? "" : " && ") + std::string("(unsigned)gt") + std::to_string(k) + " < " + std::to_string(e.eff_card(k)) + "u";
+        }
+        o << "        int hash = " << horner << ";\n";
+        o << "        if (!(" << dom << ")) { cx::raise(a.err, cx::ERR_GROUP_DOMAIN); hash = hash % " << G << "; }\n";
+        o << "        if ((unsigned)hash >= " << G << "u) continue;\n";
+        o << "        atomicOr(&g_touch[hash >> 5], 1u << (hash & 31));\n";
+        int ks = 0;
+        for (size_t k = 0; k < p.aggs.size(); ++k) {
+          const std::string ix = "(unsigned long long)hash * " + std::to_string(TS) + "ULL + " + std::to_string(p.groups.size() + k);
+          if (p.aggs[k].fn == AggFn::Count) {
+            o << "        atomicAdd(&d_result[" << ix << "], n_);\n";
+          } else {
+            o << "        { const unsigned long long v_ = cg_[" << ks << "ULL * (unsigned long long)nc_ + c]; if (v_) atomicAdd(&d_result[" << ix << "], v_); }\n";
+            ++ks;
+          }
+          if (!p.sparse) o << "        db::atomic_set_valid_bit(d_result_validity, " << ix << ");\n";
+        }
+      }
+      o << "      }\n";
+      o << "      break; }\n";
+    }
+    o << "    default: break;\n";
+    o << "  }\n";
+    o << "}\n\n";
+  }
+
   std::string run() {
     collect();
+    if (tu.cube > 0) collect_cube();
+    else cube_why = "cube path switched off";
     meta << "v 1\nshared " << MAXQ << " " << MAXQ * std::max(1, max_lits) << "\n";
     for (const Dim& d : dims) {
       meta << "ht " << d.slot << " dkm_" << lower(d.name) << " " << d.len * 4 << "\n";
@@ -2188,9 +2578,25 @@ struct SharedGen {
            << " " << (p.sparse ? 1 : 0) << " " << lit_maps[s].size() << " " << (smem_ok ? 1 : 0) << " " << NA << " "
            << (G + 31) / 32 << " " << nseen << "\n";
     }
+    if (cube_why.empty()) {
+      meta << "cube " << cattrs.size() << "\n";
+      for (size_t id = 0; id < cattrs.size(); ++id)
+        meta << "cattr " << id << " " << cattrs[id].dim << " " << cattrs[id].field << " d_" << cattrs[id].col << "\n";
+      for (size_t s = 0; s < shapes.size(); ++s) {
+        meta << "cshape " << s << " " << sum_aggs(*shapes[s]) << " " << sh_attrs[s].size();
+        for (int id : sh_attrs[s]) meta << " " << id;
+        meta << "\n";
+      }
+    }
     emit_zero();
     for (size_t di = 0; di < dims.size(); ++di) emit_index(dims[di], (int)di);
+    if (cube_why.empty())
+      for (size_t di = 0; di < dims.size(); ++di) emit_cube_index(dims[di], (int)di);
     emit_scan();
+    if (cube_why.empty()) {
+      emit_cube_scan();
+      emit_cube_answer();
+    }
     emit_keys();
     for (size_t i = 0; i < tables.size(); ++i) meta << "table " << i << " " << tables[i] << "\n";
     for (size_t i = 0; i < col_order.size(); ++i)

@@ -26,7 +26,7 @@ uint64_t ctx_scratch_bytes(const cx_exec_ctx* c);
 
 // Scratch bytes cx_shared_execute needs for a batch of queries of `shapes`
 // (program shape indexes) on program `m`.
-uint64_t shared_scratch_need(const cx_module* m, const int* shapes, int nq);
+uint64_t shared_scratch_need(const cx_module* m, const cx_exec_ctx* c, const int* shapes, int nq);
 
 // Scratch bytes a context owns after an execute that needs `need` bytes, when
 // it owns `own` bytes before (own scratch grows to 1.5x the need).

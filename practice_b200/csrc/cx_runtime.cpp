@@ -134,6 +134,14 @@ struct LaunchPlan {
   std::vector<std::pair<int, std::string>> fcols;      // shared scans: fact filter table columns
   struct SShape { uint64_t groups; int ts, grouped, sparse, nlits, smem_ok, naggs; uint64_t tw; int nseen; };
   std::vector<SShape> sshapes;
+  // Shared scans with an aggregate-cube path: its attributes (dimension index
+  // and 16-bit field of the entry, or dim -1 for a fact column) and, per shape,
+  // its SUM aggregates and attributes in cell order.
+  bool cube = false;
+  struct CAttr { int dim = -1, field = 0; std::string col; };
+  std::vector<CAttr> cattrs;
+  struct CShape { int nsums = 0; std::vector<int> attrs; };
+  std::vector<CShape> cshapes;
 };
 
 bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err) {
@@ -204,6 +212,35 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       ls >> i >> sh.groups >> sh.ts >> sh.grouped >> sh.sparse >> sh.nlits >> sh.smem_ok >> sh.naggs >> sh.tw >> sh.nseen;
       if (i != (int)lp.sshapes.size()) { err = "shape lines out of order"; return false; }
       lp.sshapes.push_back(sh);
+    } else if (k == "cube") {
+      size_t n = 0;
+      ls >> n;
+      if (n > CX_MAX_CATTRS) { err = "too many cube attributes"; return false; }
+      lp.cube = true;
+    } else if (k == "cattr") {
+      int id = 0;
+      LaunchPlan::CAttr at;
+      ls >> id >> at.dim >> at.field >> at.col;
+      if (id != (int)lp.cattrs.size() || id >= CX_MAX_CATTRS || at.field < 0 || at.field > 3 || at.dim >= CX_MAX_HTS) {
+        err = "cube attribute lines out of order or out of range";
+        return false;
+      }
+      lp.cattrs.push_back(at);
+    } else if (k == "cshape") {
+      int i = 0, na = 0;
+      LaunchPlan::CShape cs;
+      ls >> i >> cs.nsums >> na;
+      if (i != (int)lp.cshapes.size() || na < 0 || na > CX_MAX_SATTRS || cs.nsums < 0 || cs.nsums > 64) {
+        err = "cube shape lines out of order or out of range";
+        return false;
+      }
+      for (int j = 0; j < na; ++j) {
+        int id = -1;
+        ls >> id;
+        if (id < 0 || id >= (int)lp.cattrs.size()) { err = "cube shape names an unknown attribute"; return false; }
+        cs.attrs.push_back(id);
+      }
+      lp.cshapes.push_back(cs);
     } else if (k == "mht") {
       int sl = 0, t = 0, na = 1;
       ls >> sl >> t;
@@ -225,8 +262,8 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
     } else if (k == "kernel") {
       KernelSpec ks;
       ls >> ks.name >> ks.kind >> ks.table >> ks.block;
-      if (ks.kind == "build" || ks.kind == "tiles" || ks.kind == "tilescan") ls >> ks.tile;
-      else if (ks.kind == "scan" || ks.kind == "sharedscan") ls >> ks.tile >> ks.smem >> ks.ctas_per_sm;
+      if (ks.kind == "build" || ks.kind == "cubeidx" || ks.kind == "tiles" || ks.kind == "tilescan") ls >> ks.tile;
+      else if (ks.kind == "scan" || ks.kind == "sharedscan" || ks.kind == "cubescan") ls >> ks.tile >> ks.smem >> ks.ctas_per_sm;
       else { size_t z; ls >> z; }
       lp.kernels.push_back(ks);
     } else {
@@ -245,7 +282,7 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
       return false;
     }
   for (const auto& k : lp.kernels)
-    if ((k.kind == "tiles" || k.kind == "tilescan" || k.kind == "build") &&
+    if ((k.kind == "tiles" || k.kind == "tilescan" || k.kind == "build" || k.kind == "cubeidx") &&
         (k.table < 0 || k.table >= (int)lp.tables.size() || k.tile <= 0 || k.block <= 0 || k.block > 1024)) {
       err = "kernel line " + k.name + " names a table outside the plan or a bad shape";
       return false;
@@ -385,7 +422,7 @@ int load_on_device(cx_module* m, int dev, cx_module::Loaded** out) {
     r = d.ModuleGetFunction(&f, L.mod, k.name.c_str());
     if (r != CUDA_SUCCESS) { d.ModuleUnload(L.mod); return drv_fail(r, k.name.c_str()); }
     int occ = 1;
-    if (k.kind == "scan" || k.kind == "sharedscan") {
+    if (k.kind == "scan" || k.kind == "sharedscan" || k.kind == "cubescan") {
       if (m->lp.shared) {
         r = d.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, 227 * 1024);
         if (r != CUDA_SUCCESS) { d.ModuleUnload(L.mod); return drv_fail(r, "cuFuncSetAttribute(smem)"); }
@@ -414,6 +451,79 @@ int ensure_ctx_device(cx_exec_ctx* c, int dev) {
   if (!c->host_err) CX_CUDA(cudaMallocHost((void**)&c->host_err, sizeof(unsigned int)));
   c->device = dev;
   return CX_OK;
+}
+
+// Layout of a batch's aggregate cubes: per attribute its registered range, per
+// shape with queries its cell count, mixed-radix strides (last attribute
+// varies fastest), global cube offset and, when it fits the per-CTA budget, its
+// shared-memory offset.  `why` says why the batch keeps the per-query path.
+struct CubePlan {
+  bool on = false;
+  std::string why;
+  std::vector<int> lo, radix;
+  std::vector<uint64_t> cells, goff;
+  std::vector<std::vector<int>> stride;
+  std::vector<int> smem_off;
+  uint64_t smem_words = 0, gbytes = 0;
+  int chunks = 1;
+};
+
+constexpr uint64_t kCubeMaxCells = 1ULL << 24;
+constexpr uint64_t kCubeMaxGlobalBytes = 8ULL << 30;
+constexpr uint64_t kCubeSmemBudget = 96 * 1024;
+constexpr uint64_t kCubeCellsPerChunk = 16384;
+
+bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, int nq, CubePlan& cp) {
+  const int nshapes = (int)lp.sshapes.size();
+  if (!lp.cube || (int)lp.cshapes.size() != nshapes) { cp.why = "program has no cube path"; return false; }
+  std::vector<char> used(nshapes, 0);
+  for (int q = 0; q < nq; ++q)
+    if (shapes[q] >= 0 && shapes[q] < nshapes) used[shapes[q]] = 1;
+  for (const auto& at : lp.cattrs) {
+    auto it = c->ranges.find(at.col);
+    if (it == c->ranges.end()) { cp.why = "no registered range for " + at.col; return false; }
+    const int64_t lo = it->second.first, hi = it->second.second;
+    if (lo < INT32_MIN || hi > INT32_MAX || hi - lo + 1 > 65536) { cp.why = "range of " + at.col + " exceeds 65,536 values"; return false; }
+    cp.lo.push_back((int)lo);
+    cp.radix.push_back((int)(hi - lo + 1));
+  }
+  cp.cells.assign(nshapes, 0);
+  cp.goff.assign(nshapes, 0);
+  cp.stride.assign(nshapes, std::vector<int>(CX_MAX_SATTRS, 0));
+  cp.smem_off.assign(nshapes, -1);
+  uint64_t g = 0, maxcells = 0;
+  for (int s = 0; s < nshapes; ++s) {
+    if (!used[s]) continue;
+    const auto& sh = lp.cshapes[s];
+    uint64_t cells = 1;
+    for (size_t j = sh.attrs.size(); j-- > 0;) {
+      cp.stride[s][j] = (int)cells;
+      cells *= (uint64_t)cp.radix[sh.attrs[j]];
+      if (cells > kCubeMaxCells) { cp.why = "a shape's cube exceeds 16,777,216 cells"; return false; }
+    }
+    cp.cells[s] = cells;
+    cp.goff[s] = g;
+    g = align256(g + cells * (uint64_t)(sh.nsums + 1) * 8);
+    maxcells = std::max(maxcells, cells);
+  }
+  if (g > kCubeMaxGlobalBytes) { cp.why = "the batch's cubes exceed 8 GiB"; return false; }
+  cp.gbytes = g;
+  // Shared-memory copies for the smallest cubes first, within the per-CTA budget.
+  std::vector<int> order;
+  for (int s = 0; s < nshapes; ++s)
+    if (used[s]) order.push_back(s);
+  std::sort(order.begin(), order.end(), [&](int x, int y) { return cp.cells[x] < cp.cells[y]; });
+  uint64_t words = 0;
+  for (int s : order) {
+    const uint64_t w = cp.cells[s] * (uint64_t)lp.cshapes[s].nsums + (cp.cells[s] + 1) / 2;
+    if ((words + w) * 8 > kCubeSmemBudget) continue;
+    cp.smem_off[s] = (int)words;
+    words += w;
+  }
+  cp.smem_words = words;
+  cp.chunks = (int)std::max<uint64_t>(1, std::min<uint64_t>(4096, (maxcells + kCubeCellsPerChunk - 1) / kCubeCellsPerChunk));
+  cp.on = true;
+  return true;
 }
 
 }  // namespace
@@ -468,14 +578,17 @@ cx::Tuning to_tuning(const cx_tuning* tuning) {
     t.debug_stall = tuning->debug_stall;
     t.compact = tuning->compact;
     t.table_budget = tuning->table_budget;
+    t.cube = tuning->cube;
   }
   return t;
 }
 
 uint64_t grown_scratch(uint64_t own, uint64_t need) { return own >= need ? own : need + need / 2; }
 
-uint64_t shared_scratch_need(const cx_module* m, const int* shapes, int nq) {
+uint64_t shared_scratch_need(const cx_module* m, const cx_exec_ctx* c, const int* shapes, int nq) {
   const LaunchPlan& lp = m->lp;
+  CubePlan cp;
+  const bool cube = c && plan_cubes(lp, c, shapes, nq, cp);
   uint64_t off = 0;
   for (const auto& h : lp.hts) {
     off = align256(off + h.words * 4);
@@ -487,9 +600,17 @@ uint64_t shared_scratch_need(const cx_module* m, const int* shapes, int nq) {
     const auto& sh = lp.sshapes[shapes[i]];
     if (sh.grouped) off = align256(off + ((sh.groups + 31) / 32) * 4);
   }
-  const int maxq = std::max(1, std::min(lp.shared_maxq, 256));
+  if (cube) off = align256(off + cp.gbytes);
+  const int maxq = cube ? std::max(nq, 1) : std::max(1, std::min(lp.shared_maxq, 256));
   const int npass = (nq + maxq - 1) / maxq;
-  const uint64_t pass_bytes = align256((uint64_t)maxq * sizeof(CxSQ) + (uint64_t)std::max(lp.shared_maxp, 1) * 4);
+  int maxp = lp.shared_maxp;
+  if (cube) {
+    int np = 0;
+    for (int i = 0; i < nq; ++i)
+      if (shapes[i] >= 0 && shapes[i] < (int)lp.sshapes.size()) np += lp.sshapes[shapes[i]].nlits;
+    maxp = std::max(maxp, np);
+  }
+  const uint64_t pass_bytes = align256((uint64_t)maxq * sizeof(CxSQ) + (uint64_t)std::max(maxp, 1) * 4);
   off += (uint64_t)std::max(npass, 1) * pass_bytes;
   return align256(off + 16);
 }
@@ -520,6 +641,7 @@ void cx_tuning_default(cx_tuning* t) {
   t->debug_stall = d.debug_stall;
   t->compact = d.compact;
   t->table_budget = d.table_budget;
+  t->cube = d.cube;
 }
 
 int cx_codegen(const char* plan, size_t plan_len, const cx_tuning* tuning, char* out, size_t out_cap, size_t* out_len) {
@@ -1011,16 +1133,24 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
     if (q.param_off < 0 || q.param_off + sh.nlits > nparams)
       return fail(CX_E_INVALID, "cx_shared_execute: query %d parameters fall outside the parameter array", order[i]);
   }
-  // Passes of at most maxq queries; each pass gets its own descriptors and a
+  // The aggregate-cube path answers the whole batch in one pass when the
+  // registered ranges allow; otherwise passes of at most maxq queries run the
+  // per-query mask kernels.  Each pass gets its own descriptors and a
   // compacted parameter array.
-  const int maxq = std::max(1, std::min(lp.shared_maxq, 256));
+  CubePlan cp;
+  std::vector<int> qshapes(nq);
+  for (int i = 0; i < nq; ++i) qshapes[i] = queries[i].shape;
+  const bool cube = plan_cubes(lp, c, qshapes.data(), nq, cp);
+  const int maxq = cube ? std::max(nq, 1) : std::max(1, std::min(lp.shared_maxq, 256));
   const int npass = (nq + maxq - 1) / maxq;
   std::vector<int> pass_params(std::max(npass, 1), 0);
+  int maxp = lp.shared_maxp;
   for (int ps = 0; ps < npass; ++ps) {
     int np = 0;
     for (int i = ps * maxq; i < std::min(nq, (ps + 1) * maxq); ++i) np += lp.sshapes[queries[order[i]].shape].nlits;
-    if (np > lp.shared_maxp) return fail(CX_E_CAPACITY, "cx_shared_execute: %d parameters in one pass exceed %d", np, lp.shared_maxp);
+    if (!cube && np > lp.shared_maxp) return fail(CX_E_CAPACITY, "cx_shared_execute: %d parameters in one pass exceed %d", np, lp.shared_maxp);
     pass_params[ps] = np;
+    maxp = std::max(maxp, np);
   }
 
   // Scratch: dimension slot entries (zeroed per pass), touched bits per grouped
@@ -1041,7 +1171,9 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
     if (sh.grouped) { touch_off[i] = off; off = align256(off + ((sh.groups + 31) / 32) * 4); }
   }
   const uint64_t touch_end = off;
-  const size_t desc_bytes = (size_t)maxq * sizeof(CxSQ), par_bytes = (size_t)std::max(lp.shared_maxp, 1) * 4;
+  const uint64_t cube_off = off;
+  if (cube) off = align256(off + cp.gbytes);
+  const size_t desc_bytes = (size_t)maxq * sizeof(CxSQ), par_bytes = (size_t)std::max(maxp, 1) * 4;
   const size_t pass_bytes = align256(desc_bytes + par_bytes);
   const uint64_t pass_off = off; off += (uint64_t)std::max(npass, 1) * pass_bytes;
   const uint64_t err_off = off; off = align256(off + 16);
@@ -1087,8 +1219,9 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
   }
 
   size_t scan_ki = 0;
-  while (scan_ki < lp.kernels.size() && lp.kernels[scan_ki].kind != "sharedscan") ++scan_ki;
-  if (scan_ki == lp.kernels.size()) return fail(CX_E_INVALID, "cx_shared_execute: program has no shared scan kernel");
+  const char* scan_kind = cube ? "cubescan" : "sharedscan";
+  while (scan_ki < lp.kernels.size() && lp.kernels[scan_ki].kind != scan_kind) ++scan_ki;
+  if (scan_ki == lp.kernels.size()) return fail(CX_E_INVALID, "cx_shared_execute: program has no %s kernel", scan_kind);
   const KernelSpec& sk = lp.kernels[scan_ki];
   // Shared-memory group tables go into the slack the scan's own residency
   // leaves, so they never cost a resident CTA.
@@ -1119,7 +1252,7 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
     int* hpar = (int*)(hstage + desc_bytes);
     int poff = 0;
     uint64_t tab_words = 0, bit_words = 0;
-    const size_t qb_bytes = ((size_t)lp.shared_qb_bytes * (size_t)qn + 15) & ~(size_t)15;
+    const size_t qb_bytes = cube ? 0 : ((size_t)lp.shared_qb_bytes * (size_t)qn + 15) & ~(size_t)15;
     for (int j = 0; j < qn; ++j) {
       const cx_shared_query& q = queries[order[q0 + j]];
       const auto& sh = lp.sshapes[q.shape];
@@ -1133,7 +1266,7 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
       hsq[j].smem_acc = -1;
       hsq[j].smem_bits = 0;
       hsq[j].keep = keep ? (keep[order[q0 + j]] ? 1 : 0) : 0;
-      if (!sh.smem_ok) continue;
+      if (cube || !sh.smem_ok) continue;
       const uint64_t tw = tab_words + sh.groups * (uint64_t)sh.naggs;
       const uint64_t bw = bit_words + sh.tw * (uint64_t)(1 + sh.nseen);
       if (sk.smem + qb_bytes + tw * 8 + bw * 4 + 64 > smem_cap) continue;
@@ -1153,11 +1286,22 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
       const int s = hsq[j].shape;
       if (s < CX_MAX_SHAPES) { if (a.sq_num[s] == 0) a.sq_first[s] = j; ++a.sq_num[s]; }
     }
+    if (cube) {
+      for (size_t id = 0; id < cp.lo.size(); ++id) { a.cube_lo[id] = cp.lo[id]; a.cube_radix[id] = cp.radix[id]; }
+      for (int s = 0; s < nshapes && s < CX_MAX_SHAPES; ++s) {
+        for (int j = 0; j < CX_MAX_SATTRS; ++j) a.cube_stride[s * CX_MAX_SATTRS + j] = cp.stride[s][j];
+        a.cube_g[s] = cp.cells[s] ? (unsigned long long*)(scratch + cube_off + cp.goff[s]) : nullptr;
+        a.cube_cells[s] = (long long)cp.cells[s];
+        a.cube_smem[s] = cp.smem_off[s];
+      }
+      a.cube_smem_words = (int)cp.smem_words;
+      a.cube_chunks = cp.chunks;
+    }
     P.args = a;
     P.qn = qn;
     P.nparams = poff;
     P.hstage = hstage;
-    P.extra_smem = qb_bytes + (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
+    P.extra_smem = cube ? (size_t)cp.smem_words * 8 : qb_bytes + (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
     int occ = 1;
     CUresult orr = d.Occupancy(&occ, L->fns[scan_ki], sk.block, sk.smem + P.extra_smem);
     if (orr != CUDA_SUCCESS) return drv_fail(orr, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -1194,11 +1338,16 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
       if (P.nparams)
         CX_CUDA(cudaMemcpyAsync((void*)P.args.sparams, P.hstage + desc_bytes, (size_t)P.nparams * 4, cudaMemcpyHostToDevice, s));
       CX_CUDA(cudaMemsetAsync(scratch, 0, dim_end, s));
+      if (cube && cp.gbytes) CX_CUDA(cudaMemsetAsync(scratch + cube_off, 0, cp.gbytes, s));
+      // Before the scan: result zeroing and the path's dimension indexes; after
+      // it: the cube answers (cube path) and the group-key epilogue.
       for (size_t ki = 0; ki < scan_ki; ++ki) {
         const KernelSpec& k = lp.kernels[ki];
         unsigned grid;
         if (k.kind == "zero") grid = (unsigned)P.qn;
-        else grid = (unsigned)std::min<long long>((rows[k.table] + k.tile - 1) / k.tile, (long long)sms * 16);
+        else if (k.kind == (cube ? "cubeidx" : "build"))
+          grid = (unsigned)std::min<long long>((rows[k.table] + k.tile - 1) / k.tile, (long long)sms * 16);
+        else continue;
         int r = launch(ki, grid, 0, &P.args);
         if (r) return r;
       }
@@ -1206,8 +1355,14 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
       int r = launch(scan_ki, P.scan_grid, P.extra_smem, &P.args);
       if (r) return r;
       if (ps == npass - 1) CX_CUDA(rec(c->ev[2]));
-      for (size_t ki = scan_ki + 1; ki < lp.kernels.size(); ++ki)
-        if ((r = launch(ki, (unsigned)P.qn, 0, &P.args))) return r;
+      for (size_t ki = scan_ki + 1; ki < lp.kernels.size(); ++ki) {
+        const KernelSpec& k = lp.kernels[ki];
+        unsigned grid;
+        if (k.kind == "queries") grid = (unsigned)P.qn;
+        else if (cube && k.kind == "cubeans") grid = (unsigned)(P.qn * cp.chunks);
+        else continue;
+        if ((r = launch(ki, grid, 0, &P.args))) return r;
+      }
     }
     if (npass == 0) {
       CX_CUDA(rec(c->ev[1]));
@@ -1229,7 +1384,7 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
     const void* ids[] = {scratch, c->host_stage, c->host_err};
     put(ids, sizeof ids);
     put(&m->uid, sizeof m->uid);
-    const uint64_t sizes[] = {dim_end, err_off, (uint64_t)npass, (uint64_t)sms};
+    const uint64_t sizes[] = {dim_end, err_off, (uint64_t)npass, (uint64_t)sms, (uint64_t)cube, cube_off, cp.gbytes};
     put(sizes, sizeof sizes);
     for (const Pass& P : passes) {
       put(&P.args, sizeof(CxArgs));
@@ -1272,6 +1427,7 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
   c->timing.scan_grid = npass ? (int)passes.back().scan_grid : 0;
   c->timing.gpu_launches = launches;
   c->timing.graph = graph_mode;
+  c->timing.mode = cube ? 1 : 0;
   return CX_OK;
 }
 

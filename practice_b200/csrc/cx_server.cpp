@@ -180,9 +180,9 @@ int rebuild_universe(cx_server* s) {
 std::string tuning_key(const cx_tuning* t) {
   if (!t) return "default";
   char buf[256];
-  snprintf(buf, sizeof buf, "%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d", t->block_threads, t->items_per_thread,
+  snprintf(buf, sizeof buf, "%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d/%d", t->block_threads, t->items_per_thread,
            t->stages, t->ctas_per_sm, t->group_placement, t->smem_group_budget, t->bitmap_budget, t->group_merge,
-           t->prefetch, t->wait_limit_us, t->debug_stall, t->compact, t->table_budget);
+           t->prefetch, t->wait_limit_us, t->debug_stall, t->compact, t->table_budget, t->cube);
   return buf;
 }
 
@@ -476,7 +476,7 @@ void scheduler(cx_server* s) {
           Request* r = s->pending.front();
           if (!in_universe(r)) break;
           shapes.push_back(s->shape_index.at(r->shape));
-          const uint64_t need = cx_internal::shared_scratch_need(s->universe, shapes.data(), (int)shapes.size());
+          const uint64_t need = cx_internal::shared_scratch_need(s->universe, sl.ctx, shapes.data(), (int)shapes.size());
           if (!admit(cx_internal::grown_scratch(own, need) - own, add + r->est_bytes)) {
             shapes.pop_back();
             break;

@@ -8,8 +8,8 @@ from pathlib import Path
 
 import pytest
 
-from practice_b200 import _lib, queries
-from practice_b200.plan import PlanBuilder, Table, col, star
+from practice_b200 import _lib, datagen, queries
+from practice_b200.plan import PlanBuilder, Table, col, lit, star
 
 ROOT = Path(__file__).resolve().parent.parent
 
@@ -212,6 +212,30 @@ def test_shared_program_for_the_four_templates_compiles():
     assert m.info.result_words >= 0
     # literals come back in the order that numbers the shape's parameters
     assert _lib.plan_literals(plans[1].text())[0] == plans[1].steps[0][1].kids[1].val
+
+
+def test_shared_program_carries_the_cube_path_when_shapes_allow():
+    rng = random.Random(13)
+    texts = [queries.template(t, rng).text() for t in range(4)]
+    src = _lib.shared_codegen(texts)
+    assert "CubeScan_LINEORDER" in src and "cube_answer" in src and "cube_index_part" in src
+    launch = src.split("@*/")[0]
+    # quantity, discount, c_region, s_region, d_year, c_nation, p_category, p_brand1
+    assert "\ncube 8\n" in launch
+    from practice_b200.engine import SHARED_DEFAULT, make_tuning
+    assert _lib.default_tuning().cube == 4
+    t = make_tuning(**{**SHARED_DEFAULT, "cube": 0})
+    assert "CubeScan" not in _lib.shared_codegen(texts, t) and "SharedScan_LINEORDER" in _lib.shared_codegen(texts, t)
+    for ipt in (1, 2):
+        t.cube = ipt
+        m = _lib.Module(_lib.shared_codegen(texts, t), key=f"cpu_cube_{ipt}")
+        assert m.info.result_words >= 0
+    # An aggregate that reads a literal cannot be summed once for every query of its shape.
+    tables = datagen.ssb_tables(1000, queries.BATCH_COLS)
+    b = PlanBuilder(tables, "LINEORDER", name="L")
+    b.filter(col("lo_quantity").lt(10))
+    lit_agg = b.aggregate([], [("sum", col("lo_revenue") * lit(3))]).text()
+    assert "CubeScan" not in _lib.shared_codegen([lit_agg] + texts)
 
 
 def test_shared_program_rejects_unshareable_shapes():

@@ -74,10 +74,10 @@ def test_shared_scan_wait_runs_out_and_context_recovers(loaded):
     import random
     plans = [queries.template(t, random.Random(300 + t), n) for t in range(4)]
     stall = make_tuning(block_threads=1024, items_per_thread=1, stages=3, ctas_per_sm=1,
-                        wait_limit_us=LIMIT_US, debug_stall=1)
+                        wait_limit_us=LIMIT_US, debug_stall=1, cube=0)  # the per-query path waits on mbarriers
     got = db.execute_shared(plans, stall)
     assert all(g.kernel_error == 1 for g in got)
-    good = db.execute_shared(plans, make_tuning(block_threads=1024, items_per_thread=1, stages=3, ctas_per_sm=1))
+    good = db.execute_shared(plans, make_tuning(block_threads=1024, items_per_thread=1, stages=3, ctas_per_sm=1, cube=0))
     for p, g in zip(plans, good):
         assert g.kernel_error == 0
         np.testing.assert_array_equal(g.words, _ref(p, ht).words[: len(g.words)])

@@ -8,6 +8,7 @@ import pytest
 
 import oracle
 from practice_b200 import _lib, datagen, queries, results
+from practice_b200.engine import SHARED_DEFAULT, make_tuning
 from practice_b200.plan import Group, PlanBuilder, and_, col, lit, not_, or_, star
 
 pytestmark = pytest.mark.gpu
@@ -260,19 +261,59 @@ def test_shared_scan_two_passes(db):
 
 @pytest.mark.parametrize("rng_lo,rng_hi", [(40, 45), (1000, 2000), (-300, -100)])
 def test_shared_scan_values_outside_filter_windows(db, rng_lo, rng_hi):
-    """Fact values outside the filter tables' window fall back to per-query
-    evaluation: a registered range that misses most values gives the same
-    answers."""
+    """Per-query path: fact values outside the filter tables' window fall back
+    to per-query evaluation, so a registered range that misses most values
+    gives the same answers.  The aggregate-cube path takes the range as a
+    bound and reports the values outside it (kernel error 5) rather than
+    answering wrongly."""
     n = 400_009
     ht = load(db, 44, n, queries.BATCH_COLS)
     db.ctx.set_column_range("d_lo_quantity", rng_lo, rng_hi)
     db.ctx.set_column_range("d_lo_discount", rng_lo, rng_hi)
     plans = queries.batch(24, 77, n)
-    got = db.execute_shared(plans)
+    got = db.execute_shared(plans, make_tuning(**{**SHARED_DEFAULT, "cube": 0}))
+    assert got[0].timing.mode == 0
     for p, g in zip(plans, got):
         ref = oracle_run(p, ht)
         np.testing.assert_array_equal(g.words, ref.words)
         np.testing.assert_array_equal(g.validity, ref.validity)
+    got = db.execute_shared(plans, make_tuning(**SHARED_DEFAULT))
+    assert got[0].timing.mode == 1 and got[0].kernel_error == 5
+
+
+@pytest.mark.parametrize("cube,nq", [(0, 40), (1, 40), (2, 40), (4, 40), (4, 1), (4, 130)])
+def test_shared_scan_cube_and_mask_paths(db, cube, nq):
+    """A mixed batch through the aggregate-cube path (cube = rows per lane of
+    its scan; one pass whatever the batch size) and through the per-query mask
+    path (cube = 0): every query equals the oracle on its own, and the timing
+    reports which path ran.  The fact table's size is not a multiple of a warp
+    tile, so the ragged last tile is covered."""
+    n = 600_011
+    ht = load(db, 47, n, queries.BATCH_COLS)
+    plans = queries.batch(nq, 4700 + nq, n)
+    got = db.execute_shared(plans, make_tuning(**{**SHARED_DEFAULT, "cube": cube}))
+    assert got[0].kernel_error == 0
+    assert got[0].timing.mode == (1 if cube else 0)
+    for p, g in zip(plans, got):
+        ref = oracle_run(p, ht)
+        np.testing.assert_array_equal(g.words, ref.words, err_msg=p.name)
+        np.testing.assert_array_equal(g.validity, ref.validity, err_msg=p.name)
+
+
+def test_shared_scan_cube_path_falls_back_for_wide_shapes(db):
+    """A shape whose cube would exceed 16,777,216 cells (GROUP BY c_city,
+    s_city, lo_discount, d_month under region and year filters) sends the whole
+    batch down the per-query mask path; the answers still equal the oracle."""
+    n = 300_007
+    ht = load(db, 48, n, queries.BATCH_COLS)
+    rng = random.Random(48)
+    plans = [queries.wide_groups(rng, n)] + [queries.template(t, rng, n) for t in range(4)]
+    got = db.execute_shared(plans)
+    assert got[0].kernel_error == 0 and got[0].timing.mode == 0
+    for p, g in zip(plans, got):
+        ref = oracle_run(p, ht)
+        np.testing.assert_array_equal(g.words, ref.words, err_msg=p.name)
+        np.testing.assert_array_equal(g.validity, ref.validity, err_msg=p.name)
 
 
 def test_shared_scan_residual_filters(db):

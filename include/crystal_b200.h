@@ -356,6 +356,9 @@ typedef struct cx_server_config {
                              to 1024); queries join at any range boundary and finish once they
                              have covered every row, so arrivals wait for one range, not for a
                              whole-table launch */
+  uint64_t cube_bytes;    /* per slot: most device bytes the aggregate cubes of one shared launch may
+                             take (cx_tuning.cube); a batch whose cubes need more runs the
+                             per-query path.  0 = budget_bytes / (2 x slots) */
 } cx_server_config;
 
 typedef struct cx_request_info {

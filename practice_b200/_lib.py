@@ -67,7 +67,8 @@ class SortKey(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("budget_bytes", C.c_uint64), ("max_batch", C.c_int), ("slots", C.c_int), ("plain_only", C.c_int),
-                ("min_shared_batch", C.c_int), ("shared_tuning", Tuning), ("chunk_rows", C.c_uint64)]
+                ("min_shared_batch", C.c_int), ("shared_tuning", Tuning), ("chunk_rows", C.c_uint64),
+                ("cube_bytes", C.c_uint64)]
 
 
 class RequestInfo(C.Structure):

@@ -2233,6 +2233,26 @@ struct SharedGen {
     }
   }
 
+  // Bit c of colmask[s]: shape s reads staged fact column c.
+  std::vector<unsigned long long> shape_colmasks() const {
+    std::vector<unsigned long long> colmask(shapes.size(), 0ULL);
+    for (size_t si = 0; si < shapes.size(); ++si) {
+      const Plan& p = *shapes[si];
+      std::vector<std::string> cs;
+      for (const auto& st : p.steps) {
+        if (st.kind == Step::Filter) cols_of(st.filter.get(), cs);
+        else cs.push_back(st.join.fks[0]);
+      }
+      for (const auto& g : p.groups) cols_of(g.expr.get(), cs);
+      for (const auto& ag : p.aggs) cols_of(ag.arg.get(), cs);
+      for (const auto& c : cs) {
+        auto it = std::find(fact_cols.begin(), fact_cols.end(), c);
+        if (it != fact_cols.end() && it - fact_cols.begin() < 64) colmask[si] |= 1ULL << (it - fact_cols.begin());
+      }
+    }
+    return colmask;
+  }
+
   int sum_aggs(const Plan& p) const {
     int n = 0;
     for (const auto& ag : p.aggs) n += ag.fn == AggFn::Sum;
@@ -2309,7 +2329,10 @@ struct SharedGen {
     const std::string kname = "CubeScan_" + fact;
     meta << "kernel " << kname << " cubescan 0 " << CTA << " " << 32 * IPT << " " << fr_bytes << " 8\n";
     std::ostringstream& o = src;
-    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", 2) " << kname << "(const CxArgs a) {\n";
+    // Registers per thread: 128 for four rows per lane, 64 for two, 48 for one
+    // (more resident warps to cover the dimension gathers' latency).
+    const int min_blocks = IPT >= 4 ? 2 : IPT == 2 ? 4 : 5;
+    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", " << min_blocks << ") " << kname << "(const CxArgs a) {\n";
     o << "  constexpr int IPT = " << IPT << ", VW = " << VW << ", TROWS = " << 32 * IPT << ";\n";
     o << "  extern __shared__ __align__(16) unsigned char cx_smem[];\n";
     o << "  unsigned* s_fr = (unsigned*)cx_smem; (void)s_fr;\n";
@@ -2350,6 +2373,11 @@ struct SharedGen {
     for (int k = 0; k < NFC; ++k) o << "  const unsigned fb" << k << " = (unsigned)a.fbase[" << k << "], fw" << k << " = (unsigned)a.fwin[" << k << "];\n";
     o << "  bool vec_ok = true;\n";
     for (const auto& c : fact_cols) o << "  vec_ok = vec_ok && ((((unsigned long long)d_" << c << ") & 15ULL) == 0ULL);\n";
+    // Fact columns the batch's shapes read (columns of shapes without queries are not loaded).
+    if (fact_cols.size() > 64) throw PlanError("more than 64 fact columns in a shared batch");
+    const std::vector<unsigned long long> colmask = shape_colmasks();
+    o << "  unsigned long long need = 0ULL;\n";
+    for (size_t s = 0; s < shapes.size(); ++s) o << "  if (a.sq_num[" << s << "] > 0) need |= " << colmask[s] << "ULL;\n";
     o << "  const long long n = a.rows[0];\n";
     o << "  const long long ntiles = (n + TROWS - 1) / TROWS;\n";
     o << "  const long long nw = ((long long)gridDim.x * " << CTA << ") >> 5;\n";
@@ -2358,12 +2386,17 @@ struct SharedGen {
     o << "    const int nt = (int)(n - base < TROWS ? n - base : TROWS);\n";
     for (const auto& c : fact_cols) o << "    int c_" << c << "[IPT];\n";
     o << "    if (nt == TROWS && vec_ok) {\n";
-    for (const auto& c : fact_cols) o << "      WarpLoadTileV<IPT>(d_" << c << " + base, lane, c_" << c << ");\n";
+    for (size_t k = 0; k < fact_cols.size(); ++k) {
+      const std::string& c = fact_cols[k];
+      o << "      if ((need >> " << k << ") & 1ULL) WarpLoadTileV<IPT>(d_" << c << " + base, lane, c_" << c << ");\n";
+      o << "      else { \n        #pragma unroll\n        for (int i = 0; i < IPT; ++i) c_" << c << "[i] = 0;\n      }\n";
+    }
     o << "    } else {\n";
     o << "      #pragma unroll\n";
     o << "      for (int i = 0; i < IPT; ++i) {\n";
     o << "        const int r = (i / VW) * 32 * VW + lane * VW + (i % VW);\n";
-    for (const auto& c : fact_cols) o << "        c_" << c << "[i] = r < nt ? d_" << c << "[base + r] : 0;\n";
+    for (size_t k = 0; k < fact_cols.size(); ++k)
+      o << "        c_" << fact_cols[k] << "[i] = (r < nt && ((need >> " << k << ") & 1ULL)) ? d_" << fact_cols[k] << "[base + r] : 0;\n";
     o << "      }\n";
     o << "    }\n";
     // Shapes each row may belong to after the fact filter tables.
@@ -2432,11 +2465,21 @@ struct SharedGen {
         o << "          const unsigned long long x" << ks << "_ = (unsigned long long)(" << e.math_push(ag.arg.get(), true) << ");\n";
         ++ks;
       }
+      // Shared-memory cubes keep each sum as two 32-bit words (low word
+      // first, the carry of its add going into the high word) and a 32-bit
+      // row count: every update is a native 32-bit shared-memory atomic.
       o << "          if (a.cube_smem[" << s << "] >= 0) {\n";
-      o << "            unsigned long long* cs_ = s_cube + a.cube_smem[" << s << "];\n";
+      o << "            unsigned* cs_ = (unsigned*)(s_cube + a.cube_smem[" << s << "]);\n";
       o << "            const unsigned nc_ = (unsigned)a.cube_cells[" << s << "];\n";
-      for (int k = 0; k < NS; ++k) o << "            if (x" << k << "_) atomicAdd(&cs_[" << k << "u * nc_ + cell_], x" << k << "_);\n";
-      o << "            atomicAdd((unsigned*)(cs_ + " << NS << "u * nc_) + cell_, 1u);\n";
+      for (int k = 0; k < NS; ++k) {
+        o << "            if (x" << k << "_) {\n";
+        o << "              const unsigned lo_ = (unsigned)x" << k << "_;\n";
+        o << "              const unsigned old_ = atomicAdd(&cs_[" << 2 * k << "u * nc_ + cell_], lo_);\n";
+        o << "              const unsigned hi_ = (unsigned)(x" << k << "_ >> 32) + (old_ + lo_ < old_ ? 1u : 0u);\n";
+        o << "              if (hi_) atomicAdd(&cs_[" << 2 * k + 1 << "u * nc_ + cell_], hi_);\n";
+        o << "            }\n";
+      }
+      o << "            atomicAdd(&cs_[" << 2 * NS << "u * nc_ + cell_], 1u);\n";
       o << "          } else {\n";
       o << "            unsigned long long* cg_ = a.cube_g[" << s << "];\n";
       o << "            const unsigned long long nc_ = (unsigned long long)a.cube_cells[" << s << "];\n";
@@ -2453,15 +2496,16 @@ struct SharedGen {
     for (size_t s = 0; s < shapes.size(); ++s) {
       const int NS = sum_aggs(*shapes[s]);
       o << "  if (a.cube_smem[" << s << "] >= 0 && a.sq_num[" << s << "] > 0) {\n";
-      o << "    const unsigned long long* cs_ = s_cube + a.cube_smem[" << s << "];\n";
+      o << "    const unsigned* cs_ = (const unsigned*)(s_cube + a.cube_smem[" << s << "]);\n";
       o << "    const unsigned nc_ = (unsigned)a.cube_cells[" << s << "];\n";
       o << "    unsigned long long* cg_ = a.cube_g[" << s << "];\n";
       o << "    for (unsigned c = threadIdx.x; c < nc_; c += " << CTA << ") {\n";
-      o << "      const unsigned n_ = ((const unsigned*)(cs_ + " << NS << "u * nc_))[c];\n";
+      o << "      const unsigned n_ = cs_[" << 2 * NS << "u * nc_ + c];\n";
       o << "      if (!n_) continue;\n";
       o << "      atomicAdd(&cg_[" << NS << "ULL * nc_ + c], (unsigned long long)n_);\n";
       for (int k = 0; k < NS; ++k)
-        o << "      { const unsigned long long v_ = cs_[" << k << "u * nc_ + c]; if (v_) atomicAdd(&cg_[" << k << "ULL * nc_ + c], v_); }\n";
+        o << "      { const unsigned long long v_ = ((unsigned long long)cs_[" << 2 * k + 1 << "u * nc_ + c] << 32) | cs_["
+          << 2 * k << "u * nc_ + c]; if (v_) atomicAdd(&cg_[" << k << "ULL * nc_ + c], v_); }\n";
       o << "    }\n";
       o << "  }\n";
     }
@@ -2749,22 +2793,8 @@ struct SharedGen {
       o << "  }\n";
     }
     // Fact columns each shape reads (bits over the staged columns).
-    std::vector<unsigned long long> colmask(shapes.size(), 0ULL);
     if (NSC > 64) throw PlanError("more than 64 fact columns in a shared batch");
-    for (size_t si = 0; si < shapes.size(); ++si) {
-      const Plan& p = *shapes[si];
-      std::vector<std::string> cs;
-      for (const auto& st : p.steps) {
-        if (st.kind == Step::Filter) cols_of(st.filter.get(), cs);
-        else cs.push_back(st.join.fks[0]);
-      }
-      for (const auto& g : p.groups) cols_of(g.expr.get(), cs);
-      for (const auto& ag : p.aggs) cols_of(ag.arg.get(), cs);
-      for (const auto& c : cs) {
-        auto it = std::find(fact_cols.begin(), fact_cols.end(), c);
-        if (it != fact_cols.end()) colmask[si] |= 1ULL << (it - fact_cols.begin());
-      }
-    }
+    const std::vector<unsigned long long> colmask = shape_colmasks();
     // Masks of the queries that skip each dimension, that carry residual
     // filters, that have filter-table conjuncts, and of the whole batch; and
     // the fact columns the batch reads.

@@ -27,6 +27,8 @@ uint64_t ctx_scratch_bytes(const cx_exec_ctx* c);
 // Scratch bytes cx_shared_execute needs for a batch of queries of `shapes`
 // (program shape indexes) on program `m`.
 uint64_t shared_scratch_need(const cx_module* m, const cx_exec_ctx* c, const int* shapes, int nq);
+// Most bytes of aggregate cubes one shared launch on `c` may take (larger batches run the per-query path).
+void ctx_set_cube_cap(cx_exec_ctx* c, uint64_t bytes);
 
 // Scratch bytes a context owns after an execute that needs `need` bytes, when
 // it owns `own` bytes before (own scratch grows to 1.5x the need).

@@ -397,6 +397,7 @@ struct cx_exec_ctx {
   uint32_t kernel_err = 0;
   // Shared-scan batches replay a captured CUDA graph while their pass shapes repeat.
   bool graph_replay = true;
+  uint64_t cube_cap = UINT64_MAX;   // most bytes of aggregate cubes one shared launch may take
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t gexec = nullptr;
   std::vector<unsigned char> gsig;
@@ -506,7 +507,7 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
     g = align256(g + cells * (uint64_t)(sh.nsums + 1) * 8);
     maxcells = std::max(maxcells, cells);
   }
-  if (g > kCubeMaxGlobalBytes) { cp.why = "the batch's cubes exceed 8 GiB"; return false; }
+  if (g > std::min(kCubeMaxGlobalBytes, c->cube_cap)) { cp.why = "the batch's cubes exceed the context's cube budget"; return false; }
   cp.gbytes = g;
   // Shared-memory copies for the smallest cubes first, within the per-CTA budget.
   std::vector<int> order;
@@ -515,7 +516,8 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
   std::sort(order.begin(), order.end(), [&](int x, int y) { return cp.cells[x] < cp.cells[y]; });
   uint64_t words = 0;
   for (int s : order) {
-    const uint64_t w = cp.cells[s] * (uint64_t)lp.cshapes[s].nsums + (cp.cells[s] + 1) / 2;
+    // Per SUM aggregate a low and a high 32-bit word per cell, then a 32-bit row count.
+    const uint64_t w = (cp.cells[s] * (uint64_t)(2 * lp.cshapes[s].nsums + 1) + 1) / 2;
     if ((words + w) * 8 > kCubeSmemBudget) continue;
     cp.smem_off[s] = (int)words;
     words += w;
@@ -547,6 +549,8 @@ bool ctx_column_range(const cx_exec_ctx* c, const std::string& name, int64_t* lo
 }
 
 uint64_t ctx_scratch_bytes(const cx_exec_ctx* c) { return c->own_scratch_bytes; }
+
+void ctx_set_cube_cap(cx_exec_ctx* c, uint64_t bytes) { c->cube_cap = bytes; }
 
 int set_error(int code, const std::string& msg) { return fail(code, "%s", msg.c_str()); }
 

@@ -591,6 +591,8 @@ int cx_server_create(const cx_exec_ctx* tables, const cx_server_config* cfg, cx_
     // ranges), so a captured graph would be re-captured every time: launch
     // the kernels directly.
     cx_ctx_set_graph_replay(sl.ctx, 0);
+    cx_internal::ctx_set_cube_cap(sl.ctx, s->cfg.cube_bytes ? s->cfg.cube_bytes
+                                                            : s->cfg.budget_bytes / (2 * (uint64_t)s->cfg.slots));
     if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess)
       return serr(CX_E_CUDA, "cx_server_create: stream or event creation failed");

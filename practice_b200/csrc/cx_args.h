@@ -68,4 +68,11 @@ struct CxArgs {
   int cube_smem[CX_MAX_SHAPES];
   int cube_smem_words;                         // u64 words of all shared-memory cubes
   int cube_chunks;                             // answer blocks per query
+  // An attribute determined by another attribute of the shape (a dimension's
+  // functional dependency, e.g. region by nation) takes no part in the cell
+  // index: per shape attribute the position of its source attribute in the
+  // shape (-1: none), per attribute the table from the source's value offset
+  // to its own.
+  int cube_fdsrc[CX_MAX_SHAPES * CX_MAX_SATTRS];
+  const int* cube_fdtab[CX_MAX_CATTRS];
 };

@@ -2548,10 +2548,25 @@ struct SharedGen {
       o << "        const unsigned long long n_ = cg_[" << NS << "ULL * (unsigned long long)nc_ + c];\n";
       o << "        if (!n_) continue;\n";
       o << "        const unsigned cu_ = (unsigned)c;\n";
-      for (size_t j = 0; j < sh_attrs[s].size(); ++j) {
+      // Value offsets from the cell index; an attribute with a functional
+      // source (stride 0) reads its offset from the source's through its table.
+      const size_t NAT = sh_attrs[s].size();
+      for (size_t j = 0; j < NAT; ++j) {
         const int id = sh_attrs[s][j];
-        o << "        const int v_" << cattrs[id].col << " = (int)((cu_ / (unsigned)a.cube_stride[" << s * MAX_SATTRS + j
-          << "]) % (unsigned)a.cube_radix[" << id << "]) + a.cube_lo[" << id << "];\n";
+        const std::string st = "a.cube_stride[" + std::to_string(s * MAX_SATTRS + j) + "]";
+        o << "        int x" << j << "_ = " << st << " > 0 ? (int)((cu_ / (unsigned)" << st << ") % (unsigned)a.cube_radix[" << id << "]) : 0;\n";
+      }
+      for (size_t j = 0; j < NAT; ++j) {
+        const int id = sh_attrs[s][j];
+        o << "        switch (a.cube_fdsrc[" << s * MAX_SATTRS + j << "]) {\n";
+        for (size_t k = 0; k < NAT; ++k)
+          if (k != j) o << "          case " << k << ": x" << j << "_ = a.cube_fdtab[" << id << "][x" << k << "_]; break;\n";
+        o << "          default: break;\n";
+        o << "        }\n";
+      }
+      for (size_t j = 0; j < NAT; ++j) {
+        const int id = sh_attrs[s][j];
+        o << "        const int v_" << cattrs[id].col << " = x" << j << "_ + a.cube_lo[" << id << "];\n";
       }
       std::vector<const Expr*> all;
       for (const auto& st : p.steps) all.push_back(st.kind == Step::Filter ? st.filter.get() : st.join.filter.get());

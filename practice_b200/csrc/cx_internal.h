@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <string>
 
+#include <cuda_runtime.h>
+
 #include "../../include/crystal_b200.h"
 #include "cx_codegen.h"
 
@@ -29,6 +31,10 @@ uint64_t ctx_scratch_bytes(const cx_exec_ctx* c);
 uint64_t shared_scratch_need(const cx_module* m, const cx_exec_ctx* c, const int* shapes, int nq);
 // Most bytes of aggregate cubes one shared launch on `c` may take (larger batches run the per-query path).
 void ctx_set_cube_cap(cx_exec_ctx* c, uint64_t bytes);
+// Checks (once per context and column pair, waiting on `s`) which cube
+// attributes of a dimension determine others, so that later scratch estimates
+// for program `m` see the cube layout its launches will use.
+int ensure_cube_dependencies(const cx_module* m, cx_exec_ctx* c, cudaStream_t s);
 
 // Scratch bytes a context owns after an execute that needs `need` bytes, when
 // it owns `own` bytes before (own scratch grows to 1.5x the need).
@@ -50,6 +56,13 @@ uint64_t module_fact_rows(const cx_module* m, const cx_exec_ctx* c);
 
 // Takes one more reference on a module (dropped with cx_module_release).
 void module_retain(cx_module* m);
+
+// Enqueues the check whether dimension column `b` determines column `a` (n
+// rows, value offsets from lo_a / lo_b, radix_b values of b): tab (radix_b
+// ints) ends up mapping each b offset to its a offset, and *flag (zeroed by the
+// caller) becomes non-zero when some b offset has two different a offsets.
+int fd_check_launch(const int* a, const int* b, long long n, int lo_a, int lo_b, int radix_b, int* tab, unsigned* flag,
+                    cudaStream_t s);
 
 // Records `msg` as the calling thread's cx_last_error() and returns `code`.
 int set_error(int code, const std::string& msg);

@@ -2,6 +2,7 @@
 // sparse-result compaction and the seeded synthetic column generator.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -275,3 +276,45 @@ extern "C" int cx_gen_validity(uint64_t stream, uint64_t seed, uint64_t rows, ui
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? CX_OK : cuda_fail(e, "gen_validity");
 }
+
+// ------------------------------------------------- functional dependencies --
+// Whether column B of a dimension determines column A (every row with the
+// same B value has the same A value): each row claims tab[B - lo_b] for its
+// A offset; a second, different offset sets the flag.  `tab` (radix_b ints)
+// must hold -1 before the launch; afterwards it maps each B offset that
+// occurs to its A offset.
+namespace {
+
+__global__ void __launch_bounds__(256)
+fd_check(const int* __restrict__ a, const int* __restrict__ b, long long n, int lo_a, int lo_b, unsigned radix_b,
+         int* __restrict__ tab, unsigned* __restrict__ flag) {
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
+    const unsigned bo = (unsigned)(b[r] - lo_b);
+    const int ao = a[r] - lo_a;
+    if (bo >= radix_b) { atomicOr(flag, 1u); continue; }
+    const int old = atomicCAS(&tab[bo], -1, ao);
+    if (old != -1 && old != ao) atomicOr(flag, 1u);
+  }
+}
+
+}  // namespace
+
+namespace cx_internal {
+
+int fd_check_launch(const int* a, const int* b, long long n, int lo_a, int lo_b, int radix_b, int* tab, unsigned* flag,
+                    cudaStream_t s) {
+  if (!a || !b || !tab || !flag || n < 0 || radix_b <= 0) return invalid("fd_check: bad argument");
+  cudaError_t e = cudaMemsetAsync(tab, 0xFF, (size_t)radix_b * sizeof(int), s);
+  if (e != cudaSuccess) return cuda_fail(e, "fd_check: memset");
+  if (n == 0) return CX_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long blocks = std::min<long long>((n + 255) / 256, (long long)sms * 8);
+  fd_check<<<(unsigned)blocks, 256, 0, s>>>(a, b, n, lo_a, lo_b, (unsigned)radix_b, tab, flag);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "fd_check");
+  return CX_OK;
+}
+
+}  // namespace cx_internal

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <sstream>
@@ -398,6 +399,11 @@ struct cx_exec_ctx {
   // Shared-scan batches replay a captured CUDA graph while their pass shapes repeat.
   bool graph_replay = true;
   uint64_t cube_cap = UINT64_MAX;   // most bytes of aggregate cubes one shared launch may take
+  // Functional dependencies between dimension columns checked for cube
+  // layouts, by "A|B|buffers|rows|ranges": whether B determines A, and the
+  // device table from B's value offset to A's.
+  struct Fd { bool holds = false; int* tab = nullptr; };
+  std::map<std::string, Fd> fds;
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t gexec = nullptr;
   std::vector<unsigned char> gsig;
@@ -467,7 +473,85 @@ struct CubePlan {
   std::vector<int> smem_off;
   uint64_t smem_words = 0, gbytes = 0;
   int chunks = 1;
+  std::vector<std::vector<int>> fdsrc;   // per shape and attribute position: source position, -1 none
+  std::vector<const int*> fdtab;          // per attribute: its table from the source's value offset
 };
+
+// Cache key of "column B of a dimension determines column A" on a context:
+// both columns' names, buffers, the table's rows and the registered ranges.
+bool fd_key(const LaunchPlan& lp, const cx_exec_ctx* c, int a, int b, std::string* key, const int** pa,
+            const int** pb, long long* rows) {
+  const auto& A = lp.cattrs[a];
+  const auto& B = lp.cattrs[b];
+  auto ba = c->buffers.find(A.col), bb = c->buffers.find(B.col);
+  auto ra = c->ranges.find(A.col), rb = c->ranges.find(B.col);
+  if (ba == c->buffers.end() || bb == c->buffers.end() || ra == c->ranges.end() || rb == c->ranges.end()) return false;
+  int table = -1;
+  for (const auto& col : lp.cols)
+    if (col.name == A.col) table = col.table;
+  if (table < 0 || table >= (int)lp.tables.size()) return false;
+  auto rt = c->rows.find(lp.tables[table]);
+  if (rt == c->rows.end()) return false;
+  *pa = (const int*)ba->second.first;
+  *pb = (const int*)bb->second.first;
+  *rows = (long long)rt->second;
+  char buf[512];
+  snprintf(buf, sizeof buf, "%s|%s|%p|%p|%lld|%lld|%lld|%lld|%lld", A.col.c_str(), B.col.c_str(), (const void*)*pa,
+           (const void*)*pb, *rows, (long long)ra->second.first, (long long)ra->second.second,
+           (long long)rb->second.first, (long long)rb->second.second);
+  *key = buf;
+  return true;
+}
+
+// Checks, once per context and column pair, which cube attributes of one
+// dimension determine which others (on `s`, then waits for it).
+int ensure_cube_fds(const LaunchPlan& lp, cx_exec_ctx* c, cudaStream_t s) {
+  if (!lp.cube) return CX_OK;
+  struct Todo { std::string key; int* tab; };
+  std::vector<Todo> todo;
+  std::vector<std::tuple<const int*, const int*, long long, int, int, int>> args;
+  for (size_t a = 0; a < lp.cattrs.size(); ++a)
+    for (size_t b = 0; b < lp.cattrs.size(); ++b) {
+      if (a == b || lp.cattrs[a].dim < 0 || lp.cattrs[a].dim != lp.cattrs[b].dim) continue;
+      std::string key;
+      const int *pa = nullptr, *pb = nullptr;
+      long long rows = 0;
+      if (!fd_key(lp, c, (int)a, (int)b, &key, &pa, &pb, &rows) || c->fds.count(key)) continue;
+      const auto& ra = c->ranges.at(lp.cattrs[a].col);
+      const auto& rb = c->ranges.at(lp.cattrs[b].col);
+      const int64_t radix_b = rb.second - rb.first + 1;
+      if (radix_b <= 0 || radix_b > 65536 || ra.second - ra.first + 1 > 65536 || !pa || !pb) {
+        c->fds[key] = cx_exec_ctx::Fd{};
+        continue;
+      }
+      todo.push_back({key, nullptr});
+      args.emplace_back(pa, pb, rows, (int)ra.first, (int)rb.first, (int)radix_b);
+    }
+  if (todo.empty()) return CX_OK;
+  unsigned* flags = nullptr;
+  CX_CUDA(cudaMalloc(&flags, todo.size() * sizeof(unsigned)));
+  int rc = CX_OK;
+  if (cudaMemsetAsync(flags, 0, todo.size() * sizeof(unsigned), s) != cudaSuccess) rc = fail(CX_E_CUDA, "fd check: memset");
+  for (size_t i = 0; i < todo.size() && rc == CX_OK; ++i) {
+    const auto& t = args[i];
+    if (cudaMalloc(&todo[i].tab, (size_t)std::get<5>(t) * sizeof(int)) != cudaSuccess) { rc = fail(CX_E_CUDA, "fd check: cudaMalloc"); break; }
+    rc = cx_internal::fd_check_launch(std::get<0>(t), std::get<1>(t), std::get<2>(t), std::get<3>(t), std::get<4>(t),
+                                      std::get<5>(t), todo[i].tab, flags + i, s);
+  }
+  std::vector<unsigned> host(todo.size(), 1u);
+  if (rc == CX_OK && cudaMemcpyAsync(host.data(), flags, todo.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    rc = fail(CX_E_CUDA, "fd check: copy");
+  if (rc == CX_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(CX_E_CUDA, "fd check: sync");
+  cudaFree(flags);
+  for (size_t i = 0; i < todo.size(); ++i) {
+    cx_exec_ctx::Fd f;
+    f.holds = rc == CX_OK && host[i] == 0u && todo[i].tab;
+    if (f.holds) f.tab = todo[i].tab;
+    else if (todo[i].tab) cudaFree(todo[i].tab);
+    if (rc == CX_OK) c->fds[todo[i].key] = f;
+  }
+  return rc;
+}
 
 constexpr uint64_t kCubeMaxCells = 1ULL << 24;
 constexpr uint64_t kCubeMaxGlobalBytes = 8ULL << 30;
@@ -488,16 +572,49 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
     cp.lo.push_back((int)lo);
     cp.radix.push_back((int)(hi - lo + 1));
   }
+  // Dimension attributes determined by another attribute of their dimension
+  // (checked functional dependencies): the attribute with the most values is
+  // kept first, and an attribute that a kept one determines takes no part in
+  // the cells of a shape that also reads its source.
+  const int na = (int)lp.cattrs.size();
+  std::vector<int> src(na, -1), kept, by_radix(na);
+  cp.fdtab.assign(na, nullptr);
+  for (int a = 0; a < na; ++a) by_radix[a] = a;
+  std::stable_sort(by_radix.begin(), by_radix.end(), [&](int x, int y) { return cp.radix[x] > cp.radix[y]; });
+  for (int a : by_radix) {
+    if (lp.cattrs[a].dim >= 0)
+      for (int b : kept) {
+        if (lp.cattrs[b].dim != lp.cattrs[a].dim) continue;
+        std::string key;
+        const int *pa = nullptr, *pb = nullptr;
+        long long rows = 0;
+        if (!fd_key(lp, c, a, b, &key, &pa, &pb, &rows)) continue;
+        auto it = c->fds.find(key);
+        if (it == c->fds.end() || !it->second.holds) continue;
+        src[a] = b;
+        cp.fdtab[a] = it->second.tab;
+        break;
+      }
+    if (src[a] < 0) kept.push_back(a);
+  }
   cp.cells.assign(nshapes, 0);
   cp.goff.assign(nshapes, 0);
   cp.stride.assign(nshapes, std::vector<int>(CX_MAX_SATTRS, 0));
+  cp.fdsrc.assign(nshapes, std::vector<int>(CX_MAX_SATTRS, -1));
   cp.smem_off.assign(nshapes, -1);
   uint64_t g = 0, maxcells = 0;
   for (int s = 0; s < nshapes; ++s) {
     if (!used[s]) continue;
     const auto& sh = lp.cshapes[s];
+    for (size_t j = 0; j < sh.attrs.size(); ++j) {
+      const int b = src[sh.attrs[j]];
+      if (b < 0) continue;
+      for (size_t k = 0; k < sh.attrs.size(); ++k)
+        if (sh.attrs[k] == b) cp.fdsrc[s][j] = (int)k;
+    }
     uint64_t cells = 1;
     for (size_t j = sh.attrs.size(); j-- > 0;) {
+      if (cp.fdsrc[s][j] >= 0) continue;  // stride 0: the source attribute's offset decides it
       cp.stride[s][j] = (int)cells;
       cells *= (uint64_t)cp.radix[sh.attrs[j]];
       if (cells > kCubeMaxCells) { cp.why = "a shape's cube exceeds 16,777,216 cells"; return false; }
@@ -551,6 +668,10 @@ bool ctx_column_range(const cx_exec_ctx* c, const std::string& name, int64_t* lo
 uint64_t ctx_scratch_bytes(const cx_exec_ctx* c) { return c->own_scratch_bytes; }
 
 void ctx_set_cube_cap(cx_exec_ctx* c, uint64_t bytes) { c->cube_cap = bytes; }
+
+int ensure_cube_dependencies(const cx_module* m, cx_exec_ctx* c, cudaStream_t s) {
+  return m ? ensure_cube_fds(m->lp, c, s) : CX_OK;
+}
 
 int set_error(int code, const std::string& msg) { return fail(code, "%s", msg.c_str()); }
 
@@ -783,6 +904,8 @@ void cx_ctx_destroy(cx_exec_ctx* c) {
   if (c->host_stage) cudaFreeHost(c->host_stage);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  for (auto& kv : c->fds)
+    if (kv.second.tab) cudaFree(kv.second.tab);
   delete c;
 }
 
@@ -1144,6 +1267,10 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
   CubePlan cp;
   std::vector<int> qshapes(nq);
   for (int i = 0; i < nq; ++i) qshapes[i] = queries[i].shape;
+  if (lp.cube) {
+    const int frc = ensure_cube_fds(lp, c, stream);
+    if (frc) return frc;
+  }
   const bool cube = plan_cubes(lp, c, qshapes.data(), nq, cp);
   const int maxq = cube ? std::max(nq, 1) : std::max(1, std::min(lp.shared_maxq, 256));
   const int npass = (nq + maxq - 1) / maxq;
@@ -1292,8 +1419,12 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
     }
     if (cube) {
       for (size_t id = 0; id < cp.lo.size(); ++id) { a.cube_lo[id] = cp.lo[id]; a.cube_radix[id] = cp.radix[id]; }
+      for (size_t id = 0; id < cp.fdtab.size(); ++id) a.cube_fdtab[id] = cp.fdtab[id];
       for (int s = 0; s < nshapes && s < CX_MAX_SHAPES; ++s) {
-        for (int j = 0; j < CX_MAX_SATTRS; ++j) a.cube_stride[s * CX_MAX_SATTRS + j] = cp.stride[s][j];
+        for (int j = 0; j < CX_MAX_SATTRS; ++j) {
+          a.cube_stride[s * CX_MAX_SATTRS + j] = cp.stride[s][j];
+          a.cube_fdsrc[s * CX_MAX_SATTRS + j] = cp.fdsrc[s][j];
+        }
         a.cube_g[s] = cp.cells[s] ? (unsigned long long*)(scratch + cube_off + cp.goff[s]) : nullptr;
         a.cube_cells[s] = (long long)cp.cells[s];
         a.cube_smem[s] = cp.smem_off[s];

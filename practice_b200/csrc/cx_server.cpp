@@ -472,6 +472,7 @@ void scheduler(cx_server* s) {
             s->circ_idle.erase(s->circ_idle.begin());
           }
         }
+        cx_internal::ensure_cube_dependencies(s->universe, sl.ctx, sl.stream);
         while (!s->pending.empty() && (int)batch.size() < s->cfg.max_batch) {
           Request* r = s->pending.front();
           if (!in_universe(r)) break;

@@ -2421,7 +2421,10 @@ struct SharedGen {
       o << "      e" << di << "_[i] = make_int4(0, 0, 0, 0);\n";
       o << "      if (rel_[i] & " << joiners[di] << "u) {\n";
       o << "        const int h_ = cx_detail::pht_slot<int>(c_" << d.fk << "[i], " << d.len << ", " << d.keymin << ");\n";
-      o << "        if (h_ >= 0) e" << di << "_[i] = __ldg(&ci_" << lower(d.name) << "[h_]);\n";
+      // Entries of a small dimension stay in L1; a large dimension's entries
+      // bypass it (L2 only), so its random gathers do not evict the small ones.
+      const char* ld = d.len * 16 <= (1LL << 20) ? "__ldg" : "__ldcg";
+      o << "        if (h_ >= 0) e" << di << "_[i] = " << ld << "(&ci_" << lower(d.name) << "[h_]);\n";
       o << "      }\n";
     }
     o << "    }\n";

@@ -75,4 +75,20 @@ struct CxArgs {
   // to its own.
   int cube_fdsrc[CX_MAX_SHAPES * CX_MAX_SATTRS];
   const int* cube_fdtab[CX_MAX_CATTRS];
+  // Dimensions whose entries fit in shared memory as compact words (bit 0:
+  // a row has this key, then one bit per plan shape, then the attribute
+  // offsets), one word per key of the dimension's key range, indexed by
+  // key - range minimum (distinct keys, distinct words: no key check): per
+  // dimension the byte offset of its copy in shared memory (-1: int4 entries
+  // gathered from global memory), the bytes of one word (1, 2 or 4), the key
+  // range's minimum and size, the array the index kernel writes, and per
+  // attribute field its bit shift and mask.
+  int cube_dsm[CX_MAX_HTS];
+  int cube_desz[CX_MAX_HTS];
+  int cube_dbase[CX_MAX_HTS];
+  int cube_dlen[CX_MAX_HTS];
+  unsigned char* cube_dcomp[CX_MAX_HTS];
+  int cube_fsh[CX_MAX_HTS * 4];
+  int cube_fmk[CX_MAX_HTS * 4];
+  int cube_dsm_bytes;                          // shared-memory bytes of all compact dimension copies
 };

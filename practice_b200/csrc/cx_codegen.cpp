@@ -2313,6 +2313,19 @@ struct SharedGen {
     }
     o << "    if (atomicCAS(&ent[h].x, 0, k) != 0) { cx::raise(a.err, cx::ERR_DIM_COLLISION); continue; }\n";
     o << "    ent[h] = make_int4(k, (int)rel, (int)(f_[0] | (f_[1] << 16)), (int)(f_[2] | (f_[3] << 16)));\n";
+    // The compact word of a dimension kept in shared memory, at key - key range minimum.
+    o << "    if (a.cube_desz[" << di << "] > 0) {\n";
+    o << "      const long long o_ = (long long)k - a.cube_dbase[" << di << "];\n";
+    o << "      if (o_ >= 0 && o_ < a.cube_dlen[" << di << "]) {\n";
+    o << "        unsigned w_ = 1u | (rel << 1);\n";
+    o << "        #pragma unroll\n";
+    o << "        for (int j = 0; j < 4; ++j) w_ |= f_[j] << a.cube_fsh[" << di * 4 << " + j];\n";
+    o << "        unsigned char* cw_ = a.cube_dcomp[" << di << "];\n";
+    o << "        if (a.cube_desz[" << di << "] == 1) cw_[o_] = (unsigned char)w_;\n";
+    o << "        else if (a.cube_desz[" << di << "] == 2) ((unsigned short*)cw_)[o_] = (unsigned short)w_;\n";
+    o << "        else ((unsigned*)cw_)[o_] = w_;\n";
+    o << "      }\n";
+    o << "    }\n";
     o << "  }\n}\n\n";
   }
 
@@ -2322,23 +2335,34 @@ struct SharedGen {
   // then per such shape one cell update -- shared-memory cubes per CTA, merged
   // into the global cube at the end, or global atomics for large cubes.
   void emit_cube_scan() {
-    const int CTA = 256, IPT = std::max(1, std::min(4, tu.cube)), VW = IPT >= 4 ? 4 : IPT;
+    // One CTA per SM, so each SM holds one copy of the shared-memory cubes and
+    // dimension words: 1024 threads (64 registers) for one or two rows per
+    // lane, 512 (128 registers) for four.
+    const int IPT = std::max(1, std::min(4, tu.cube)), VW = IPT >= 4 ? 4 : IPT;
+    const int CTA = IPT >= 4 ? 512 : 1024;
     if (IPT == 3) throw PlanError("cube scans take 1, 2 or 4 rows per lane");
     const int NFC = (int)fcols.size();
     const unsigned long long fr_bytes = ((unsigned long long)NFC * FW * 4 + 15) & ~15ULL;
     const std::string kname = "CubeScan_" + fact;
-    meta << "kernel " << kname << " cubescan 0 " << CTA << " " << 32 * IPT << " " << fr_bytes << " 8\n";
+    meta << "kernel " << kname << " cubescan 0 " << CTA << " " << 32 * IPT << " " << fr_bytes << " 1\n";
     std::ostringstream& o = src;
-    // Registers per thread: 128 for four rows per lane, 64 for two, 48 for one
-    // (more resident warps to cover the dimension gathers' latency).
-    const int min_blocks = IPT >= 4 ? 2 : IPT == 2 ? 4 : 5;
-    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", " << min_blocks << ") " << kname << "(const CxArgs a) {\n";
+    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", 1) " << kname << "(const CxArgs a) {\n";
     o << "  constexpr int IPT = " << IPT << ", VW = " << VW << ", TROWS = " << 32 * IPT << ";\n";
     o << "  extern __shared__ __align__(16) unsigned char cx_smem[];\n";
     o << "  unsigned* s_fr = (unsigned*)cx_smem; (void)s_fr;\n";
-    o << "  unsigned long long* s_cube = (unsigned long long*)(cx_smem + " << fr_bytes << ");\n";
+    o << "  unsigned char* s_dim = cx_smem + " << fr_bytes << "; (void)s_dim;\n";
+    o << "  unsigned long long* s_cube = (unsigned long long*)(cx_smem + " << fr_bytes << " + a.cube_dsm_bytes);\n";
     o << "  const int lane = threadIdx.x & 31;\n";
     o << "  for (int w = threadIdx.x; w < a.cube_smem_words; w += " << CTA << ") s_cube[w] = 0ULL;\n";
+    // Compact dimension words into shared memory (16-byte copies; the arrays are padded to 16 bytes).
+    for (size_t di = 0; di < dims.size(); ++di) {
+      o << "  if (a.cube_dsm[" << di << "] >= 0) {\n";
+      o << "    const uint4* src_ = (const uint4*)a.cube_dcomp[" << di << "];\n";
+      o << "    uint4* dst_ = (uint4*)(s_dim + a.cube_dsm[" << di << "]);\n";
+      o << "    const int n16_ = (int)(((long long)a.cube_dlen[" << di << "] * a.cube_desz[" << di << "] + 15) / 16);\n";
+      o << "    for (int w = threadIdx.x; w < n16_; w += " << CTA << ") dst_[w] = src_[w];\n";
+      o << "  }\n";
+    }
     o << "  unsigned live = 0u;\n";
     for (size_t s = 0; s < shapes.size(); ++s) o << "  if (a.sq_num[" << s << "] > 0) live |= " << (1u << s) << "u;\n";
     // Filter tables: bit s of s_fr[k * FW + v] clears when no query of shape s
@@ -2409,17 +2433,41 @@ struct SharedGen {
       o << "      { const unsigned d_ = (unsigned)c_" << fcols[k] << "[i] - fb" << k << "; if (d_ < fw" << k << ") m &= s_fr[" << k * FW << " + d_]; }\n";
     o << "      rel_[i] = m;\n";
     o << "    }\n";
-    // Every dimension entry of every row in flight together.
     std::vector<unsigned> joiners(dims.size(), 0u);
     for (size_t s = 0; s < shapes.size(); ++s)
       for (const auto& kv : preds[s].joins) joiners[kv.first] |= 1u << s;
+    const unsigned all_shapes = (1u << shapes.size()) - 1u;
+    // Dimensions kept in shared memory first: their compact words cost no
+    // gather, and the shapes they rule out skip the other dimensions' gathers.
+    for (size_t di = 0; di < dims.size(); ++di) o << "    unsigned w" << di << "_[IPT];\n";
+    o << "    #pragma unroll\n";
+    o << "    for (int i = 0; i < IPT; ++i) {\n";
+    o << "      unsigned m = rel_[i];\n";
+    for (size_t di = 0; di < dims.size(); ++di) {
+      const Dim& d = dims[di];
+      o << "      w" << di << "_[i] = 0u;\n";
+      o << "      if (a.cube_dsm[" << di << "] >= 0) {\n";
+      o << "        if (m & " << joiners[di] << "u) {\n";
+      o << "          const long long o_ = (long long)c_" << d.fk << "[i] - a.cube_dbase[" << di << "];\n";
+      o << "          if (o_ >= 0 && o_ < a.cube_dlen[" << di << "]) {\n";
+      o << "            const unsigned char* sd_ = s_dim + a.cube_dsm[" << di << "];\n";
+      o << "            const int es_ = a.cube_desz[" << di << "];\n";
+      o << "            w" << di << "_[i] = es_ == 1 ? (unsigned)sd_[o_] : es_ == 2 ? (unsigned)((const unsigned short*)sd_)[o_] : ((const unsigned*)sd_)[o_];\n";
+      o << "          }\n";
+      o << "        }\n";
+      o << "        m &= (w" << di << "_[i] & 1u) ? (w" << di << "_[i] >> 1) : " << (~joiners[di] & all_shapes) << "u;\n";
+      o << "      }\n";
+    }
+    o << "      rel_[i] = m;\n";
+    o << "    }\n";
+    // The other dimensions' int4 entries: every gather of the tile's rows in flight together.
     for (size_t di = 0; di < dims.size(); ++di) o << "    int4 e" << di << "_[IPT];\n";
     o << "    #pragma unroll\n";
     o << "    for (int i = 0; i < IPT; ++i) {\n";
     for (size_t di = 0; di < dims.size(); ++di) {
       const Dim& d = dims[di];
       o << "      e" << di << "_[i] = make_int4(0, 0, 0, 0);\n";
-      o << "      if (rel_[i] & " << joiners[di] << "u) {\n";
+      o << "      if (a.cube_dsm[" << di << "] < 0 && (rel_[i] & " << joiners[di] << "u)) {\n";
       o << "        const int h_ = cx_detail::pht_slot<int>(c_" << d.fk << "[i], " << d.len << ", " << d.keymin << ");\n";
       // Entries of a small dimension stay in L1; a large dimension's entries
       // bypass it (L2 only), so its random gathers do not evict the small ones.
@@ -2433,9 +2481,11 @@ struct SharedGen {
     o << "      unsigned m = rel_[i];\n";
     for (size_t di = 0; di < dims.size(); ++di) {
       const Dim& d = dims[di];
-      o << "      { const int4 g_ = e" << di << "_[i];\n";
+      o << "      if (a.cube_dsm[" << di << "] < 0) {\n";
+      o << "        const int4 g_ = e" << di << "_[i];\n";
       o << "        const bool hit_ = g_.x != 0 && g_.x == c_" << d.fk << "[i];\n";
-      o << "        m &= hit_ ? (unsigned)g_.y : " << (~joiners[di] & ((1u << shapes.size()) - 1u)) << "u; }\n";
+      o << "        m &= hit_ ? (unsigned)g_.y : " << (~joiners[di] & all_shapes) << "u;\n";
+      o << "      }\n";
     }
     o << "      if (m == 0u) continue;\n";
     const char* fld[4] = {"((unsigned)g_.z & 0xFFFFu)", "((unsigned)g_.z >> 16)", "((unsigned)g_.w & 0xFFFFu)", "((unsigned)g_.w >> 16)"};
@@ -2456,7 +2506,11 @@ struct SharedGen {
           o << "          in_ = in_ && x_ < (unsigned)a.cube_radix[" << id << "];\n";
           o << "          cell_ += x_ * " << stride << "; }\n";
         } else {
-          o << "        { const int4 g_ = e" << at.dim << "_[i]; cell_ += " << fld[at.field] << " * " << stride << "; }\n";
+          const std::string fi = std::to_string(at.dim * 4 + at.field);
+          o << "        { const int4 g_ = e" << at.dim << "_[i];\n";
+          o << "          const unsigned f_ = a.cube_dsm[" << at.dim << "] >= 0 ? ((w" << at.dim << "_[i] >> a.cube_fsh[" << fi
+            << "]) & (unsigned)a.cube_fmk[" << fi << "]) : " << fld[at.field] << ";\n";
+          o << "          cell_ += f_ * " << stride << "; }\n";
         }
       }
       o << "        if (!in_) {\n";
@@ -2649,6 +2703,9 @@ struct SharedGen {
         for (int id : sh_attrs[s]) meta << " " << id;
         meta << "\n";
       }
+      for (size_t di = 0; di < dims.size(); ++di)
+        meta << "cdim " << di << " " << dims[di].table << " " << dims[di].len << " " << dims[di].keymin << " d_"
+             << dims[di].fk << " d_" << dims[di].pk << "\n";
     }
     emit_zero();
     for (size_t di = 0; di < dims.size(); ++di) emit_index(dims[di], (int)di);

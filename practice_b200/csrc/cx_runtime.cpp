@@ -143,6 +143,8 @@ struct LaunchPlan {
   std::vector<CAttr> cattrs;
   struct CShape { int nsums = 0; std::vector<int> attrs; };
   std::vector<CShape> cshapes;
+  struct CDim { int table = 0; long long len = 0, keymin = 0; std::string fk, pk; };
+  std::vector<CDim> cdims;
 };
 
 bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err) {
@@ -242,6 +244,12 @@ bool parse_launch_plan(const std::string& src, LaunchPlan& lp, std::string& err)
         cs.attrs.push_back(id);
       }
       lp.cshapes.push_back(cs);
+    } else if (k == "cdim") {
+      int i = 0;
+      LaunchPlan::CDim cd;
+      ls >> i >> cd.table >> cd.len >> cd.keymin >> cd.fk >> cd.pk;
+      if (i != (int)lp.cdims.size() || i >= CX_MAX_HTS || cd.len <= 0) { err = "cube dimension lines out of order or out of range"; return false; }
+      lp.cdims.push_back(cd);
     } else if (k == "mht") {
       int sl = 0, t = 0, na = 1;
       ls >> sl >> t;
@@ -475,6 +483,12 @@ struct CubePlan {
   int chunks = 1;
   std::vector<std::vector<int>> fdsrc;   // per shape and attribute position: source position, -1 none
   std::vector<const int*> fdtab;          // per attribute: its table from the source's value offset
+  // Dimensions kept in shared memory as compact words: byte offset (-1: none),
+  // bytes per word, per field bit shift and mask, scratch offset and size of
+  // the array the index kernel writes.
+  std::vector<int> dsm, desz, dbase, dlen, fsh, fmk;
+  std::vector<uint64_t> dcomp_off, dcomp_bytes;
+  uint64_t dsm_bytes = 0;
 };
 
 // Cache key of "column B of a dimension determines column A" on a context:
@@ -557,6 +571,7 @@ constexpr uint64_t kCubeMaxCells = 1ULL << 24;
 constexpr uint64_t kCubeMaxGlobalBytes = 8ULL << 30;
 constexpr uint64_t kCubeSmemBudget = 96 * 1024;
 constexpr uint64_t kCubeCellsPerChunk = 16384;
+constexpr uint64_t kDimSmemBudget = 96 * 1024;
 
 bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, int nq, CubePlan& cp) {
   const int nshapes = (int)lp.sshapes.size();
@@ -641,6 +656,54 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
   }
   cp.smem_words = words;
   cp.chunks = (int)std::max<uint64_t>(1, std::min<uint64_t>(4096, (maxcells + kCubeCellsPerChunk - 1) / kCubeCellsPerChunk));
+  // Dimensions whose compact words (present bit, one bit per shape, the
+  // attribute offsets) fit in 32 bits and whose key ranges, one word per key,
+  // fit the budget together.
+  const int nd = (int)lp.cdims.size();
+  cp.dsm.assign(CX_MAX_HTS, -1);
+  cp.desz.assign(CX_MAX_HTS, 0);
+  cp.dbase.assign(CX_MAX_HTS, 0);
+  cp.dlen.assign(CX_MAX_HTS, 0);
+  cp.fsh.assign(CX_MAX_HTS * 4, 0);
+  cp.fmk.assign(CX_MAX_HTS * 4, 0);
+  cp.dcomp_off.assign(CX_MAX_HTS, 0);
+  cp.dcomp_bytes.assign(CX_MAX_HTS, 0);
+  std::vector<std::pair<uint64_t, int>> cand;
+  for (int d = 0; d < nd && d < CX_MAX_HTS; ++d) {
+    const auto& cd = lp.cdims[d];
+    auto rp = c->ranges.find(cd.pk);
+    if (rp == c->ranges.end()) continue;
+    const int64_t klo = rp->second.first, kn = rp->second.second - rp->second.first + 1;
+    if (klo < INT32_MIN || rp->second.second > INT32_MAX || kn <= 0 || kn > (int64_t)(kDimSmemBudget)) continue;
+    int bits = 1 + nshapes;
+    int fw[4] = {0, 0, 0, 0};
+    for (size_t a = 0; a < lp.cattrs.size(); ++a) {
+      if (lp.cattrs[a].dim != d) continue;
+      int w = 1;
+      while ((1LL << w) < (long long)cp.radix[a]) ++w;
+      fw[lp.cattrs[a].field] = w;
+    }
+    for (int f = 0; f < 4; ++f) {
+      if (!fw[f]) continue;
+      cp.fsh[d * 4 + f] = bits;
+      cp.fmk[d * 4 + f] = (int)((1u << fw[f]) - 1u);
+      bits += fw[f];
+    }
+    if (bits > 32) continue;
+    cp.desz[d] = bits <= 8 ? 1 : bits <= 16 ? 2 : 4;
+    cp.dbase[d] = (int)klo;
+    cp.dlen[d] = (int)kn;
+    cp.dcomp_bytes[d] = ((uint64_t)kn * (uint64_t)cp.desz[d] + 15) & ~15ULL;
+    cand.emplace_back(cp.dcomp_bytes[d], d);
+  }
+  std::sort(cand.begin(), cand.end());
+  uint64_t dbytes = 0;
+  for (const auto& cd : cand) {
+    if (dbytes + cd.first > kDimSmemBudget) { cp.desz[cd.second] = 0; cp.dcomp_bytes[cd.second] = 0; continue; }
+    cp.dsm[cd.second] = (int)dbytes;
+    dbytes += cd.first;
+  }
+  cp.dsm_bytes = dbytes;
   cp.on = true;
   return true;
 }
@@ -725,7 +788,10 @@ uint64_t shared_scratch_need(const cx_module* m, const cx_exec_ctx* c, const int
     const auto& sh = lp.sshapes[shapes[i]];
     if (sh.grouped) off = align256(off + ((sh.groups + 31) / 32) * 4);
   }
-  if (cube) off = align256(off + cp.gbytes);
+  if (cube) {
+    off = align256(off + cp.gbytes);
+    for (int d = 0; d < CX_MAX_HTS; ++d) off = align256(off + cp.dcomp_bytes[d]);
+  }
   const int maxq = cube ? std::max(nq, 1) : std::max(1, std::min(lp.shared_maxq, 256));
   const int npass = (nq + maxq - 1) / maxq;
   int maxp = lp.shared_maxp;
@@ -1295,6 +1361,9 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
     dat_off.push_back(off);
     if (it != lp.dat_words.end()) off = align256(off + it->second * 4);
   }
+  if (cube)
+    for (int d = 0; d < CX_MAX_HTS; ++d)
+      if (cp.dcomp_bytes[d]) { cp.dcomp_off[d] = off; off = align256(off + cp.dcomp_bytes[d]); }
   const uint64_t dim_end = off;
   std::vector<uint64_t> touch_off(nq, 0);
   for (int i = 0; i < nq; ++i) {
@@ -1431,12 +1500,21 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
       }
       a.cube_smem_words = (int)cp.smem_words;
       a.cube_chunks = cp.chunks;
+      for (int d = 0; d < CX_MAX_HTS; ++d) {
+        a.cube_dsm[d] = cp.dsm[d];
+        a.cube_desz[d] = cp.desz[d];
+        a.cube_dbase[d] = cp.dbase[d];
+        a.cube_dlen[d] = cp.dlen[d];
+        a.cube_dcomp[d] = cp.dcomp_bytes[d] ? (unsigned char*)(scratch + cp.dcomp_off[d]) : nullptr;
+        for (int f = 0; f < 4; ++f) { a.cube_fsh[d * 4 + f] = cp.fsh[d * 4 + f]; a.cube_fmk[d * 4 + f] = cp.fmk[d * 4 + f]; }
+      }
+      a.cube_dsm_bytes = (int)cp.dsm_bytes;
     }
     P.args = a;
     P.qn = qn;
     P.nparams = poff;
     P.hstage = hstage;
-    P.extra_smem = cube ? (size_t)cp.smem_words * 8 : qb_bytes + (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
+    P.extra_smem = cube ? (size_t)cp.dsm_bytes + (size_t)cp.smem_words * 8 : qb_bytes + (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
     int occ = 1;
     CUresult orr = d.Occupancy(&occ, L->fns[scan_ki], sk.block, sk.smem + P.extra_smem);
     if (orr != CUDA_SUCCESS) return drv_fail(orr, "cuOccupancyMaxActiveBlocksPerMultiprocessor");

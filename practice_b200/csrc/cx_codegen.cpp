@@ -23,6 +23,8 @@
 #include <functional>
 #include <map>
 #include <set>
+#include <cstring>
+#include <cctype>
 #include <sstream>
 
 namespace cx {
@@ -2345,7 +2347,7 @@ struct SharedGen {
     const unsigned long long fr_bytes = ((unsigned long long)NFC * FW * 4 + 15) & ~15ULL;
     const std::string kname = "CubeScan_" + fact;
     meta << "kernel " << kname << " cubescan 0 " << CTA << " " << 32 * IPT << " " << fr_bytes << " 1\n";
-    std::ostringstream& o = src;
+    std::ostringstream o;
     o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", 1) " << kname << "(const CxArgs a) {\n";
     o << "  constexpr int IPT = " << IPT << ", VW = " << VW << ", TROWS = " << 32 * IPT << ";\n";
     o << "  extern __shared__ __align__(16) unsigned char cx_smem[];\n";
@@ -2567,6 +2569,51 @@ struct SharedGen {
       o << "  }\n";
     }
     o << "}\n\n";
+    // The batch's cube layout (dimension words, strides, cube offsets and
+    // sizes, attribute ranges) is read through CXS_* macros: by default the
+    // kernel arguments, while the runtime recompiles this region once per
+    // layout with the values as constants (-DCXS_SPEC), which folds the
+    // layout's branches and multiplications away.
+    std::string body = o.str();
+    static const std::pair<const char*, const char*> hooks[] = {
+        {"a.cube_dsm_bytes", "CXS_DSMB"}, {"a.cube_dsm[", "CXS_DSM"}, {"a.cube_desz[", "CXS_DESZ"},
+        {"a.cube_dbase[", "CXS_DBASE"}, {"a.cube_dlen[", "CXS_DLEN"}, {"a.cube_fsh[", "CXS_FSH"},
+        {"a.cube_fmk[", "CXS_FMK"}, {"a.cube_stride[", "CXS_STRIDE"}, {"a.cube_smem[", "CXS_SMEM"},
+        {"a.cube_cells[", "CXS_CELLS"}, {"a.cube_lo[", "CXS_LO"}, {"a.cube_radix[", "CXS_RADIX"},
+        {"a.cube_smem_words", "CXS_SMEMW"}};
+    std::set<std::string> used;
+    std::string out;
+    for (size_t i = 0; i < body.size();) {
+      bool hit = false;
+      for (const auto& h : hooks) {
+        const size_t n = strlen(h.first);
+        if (body.compare(i, n, h.first) != 0) continue;
+        if (h.first[n - 1] == '[') {
+          const size_t close = body.find(']', i + n);
+          const std::string idx = body.substr(i + n, close - i - n);
+          bool digits = !idx.empty();
+          for (char ch : idx) digits = digits && isdigit((unsigned char)ch);
+          if (!digits) continue;  // a run-time index stays an argument read
+          const std::string name = std::string(h.second) + "_" + idx;
+          used.insert(std::string(h.first) + idx + "]|" + name);
+          out += name;
+          i = close + 1;
+        } else {
+          used.insert(std::string(h.first) + "|" + h.second);
+          out += h.second;
+          i += n;
+        }
+        hit = true;
+        break;
+      }
+      if (!hit) out += body[i++];
+    }
+    src << "//@cx-cube-begin\n#ifndef CXS_SPEC\n";
+    for (const auto& u : used) {
+      const size_t bar = u.find('|');
+      src << "#define " << u.substr(bar + 1) << " (" << u.substr(0, bar) << ")\n";
+    }
+    src << "#endif\n" << out << "//@cx-cube-end\n";
   }
 
   // Per query: the cells of its shape's cube that its predicates accept, added
@@ -2726,7 +2773,8 @@ struct SharedGen {
     out << "#include \"cx_args.h\"\n#include \"crystal_sm100.cuh\"\n\n";
     out << "template <typename A, typename B>\n"
            "__device__ __forceinline__ auto cx_mdiv(A x, B y) -> decltype(x / y) {\n"
-           "  return (y == 0) ? (decltype(x / y))0 : x / y;\n}\n\n";
+           "  return (y == 0) ? (decltype(x / y))0 : x / y;\n}\n";
+    out << "//@cx-prelude-end\n\n";
     out << src.str();
     return out.str();
   }

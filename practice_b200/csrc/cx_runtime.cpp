@@ -380,6 +380,11 @@ struct cx_module {
     std::vector<int> occupancy;  // scan kernels: CTAs per SM at their smem size
   };
   std::map<int, Loaded> per_device;
+  // Shared programs with a cube path: the source, and the cube scan compiled
+  // once per cube layout with the layout as constants, per layout and device.
+  std::string source;
+  struct Spec { CUmodule mod = nullptr; CUfunction fn = nullptr; bool failed = false; };
+  std::map<std::string, std::map<int, Spec>> cube_specs;
 };
 
 struct cx_exec_ctx {
@@ -457,6 +462,95 @@ int load_on_device(cx_module* m, int dev, cx_module::Loaded** out) {
   return CX_OK;
 }
 
+// The cube scan of a shared program compiled with one batch layout as
+// constants: the program's prelude, `#define`s of the CXS_* layout macros
+// (values from the batch's arguments) and the program's cube region.  Cached
+// per layout and device; *fn stays null (the generic kernel runs) if the
+// program has no cube region or the compile fails.
+int cube_spec_function(cx_module* m, int dev, const CxArgs& a, const std::string& kname, size_t smem_max, CUfunction* fn) {
+  *fn = nullptr;
+  const std::string& src = m->source;
+  const size_t p0 = src.find("@*/"), p1 = src.find("//@cx-prelude-end");
+  const size_t r0 = src.find("//@cx-cube-begin"), r1 = src.find("//@cx-cube-end");
+  if (p0 == std::string::npos || p1 == std::string::npos || r0 == std::string::npos || r1 == std::string::npos) return CX_OK;
+  std::string region = src.substr(r0, r1 - r0);
+  // Default lines: "#define NAME (a.field[idx])" or "#define NAME (a.field)".
+  std::string defs = "#define CXS_SPEC 1\n";
+  std::istringstream in(region);
+  std::string line;
+  auto value = [&](const std::string& f, int i, bool* ok) -> long long {
+    *ok = true;
+    auto in_range = [&](int n) { if (i < 0 || i >= n) *ok = false; return *ok; };
+    if (f == "cube_dsm_bytes") return a.cube_dsm_bytes;
+    if (f == "cube_smem_words") return a.cube_smem_words;
+    if (f == "cube_dsm" && in_range(CX_MAX_HTS)) return a.cube_dsm[i];
+    if (f == "cube_desz" && in_range(CX_MAX_HTS)) return a.cube_desz[i];
+    if (f == "cube_dbase" && in_range(CX_MAX_HTS)) return a.cube_dbase[i];
+    if (f == "cube_dlen" && in_range(CX_MAX_HTS)) return a.cube_dlen[i];
+    if (f == "cube_fsh" && in_range(CX_MAX_HTS * 4)) return a.cube_fsh[i];
+    if (f == "cube_fmk" && in_range(CX_MAX_HTS * 4)) return a.cube_fmk[i];
+    if (f == "cube_stride" && in_range(CX_MAX_SHAPES * CX_MAX_SATTRS)) return a.cube_stride[i];
+    if (f == "cube_smem" && in_range(CX_MAX_SHAPES)) return a.cube_smem[i];
+    if (f == "cube_cells" && in_range(CX_MAX_SHAPES)) return a.cube_cells[i];
+    if (f == "cube_lo" && in_range(CX_MAX_CATTRS)) return a.cube_lo[i];
+    if (f == "cube_radix" && in_range(CX_MAX_CATTRS)) return a.cube_radix[i];
+    *ok = false;
+    return 0;
+  };
+  while (std::getline(in, line)) {
+    if (line.rfind("#define CXS_", 0) != 0) continue;
+    std::istringstream ls(line);
+    std::string def, name, expr;
+    ls >> def >> name >> expr;
+    // expr: "(a.field[idx])" or "(a.field)"
+    if (expr.size() < 5 || expr.compare(0, 3, "(a.") != 0) return CX_OK;
+    std::string body = expr.substr(3, expr.size() - 4);
+    int idx = -1;
+    const size_t lb = body.find('[');
+    if (lb != std::string::npos) {
+      idx = atoi(body.c_str() + lb + 1);
+      body = body.substr(0, lb);
+    }
+    bool ok = false;
+    const long long v = value(body, idx, &ok);
+    if (!ok) return CX_OK;
+    defs += "#define " + name + " (" + std::to_string(v) + (body == "cube_cells" ? "LL" : "") + ")\n";
+  }
+  std::lock_guard<std::mutex> lk(m->mu);
+  cx_module::Spec& sp = m->cube_specs[defs][dev];
+  if (sp.fn || sp.failed) { *fn = sp.fn; return CX_OK; }
+  const std::string prog_src = src.substr(p0 + 3, p1 - p0 - 3) + "\n" + defs + region;
+  nvrtcProgram prog;
+  const char* headers[] = {kCxEmbeddedCrystalHeader, kCxEmbeddedArgsHeader};
+  const char* names[] = {"crystal_sm100.cuh", "cx_args.h"};
+  sp.failed = true;
+  if (nvrtcCreateProgram(&prog, prog_src.c_str(), "cx_cube_layout.cu", 2, headers, names) != NVRTC_SUCCESS) return CX_OK;
+  const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-default-device"};
+  const bool compiled = nvrtcCompileProgram(prog, 4, opts) == NVRTC_SUCCESS;
+  std::vector<char> cubin;
+  if (compiled) {
+    size_t csz = 0;
+    nvrtcGetCUBINSize(prog, &csz);
+    cubin.resize(csz);
+    nvrtcGetCUBIN(prog, cubin.data());
+  }
+  nvrtcDestroyProgram(&prog);
+  if (!compiled) return CX_OK;
+  Driver& d = driver();
+  if (d.ModuleLoadData(&sp.mod, cubin.data()) != CUDA_SUCCESS) { sp.mod = nullptr; return CX_OK; }
+  CUfunction f = nullptr;
+  if (d.ModuleGetFunction(&f, sp.mod, kname.c_str()) != CUDA_SUCCESS ||
+      d.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem_max) != CUDA_SUCCESS) {
+    d.ModuleUnload(sp.mod);
+    sp.mod = nullptr;
+    return CX_OK;
+  }
+  sp.fn = f;
+  sp.failed = false;
+  *fn = f;
+  return CX_OK;
+}
+
 int ensure_ctx_device(cx_exec_ctx* c, int dev) {
   if (c->device == dev && c->ev[0]) return CX_OK;
   if (c->ev[0]) {
@@ -487,6 +581,7 @@ struct CubePlan {
   // bytes per word, per field bit shift and mask, scratch offset and size of
   // the array the index kernel writes.
   std::vector<int> dsm, desz, dbase, dlen, fsh, fmk;
+  std::vector<char> used;                 // per shape: the batch has queries of it
   std::vector<uint64_t> dcomp_off, dcomp_bytes;
   uint64_t dsm_bytes = 0;
 };
@@ -576,7 +671,8 @@ constexpr uint64_t kDimSmemBudget = 96 * 1024;
 bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, int nq, CubePlan& cp) {
   const int nshapes = (int)lp.sshapes.size();
   if (!lp.cube || (int)lp.cshapes.size() != nshapes) { cp.why = "program has no cube path"; return false; }
-  std::vector<char> used(nshapes, 0);
+  std::vector<char>& used = cp.used;
+  used.assign(nshapes, 0);
   for (int q = 0; q < nq; ++q)
     if (shapes[q] >= 0 && shapes[q] < nshapes) used[shapes[q]] = 1;
   for (const auto& at : lp.cattrs) {
@@ -617,9 +713,11 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
   cp.stride.assign(nshapes, std::vector<int>(CX_MAX_SATTRS, 0));
   cp.fdsrc.assign(nshapes, std::vector<int>(CX_MAX_SATTRS, -1));
   cp.smem_off.assign(nshapes, -1);
+  // Every shape's cells and strides, used by the batch or not, so that the
+  // layout (and the scan compiled for it) stays the same from batch to batch;
+  // global cubes only for the shapes the batch uses.
   uint64_t g = 0, maxcells = 0;
   for (int s = 0; s < nshapes; ++s) {
-    if (!used[s]) continue;
     const auto& sh = lp.cshapes[s];
     for (size_t j = 0; j < sh.attrs.size(); ++j) {
       const int b = src[sh.attrs[j]];
@@ -628,13 +726,18 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
         if (sh.attrs[k] == b) cp.fdsrc[s][j] = (int)k;
     }
     uint64_t cells = 1;
-    for (size_t j = sh.attrs.size(); j-- > 0;) {
+    for (size_t j = sh.attrs.size(); j-- > 0 && cells <= kCubeMaxCells;) {
       if (cp.fdsrc[s][j] >= 0) continue;  // stride 0: the source attribute's offset decides it
       cp.stride[s][j] = (int)cells;
       cells *= (uint64_t)cp.radix[sh.attrs[j]];
-      if (cells > kCubeMaxCells) { cp.why = "a shape's cube exceeds 16,777,216 cells"; return false; }
+    }
+    if (cells > kCubeMaxCells) {
+      if (used[s]) { cp.why = "a shape's cube exceeds 16,777,216 cells"; return false; }
+      std::fill(cp.stride[s].begin(), cp.stride[s].end(), 0);
+      continue;  // cells 0: never placed, never updated (no query of the shape)
     }
     cp.cells[s] = cells;
+    if (!used[s]) continue;
     cp.goff[s] = g;
     g = align256(g + cells * (uint64_t)(sh.nsums + 1) * 8);
     maxcells = std::max(maxcells, cells);
@@ -644,7 +747,7 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
   // Shared-memory copies for the smallest cubes first, within the per-CTA budget.
   std::vector<int> order;
   for (int s = 0; s < nshapes; ++s)
-    if (used[s]) order.push_back(s);
+    if (cp.cells[s]) order.push_back(s);
   std::sort(order.begin(), order.end(), [&](int x, int y) { return cp.cells[x] < cp.cells[y]; });
   uint64_t words = 0;
   for (int s : order) {
@@ -887,6 +990,7 @@ int cx_compile(const char* src, size_t src_len, const char* key, cx_module** out
   std::string perr;
   if (!parse_launch_plan(source, m->lp, perr)) return fail(CX_E_INVALID, "cx_compile: %s", perr.c_str());
   m->sl = scratch_layout(m->lp);
+  if (m->lp.cube) m->source = source;
 
   nvrtcProgram prog;
   const char* headers[] = {kCxEmbeddedCrystalHeader, kCxEmbeddedArgsHeader};
@@ -923,6 +1027,9 @@ int cx_compile(const char* src, size_t src_len, const char* key, cx_module** out
       cx_module* old = it->second;
       for (auto& kv : old->per_device)
         if (kv.second.mod && driver().ok) driver().ModuleUnload(kv.second.mod);
+      for (auto& sp : old->cube_specs)
+        for (auto& kv : sp.second)
+          if (kv.second.mod && driver().ok) driver().ModuleUnload(kv.second.mod);
       delete old;
     }
     g_cache.erase(it);
@@ -939,6 +1046,9 @@ int cx_module_release(cx_module* m) {
   if (m->refs.fetch_sub(1) == 1) {
     for (auto& kv : m->per_device)
       if (kv.second.mod && driver().ok) driver().ModuleUnload(kv.second.mod);
+    for (auto& sp : m->cube_specs)
+      for (auto& kv : sp.second)
+        if (kv.second.mod && driver().ok) driver().ModuleUnload(kv.second.mod);
     delete m;
   }
   return CX_OK;
@@ -1442,6 +1552,7 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
     size_t extra_smem = 0;
     unsigned scan_grid = 0;
     char* hstage = nullptr;
+    CUfunction scan_fn = nullptr;  // the generic scan kernel, or its build for the batch's cube layout
   };
   std::vector<Pass> passes(npass);
   for (int ps = 0; ps < npass; ++ps) {
@@ -1494,7 +1605,7 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
           a.cube_stride[s * CX_MAX_SATTRS + j] = cp.stride[s][j];
           a.cube_fdsrc[s * CX_MAX_SATTRS + j] = cp.fdsrc[s][j];
         }
-        a.cube_g[s] = cp.cells[s] ? (unsigned long long*)(scratch + cube_off + cp.goff[s]) : nullptr;
+        a.cube_g[s] = cp.used[s] && cp.cells[s] ? (unsigned long long*)(scratch + cube_off + cp.goff[s]) : nullptr;
         a.cube_cells[s] = (long long)cp.cells[s];
         a.cube_smem[s] = cp.smem_off[s];
       }
@@ -1515,8 +1626,14 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
     P.nparams = poff;
     P.hstage = hstage;
     P.extra_smem = cube ? (size_t)cp.dsm_bytes + (size_t)cp.smem_words * 8 : qb_bytes + (size_t)tab_words * 8 + (size_t)bit_words * 4 + 16;
+    P.scan_fn = L->fns[scan_ki];
+    if (cube) {
+      CUfunction spec = nullptr;
+      cube_spec_function(m, dev, P.args, sk.name, 227 * 1024, &spec);
+      if (spec) P.scan_fn = spec;
+    }
     int occ = 1;
-    CUresult orr = d.Occupancy(&occ, L->fns[scan_ki], sk.block, sk.smem + P.extra_smem);
+    CUresult orr = d.Occupancy(&occ, P.scan_fn, sk.block, sk.smem + P.extra_smem);
     if (orr != CUDA_SUCCESS) return drv_fail(orr, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
     if (occ < 1) return fail(CX_E_CAPACITY, "cx_shared_execute: shared scan cannot be resident with %zu bytes of shared memory", sk.smem + P.extra_smem);
     const long long tiles = (rows[0] + sk.tile - 1) / sk.tile;
@@ -1534,11 +1651,11 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
     auto rec = [&](cudaEvent_t e) {
       return capturing ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal) : cudaEventRecord(e, s);
     };
-    auto launch = [&](size_t ki, unsigned grid, size_t extra, CxArgs* args) -> int {
+    auto launch = [&](size_t ki, unsigned grid, size_t extra, CxArgs* args, CUfunction fn = nullptr) -> int {
       const KernelSpec& k = lp.kernels[ki];
       if (grid == 0) return CX_OK;
       void* kp[] = {args};
-      CUresult r = d.LaunchKernel(L->fns[ki], grid, 1, 1, k.block, 1, 1, (unsigned)(k.smem + extra), (CUstream)s, kp, nullptr);
+      CUresult r = d.LaunchKernel(fn ? fn : L->fns[ki], grid, 1, 1, k.block, 1, 1, (unsigned)(k.smem + extra), (CUstream)s, kp, nullptr);
       if (r != CUDA_SUCCESS) return drv_fail(r, k.name.c_str());
       ++launches;
       return CX_OK;
@@ -1565,7 +1682,7 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
         if (r) return r;
       }
       if (ps == 0) CX_CUDA(rec(c->ev[1]));
-      int r = launch(scan_ki, P.scan_grid, P.extra_smem, &P.args);
+      int r = launch(scan_ki, P.scan_grid, P.extra_smem, &P.args, P.scan_fn);
       if (r) return r;
       if (ps == npass - 1) CX_CUDA(rec(c->ev[2]));
       for (size_t ki = scan_ki + 1; ki < lp.kernels.size(); ++ki) {

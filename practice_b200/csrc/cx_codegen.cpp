@@ -2538,12 +2538,17 @@ struct SharedGen {
         o << "              if (hi_) atomicAdd(&cs_[" << 2 * k + 1 << "u * nc_ + cell_], hi_);\n";
         o << "            }\n";
       }
-      o << "            atomicAdd(&cs_[" << 2 * NS << "u * nc_ + cell_], 1u);\n";
+      // A shape without COUNT aggregates needs only whether a cell has rows:
+      // a plain store of 1 instead of an atomic count.
+      const bool counts = (int)p.aggs.size() > NS;
+      if (counts) o << "            atomicAdd(&cs_[" << 2 * NS << "u * nc_ + cell_], 1u);\n";
+      else o << "            cs_[" << 2 * NS << "u * nc_ + cell_] = 1u;\n";
       o << "          } else {\n";
       o << "            unsigned long long* cg_ = a.cube_g[" << s << "];\n";
       o << "            const unsigned long long nc_ = (unsigned long long)a.cube_cells[" << s << "];\n";
       for (int k = 0; k < NS; ++k) o << "            if (x" << k << "_) atomicAdd(&cg_[" << k << "ULL * nc_ + cell_], x" << k << "_);\n";
-      o << "            atomicAdd(&cg_[" << NS << "ULL * nc_ + cell_], 1ULL);\n";
+      if (counts) o << "            atomicAdd(&cg_[" << NS << "ULL * nc_ + cell_], 1ULL);\n";
+      else o << "            cg_[" << NS << "ULL * nc_ + cell_] = 1ULL;\n";
       o << "          }\n";
       o << "        }\n";
       o << "      }\n";
@@ -2561,7 +2566,8 @@ struct SharedGen {
       o << "    for (unsigned c = threadIdx.x; c < nc_; c += " << CTA << ") {\n";
       o << "      const unsigned n_ = cs_[" << 2 * NS << "u * nc_ + c];\n";
       o << "      if (!n_) continue;\n";
-      o << "      atomicAdd(&cg_[" << NS << "ULL * nc_ + c], (unsigned long long)n_);\n";
+      if ((int)shapes[s]->aggs.size() > NS) o << "      atomicAdd(&cg_[" << NS << "ULL * nc_ + c], (unsigned long long)n_);\n";
+      else o << "      cg_[" << NS << "ULL * nc_ + c] = 1ULL;\n";
       for (int k = 0; k < NS; ++k)
         o << "      { const unsigned long long v_ = ((unsigned long long)cs_[" << 2 * k + 1 << "u * nc_ + c] << 32) | cs_["
           << 2 * k << "u * nc_ + c]; if (v_) atomicAdd(&cg_[" << k << "ULL * nc_ + c], v_); }\n";

@@ -2337,18 +2337,20 @@ struct SharedGen {
   // then per such shape one cell update -- shared-memory cubes per CTA, merged
   // into the global cube at the end, or global atomics for large cubes.
   void emit_cube_scan() {
-    // One CTA per SM, so each SM holds one copy of the shared-memory cubes and
-    // dimension words: 1024 threads (64 registers) for one or two rows per
-    // lane, 512 (128 registers) for four.
+    // Few CTAs per SM, so each SM holds few copies of the shared-memory cubes
+    // and dimension words: two rows per lane in one 1024-thread CTA (64
+    // registers), four in one 512-thread CTA (128), one in two 768-thread CTAs
+    // (40 registers, 48 warps).
     const int IPT = std::max(1, std::min(4, tu.cube)), VW = IPT >= 4 ? 4 : IPT;
-    const int CTA = IPT >= 4 ? 512 : 1024;
+    const int CTA = IPT >= 4 ? 512 : IPT == 2 ? 1024 : 768;
+    const int min_blocks = IPT == 1 ? 2 : 1;
     if (IPT == 3) throw PlanError("cube scans take 1, 2 or 4 rows per lane");
     const int NFC = (int)fcols.size();
     const unsigned long long fr_bytes = ((unsigned long long)NFC * FW * 4 + 15) & ~15ULL;
     const std::string kname = "CubeScan_" + fact;
-    meta << "kernel " << kname << " cubescan 0 " << CTA << " " << 32 * IPT << " " << fr_bytes << " 1\n";
+    meta << "kernel " << kname << " cubescan 0 " << CTA << " " << 32 * IPT << " " << fr_bytes << " " << min_blocks << "\n";
     std::ostringstream o;
-    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", 1) " << kname << "(const CxArgs a) {\n";
+    o << "extern \"C\" __global__ void __launch_bounds__(" << CTA << ", " << min_blocks << ") " << kname << "(const CxArgs a) {\n";
     o << "  constexpr int IPT = " << IPT << ", VW = " << VW << ", TROWS = " << 32 * IPT << ";\n";
     o << "  extern __shared__ __align__(16) unsigned char cx_smem[];\n";
     o << "  unsigned* s_fr = (unsigned*)cx_smem; (void)s_fr;\n";

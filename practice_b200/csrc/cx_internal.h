@@ -35,6 +35,10 @@ void ctx_set_cube_cap(cx_exec_ctx* c, uint64_t bytes);
 // attributes of a dimension determine others, so that later scratch estimates
 // for program `m` see the cube layout its launches will use.
 int ensure_cube_dependencies(const cx_module* m, cx_exec_ctx* c, cudaStream_t s);
+// Compiles ahead of the first batch the cube scan of program `m` for the cube
+// layout batches on `c` will use (every batch of a program shares one), so no
+// batch waits for it.
+int prepare_cube_layout(cx_module* m, cx_exec_ctx* c, cudaStream_t s);
 
 // Scratch bytes a context owns after an execute that needs `need` bytes, when
 // it owns `own` bytes before (own scratch grows to 1.5x the need).

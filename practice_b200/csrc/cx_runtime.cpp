@@ -811,6 +811,34 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
   return true;
 }
 
+// The kernel arguments of a cube layout (`scratch` null: no buffers, for a
+// compile of the layout ahead of its first batch).
+void fill_cube_args(CxArgs& a, const CubePlan& cp, int nshapes, char* scratch, uint64_t cube_off) {
+  for (size_t id = 0; id < cp.lo.size(); ++id) { a.cube_lo[id] = cp.lo[id]; a.cube_radix[id] = cp.radix[id]; }
+  for (size_t id = 0; id < cp.fdtab.size(); ++id) a.cube_fdtab[id] = cp.fdtab[id];
+  for (int s = 0; s < nshapes && s < CX_MAX_SHAPES; ++s) {
+    for (int j = 0; j < CX_MAX_SATTRS; ++j) {
+      a.cube_stride[s * CX_MAX_SATTRS + j] = cp.stride[s][j];
+      a.cube_fdsrc[s * CX_MAX_SATTRS + j] = cp.fdsrc[s][j];
+    }
+    a.cube_g[s] = scratch && cp.used[s] && cp.cells[s] ? (unsigned long long*)(scratch + cube_off + cp.goff[s]) : nullptr;
+    a.cube_cells[s] = (long long)cp.cells[s];
+    a.cube_smem[s] = cp.smem_off[s];
+  }
+  a.cube_smem_words = (int)cp.smem_words;
+  a.cube_chunks = cp.chunks;
+  for (int d = 0; d < CX_MAX_HTS; ++d) {
+    a.cube_dsm[d] = cp.dsm[d];
+    a.cube_desz[d] = cp.desz[d];
+    a.cube_dbase[d] = cp.dbase[d];
+    a.cube_dlen[d] = cp.dlen[d];
+    a.cube_dcomp[d] = scratch && cp.dcomp_bytes[d] ? (unsigned char*)(scratch + cp.dcomp_off[d]) : nullptr;
+    for (int f = 0; f < 4; ++f) { a.cube_fsh[d * 4 + f] = cp.fsh[d * 4 + f]; a.cube_fmk[d * 4 + f] = cp.fmk[d * 4 + f]; }
+  }
+  a.cube_dsm_bytes = (int)cp.dsm_bytes;
+}
+
+
 }  // namespace
 
 // ============================================================ internal ===
@@ -837,6 +865,26 @@ void ctx_set_cube_cap(cx_exec_ctx* c, uint64_t bytes) { c->cube_cap = bytes; }
 
 int ensure_cube_dependencies(const cx_module* m, cx_exec_ctx* c, cudaStream_t s) {
   return m ? ensure_cube_fds(m->lp, c, s) : CX_OK;
+}
+
+int prepare_cube_layout(cx_module* m, cx_exec_ctx* c, cudaStream_t s) {
+  if (!m || !c || !m->lp.cube) return CX_OK;
+  int rc = ensure_cube_fds(m->lp, c, s);
+  if (rc) return rc;
+  std::vector<int> all(m->lp.sshapes.size());
+  for (size_t i = 0; i < all.size(); ++i) all[i] = (int)i;
+  CubePlan cp;
+  if (!plan_cubes(m->lp, c, all.data(), (int)all.size(), cp)) return CX_OK;  // batches will take the mask path
+  size_t ki = 0;
+  while (ki < m->lp.kernels.size() && m->lp.kernels[ki].kind != "cubescan") ++ki;
+  if (ki == m->lp.kernels.size()) return CX_OK;
+  int dev = 0;
+  CX_CUDA(cudaGetDevice(&dev));
+  CxArgs a;
+  memset(&a, 0, sizeof a);
+  fill_cube_args(a, cp, (int)m->lp.sshapes.size(), nullptr, 0);
+  CUfunction fn = nullptr;
+  return cube_spec_function(m, dev, a, m->lp.kernels[ki].name, 227 * 1024, &fn);
 }
 
 int set_error(int code, const std::string& msg) { return fail(code, "%s", msg.c_str()); }
@@ -1597,30 +1645,7 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
       const int s = hsq[j].shape;
       if (s < CX_MAX_SHAPES) { if (a.sq_num[s] == 0) a.sq_first[s] = j; ++a.sq_num[s]; }
     }
-    if (cube) {
-      for (size_t id = 0; id < cp.lo.size(); ++id) { a.cube_lo[id] = cp.lo[id]; a.cube_radix[id] = cp.radix[id]; }
-      for (size_t id = 0; id < cp.fdtab.size(); ++id) a.cube_fdtab[id] = cp.fdtab[id];
-      for (int s = 0; s < nshapes && s < CX_MAX_SHAPES; ++s) {
-        for (int j = 0; j < CX_MAX_SATTRS; ++j) {
-          a.cube_stride[s * CX_MAX_SATTRS + j] = cp.stride[s][j];
-          a.cube_fdsrc[s * CX_MAX_SATTRS + j] = cp.fdsrc[s][j];
-        }
-        a.cube_g[s] = cp.used[s] && cp.cells[s] ? (unsigned long long*)(scratch + cube_off + cp.goff[s]) : nullptr;
-        a.cube_cells[s] = (long long)cp.cells[s];
-        a.cube_smem[s] = cp.smem_off[s];
-      }
-      a.cube_smem_words = (int)cp.smem_words;
-      a.cube_chunks = cp.chunks;
-      for (int d = 0; d < CX_MAX_HTS; ++d) {
-        a.cube_dsm[d] = cp.dsm[d];
-        a.cube_desz[d] = cp.desz[d];
-        a.cube_dbase[d] = cp.dbase[d];
-        a.cube_dlen[d] = cp.dlen[d];
-        a.cube_dcomp[d] = cp.dcomp_bytes[d] ? (unsigned char*)(scratch + cp.dcomp_off[d]) : nullptr;
-        for (int f = 0; f < 4; ++f) { a.cube_fsh[d * 4 + f] = cp.fsh[d * 4 + f]; a.cube_fmk[d * 4 + f] = cp.fmk[d * 4 + f]; }
-      }
-      a.cube_dsm_bytes = (int)cp.dsm_bytes;
-    }
+    if (cube) fill_cube_args(a, cp, nshapes, scratch, cube_off);
     P.args = a;
     P.qn = qn;
     P.nparams = poff;

@@ -168,6 +168,8 @@ int rebuild_universe(cx_server* s) {
   char log[4096];
   const int rc = cx_compile(src.data(), src.size(), nullptr, &m, log, sizeof log);
   if (rc) return rc;
+  // The cube scan for the slots' layout, compiled before any batch needs it.
+  for (Slot& sl : s->slots) cx_internal::prepare_cube_layout(m, sl.ctx, sl.stream);
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->universe) cx_module_release(s->universe);
   s->universe = m;

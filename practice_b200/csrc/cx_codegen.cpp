@@ -2452,8 +2452,9 @@ struct SharedGen {
       o << "      w" << di << "_[i] = 0u;\n";
       o << "      if (a.cube_dsm[" << di << "] >= 0) {\n";
       o << "        if (m & " << joiners[di] << "u) {\n";
-      o << "          const long long o_ = (long long)c_" << d.fk << "[i] - a.cube_dbase[" << di << "];\n";
-      o << "          if (o_ >= 0 && o_ < a.cube_dlen[" << di << "]) {\n";
+      // 32-bit wrap-around: o_ < dlen exactly when the key lies in [dbase, dbase + dlen).
+      o << "          const unsigned o_ = (unsigned)c_" << d.fk << "[i] - (unsigned)a.cube_dbase[" << di << "];\n";
+      o << "          if (o_ < (unsigned)a.cube_dlen[" << di << "]) {\n";
       o << "            const unsigned char* sd_ = s_dim + a.cube_dsm[" << di << "];\n";
       o << "            const int es_ = a.cube_desz[" << di << "];\n";
       o << "            w" << di << "_[i] = es_ == 1 ? (unsigned)sd_[o_] : es_ == 2 ? (unsigned)((const unsigned short*)sd_)[o_] : ((const unsigned*)sd_)[o_];\n";

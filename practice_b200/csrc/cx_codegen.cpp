@@ -616,6 +616,12 @@ struct Emitter {
     return "((" + valid_of(g.expr.get()) + ") ? (" + v + " - " + std::to_string(g.min) + " + 1) : 0)";
   }
   long long eff_card(size_t k) const { return p.groups[k].card + (p.groups[k].nullable ? 1 : 0); }
+  // Storage slot of an unconditional COUNT(*) aggregate (-1 if none).
+  int count_star_slot() const {
+    for (size_t k = 0; k < p.aggs.size(); ++k)
+      if (p.aggs[k].fn == AggFn::Count && p.aggs[k].arg && p.aggs[k].arg->op == Op::Star) return (int)(p.groups.size() + k);
+    return -1;
+  }
   unsigned long long total_groups() const {
     unsigned long long t = 1;
     for (size_t k = 0; k < p.groups.size(); ++k) t *= (unsigned long long)eff_card(k);
@@ -1183,7 +1189,8 @@ struct Emitter {
     // global group table (no warp merging: lanes run different expansions).
     auto atomic_update = [&](const std::string& ii) {
       const std::string bit = "(1u << (hash & 31))";
-      o << ii << (smem_groups ? "atomicOr(&s_touch[hash >> 5], " : "atomicOr(&g_touch[hash >> 5], ") << bit << ");\n";
+      if (smem_groups) o << ii << "atomicOr(&s_touch[hash >> 5], " << bit << ");\n";
+      else if (count_star_slot() < 0) o << ii << "atomicOr(&g_touch[hash >> 5], " << bit << ");\n";
       for (int k = 0; k < NA; ++k) {
         const Agg& ag = p.aggs[k];
         const int slot = (int)p.groups.size() + k;
@@ -1333,7 +1340,7 @@ struct Emitter {
       o << ind << "    if (lane == leader) {\n";
       const std::string bit = "(1u << (hash & 31))";
       if (smem_groups) o << ind << "      atomicOr(&s_touch[hash >> 5], " << bit << ");\n";
-      else o << ind << "      atomicOr(&g_touch[hash >> 5], " << bit << ");\n";
+      else if (count_star_slot() < 0) o << ind << "      atomicOr(&g_touch[hash >> 5], " << bit << ");\n";
       for (int k = 0; k < NA; ++k) {
         const Agg& ag = p.aggs[k];
         const int slot = (int)p.groups.size() + k;
@@ -1706,7 +1713,12 @@ struct Emitter {
       o << "  uint64_t* d_result_validity = (uint64_t*)a.result_validity; (void)d_result_validity;\n";
       o << "  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;\n";
       o << "  if (g >= " << G << "LL) return;\n";
-      o << "  if (!((a.touched[g >> 5] >> (g & 31)) & 1u)) return;\n";
+      // A COUNT(*) slot is non-zero exactly for the groups some row reached, so
+      // plans with one keep no touched bits in global memory.
+      if (count_star_slot() >= 0)
+        o << "  if (d_result[(unsigned long long)g * " << p.storage_ts() << "ULL + " << count_star_slot() << "] == 0ULL) return;\n";
+      else
+        o << "  if (!((a.touched[g >> 5] >> (g & 31)) & 1u)) return;\n";
       emit_key_store(o, "g", "  ");
       o << "}\n\n";
     }

@@ -91,4 +91,5 @@ struct CxArgs {
   int cube_fsh[CX_MAX_HTS * 4];
   int cube_fmk[CX_MAX_HTS * 4];
   int cube_dsm_bytes;                          // shared-memory bytes of all compact dimension copies
+  int cube_dgl[CX_MAX_HTS];                    // 1: compact words gathered from global memory instead
 };

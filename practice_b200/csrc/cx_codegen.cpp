@@ -2477,14 +2477,26 @@ struct SharedGen {
     }
     o << "      rel_[i] = m;\n";
     o << "    }\n";
-    // The other dimensions' int4 entries: every gather of the tile's rows in flight together.
+    // The other dimensions: their compact words gathered from global memory
+    // (one word per key, no key check), or else their int4 entries; every
+    // gather of the tile's rows in flight together.
     for (size_t di = 0; di < dims.size(); ++di) o << "    int4 e" << di << "_[IPT];\n";
     o << "    #pragma unroll\n";
     o << "    for (int i = 0; i < IPT; ++i) {\n";
     for (size_t di = 0; di < dims.size(); ++di) {
       const Dim& d = dims[di];
+      const char* ldw = d.len * 16 <= (1LL << 20) ? "__ldg" : "__ldcg";
+      o << "      if (a.cube_dsm[" << di << "] < 0 && a.cube_dgl[" << di << "] && (rel_[i] & " << joiners[di] << "u)) {\n";
+      o << "        const unsigned o_ = (unsigned)c_" << d.fk << "[i] - (unsigned)a.cube_dbase[" << di << "];\n";
+      o << "        if (o_ < (unsigned)a.cube_dlen[" << di << "]) {\n";
+      o << "          const unsigned char* gd_ = a.cube_dcomp[" << di << "];\n";
+      o << "          const int es_ = a.cube_desz[" << di << "];\n";
+      o << "          w" << di << "_[i] = es_ == 1 ? (unsigned)" << ldw << "(gd_ + o_) : es_ == 2 ? (unsigned)" << ldw
+        << "((const unsigned short*)gd_ + o_) : " << ldw << "((const unsigned*)gd_ + o_);\n";
+      o << "        }\n";
+      o << "      }\n";
       o << "      e" << di << "_[i] = make_int4(0, 0, 0, 0);\n";
-      o << "      if (a.cube_dsm[" << di << "] < 0 && (rel_[i] & " << joiners[di] << "u)) {\n";
+      o << "      if (a.cube_dsm[" << di << "] < 0 && !a.cube_dgl[" << di << "] && (rel_[i] & " << joiners[di] << "u)) {\n";
       o << "        const int h_ = cx_detail::pht_slot<int>(c_" << d.fk << "[i], " << d.len << ", " << d.keymin << ");\n";
       // Entries of a small dimension stay in L1; a large dimension's entries
       // bypass it (L2 only), so its random gathers do not evict the small ones.
@@ -2498,7 +2510,9 @@ struct SharedGen {
     o << "      unsigned m = rel_[i];\n";
     for (size_t di = 0; di < dims.size(); ++di) {
       const Dim& d = dims[di];
-      o << "      if (a.cube_dsm[" << di << "] < 0) {\n";
+      o << "      if (a.cube_dsm[" << di << "] < 0 && a.cube_dgl[" << di << "]) m &= (w" << di << "_[i] & 1u) ? (w" << di
+        << "_[i] >> 1) : " << (~joiners[di] & all_shapes) << "u;\n";
+      o << "      if (a.cube_dsm[" << di << "] < 0 && !a.cube_dgl[" << di << "]) {\n";
       o << "        const int4 g_ = e" << di << "_[i];\n";
       o << "        const bool hit_ = g_.x != 0 && g_.x == c_" << d.fk << "[i];\n";
       o << "        m &= hit_ ? (unsigned)g_.y : " << (~joiners[di] & all_shapes) << "u;\n";
@@ -2525,7 +2539,7 @@ struct SharedGen {
         } else {
           const std::string fi = std::to_string(at.dim * 4 + at.field);
           o << "        { const int4 g_ = e" << at.dim << "_[i];\n";
-          o << "          const unsigned f_ = a.cube_dsm[" << at.dim << "] >= 0 ? ((w" << at.dim << "_[i] >> a.cube_fsh[" << fi
+          o << "          const unsigned f_ = (a.cube_dsm[" << at.dim << "] >= 0 || a.cube_dgl[" << at.dim << "]) ? ((w" << at.dim << "_[i] >> a.cube_fsh[" << fi
             << "]) & (unsigned)a.cube_fmk[" << fi << "]) : " << fld[at.field] << ";\n";
           o << "          cell_ += f_ * " << stride << "; }\n";
         }
@@ -2600,7 +2614,7 @@ struct SharedGen {
         {"a.cube_dsm_bytes", "CXS_DSMB"}, {"a.cube_dsm[", "CXS_DSM"}, {"a.cube_desz[", "CXS_DESZ"},
         {"a.cube_dbase[", "CXS_DBASE"}, {"a.cube_dlen[", "CXS_DLEN"}, {"a.cube_fsh[", "CXS_FSH"},
         {"a.cube_fmk[", "CXS_FMK"}, {"a.cube_stride[", "CXS_STRIDE"}, {"a.cube_smem[", "CXS_SMEM"},
-        {"a.cube_cells[", "CXS_CELLS"}, {"a.cube_lo[", "CXS_LO"}, {"a.cube_radix[", "CXS_RADIX"},
+        {"a.cube_cells[", "CXS_CELLS"}, {"a.cube_lo[", "CXS_LO"}, {"a.cube_radix[", "CXS_RADIX"}, {"a.cube_dgl[", "CXS_DGL"},
         {"a.cube_smem_words", "CXS_SMEMW"}};
     std::set<std::string> used;
     std::string out;

@@ -484,6 +484,7 @@ int cube_spec_function(cx_module* m, int dev, const CxArgs& a, const std::string
     if (f == "cube_dsm_bytes") return a.cube_dsm_bytes;
     if (f == "cube_smem_words") return a.cube_smem_words;
     if (f == "cube_dsm" && in_range(CX_MAX_HTS)) return a.cube_dsm[i];
+    if (f == "cube_dgl" && in_range(CX_MAX_HTS)) return a.cube_dgl[i];
     if (f == "cube_desz" && in_range(CX_MAX_HTS)) return a.cube_desz[i];
     if (f == "cube_dbase" && in_range(CX_MAX_HTS)) return a.cube_dbase[i];
     if (f == "cube_dlen" && in_range(CX_MAX_HTS)) return a.cube_dlen[i];
@@ -580,7 +581,7 @@ struct CubePlan {
   // Dimensions kept in shared memory as compact words: byte offset (-1: none),
   // bytes per word, per field bit shift and mask, scratch offset and size of
   // the array the index kernel writes.
-  std::vector<int> dsm, desz, dbase, dlen, fsh, fmk;
+  std::vector<int> dsm, dgl, desz, dbase, dlen, fsh, fmk;
   std::vector<char> used;                 // per shape: the batch has queries of it
   std::vector<uint64_t> dcomp_off, dcomp_bytes;
   uint64_t dsm_bytes = 0;
@@ -667,6 +668,7 @@ constexpr uint64_t kCubeMaxGlobalBytes = 8ULL << 30;
 constexpr uint64_t kCubeSmemBudget = 96 * 1024;
 constexpr uint64_t kCubeCellsPerChunk = 16384;
 constexpr uint64_t kDimSmemBudget = 96 * 1024;
+constexpr int64_t kDimGlobalKeys = 1LL << 26;  // keys of a dimension whose words may live in global memory
 
 bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, int nq, CubePlan& cp) {
   const int nshapes = (int)lp.sshapes.size();
@@ -764,6 +766,7 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
   // fit the budget together.
   const int nd = (int)lp.cdims.size();
   cp.dsm.assign(CX_MAX_HTS, -1);
+  cp.dgl.assign(CX_MAX_HTS, 0);
   cp.desz.assign(CX_MAX_HTS, 0);
   cp.dbase.assign(CX_MAX_HTS, 0);
   cp.dlen.assign(CX_MAX_HTS, 0);
@@ -777,7 +780,7 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
     auto rp = c->ranges.find(cd.pk);
     if (rp == c->ranges.end()) continue;
     const int64_t klo = rp->second.first, kn = rp->second.second - rp->second.first + 1;
-    if (klo < INT32_MIN || rp->second.second > INT32_MAX || kn <= 0 || kn > (int64_t)(kDimSmemBudget)) continue;
+    if (klo < INT32_MIN || rp->second.second > INT32_MAX || kn <= 0 || kn > kDimGlobalKeys) continue;
     int bits = 1 + nshapes;
     int fw[4] = {0, 0, 0, 0};
     for (size_t a = 0; a < lp.cattrs.size(); ++a) {
@@ -801,8 +804,10 @@ bool plan_cubes(const LaunchPlan& lp, const cx_exec_ctx* c, const int* shapes, i
   }
   std::sort(cand.begin(), cand.end());
   uint64_t dbytes = 0;
+  // Smallest first into shared memory; the rest keep their words in global
+  // memory (one 1-4 byte gather per row instead of a 16-byte entry).
   for (const auto& cd : cand) {
-    if (dbytes + cd.first > kDimSmemBudget) { cp.desz[cd.second] = 0; cp.dcomp_bytes[cd.second] = 0; continue; }
+    if (dbytes + cd.first > kDimSmemBudget) { cp.dgl[cd.second] = 1; continue; }
     cp.dsm[cd.second] = (int)dbytes;
     dbytes += cd.first;
   }
@@ -829,6 +834,7 @@ void fill_cube_args(CxArgs& a, const CubePlan& cp, int nshapes, char* scratch, u
   a.cube_chunks = cp.chunks;
   for (int d = 0; d < CX_MAX_HTS; ++d) {
     a.cube_dsm[d] = cp.dsm[d];
+    a.cube_dgl[d] = cp.dgl[d];
     a.cube_desz[d] = cp.desz[d];
     a.cube_dbase[d] = cp.dbase[d];
     a.cube_dlen[d] = cp.dlen[d];

@@ -2325,21 +2325,25 @@ struct SharedGen {
       o << "      if (" << f << ") { rel |= " << (1u << s) << "u; break; }\n";
       o << "    }\n";
     }
+    // A dimension kept as compact words: its word at key - key range minimum
+    // (set with a 32-bit atomic OR on the word's 4-byte container, so a second
+    // row with the same key is seen by its present bit), and no int4 entry.
+    o << "    if (a.cube_desz[" << di << "] > 0) {\n";
+    o << "      const unsigned o_ = (unsigned)k - (unsigned)a.cube_dbase[" << di << "];\n";
+    o << "      if (o_ >= (unsigned)a.cube_dlen[" << di << "]) { cx::raise(a.err, cx::ERR_CUBE_RANGE); continue; }\n";
+    o << "      unsigned w_ = 1u | (rel << 1);\n";
+    o << "      #pragma unroll\n";
+    o << "      for (int j = 0; j < 4; ++j) w_ |= f_[j] << a.cube_fsh[" << di * 4 << " + j];\n";
+    o << "      unsigned* cw_ = (unsigned*)a.cube_dcomp[" << di << "];\n";
+    o << "      const int es_ = a.cube_desz[" << di << "];\n";
+    o << "      const unsigned sh_ = es_ == 1 ? (o_ & 3u) * 8u : es_ == 2 ? (o_ & 1u) * 16u : 0u;\n";
+    o << "      const unsigned wi_ = es_ == 1 ? (o_ >> 2) : es_ == 2 ? (o_ >> 1) : o_;\n";
+    o << "      const unsigned old_ = atomicOr(&cw_[wi_], w_ << sh_);\n";
+    o << "      if ((old_ >> sh_) & 1u) cx::raise(a.err, cx::ERR_DIM_COLLISION);\n";
+    o << "      continue;\n";
+    o << "    }\n";
     o << "    if (atomicCAS(&ent[h].x, 0, k) != 0) { cx::raise(a.err, cx::ERR_DIM_COLLISION); continue; }\n";
     o << "    ent[h] = make_int4(k, (int)rel, (int)(f_[0] | (f_[1] << 16)), (int)(f_[2] | (f_[3] << 16)));\n";
-    // The compact word of a dimension kept in shared memory, at key - key range minimum.
-    o << "    if (a.cube_desz[" << di << "] > 0) {\n";
-    o << "      const long long o_ = (long long)k - a.cube_dbase[" << di << "];\n";
-    o << "      if (o_ >= 0 && o_ < a.cube_dlen[" << di << "]) {\n";
-    o << "        unsigned w_ = 1u | (rel << 1);\n";
-    o << "        #pragma unroll\n";
-    o << "        for (int j = 0; j < 4; ++j) w_ |= f_[j] << a.cube_fsh[" << di * 4 << " + j];\n";
-    o << "        unsigned char* cw_ = a.cube_dcomp[" << di << "];\n";
-    o << "        if (a.cube_desz[" << di << "] == 1) cw_[o_] = (unsigned char)w_;\n";
-    o << "        else if (a.cube_desz[" << di << "] == 2) ((unsigned short*)cw_)[o_] = (unsigned short)w_;\n";
-    o << "        else ((unsigned*)cw_)[o_] = w_;\n";
-    o << "      }\n";
-    o << "    }\n";
     o << "  }\n}\n\n";
   }
 
@@ -2350,11 +2354,11 @@ struct SharedGen {
   // into the global cube at the end, or global atomics for large cubes.
   void emit_cube_scan() {
     // Few CTAs per SM, so each SM holds few copies of the shared-memory cubes
-    // and dimension words: two rows per lane in one 1024-thread CTA (64
-    // registers), four in one 512-thread CTA (128), one in two 768-thread CTAs
-    // (40 registers, 48 warps).
+    // and dimension words: two or four rows per lane in one 1024-thread CTA (64
+    // registers; compact dimension words keep four rows' state in them), one
+    // in two 768-thread CTAs (40 registers, 48 warps).
     const int IPT = std::max(1, std::min(4, tu.cube)), VW = IPT >= 4 ? 4 : IPT;
-    const int CTA = IPT >= 4 ? 512 : IPT == 2 ? 1024 : 768;
+    const int CTA = IPT >= 2 ? 1024 : 768;
     const int min_blocks = IPT == 1 ? 2 : 1;
     if (IPT == 3) throw PlanError("cube scans take 1, 2 or 4 rows per lane");
     const int NFC = (int)fcols.size();

@@ -936,9 +936,9 @@ uint64_t shared_scratch_need(const cx_module* m, const cx_exec_ctx* c, const int
   const bool cube = c && plan_cubes(lp, c, shapes, nq, cp);
   uint64_t off = 0;
   for (const auto& h : lp.hts) {
-    off = align256(off + h.words * 4);
+    if (!(cube && h.slot >= 0 && h.slot < CX_MAX_HTS && cp.desz[h.slot] > 0)) off = align256(off + h.words * 4);
     auto it = lp.dat_words.find(h.slot);
-    if (it != lp.dat_words.end()) off = align256(off + it->second * 4);
+    if (!cube && it != lp.dat_words.end()) off = align256(off + it->second * 4);
   }
   for (int i = 0; i < nq; ++i) {
     if (shapes[i] < 0 || shapes[i] >= (int)lp.sshapes.size()) continue;
@@ -1518,12 +1518,15 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
   // query, per-pass descriptors and parameters, error word.
   uint64_t off = 0;
   std::vector<uint64_t> dkm_off, dat_off;
+  // The cube path needs no int4 entries for dimensions kept as compact words,
+  // and no extra-attribute arrays at all (those serve the mask path).
+  auto compact_dim = [&](int slot) { return cube && slot >= 0 && slot < CX_MAX_HTS && cp.desz[slot] > 0; };
   for (const auto& h : lp.hts) {
     dkm_off.push_back(off);
-    off = align256(off + h.words * 4);
+    if (!compact_dim(h.slot)) off = align256(off + h.words * 4);
     auto it = lp.dat_words.find(h.slot);
     dat_off.push_back(off);
-    if (it != lp.dat_words.end()) off = align256(off + it->second * 4);
+    if (!cube && it != lp.dat_words.end()) off = align256(off + it->second * 4);
   }
   if (cube)
     for (int d = 0; d < CX_MAX_HTS; ++d)
@@ -1566,8 +1569,8 @@ int cx_shared_execute_rows(cx_module* m, cx_exec_ctx* c, const cx_shared_query* 
     scratch = (char*)c->own_scratch;
   }
   for (size_t i = 0; i < lp.hts.size(); ++i) {
-    a.ht[lp.hts[i].slot] = (int*)(scratch + dkm_off[i]);
-    if (lp.dat_words.count(lp.hts[i].slot)) a.dat[lp.hts[i].slot] = (int*)(scratch + dat_off[i]);
+    a.ht[lp.hts[i].slot] = compact_dim(lp.hts[i].slot) ? nullptr : (int*)(scratch + dkm_off[i]);
+    if (!cube && lp.dat_words.count(lp.hts[i].slot)) a.dat[lp.hts[i].slot] = (int*)(scratch + dat_off[i]);
   }
   a.err = (unsigned int*)(scratch + err_off);
 

@@ -498,3 +498,21 @@ def test_payload_tables_with_values_outside_the_catalog_range(db, compact):
         fw = int(m.info.final_words)
         np.testing.assert_array_equal(res.cpu().numpy().view(np.uint64)[:fw], ref.words[:fw])
         np.testing.assert_array_equal(val.cpu().numpy().view(np.uint64)[: (fw + 63) // 64], ref.validity[: (fw + 63) // 64])
+
+
+@pytest.mark.parametrize("cube", [0, 2])
+def test_shared_scan_duplicate_dimension_key_is_reported(db, cube):
+    """Two CUSTOMER rows with the same key make a shared batch that joins
+    CUSTOMER fail with kernel error 4 on both paths, rather than answer from
+    whichever row was indexed last."""
+    n = 100_003
+    ht = datagen.host_tables(49, n, queries.BATCH_COLS)
+    keys = ht.columns["c_custkey"].copy()
+    keys[7] = keys[6]
+    ht.columns["c_custkey"] = keys
+    db.reset()
+    db.load_host_tables(ht, datagen.ssb_tables(n, queries.BATCH_COLS))
+    plans = [queries.template(2, random.Random(3 + k), n) for k in range(4)]
+    got = db.execute_shared(plans, make_tuning(**{**SHARED_DEFAULT, "cube": cube}))
+    assert got[0].timing.mode == (1 if cube else 0)
+    assert got[0].kernel_error == 4

@@ -82,7 +82,7 @@ typedef struct cx_tuning {
                             together -- instead of a membership bitmap and a payload load from the
                             hash table */
   int cube;              /* shared scans: 0 = answer every query from per-query row masks; 1, 2 or
-                            4 (default 2) = the program also carries the aggregate-cube path, which
+                            4 (default 4) = the program also carries the aggregate-cube path, which
                             cx_shared_execute takes when every column the batch's predicates and
                             GROUP BY keys read has a registered range (cx_ctx_set_column_range) of
                             at most 65,536 values and each shape's cube has at most 16,777,216

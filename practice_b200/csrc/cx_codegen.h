@@ -33,7 +33,7 @@ struct Tuning {
                                // membership tests and run the rest on 32 queued rows at a time
   int table_budget = 0;        // bytes of shared memory for payload tables (one byte per slot); opt-in:
                                // measured no faster than bitmaps once rows are warp-compacted
-  int cube = 2;                // shared scans: 0 = per-query row masks only; 1, 2 or 4 = also the
+  int cube = 4;                // shared scans: 0 = per-query row masks only; 1, 2 or 4 = also the
                                // aggregate-cube path (rows per lane of its scan), which the runtime
                                // takes when the batch's attribute ranges allow
 };

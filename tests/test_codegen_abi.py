@@ -223,7 +223,7 @@ def test_shared_program_carries_the_cube_path_when_shapes_allow():
     # quantity, discount, c_region, s_region, d_year, c_nation, p_category, p_brand1
     assert "\ncube 8\n" in launch
     from practice_b200.engine import SHARED_DEFAULT, make_tuning
-    assert _lib.default_tuning().cube == 2
+    assert _lib.default_tuning().cube == 4
     t = make_tuning(**{**SHARED_DEFAULT, "cube": 0})
     assert "CubeScan" not in _lib.shared_codegen(texts, t) and "SharedScan_LINEORDER" in _lib.shared_codegen(texts, t)
     for ipt in (1, 2):

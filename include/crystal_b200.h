@@ -75,7 +75,9 @@ typedef struct cx_tuning {
   int compact;           /* plain grouped scans without expanding joins, unstaged vector loads:
                             1 = each warp queues the rows that pass the join bitmaps and fact
                             filters (ballot / popc into shared memory) and runs payload fetches,
-                            remaining probes and the group update on 32 queued rows at a time */
+                            remaining probes and the group update on 32 queued rows at a time;
+                            2 = the same on 64 queued rows at a time (two rows per lane, their
+                            gathers in flight together, half as many drains) */
   int table_budget;      /* bytes of shared memory for payload tables (default 0 = none; the
                             autotuner tries 96 KiB): a join whose payload's catalog range has at
                             most 254 values keeps one byte per hash slot -- membership and payload

@@ -780,6 +780,9 @@ struct Emitter {
     // every lane busy, instead of on mostly idle lanes of every tile.
     const bool vec_pf_all = STAGES == 0 && NSC > 0 && (IPT == 1 || IPT == 2 || IPT % 4 == 0) && tu.prefetch > 0;
     const bool compact = tu.compact > 0 && !expanding && grouped && vec_pf_all;
+    // Queued rows run the rest of the pipeline 32 x DB at a time (compact = 2:
+    // two batches' gathers in flight together, half the drains).
+    const int DB = compact ? std::max(1, std::min(2, tu.compact)) : 1;
     std::set<std::string> exact_set;
     for (const auto& b : sbms) exact_set.insert(b.dim);
     auto fact_only = [&](const Expr* e) {
@@ -818,7 +821,7 @@ struct Emitter {
     }
     int NQ = 0;
     for (const auto& c : qcols) NQ += 1 + (nullable(c) ? 1 : 0);
-    const int QCAP = 32 * (IPT + 1);
+    const int QCAP = 32 * (IPT + DB);
     unsigned long long q_off = 0;
     if (compact && NQ > 0) {
       q_off = (off + 15) & ~15ULL;
@@ -1536,14 +1539,14 @@ struct Emitter {
       o << "   }\n";  // live_
       // Run the rest of the pipeline on 32 queued rows at a time (the last,
       // partial batch once the warp has no tiles left).
-      o << "   while (q_n >= 32 || (!live_ && q_n > 0)) {\n";
-      o << "    const int cnt_ = q_n < 32 ? q_n : 32;\n";
+      o << "   while (q_n >= " << 32 * DB << " || (!live_ && q_n > 0)) {\n";
+      o << "    const int cnt_ = q_n < " << 32 * DB << " ? q_n : " << 32 * DB << ";\n";
       o << "    __syncwarp();\n";
       o << "    {\n";
-      o << "    constexpr int ITEMS_PER_THREAD = 1;\n";
+      o << "    constexpr int ITEMS_PER_THREAD = " << DB << ";\n";
       o << "    const int num_tile_items = cnt_;\n";
-      o << "    int flags[1];\n";
-      o << "    flags[0] = lane < cnt_ ? 1 : 0;\n";
+      o << "    int flags[" << DB << "];\n";
+      for (int j = 0; j < DB; ++j) o << "    flags[" << j << "] = lane + " << 32 * j << " < cnt_ ? 1 : 0;\n";
       std::vector<std::string> dregs = qcols;
       for (const auto& c : payload_cols) dregs.push_back(c);
       declare_regs(o, dregs, "    ");
@@ -1553,10 +1556,12 @@ struct Emitter {
       {
         int qi = 0;
         for (const auto& c : qcols) {
-          o << "    " << c << "[0] = q_base[" << qi++ * QCAP << " + lane];\n";
+          for (int j = 0; j < DB; ++j) o << "    " << c << "[" << j << "] = q_base[" << qi * QCAP + 32 * j << " + lane];\n";
+          ++qi;
           loaded.insert(c);
           if (nullable(c)) {
-            o << "    " << c << "_valid[0] = q_base[" << qi++ * QCAP << " + lane];\n";
+            for (int j = 0; j < DB; ++j) o << "    " << c << "_valid[" << j << "] = q_base[" << qi * QCAP + 32 * j << " + lane];\n";
+            ++qi;
             valid_regs.insert(c);
           }
         }
@@ -1573,7 +1578,7 @@ struct Emitter {
       o << "      const int e_ = b_ + lane;\n";
       o << "      int v_[" << std::max(NQ, 1) << "];\n";
       o << "      if (e_ < rest_) {\n";
-      for (int qi = 0; qi < NQ; ++qi) o << "        v_[" << qi << "] = q_base[" << qi * QCAP << " + 32 + e_];\n";
+      for (int qi = 0; qi < NQ; ++qi) o << "        v_[" << qi << "] = q_base[" << qi * QCAP << " + cnt_ + e_];\n";
       o << "      }\n";
       o << "      __syncwarp();\n";
       o << "      if (e_ < rest_) {\n";

@@ -322,6 +322,12 @@ def test_compacted_scans_compile(name, ipt):
     src = _lib.codegen(plan.text(), t)
     assert "q_base" in src and "while (q_n >= 32 || (!live_ && q_n > 0))" in src
     _lib.Module(src, key=f"compact_{name}_{ipt}")
+    # Two queued batches per drain.
+    t.compact = 2
+    src2 = _lib.codegen(plan.text(), t)
+    assert "while (q_n >= 64 || (!live_ && q_n > 0))" in src2
+    _lib.Module(src2, key=f"compact2_{name}_{ipt}")
+    t.compact = 1
     # Scalar plans and staged scans keep the direct path.
     t.stages, t.block_threads = 2, 256
     assert "q_base" not in _lib.codegen(plan.text(), t)

@@ -22,7 +22,8 @@ pytestmark = pytest.mark.gpu
 N = 400_003
 NULLABLE = ("lo_revenue", "c_nation")
 TUNINGS = {"default": None, "tma": dict(block_threads=256, items_per_thread=4, stages=3, ctas_per_sm=2),
-           "compact": dict(compact=1), "compact_ipt2": dict(block_threads=512, items_per_thread=2, compact=1)}
+           "compact": dict(compact=1), "compact_ipt2": dict(block_threads=512, items_per_thread=2, compact=1),
+           "compact_drain64": dict(compact=2)}
 
 
 @pytest.fixture(scope="module")

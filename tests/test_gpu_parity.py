@@ -70,7 +70,7 @@ def test_q31_nullable(db):
     assert any(r[3] < r[2] for r in rs), "COUNT(revenue) must skip NULL revenue"
 
 
-@pytest.mark.parametrize("compact", [0, 1])
+@pytest.mark.parametrize("compact", [0, 1, 2])
 @pytest.mark.parametrize("t", [0, 1, 2, 3])
 def test_shared_scan_templates(db, t, compact):
     n = 1_500_000
@@ -85,7 +85,8 @@ def test_shared_scan_templates(db, t, compact):
 @pytest.mark.parametrize("bt,ipt,stages,place,merge,bitmaps,compact", [
     (128, 4, 4, 0, 0, 98304, 0), (256, 8, 2, 0, 1, 0, 0), (512, 2, 3, 2, 0, 98304, 0), (256, 4, 0, 1, 2, 98304, 0),
     (1024, 1, 2, 0, 2, 0, 0), (256, 4, 6, 2, 1, 98304, 0), (1024, 2, 0, 1, 1, 98304, 0),
-    (1024, 4, 0, 0, 0, 49152, 1), (512, 8, 0, 2, 0, 49152, 1), (1024, 4, 0, 1, 0, 0, 1), (256, 2, 0, 0, 2, 98304, 1)])
+    (1024, 4, 0, 0, 0, 49152, 1), (512, 8, 0, 2, 0, 49152, 1), (1024, 4, 0, 1, 0, 0, 1), (256, 2, 0, 0, 2, 98304, 1),
+    (1024, 4, 0, 0, 0, 49152, 2), (512, 2, 0, 2, 0, 49152, 2)])
 def test_tuning_invariance(db, bt, ipt, stages, place, merge, bitmaps, compact):
     n = 777_777
     ht = load(db, 15, n, queries.Q31_COLS, nulls={"lo_revenue": 100, "c_city": 50})

@@ -168,8 +168,19 @@ int rebuild_universe(cx_server* s) {
   char log[4096];
   const int rc = cx_compile(src.data(), src.size(), nullptr, &m, log, sizeof log);
   if (rc) return rc;
-  // The cube scan for the slots' layout, compiled before any batch needs it.
-  for (Slot& sl : s->slots) cx_internal::prepare_cube_layout(m, sl.ctx, sl.stream);
+  // The cube scan for the slots' layout, compiled before any batch needs it
+  // (on a context and stream of its own: the scheduler may be running a batch
+  // on the slots' contexts meanwhile; the compiled scan is kept by the module).
+  {
+    cx_exec_ctx* tmp = cx_ctx_create();
+    cudaStream_t st = nullptr;
+    if (tmp && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess) {
+      cx_internal::ctx_copy_tables(s->tables, tmp);
+      cx_internal::prepare_cube_layout(m, tmp, st);
+      cudaStreamDestroy(st);
+    }
+    cx_ctx_destroy(tmp);
+  }
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->universe) cx_module_release(s->universe);
   s->universe = m;

@@ -358,3 +358,26 @@ def test_payload_tables_follow_the_catalog_range_and_budget():
     src = _lib.codegen(text, t)
     assert "BlockFetchPayloadTable" in src and "q_base" in src
     _lib.Module(src, key="ptable_q31_compact")
+
+
+def test_cube_scan_region_compiles_with_its_layout_as_constants():
+    """The runtime recompiles a shared program's cube region with the batch's
+    layout as constants: the region reads its layout only through CXS_*
+    macros (defaults: the kernel arguments), and the prelude plus `#define`s
+    of every such macro plus the region compile on their own."""
+    import re
+    from practice_b200.engine import SHARED_DEFAULT, make_tuning
+    rng = random.Random(21)
+    src = _lib.shared_codegen([queries.template(t, rng).text() for t in range(4)], make_tuning(**SHARED_DEFAULT))
+    p0, p1 = src.index("@*/") + 3, src.index("//@cx-prelude-end")
+    r0, r1 = src.index("//@cx-cube-begin"), src.index("//@cx-cube-end")
+    region = src[r0:r1]
+    kernel = region[region.index("#endif"):]
+    assert "a.cube_stride[" not in kernel and "a.cube_dsm[" not in kernel  # every layout read is a hook
+    defaults = re.findall(r"#define (CXS_\w+) \(a\.(\w+)(?:\[(\d+)\])?\)", region)
+    assert defaults
+    values = {"cube_dsm": -1, "cube_dgl": 1, "cube_desz": 2, "cube_cells": 1000}
+    defs = "#define CXS_SPEC 1\n" + "".join(
+        f"#define {name} ({values.get(field, 3)}{'LL' if field == 'cube_cells' else ''})\n" for name, field, _ in defaults)
+    spec = "/*@cx-launch\nv 1\n@*/\n" + src[p0:p1] + "\n" + defs + region
+    _lib.Module(spec, key="cube_layout_constants")

@@ -65,7 +65,8 @@ typedef struct cx_tuning {
   int prefetch;          /* unstaged plain scans (stages = 0): 0 = each column loaded where the
                             pipeline first reads it, 1 = vector loads of every column at the tile
                             start (default), 2 = as 1 with the next tile's loads issued a tile
-                            ahead */
+                            ahead, 3 = as 1 with the warp's next tile prefetched into L2 (one
+                            bulk prefetch per column, no registers held) */
   int wait_limit_us;     /* every wait of a kernel on an mbarrier gives up after this many
                             microseconds (global timer) and raises kernel error 1 (CX_E_KERNEL
                             from cx_ctx_sync); default 500000, range 1 .. 60000000 */

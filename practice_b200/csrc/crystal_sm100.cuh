@@ -908,6 +908,14 @@ CX_DEVICE void bulk_g2s(void* smem_dst, const void* gmem_src, unsigned bytes, un
       : "memory");
 }
 
+// Bulk prefetch of `bytes` of global memory into L2 (no destination, no
+// completion to wait for): a warp asks for its next tile's columns a tile ahead
+// at no register cost.  Address 16-byte aligned, bytes a multiple of 16, the
+// range inside the buffer.
+CX_DEVICE void l2_prefetch_bulk(const void* gmem_src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gmem_src), "r"(bytes) : "memory");
+}
+
 CX_DEVICE void debug_stall(unsigned long long* bar, unsigned int* err, unsigned limit_us) {
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);

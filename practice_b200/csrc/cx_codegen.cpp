@@ -969,7 +969,8 @@ struct Emitter {
     // vector loads (vector-striped rows) one tile ahead, so the next tile's
     // loads are in flight while this one probes and aggregates.
     const bool vec_pf = STAGES == 0 && NSC > 0 && (IPT == 1 || IPT == 2 || IPT % 4 == 0) && tu.prefetch > 0;
-    const bool ahead = vec_pf && tu.prefetch >= 2;
+    const bool ahead = vec_pf && tu.prefetch == 2;
+    const bool l2_ahead = vec_pf && tu.prefetch == 3;
     if (vec_pf) {
       o << "  bool vec_ok = true;\n";
       for (const auto& c : fact_cols) o << "  vec_ok = vec_ok && ((((unsigned long long)d_" << c << ") & 15ULL) == 0ULL);\n";
@@ -1012,6 +1013,14 @@ struct Emitter {
     o << "    InitFlags<BLOCK_THREADS, ITEMS_PER_THREAD>(flags);\n";
     if (vec_pf) {
       o << "    if (vec_ok && t < full_tiles) {\n";
+      if (l2_ahead) {
+        // The warp's next tile into L2 while this one is processed: its loads
+        // then wait on L2, not DRAM (no registers held for it).
+        o << "      if (lane == 0 && t + nwarps < full_tiles) {\n";
+        for (const auto& c : fact_cols)
+          o << "        cx::l2_prefetch_bulk(d_" << c << " + (t + nwarps) * TILE_SIZE, TILE_SIZE * 4u);\n";
+        o << "      }\n";
+      }
       if (ahead) {
         o << "      #pragma unroll\n      for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
         for (const auto& c : fact_cols) o << "        " << c << "[i] = pf_" << c << "[i];\n";
@@ -2430,6 +2439,7 @@ struct SharedGen {
     o << "  const long long n = a.rows[0];\n";
     o << "  const long long ntiles = (n + TROWS - 1) / TROWS;\n";
     o << "  const long long nw = ((long long)gridDim.x * " << CTA << ") >> 5;\n";
+    o << "  bool bad_ = false;\n";
     o << "  for (long long t = ((long long)blockIdx.x * " << CTA << " + threadIdx.x) >> 5; t < ntiles; t += nw) {\n";
     o << "    const long long base = t * TROWS;\n";
     o << "    const int nt = (int)(n - base < TROWS ? n - base : TROWS);\n";
@@ -2464,28 +2474,31 @@ struct SharedGen {
     const unsigned all_shapes = (1u << shapes.size()) - 1u;
     // Dimensions kept in shared memory first: their compact words cost no
     // gather, and the shapes they rule out skip the other dimensions' gathers.
+    // Dimension by dimension over the lane's rows, so the rows' lookups are
+    // independent instructions in flight together.
     for (size_t di = 0; di < dims.size(); ++di) o << "    unsigned w" << di << "_[IPT];\n";
-    o << "    #pragma unroll\n";
-    o << "    for (int i = 0; i < IPT; ++i) {\n";
-    o << "      unsigned m = rel_[i];\n";
     for (size_t di = 0; di < dims.size(); ++di) {
       const Dim& d = dims[di];
-      o << "      w" << di << "_[i] = 0u;\n";
-      o << "      if (a.cube_dsm[" << di << "] >= 0) {\n";
-      o << "        if (m & " << joiners[di] << "u) {\n";
+      o << "    if (a.cube_dsm[" << di << "] >= 0) {\n";
+      o << "      const unsigned char* sd_ = s_dim + a.cube_dsm[" << di << "];\n";
+      o << "      const int es_ = a.cube_desz[" << di << "];\n";
+      o << "      #pragma unroll\n";
+      o << "      for (int i = 0; i < IPT; ++i) {\n";
       // 32-bit wrap-around: o_ < dlen exactly when the key lies in [dbase, dbase + dlen).
-      o << "          const unsigned o_ = (unsigned)c_" << d.fk << "[i] - (unsigned)a.cube_dbase[" << di << "];\n";
-      o << "          if (o_ < (unsigned)a.cube_dlen[" << di << "]) {\n";
-      o << "            const unsigned char* sd_ = s_dim + a.cube_dsm[" << di << "];\n";
-      o << "            const int es_ = a.cube_desz[" << di << "];\n";
-      o << "            w" << di << "_[i] = es_ == 1 ? (unsigned)sd_[o_] : es_ == 2 ? (unsigned)((const unsigned short*)sd_)[o_] : ((const unsigned*)sd_)[o_];\n";
-      o << "          }\n";
-      o << "        }\n";
-      o << "        m &= (w" << di << "_[i] & 1u) ? (w" << di << "_[i] >> 1) : " << (~joiners[di] & all_shapes) << "u;\n";
+      o << "        const unsigned o_ = (unsigned)c_" << d.fk << "[i] - (unsigned)a.cube_dbase[" << di << "];\n";
+      o << "        w" << di << "_[i] = ((rel_[i] & " << joiners[di] << "u) && o_ < (unsigned)a.cube_dlen[" << di
+        << "]) ? (es_ == 1 ? (unsigned)sd_[o_] : es_ == 2 ? (unsigned)((const unsigned short*)sd_)[o_] : ((const unsigned*)sd_)[o_]) : 0u;\n";
       o << "      }\n";
+      o << "      #pragma unroll\n";
+      // A word's shape bits are set for the shapes that do not join the
+      // dimension; an absent key's word is 0 (no shape bits): OR-ing in the
+      // non-joining shapes gives both cases without testing the present bit.
+      o << "      for (int i = 0; i < IPT; ++i) rel_[i] &= (w" << di << "_[i] >> 1) | " << (~joiners[di] & all_shapes) << "u;\n";
+      o << "    } else {\n";
+      o << "      #pragma unroll\n";
+      o << "      for (int i = 0; i < IPT; ++i) w" << di << "_[i] = 0u;\n";
+      o << "    }\n";
     }
-    o << "      rel_[i] = m;\n";
-    o << "    }\n";
     // The other dimensions: their compact words gathered from global memory
     // (one word per key, no key check), or else their int4 entries; every
     // gather of the tile's rows in flight together.
@@ -2519,8 +2532,8 @@ struct SharedGen {
     o << "      unsigned m = rel_[i];\n";
     for (size_t di = 0; di < dims.size(); ++di) {
       const Dim& d = dims[di];
-      o << "      if (a.cube_dsm[" << di << "] < 0 && a.cube_dgl[" << di << "]) m &= (w" << di << "_[i] & 1u) ? (w" << di
-        << "_[i] >> 1) : " << (~joiners[di] & all_shapes) << "u;\n";
+      o << "      if (a.cube_dsm[" << di << "] < 0 && a.cube_dgl[" << di << "]) m &= (w" << di << "_[i] >> 1) | "
+        << (~joiners[di] & all_shapes) << "u;\n";
       o << "      if (a.cube_dsm[" << di << "] < 0 && !a.cube_dgl[" << di << "]) {\n";
       o << "        const int4 g_ = e" << di << "_[i];\n";
       o << "        const bool hit_ = g_.x != 0 && g_.x == c_" << d.fk << "[i];\n";
@@ -2553,9 +2566,10 @@ struct SharedGen {
           o << "          cell_ += f_ * " << stride << "; }\n";
         }
       }
-      o << "        if (!in_) {\n";
-      o << "          cx::raise(a.err, cx::ERR_CUBE_RANGE);\n";
-      o << "        } else {\n";
+      // A value outside its attribute's range is reported once per thread
+      // after the scan; the row updates nothing.
+      o << "        bad_ = bad_ || !in_;\n";
+      o << "        if (in_) {\n";
       int ks = 0;
       for (const auto& ag : p.aggs) {
         if (ag.fn != AggFn::Sum) continue;
@@ -2569,7 +2583,7 @@ struct SharedGen {
       o << "            unsigned* cs_ = (unsigned*)(s_cube + a.cube_smem[" << s << "]);\n";
       o << "            const unsigned nc_ = (unsigned)a.cube_cells[" << s << "];\n";
       for (int k = 0; k < NS; ++k) {
-        o << "            if (x" << k << "_) {\n";
+        o << "            {\n";
         o << "              const unsigned lo_ = (unsigned)x" << k << "_;\n";
         o << "              const unsigned old_ = atomicAdd(&cs_[" << 2 * k << "u * nc_ + cell_], lo_);\n";
         o << "              const unsigned hi_ = (unsigned)(x" << k << "_ >> 32) + (old_ + lo_ < old_ ? 1u : 0u);\n";
@@ -2593,6 +2607,7 @@ struct SharedGen {
     }
     o << "    }\n";
     o << "  }\n";
+    o << "  if (bad_) cx::raise(a.err, cx::ERR_CUBE_RANGE);\n";
     // Shared-memory cubes into the global cubes.
     o << "  __syncthreads();\n";
     for (size_t s = 0; s < shapes.size(); ++s) {

@@ -26,7 +26,8 @@ struct Tuning {
   int parametric = 0;          // plain kernels: literals read from CxArgs.lits at run time
   int prefetch = 1;            // unstaged plain scans: 0 columns loaded where first used,
                                // 1 vector loads of every column at the tile start,
-                               // 2 as 1 and the next tile's loads issued one tile ahead
+                               // 2 as 1 and the next tile's loads issued one tile ahead,
+                               // 3 as 1 and an L2 bulk prefetch of the warp's next tile
   int wait_limit_us = 500000;  // a bounded mbarrier wait gives up after this many microseconds
   int debug_stall = 0;         // test hook: 1 = every CTA first waits on a barrier nothing completes
   int compact = 0;             // plain grouped scans: 1 = queue qualifying rows per warp after the

@@ -73,10 +73,11 @@ def test_tuning_space_compiles(bt, ipt, stages, place):
         _lib.Module(_lib.codegen(plan.text(), t), key=f"tune_{name}_{bt}_{ipt}_{stages}_{place}")
 
 
-@pytest.mark.parametrize("prefetch,place,merge", [(0, 4, 0), (1, 3, 0), (2, 0, 0), (1, 0, 1), (1, 2, 2), (1, 1, 1)])
+@pytest.mark.parametrize("prefetch,place,merge", [(0, 4, 0), (1, 3, 0), (2, 0, 0), (1, 0, 1), (1, 2, 2), (1, 1, 1),
+                                                   (3, 0, 0)])
 def test_launch_knobs_compile(prefetch, place, merge):
     """Unstaged loads (where first used / vector loads at the tile start / one
-    tile ahead), per-thread shared-memory and register group slots, warp-merged
+    tile ahead / an L2 prefetch of the next tile), per-thread shared-memory and register group slots, warp-merged
     and per-lane group updates, including the expanding joins' uniform loop."""
     t = _lib.default_tuning()
     t.prefetch, t.group_placement, t.group_merge = prefetch, place, merge
@@ -85,6 +86,8 @@ def test_launch_knobs_compile(prefetch, place, merge):
         src = _lib.codegen(plans[name].text(), t)
         if prefetch == 0:
             assert "WarpLoadTileV" not in src
+        if prefetch == 3 and name in ("T1", "T2"):
+            assert "l2_prefetch_bulk" in src
         if place == 4 and name == "T1":
             assert "s_lacc" in src
         _lib.Module(src, key=f"knobs_{name}_{prefetch}_{place}_{merge}")

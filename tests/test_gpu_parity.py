@@ -82,17 +82,19 @@ def test_shared_scan_templates(db, t, compact):
         assert_parity(db, queries.template(t, rng, n), ht, tun)
 
 
-@pytest.mark.parametrize("bt,ipt,stages,place,merge,bitmaps,compact", [
-    (128, 4, 4, 0, 0, 98304, 0), (256, 8, 2, 0, 1, 0, 0), (512, 2, 3, 2, 0, 98304, 0), (256, 4, 0, 1, 2, 98304, 0),
-    (1024, 1, 2, 0, 2, 0, 0), (256, 4, 6, 2, 1, 98304, 0), (1024, 2, 0, 1, 1, 98304, 0),
-    (1024, 4, 0, 0, 0, 49152, 1), (512, 8, 0, 2, 0, 49152, 1), (1024, 4, 0, 1, 0, 0, 1), (256, 2, 0, 0, 2, 98304, 1),
-    (1024, 4, 0, 0, 0, 49152, 2), (512, 2, 0, 2, 0, 49152, 2)])
-def test_tuning_invariance(db, bt, ipt, stages, place, merge, bitmaps, compact):
+@pytest.mark.parametrize("bt,ipt,stages,place,merge,bitmaps,compact,prefetch", [
+    (128, 4, 4, 0, 0, 98304, 0, 1), (256, 8, 2, 0, 1, 0, 0, 1), (512, 2, 3, 2, 0, 98304, 0, 1),
+    (256, 4, 0, 1, 2, 98304, 0, 1), (1024, 1, 2, 0, 2, 0, 0, 1), (256, 4, 6, 2, 1, 98304, 0, 1),
+    (1024, 2, 0, 1, 1, 98304, 0, 1), (1024, 4, 0, 0, 0, 49152, 1, 1), (512, 8, 0, 2, 0, 49152, 1, 1),
+    (1024, 4, 0, 1, 0, 0, 1, 1), (256, 2, 0, 0, 2, 98304, 1, 1), (1024, 4, 0, 0, 0, 49152, 2, 1),
+    (512, 2, 0, 2, 0, 49152, 2, 1), (1024, 4, 0, 0, 0, 49152, 1, 3), (512, 2, 0, 2, 0, 0, 0, 3),
+    (1024, 2, 0, 0, 0, 49152, 2, 3), (256, 4, 0, 1, 2, 98304, 0, 2)])
+def test_tuning_invariance(db, bt, ipt, stages, place, merge, bitmaps, compact, prefetch):
     n = 777_777
     ht = load(db, 15, n, queries.Q31_COLS, nulls={"lo_revenue": 100, "c_city": 50})
     t = _lib.default_tuning()
     t.block_threads, t.items_per_thread, t.stages, t.group_placement = bt, ipt, stages, place
-    t.group_merge, t.bitmap_budget, t.compact = merge, bitmaps, compact
+    t.group_merge, t.bitmap_budget, t.compact, t.prefetch = merge, bitmaps, compact, prefetch
     assert_parity(db, queries.ssb_q31_nullable(n), ht, t)
     assert_parity(db, queries.ssb_q31(n), ht, t)
 

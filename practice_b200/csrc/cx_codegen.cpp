@@ -2542,13 +2542,20 @@ struct SharedGen {
     }
     o << "      if (m == 0u) continue;\n";
     const char* fld[4] = {"((unsigned)g_.z & 0xFFFFu)", "((unsigned)g_.z >> 16)", "((unsigned)g_.w & 0xFFFFu)", "((unsigned)g_.w >> 16)"};
+    // The row's cell in every shape's cube (plain arithmetic, no branches),
+    // then the low-word atomics of all its shared-memory cubes issued
+    // together, then the carries, counts and global-cube updates: the
+    // atomics' round trips overlap instead of following one another.
+    std::vector<std::vector<std::string>> xs(shapes.size());
     for (size_t s = 0; s < shapes.size(); ++s) {
       const Plan& p = *shapes[s];
       Emitter e(p, tu);
       for (const auto& c : fact_cols) e.col_expr[c] = "c_" + c + "[i]";
-      const int NS = sum_aggs(p);
-      o << "      if ((m >> " << s << ") & 1u) {\n";
-      o << "        unsigned cell_ = 0u;\n";
+      for (const auto& ag : p.aggs)
+        if (ag.fn == AggFn::Sum) xs[s].push_back("(unsigned long long)(" + e.math_push(ag.arg.get(), true) + ")");
+      o << "      unsigned cl" << s << "_ = 0u;\n";
+      o << "      bool h" << s << "_;\n";
+      o << "      {\n";
       o << "        bool in_ = true;\n";
       for (size_t j = 0; j < sh_attrs[s].size(); ++j) {
         const int id = sh_attrs[s][j];
@@ -2557,51 +2564,64 @@ struct SharedGen {
         if (at.dim < 0) {
           o << "        { const unsigned x_ = (unsigned)(c_" << at.col << "[i] - a.cube_lo[" << id << "]);\n";
           o << "          in_ = in_ && x_ < (unsigned)a.cube_radix[" << id << "];\n";
-          o << "          cell_ += x_ * " << stride << "; }\n";
+          o << "          cl" << s << "_ += x_ * " << stride << "; }\n";
         } else {
           const std::string fi = std::to_string(at.dim * 4 + at.field);
           o << "        { const int4 g_ = e" << at.dim << "_[i];\n";
           o << "          const unsigned f_ = (a.cube_dsm[" << at.dim << "] >= 0 || a.cube_dgl[" << at.dim << "]) ? ((w" << at.dim << "_[i] >> a.cube_fsh[" << fi
             << "]) & (unsigned)a.cube_fmk[" << fi << "]) : " << fld[at.field] << ";\n";
-          o << "          cell_ += f_ * " << stride << "; }\n";
+          o << "          cl" << s << "_ += f_ * " << stride << "; }\n";
         }
       }
       // A value outside its attribute's range is reported once per thread
       // after the scan; the row updates nothing.
-      o << "        bad_ = bad_ || !in_;\n";
-      o << "        if (in_) {\n";
-      int ks = 0;
-      for (const auto& ag : p.aggs) {
-        if (ag.fn != AggFn::Sum) continue;
-        o << "          const unsigned long long x" << ks << "_ = (unsigned long long)(" << e.math_push(ag.arg.get(), true) << ");\n";
-        ++ks;
+      o << "        const bool b_ = ((m >> " << s << ") & 1u) != 0u;\n";
+      o << "        bad_ = bad_ || (b_ && !in_);\n";
+      o << "        h" << s << "_ = b_ && in_;\n";
+      o << "      }\n";
+    }
+    // Shared-memory cubes keep each sum as two 32-bit words (low word first,
+    // the carry of its add going into the high word) and a 32-bit row count:
+    // every update is a native 32-bit shared-memory atomic.
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      for (size_t k = 0; k < xs[s].size(); ++k) {
+        o << "      unsigned long long x" << s << "_" << k << " = 0ULL;\n";
+        o << "      unsigned o" << s << "_" << k << " = 0u;\n";
       }
-      // Shared-memory cubes keep each sum as two 32-bit words (low word
-      // first, the carry of its add going into the high word) and a 32-bit
-      // row count: every update is a native 32-bit shared-memory atomic.
-      o << "          if (a.cube_smem[" << s << "] >= 0) {\n";
-      o << "            unsigned* cs_ = (unsigned*)(s_cube + a.cube_smem[" << s << "]);\n";
-      o << "            const unsigned nc_ = (unsigned)a.cube_cells[" << s << "];\n";
+      o << "      if (a.cube_smem[" << s << "] >= 0) {\n";
+      o << "        unsigned* cs_ = (unsigned*)(s_cube + a.cube_smem[" << s << "]);\n";
+      o << "        const unsigned nc_ = (unsigned)a.cube_cells[" << s << "];\n";
+      for (size_t k = 0; k < xs[s].size(); ++k) {
+        o << "        x" << s << "_" << k << " = " << xs[s][k] << ";\n";
+        o << "        o" << s << "_" << k << " = h" << s << "_ ? atomicAdd(&cs_[" << 2 * k << "u * nc_ + cl" << s << "_], (unsigned)x" << s << "_" << k << ") : 0u;\n";
+      }
+      o << "      }\n";
+    }
+    for (size_t s = 0; s < shapes.size(); ++s) {
+      const Plan& p = *shapes[s];
+      const int NS = (int)xs[s].size();
+      const bool counts = (int)p.aggs.size() > NS;
+      o << "      if (h" << s << "_) {\n";
+      o << "        if (a.cube_smem[" << s << "] >= 0) {\n";
+      o << "          unsigned* cs_ = (unsigned*)(s_cube + a.cube_smem[" << s << "]);\n";
+      o << "          const unsigned nc_ = (unsigned)a.cube_cells[" << s << "];\n";
       for (int k = 0; k < NS; ++k) {
-        o << "            {\n";
-        o << "              const unsigned lo_ = (unsigned)x" << k << "_;\n";
-        o << "              const unsigned old_ = atomicAdd(&cs_[" << 2 * k << "u * nc_ + cell_], lo_);\n";
-        o << "              const unsigned hi_ = (unsigned)(x" << k << "_ >> 32) + (old_ + lo_ < old_ ? 1u : 0u);\n";
-        o << "              if (hi_) atomicAdd(&cs_[" << 2 * k + 1 << "u * nc_ + cell_], hi_);\n";
-        o << "            }\n";
+        const std::string x = "x" + std::to_string(s) + "_" + std::to_string(k), ov = "o" + std::to_string(s) + "_" + std::to_string(k);
+        o << "          { const unsigned lo_ = (unsigned)" << x << ";\n";
+        o << "            const unsigned hi_ = (unsigned)(" << x << " >> 32) + (" << ov << " + lo_ < " << ov << " ? 1u : 0u);\n";
+        o << "            if (hi_) atomicAdd(&cs_[" << 2 * k + 1 << "u * nc_ + cl" << s << "_], hi_); }\n";
       }
       // A shape without COUNT aggregates needs only whether a cell has rows:
       // a plain store of 1 instead of an atomic count.
-      const bool counts = (int)p.aggs.size() > NS;
-      if (counts) o << "            atomicAdd(&cs_[" << 2 * NS << "u * nc_ + cell_], 1u);\n";
-      else o << "            cs_[" << 2 * NS << "u * nc_ + cell_] = 1u;\n";
-      o << "          } else {\n";
-      o << "            unsigned long long* cg_ = a.cube_g[" << s << "];\n";
-      o << "            const unsigned long long nc_ = (unsigned long long)a.cube_cells[" << s << "];\n";
-      for (int k = 0; k < NS; ++k) o << "            if (x" << k << "_) atomicAdd(&cg_[" << k << "ULL * nc_ + cell_], x" << k << "_);\n";
-      if (counts) o << "            atomicAdd(&cg_[" << NS << "ULL * nc_ + cell_], 1ULL);\n";
-      else o << "            cg_[" << NS << "ULL * nc_ + cell_] = 1ULL;\n";
-      o << "          }\n";
+      if (counts) o << "          atomicAdd(&cs_[" << 2 * NS << "u * nc_ + cl" << s << "_], 1u);\n";
+      else o << "          cs_[" << 2 * NS << "u * nc_ + cl" << s << "_] = 1u;\n";
+      o << "        } else {\n";
+      o << "          unsigned long long* cg_ = a.cube_g[" << s << "];\n";
+      o << "          const unsigned long long nc_ = (unsigned long long)a.cube_cells[" << s << "];\n";
+      for (int k = 0; k < NS; ++k)
+        o << "          { const unsigned long long x_ = " << xs[s][k] << "; if (x_) atomicAdd(&cg_[" << k << "ULL * nc_ + cl" << s << "_], x_); }\n";
+      if (counts) o << "          atomicAdd(&cg_[" << NS << "ULL * nc_ + cl" << s << "_], 1ULL);\n";
+      else o << "          cg_[" << NS << "ULL * nc_ + cl" << s << "_] = 1ULL;\n";
       o << "        }\n";
       o << "      }\n";
     }

@@ -232,9 +232,9 @@ def config_block(args):
 # DRAM bytes (read + write) per fact row of one shared-scan launch over the
 # 8-column batch table, by path: ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum) of one 30M-row launch of the 32-query batch (per-query
-# masks: 972.6 MB; aggregate cubes: 964.7 MB); the traffic of a launch grows
+# masks: 972.6 MB; aggregate cubes: 964.9 MB); the traffic of a launch grows
 # with its rows.
-SHARED_DRAM_BYTES_PER_ROW = {"masks": (968.457472e6 + 4.109056e6) / 30e6, "cube": (961.595904e6 + 3.084800e6) / 30e6}
+SHARED_DRAM_BYTES_PER_ROW = {"masks": (968.457472e6 + 4.109056e6) / 30e6, "cube": (961.588480e6 + 3.345152e6) / 30e6}
 
 PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas_per_sm=16, bitmap_budget=bm,
                          prefetch=pf, group_placement=pl, compact=cp, table_budget=tb)

@@ -352,7 +352,7 @@ def shared_leg(torch, db, plans, stream, args, pg, device, sample_clocks: bool):
         db.autotune_shared(plans, SHARED_CANDIDATES, reps=1)
     tun = db.shared_tuning_for(plans)
     prog = db.shared_program(plans, tun)
-    squeries, sparams, sbufs = db.shared_prepare(prog, plans)
+    squeries, sparams, sbufs, sarena = db.shared_prepare_arena(prog, plans)
     sctx = db.ctx
     for t, n in db.rows.items():
         sctx.set_rows(t, n)
@@ -385,28 +385,28 @@ def shared_leg(torch, db, plans, stream, args, pg, device, sample_clocks: bool):
     results = [result_words(r, v, words) for r, v, words in sbufs]
     return {"ms_per_step": ms / args.steps, "scan_ms": tm.scan_ms, "launches_per_step": tm.gpu_launches,
             "graph": tm.graph, "path": "cube" if tm.mode == 1 else "masks", "tuning": {k: getattr(tun, k) for k, _ in _lib.Tuning._fields_} if tun else None,
-            "prog": prog, "squeries": squeries, "sparams": sparams, "sbufs": sbufs, "clocks": clocks}, results
+            "prog": prog, "squeries": squeries, "sparams": sparams, "sbufs": sbufs, "sarena": sarena,
+            "clocks": clocks}, results
 
 
 def e2e_shared(torch, db, plans, sh, stream, args, world):
     """The batch end to end through the public API: the query descriptors and
     literals uploaded, the shared scan, and every query's result and validity
-    words read back to pinned host memory, each step."""
+    words read back to pinned host memory (one copy of the batch's result
+    arena), each step."""
     sctx = db.ctx
-    sbufs = sh["sbufs"]
-    pinned = [torch.empty(r.numel(), dtype=torch.int64, pin_memory=True) for r, _, _ in sbufs]
-    pinned_v = [torch.empty(v.numel(), dtype=torch.int64, pin_memory=True) for _, v, _ in sbufs]
+    arena = sh["sarena"]
+    pinned = torch.empty(arena.numel(), dtype=torch.int64, pin_memory=True)
     h2d = len(sh["squeries"]) * 40 + len(sh["sparams"]) * 4
-    d2h = sum(p.numel() * 8 + q.numel() * 8 for p, q in zip(pinned, pinned_v))
+    d2h = pinned.numel() * 8
     steps = max(2, args.steps)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(steps):
         prog = db.shared_program(plans, db.shared_tuning_for(plans))
         sctx.shared_execute(prog.module, sh["squeries"], sh["sparams"], stream.cuda_stream)
-        for i, (r, v, _) in enumerate(sbufs):
-            pinned[i].copy_(r, non_blocking=True)
-            pinned_v[i].copy_(v, non_blocking=True)
+        with torch.cuda.stream(stream):
+            pinned.copy_(arena, non_blocking=True)
         stream.synchronize()
     e2e_s = time.perf_counter() - t0
     return {"value": len(plans) * steps * world / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": int(h2d),

@@ -56,7 +56,7 @@ class QueryResult:
 def shape_key(plan: Plan) -> str:
     """A plan's shape: its text with every integer literal abstracted.  Queries
     of one shape share a launch configuration."""
-    return re.sub(r"\(int -?\d+\)", "(int ?)", plan.text())
+    return plan.memo("shape", lambda: re.sub(r"\(int -?\d+\)", "(int ?)", plan.text()))
 
 
 DEFAULT_CANDIDATES = [
@@ -290,18 +290,30 @@ class Database:
 
     def shared_prepare(self, prog: SharedProgram, plans: list[Plan]):
         """Per-query result buffers, descriptors and the parameter array."""
+        queries, params, bufs, _ = self.shared_prepare_arena(prog, plans)
+        return queries, params, bufs
+
+    def shared_prepare_arena(self, prog: SharedProgram, plans: list[Plan]):
+        """As shared_prepare, with every query's result and validity words
+        placed in one device arena (16-byte aligned views), so that a batch's
+        results come back to the host in one copy; returns the arena too."""
         torch = self.torch
-        queries, params, bufs = [], [], []
+        lay, off = [], 0
         for p in plans:
-            s = prog.index[shape_key(p)]
             words = p.group_slots * p.storage_ts
-            res = torch.empty(max(words, 1), dtype=torch.int64, device=self.device)
-            val = torch.empty(max((words + 63) // 64, 1), dtype=torch.int64, device=self.device)
+            rw, vw = max(words, 1), max((words + 63) // 64, 1)
+            lay.append((words, off, rw, off + (rw + 1) // 2 * 2, vw))
+            off += (rw + 1) // 2 * 2 + (vw + 1) // 2 * 2
+        arena = torch.empty(max(off, 2), dtype=torch.int64, device=self.device)
+        queries, params, bufs = [], [], []
+        for p, (words, ro, rw, vo, vw) in zip(plans, lay):
+            s = prog.index[shape_key(p)]
+            res, val = arena[ro:ro + rw], arena[vo:vo + vw]
             lits = _lib.plan_literals(p.text())
             queries.append(_lib.SharedQuery(s, len(params), res.data_ptr(), res.numel(), val.data_ptr(), val.numel()))
             params.extend(lits)
             bufs.append((res, val, words))
-        return queries, params, bufs
+        return queries, params, bufs, arena
 
     def execute_shared(self, plans: list[Plan], tuning: _lib.Tuning | None = None,
                        stream=None) -> list[QueryResult]:
@@ -309,7 +321,7 @@ class Database:
         if tuning is None:
             tuning = self.shared_tuning_for(plans) or make_tuning(**SHARED_DEFAULT)
         prog = self.shared_program(plans, tuning)
-        queries, params, bufs = self.shared_prepare(prog, plans)
+        queries, params, bufs, arena = self.shared_prepare_arena(prog, plans)
         for t, n in self.rows.items():
             self.ctx.set_rows(t, n)
         s = stream if stream is not None else torch.cuda.current_stream()
@@ -322,10 +334,13 @@ class Database:
                 raise
             err = self.ctx.kernel_error()
         timing = self.ctx.timing()
+        host = arena.cpu().numpy().view(np.uint64)
+        base = arena.data_ptr()
         out = []
         for res, val, words in bufs:
-            w = res.cpu().numpy().view(np.uint64)[:words].copy()
-            v = val.cpu().numpy().view(np.uint64)[: (words + 63) // 64].copy()
+            ro, vo = (res.data_ptr() - base) // 8, (val.data_ptr() - base) // 8
+            w = host[ro:ro + words].copy()
+            v = host[vo:vo + (words + 63) // 64].copy()
             out.append(QueryResult(w, v, timing, err))
         return out
 

@@ -180,7 +180,24 @@ class Plan:
     def fact(self) -> Table:
         return next(t for t in self.tables if t.fact)
 
+    # A built plan is not changed in place; assigning any field drops what was
+    # derived from it (its text, its shape), so a query submitted again costs
+    # no re-rendering.
+    def __setattr__(self, name, value):
+        object.__setattr__(self, name, value)
+        if name != "_memo":
+            object.__setattr__(self, "_memo", {})
+
+    def memo(self, key: str, fn):
+        m = self.__dict__.setdefault("_memo", {})
+        if key not in m:
+            m[key] = fn()
+        return m[key]
+
     def text(self) -> str:
+        return self.memo("text", self._render)
+
+    def _render(self) -> str:
         out = ["(query"]
         for t in self.tables:
             out.append(f"  (table {t.name}{' fact' if t.fact else ''} (cols {' '.join(t.cols)}))")

@@ -31,7 +31,7 @@ def main(argv: list[str] | None = None) -> None:
     ap.add_argument("mode", choices=["shared", "plain", "tour"])
     ap.add_argument("--rows", type=int, default=30_000_000)
     ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--query", default="T1", help="T0..T3, q11, q31 or one of " + ", ".join(EXPANDING) +
+    ap.add_argument("--query", default="T1", help="T0..T3, q11, q31, q31n (nullable Q3.1) or one of " + ", ".join(EXPANDING) +
                     " (plain mode)")
     ap.add_argument("--template", type=int, default=-1, help="shared mode: draw every query from this template")
     ap.add_argument("--seed", type=int, default=2024)
@@ -46,13 +46,15 @@ def main(argv: list[str] | None = None) -> None:
         tour(args)
         return
     kw, shared_default, make_tuning = _tuning(args.tuning)
-    cols = {"q11": queries.Q11_COLS, "q31": queries.Q31_COLS}.get(args.query, queries.BATCH_COLS)
+    cols = {"q11": queries.Q11_COLS, "q31": queries.Q31_COLS, "q31n": queries.Q31_COLS}.get(args.query, queries.BATCH_COLS)
+    # The nullable Q3.1 shape reads 10 % NULL revenue and 5 % NULL c_city.
+    nulls = {"lo_revenue": 100, "c_city": 50} if args.query == "q31n" else None
     dims = ("DDATE", "CUSTOMER", "SUPPLIER", "PART")
     if args.query in EXPANDING:
         cols = sorted(set(queries.OR_COLS) | set(queries.MHT_COLS))
         dims = dims + ("PARTSUPP",)
     db = Database(0)
-    db.generate_ssb(args.rows, args.seed, queries.BATCH_COLS if args.mode == "shared" else cols, dims=dims)
+    db.generate_ssb(args.rows, args.seed, queries.BATCH_COLS if args.mode == "shared" else cols, nulls=nulls, dims=dims)
     if args.mode == "shared":
         if args.template >= 0:
             rng = random.Random(args.seed)
@@ -73,6 +75,8 @@ def main(argv: list[str] | None = None) -> None:
         plan = queries.ssb_q11(args.rows)
     elif q in EXPANDING:
         plan = getattr(queries, EXPANDING[q])(args.rows)
+    elif q == "q31n":
+        plan = queries.ssb_q31_nullable(args.rows)
     else:
         plan = queries.ssb_q31(args.rows)
     t = make_tuning(**kw) if kw else None

@@ -164,9 +164,21 @@ CX_DEVICE void WarpLoadTileV(const int* tile, int lane, int (&items)[IPT]) {
 template <int IPT>
 CX_DEVICE void WarpLoadValidityV(const uint64_t* null_bitmap, int lane, long long tile_offset, int (&valid)[IPT]) {
   constexpr int VW = IPT >= 4 ? 4 : IPT;
+  static_assert(IPT % VW == 0 && 64 % VW == 0, "items per thread must be 1, 2 or a multiple of 4");
+  if (null_bitmap == nullptr) {
 #pragma unroll
-  for (int i = 0; i < IPT; ++i)
-    valid[i] = ColumnValidAt(null_bitmap, tile_offset + (i / VW) * 32 * VW + lane * VW + i % VW);
+    for (int i = 0; i < IPT; ++i) valid[i] = 1;
+    return;
+  }
+  // A lane's VW rows start at a multiple of VW (tile_offset is a multiple of
+  // 32 * IPT), so they share one word: one load per vector, not per row.
+#pragma unroll
+  for (int j = 0; j < IPT / VW; ++j) {
+    const long long base = tile_offset + (long long)j * 32 * VW + lane * VW;
+    const uint64_t bits = null_bitmap[base >> 6] >> (base & 63);
+#pragma unroll
+    for (int k = 0; k < VW; ++k) valid[j * VW + k] = (int)((bits >> k) & 1ULL);
+  }
 }
 
 template <int BLOCK_THREADS, int ITEMS_PER_THREAD>

@@ -245,7 +245,8 @@ PLAIN_CANDIDATES = [dict(block_threads=bt, items_per_thread=ipt, stages=st, ctas
                         (512, 8, 4, 0, 0, 0, 0, 0), (1024, 4, 0, 49152, 1, 0, 1, 98304),
                         (512, 4, 0, 49152, 1, 0, 1, 98304), (1024, 2, 0, 49152, 1, 0, 1, 98304),
                         (1024, 2, 0, 49152, 1, 0, 1, 0), (1024, 4, 0, 49152, 1, 0, 2, 0),
-                        (1024, 2, 0, 49152, 1, 0, 2, 0), (1024, 4, 0, 49152, 3, 0, 0, 98304))]
+                        (1024, 2, 0, 49152, 1, 0, 2, 0), (1024, 4, 0, 49152, 3, 0, 0, 98304),
+                        (1024, 8, 0, 49152, 1, 0, 2, 0))]
 # Per-query mask path (cube = 0) launch shapes, then the aggregate-cube path at
 # 1, 2 and 4 rows per lane (the runtime falls back to the mask path when the
 # batch's attribute ranges do not allow cubes).

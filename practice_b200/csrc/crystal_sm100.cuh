@@ -568,28 +568,36 @@ CX_DEVICE void BlockProbeBitmapAnd(int tid, K (&items)[ITEMS_PER_THREAD], int (&
 // [key_min, key_min + len) that bit is the probe's answer (HASH maps the key
 // to slot key - key_min), so no table access is needed; a key outside the
 // window falls back to the full probe of `ht` (`pair` = 1 for [key, payload]
-// slots).  Clears the flag of every item that misses; no branch for in-window
-// keys.  No counterpart in the reference API.
+// slots).  Clears the flag of every item that misses.  The in-window test is
+// branch-free (an outside key reads bit 0 of word 0 and masks it off); the
+// items with an outside key and a set flag are probed afterwards, behind one
+// branch per call instead of one per item.  No counterpart in the reference
+// API.
 template <typename K, int BLOCK_THREADS, int ITEMS_PER_THREAD>
 CX_DEVICE void BlockProbeExactBitmap(int tid, K (&items)[ITEMS_PER_THREAD], int (&flags)[ITEMS_PER_THREAD],
                                      const unsigned int* bitmap, const K* ht, int pair, int ht_len, K key_min,
                                      int num_items) {
+  static_assert(ITEMS_PER_THREAD <= 32, "one bit per item");
   const bool guarded = !cx_detail::tile_is_full<BLOCK_THREADS, ITEMS_PER_THREAD>(num_items);
+  unsigned outside = 0u;  // bit i: item i's key lies outside the window and its flag is set
 #pragma unroll
   for (int i = 0; i < ITEMS_PER_THREAD; ++i) {
-    if (guarded && i * BLOCK_THREADS + tid >= num_items) continue;
+    const bool live = !guarded || i * BLOCK_THREADS + tid < num_items;
     const K d = items[i] - key_min;
-    int hit;
-    if (sizeof(K) == 4 ? (unsigned)d < (unsigned)ht_len : (d >= K(0) && d < K(ht_len))) {
-      hit = (int)((bitmap[(unsigned)d >> 5] >> ((unsigned)d & 31u)) & 1u);
-    } else {
-      hit = 0;
-      if (flags[i]) {
-        const int h = cx_detail::pht_slot<K>(items[i], ht_len, key_min);
-        hit = (h >= 0 && ht[(long long)h << pair] == items[i]) ? 1 : 0;
-      }
+    const bool in = sizeof(K) == 4 ? (unsigned)d < (unsigned)ht_len : (d >= K(0) && d < K(ht_len));
+    const unsigned o = in ? (unsigned)d : 0u;
+    const int hit = (int)((bitmap[o >> 5] >> (o & 31u)) & 1u) & (int)in;
+    const int f = (int)(flags[i] != 0);
+    outside |= (unsigned)(live && !in && f) << i;
+    flags[i] = live ? (f & hit) : flags[i];
+  }
+  if (outside) {
+#pragma unroll
+    for (int i = 0; i < ITEMS_PER_THREAD; ++i) {
+      if (!((outside >> i) & 1u)) continue;
+      const int h = cx_detail::pht_slot<K>(items[i], ht_len, key_min);
+      flags[i] = (h >= 0 && ht[(long long)h << pair] == items[i]) ? 1 : 0;
     }
-    flags[i] = (int)(flags[i] != 0) & hit;
   }
 }
 

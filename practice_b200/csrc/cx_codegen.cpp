@@ -34,25 +34,43 @@ namespace {
 bool lit_true(const std::string& v) { return v == "1" || v == "true" || v == "(1)" || v == "(true)"; }
 bool lit_false(const std::string& v) { return v == "0" || v == "false" || v == "(0)" || v == "(false)"; }
 
+// Eager mode: conjunctions and disjunctions are emitted as `&` / `|` over
+// operands converted to bool, so the generated code evaluates every operand
+// and needs no branch per short-circuit.  Only for expressions whose operands
+// are safe to evaluate whatever the others' values (registers, literals,
+// parameters and the total db::safe_* functions): the fact-filter conditions.
+thread_local bool g_eager = false;
+struct EagerScope {
+  bool prev;
+  EagerScope() : prev(g_eager) { g_eager = true; }
+  ~EagerScope() { g_eager = prev; }
+};
+std::string eager_term(const std::string& t) { return "(bool)(" + t + ")"; }
+
 std::string and_terms(const std::vector<std::string>& terms) {
   std::string out;
+  int n = 0;
   for (const auto& t : terms) {
     if (t.empty() || lit_true(t)) continue;
-    if (!out.empty()) out += " && ";
-    out += t;
+    if (!out.empty()) out += g_eager ? " & " : " && ";
+    out += g_eager ? eager_term(t) : t;
+    ++n;
   }
-  return out.empty() ? "1" : out;
+  if (out.empty()) return "1";
+  return g_eager && n > 1 ? "(" + out + ")" : out;
 }
 std::string b_and(const std::string& a, const std::string& b) {
   if (lit_false(a) || lit_false(b)) return "0";
   if (lit_true(a)) return b;
   if (lit_true(b)) return a;
+  if (g_eager) return "(" + eager_term(a) + " & " + eager_term(b) + ")";
   return "(" + a + " && " + b + ")";
 }
 std::string b_or(const std::string& a, const std::string& b) {
   if (lit_true(a) || lit_true(b)) return "1";
   if (lit_false(a)) return b;
   if (lit_false(b)) return a;
+  if (g_eager) return "(" + eager_term(a) + " | " + eager_term(b) + ")";
   return "(" + a + " || " + b + ")";
 }
 std::string b_not(const std::string& a) {
@@ -277,11 +295,16 @@ struct Emitter {
         << e->kids[0]->name << ", flags, " << int_lit(e->kids[1].get()) << ", num_tile_items);\n";
       return;
     }
-    const std::string cond = and_terms({valid_of(e), value_of(e)});
+    std::string cond;
+    {
+      EagerScope eager;  // the whole condition evaluated without branches
+      cond = and_terms({valid_of(e), value_of(e)});
+    }
     if (lit_true(cond)) return;
     o << ind << "#pragma unroll\n"
       << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n"
-      << ind << "  if (tid + BLOCK_THREADS * i < num_tile_items) flags[i] = flags[i] && (" << cond << ");\n"
+      << ind << "  flags[i] = (tid + BLOCK_THREADS * i < num_tile_items) ? ((int)(flags[i] != 0) & (int)(bool)(" << cond
+      << ")) : flags[i];\n"
       << ind << "}\n";
   }
 

@@ -928,6 +928,18 @@ CX_DEVICE void bulk_g2s(void* smem_dst, const void* gmem_src, unsigned bytes, un
       : "memory");
 }
 
+// Store of one 32-bit word to shared memory under a predicate: a lane whose
+// predicate is false issues nothing, and no branch is needed around the store.
+// `addr` must point into shared memory (it is converted to a shared-window
+// address); it is not accessed when `pred` is false.
+CX_DEVICE void st_shared_if(bool pred, int* addr, int v) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(addr);
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %2, 0;\n\t@p st.shared.b32 [%0], %1;\n\t}" ::"r"(a), "r"(v),
+      "r"((unsigned)pred)
+      : "memory");
+}
+
 // Bulk prefetch of `bytes` of global memory into L2 (no destination, no
 // completion to wait for): a warp asks for its next tile's columns a tile ahead
 // at no register cost.  Address 16-byte aligned, bytes a multiple of 16, the

@@ -1556,16 +1556,16 @@ struct Emitter {
       o << ind << "#pragma unroll\n" << ind << "for (int i = 0; i < ITEMS_PER_THREAD; ++i) {\n";
       o << ind << "  const bool f_ = flags[i] && (tid + BLOCK_THREADS * i < num_tile_items);\n";
       o << ind << "  const unsigned m_ = __ballot_sync(0xffffffffu, f_);\n";
-      o << ind << "  if (f_) {\n";
-      o << ind << "    const int p_ = q_n + __popc(m_ & ((1u << lane) - 1u));\n";
+      // Every lane computes its slot (at most q_n + 31, inside the queue);
+      // only qualifying lanes store, by predicated stores without a branch.
+      o << ind << "  const int p_ = q_n + __popc(m_ & ((1u << lane) - 1u));\n";
       {
         int qi = 0;
         for (const auto& c : qcols) {
-          o << ind << "    q_base[" << qi++ * QCAP << " + p_] = " << c << "[i];\n";
-          if (nullable(c)) o << ind << "    q_base[" << qi++ * QCAP << " + p_] = " << c << "_valid[i];\n";
+          o << ind << "  cx::st_shared_if(f_, &q_base[" << qi++ * QCAP << " + p_], " << c << "[i]);\n";
+          if (nullable(c)) o << ind << "  cx::st_shared_if(f_, &q_base[" << qi++ * QCAP << " + p_], " << c << "_valid[i]);\n";
         }
       }
-      o << ind << "  }\n";
       o << ind << "  q_n += __popc(m_);\n";
       o << ind << "}\n";
       o << "   }\n";  // live_

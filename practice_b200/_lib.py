@@ -90,6 +90,10 @@ class Timing(C.Structure):
                 ("mode", C.c_int)]
 
 
+# CX_ABI_VERSION of include/crystal_b200.h that the structures above mirror.
+ABI_VERSION = 1
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(f"{LIB_PATH} is not built; run `python -m practice_b200.build`")
@@ -148,6 +152,9 @@ def _load() -> C.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+    if lib.cx_abi_version() != ABI_VERSION:
+        raise ImportError(f"{LIB_PATH} has C ABI version {lib.cx_abi_version()}, these bindings expect "
+                          f"{ABI_VERSION}; rebuild with `python -m practice_b200.build`")
     return lib
 
 

@@ -384,3 +384,42 @@ def test_cube_scan_region_compiles_with_its_layout_as_constants():
         f"#define {name} ({values.get(field, 3)}{'LL' if field == 'cube_cells' else ''})\n" for name, field, _ in defaults)
     spec = "/*@cx-launch\nv 1\n@*/\n" + src[p0:p1] + "\n" + defs + region
     _lib.Module(spec, key="cube_layout_constants")
+
+
+@pytest.mark.parametrize("bt,ipt,compact", [(1024, 4, 1), (1024, 4, 2), (512, 2, 1), (1024, 8, 2), (256, 1, 1)])
+def test_compaction_queue_slots_stay_inside_the_warp_queue(bt, ipt, compact):
+    """Every lane computes its queue slot (q_n + its rank among the
+    qualifying lanes) and only qualifying lanes store, by predicated stores:
+    the slot of every lane must still lie inside its column's queue.  The
+    queue layout and the drain size are read from the generated scan; the
+    warp's queue is then driven with worst-case ballots (all lanes
+    qualifying) and random ones."""
+    import random as _random
+    import re as _re
+
+    t = _lib.default_tuning()
+    t.block_threads, t.items_per_thread, t.compact = bt, ipt, compact
+    src = None
+    for name in ("ssb_q31_nullable", "T1"):  # the first that fits this launch shape's shared memory
+        try:
+            src = _lib.codegen(all_plans()[name].text(), t)
+            break
+        except _lib.CxError:
+            continue
+    assert src is not None
+    offs = sorted(int(x) for x in _re.findall(r"st_shared_if\(f_, &q_base\[(\d+) \+ p_\]", src))
+    per_warp = int(_re.search(r"\(long long\)warp \* (\d+)LL; \(void\)q_base;", src).group(1))
+    drain = int(_re.search(r"while \(q_n >= (\d+) \|\|", src).group(1))
+    assert offs and offs[0] == 0
+    cap = offs[1] - offs[0] if len(offs) > 1 else per_warp
+    assert all(b - a == cap for a, b in zip(offs, offs[1:])) and offs[-1] + cap == per_warp
+    rng = _random.Random(bt * 131 + ipt * 7 + compact)
+    for trial in range(200):
+        q_n = 0
+        for _tile in range(50):
+            for _item in range(ipt):
+                ballot = 32 if trial % 2 == 0 else rng.choice((0, 1, 5, 31, 32))
+                assert q_n + 31 < cap  # the highest slot any lane computes
+                q_n += ballot
+            while q_n >= drain:
+                q_n -= drain

@@ -1,0 +1,167 @@
+"""Device primitives of `crystal_sm100.cuh` compiled for the host and checked
+against their per-row definitions on the CPU.
+
+`BlockProbeExactBitmap` (exact membership from a shared-memory slot bitmap,
+branch-free for in-window keys, outside keys probed through the PHT) and
+`WarpLoadValidityV` (validity bits of a vector-striped tile, one word load per
+lane vector) are plain C++ once `CX_DEVICE` is defined for the host: their
+source is taken from the header as it ships, compiled with g++, and compared
+with the reference semantics they must keep -- the PHT probe of
+`include/crystal/join.h:7-60` (a key is a member when the slot `HASH` gives
+holds it) and `ColumnValidAt` of `include/crystal/load.h:72-76` (bit r of the
+uint64 word array).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import random
+import re
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+HEADER = Path(__file__).resolve().parent.parent / "practice_b200" / "csrc" / "crystal_sm100.cuh"
+GXX = shutil.which("g++") or "/usr/bin/g++"
+
+
+def _function(src: str, name: str) -> str:
+    """The template header and body of device function `name`."""
+    m = re.search(r"(template <[^\n]*>\n)?CX_DEVICE [^\n]*\b" + name + r"\(", src)
+    assert m, name
+    i = src.index("{", m.end())
+    depth = 0
+    for j in range(i, len(src)):
+        depth += {"{": 1, "}": -1}.get(src[j], 0)
+        if depth == 0:
+            return src[m.start():j + 1]
+    raise AssertionError(f"unbalanced braces in {name}")
+
+
+@pytest.fixture(scope="module")
+def lib(tmp_path_factory):
+    if not os.path.exists(GXX):
+        pytest.skip("needs a host C++ compiler")
+    src = HEADER.read_text()
+    prelude = src[:src.index("}  // namespace cx_detail") + len("}  // namespace cx_detail")]
+    prelude = prelude[prelude.index("#if defined(__CUDACC_RTC__)"):]
+    parts = ["#define CX_DEVICE static inline", prelude,
+             _function(src, "ColumnValidAt"), _function(src, "WarpLoadValidityV"),
+             _function(src, "BlockProbeExactBitmap")]
+    parts.append("""
+template <int IPT>
+static void probe_t(int tid, int num_items, const int* items_in, int* flags_io, const unsigned* bitmap,
+                    const int* ht, int pair, int len, int key_min) {
+  int items[IPT], flags[IPT];
+  for (int i = 0; i < IPT; ++i) { items[i] = items_in[i]; flags[i] = flags_io[i]; }
+  BlockProbeExactBitmap<int, 32, IPT>(tid, items, flags, bitmap, ht, pair, len, key_min, num_items);
+  for (int i = 0; i < IPT; ++i) flags_io[i] = flags[i];
+}
+extern "C" void probe4(int tid, int n, const int* it, int* fl, const unsigned* bm, const int* ht, int pair, int len,
+                       int kmin) { probe_t<4>(tid, n, it, fl, bm, ht, pair, len, kmin); }
+extern "C" void probe2(int tid, int n, const int* it, int* fl, const unsigned* bm, const int* ht, int pair, int len,
+                       int kmin) { probe_t<2>(tid, n, it, fl, bm, ht, pair, len, kmin); }
+template <int IPT>
+static void valid_t(const uint64_t* bm, int lane, long long tile_offset, int* out) {
+  int v[IPT];
+  WarpLoadValidityV<IPT>(bm, lane, tile_offset, v);
+  for (int i = 0; i < IPT; ++i) out[i] = v[i];
+}
+extern "C" void valid1(const uint64_t* bm, int lane, long long off, int* out) { valid_t<1>(bm, lane, off, out); }
+extern "C" void valid2(const uint64_t* bm, int lane, long long off, int* out) { valid_t<2>(bm, lane, off, out); }
+extern "C" void valid4(const uint64_t* bm, int lane, long long off, int* out) { valid_t<4>(bm, lane, off, out); }
+extern "C" void valid8(const uint64_t* bm, int lane, long long off, int* out) { valid_t<8>(bm, lane, off, out); }
+""")
+    d = tmp_path_factory.mktemp("prims")
+    cpp, so = d / "prims.cpp", d / "libprims.so"
+    cpp.write_text("\n".join(parts) + "\n")
+    subprocess.run([GXX, "-O1", "-std=c++17", "-shared", "-fPIC", "-Wno-unknown-pragmas", "-o", str(so), str(cpp)],
+                   check=True)
+    return ctypes.CDLL(str(so))
+
+
+def _c_mod(a: int, b: int) -> int:
+    """C's % on ints: the remainder takes the dividend's sign."""
+    r = abs(a) % abs(b)
+    return -r if a < 0 else r
+
+
+def _slot(key: int, length: int, key_min: int) -> int:
+    d = key - key_min
+    if 0 <= d < length:
+        return d
+    h = _c_mod(key - key_min, length)
+    return h if 0 <= h < length else -1
+
+
+def _pht(rng: random.Random, length: int, key_min: int, pair: int):
+    """A PHT of `length` slots filled from keys around its window (first key
+    into a slot wins), and its exact membership bitmap (bit h set when slot h
+    holds key_min + h)."""
+    ht = np.zeros(length << pair, dtype=np.int32)
+    for _ in range(length):
+        k = rng.randint(key_min - 3 * length, key_min + 4 * length)
+        h = _slot(k, length, key_min)
+        if h >= 0 and ht[h << pair] == 0:
+            ht[h << pair] = k
+            if pair:
+                ht[(h << 1) + 1] = rng.randint(0, 99)
+    bm = np.zeros((length + 31) // 32, dtype=np.uint32)
+    for h in range(length):
+        if ht[h << pair] == key_min + h:
+            bm[h >> 5] |= np.uint32(1 << (h & 31))
+    return ht, bm
+
+
+@pytest.mark.parametrize("ipt", [2, 4])
+@pytest.mark.parametrize("pair", [0, 1])
+def test_exact_bitmap_probe_matches_the_pht_probe(lib, ipt, pair):
+    rng = random.Random(1000 * ipt + pair)
+    fn = getattr(lib, f"probe{ipt}")
+    ip = ctypes.POINTER(ctypes.c_int)
+    up = ctypes.POINTER(ctypes.c_uint)
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ip, ip, up, ip, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    for trial in range(300):
+        length = rng.choice((1, 7, 32, 100, 1000))
+        key_min = rng.choice((1000, 19920101, -500))
+        ht, bm = _pht(rng, length, key_min, pair)
+        stored = [int(k) for k in ht[::1 << pair] if k != 0]
+        tid = rng.randrange(32)
+        n = 32 * ipt if rng.random() < 0.5 else rng.randint(0, 32 * ipt)
+        items = np.array([rng.choice(stored) if stored and rng.random() < 0.5 else
+                          rng.randint(key_min - 5 * length, key_min + 6 * length) for _ in range(ipt)], dtype=np.int32)
+        flags = np.array([rng.choice((0, 1, 1, 2)) for _ in range(ipt)], dtype=np.int32)
+        want = flags.copy()
+        for i in range(ipt):
+            if n == 32 * ipt or i * 32 + tid < n:  # live item: the flag keeps only members
+                h = _slot(int(items[i]), length, key_min)
+                hit = h >= 0 and int(ht[h << pair]) == int(items[i])
+                want[i] = int(flags[i] != 0 and hit)
+        got = flags.copy()
+        fn(tid, n, items.ctypes.data_as(ip), got.ctypes.data_as(ip), bm.ctypes.data_as(up), ht.ctypes.data_as(ip),
+           pair, length, key_min)
+        assert np.array_equal(got, want), (trial, length, key_min, tid, n, items, flags, got, want)
+
+
+@pytest.mark.parametrize("ipt", [1, 2, 4, 8])
+def test_vector_validity_bits_match_column_valid_at(lib, ipt):
+    rng = np.random.default_rng(ipt)
+    words = rng.integers(0, 2 ** 64, size=64, dtype=np.uint64)
+    fn = getattr(lib, f"valid{ipt}")
+    vw = min(ipt, 4)
+    out = np.zeros(ipt, dtype=np.int32)
+    u64p, ip = ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int)
+    fn.argtypes = [u64p, ctypes.c_int, ctypes.c_longlong, ip]
+    tiles = (64 * 64) // (32 * ipt)
+    for t in range(tiles):
+        off = t * 32 * ipt
+        for lane in range(32):
+            fn(words.ctypes.data_as(u64p), lane, off, out.ctypes.data_as(ip))
+            for i in range(ipt):
+                r = off + (i // vw) * 32 * vw + lane * vw + i % vw
+                assert out[i] == (int(words[r >> 6]) >> (r & 63)) & 1, (t, lane, i)
+            fn(None, lane, off, out.ctypes.data_as(ip))  # no bitmap: every row valid
+            assert out.tolist() == [1] * ipt

@@ -4,8 +4,8 @@ the CPU.
 The scan kernel evaluates every non-trivial filter leaf as one expression per
 row, with `&` / `|` over operands converted to bool (no short-circuit branch).
 These tests take the emitted conditions of seeded random predicates over three
-nullable int columns, compile them for the host with g++ (the `db::safe_*`
-helpers restated as plain integer functions), and compare the rows they keep,
+nullable int columns, compile them for the host with g++ (with the header's own `db::safe_*`
+helpers), and compare the rows they keep,
 over every combination of a few values and NULL, with an independent Python
 evaluation of SQL's three-valued logic: WHERE keeps a row only when the
 predicate is TRUE (AND is FALSE if either side is, OR is TRUE if either side
@@ -21,6 +21,7 @@ import os
 import random
 import shutil
 import subprocess
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -33,20 +34,16 @@ VALUES = (-2, 0, 1, 3, 5)
 PREFIX = "flags[i] = (tid + BLOCK_THREADS * i < num_tile_items) ? ((int)(flags[i] != 0) & (int)(bool)("
 SUFFIX = ")) : flags[i];"
 
-HOST_SAFE = """
-namespace db {
-template <class A, class B> long long safe_add(A a, B b) { return (long long)a + (long long)b; }
-template <class A, class B> long long safe_sub(A a, B b) { return (long long)a - (long long)b; }
-template <class A, class B> long long safe_mul(A a, B b) { return (long long)a * (long long)b; }
-template <class A, class B> long long safe_div(A a, B b) { return (long long)b == 0 ? 0 : (long long)a / (long long)b; }
-template <class A, class B> int safe_lt(A a, B b) { return (long long)a < (long long)b; }
-template <class A, class B> int safe_gt(A a, B b) { return (long long)a > (long long)b; }
-template <class A, class B> int safe_lte(A a, B b) { return (long long)a <= (long long)b; }
-template <class A, class B> int safe_gte(A a, B b) { return (long long)a >= (long long)b; }
-template <class A, class B> int safe_eq(A a, B b) { return (long long)a == (long long)b; }
-template <class A, class B> int safe_neq(A a, B b) { return (long long)a != (long long)b; }
-}
-"""
+HEADER = Path(__file__).resolve().parent.parent / "practice_b200" / "csrc" / "crystal_sm100.cuh"
+
+
+def _host_safe_helpers() -> str:
+    """The `db::safe_*` helpers of the shipped header (its integer part, up to
+    the atomics), compiled for the host."""
+    src = HEADER.read_text()
+    i = src.index("namespace db {")
+    j = src.index("CX_DEVICE unsigned long long bit_cast_double_to_ull", i)
+    return "#include <cstdint>\n#define CX_DEVICE static inline\n" + src[i:j] + "}  // namespace db\n"
 
 
 # ------------------------------------------------------------ random predicates
@@ -138,7 +135,7 @@ def _conditions(pred) -> list[str]:
 
 
 def _compile(funcs: list[list[str]], tmp_path) -> ctypes.CDLL:
-    body = [HOST_SAFE]
+    body = [_host_safe_helpers()]
     for k, conds in enumerate(funcs):
         body.append(f'extern "C" void eval_{k}(int n, const int* A, const int* AV, const int* B, const int* BV, '
                     "const int* C, const int* CV, int* out) {")

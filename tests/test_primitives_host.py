@@ -48,9 +48,13 @@ def lib(tmp_path_factory):
     src = HEADER.read_text()
     prelude = src[:src.index("}  // namespace cx_detail") + len("}  // namespace cx_detail")]
     prelude = prelude[prelude.index("#if defined(__CUDACC_RTC__)"):]
-    parts = ["#define CX_DEVICE static inline", prelude,
+    # One host thread: a compare-and-swap is a plain read and conditional write.
+    stubs = ("struct int2 { int x, y; };\n"
+             "template <class T> static T atomicCAS(T* a, T cmp, T v) { T old = *a; if (old == cmp) *a = v; return old; }\n")
+    parts = ["#define CX_DEVICE static inline", prelude, stubs,
              _function(src, "ColumnValidAt"), _function(src, "WarpLoadValidityV"),
-             _function(src, "BlockProbeExactBitmap")]
+             _function(src, "BlockProbeExactBitmap"),
+             "namespace cx_detail {", _function(src, "pht_probe"), _function(src, "pht_build"), "}"]
     parts.append("""
 template <int IPT>
 static void probe_t(int tid, int num_items, const int* items_in, int* flags_io, const unsigned* bitmap,
@@ -74,6 +78,27 @@ extern "C" void valid1(const uint64_t* bm, int lane, long long off, int* out) { 
 extern "C" void valid2(const uint64_t* bm, int lane, long long off, int* out) { valid_t<2>(bm, lane, off, out); }
 extern "C" void valid4(const uint64_t* bm, int lane, long long off, int* out) { valid_t<4>(bm, lane, off, out); }
 extern "C" void valid8(const uint64_t* bm, int lane, long long off, int* out) { valid_t<8>(bm, lane, off, out); }
+template <bool PAIR>
+static void build_t(int tid, int n, const int* k_in, const int* v_in, const int* f_in, int* ht, int len, int kmin) {
+  int keys[4], vals[4], flags[4];
+  for (int i = 0; i < 4; ++i) { keys[i] = k_in[i]; vals[i] = v_in[i]; flags[i] = f_in[i]; }
+  cx_detail::pht_build<int, int, 32, 4, PAIR>(tid, keys, vals, flags, ht, len, kmin, n, n != 128);
+}
+template <bool PAIR>
+static void pprobe_t(int tid, int n, const int* k_in, int* f_io, int* res, const int* ht, int len, int kmin) {
+  int items[4], flags[4];
+  for (int i = 0; i < 4; ++i) { items[i] = k_in[i]; flags[i] = f_io[i]; }
+  cx_detail::pht_probe<int, int, 32, 4, PAIR>(tid, items, res, flags, ht, len, kmin, n, n != 128);
+  for (int i = 0; i < 4; ++i) f_io[i] = flags[i];
+}
+extern "C" void build1(int tid, int n, const int* k, const int* v, const int* f, int* ht, int len, int kmin) {
+  build_t<false>(tid, n, k, v, f, ht, len, kmin); }
+extern "C" void build2(int tid, int n, const int* k, const int* v, const int* f, int* ht, int len, int kmin) {
+  build_t<true>(tid, n, k, v, f, ht, len, kmin); }
+extern "C" void pprobe1(int tid, int n, const int* k, int* f, int* res, const int* ht, int len, int kmin) {
+  pprobe_t<false>(tid, n, k, f, res, ht, len, kmin); }
+extern "C" void pprobe2(int tid, int n, const int* k, int* f, int* res, const int* ht, int len, int kmin) {
+  pprobe_t<true>(tid, n, k, f, res, ht, len, kmin); }
 """)
     d = tmp_path_factory.mktemp("prims")
     cpp, so = d / "prims.cpp", d / "libprims.so"
@@ -165,3 +190,76 @@ def test_vector_validity_bits_match_column_valid_at(lib, ipt):
                 assert out[i] == (int(words[r >> 6]) >> (r & 63)) & 1, (t, lane, i)
             fn(None, lane, off, out.ctypes.data_as(ip))  # no bitmap: every row valid
             assert out.tolist() == [1] * ipt
+
+
+@pytest.mark.parametrize("pair", [0, 1])
+def test_pht_build_then_probe_match_the_reference_rules(lib, pair):
+    """Build (`BlockBuildSelectivePHT_1/2`: compare-and-swap of the key into
+    the slot `HASH` gives; a pair slot takes the payload when the slot was empty
+    or already held the key) then probe (`BlockProbeAndPHT_1/2`: a member when
+    the slot holds the key, the payload read beside it), item by item in the
+    same order as a sequential model; keys around and outside the window,
+    partial tiles, flags cleared or of any value, odd table addresses (no
+    8-byte pair load) and aligned ones."""
+    rng = random.Random(77 + pair)
+    ip = ctypes.POINTER(ctypes.c_int)
+    build = getattr(lib, f"build{pair + 1}")
+    probe = getattr(lib, f"pprobe{pair + 1}")
+    build.argtypes = [ctypes.c_int, ctypes.c_int, ip, ip, ip, ip, ctypes.c_int, ctypes.c_int]
+    probe.argtypes = [ctypes.c_int, ctypes.c_int, ip, ip, ip, ip, ctypes.c_int, ctypes.c_int]
+    for trial in range(200):
+        length = rng.choice((1, 5, 64, 300))
+        key_min = rng.choice((1, 1000, 19920101))
+        width = length << pair
+        backing = np.zeros(width + 1, dtype=np.int32)
+        ht = backing[1:] if trial % 2 else backing[:-1]  # odd trials: table at a 4-byte, not 8-byte, boundary
+        model = np.zeros(width, dtype=np.int64)
+        for _tile in range(6):
+            tid = rng.randrange(32)
+            n = 128 if rng.random() < 0.5 else rng.randint(0, 128)
+            keys = np.array([rng.randint(key_min - 2 * length, key_min + 3 * length) or 1 for _ in range(4)],
+                            dtype=np.int32)
+            vals = np.array([rng.randint(1, 50) for _ in range(4)], dtype=np.int32)
+            flags = np.array([rng.choice((0, 1, 3)) for _ in range(4)], dtype=np.int32)
+            for i in range(4):
+                if not (n == 128 or i * 32 + tid < n) or not flags[i]:
+                    continue
+                h = _slot(int(keys[i]), length, key_min)
+                if h < 0:
+                    continue
+                if pair:
+                    prev = model[2 * h]
+                    if prev == 0:
+                        model[2 * h] = keys[i]
+                    if prev == 0 or prev == keys[i]:
+                        model[2 * h + 1] = vals[i]
+                elif model[h] == 0:
+                    model[h] = keys[i]
+            build(tid, n, keys.ctypes.data_as(ip), vals.ctypes.data_as(ip), flags.ctypes.data_as(ip),
+                  ht.ctypes.data_as(ip), length, key_min)
+        assert np.array_equal(ht.astype(np.int64), model), trial
+        stored = [int(k) for k in model[::1 << pair] if k != 0]
+        for _tile in range(6):
+            tid = rng.randrange(32)
+            n = 128 if rng.random() < 0.5 else rng.randint(0, 128)
+            items = np.array([rng.choice(stored) if stored and rng.random() < 0.6 else
+                              rng.randint(key_min - 3 * length, key_min + 4 * length) for _ in range(4)], dtype=np.int32)
+            flags = np.array([rng.choice((0, 1, 2)) for _ in range(4)], dtype=np.int32)
+            res = np.full(4, -7, dtype=np.int32)
+            want_f, want_r = flags.copy(), res.copy()
+            for i in range(4):
+                if not (n == 128 or i * 32 + tid < n) or not flags[i]:
+                    continue
+                h = _slot(int(items[i]), length, key_min)
+                if h < 0:
+                    want_f[i] = 0
+                elif pair:
+                    if model[2 * h] == items[i]:
+                        want_r[i] = model[2 * h + 1]
+                    else:
+                        want_f[i] = 0
+                else:
+                    want_f[i] = int(model[h] == items[i])
+            probe(tid, n, items.ctypes.data_as(ip), flags.ctypes.data_as(ip), res.ctypes.data_as(ip),
+                  ht.ctypes.data_as(ip), length, key_min)
+            assert np.array_equal(flags, want_f) and np.array_equal(res, want_r), (trial, items, flags, want_f)

@@ -612,11 +612,16 @@ def serving_leg(db, args, shared_tuning):
     # the one-off dimension checks; the timed streams start after them.
     warm_texts = [p.text() for p in queries.serving_stream(args.serve_warm, args.seed + 13, args.rows)]
 
+    warm_failed = []
+
     def warm(srv):
         ids = [srv.submit(t) for t in warm_texts]
+        bad = 0
         for rid in ids:
-            srv.wait(rid)
+            info = srv.wait(rid)
+            bad += int(info.status != 0 or info.kernel_error != 0)
             srv.release(rid)
+        warm_failed.append(bad)
 
     def stream(srv, rate, first, n):
         rng = np.random.default_rng(args.seed + int(rate))
@@ -716,6 +721,7 @@ def serving_leg(db, args, shared_tuning):
                         "failed": bad, "launches": int(st.launches), "mean_batch": st.mean_batch}
     finally:
         srv.close()
+    out["warmup_failed"] = sum(warm_failed)
     return out
 
 

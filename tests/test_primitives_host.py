@@ -2,14 +2,15 @@
 against their per-row definitions on the CPU.
 
 `BlockProbeExactBitmap` (exact membership from a shared-memory slot bitmap,
-branch-free for in-window keys, outside keys probed through the PHT) and
+branch-free for in-window keys, outside keys probed through the PHT),
 `WarpLoadValidityV` (validity bits of a vector-striped tile, one word load per
-lane vector) are plain C++ once `CX_DEVICE` is defined for the host: their
-source is taken from the header as it ships, compiled with g++, and compared
-with the reference semantics they must keep -- the PHT probe of
-`include/crystal/join.h:7-60` (a key is a member when the slot `HASH` gives
-holds it) and `ColumnValidAt` of `include/crystal/load.h:72-76` (bit r of the
-uint64 word array).
+lane vector), the PHT build and probe cores and the `BlockPred*` predicates are
+plain C++ once `CX_DEVICE` is defined for the host: their source is taken from
+the header as it ships, compiled with g++, and compared with the reference
+semantics they must keep -- the PHT build and probe of
+`include/crystal/join.h:7-160` (a key is a member when the slot `HASH` gives
+holds it), `ColumnValidAt` of `include/crystal/load.h:72-76` (bit r of the
+uint64 word array) and the set / AND / OR rules of `include/crystal/pred.h`.
 """
 from __future__ import annotations
 
@@ -263,3 +264,75 @@ def test_pht_build_then_probe_match_the_reference_rules(lib, pair):
             probe(tid, n, items.ctypes.data_as(ip), flags.ctypes.data_as(ip), res.ctypes.data_as(ip),
                   ht.ctypes.data_as(ip), length, key_min)
             assert np.array_equal(flags, want_f) and np.array_equal(res, want_r), (trial, items, flags, want_f)
+
+
+PRED_OPS = {"LT": "<", "GT": ">", "LTE": "<=", "GTE": ">=", "Eq": "==", "NEq": "!="}
+# Literal forms (pred.h:153-260): set, AND and OR variants; the OR form of Eq/NEq is spelled BlockPredOr<Op>.
+LITERAL_PREDS = [(f"BlockPred{op}", op, "set") for op in PRED_OPS] + \
+                [(f"BlockPredA{op}", op, "and") for op in PRED_OPS] + \
+                [(f"BlockPredOr{op}" if op in ("Eq", "NEq") else f"BlockPredO{op}", op, "or") for op in PRED_OPS]
+COLS_PREDS = [(f"BlockPred{op}_Cols", op, "set") for op in PRED_OPS] + \
+             [(f"BlockPredA{op}_Cols", op, "and") for op in PRED_OPS] + \
+             [(f"BlockPredOr{op}_Cols", op, "or") for op in PRED_OPS]
+
+
+@pytest.fixture(scope="module")
+def predlib(tmp_path_factory):
+    if not os.path.exists(GXX):
+        pytest.skip("needs a host C++ compiler")
+    src = HEADER.read_text()
+    prelude = src[src.index("#if defined(__CUDACC_RTC__)"):src.index("}  // namespace cx_detail") + 26]
+    preds = src[src.index("// ------------------------------------------------------------- predicates ---"):
+                src.index("// ------------------------------------------------- perfect hash tables (PHT) ---")]
+    parts = ["#define CX_DEVICE inline", prelude, preds]  # also marks the functors' members: no `static`
+    for name, _, _ in LITERAL_PREDS:
+        parts.append(f'extern "C" void lit_{name}(int tid, int n, const int* it, int c, int* fl) {{ int items[4], flags[4];'
+                     f" for (int i = 0; i < 4; ++i) {{ items[i] = it[i]; flags[i] = fl[i]; }}"
+                     f" {name}<int, 32, 4>(tid, items, flags, c, n); for (int i = 0; i < 4; ++i) fl[i] = flags[i]; }}")
+    for name, _, _ in COLS_PREDS:
+        parts.append(f'extern "C" void col_{name}(int tid, int n, const int* a, const int* b, int* fl) {{'
+                     f" int x[4], y[4], flags[4]; for (int i = 0; i < 4; ++i) {{ x[i] = a[i]; y[i] = b[i]; flags[i] = fl[i]; }}"
+                     f" {name}<int, 32, 4>(tid, x, y, flags, n); for (int i = 0; i < 4; ++i) fl[i] = flags[i]; }}")
+    d = tmp_path_factory.mktemp("preds")
+    cpp, so = d / "preds.cpp", d / "libpreds.so"
+    cpp.write_text("\n".join(parts) + "\n")
+    subprocess.run([GXX, "-O1", "-std=c++17", "-shared", "-fPIC", "-Wno-unknown-pragmas", "-o", str(so), str(cpp)],
+                   check=True)
+    return ctypes.CDLL(str(so))
+
+
+def _cmp(op: str, x: int, y: int) -> bool:
+    return {"LT": x < y, "GT": x > y, "LTE": x <= y, "GTE": x >= y, "Eq": x == y, "NEq": x != y}[op]
+
+
+def _combine(mode: str, flag: int, p: bool) -> int:
+    return int(p) if mode == "set" else int(bool(flag) and p) if mode == "and" else int(bool(flag) or p)
+
+
+@pytest.mark.parametrize("cols", [False, True])
+def test_block_predicates_follow_the_reference_combine_rules(predlib, cols):
+    """`BlockPred*` set the flag, `BlockPredA*` AND into it, `BlockPredO*` /
+    `BlockPredOr*` OR into it, for items inside the tile (a full tile: all;
+    else item i of thread tid when i * 32 + tid < num_items); other items keep
+    their flag.  Literal and column-vs-column forms (pred.h:153-445)."""
+    rng = random.Random(5 + cols)
+    ip = ctypes.POINTER(ctypes.c_int)
+    for name, op, mode in (COLS_PREDS if cols else LITERAL_PREDS):
+        fn = getattr(predlib, ("col_" if cols else "lit_") + name)
+        fn.argtypes = [ctypes.c_int, ctypes.c_int, ip, ip, ip] if cols else [ctypes.c_int, ctypes.c_int, ip, ctypes.c_int, ip]
+        for _ in range(100):
+            tid = rng.randrange(32)
+            n = 128 if rng.random() < 0.4 else rng.randint(0, 128)
+            a = np.array([rng.randint(-3, 3) for _ in range(4)], dtype=np.int32)
+            b = np.array([rng.randint(-3, 3) for _ in range(4)], dtype=np.int32)
+            c = rng.randint(-3, 3)
+            flags = np.array([rng.choice((0, 1, 2)) for _ in range(4)], dtype=np.int32)
+            want = flags.copy()
+            for i in range(4):
+                if n == 128 or i * 32 + tid < n:
+                    want[i] = _combine(mode, int(flags[i]), _cmp(op, int(a[i]), int(b[i]) if cols else c))
+            if cols:
+                fn(tid, n, a.ctypes.data_as(ip), b.ctypes.data_as(ip), flags.ctypes.data_as(ip))
+            else:
+                fn(tid, n, a.ctypes.data_as(ip), c, flags.ctypes.data_as(ip))
+            assert np.array_equal(flags, want), (name, tid, n, a, b, c, flags, want)

@@ -8,7 +8,7 @@ lane vector), the PHT build and probe cores and the `BlockPred*` predicates are
 plain C++ once `CX_DEVICE` is defined for the host: their source is taken from
 the header as it ships, compiled with g++, and compared with the reference
 semantics they must keep -- the PHT build and probe of
-`include/crystal/join.h:7-160` (a key is a member when the slot `HASH` gives
+`include/crystal/join.h:3-250` (a key is a member when the slot `HASH` gives
 holds it), `ColumnValidAt` of `include/crystal/load.h:72-76` (bit r of the
 uint64 word array) and the set / AND / OR rules of `include/crystal/pred.h`.
 """
@@ -197,7 +197,9 @@ def test_vector_validity_bits_match_column_valid_at(lib, ipt):
 def test_pht_build_then_probe_match_the_reference_rules(lib, pair):
     """Build (`BlockBuildSelectivePHT_1/2`: compare-and-swap of the key into
     the slot `HASH` gives; a pair slot takes the payload when the slot was empty
-    or already held the key) then probe (`BlockProbeAndPHT_1/2`: a member when
+    or already held the key -- the reference writes it unconditionally, which
+    differs only when two build keys share a slot, a documented divergence)
+    then probe (`BlockProbeAndPHT_1/2`: a member when
     the slot holds the key, the payload read beside it), item by item in the
     same order as a sequential model; keys around and outside the window,
     partial tiles, flags cleared or of any value, odd table addresses (no

@@ -4,7 +4,9 @@
 #include <algorithm>
 #include <cctype>
 #include <cstdlib>
+#include <cstring>
 #include <functional>
+#include <set>
 
 namespace cx {
 
@@ -86,6 +88,78 @@ long long to_int(const Node& n, const char* what) {
 const std::string& to_name(const Node& n, const char* what) {
   if (!n.atom) throw PlanError(std::string("expected name for ") + what);
   return n.text;
+}
+
+// Column names become identifiers of the generated kernels (one register
+// array per column, plus names derived from it), so a name must be a C
+// identifier that is not a C++ keyword, a CUDA built-in, a name of this
+// library's primitives, or one of the generated code's own identifiers
+// (fixed names, and numbered temporaries such as gt3 or x5_).
+void check_column_name(const std::string& c) {
+  static const std::set<std::string> reserved = {
+      // C++ keywords
+      "alignas", "alignof", "and", "and_eq", "asm", "auto", "bitand", "bitor", "bool", "break", "case", "catch",
+      "char", "char8_t", "char16_t", "char32_t", "class", "compl", "concept", "const", "consteval", "constexpr",
+      "constinit", "const_cast", "continue", "co_await", "co_return", "co_yield", "decltype", "default", "delete",
+      "do", "double", "dynamic_cast", "else", "enum", "explicit", "export", "extern", "false", "float", "for",
+      "friend", "goto", "if", "inline", "int", "long", "mutable", "namespace", "new", "noexcept", "not", "not_eq",
+      "nullptr", "operator", "or", "or_eq", "private", "protected", "public", "register", "reinterpret_cast",
+      "requires", "return", "short", "signed", "sizeof", "static", "static_assert", "static_cast", "struct",
+      "switch", "template", "this", "thread_local", "throw", "true", "try", "typedef", "typeid", "typename",
+      "union", "unsigned", "using", "virtual", "void", "volatile", "wchar_t", "while", "xor", "xor_eq",
+      // CUDA built-ins and types, namespaces and primitives of the generated code
+      "threadIdx", "blockIdx", "blockDim", "gridDim", "warpSize", "int2", "int4", "uint2", "uint4", "int32_t",
+      "int64_t", "uint32_t", "uint64_t", "size_t", "std", "db", "cx", "cx_detail", "HASH", "CxArgs", "InitFlags",
+      "InitFlagsZero", "ColumnValidAt", "ProbePHT_1", "ProbePHT_2", "ProbeMultiHT", "GreaterThan", "LessThan",
+      "GreaterThanEq", "LessThanEq", "Equal", "NotEqual", "PromoteType", "Promoted",
+      // fixed identifiers of the generated kernels
+      "BLOCK_THREADS", "IPT", "ITEMS_PER_THREAD", "NWARP", "NSTAGE", "NSC", "TILE_SIZE", "TROWS", "VW", "TR",
+      "aborted", "act", "amask", "any_", "avg_", "bad_", "bar_empty", "bar_full", "bar_ready", "bars", "base",
+      "bb_", "bits", "blk_", "blo_", "bm_", "bw_", "carry", "cg_", "cnt_", "cs_", "cu_", "cw", "cw_", "cx_smem",
+      "d_", "d_result", "d_result_validity", "d_visible_result", "d_visible_validity", "dkm", "dst_", "ent",
+      "es_", "ex", "f_", "fk_", "flags", "full_tiles", "fv_", "g_touch", "gd_", "gm_", "gwarp", "hash", "hi_",
+      "hit_", "ht", "ht_dir", "in_", "k_iter", "key", "kk", "l2_policy", "lane", "leader", "live", "live_", "lo_",
+      "loc", "lpb_", "m_", "m_cols", "m_res", "mht_bsum", "mht_counts", "mht_offsets", "mht_payload", "mht_wpos",
+      "mk_", "mst_", "n16_", "n_", "n_rows", "n_tile", "nblk", "nc_", "nch", "need", "ni", "nq", "nq_", "nt",
+      "ntiles", "num_tile_items", "num_tiles", "nv", "nw", "nwarps", "o_", "ok_", "okm_", "old_", "oow", "ow_",
+      "p_", "pass", "peers", "peers_", "per_", "perb_", "pos_", "pw", "q_", "q_base", "q_n", "qbits", "qtab",
+      "qw_", "r_", "red", "rel", "rel_", "rem", "rest_", "ri_", "row_ids", "rtouch", "run", "rv_", "s_", "s_abort",
+      "s_acc", "s_acc_all", "s_attr", "s_bits", "s_cube", "s_dim", "s_fm", "s_fr", "s_gm", "s_gm_t", "s_lacc",
+      "s_nissued", "s_nj", "s_params", "s_qacc", "s_qb", "s_qb_t", "s_seen", "s_seen_all", "s_shape", "s_tab",
+      "s_touch", "s_touch_all", "sc", "sd_", "seen_", "sh_", "slices", "slot", "src", "src_", "stage",
+      "stage_buf", "stage_tx", "staged", "staged_ok", "t_", "tacc", "tid", "tile", "tile_offset", "timed_out",
+      "tot", "touch_all", "touched_", "ttouch", "units", "v_", "vec_ok", "w_", "wg_", "wh_", "wi_", "wl_", "x_",
+      "y_"};
+  auto bad = [&](const char* why) {
+    throw PlanError("column name '" + c + "' " + why + "; rename the column");
+  };
+  if (c.empty() || !(std::isalpha((unsigned char)c[0]) || c[0] == '_')) bad("is not a C identifier");
+  for (char ch : c)
+    if (!(std::isalnum((unsigned char)ch) || ch == '_')) bad("is not a C identifier");
+  if (c.size() == 1) bad("is a one-letter name, which the generated kernels use");
+  if (c[0] == '_' && (c.size() < 2 || c[1] == '_' || std::isupper((unsigned char)c[1]))) bad("is a reserved identifier");
+  if (reserved.count(c)) bad("collides with an identifier of the generated kernels");
+  auto prefixed = [&](const char* pre) {
+    const size_t n = std::strlen(pre);
+    return c.size() > n && c.compare(0, n, pre) == 0 && std::isupper((unsigned char)c[n]);
+  };
+  if (prefixed("Block") || prefixed("Warp") || prefixed("atomic") || c.compare(0, 3, "cx_") == 0 ||
+      c.compare(0, 3, "CX_") == 0 || c.compare(0, 2, "__") == 0)
+    bad("collides with this library's primitives");
+  // Numbered temporaries: a short stem, digits, optionally _digits and a trailing underscore.
+  static const char* stems[] = {"gt", "gd", "x", "v", "h", "k", "e", "w", "g", "cl", "o", "j", "b", "s", "at",
+                                "off", "acc_", "seen_", "t", "c", "l", "fb", "fw", "m", "p", "r", "q", "y", "z"};
+  for (const char* st : stems) {
+    const size_t n = std::strlen(st);
+    if (c.size() <= n || c.compare(0, n, st) != 0 || !std::isdigit((unsigned char)c[n])) continue;
+    size_t i = n;
+    while (i < c.size() && std::isdigit((unsigned char)c[i])) ++i;
+    if (i < c.size() && c[i] == '_') {
+      ++i;
+      while (i < c.size() && std::isdigit((unsigned char)c[i])) ++i;
+    }
+    if (i == c.size()) bad("has the form of a numbered temporary of the generated kernels");
+  }
 }
 
 // (key value) lookup inside a list node.
@@ -214,7 +288,10 @@ std::unique_ptr<Plan> parse_plan(const std::string& text) {
       for (size_t k = 2; k < n.items.size(); ++k) {
         if (n.items[k].atom && n.items[k].text == "fact") t.fact = true;
         else if (head(n.items[k]) == "cols")
-          for (size_t c = 1; c < n.items[k].items.size(); ++c) t.cols.push_back(to_name(n.items[k].items[c], "cols"));
+          for (size_t c = 1; c < n.items[k].items.size(); ++c) {
+            t.cols.push_back(to_name(n.items[k].items[c], "cols"));
+            check_column_name(t.cols.back());
+          }
         else throw PlanError("unexpected item in (table " + t.name + " ...)");
       }
       if (p->table_slot(t.name) >= 0) throw PlanError("table declared twice: " + t.name);
@@ -367,6 +444,15 @@ std::unique_ptr<Plan> parse_plan(const std::string& text) {
   for (const auto& g : p->groups) check(g.expr.get(), visible, "GROUP BY");
   for (const auto& a : p->aggs) check(a.arg.get(), visible, "aggregate");
   if (p->group_count() > (1ULL << 31)) throw PlanError("group domain too large for a perfect hash");
+  {
+    // A column X_valid would share its name with the validity register of a column X.
+    std::set<std::string> all;
+    for (const auto& t : p->tables) all.insert(t.cols.begin(), t.cols.end());
+    for (const auto& c : all)
+      if (c.size() > 6 && c.compare(c.size() - 6, 6, "_valid") == 0 && all.count(c.substr(0, c.size() - 6)))
+        throw PlanError("column name '" + c + "' collides with the validity register of column '" +
+                        c.substr(0, c.size() - 6) + "'; rename the column");
+  }
   return p;
 }
 

@@ -134,28 +134,29 @@ extern "C" __global__ void ref_style(int* d_lo_quantity, int* d_lo_orderdate, in
 
 def test_bad_plans_return_invalid_status():
     with pytest.raises(_lib.CxError) as e:
-        _lib.codegen("(query (table T fact (cols a)) (filter (col nope)) (aggregate (count (star))))")
+        _lib.codegen("(query (table T fact (cols qty)) (filter (col nope)) (aggregate (count (star))))")
     assert e.value.code == -1 and "nope" in str(e.value)
     with pytest.raises(_lib.CxError):
-        _lib.codegen("(query (table T fact (cols a)))")  # no aggregate
+        _lib.codegen("(query (table T fact (cols qty)))")  # no aggregate
     with pytest.raises(_lib.CxError):
-        _lib.codegen("(query (table T fact (cols a)) (aggregate (group (add (col a) (int 1)) (min 0) (card 2)) (count (star))))")
+        _lib.codegen("(query (table T fact (cols qty)) (aggregate (group (add (col qty) (int 1)) (min 0) (card 2)) "
+                     "(count (star))))")
     with pytest.raises(_lib.CxError) as e:
         _lib.Module("__global__ void k() {}")
     assert e.value.code == -1
 
 
 def test_bad_or_and_multi_value_joins_are_rejected():
-    base = ("(query (table F fact (cols f1 f2 f3 v)) (table D (cols k p q)) {join} "
-            "(aggregate (sum (col v))))")
-    ok = "(join D (pk k) (fk f1 f2) (len 10) (keymin 0) (multi 1) (payload p q))"
+    base = ("(query (table F fact (cols f1 f2 f3 val)) (table D (cols dkey pay1 pay2)) {join} "
+            "(aggregate (sum (col val))))")
+    ok = "(join D (pk dkey) (fk f1 f2) (len 10) (keymin 0) (multi 1) (payload pay1 pay2))"
     _lib.codegen(base.format(join=ok))
     bad = {
-        "(join D (pk k) (fk f1 f1) (len 10) (keymin 0))": "listed twice",
-        "(join D (pk k) (fk f1 f2 f3 f1 f2) (len 10) (keymin 0))": "at most 4",
-        "(join D (pk k) (fk f1) (len 10) (keymin 0) (payload p q))": "one payload",
-        "(join D (pk k) (fk f1) (len 10) (keymin 0) (multi 1) (payload p p))": "listed twice",
-        "(join D (pk k) (fk f1) (len 10) (keymin 0) (multi 1) (payload zz))": "not a column",
+        "(join D (pk dkey) (fk f1 f1) (len 10) (keymin 0))": "listed twice",
+        "(join D (pk dkey) (fk f1 f2 f3 f1 f2) (len 10) (keymin 0))": "at most 4",
+        "(join D (pk dkey) (fk f1) (len 10) (keymin 0) (payload pay1 pay2))": "one payload",
+        "(join D (pk dkey) (fk f1) (len 10) (keymin 0) (multi 1) (payload pay1 pay1))": "listed twice",
+        "(join D (pk dkey) (fk f1) (len 10) (keymin 0) (multi 1) (payload zz))": "not a column",
     }
     for join, msg in bad.items():
         with pytest.raises(_lib.CxError) as e:

@@ -29,7 +29,7 @@ import pytest
 from practice_b200 import _lib
 from practice_b200.plan import PlanBuilder, Table, and_, case, col, lit, not_, or_, star
 
-COLS = ("a", "b", "c")
+COLS = ("qty", "price", "disc")
 VALUES = (-2, 0, 1, 3, 5)
 PREFIX = "flags[i] = (tid + BLOCK_THREADS * i < num_tile_items) ? ((int)(flags[i] != 0) & (int)(bool)("
 SUFFIX = ")) : flags[i];"
@@ -141,9 +141,9 @@ def _compile(funcs: list[list[str]], tmp_path) -> ctypes.CDLL:
                     "const int* C, const int* CV, int* out) {")
         body.append("  for (int r = 0; r < n; ++r) {")
         body.append("    const int i = 0;")
-        body.append("    int a[1] = {A[r]}, a_valid[1] = {AV[r]}, b[1] = {B[r]}, b_valid[1] = {BV[r]};")
-        body.append("    int c[1] = {C[r]}, c_valid[1] = {CV[r]};")
-        body.append("    (void)a; (void)a_valid; (void)b; (void)b_valid; (void)c; (void)c_valid; (void)i;")
+        body.append("    int qty[1] = {A[r]}, qty_valid[1] = {AV[r]}, price[1] = {B[r]}, price_valid[1] = {BV[r]};")
+        body.append("    int disc[1] = {C[r]}, disc_valid[1] = {CV[r]};")
+        body.append("    (void)qty; (void)qty_valid; (void)price; (void)price_valid; (void)disc; (void)disc_valid; (void)i;")
         body.append("    int keep = 1;")
         for cond in conds:
             body.append(f"    keep &= (int)(bool)({cond});")
@@ -196,3 +196,28 @@ def test_emitted_filters_follow_three_valued_logic(tmp_path):
         kept_any += int(want.any())
         dropped_any += int((want == 0).any())
     assert kept_any > 20 and dropped_any > 20  # the predicates are not trivially constant
+
+
+@pytest.mark.parametrize("name", ["a", "flags", "tid", "hash", "int", "threadIdx", "BlockLoad", "gt3", "x5_", "h0_1",
+                                  "acc_2", "__x", "atomicAdd", "2col", "lo-rev"])
+def test_column_names_that_collide_with_generated_identifiers_are_rejected(name):
+    """A column name that the generated kernels already use (or that is not a
+    C identifier) would make NVRTC fail with an unrelated message; the plan
+    reader rejects it and names the column."""
+    t = {"T": Table("T", ["lo_quantity", name], 1000, fact=True)}
+    plan = PlanBuilder(t, "T", name="reserved").aggregate([], [("count", star())])
+    with pytest.raises(_lib.CxError) as e:
+        _lib.codegen(plan.text())
+    assert e.value.code == -1 and name in str(e.value)  # CX_E_INVALID
+
+
+def test_validity_register_collision_is_rejected_and_plain_names_compile():
+    t = {"T": Table("T", ["qty", "qty_valid"], 1000, fact=True)}
+    plan = PlanBuilder(t, "T", nullable={"qty"}, name="v").filter(col("qty").gt(lit(1))).aggregate(
+        [], [("count", star())])
+    with pytest.raises(_lib.CxError, match="qty_valid"):
+        _lib.codegen(plan.text())
+    t = {"T": Table("T", list(COLS), 1000, fact=True)}
+    plan = PlanBuilder(t, "T", nullable={"qty"}, name="ok").filter(col("qty").gt(lit(1))).aggregate(
+        [], [("count", star())])
+    _lib.Module(_lib.codegen(plan.text()), key="plain_names_compile")
